@@ -1,0 +1,375 @@
+"""Synthetic CTurboBFM cases: structured grids, BFM input fields, boundary patches
+and input.ini settings, written in the reference's file formats.
+
+File formats follow the reference:
+  * grid CSV: ``NI=``/``NJ=``/``NK=`` header lines, a ``x,y,z[,field...]``
+    header, then one row per node in i-major, k-fastest order
+    (src/input.cpp:14-82);
+  * ``boundaries.csv``: lines containing ``=`` are skipped, a header line
+    containing ``PATCH_NAME``, then ``NAME,I_MIN,I_MAX,J_MIN,J_MAX,K_MIN,K_MAX``
+    in node indices (src/solver.cpp:232-294);
+  * ``input.ini``: ``KEY = value`` lines, ``;`` comments (src/config.cpp:15-44).
+
+The workloads are seeded synthetic stand-ins for the reference's validation
+geometries; no data set is involved.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+# Names of the per-node input fields the grid CSV may carry
+# (include/types.hpp:1036-1078). Only the ones the hot path reads are used.
+BFM_FIELDS = (
+    "blockage",
+    "normalAxial",
+    "normalRadial",
+    "normalTangential",
+    "rpm",
+    "streamwiseLength",
+    "bladePresent",
+    "numberBlades",
+    "bladeMetalAngle",
+    "bladeGasPathAngle",
+    "bladeLeanAngle",
+)
+
+
+@dataclasses.dataclass
+class Patch:
+    name: str
+    i_min: int
+    i_max: int
+    j_min: int
+    j_max: int
+    k_min: int
+    k_max: int
+    spec: str  # right-hand side of the INI patch line, e.g. "inlet, 101325, 288.15, 1, 0, 0"
+
+    @property
+    def kind(self) -> str:
+        return self.spec.split(",")[0].strip().lower()
+
+    @property
+    def values(self) -> List[float]:
+        parts = [p.strip() for p in self.spec.split(",")[1:]]
+        return [float(p) for p in parts if p]
+
+
+@dataclasses.dataclass
+class Case:
+    """One operating point: grid, fields, patches and solver settings."""
+
+    name: str
+    x: np.ndarray  # (NI, NJ, NK) float64
+    y: np.ndarray
+    z: np.ndarray
+    fields: Dict[str, np.ndarray]
+    patches: List[Patch]
+    settings: Dict[str, str]
+
+    @property
+    def shape(self) -> Tuple[int, int, int]:
+        return tuple(int(s) for s in self.x.shape)  # type: ignore[return-value]
+
+    @property
+    def n_nodes(self) -> int:
+        ni, nj, nk = self.shape
+        return ni * nj * nk
+
+    @property
+    def n_stages(self) -> int:
+        ti = self.settings.get("TIME_INTEGRATION_TYPE", "0").strip().lower()
+        return 3 if ti in ("1", "rk3", "explicit_rk3", "runge_kutta_3") else 4
+
+    def with_settings(self, **kw: str) -> "Case":
+        s = dict(self.settings)
+        s.update({k: str(v) for k, v in kw.items()})
+        return dataclasses.replace(self, settings=s)
+
+    # -- file output ------------------------------------------------------
+    def write(self, directory: str) -> str:
+        """Writes grid.csv, boundaries.csv and input.ini; returns the ini path."""
+        os.makedirs(directory, exist_ok=True)
+        ni, nj, nk = self.shape
+        names = ["x", "y", "z"] + list(self.fields.keys())
+        cols = [self.x, self.y, self.z] + [self.fields[n] for n in self.fields]
+        data = np.stack([c.reshape(-1) for c in cols], axis=1)
+        with open(os.path.join(directory, "grid.csv"), "w") as f:
+            f.write(f"NDIMENSIONS={3 if nk > 1 else 2}\nNI={ni}\nNJ={nj}\nNK={nk}\n")
+            f.write(",".join(names) + "\n")
+            np.savetxt(f, data, fmt="%.17g", delimiter=",")
+        with open(os.path.join(directory, "boundaries.csv"), "w") as f:
+            f.write(f"NI={ni}\nNJ={nj}\nNK={nk}\n")
+            f.write("PATCH_NAME,I_MIN,I_MAX,J_MIN,J_MAX,K_MIN,K_MAX\n")
+            for p in self.patches:
+                f.write(f"{p.name},{p.i_min},{p.i_max},{p.j_min},{p.j_max},{p.k_min},{p.k_max}\n")
+        settings = dict(self.settings)
+        settings["GRID_FILE"] = "grid.csv"
+        settings["BOUNDARY_CONDITIONS_FILEPATH"] = "boundaries.csv"
+        for p in self.patches:
+            settings[p.name] = p.spec
+        ini = os.path.join(directory, "input.ini")
+        with open(ini, "w") as f:
+            f.write("[CFD]\n")
+            for k, v in settings.items():
+                f.write(f"{k} = {v}\n")
+        return ini
+
+
+def _base_settings(topology: str) -> Dict[str, str]:
+    return {
+        "SOLUTION_NAME": "results",
+        "RESTART_SOLUTION": "no",
+        "KIND_SOLVER": "Euler",
+        "TOPOLOGY": topology,
+        "FLUID_GAMMA": "1.4",
+        "FLUID_NAME": "Air",
+        "FLUID_MODEL": "Ideal",
+        "FLUID_R_CONSTANT": "287.05",
+        "INIT_DIRECTION": "1, 0, 0",
+        "SAVE_UNSTEADY": "no",
+        "SAVE_ITERATIONS_INTERVAL": "1000000",
+        "HISTORY_BUFFER_SIZE": "1000000",
+        "RESIDUALS_DROP_CONVERGENCE": "16",
+        "TIME_INTEGRATION_TYPE": "0",
+        "TIME_STEP_METHOD": "local",
+        "CONVECTION_SCHEME": "JST",
+        "MUSCL_RECONSTRUCTION": "no",
+        "FLUX_LIMITER": "None",
+        "OUTPUT_FIELDS_TYPE": "primary",
+    }
+
+
+def static_state(pt: float, tt: float, mach: float, gamma: float = 1.4) -> Tuple[float, float]:
+    """Isentropic static pressure and temperature for a Mach number."""
+    f = 1.0 + 0.5 * (gamma - 1.0) * mach * mach
+    return pt * f ** (-gamma / (gamma - 1.0)), tt / f
+
+
+def _tanh_cluster(n: int, beta: float) -> np.ndarray:
+    """Two-sided tanh clustering of n points on [0, 1]."""
+    s = np.linspace(-1.0, 1.0, n)
+    return 0.5 * (1.0 + np.tanh(beta * s) / math.tanh(beta))
+
+
+def bump2d(ni: int = 192, nj: int = 64, n_iter: int = 5000, cfl: float = 2.0,
+           scheme: str = "JST", muscl: bool = False, limiter: str = "None",
+           rk: int = 4, mach: float = 0.5, name: str = "bump2d") -> Case:
+    """Circular-arc bump channel: length 3, height 1, 10%-thick arc on the lower
+    wall between x = 1 and x = 2; uniform in x, two-sided tanh wall clustering
+    (beta = 2) in y; total-condition inlet, static outlet for inlet Mach, walls."""
+    radius = (0.25 + 0.01) / 0.2
+    xs = np.linspace(0.0, 3.0, ni)
+    yb = np.where((xs >= 1.0) & (xs <= 2.0),
+                  np.sqrt(np.maximum(radius ** 2 - (xs - 1.5) ** 2, 0.0)) - (radius - 0.1), 0.0)
+    eta = _tanh_cluster(nj, 2.0)
+    x = np.repeat(xs[:, None], nj, axis=1)
+    y = yb[:, None] + (1.0 - yb[:, None]) * eta[None, :]
+    z = np.zeros_like(x)
+    x, y, z = (a[:, :, None].copy() for a in (x, y, z))
+    pt, tt = 101325.0, 288.15
+    ps, ts = static_state(pt, tt, mach)
+    s = _base_settings("2D")
+    s.update({
+        "INIT_MACH_NUMBER": f"{mach!r}",
+        "INIT_TEMPERATURE": f"{ts!r}",
+        "INIT_PRESSURE": f"{ps!r}",
+        "CFL": f"{cfl!r}",
+        "N_ITERATIONS": str(n_iter),
+        "TIME_INTEGRATION_TYPE": "0" if rk == 4 else "1",
+        "CONVECTION_SCHEME": scheme,
+        "MUSCL_RECONSTRUCTION": "yes" if muscl else "no",
+        "FLUX_LIMITER": limiter,
+    })
+    patches = [
+        Patch("INFLOW", 0, 0, 0, nj, 0, 1, f"inlet, {pt!r}, {tt!r}, 1, 0, 0"),
+        Patch("OUTFLOW", ni, ni, 0, nj, 0, 1, f"outlet, {ps!r}"),
+        Patch("LOWER_WALL", 0, ni, 0, 0, 0, 1, "inviscid_wall"),
+        Patch("UPPER_WALL", 0, ni, nj, nj, 0, 1, "inviscid_wall"),
+    ]
+    return Case(name, x, y, z, {}, patches, s)
+
+
+def _row_fields(xs: np.ndarray, rs: np.ndarray, rows, nk: int) -> Dict[str, np.ndarray]:
+    """BFM input fields for blade rows given as (x_le, x_te, kappa_hub_deg,
+    kappa_tip_deg, rpm, n_blades, max_blockage_loss) tuples. Blockage is
+    b = 1 - loss * sin^2(pi * xi) with xi the chordwise fraction, so its
+    gradient is non-zero inside a row; the metal angle varies linearly from hub
+    to tip; the camber normal is (-sin k, 0, cos k) in (axial, radial,
+    tangential) components."""
+    ni, nj = xs.size, rs.size
+    shape = (ni, nj, nk)
+    f = {n: np.zeros(shape) for n in BFM_FIELDS}
+    f["blockage"][:] = 1.0
+    span = (rs - rs[0]) / (rs[-1] - rs[0])
+    for (x_le, x_te, k_hub, k_tip, rpm, nb, loss) in rows:
+        inside = (xs >= x_le) & (xs <= x_te)
+        if not inside.any():
+            continue
+        xi = (xs - x_le) / (x_te - x_le)
+        kappa = np.deg2rad(k_hub + (k_tip - k_hub) * span)  # (nj,)
+        for i in np.nonzero(inside)[0]:
+            f["blockage"][i] = 1.0 - loss * math.sin(math.pi * xi[i]) ** 2
+            f["bladePresent"][i] = 1.0
+            f["numberBlades"][i] = nb
+            f["rpm"][i] = rpm
+            f["streamwiseLength"][i] = xs[i] - x_le
+            f["bladeMetalAngle"][i] = kappa[:, None]
+            f["normalAxial"][i] = -np.sin(kappa)[:, None]
+            f["normalTangential"][i] = np.cos(kappa)[:, None]
+    return f
+
+
+def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
+              cfl: float = 1.2, scheme: str = "Roe", muscl: bool = True,
+              limiter: str = "van albada", rk: int = 3, bfm_model: str = "Hall",
+              rpm: float = 10000.0, p_ratio: float = 1.15, mach: float = 0.3,
+              name: str = "annulus3d") -> Case:
+    """Full-annulus axial rotor + stator: hub radius 0.20 m, tip 0.40 m, axial
+    length 0.6 m; rotor at 0.2-0.3 m (blockage loss 0.4, metal angle magnitude
+    50 deg at hub to 60 deg at tip, negative in the solver's sign convention
+    for positive rpm), stator at 0.35-0.45 m. k = 0 and k = nk - 1 are 360
+    degree periodic duplicates (identical coordinates)."""
+    xs = np.linspace(0.0, 0.6, ni)
+    rs = np.linspace(0.20, 0.40, nj)
+    th = np.array([2.0 * math.pi * k / (nk - 1) for k in range(nk - 1)] + [0.0])
+    X = np.broadcast_to(xs[:, None, None], (ni, nj, nk)).copy()
+    R = np.broadcast_to(rs[None, :, None], (ni, nj, nk))
+    T = np.broadcast_to(th[None, None, :], (ni, nj, nk))
+    Y = R * np.cos(T)
+    Z = R * np.sin(T)
+    rows = [(0.2, 0.3, -50.0, -60.0, rpm, 24, 0.4),
+            (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
+    fields = _row_fields(xs, rs, rows, nk)
+    pt, tt = 101325.0, 288.15
+    ps, ts = static_state(pt, tt, mach)
+    s = _base_settings("3D")
+    s.update({
+        "BFM_ACTIVE": "yes",
+        "BLOCKAGE_ACTIVE": "yes",
+        "BFM_MODEL": bfm_model,
+        "HALL_THOLLET_COEFFICIENT_KN": "1.0",
+        "HALL_THOLLET_COEFFICIENT_KF": "1.0",
+        "HALL_THOLLET_COEFFICIENT_KD": "1.0",
+        "HALL_THOLLET_OFF_DESIGN_ACTIVE": "no",
+        "FLUID_KINEMATIC_VISCOSITY": "1.48E-5",
+        "INIT_MACH_NUMBER": f"{mach!r}",
+        "INIT_TEMPERATURE": f"{ts!r}",
+        "INIT_PRESSURE": f"{ps!r}",
+        "CFL": f"{cfl!r}",
+        "N_ITERATIONS": str(n_iter),
+        "TIME_INTEGRATION_TYPE": "0" if rk == 4 else "1",
+        "CONVECTION_SCHEME": scheme,
+        "MUSCL_RECONSTRUCTION": "yes" if muscl else "no",
+        "FLUX_LIMITER": limiter,
+        "TURBO_DIRECTION": "i",
+    })
+    patches = [
+        Patch("INFLOW", 0, 0, 0, nj, 0, nk, f"inlet, {pt!r}, {tt!r}, 1, 0, 0"),
+        Patch("OUTFLOW", ni, ni, 0, nj, 0, nk, f"outlet, {p_ratio * pt!r}"),
+        Patch("HUB", 0, ni, 0, 0, 0, nk, "inviscid_wall"),
+        Patch("SHROUD", 0, ni, nj, nj, 0, nk, "inviscid_wall"),
+        Patch("PER1", 0, ni, 0, nj, 0, 0, "periodic, 0, 0, 360.0"),
+        Patch("PER2", 0, ni, 0, nj, nk, nk, "periodic, 1, 0, 360.0"),
+    ]
+    return Case(name, X, Y, Z, fields, patches, s)
+
+
+def meridional(ni: int = 96, nj: int = 32, n_iter: int = 20000, cfl: float = 1.3,
+               p_ratio: float = 1.15, speed: float = 1.0, bfm_model: str = "Hall",
+               outlet: str = "outlet", drop: int = 8, mach: float = 0.3,
+               scheme: str = "JST", rk: int = 4, name: str = "meridional") -> Case:
+    """Axisymmetric meridional plane of the rotor/stator stage of annulus3d
+    (nk = 1; the solver builds a 1 degree wedge around it)."""
+    xs = np.linspace(0.0, 0.6, ni)
+    rs = np.linspace(0.20, 0.40, nj)
+    X = np.broadcast_to(xs[:, None, None], (ni, nj, 1)).copy()
+    Y = np.broadcast_to(rs[None, :, None], (ni, nj, 1)).copy()
+    Z = np.zeros_like(X)
+    rows = [(0.2, 0.3, -50.0, -60.0, 10000.0, 24, 0.4),
+            (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
+    fields = _row_fields(xs, rs, rows, 1)
+    pt, tt = 101325.0, 288.15
+    ps, ts = static_state(pt, tt, mach)
+    s = _base_settings("axisymmetric")
+    s.update({
+        "BFM_ACTIVE": "yes",
+        "BLOCKAGE_ACTIVE": "yes",
+        "BFM_MODEL": bfm_model,
+        "HALL_THOLLET_COEFFICIENT_KN": "1.0",
+        "HALL_THOLLET_COEFFICIENT_KF": "1.0",
+        "HALL_THOLLET_COEFFICIENT_KD": "1.0",
+        "HALL_THOLLET_OFF_DESIGN_ACTIVE": "no",
+        "FLUID_KINEMATIC_VISCOSITY": "1.48E-5",
+        "ROTATIONAL_SPEED_SCALING_FACTOR": f"{speed!r}",
+        "INIT_MACH_NUMBER": f"{mach!r}",
+        "INIT_TEMPERATURE": f"{ts!r}",
+        "INIT_PRESSURE": f"{ps!r}",
+        "CFL": f"{cfl!r}",
+        "N_ITERATIONS": str(n_iter),
+        "RESIDUALS_DROP_CONVERGENCE": str(drop),
+        "TIME_INTEGRATION_TYPE": "0" if rk == 4 else "1",
+        "CONVECTION_SCHEME": scheme,
+        "TURBO_OUTPUT": "yes",
+        "TURBO_DIRECTION": "i",
+    })
+    if outlet == "outlet":
+        out_spec = f"outlet, {p_ratio * pt!r}"
+    elif outlet == "radial_equilibrium":
+        out_spec = f"radial_equilibrium, {p_ratio * pt!r}"
+    else:
+        raise ValueError(outlet)
+    patches = [
+        Patch("INFLOW", 0, 0, 0, nj, 0, 1, f"inlet, {pt!r}, {tt!r}, 1, 0, 0"),
+        Patch("OUTFLOW", ni, ni, 0, nj, 0, 1, out_spec),
+        Patch("HUB", 0, ni, 0, 0, 0, 1, "inviscid_wall"),
+        Patch("SHROUD", 0, ni, nj, nj, 0, 1, "inviscid_wall"),
+    ]
+    return Case(name, X, Y, Z, fields, patches, s)
+
+
+def compressor_map(n: int = 256, seed: int = 20261203, ni_range=(64, 256),
+                   nj_range=(24, 96), p_ratio_range=(1.00, 1.35),
+                   speed_range=(0.70, 1.05), n_iter: int = 20000) -> List[Case]:
+    """The batched compressor-map workload: n axisymmetric meridional
+    instances with independently drawn grid sizes, back-pressure ratios and
+    shaft-speed scalings from a seeded PCG64 generator. Each runs JST + RK4 to
+    an 8-order residual drop."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for m in range(n):
+        ni = int(rng.integers(ni_range[0], ni_range[1] + 1))
+        nj = int(rng.integers(nj_range[0], nj_range[1] + 1))
+        pr = float(rng.uniform(*p_ratio_range))
+        sp = float(rng.uniform(*speed_range))
+        out.append(meridional(ni=ni, nj=nj, n_iter=n_iter, p_ratio=pr, speed=sp,
+                              drop=8, name=f"map{m:03d}"))
+    return out
+
+
+def read_grid_csv(path: str) -> Tuple[Tuple[int, int, int], Dict[str, np.ndarray]]:
+    """Reads a grid CSV in the reference's format (src/input.cpp:14-82)."""
+    ni = nj = nk = None
+    with open(path) as f:
+        while True:
+            line = f.readline()
+            if not line:
+                raise ValueError("no x,y,z header in " + path)
+            if line.startswith("NI="):
+                ni = int(line[3:])
+            elif line.startswith("NJ="):
+                nj = int(line[3:])
+            elif line.startswith("NK="):
+                nk = int(line[3:])
+            elif line.startswith("x,y,z"):
+                names = line.strip().split(",")
+                break
+        data = np.loadtxt(f, delimiter=",", ndmin=2)
+    shape = (ni, nj, nk)
+    return shape, {n: data[:, c].reshape(shape).copy() for c, n in enumerate(names)}

@@ -1,0 +1,2143 @@
+/* CPU oracle for the CTurboBFM explicit residual-and-update loop.
+ *
+ * TEST INFRASTRUCTURE ONLY (see ctbfm_oracle.h). A plain-C restatement of the
+ * reference's serial FP64 algorithm; every function cites the reference
+ * file:line it follows. Compiled with -ffp-contract=off so that each
+ * expression rounds exactly as the reference's does (pinned in tests against
+ * oracle/_ref/ref_harness, the reference built from its own sources).
+ *
+ * Scope: the explicit Runge-Kutta path for 2-D, axisymmetric and 3-D
+ * topologies, ideal gas, JST and Roe (+MUSCL) fluxes, inlet / outlet /
+ * throttle / radial-equilibrium / inviscid-wall / periodic / wedge boundaries,
+ * axisymmetric, blade-row geometric, Gong and BFM (Hall, Hall-Thollet,
+ * Lift-Drag, blockage) sources, local / global / fixed time steps, residual
+ * norms, convergence test, turbo performance and the Greitzer plenum.
+ */
+#define _GNU_SOURCE
+#include "ctbfm_oracle.h"
+
+#include <ctype.h>
+#include <errno.h>
+#include <float.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ errors */
+
+static char g_err[1024];
+
+static int fail(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return 1;
+}
+
+const char* oracle_last_error(void) { return g_err; }
+
+/* -------------------------------------------------------------- vector ops */
+/* Vector3D (include/types.hpp:15-125). Every operation keeps the reference's
+ * left-to-right evaluation order. */
+
+typedef struct { double x, y, z; } vec3;
+
+static vec3 v3(double x, double y, double z) { vec3 r = {x, y, z}; return r; }
+static vec3 vadd(vec3 a, vec3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static vec3 vsub(vec3 a, vec3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static vec3 vmul(vec3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
+static vec3 vdiv(vec3 a, double s) { return v3(a.x / s, a.y / s, a.z / s); }
+static vec3 vneg(vec3 a) { return v3(-a.x, -a.y, -a.z); }
+static double vdot(vec3 a, vec3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static double vmag(vec3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+static vec3 vnormalized(vec3 a) {
+    double m = vmag(a);
+    return (m == 0) ? v3(0, 0, 0) : vdiv(a, m);
+}
+static vec3 vcross(vec3 a, vec3 b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+/* StateVector (include/types.hpp:650-757). */
+typedef struct { double v[5]; } sv5;
+
+static sv5 sadd(sv5 a, sv5 b) { sv5 r; for (int i = 0; i < 5; i++) r.v[i] = a.v[i] + b.v[i]; return r; }
+static sv5 ssub(sv5 a, sv5 b) { sv5 r; for (int i = 0; i < 5; i++) r.v[i] = a.v[i] - b.v[i]; return r; }
+static sv5 smul(sv5 a, double s) { sv5 r; for (int i = 0; i < 5; i++) r.v[i] = a.v[i] * s; return r; }
+static sv5 sdiv(sv5 a, double s) { sv5 r; for (int i = 0; i < 5; i++) r.v[i] = a.v[i] / s; return r; }
+static sv5 szero(void) { sv5 r = {{0, 0, 0, 0, 0}}; return r; }
+
+static double dmax(double a, double b) { return (a < b) ? b : a; } /* std::max */
+static double dmin(double a, double b) { return (b < a) ? b : a; } /* std::min */
+
+/* ------------------------------------------------------------------ config */
+/* Config::load (src/config.cpp:15-44): "KEY = value", ';' and '[' lines
+ * skipped, keys exact-case, later keys overwrite earlier ones. */
+
+typedef struct { char* key; char* val; } kv;
+typedef struct { kv* items; int n, cap; } config;
+
+static void trim(char* s, const char* ws) {
+    size_t n = strlen(s), a = 0;
+    while (a < n && strchr(ws, s[a])) a++;
+    size_t b = n;
+    while (b > a && strchr(ws, s[b - 1])) b--;
+    memmove(s, s + a, b - a);
+    s[b - a] = 0;
+}
+
+static const char* cfg_get(const config* c, const char* key) {
+    for (int i = 0; i < c->n; i++)
+        if (strcmp(c->items[i].key, key) == 0) return c->items[i].val;
+    return NULL;
+}
+
+static void cfg_set(config* c, const char* key, const char* val) {
+    for (int i = 0; i < c->n; i++)
+        if (strcmp(c->items[i].key, key) == 0) {
+            free(c->items[i].val);
+            c->items[i].val = strdup(val);
+            return;
+        }
+    if (c->n == c->cap) {
+        c->cap = c->cap ? 2 * c->cap : 64;
+        c->items = (kv*)realloc(c->items, sizeof(kv) * c->cap);
+    }
+    c->items[c->n].key = strdup(key);
+    c->items[c->n].val = strdup(val);
+    c->n++;
+}
+
+static int cfg_load(config* c, const char* path) {
+    FILE* f = fopen(path, "r");
+    if (!f) return fail("Failed to load configuration file: %s", path);
+    char line[4096];
+    while (fgets(line, sizeof line, f)) {
+        trim(line, " \t\r\n");
+        if (!line[0] || line[0] == ';' || line[0] == '[') continue;
+        char* eq = strchr(line, '=');
+        if (!eq) continue;
+        *eq = 0;
+        char key[4096], val[4096];
+        snprintf(key, sizeof key, "%s", line);
+        snprintf(val, sizeof val, "%s", eq + 1);
+        trim(key, " \t");
+        trim(val, " \t");
+        cfg_set(c, key, val);
+    }
+    fclose(f);
+    return 0;
+}
+
+static void cfg_free(config* c) {
+    for (int i = 0; i < c->n; i++) { free(c->items[i].key); free(c->items[i].val); }
+    free(c->items);
+    memset(c, 0, sizeof *c);
+}
+
+/* std::stod semantics: leading blanks skipped, at least one digit consumed. */
+static int parse_double(const char* s, double* out) {
+    char* end;
+    errno = 0;
+    double v = strtod(s, &end);
+    if (end == s) return 1;
+    *out = v;
+    return 0;
+}
+
+static int cfg_float(const config* c, const char* key, double* out) {
+    const char* v = cfg_get(c, key);
+    if (!v) return fail("Not found value for key \"%s\" in configuration.", key);
+    if (parse_double(v, out)) return fail("Invalid float format for key \"%s\": \"%s\"", key, v);
+    return 0;
+}
+
+static int cfg_float_def(const config* c, const char* key, double def, double* out) {
+    if (!cfg_get(c, key)) { *out = def; return 0; }
+    return cfg_float(c, key, out);
+}
+
+static int cfg_int_def(const config* c, const char* key, int def, int* out) {
+    double d;
+    if (!cfg_get(c, key)) { *out = def; return 0; }
+    if (cfg_float(c, key, &d)) return 1;
+    *out = (int)d;
+    return 0;
+}
+
+/* Config::parseBool (src/config.cpp:141-159). */
+static int cfg_bool(const config* c, const char* key, int def, int* out) {
+    const char* v = cfg_get(c, key);
+    if (!v) { *out = def; return 0; }
+    char low[256];
+    snprintf(low, sizeof low, "%s", v);
+    for (char* p = low; *p; p++) *p = (char)tolower((unsigned char)*p);
+    if (!strcmp(low, "true") || !strcmp(low, "yes") || !strcmp(low, "1")) { *out = 1; return 0; }
+    if (!strcmp(low, "false") || !strcmp(low, "no") || !strcmp(low, "0")) { *out = 0; return 0; }
+    return fail("Invalid value for key \"%s\" in configuration.", key);
+}
+
+/* Config::parseVector<std::string> (include/config.hpp:29-51): comma
+ * separated, items trimmed, empty items dropped. */
+static int cfg_list(const config* c, const char* key, char items[][128], int max_items) {
+    const char* v = cfg_get(c, key);
+    if (!v) return -1;
+    int n = 0;
+    char buf[4096];
+    snprintf(buf, sizeof buf, "%s", v);
+    char* save = NULL;
+    /* strtok_r would merge empty fields; the reference drops empty items too. */
+    for (char* tok = strtok_r(buf, ",", &save); tok; tok = strtok_r(NULL, ",", &save)) {
+        char item[1024];
+        snprintf(item, sizeof item, "%s", tok);
+        trim(item, " \t\r\n");
+        if (!item[0]) continue;
+        if (n < max_items) snprintf(items[n], 128, "%s", item);
+        n++;
+    }
+    return n;
+}
+
+/* ------------------------------------------------------------------- enums */
+
+enum { TOPO_2D = 0, TOPO_3D = 1, TOPO_AXI = 2, TOPO_1D = 3 };
+enum { SCHEME_JST = 0, SCHEME_ROE = 1 };
+enum { LIM_NONE = 0, LIM_VAN_ALBADA, LIM_VAN_LEER, LIM_MIN_MOD };
+enum { DT_LOCAL = 0, DT_GLOBAL, DT_FIXED };
+enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE };
+/* BoundaryType (include/types.hpp:178-194), restricted to the types on the path. */
+enum {
+    BC_INLET = 0, BC_OUTLET, BC_RADIAL_EQ, BC_INVISCID_WALL, BC_WEDGE, BC_PERIODIC, BC_THROTTLE,
+    BC_EMPTY
+};
+enum { BI_ISTART = 0, BI_IEND, BI_JSTART, BI_JEND, BI_KSTART, BI_KEND };
+
+/* ---------------------------------------------------------------- solver */
+
+typedef struct {
+    char name[128];
+    int type;
+    double values[16];
+    int nvalues;
+    long i_min, i_max, j_min, j_max, k_min, k_max;
+    int orientation;
+    int profile; /* index into the radial profiles for throttle / radial equilibrium */
+} patch;
+
+typedef struct {
+    double* pressure; /* size n */
+    double* radius;   /* size n or 0 */
+    int n, nradius;
+    int patch;
+} radial_profile;
+
+enum {
+    F_BLOCKAGE = 0, F_NAX, F_NRAD, F_NTAN, F_RPM, F_STWL, F_BLADE_PRESENT, F_NBLADES, F_METAL,
+    F_GASPATH, F_LEAN, F_DEV_PIVOT, F_DEV_STALL, F_LD_BETA0, F_LD_KP, F_COUNT
+};
+static const char* FIELD_NAMES[F_COUNT] = {
+    "blockage", "normalAxial", "normalRadial", "normalTangential", "rpm", "streamwiseLength",
+    "bladePresent", "numberBlades", "bladeMetalAngle", "bladeGasPathAngle", "bladeLeanAngle",
+    "deviationAnglePivot", "deviationAngleStall", "liftDragBeta0", "liftDragKpEtamax"};
+
+struct oracle_solver {
+    config cfg;
+    long ni, nj, nk, n;
+    int topology, ndim;
+    /* settings */
+    int scheme, muscl, limiter, nstages, dt_method, steady, drop;
+    double coeffs[4], cfl, fixed_dt, gamma, rgas, cp;
+    int bfm_active, blockage_active, bfm_model, stalled, perturb;
+    double kn, kf, kd, nu;
+    int offdesign, has_nu;
+    double speed_scale;
+    int accel; double acc_t0, acc_t1, acc_s0, acc_s1;
+    double pert_center[3], pert_radius, pert_scale, pert_t0, pert_dur;
+    long le_idx, te_idx;
+    int inlet_cyl;
+    double ramp_iters, init_p;
+    int need_turbo;
+    int turbo_dir; /* bcIndices pair */
+    int greitzer;
+    double plenum_volume, ambient_p, gz_p, gz_min, gz_mout, gz_T, gz_t, throttle_kt;
+    /* mesh */
+    vec3* vert;  /* n */
+    vec3* dual;  /* (ni+1)(nj+1)(nk+1) */
+    vec3 *sI, *sJ, *sK, *cI, *cJ, *cK;
+    double* vol;
+    double wedge;
+    double* field[F_COUNT];
+    vec3* gradb;
+    int periodic;
+    double per_angle_rad, per_angle_deg, per_transl;
+    /* boundaries */
+    patch* patches;
+    int npatches;
+    int* mapI; /* 2 x nj x nk */
+    int* mapJ; /* ni x 2 x nk */
+    int* mapK; /* ni x nj x 2 */
+    radial_profile* profiles;
+    int nprofiles;
+    double hub_p;
+    /* state */
+    double *U[5], *Utmp[5], *R[5], *dt;
+    double t;
+    double massflow[6];
+    double turbo[4];
+    int has_turbo;
+    double init_log[5];
+    int has_init_log;
+    long iter; /* iterations performed so far (the reference's loop counter) */
+    /* history of the last run */
+    double* hist;
+    long nhist, hist_cap;
+};
+
+static long idx3(const oracle_solver* s, long i, long j, long k) { return (i * s->nj + j) * s->nk + k; }
+static long didx(const oracle_solver* s, long i, long j, long k) {
+    return (i * (s->nj + 1) + j) * (s->nk + 1) + k;
+}
+/* surfaces/centres I: (ni+1, nj, nk); J: (ni, nj+1, nk); K: (ni, nj, nk+1) */
+static long sIi(const oracle_solver* s, long i, long j, long k) { return (i * s->nj + j) * s->nk + k; }
+static long sJi(const oracle_solver* s, long i, long j, long k) { return (i * (s->nj + 1) + j) * s->nk + k; }
+static long sKi(const oracle_solver* s, long i, long j, long k) { return (i * s->nj + j) * (s->nk + 1) + k; }
+
+static sv5 state_at(const oracle_solver* s, double* const* U, long i, long j, long k) {
+    long q = idx3(s, i, j, k);
+    sv5 r = {{U[0][q], U[1][q], U[2][q], U[3][q], U[4][q]}};
+    return r;
+}
+static void state_set(const oracle_solver* s, double** U, long i, long j, long k, sv5 v) {
+    long q = idx3(s, i, j, k);
+    for (int c = 0; c < 5; c++) U[c][q] = v.v[c];
+}
+static void res_add(oracle_solver* s, long i, long j, long k, sv5 d) {
+    long q = idx3(s, i, j, k);
+    for (int c = 0; c < 5; c++) s->R[c][q] += d.v[c];
+}
+static void res_sub(oracle_solver* s, long i, long j, long k, sv5 d) {
+    long q = idx3(s, i, j, k);
+    for (int c = 0; c < 5; c++) s->R[c][q] -= d.v[c];
+}
+
+/* ------------------------------------------------------- fluid (ideal gas) */
+/* FluidIdeal (src/fluid_ideal.cpp). */
+
+static double f_pressure_rho_e(const oracle_solver* s, double rho, double e) { /* :14-16 */
+    return (s->gamma - 1) * rho * e;
+}
+static double f_static_energy_u_et(vec3 u, double et) { /* :74-77, pow(|u|,2) == |u|*|u| */
+    double m = vmag(u);
+    double m2 = m * m;
+    return et - 0.5 * m2;
+}
+static double f_pressure_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :89-92 */
+    double e = f_static_energy_u_et(u, et);
+    return f_pressure_rho_e(s, rho, e);
+}
+static double f_sound_speed_p_rho(const oracle_solver* s, double p, double rho) { /* :70-72 */
+    return sqrt(s->gamma * p / rho);
+}
+static double f_sound_speed_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :83-87 */
+    double e = f_static_energy_u_et(u, et);
+    double p = f_pressure_rho_e(s, rho, e);
+    return f_sound_speed_p_rho(s, p, rho);
+}
+static double f_sound_speed_rho_e(const oracle_solver* s, double rho, double e) { /* :22-24 */
+    (void)rho;
+    return sqrt(s->gamma * (s->gamma - 1.0) * e);
+}
+static double f_total_enthalpy_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :114-118 */
+    double e = f_static_energy_u_et(u, et);
+    double p = f_pressure_rho_e(s, rho, e);
+    return et + p / rho;
+}
+static double f_temperature_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :109-112 */
+    double p = f_pressure_rho_u_et(s, rho, u, et);
+    return p / (rho * s->rgas);
+}
+static double f_static_energy_p_rho(const oracle_solver* s, double p, double rho) { /* :10-12 */
+    return p / ((s->gamma - 1) * rho);
+}
+static double f_mach_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :137-141 */
+    double a = f_sound_speed_rho_u_et(s, rho, u, et);
+    double um = vmag(u);
+    return um / a;
+}
+static double f_total_pressure_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :94-98 */
+    double p = f_pressure_rho_u_et(s, rho, u, et);
+    double M = f_mach_rho_u_et(s, rho, u, et);
+    return p * pow(1.0 + (s->gamma - 1.0) / 2.0 * M * M, s->gamma / (s->gamma - 1));
+}
+static double f_total_temperature_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :100-104 */
+    double T = f_temperature_rho_u_et(s, rho, u, et);
+    double M = f_mach_rho_u_et(s, rho, u, et);
+    return T * (1.0 + (s->gamma - 1.0) / 2.0 * M * M);
+}
+static double f_entropy_p_T(const oracle_solver* s, double p, double T) { /* :195-198 */
+    return s->cp * log(T / 288.15) - s->rgas * log(p / 101325);
+}
+static double f_entropy_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :128-135 */
+    double p = f_pressure_rho_u_et(s, rho, u, et);
+    double T = f_temperature_rho_u_et(s, rho, u, et);
+    return f_entropy_p_T(s, p, T);
+}
+static double f_efficiency(const oracle_solver* s, double pr, double tr) { /* :179-191 */
+    double dT = tr - 1.0;
+    double dTs = pow(pr, (s->gamma - 1.0) / s->gamma) - 1.0;
+    if (fabs(dT) < 1e-12) return 1.0;
+    if (dT >= 0.0) return dTs / dT;
+    if (fabs(dTs) < 1e-12) return 1.0;
+    return dT / dTs;
+}
+
+/* getPrimitiveVariablesFromConservative (src/math_utils.cpp:49-57). */
+static sv5 prim_of(sv5 U) {
+    sv5 W;
+    W.v[0] = U.v[0];
+    W.v[1] = U.v[1] / U.v[0];
+    W.v[2] = U.v[2] / U.v[0];
+    W.v[3] = U.v[3] / U.v[0];
+    W.v[4] = U.v[4] / U.v[0];
+    return W;
+}
+static vec3 vel_of(sv5 W) { return v3(W.v[1], W.v[2], W.v[3]); }
+static double pressure_prim(const oracle_solver* s, sv5 W) { /* fluid_ideal.cpp:172-176 */
+    return f_pressure_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
+}
+
+/* computeAdvectionFluxFromPrimitive (src/math_utils.cpp:71-86). */
+static sv5 adv_flux(const oracle_solver* s, sv5 W, vec3 S) {
+    vec3 n = vdiv(S, vmag(S));
+    vec3 u = vel_of(W);
+    double un = vdot(u, n);
+    double p = f_pressure_rho_u_et(s, W.v[0], u, W.v[4]);
+    double ht = f_total_enthalpy_rho_u_et(s, W.v[0], u, W.v[4]);
+    sv5 F;
+    F.v[0] = W.v[0] * un;
+    F.v[1] = W.v[0] * un * u.x + p * n.x;
+    F.v[2] = W.v[0] * un * u.y + p * n.y;
+    F.v[3] = W.v[0] * un * u.z + p * n.z;
+    F.v[4] = W.v[0] * un * ht;
+    return F;
+}
+
+/* --------------------------------------------------------------- cylinder */
+/* src/math_utils.cpp:109-138; theta rotations about the x axis. */
+static vec3 rot_x(vec3 v, double th) {
+    vec3 r;
+    r.x = v.x;
+    r.y = v.y * cos(th) - v.z * sin(th);
+    r.z = v.y * sin(th) + v.z * cos(th);
+    return r;
+}
+static sv5 rot_state(sv5 a, double th) {
+    vec3 r = rot_x(v3(a.v[1], a.v[2], a.v[3]), th);
+    sv5 o = {{a.v[0], r.x, r.y, r.z, a.v[4]}};
+    return o;
+}
+static vec3 cyl_of_cart(vec3 v, double th) {
+    vec3 r;
+    r.x = v.x;
+    r.y = v.y * cos(th) + v.z * sin(th);
+    r.z = -v.y * sin(th) + v.z * cos(th);
+    return r;
+}
+static vec3 cart_of_cyl(vec3 v, double th) {
+    vec3 r;
+    r.x = v.x;
+    r.y = v.y * cos(th) - v.z * sin(th);
+    r.z = v.y * sin(th) + v.z * cos(th);
+    return r;
+}
+static double node_radius(const oracle_solver* s, long i, long j, long k) { /* mesh.hpp:64-66 */
+    vec3 p = s->vert[idx3(s, i, j, k)];
+    return sqrt(p.y * p.y + p.z * p.z);
+}
+static double node_theta(const oracle_solver* s, long i, long j, long k) { /* mesh.hpp:68-70 */
+    vec3 p = s->vert[idx3(s, i, j, k)];
+    return atan2(p.z, p.y);
+}
+
+/* ------------------------------------------------------------- advection */
+
+/* AdvectionJst::computeFlux (src/advection_jst.cpp:4-57), constants
+ * include/advection_jst.hpp:23. */
+static double jst_r(const oracle_solver* s, sv5 W) {
+    vec3 u = vel_of(W);
+    double vm = vmag(u);
+    double a = f_sound_speed_rho_u_et(s, W.v[0], u, W.v[4]);
+    return vm + a;
+}
+static double jst_s(const oracle_solver* s, sv5 W1, sv5 W2, sv5 W3) {
+    double p1 = pressure_prim(s, W1), p2 = pressure_prim(s, W2), p3 = pressure_prim(s, W3);
+    return fabs((p1 - 2 * p2 + p3) / (p1 + 2 * p2 + p3));
+}
+static sv5 flux_jst(const oracle_solver* s, sv5 Ull, sv5 Ul, sv5 Ur, sv5 Urr, vec3 S) {
+    sv5 Wll = prim_of(Ull), Wl = prim_of(Ul), Wr = prim_of(Ur), Wrr = prim_of(Urr);
+    sv5 Wavg = smul(sadd(Wl, Wr), 0.5);
+    double rL = jst_r(s, Wl), rR = jst_r(s, Wr);
+    double sL = jst_s(s, Wll, Wl, Wr), sR = jst_s(s, Wl, Wr, Wrr);
+    double r = dmax(rL, rR);
+    double sf = dmax(sL, sR);
+    double psi2 = 0.5 * sf * r;
+    double psi4 = dmax(0.0, 0.02 * r - 2.0 * psi2);
+    sv5 F = adv_flux(s, Wavg, S);
+    sv5 d = ssub(smul(ssub(Ur, Ul), psi2),
+                 smul(sadd(ssub(ssub(Urr, Ur), smul(ssub(Ur, Ul), 2)), ssub(Ul, Ull)), psi4));
+    return ssub(F, d);
+}
+
+/* AdvectionBase MUSCL helpers (src/advection_base.cpp:10-64). */
+static sv5 muscl_smooth(sv5 Wl, sv5 Wc, sv5 Wr) {
+    sv5 r;
+    for (int i = 0; i < 5; i++) {
+        double dR = Wr.v[i] - Wc.v[i];
+        double dL = Wc.v[i] - Wl.v[i];
+        r.v[i] = (fabs(dR) < 1E-12) ? 0.0 : dL / dR;
+    }
+    return r;
+}
+static sv5 muscl_limiter(const oracle_solver* s, sv5 sm) {
+    sv5 l = szero();
+    for (int i = 0; i < 5; i++) {
+        double x = sm.v[i];
+        switch (s->limiter) {
+            case LIM_NONE: l.v[i] = 0.0; break;
+            case LIM_VAN_ALBADA: l.v[i] = (x <= 0.0) ? 0.0 : (x * x + x) / (1.0 + x * x); break;
+            case LIM_VAN_LEER: l.v[i] = (x + fabs(x)) / (1.0 + fabs(x)); break;
+            case LIM_MIN_MOD: l.v[i] = dmax(0.0, dmin(1.0, x)); break;
+        }
+    }
+    return l;
+}
+
+/* AdvectionRoe (src/advection_roe.cpp:6-220, include/advection_roe.hpp:63). */
+static double roe_avg(double rl, double rr, double pl, double pr) {
+    return (sqrt(rl) * pl + sqrt(rr) * pr) / (sqrt(rl) + sqrt(rr));
+}
+static sv5 flux_roe(const oracle_solver* s, sv5 Ull, sv5 Ul, sv5 Ur, sv5 Urr, vec3 S) {
+    sv5 Wl = prim_of(Ul), Wr = prim_of(Ur), Wrr = prim_of(Urr), Wll = prim_of(Ull);
+    if (s->muscl) {
+        sv5 smL = muscl_smooth(Wll, Wl, Wr);
+        sv5 smR = muscl_smooth(Wl, Wr, Wrr);
+        sv5 limL = muscl_limiter(s, smL);
+        sv5 limR = muscl_limiter(s, smR);
+        for (int i = 0; i < 5; i++) Wl.v[i] += limL.v[i] * (Wr.v[i] - Wl.v[i]) * 0.5;
+        for (int i = 0; i < 5; i++) Wr.v[i] -= limR.v[i] * (Wrr.v[i] - Wr.v[i]) * 0.5;
+    }
+    /* normal triad :41-58 */
+    vec3 n1 = vnormalized(S), n2;
+    if (n1.x == 0 && n1.y == 0) n2 = v3(1, 0, 0);
+    else n2 = v3(-n1.y, n1.x, 0);
+    n2 = vnormalized(n2);
+    vec3 n3 = vcross(n1, n2);
+    /* rotated primitives :61-65 */
+    vec3 uL = vel_of(Wl), uR = vel_of(Wr);
+    sv5 L = {{Wl.v[0], vdot(uL, n1), vdot(uL, n2), vdot(uL, n3), Wl.v[4]}};
+    sv5 Rr = {{Wr.v[0], vdot(uR, n1), vdot(uR, n2), vdot(uR, n3), Wr.v[4]}};
+    /* Roe averages :68-143 */
+    double rhoL = L.v[0], rhoR = Rr.v[0];
+    double u1L = L.v[1], u1R = Rr.v[1], u2L = L.v[2], u2R = Rr.v[2], u3L = L.v[3], u3R = Rr.v[3];
+    double etL = L.v[4], etR = Rr.v[4];
+    double htL = f_total_enthalpy_rho_u_et(s, rhoL, v3(u1L, u2L, u3L), etL);
+    double htR = f_total_enthalpy_rho_u_et(s, rhoR, v3(u1R, u2R, u3R), etR);
+    double rhoA = sqrt(rhoL * rhoR);
+    double u1A = roe_avg(rhoL, rhoR, u1L, u1R);
+    double u2A = roe_avg(rhoL, rhoR, u2L, u2R);
+    double u3A = roe_avg(rhoL, rhoR, u3L, u3R);
+    double htA = roe_avg(rhoL, rhoR, htL, htR);
+    double eL = etL - 0.5 * (u1L * u1L + u2L * u2L + u3L * u3L);
+    double eR = etR - 0.5 * (u1R * u1R + u2R * u2R + u3R * u3R);
+    double pL = f_pressure_rho_e(s, rhoL, eL);
+    double pR = f_pressure_rho_e(s, rhoR, eR);
+    double chiL = (s->gamma - 1.0) * eL, kapL = (s->gamma - 1.0) * rhoL;
+    double chiR = (s->gamma - 1.0) * eR, kapR = (s->gamma - 1.0) * rhoR;
+    double barChi = 0.5 * (chiL + chiR);
+    double barKap = 0.5 * (kapL + kapR);
+    double barRho = 0.5 * (rhoL + rhoR);
+    double barE = 0.5 * (eL + eR);
+    double dP = pR - pL, dRho = rhoR - rhoL, dE = eR - eL;
+    double dRhoHat = (barRho > 1e-12) ? dRho / barRho : 0.0;
+    double dEHat = (fabs(barE) > 1e-12) ? dE / fabs(barE) : 0.0;
+    double dNorm2 = dRhoHat * dRhoHat + dEHat * dEHat;
+    double chiT = barChi, kapT = barKap;
+    if (dNorm2 > 1e-12) {
+        double res = dP - (barChi * dRho + barKap * dE);
+        chiT += (res * dRhoHat) / (dNorm2 * barRho);
+        kapT += (res * dEHat) / (dNorm2 * fabs(barE));
+    }
+    if (barKap > 0.0 && kapT <= 0.0) kapT = 0.01 * barKap;
+    double kapP = (rhoA > 1e-12) ? kapT / rhoA : 0.4;
+    double eA = roe_avg(rhoL, rhoR, eL, eR);
+    double chiP = chiT - kapP * eA;
+    double q2 = u1A * u1A + u2A * u2A + u3A * u3A;
+    double hA = htA - 0.5 * q2;
+    double a2 = chiP + kapP * hA;
+    if (a2 <= 0.0) {
+        double aL = f_sound_speed_rho_e(s, rhoL, eL);
+        double aR = f_sound_speed_rho_e(s, rhoR, eR);
+        a2 = 0.5 * (aL * aL + aR * aR);
+    }
+    double aA = sqrt(a2);
+    /* eigenvalues / eigenvectors :146-169 */
+    double lam[5] = {u1A - aA, u1A, u1A, u1A, u1A + aA};
+    double cE5 = htA - (aA * aA) / kapP;
+    double ev[5][5] = {
+        {1.0, u1A - aA, u2A, u3A, htA - aA * u1A},
+        {1.0, u1A, u2A, u3A, cE5},
+        {0.0, 0.0, 1.0, 0.0, u2A},
+        {0.0, 0.0, 0.0, 1.0, u3A},
+        {1.0, u1A + aA, u2A, u3A, htA + aA * u1A}};
+    /* wave strengths :172-185 */
+    double ddRho = Rr.v[0] - L.v[0];
+    double du1 = Rr.v[1] - L.v[1], du2 = Rr.v[2] - L.v[2], du3 = Rr.v[3] - L.v[3];
+    double ppL = f_pressure_rho_u_et(s, L.v[0], v3(L.v[1], L.v[2], L.v[3]), L.v[4]);
+    double ppR = f_pressure_rho_u_et(s, Rr.v[0], v3(Rr.v[1], Rr.v[2], Rr.v[3]), Rr.v[4]);
+    double ddP = ppR - ppL;
+    double ws[5];
+    ws[0] = 1.0 / (2.0 * aA * aA) * (ddP - rhoA * aA * du1);
+    ws[1] = ddRho - ddP / (aA * aA);
+    ws[2] = rhoA * du2;
+    ws[3] = rhoA * du3;
+    ws[4] = 1.0 / (2.0 * aA * aA) * (ddP + rhoA * aA * du1);
+    /* assembly :188-220 */
+    sv5 FL = adv_flux(s, L, v3(1.0, 0.0, 0.0));
+    sv5 FR = adv_flux(s, Rr, v3(1.0, 0.0, 0.0));
+    double fix[5];
+    for (int i = 0; i < 5; i++) fix[i] = (fabs(lam[i]) < 0.01) ? 0.01 : fabs(lam[i]);
+    sv5 Fr = smul(sadd(FL, FR), 0.5);
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) Fr.v[i] -= 0.5 * ws[j] * fix[j] * ev[j][i];
+    vec3 ex = v3(1.0, 0.0, 0.0), ey = v3(0.0, 1.0, 0.0), ez = v3(0.0, 0.0, 1.0);
+    sv5 F;
+    F.v[0] = Fr.v[0];
+    F.v[1] = Fr.v[1] * (vdot(n1, ex)) + Fr.v[2] * (vdot(n2, ex)) + Fr.v[3] * (vdot(n3, ex));
+    F.v[2] = Fr.v[1] * (vdot(n1, ey)) + Fr.v[2] * (vdot(n2, ey)) + Fr.v[3] * (vdot(n3, ey));
+    F.v[3] = Fr.v[1] * (vdot(n1, ez)) + Fr.v[2] * (vdot(n2, ez)) + Fr.v[3] * (vdot(n3, ez));
+    F.v[4] = Fr.v[4];
+    return F;
+}
+
+static sv5 flux_interior(const oracle_solver* s, sv5 Ull, sv5 Ul, sv5 Ur, sv5 Urr, vec3 S) {
+    return (s->scheme == SCHEME_JST) ? flux_jst(s, Ull, Ul, Ur, Urr, S)
+                                     : flux_roe(s, Ull, Ul, Ur, Urr, S);
+}
+
+/* ------------------------------------------------------------- boundaries */
+
+/* Config::computeRampedOutletPressure (src/config.cpp:430-439). */
+static double ramped_outlet_pressure(const oracle_solver* s, long it, double p_out) {
+    double maxIter = s->ramp_iters;
+    double ratio = (double)it / maxIter;
+    if (ratio >= 1.0) return p_out;
+    return s->init_p + (p_out - s->init_p) * ratio;
+}
+
+/* BoundaryBase::computeOutletFlux (src/boundary_base.cpp:181-224). */
+static sv5 bc_outlet(const oracle_solver* s, sv5 Uint, vec3 S, double p_b, long it) {
+    sv5 W = prim_of(Uint);
+    vec3 u = vel_of(W);
+    double rho = W.v[0];
+    double p = f_pressure_rho_u_et(s, rho, u, W.v[4]);
+    double a = f_sound_speed_p_rho(s, p, W.v[0]);
+    if (vmag(u) >= a) return adv_flux(s, W, S);
+    double pb = ramped_outlet_pressure(s, it, p_b);
+    double rhob = pb * rho / p;
+    double eb = f_static_energy_p_rho(s, pb, rhob);
+    double etb = eb + 0.5 * vdot(u, u);
+    sv5 Wb = {{rhob, u.x, u.y, u.z, etb}};
+    return adv_flux(s, Wb, S);
+}
+
+/* BoundaryInviscidWall::computeBoundaryFlux (src/boundary_inviscid_wall.cpp:5-30). */
+static sv5 bc_wall(const oracle_solver* s, sv5 Uint, vec3 S) {
+    sv5 W = prim_of(Uint);
+    vec3 u = vel_of(W);
+    double p = f_pressure_rho_u_et(s, W.v[0], u, W.v[4]);
+    vec3 d = vdiv(S, vmag(S));
+    double un = vdot(u, d);
+    double a = f_sound_speed_p_rho(s, p, W.v[0]);
+    double pw = p + W.v[0] * un * a;
+    if (pw < 0.01 * p) pw = 0.01 * p;
+    sv5 F = {{0.0, pw * d.x, pw * d.y, pw * d.z, 0.0}};
+    return F;
+}
+
+/* BoundaryInlet::computeBoundaryFlux (src/boundary_inlet.cpp:4-43) and
+ * BoundaryBase::computeSubsonicInletFlux (src/boundary_base.cpp:7-124). */
+static sv5 bc_inlet(const oracle_solver* s, const patch* pt, sv5 Uint, vec3 S, long fi, long fj,
+                    long fk) {
+    double Pt = pt->values[0], Tt = pt->values[1];
+    vec3 dir = v3(pt->values[2], pt->values[3], pt->values[4]);
+    if (s->inlet_cyl) dir = cart_of_cyl(dir, node_theta(s, fi, fj, fk));
+    if (dir.x == 1.0 && dir.y == 1.0 && dir.z == 1.0) dir = vneg(S);
+    dir = vdiv(dir, vmag(dir));
+
+    sv5 W = prim_of(Uint);
+    vec3 u = vel_of(W);
+    double aInt = f_sound_speed_rho_u_et(s, W.v[0], u, W.v[4]);
+    vec3 n = vdiv(S, vmag(S));
+    double unInt = vdot(u, n);
+    double Z = W.v[0] * aInt;
+    double pInt = f_pressure_rho_u_et(s, W.v[0], u, W.v[4]);
+    double Cg = vdot(dir, n);
+    if (Cg >= 0.0) Cg = -1.0;
+    double Rout = pInt + Z * unInt;
+    double g = s->gamma, Rg = s->rgas;
+    double cp = g * Rg / (g - 1.0);
+    double htIn = cp * Tt;
+    double pLow = 0.05 * Pt, pHigh = 0.999999 * Pt;
+    double pB = 0.5 * (pLow + pHigh);
+    for (int iter = 0; iter < 30; ++iter) {
+        double pMid = 0.5 * (pLow + pHigh);
+        double TMid = Tt * pow(pMid / Pt, (g - 1.0) / g);
+        double hMid = cp * TMid;
+        double VMid = sqrt(2.0 * dmax(0.0, htIn - hMid));
+        double res = pMid + Z * Cg * VMid - Rout;
+        if (fabs(res) < 1e-4 * Pt) { pB = pMid; break; }
+        if (res < 0.0) pLow = pMid; else pHigh = pMid;
+        pB = pMid;
+    }
+    double TB = Tt * pow(pB / Pt, (g - 1.0) / g);
+    double hB = cp * TB;
+    double VB = sqrt(2.0 * dmax(0.0, htIn - hB));
+    vec3 uB = vmul(dir, VB);
+    double rhoB = pB / (Rg * TB);
+    double eB = f_static_energy_p_rho(s, pB, rhoB);
+    double etB = eB + 0.5 * vdot(uB, uB);
+    sv5 Wb = {{rhoB, uB.x, uB.y, uB.z, etB}};
+    return adv_flux(s, Wb, S);
+}
+
+static sv5 boundary_flux(oracle_solver* s, int pidx, sv5 Uint, vec3 S, long fi, long fj, long fk,
+                         long it) {
+    const patch* p = &s->patches[pidx];
+    switch (p->type) {
+        case BC_INLET: return bc_inlet(s, p, Uint, S, fi, fj, fk);
+        case BC_OUTLET: return bc_outlet(s, Uint, S, p->values[0], it);
+        case BC_RADIAL_EQ:
+        case BC_THROTTLE: /* src/boundary_outlet_throttle.cpp:5-16, radial_equilibrium.cpp:5-16 */
+            return bc_outlet(s, Uint, S, s->profiles[p->profile].pressure[fj], it);
+        case BC_INVISCID_WALL: return bc_wall(s, Uint, S);
+        default: return szero(); /* BoundaryFake (src/boundary_fake.cpp:4-13) */
+    }
+}
+
+/* ------------------------------------------------------------ residuals */
+
+/* Solver::computeAdvectionFluxResidualsImpl (src/solver.cpp:1865-2040). */
+static void advection_residuals(oracle_solver* s, int dir, double* const* U, long it) {
+    long nfi, nfj, nfk;
+    const vec3* surf;
+    const int* map;
+    if (dir == 0) { nfi = s->ni + 1; nfj = s->nj; nfk = s->nk; surf = s->sI; map = s->mapI; }
+    else if (dir == 1) { nfi = s->ni; nfj = s->nj + 1; nfk = s->nk; surf = s->sJ; map = s->mapJ; }
+    else { nfi = s->ni; nfj = s->nj; nfk = s->nk + 1; surf = s->sK; map = s->mapK; }
+    const long st[3] = {dir == 0, dir == 1, dir == 2};
+    const long nface[3] = {nfi, nfj, nfk};
+    const long stop = nface[dir] - 1;
+
+    for (long a = 0; a < (dir == 0 ? nfj : nfi); a++) {
+        for (long b = 0; b < (dir == 2 ? nfj : nfk); b++) {
+            for (long c = 0; c < nface[dir]; c++) {
+                long fi, fj, fk;
+                if (dir == 0) { fj = a; fk = b; fi = c; }
+                else if (dir == 1) { fi = a; fk = b; fj = c; }
+                else { fi = a; fj = b; fk = c; }
+                long sidx = (dir == 0) ? sIi(s, fi, fj, fk) : (dir == 1) ? sJi(s, fi, fj, fk) : sKi(s, fi, fj, fk);
+                long dface = (dir == 0) ? fi : (dir == 1) ? fj : fk;
+                if (dir == 2 && s->bfm_active) {
+                    if (s->field[F_BLADE_PRESENT][idx3(s, fi, fj, 0)] > 0.0) continue;
+                }
+                if (dface == 0) {
+                    sv5 Ui = state_at(s, U, fi, fj, fk);
+                    vec3 S = vneg(surf[sidx]);
+                    long mi = (dir == 0) ? (0 * s->nj + fj) * s->nk + fk
+                            : (dir == 1) ? (fi * 2 + 0) * s->nk + fk
+                                         : (fi * s->nj + fj) * 2 + 0;
+                    sv5 F = boundary_flux(s, map[mi], Ui, S, fi, fj, fk, it);
+                    res_add(s, fi, fj, fk, smul(F, vmag(S)));
+                } else if (dface == stop) {
+                    long ii = fi - st[0], jj = fj - st[1], kk = fk - st[2];
+                    sv5 Ui = state_at(s, U, ii, jj, kk);
+                    vec3 S = surf[sidx];
+                    long mi = (dir == 0) ? (1 * s->nj + fj) * s->nk + fk
+                            : (dir == 1) ? (fi * 2 + 1) * s->nk + fk
+                                         : (fi * s->nj + fj) * 2 + 1;
+                    sv5 F = boundary_flux(s, map[mi], Ui, S, fi, fj, fk, it);
+                    res_add(s, ii, jj, kk, smul(F, vmag(S)));
+                } else {
+                    sv5 Ul = state_at(s, U, fi - st[0], fj - st[1], fk - st[2]);
+                    sv5 Ur = state_at(s, U, fi, fj, fk);
+                    sv5 Ull, Urr;
+                    if (dir == 2 && s->periodic) {
+                        if (dface == 1) {
+                            Ull = state_at(s, U, fi, fj, nfk - 3);
+                            Ull = rot_state(Ull, -s->per_angle_rad);
+                            Urr = state_at(s, U, fi, fj, fk + 1);
+                        } else if (dface == stop - 1) {
+                            Ull = state_at(s, U, fi, fj, fk - 2);
+                            Urr = state_at(s, U, fi, fj, 1);
+                            Urr = rot_state(Urr, s->per_angle_rad);
+                        } else {
+                            Ull = state_at(s, U, fi - 2 * st[0], fj - 2 * st[1], fk - 2 * st[2]);
+                            Urr = state_at(s, U, fi + st[0], fj + st[1], fk + st[2]);
+                        }
+                    } else {
+                        if (dface == 1) {
+                            Ull = ssub(Ul, ssub(Ur, Ul));
+                            Urr = state_at(s, U, fi + st[0], fj + st[1], fk + st[2]);
+                        } else if (dface == stop - 1) {
+                            Ull = state_at(s, U, fi - 2 * st[0], fj - 2 * st[1], fk - 2 * st[2]);
+                            Urr = sadd(Ur, ssub(Ur, Ul));
+                        } else {
+                            Ull = state_at(s, U, fi - 2 * st[0], fj - 2 * st[1], fk - 2 * st[2]);
+                            Urr = state_at(s, U, fi + st[0], fj + st[1], fk + st[2]);
+                        }
+                    }
+                    vec3 S = surf[sidx];
+                    sv5 F = flux_interior(s, Ull, Ul, Ur, Urr, S);
+                    res_add(s, fi - st[0], fj - st[1], fk - st[2], smul(F, vmag(S)));
+                    res_sub(s, fi, fj, fk, smul(F, vmag(S)));
+                }
+            }
+        }
+    }
+}
+
+/* Solver::getRotationalSpeedScalingFactor (src/config.cpp:695-718). */
+static double speed_scaling(const oracle_solver* s, double t) {
+    if (!s->accel) return s->speed_scale;
+    if (t < s->acc_t0 || t > s->acc_t1) return s->speed_scale;
+    return s->acc_s0 + (s->acc_s1 - s->acc_s0) * (t - s->acc_t0) / (s->acc_t1 - s->acc_t0);
+}
+
+/* Solver::computeGongSource (src/solver.cpp:3074-3145). */
+static sv5 gong_source(const oracle_solver* s, double* const* U, double omega, long i, long j,
+                       long k, double vol) {
+    if (fabs(omega) < 1E-3) return szero();
+    sv5 U0, U1, U2;
+    long nk = s->nk;
+    if (omega > 0) {
+        if (k == 0) { U0 = state_at(s, U, i, j, k); U1 = state_at(s, U, i, j, nk - 2); U2 = state_at(s, U, i, j, nk - 3); }
+        else if (k == 1) { U0 = state_at(s, U, i, j, k); U1 = state_at(s, U, i, j, 0); U2 = state_at(s, U, i, j, nk - 2); }
+        else { U0 = state_at(s, U, i, j, k); U1 = state_at(s, U, i, j, k - 1); U2 = state_at(s, U, i, j, k - 2); }
+    } else {
+        if (k == nk - 1) { U0 = state_at(s, U, i, j, 0); U1 = state_at(s, U, i, j, 1); U2 = state_at(s, U, i, j, 2); }
+        else if (k == nk - 2) { U0 = state_at(s, U, i, j, k); U1 = state_at(s, U, i, j, 0); U2 = state_at(s, U, i, j, 1); }
+        else { U0 = state_at(s, U, i, j, k); U1 = state_at(s, U, i, j, k + 1); U2 = state_at(s, U, i, j, k + 2); }
+    }
+    double dth = (2 * M_PI / (double)(nk - 1));
+    sv5 d;
+    if (omega > 0.0) d = sdiv(sadd(ssub(smul(U0, 3.0), smul(U1, 4.0)), U2), 2 * dth);
+    else d = sdiv(ssub(sadd(smul(U0, -3.0), smul(U1, 4.0)), U2), 2 * dth);
+    sv5 src;
+    for (int c = 0; c < 5; c++) src.v[c] = -d.v[c] * omega;
+    return smul(src, vol);
+}
+
+/* SourceBFMBase flow state (src/source_bfm_base.cpp:104-199). */
+typedef struct {
+    double radius, theta, omega, pitch, staggered, nblades, blockage, flow_angle, dev;
+    vec3 velCyl, relCyl, relCart, nCyl, invDirCyl, viscDirCyl;
+} bfm_state;
+
+static double bfm_deviation(vec3 rel, vec3 ncam) { /* :152-166 */
+    vec3 n = vdiv(ncam, vmag(ncam));
+    vec3 vm = v3(rel.x, rel.y, 0.0);
+    vec3 span = v3(-vm.y, vm.x, 0.0);
+    span = vdiv(span, vmag(span));
+    vec3 vin = vsub(rel, vmul(span, vdot(rel, span)));
+    double nv = vdot(vin, n);
+    return -asin(nv / vmag(vin));
+}
+
+static vec3 bfm_inviscid_dir(const oracle_solver* s, vec3 rel, vec3 ncam, double dev, long q) { /* :168-199 */
+    vec3 rd = vnormalized(rel);
+    vec3 nd = vnormalized(ncam);
+    vec3 ver;
+    if (s->stalled && dev > s->field[F_DEV_STALL][q]) ver = nd;
+    else ver = vnormalized(vsub(nd, vmul(rd, vdot(nd, rd))));
+    vec3 vm = v3(rel.x, rel.y, 0.0);
+    vec3 sd = vnormalized(v3(vm.y, -vm.x, 0.0));
+    return vnormalized(vsub(ver, vmul(sd, vdot(ver, sd))));
+}
+
+static void bfm_flow_state(const oracle_solver* s, long i, long j, long k, sv5 W, double t,
+                           bfm_state* b) {
+    long q = idx3(s, i, j, k);
+    b->radius = node_radius(s, i, j, k);
+    b->theta = node_theta(s, i, j, k);
+    vec3 vc = vel_of(W);
+    b->velCyl = cyl_of_cart(vc, b->theta);
+    b->omega = s->field[F_RPM][q] * 2 * M_PI / 60;
+    b->omega *= speed_scaling(s, t);
+    vec3 drag = v3(0, 0, b->omega * b->radius);
+    b->relCyl = vsub(b->velCyl, drag);
+    b->relCart = cart_of_cyl(b->relCyl, b->theta);
+    double vmer = sqrt(b->velCyl.x * b->velCyl.x + b->velCyl.y * b->velCyl.y);
+    b->nblades = s->field[F_NBLADES][q];
+    b->pitch = 2.0 * M_PI * b->radius / b->nblades;
+    b->nCyl = v3(s->field[F_NAX][q], s->field[F_NRAD][q], s->field[F_NTAN][q]);
+    b->blockage = s->field[F_BLOCKAGE][q];
+    double metal = s->field[F_METAL] ? s->field[F_METAL][q] : 0.0;
+    b->staggered = b->pitch * cos(metal);
+    b->flow_angle = atan2(b->relCyl.z, vmer);
+    b->dev = bfm_deviation(b->relCyl, b->nCyl);
+    b->invDirCyl = bfm_inviscid_dir(s, b->relCyl, b->nCyl, b->dev, q);
+    b->viscDirCyl = vneg(vnormalized(b->relCyl));
+}
+
+static sv5 force_source(vec3 fcyl, const bfm_state* b, double vol, double rho) {
+    vec3 fc = cart_of_cyl(fcyl, b->theta);
+    sv5 src = {{0, fc.x, fc.y, fc.z, fcyl.z * b->omega * b->radius}};
+    return smul(smul(src, vol), rho);
+}
+
+/* SourceBFMThollet::computeCompressibilityCorrection (src/source_bfm_thollet.cpp:48-70). */
+static double thollet_kmach(const oracle_solver* s, vec3 rel, sv5 W) {
+    double a = f_sound_speed_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
+    double M = vmag(rel) / a;
+    if (fabs(M - 1.0) < 1E-03) M = 0.999;
+    double kp;
+    if (M < 1.0) kp = 1.0 / sqrt(1.0 - M * M);
+    else kp = 2.0 / M_PI / sqrt(M * M - 1.0);
+    return dmin(3.0, kp);
+}
+
+static sv5 bfm_body_force(const oracle_solver* s, long i, long j, long k, sv5 W, double t) {
+    long q = idx3(s, i, j, k);
+    bfm_state b;
+    bfm_flow_state(s, i, j, k, W, t, &b);
+    double vol = s->vol[q];
+    double w2 = vdot(b.relCyl, b.relCyl);
+    if (s->bfm_model == BFM_HALL) { /* src/source_bfm_hall.cpp:3-34 */
+        double fm = w2 * M_PI * b.dev / b.pitch / fabs(b.nCyl.z);
+        return force_source(vmul(b.invDirCyl, fm), &b, vol, W.v[0]);
+    }
+    if (s->bfm_model == BFM_THOLLET) { /* src/source_bfm_thollet.cpp:3-138 */
+        double km = thollet_kmach(s, b.relCyl, W);
+        double fm = s->kn * km * w2 * M_PI * b.dev / b.pitch / fabs(b.nCyl.z) / b.blockage;
+        sv5 inv = force_source(vmul(b.invDirCyl, fm), &b, vol, W.v[0]);
+        sv5 visc;
+        if (s->stalled && b.dev > s->field[F_DEV_STALL][q]) {
+            visc = szero();
+        } else {
+            double nu = s->nu;
+            double stwl = s->field[F_STWL][q];
+            if (stwl < 1E-06) {
+                if (i + 1 < s->ni) stwl = (s->field[F_STWL][idx3(s, i + 1, j, k)] + s->field[F_STWL][q]) / 2.0;
+                if (stwl < 1E-06) stwl = 1E-06;
+            }
+            double rex = vmag(b.relCyl) * stwl / nu;
+            double cf = 0.0592 * pow(rex, -0.2);
+            double fmv;
+            if (!s->offdesign) {
+                fmv = w2 / (b.pitch * b.blockage * fabs(b.nCyl.z)) * (s->kf * cf);
+            } else {
+                double piv = s->field[F_DEV_PIVOT][q];
+                double km2 = thollet_kmach(s, b.relCyl, W);
+                fmv = w2 / (b.pitch * b.blockage * fabs(b.nCyl.z)) *
+                      (s->kf * cf + M_PI * km2 * pow(fabs(b.dev - piv), 2.0 * s->kd));
+            }
+            visc = force_source(vmul(b.viscDirCyl, fmv), &b, vol, W.v[0]);
+        }
+        return sadd(inv, visc);
+    }
+    if (s->bfm_model == BFM_LIFT_DRAG) { /* src/source_bfm_lift_drag.cpp:3-88 */
+        double chord = s->field[F_STWL][idx3(s, s->te_idx, j, k)] - s->field[F_STWL][idx3(s, s->le_idx, j, k)];
+        double sol = chord / b.pitch;
+        double w = vmag(b.relCart);
+        double beta0 = s->field[F_LD_BETA0][q];
+        double sgn = (b.nCyl.z >= 0.0) ? 1.0 : -1.0;
+        double fm = 0.5 * w * w * 2.0 * M_PI / b.staggered * sgn * (-b.flow_angle + beta0);
+        sv5 inv = force_source(vmul(b.invDirCyl, fm), &b, vol, W.v[0]);
+        double kp0 = s->field[F_LD_KP][q];
+        double d = b.flow_angle - beta0;
+        double kp = kp0 + 2.0 * M_PI * sol * (d * d);
+        double fmv = kp * w * w / b.staggered;
+        sv5 visc = force_source(vmul(b.viscDirCyl, fmv), &b, vol, W.v[0]);
+        return sadd(inv, visc);
+    }
+    return szero();
+}
+
+/* SourceBFMBase::computePerturbationFactor (src/source_bfm_base.cpp:215-243). */
+static double bfm_perturbation(const oracle_solver* s, long i, long j, long k, double t) {
+    if (!s->perturb) return 0.0;
+    if (t < s->pert_t0 || t > s->pert_t0 + s->pert_dur) return 0.0;
+    vec3 p = s->vert[idx3(s, i, j, k)];
+    double dist = vmag(vsub(p, v3(s->pert_center[0], s->pert_center[1], s->pert_center[2])));
+    if (dist > 3.0 * s->pert_radius) return 0.0;
+    double sm = exp(-(dist * dist) / (s->pert_radius * s->pert_radius));
+    double peak = s->pert_t0 + s->pert_dur / 2.0;
+    double sig = s->pert_dur / 3.0;
+    double dtp = t - peak;
+    double tm = exp(-(dtp * dtp) / (sig * sig));
+    return s->pert_scale * sm * tm;
+}
+
+/* SourceBFMBase::computeTotalSource (src/source_bfm_base.cpp:25-84). */
+static sv5 bfm_total_source(const oracle_solver* s, long i, long j, long k, sv5 W, double t) {
+    long q = idx3(s, i, j, k);
+    sv5 blk = szero();
+    if (s->blockage_active) {
+        vec3 u = vel_of(W);
+        double ht = f_total_enthalpy_rho_u_et(s, W.v[0], u, W.v[4]);
+        double bb = s->field[F_BLOCKAGE][q];
+        vec3 gb = s->gradb[q];
+        double vol = s->vol[q];
+        double ct = -1.0 / bb * W.v[0] * vdot(u, gb);
+        sv5 src = {{ct, ct * u.x, ct * u.y, ct * u.z, ct * ht}};
+        blk = smul(src, vol);
+    }
+    if (s->field[F_NBLADES][q] == 0) return blk;
+    sv5 bf = bfm_body_force(s, i, j, k, W, t);
+    double pf = bfm_perturbation(s, i, j, k, t);
+    return sadd(blk, smul(bf, 1.0 + pf));
+}
+
+/* Solver::computeSourceResiduals (src/solver.cpp:2790-2924). */
+static void source_residuals(oracle_solver* s, double* const* U) {
+    if (s->topology == TOPO_3D && !s->bfm_active) return;
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                long q = idx3(s, i, j, k);
+                sv5 W = prim_of(state_at(s, U, i, j, k));
+                double vol = s->vol[q];
+                double p = f_pressure_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
+                double r = node_radius(s, i, j, k);
+                double th = node_theta(s, i, j, k);
+                int geo = 0, gong = 0;
+                if (s->topology == TOPO_3D && s->bfm_active) {
+                    geo = gong = (s->field[F_BLADE_PRESENT][q] > 0.0);
+                } else if (s->topology == TOPO_AXI) {
+                    geo = 1;
+                }
+                if (geo) {
+                    vec3 vc = cyl_of_cart(vel_of(W), th);
+                    vec3 sc, sCart;
+                    if (s->topology == TOPO_AXI) {
+                        double aK = vmag(s->sK[sKi(s, i, j, 0)]);
+                        double gf = aK * s->wedge;
+                        sc.x = 0.0;
+                        sc.y = (+W.v[0] * vc.z * vc.z + p) * gf;
+                        sc.z = -W.v[0] * vc.y * vc.z * gf;
+                        sCart = cart_of_cyl(sc, th);
+                        sv5 g = {{0.0, sCart.x, sCart.y, sCart.z, 0.0}};
+                        res_sub(s, i, j, k, g);
+                    } else {
+                        sc.x = 0.0;
+                        sc.y = (+W.v[0] * vc.z * vc.z + p) / r;
+                        sc.z = -W.v[0] * vc.y * vc.z / r;
+                        sCart = cart_of_cyl(sc, th);
+                        sv5 g = {{0.0, sCart.x, sCart.y, sCart.z, 0.0}};
+                        res_sub(s, i, j, k, smul(g, vol));
+                    }
+                }
+                if (gong) {
+                    double om = s->field[F_RPM][q] * 2 * M_PI / 60;
+                    om *= speed_scaling(s, s->t);
+                    res_sub(s, i, j, k, gong_source(s, U, om, i, j, k, vol));
+                }
+                if (s->bfm_active) {
+                    if (vmag(s->gradb[q]) > 1E-10) res_sub(s, i, j, k, bfm_total_source(s, i, j, k, W, s->t));
+                }
+            }
+}
+
+/* Solver::enforcePeriodicityOnResiduals (src/solver.cpp:1836-1853). */
+static void periodic_residuals(oracle_solver* s) {
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++) {
+            sv5 R1 = state_at(s, s->R, i, j, 0);
+            sv5 R2 = state_at(s, s->R, i, j, s->nk - 1);
+            sv5 R2f = rot_state(R2, -s->per_angle_rad);
+            sv5 Ra = smul(sadd(R1, R2f), 0.5);
+            state_set(s, s->R, i, j, 0, Ra);
+            state_set(s, s->R, i, j, s->nk - 1, rot_state(Ra, +s->per_angle_rad));
+        }
+}
+
+/* Solver::computeResiduals (src/solver.cpp:1783-1833). */
+static void compute_residuals(oracle_solver* s, double* const* U, long it) {
+    for (int c = 0; c < 5; c++) memset(s->R[c], 0, sizeof(double) * s->n);
+    advection_residuals(s, 0, U, it);
+    if (s->topology != TOPO_1D) advection_residuals(s, 1, U, it);
+    if (s->topology == TOPO_3D) advection_residuals(s, 2, U, it);
+    source_residuals(s, U);
+    if (s->periodic) periodic_residuals(s);
+}
+
+/* Solver::computeTimestepArray (src/solver.cpp:1531-1630). */
+static void compute_timestep(oracle_solver* s, double* const* U) {
+    if (s->dt_method == DT_FIXED) {
+        for (long q = 0; q < s->n; q++) s->dt[q] = s->fixed_dt;
+        return;
+    }
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                vec3 p0 = s->dual[didx(s, i, j, k)];
+                vec3 eI = vsub(s->dual[didx(s, i + 1, j, k)], p0);
+                vec3 eJ = vsub(s->dual[didx(s, i, j + 1, k)], p0);
+                vec3 eK = vsub(s->dual[didx(s, i, j, k + 1)], p0);
+                double dsI = vmag(eI), dsJ = vmag(eJ), dsK = vmag(eK);
+                vec3 dI = vdiv(eI, dsI), dJ = vdiv(eJ, dsJ), dK = vdiv(eK, dsK);
+                sv5 W = prim_of(state_at(s, U, i, j, k));
+                vec3 u = vel_of(W);
+                double rho = W.v[0];
+                double a = f_sound_speed_rho_u_et(s, W.v[0], u, W.v[4]);
+                double mu = 0.0, mut = 0.0;
+                double nu = mu / rho, nut = mut / rho;
+                double ui = fabs(vdot(u, dI)), uj = fabs(vdot(u, dJ)), uk = fabs(vdot(u, dK));
+                double lc = (ui + a) / dsI;
+                double ih2 = 1.0 / (dsI * dsI);
+                if (s->topology != TOPO_1D) { lc += (uj + a) / dsJ; ih2 += 1.0 / (dsJ * dsJ); }
+                if (s->topology == TOPO_3D) { lc += (uk + a) / dsK; ih2 += 1.0 / (dsK * dsK); }
+                double lv = 4.0 * (nu + nut) * ih2;
+                s->dt[idx3(s, i, j, k)] = s->cfl / (lc + lv);
+            }
+    if (s->dt_method == DT_GLOBAL) {
+        double m = s->dt[0];
+        for (long q = 1; q < s->n; q++) if (s->dt[q] < m) m = s->dt[q];
+        for (long q = 0; q < s->n; q++) s->dt[q] = m;
+    }
+}
+
+/* Solver::updateSolution (src/solver.cpp:2230-2249). */
+static void update_solution(oracle_solver* s, double alpha) {
+    for (long q = 0; q < s->n; q++) {
+        double f = alpha * s->dt[q] / s->vol[q];
+        for (int c = 0; c < 5; c++) s->Utmp[c][q] = s->U[c][q] - s->R[c][q] * f;
+    }
+}
+
+/* Solver::enforcePeriodicityOnSolution (src/solver.cpp:2308-2327). */
+static void periodic_solution(oracle_solver* s) {
+    if (!s->periodic) return;
+    double ang = s->per_angle_rad, inv = -ang;
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++) {
+            sv5 U1 = state_at(s, s->Utmp, i, j, 0);
+            sv5 U2 = state_at(s, s->Utmp, i, j, s->nk - 1);
+            sv5 Ua = smul(sadd(U1, rot_state(U2, inv)), 0.5);
+            state_set(s, s->Utmp, i, j, 0, Ua);
+            state_set(s, s->Utmp, i, j, s->nk - 1, rot_state(Ua, ang));
+        }
+}
+
+/* ---------------------------------------------------- mass flow and turbo */
+
+static vec3 boundary_surface(const oracle_solver* s, int bi, long a, long b) {
+    switch (bi) {
+        case BI_ISTART: return s->sI[sIi(s, 0, a, b)];
+        case BI_IEND: return s->sI[sIi(s, s->ni, a, b)];
+        case BI_JSTART: return s->sJ[sJi(s, a, 0, b)];
+        case BI_JEND: return s->sJ[sJi(s, a, s->nj, b)];
+        case BI_KSTART: return s->sK[sKi(s, a, b, 0)];
+        default: return s->sK[sKi(s, a, b, s->nk)];
+    }
+}
+static void boundary_extent(const oracle_solver* s, int bi, long* na, long* nb) {
+    if (bi <= BI_IEND) { *na = s->nj; *nb = s->nk; }
+    else if (bi <= BI_JEND) { *na = s->ni; *nb = s->nk; }
+    else { *na = s->ni; *nb = s->nj; }
+}
+static long boundary_node(const oracle_solver* s, int bi, long a, long b) {
+    switch (bi) {
+        case BI_ISTART: return idx3(s, 0, a, b);
+        case BI_IEND: return idx3(s, s->ni - 1, a, b);
+        case BI_JSTART: return idx3(s, a, 0, b);
+        case BI_JEND: return idx3(s, a, s->nj - 1, b);
+        case BI_KSTART: return idx3(s, a, b, 0);
+        default: return idx3(s, a, b, s->nk - 1);
+    }
+}
+
+/* Solver::updateMassFlows (src/solver.cpp:1633-1649) with computeSurfaceIntegral
+ * (src/math_utils.cpp:18-33). */
+static void update_mass_flows(oracle_solver* s, double* const* U) {
+    for (int bi = 0; bi < 6; bi++) {
+        long na, nb;
+        boundary_extent(s, bi, &na, &nb);
+        double sum = 0.0;
+        for (long a = 0; a < na; a++)
+            for (long b = 0; b < nb; b++) {
+                vec3 S = boundary_surface(s, bi, a, b);
+                long q = boundary_node(s, bi, a, b);
+                sum += S.x * U[1][q] + S.y * U[2][q] + S.z * U[3][q];
+            }
+        s->massflow[bi] = sum;
+    }
+}
+
+/* Solver::updateTurboPerformance (src/solver.cpp:1652-1781). */
+static void update_turbo(oracle_solver* s, double* const* U) {
+    int bci[2];
+    switch (s->turbo_dir) {
+        case 1: bci[0] = BI_IEND; bci[1] = BI_ISTART; break;
+        case 2: bci[0] = BI_JSTART; bci[1] = BI_JEND; break;
+        case 3: bci[0] = BI_JEND; bci[1] = BI_JSTART; break;
+        default: bci[0] = BI_ISTART; bci[1] = BI_IEND; break;
+    }
+    double mflow = 0.5 * (fabs(s->massflow[bci[0]]) + fabs(s->massflow[bci[1]]));
+    if (s->topology == TOPO_AXI) mflow *= 2.0 * M_PI / s->wedge;
+    else if (s->per_angle_deg != 0.0) mflow *= 360.0 / s->per_angle_deg;
+    double pt[2], tt[2];
+    for (int m = 0; m < 2; m++) {
+        int bi = bci[m];
+        long na, nb;
+        boundary_extent(s, bi, &na, &nb);
+        double sp = 0.0, stt = 0.0;
+        for (long a = 0; a < na; a++)
+            for (long b = 0; b < nb; b++) {
+                long q;
+                /* getPrimitiveAtBoundary: K planes fall back to (0, a, b). */
+                if (bi <= BI_JEND) q = boundary_node(s, bi, a, b);
+                else q = idx3(s, 0, a, b);
+                sv5 Uc = {{U[0][q], U[1][q], U[2][q], U[3][q], U[4][q]}};
+                sv5 W = prim_of(Uc);
+                double rho = W.v[0];
+                vec3 u = vel_of(W);
+                double et = W.v[4];
+                double P = f_total_pressure_rho_u_et(s, rho, u, et);
+                double T = f_total_temperature_rho_u_et(s, rho, u, et);
+                vec3 S = boundary_surface(s, bi, a, b);
+                sp += S.x * (rho * u.x * P) + S.y * (rho * u.y * P) + S.z * (rho * u.z * P);
+                stt += S.x * (rho * u.x * T) + S.y * (rho * u.y * T) + S.z * (rho * u.z * T);
+            }
+        double mf = s->massflow[bi];
+        if (fabs(mf) < 1e-12) mf = (mf >= 0.0 ? 1e-12 : -1e-12);
+        pt[m] = sp / mf;
+        tt[m] = stt / mf;
+    }
+    double pr = (fabs(pt[0]) > 1e-12) ? pt[1] / pt[0] : 1.0;
+    double tr = (fabs(tt[0]) > 1e-12) ? tt[1] / tt[0] : 1.0;
+    s->turbo[0] = mflow;
+    s->turbo[1] = pr;
+    s->turbo[2] = tr;
+    s->turbo[3] = f_efficiency(s, pr, tr);
+    s->has_turbo = 1;
+}
+
+/* integrateRadialEquilibrium (src/math_utils.cpp:141-170). */
+static void integrate_radial_eq(const double* rho, const double* ut, const double* r, double* p,
+                                int n, double hub) {
+    p[0] = hub;
+    for (int i = 1; i < n; ++i) {
+        double r1 = r[i - 1], r2 = r[i];
+        double dr = r2 - r1;
+        double d1 = rho[i - 1] * ut[i - 1] * ut[i - 1] / r1;
+        double d2 = rho[i] * ut[i] * ut[i] / r2;
+        p[i] = p[i - 1] + 0.5 * (d1 + d2) * dr;
+    }
+}
+
+/* GreitzerModel::computePlenumPressure (src/greitzer_model.cpp:36-56). */
+static double greitzer_step(oracle_solver* s, double mflow) {
+    s->gz_min = mflow;
+    s->gz_t += s->fixed_dt;
+    double a = sqrt(s->gamma * s->rgas * s->gz_T);
+    double np = s->gz_p + s->fixed_dt * a * a / s->plenum_volume * (s->gz_min - s->gz_mout);
+    s->gz_p = np;
+    double dp = s->gz_p - s->ambient_p;
+    s->gz_mout = (dp > 0.0) ? sqrt(dp / s->throttle_kt) : 0.0;
+    return s->gz_p;
+}
+
+/* Solver::updateRadialProfiles (src/solver.cpp:2688-2787). */
+static void update_radial_profiles(oracle_solver* s, double* const* U) {
+    if (!s->has_turbo) {
+        update_mass_flows(s, U);
+        update_turbo(s, U);
+    }
+    if (s->greitzer) s->hub_p = greitzer_step(s, s->turbo[0]);
+    for (int m = 0; m < s->nprofiles; m++) {
+        radial_profile* rp = &s->profiles[m];
+        const patch* bp = &s->patches[rp->patch];
+        double* dens = (double*)calloc(rp->n, sizeof(double));
+        double* vt = (double*)calloc(rp->n, sizeof(double));
+        long i = (bp->i_min > 0) ? (bp->i_min - 1) : 0;
+        int kk = 0;
+        for (long j = bp->j_min; j < bp->j_max && kk < rp->n; j++) {
+            sv5 W = prim_of(state_at(s, U, i, j, 0));
+            double th = node_theta(s, i, j, 0);
+            vec3 vcyl = cyl_of_cart(vel_of(W), th);
+            dens[kk] = W.v[0];
+            vt[kk] = fabs(vcyl.z);
+            kk++;
+        }
+        if (s->greitzer) {
+        } else if (bp->type == BC_THROTTLE) {
+            double kt = bp->values[0];
+            double mf = s->turbo[0];
+            double ptin = 0.0;
+            for (int b = 0; b < s->npatches; b++)
+                if (s->patches[b].type == BC_INLET) { ptin = s->patches[b].values[0]; break; }
+            s->hub_p = ptin + kt * mf * mf;
+        } else if (bp->type == BC_RADIAL_EQ) {
+            s->hub_p = rp->pressure[0];
+        }
+        if (rp->nradius == rp->n && rp->nradius > 1)
+            integrate_radial_eq(dens, vt, rp->radius, rp->pressure, rp->n, s->hub_p);
+        else
+            for (int q = 0; q < rp->n; q++) rp->pressure[q] = s->hub_p;
+        free(dens);
+        free(vt);
+    }
+}
+
+/* Solver::computeLogResidualNorm (src/solver.cpp:1488-1508), Matrix3D::norm
+ * (include/types.hpp:441-448). */
+static int log_residual_norm(const oracle_solver* s, double out[5]) {
+    for (int v = 0; v < 5; v++) {
+        double sum = 0;
+        for (long q = 0; q < s->n; q++) sum += s->R[v][q] * s->R[v][q];
+        double nrm = sqrt(sum);
+        if (isnan(nrm) || isinf(nrm)) return fail("Solver diverged: NaN or Inf detected in residual variable %d", v);
+        if (nrm >= DBL_MIN) out[v] = log10(nrm / (double)(s->ni * s->nj * s->nk));
+        else out[v] = -16.0;
+        if (out[v] < -16.0) out[v] = -16.0;
+    }
+    return 0;
+}
+
+/* Solver::checkConvergence (src/solver.cpp:2985-3015). */
+static int check_convergence(const oracle_solver* s, const double cur[5]) {
+    if (!s->steady) return 0;
+    for (int v = 0; v < 5; ++v) {
+        if (v == 3 && s->topology != TOPO_3D && s->topology != TOPO_AXI) continue;
+        if (v == 2 && s->topology == TOPO_1D) continue;
+        if (s->init_log[v] <= -15.99) continue;
+        if (cur[v] <= -15.0) continue;
+        if (cur[v] >= s->init_log[v] - (double)s->drop) return 0;
+    }
+    return 1;
+}
+
+/* -------------------------------------------------------------- set-up */
+
+static int read_grid(oracle_solver* s, const char* path) { /* src/input.cpp:14-82 */
+    FILE* f = fopen(path, "r");
+    if (!f) return fail("Error opening coordinates CSV file '%s'", path);
+    char* line = NULL;
+    size_t cap = 0;
+    long ni = 0, nj = 0, nk = 0;
+    char names[64][64];
+    int nh = 0;
+    while (getline(&line, &cap, f) > 0) {
+        if (!strncmp(line, "NI=", 3)) ni = atol(line + 3);
+        else if (!strncmp(line, "NJ=", 3)) nj = atol(line + 3);
+        else if (!strncmp(line, "NK=", 3)) nk = atol(line + 3);
+        else if (!strncmp(line, "x,y,z", 5)) {
+            char* save = NULL;
+            trim(line, "\r\n");
+            for (char* t = strtok_r(line, ",", &save); t && nh < 64; t = strtok_r(NULL, ",", &save))
+                snprintf(names[nh++], 64, "%s", t);
+            break;
+        }
+    }
+    s->ni = ni; s->nj = nj; s->nk = nk; s->n = ni * nj * nk;
+    if (s->n <= 0) { fclose(f); free(line); return fail("bad grid header in %s", path); }
+    double** cols = (double**)calloc(nh, sizeof(double*));
+    for (int h = 0; h < nh; h++) cols[h] = (double*)calloc(s->n, sizeof(double));
+    long np = 0;
+    while (getline(&line, &cap, f) > 0 && np < s->n) {
+        double vals[64];
+        int nv = 0;
+        char* p = line;
+        while (*p && nv < 64) {
+            char* end;
+            double v = strtod(p, &end);
+            if (end == p) break;
+            vals[nv++] = v;
+            p = end;
+            while (*p == ',' || *p == ' ') p++;
+            if (*p == '\r' || *p == '\n') break;
+        }
+        if (nv != nh) continue;
+        for (int h = 0; h < nh; h++) cols[h][np] = vals[h];
+        np++;
+    }
+    fclose(f);
+    free(line);
+    if (np != s->n) return fail("grid %s: read %ld points, expected %ld", path, np, s->n);
+    s->vert = (vec3*)calloc(s->n, sizeof(vec3));
+    for (int h = 0; h < nh; h++) {
+        int used = 0;
+        if (!strcmp(names[h], "x")) { for (long q = 0; q < s->n; q++) s->vert[q].x = cols[h][q]; used = 1; }
+        if (!strcmp(names[h], "y")) { for (long q = 0; q < s->n; q++) s->vert[q].y = cols[h][q]; used = 1; }
+        if (!strcmp(names[h], "z")) { for (long q = 0; q < s->n; q++) s->vert[q].z = cols[h][q]; used = 1; }
+        for (int fdx = 0; fdx < F_COUNT && !used; fdx++)
+            if (!strcmp(names[h], FIELD_NAMES[fdx])) { s->field[fdx] = cols[h]; cols[h] = NULL; used = 1; }
+        free(cols[h]);
+    }
+    free(cols);
+    if (nj == 1 && nk == 1) s->ndim = 1;
+    else if (nk == 1) s->ndim = 2;
+    else s->ndim = 3;
+    return 0;
+}
+
+/* Mesh::computeSurfaceVectorAndCenter (src/mesh.cpp:165-190). */
+static void surface_and_center(vec3 p1, vec3 p2, vec3 p3, vec3 p4, vec3* nrm, vec3* ctr) {
+    vec3 a1 = vsub(p2, p1), b1 = vsub(p3, p2), a2 = vsub(p3, p1), b2 = vsub(p4, p3);
+    vec3 s1 = vdiv(vcross(a1, b1), 2.0);
+    vec3 s2 = vdiv(vcross(a2, b2), 2.0);
+    *nrm = vadd(s1, s2);
+    vec3 c1 = vdiv(vadd(vadd(p1, p2), p3), 3.0);
+    vec3 c2 = vdiv(vadd(vadd(p1, p3), p4), 3.0);
+    *ctr = vdiv(vadd(vmul(c1, vmag(s1)), vmul(c2, vmag(s2))), vmag(s1) + vmag(s2));
+}
+
+static void build_dual_2d(oracle_solver* s) { /* src/mesh.cpp:373-435 */
+    long NI = s->ni, NJ = s->nj, DI = NI + 1, DJ = NJ + 1;
+    vec3* nodes = (vec3*)calloc(DI * DJ, sizeof(vec3));
+#define ND(i, j) nodes[(i) * DJ + (j)]
+#define VX(i, j) s->vert[idx3(s, (i), (j), 0)]
+    for (long i = 1; i < DI - 1; i++)
+        for (long j = 1; j < DJ - 1; j++)
+            ND(i, j) = vdiv(vadd(vadd(vadd(VX(i - 1, j - 1), VX(i, j - 1)), VX(i, j)), VX(i - 1, j)), 4.0);
+    ND(0, 0) = VX(0, 0);
+    ND(0, DJ - 1) = VX(0, NJ - 1);
+    ND(DI - 1, 0) = VX(NI - 1, 0);
+    ND(DI - 1, DJ - 1) = VX(NI - 1, NJ - 1);
+    for (long i = 1; i < DI - 1; i++) {
+        ND(i, 0) = vdiv(vadd(VX(i - 1, 0), VX(i, 0)), 2.0);
+        ND(i, DJ - 1) = vdiv(vadd(VX(i - 1, NJ - 1), VX(i, NJ - 1)), 2.0);
+    }
+    for (long j = 1; j < DJ - 1; j++) {
+        ND(0, j) = vdiv(vadd(VX(0, j - 1), VX(0, j)), 2.0);
+        ND(DI - 1, j) = vdiv(vadd(VX(NI - 1, j - 1), VX(NI - 1, j)), 2.0);
+    }
+    if (s->topology == TOPO_AXI) {
+        s->wedge = 1.0 * M_PI / 180.0;
+        for (long i = 0; i < DI; i++)
+            for (long j = 0; j < DJ; j++) {
+                vec3* d0 = &s->dual[didx(s, i, j, 0)];
+                vec3* d1 = &s->dual[didx(s, i, j, 1)];
+                d0->x = ND(i, j).x; d1->x = ND(i, j).x;
+                d0->y = ND(i, j).y * cos(-s->wedge / 2.0);
+                d1->y = ND(i, j).y * cos(+s->wedge / 2.0);
+                d0->z = ND(i, j).y * sin(-s->wedge / 2.0);
+                d1->z = ND(i, j).y * sin(+s->wedge / 2.0);
+            }
+    } else {
+        double th = 1.0;
+        for (long i = 0; i < DI; i++)
+            for (long j = 0; j < DJ; j++) {
+                vec3* d0 = &s->dual[didx(s, i, j, 0)];
+                vec3* d1 = &s->dual[didx(s, i, j, 1)];
+                d0->x = ND(i, j).x; d1->x = ND(i, j).x;
+                d0->y = ND(i, j).y; d1->y = ND(i, j).y;
+                d0->z = -th / 2.0; d1->z = +th / 2.0;
+            }
+    }
+#undef ND
+#undef VX
+    free(nodes);
+}
+
+static void build_dual_3d(oracle_solver* s) { /* src/mesh.cpp:478-557 */
+    long NI = s->ni, NJ = s->nj, NK = s->nk, DI = NI + 1, DJ = NJ + 1, DK = NK + 1;
+#define D(i, j, k) s->dual[didx(s, (i), (j), (k))]
+#define V(i, j, k) s->vert[idx3(s, (i), (j), (k))]
+    for (long i = 1; i < DI - 1; i++)
+        for (long j = 1; j < DJ - 1; j++)
+            for (long k = 1; k < DK - 1; k++) {
+                vec3 a = vadd(vadd(vadd(V(i - 1, j - 1, k - 1), V(i, j - 1, k - 1)), V(i - 1, j, k - 1)), V(i - 1, j - 1, k));
+                a = vadd(vadd(vadd(vadd(a, V(i, j, k - 1)), V(i, j - 1, k)), V(i - 1, j, k)), V(i, j, k));
+                D(i, j, k) = vdiv(a, 8.0);
+            }
+    D(0, 0, 0) = V(0, 0, 0);
+    D(DI - 1, 0, 0) = V(NI - 1, 0, 0);
+    D(0, DJ - 1, 0) = V(0, NJ - 1, 0);
+    D(0, 0, DK - 1) = V(0, 0, NK - 1);
+    D(DI - 1, DJ - 1, 0) = V(NI - 1, NJ - 1, 0);
+    D(DI - 1, 0, DK - 1) = V(NI - 1, 0, NK - 1);
+    D(0, DJ - 1, DK - 1) = V(0, NJ - 1, NK - 1);
+    D(DI - 1, DJ - 1, DK - 1) = V(NI - 1, NJ - 1, NK - 1);
+    for (long i = 1; i < DI - 1; i++) {
+        D(i, 0, 0) = vdiv(vadd(V(i - 1, 0, 0), V(i, 0, 0)), 2.0);
+        D(i, DJ - 1, 0) = vdiv(vadd(V(i - 1, NJ - 1, 0), V(i, NJ - 1, 0)), 2.0);
+        D(i, 0, DK - 1) = vdiv(vadd(V(i - 1, 0, NK - 1), V(i, 0, NK - 1)), 2.0);
+        D(i, DJ - 1, DK - 1) = vdiv(vadd(V(i - 1, NJ - 1, NK - 1), V(i, NJ - 1, NK - 1)), 2.0);
+    }
+    for (long j = 1; j < DJ - 1; j++) {
+        D(0, j, 0) = vdiv(vadd(V(0, j - 1, 0), V(0, j, 0)), 2.0);
+        D(DI - 1, j, 0) = vdiv(vadd(V(NI - 1, j - 1, 0), V(NI - 1, j, 0)), 2.0);
+        D(0, j, DK - 1) = vdiv(vadd(V(0, j - 1, NK - 1), V(0, j, NK - 1)), 2.0);
+        D(DI - 1, j, DK - 1) = vdiv(vadd(V(NI - 1, j - 1, NK - 1), V(NI - 1, j, NK - 1)), 2.0);
+    }
+    for (long k = 1; k < DK - 1; k++) {
+        D(0, 0, k) = vdiv(vadd(V(0, 0, k - 1), V(0, 0, k)), 2.0);
+        D(DI - 1, 0, k) = vdiv(vadd(V(NI - 1, 0, k - 1), V(NI - 1, 0, k)), 2.0);
+        D(0, DJ - 1, k) = vdiv(vadd(V(0, NJ - 1, k - 1), V(0, NJ - 1, k)), 2.0);
+        D(DI - 1, DJ - 1, k) = vdiv(vadd(V(NI - 1, NJ - 1, k - 1), V(NI - 1, NJ - 1, k)), 2.0);
+    }
+    for (long j = 1; j < DJ - 1; j++)
+        for (long k = 1; k < DK - 1; k++) {
+            D(0, j, k) = vdiv(vadd(vadd(vadd(V(0, j - 1, k - 1), V(0, j, k - 1)), V(0, j - 1, k)), V(0, j, k)), 4.0);
+            D(DI - 1, j, k) = vdiv(vadd(vadd(vadd(V(NI - 1, j - 1, k - 1), V(NI - 1, j, k - 1)), V(NI - 1, j - 1, k)), V(NI - 1, j, k)), 4.0);
+        }
+    for (long i = 1; i < DI - 1; i++)
+        for (long k = 1; k < DK - 1; k++) {
+            D(i, 0, k) = vdiv(vadd(vadd(vadd(V(i - 1, 0, k - 1), V(i, 0, k - 1)), V(i - 1, 0, k)), V(i, 0, k)), 4.0);
+            D(i, DJ - 1, k) = vdiv(vadd(vadd(vadd(V(i - 1, NJ - 1, k - 1), V(i, NJ - 1, k - 1)), V(i - 1, NJ - 1, k)), V(i, NJ - 1, k)), 4.0);
+        }
+    for (long i = 1; i < DI - 1; i++)
+        for (long j = 1; j < DJ - 1; j++) {
+            D(i, j, 0) = vdiv(vadd(vadd(vadd(V(i - 1, j - 1, 0), V(i, j - 1, 0)), V(i - 1, j, 0)), V(i, j, 0)), 4.0);
+            D(i, j, DK - 1) = vdiv(vadd(vadd(vadd(V(i - 1, j - 1, NK - 1), V(i, j - 1, NK - 1)), V(i - 1, j, NK - 1)), V(i, j, NK - 1)), 4.0);
+        }
+#undef D
+#undef V
+}
+
+static void build_interfaces(oracle_solver* s) { /* src/mesh.cpp:116-163 */
+    long DI = s->ni + 1, DJ = s->nj + 1, DK = s->nk + 1;
+#define D(i, j, k) s->dual[didx(s, (i), (j), (k))]
+    for (long i = 0; i < DI; i++)
+        for (long j = 0; j < DJ - 1; j++)
+            for (long k = 0; k < DK - 1; k++)
+                surface_and_center(D(i, j, k), D(i, j + 1, k), D(i, j + 1, k + 1), D(i, j, k + 1),
+                                   &s->sI[sIi(s, i, j, k)], &s->cI[sIi(s, i, j, k)]);
+    for (long i = 0; i < DI - 1; i++)
+        for (long j = 0; j < DJ; j++)
+            for (long k = 0; k < DK - 1; k++)
+                surface_and_center(D(i, j, k), D(i, j, k + 1), D(i + 1, j, k + 1), D(i + 1, j, k),
+                                   &s->sJ[sJi(s, i, j, k)], &s->cJ[sJi(s, i, j, k)]);
+    for (long i = 0; i < DI - 1; i++)
+        for (long j = 0; j < DJ - 1; j++)
+            for (long k = 0; k < DK; k++)
+                surface_and_center(D(i, j, k), D(i + 1, j, k), D(i + 1, j + 1, k), D(i, j + 1, k),
+                                   &s->sK[sKi(s, i, j, k)], &s->cK[sKi(s, i, j, k)]);
+#undef D
+}
+
+static void build_volumes(oracle_solver* s) { /* src/mesh.cpp:192-230 */
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                vec3 sf[6] = {vneg(s->sI[sIi(s, i, j, k)]), vneg(s->sJ[sJi(s, i, j, k)]),
+                              vneg(s->sK[sKi(s, i, j, k)]), s->sI[sIi(s, i + 1, j, k)],
+                              s->sJ[sJi(s, i, j + 1, k)], s->sK[sKi(s, i, j, k + 1)]};
+                vec3 cc[6] = {s->cI[sIi(s, i, j, k)], s->cJ[sJi(s, i, j, k)], s->cK[sKi(s, i, j, k)],
+                              s->cI[sIi(s, i + 1, j, k)], s->cJ[sJi(s, i, j + 1, k)], s->cK[sKi(s, i, j, k + 1)]};
+                double v = 0.0;
+                for (int f = 0; f < 6; f++) v += sf[f].x * cc[f].x;
+                s->vol[idx3(s, i, j, k)] = v;
+            }
+}
+
+/* interpolateScalar (src/math_utils.cpp:395-463), direction codes
+ * 0 W, 1 E, 2 N, 3 S, 4 B, 5 T. */
+static double interp_scalar(const oracle_solver* s, const double* fld, long i, long j, long k,
+                            vec3 pt, int dir) {
+    vec3 p0 = s->vert[idx3(s, i, j, k)];
+    double f0 = fld[idx3(s, i, j, k)];
+    long i1 = i, j1 = j, k1 = k;
+    switch (dir) {
+        case 0: if (i == 0) return f0; i1 = i - 1; break;
+        case 1: if (i == s->ni - 1) return f0; i1 = i + 1; break;
+        case 2: if (j == s->nj - 1) return f0; j1 = j + 1; break;
+        case 3: if (j == 0) return f0; j1 = j - 1; break;
+        case 4: if (k == 0) return f0; k1 = k - 1; break;
+        default: if (k == s->nk - 1) return f0; k1 = k + 1; break;
+    }
+    vec3 p1 = s->vert[idx3(s, i1, j1, k1)];
+    double f1 = fld[idx3(s, i1, j1, k1)];
+    double d0 = vmag(vsub(pt, p0)), d1 = vmag(vsub(pt, p1));
+    return f0 + (f1 - f0) * d0 / (d0 + d1);
+}
+
+/* computeGradientGreenGauss (src/math_utils.cpp:173-234) for the blockage
+ * (Mesh::computeInputGradients, src/mesh.cpp:571-581). */
+static void build_blockage_gradient(oracle_solver* s) {
+    s->gradb = (vec3*)calloc(s->n, sizeof(vec3));
+    const double* b = s->field[F_BLOCKAGE];
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                vec3 sf[6] = {vneg(s->sI[sIi(s, i, j, k)]), s->sI[sIi(s, i + 1, j, k)],
+                              s->sJ[sJi(s, i, j + 1, k)], vneg(s->sJ[sJi(s, i, j, k)]),
+                              vneg(s->sK[sKi(s, i, j, k)]), s->sK[sKi(s, i, j, k + 1)]};
+                vec3 cc[6] = {s->cI[sIi(s, i, j, k)], s->cI[sIi(s, i + 1, j, k)], s->cJ[sJi(s, i, j + 1, k)],
+                              s->cJ[sJi(s, i, j, k)], s->cK[sKi(s, i, j, k)], s->cK[sKi(s, i, j, k + 1)]};
+                int dirs[6] = {0, 1, 2, 3, 4, 5};
+                vec3 g = v3(0, 0, 0);
+                for (int f = 0; f < 6; f++) {
+                    double sc = interp_scalar(s, b, i, j, k, cc[f], dirs[f]);
+                    g = vadd(g, vmul(sf[f], sc));
+                }
+                s->gradb[idx3(s, i, j, k)] = vdiv(g, s->vol[idx3(s, i, j, k)]);
+            }
+}
+
+/* atan2FromZeroTo2pi (src/math_utils.cpp:466-471). */
+static double atan2_0_2pi(double y, double x) {
+    double a = atan2(y, x);
+    if (a < 0) a += 2 * M_PI;
+    return a;
+}
+
+/* Mesh::checkPeriodicity (src/mesh.cpp:584-619). */
+static int check_periodicity(oracle_solver* s, double transl, double angle) {
+    vec3 drag = v3(0.0, 0.0, transl);
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++) {
+            vec3 a = s->vert[idx3(s, i, j, 0)];
+            vec3 b = vsub(s->vert[idx3(s, i, j, s->nk - 1)], drag);
+            double ta = atan2_0_2pi(a.z, a.y), tb = atan2_0_2pi(b.z, b.y);
+            double dth = fmod(tb - ta, 2.0 * M_PI);
+            if (fabs(dth - angle) > 1E-4)
+                return fail("Periodicity check failed at (i,j)=(%ld,%ld)", i, j);
+            if (fabs(transl) > 1e-6 && angle == 0.0) {
+                if (fabs(b.z - a.z) > 1E-4) return fail("Axial translation mismatch at (%ld,%ld)", i, j);
+            }
+        }
+    s->periodic = 1;
+    return 0;
+}
+
+static int bc_type_of(const char* name, int* out) { /* boundaryTypeFromString, include/types.hpp:202-232 */
+    char low[128];
+    snprintf(low, sizeof low, "%s", name);
+    for (char* p = low; *p; p++) *p = (char)tolower((unsigned char)*p);
+    if (!strcmp(low, "inlet")) *out = BC_INLET;
+    else if (!strcmp(low, "outlet")) *out = BC_OUTLET;
+    else if (!strcmp(low, "radial_equilibrium")) *out = BC_RADIAL_EQ;
+    else if (!strcmp(low, "inviscid_wall")) *out = BC_INVISCID_WALL;
+    else if (!strcmp(low, "wedge")) *out = BC_WEDGE;
+    else if (!strcmp(low, "periodic")) *out = BC_PERIODIC;
+    else if (!strcmp(low, "throttle")) *out = BC_THROTTLE;
+    else if (!strcmp(low, "empty")) *out = BC_EMPTY;
+    else return fail("Boundary type '%s' is not supported by the oracle", name);
+    return 0;
+}
+
+static void dir_join(char* out, size_t n, const char* base_dir, const char* file) {
+    if (file[0] == '/') snprintf(out, n, "%s", file);
+    else snprintf(out, n, "%s/%s", base_dir, file);
+}
+
+/* Solver::readBoundaryFile + buildBoundaryDataStructures + map
+ * (src/solver.cpp:224-561). */
+static int read_boundaries(oracle_solver* s, const char* path) {
+    FILE* f = fopen(path, "r");
+    if (!f) return fail("Cannot open file: %s", path);
+    char line[4096];
+    int in_data = 0;
+    while (fgets(line, sizeof line, f)) {
+        trim(line, "\r\n");
+        if (!line[0]) continue;
+        if (strchr(line, '=')) continue;
+        if (strstr(line, "PATCH_NAME")) { in_data = 1; continue; }
+        if (!in_data) continue;
+        patch p;
+        memset(&p, 0, sizeof p);
+        char* save = NULL;
+        char* tok = strtok_r(line, ",", &save);
+        if (!tok) continue;
+        int w = 0;
+        for (char* c = tok; *c; c++) if (*c != ' ') p.name[w++] = *c;
+        p.name[w] = 0;
+        long v[6];
+        for (int q = 0; q < 6; q++) {
+            tok = strtok_r(NULL, ",", &save);
+            if (!tok) { fclose(f); return fail("bad boundary row for %s", p.name); }
+            v[q] = atol(tok);
+        }
+        p.i_min = v[0]; p.i_max = v[1]; p.j_min = v[2]; p.j_max = v[3]; p.k_min = v[4]; p.k_max = v[5];
+        char items[32][128];
+        int ni = cfg_list(&s->cfg, p.name, items, 32);
+        if (ni < 1) { fclose(f); return fail("Boundary info for %s is missing in configuration.", p.name); }
+        if (bc_type_of(items[0], &p.type)) { fclose(f); return 1; }
+        p.nvalues = 0;
+        for (int q = 1; q < ni && q < 17; q++) {
+            if (parse_double(items[q], &p.values[p.nvalues])) { fclose(f); return fail("Invalid float format for boundary value"); }
+            p.nvalues++;
+        }
+        if (p.i_min == p.i_max) p.orientation = p.i_min == 0 ? BI_ISTART : BI_IEND;
+        else if (p.j_min == p.j_max) p.orientation = p.j_min == 0 ? BI_JSTART : BI_JEND;
+        else p.orientation = p.k_min == 0 ? BI_KSTART : BI_KEND;
+        p.profile = -1;
+        s->patches = (patch*)realloc(s->patches, sizeof(patch) * (s->npatches + 1));
+        s->patches[s->npatches++] = p;
+    }
+    fclose(f);
+    return 0;
+}
+
+static int build_boundary_structures(oracle_solver* s) {
+    for (int m = 0; m < s->npatches; m++) {
+        patch* p = &s->patches[m];
+        if (p->type == BC_RADIAL_EQ || p->type == BC_THROTTLE) {
+            if (p->i_min != p->i_max) return fail("Radial equilibrium only supported on j-k patches");
+            if (p->i_min == 0) return fail("Radial equilibrium only supported to the last i-position");
+            if (p->j_max <= p->j_min) return fail("Invalid boundary indices for radial equilibrium patch: %s", p->name);
+            radial_profile rp;
+            memset(&rp, 0, sizeof rp);
+            rp.n = (int)(p->j_max - p->j_min);
+            rp.nradius = rp.n;
+            rp.pressure = (double*)calloc(rp.n, sizeof(double));
+            rp.radius = (double*)calloc(rp.n, sizeof(double));
+            for (long j = p->j_min; j < p->j_max; j++) rp.radius[j - p->j_min] = node_radius(s, p->i_max - 1, j, 0);
+            rp.patch = m;
+            p->profile = s->nprofiles;
+            s->profiles = (radial_profile*)realloc(s->profiles, sizeof(radial_profile) * (s->nprofiles + 1));
+            s->profiles[s->nprofiles++] = rp;
+        } else if (p->type == BC_PERIODIC) {
+            double id = p->values[0];
+            if (id == 0) {
+                s->per_transl = p->values[1];
+                s->per_angle_deg = p->values[2];
+                if (s->per_angle_deg == 360.0) s->per_angle_deg = 0.0;
+                s->per_angle_rad = s->per_angle_deg * M_PI / 180.0;
+                if (check_periodicity(s, s->per_transl, s->per_angle_rad)) return 1;
+            }
+            if (p->k_min != p->k_max) return fail("Periodic boundary only supported on i-j patches");
+            if (p->i_min != 0 || p->j_min != 0 || p->i_max != s->ni || p->j_max != s->nj)
+                return fail("Periodic boundary only supported on full i-j patches");
+            if (p->k_min == 0 && id != 0) return fail("Periodic boundary with i_min=0 must have boundary id 0");
+        }
+    }
+    s->mapI = (int*)malloc(sizeof(int) * 2 * s->nj * s->nk);
+    s->mapJ = (int*)malloc(sizeof(int) * s->ni * 2 * s->nk);
+    s->mapK = (int*)malloc(sizeof(int) * s->ni * s->nj * 2);
+    for (long q = 0; q < 2 * s->nj * s->nk; q++) s->mapI[q] = -1;
+    for (long q = 0; q < s->ni * 2 * s->nk; q++) s->mapJ[q] = -1;
+    for (long q = 0; q < s->ni * s->nj * 2; q++) s->mapK[q] = -1;
+    for (int m = 0; m < s->npatches; m++) {
+        const patch* p = &s->patches[m];
+        if (p->i_min == p->i_max) {
+            long t = p->i_min == 0 ? 0 : 1;
+            for (long j = p->j_min; j < p->j_max; j++)
+                for (long k = p->k_min; k < p->k_max; k++) s->mapI[(t * s->nj + j) * s->nk + k] = m;
+        } else if (p->j_min == p->j_max) {
+            long t = p->j_min == 0 ? 0 : 1;
+            for (long i = p->i_min; i < p->i_max; i++)
+                for (long k = p->k_min; k < p->k_max; k++) s->mapJ[(i * 2 + t) * s->nk + k] = m;
+        } else if (p->k_min == p->k_max) {
+            long t = p->k_min == 0 ? 0 : 1;
+            for (long i = p->i_min; i < p->i_max; i++)
+                for (long j = p->j_min; j < p->j_max; j++) s->mapK[(i * s->nj + j) * 2 + t] = m;
+        } else {
+            return fail("Invalid boundary definition: %s", p->name);
+        }
+    }
+    /* checkBoundaryConditionsMap (src/solver.cpp:565-593) */
+    for (long q = 0; q < 2 * s->nj * s->nk; q++) if (s->mapI[q] < 0) return fail("Missing boundary condition (I)");
+    if (s->topology != TOPO_1D)
+        for (long q = 0; q < s->ni * 2 * s->nk; q++) if (s->mapJ[q] < 0) return fail("Missing boundary condition (J)");
+    if (s->topology == TOPO_3D)
+        for (long q = 0; q < s->ni * s->nj * 2; q++) if (s->mapK[q] < 0) return fail("Missing boundary condition (K)");
+    return 0;
+}
+
+static int read_settings(oracle_solver* s) {
+    config* c = &s->cfg;
+    const char* v;
+    v = cfg_get(c, "TOPOLOGY");
+    if (!v) return fail("Not found value for key \"TOPOLOGY\" in configuration.");
+    if (!strcmp(v, "2D") || !strcmp(v, "2d")) s->topology = TOPO_2D;
+    else if (!strcmp(v, "3D") || !strcmp(v, "3d")) s->topology = TOPO_3D;
+    else if (!strcmp(v, "axisymmetric") || !strcmp(v, "Axisymmetric") || !strcmp(v, "AXISYMMETRIC")) s->topology = TOPO_AXI;
+    else if (!strcmp(v, "1D") || !strcmp(v, "1d")) s->topology = TOPO_1D;
+    else return fail("Invalid value for key \"TOPOLOGY\" in configuration.");
+    if (s->topology == TOPO_1D) return fail("1-D topology is outside the oracle's scope");
+
+    v = cfg_get(c, "CONVECTION_SCHEME");
+    if (!v) return fail("Not found value for key \"CONVECTION_SCHEME\" in configuration.");
+    if (!strcmp(v, "JST")) s->scheme = SCHEME_JST;
+    else if (!strcmp(v, "ROE") || !strcmp(v, "roe") || !strcmp(v, "Roe")) s->scheme = SCHEME_ROE;
+    else return fail("Invalid value for key \"CONVECTION_SCHEME\" in configuration.");
+    if (cfg_bool(c, "MUSCL_RECONSTRUCTION", 0, &s->muscl)) return 1;
+    v = cfg_get(c, "FLUX_LIMITER");
+    if (!v || !strcmp(v, "None")) s->limiter = LIM_NONE;
+    else if (!strcmp(v, "van albada")) s->limiter = LIM_VAN_ALBADA;
+    else if (!strcmp(v, "van leer")) s->limiter = LIM_VAN_LEER;
+    else if (!strcmp(v, "min mod")) s->limiter = LIM_MIN_MOD;
+    else return fail("Invalid value for key \"FLUX_LIMITER\" in configuration.");
+
+    /* Config::getTimeIntegration (src/config.cpp:250-276) */
+    const char* tik = cfg_get(c, "TIME_INTEGRATION") ? "TIME_INTEGRATION" : "TIME_INTEGRATION_TYPE";
+    v = cfg_get(c, tik);
+    char ti[64] = "0";
+    if (v) {
+        int w = 0;
+        for (const char* p = v; *p && w < 63; p++)
+            if (!isspace((unsigned char)*p)) ti[w++] = (char)tolower((unsigned char)*p);
+        ti[w] = 0;
+    }
+    if (!strcmp(ti, "0") || !strcmp(ti, "explicit_rk4") || !strcmp(ti, "rk4") || !strcmp(ti, "runge_kutta_4")) {
+        s->nstages = 4;
+        s->coeffs[0] = 1.0 / 4.0; s->coeffs[1] = 5.0 / 14.0; s->coeffs[2] = 14.0 / 25.0; s->coeffs[3] = 1.0;
+    } else if (!strcmp(ti, "1") || !strcmp(ti, "explicit_rk3") || !strcmp(ti, "rk3") || !strcmp(ti, "runge_kutta_3")) {
+        s->nstages = 3;
+        s->coeffs[0] = 8.0 / 17.0; s->coeffs[1] = 17.0 / 20.0; s->coeffs[2] = 1.0;
+    } else {
+        return fail("Only the explicit Runge-Kutta integrators are in the oracle's scope");
+    }
+
+    v = cfg_get(c, "TIME_STEP_METHOD");
+    if (!v) return fail("Not found value for key \"TIME_STEP_METHOD\" in configuration.");
+    if (!strcmp(v, "local")) s->dt_method = DT_LOCAL;
+    else if (!strcmp(v, "global")) s->dt_method = DT_GLOBAL;
+    else if (!strcmp(v, "fixed")) s->dt_method = DT_FIXED;
+    else return fail("Invalid value for key \"TIME_STEP_METHOD\" in configuration.");
+    /* Config::getCFL (include/config.hpp:124-133) */
+    if (cfg_get(c, "CFL")) { if (cfg_float(c, "CFL", &s->cfl)) return 1; }
+    else if (cfg_get(c, "CFL_START")) { if (cfg_float(c, "CFL_START", &s->cfl)) return 1; }
+    else if (cfg_get(c, "CFL_MAX")) { if (cfg_float(c, "CFL_MAX", &s->cfl)) return 1; }
+    else if (cfg_float(c, "CFL", &s->cfl)) return 1;
+    if (s->dt_method == DT_FIXED && cfg_float(c, "FIXED_TIME_STEP", &s->fixed_dt)) return 1;
+
+    int visc = 0;
+    if (cfg_bool(c, "VISCOSITY_ACTIVE", 0, &visc)) return 1;
+    if (visc) return fail("Viscous fluxes are outside the oracle's scope");
+    v = cfg_get(c, "FLUID_MODEL");
+    if (v && strcmp(v, "None") && strcmp(v, "Ideal") && strcmp(v, "ideal") && strcmp(v, "IDEAL"))
+        return fail("Only the ideal-gas model is in the oracle's scope");
+    if (cfg_float(c, "FLUID_GAMMA", &s->gamma)) return 1;
+    if (cfg_float(c, "FLUID_R_CONSTANT", &s->rgas)) return 1;
+    s->cp = (s->gamma * s->rgas) / (s->gamma - 1);
+
+    if (cfg_bool(c, "SIMULATION_IS_STEADY", 1, &s->steady)) return 1;
+    if (cfg_int_def(c, "RESIDUALS_DROP_CONVERGENCE", 16, &s->drop)) return 1;
+    if (cfg_float(c, "INIT_PRESSURE", &s->init_p)) return 1;
+    if (cfg_float_def(c, "OUTLET_PRESSURE_RAMP_ITERATIONS", 0.0, &s->ramp_iters)) return 1;
+    v = cfg_get(c, "INLET_REFERENCE_FRAME");
+    if (!v || !strcmp(v, "Cartesian") || !strcmp(v, "cartesian") || !strcmp(v, "CARTESIAN") || !strcmp(v, "None")) s->inlet_cyl = 0;
+    else if (!strcmp(v, "Cylindrical") || !strcmp(v, "cylindrical") || !strcmp(v, "CYLINDRICAL")) s->inlet_cyl = 1;
+    else return fail("Invalid value for key \"INLET_REFERENCE_FRAME\" in configuration.");
+
+    /* BFM (src/config.cpp:166-190, include/config.hpp) */
+    if (cfg_bool(c, "BFM_ACTIVE", 0, &s->bfm_active)) return 1;
+    if (cfg_bool(c, "BLOCKAGE_ACTIVE", 0, &s->blockage_active)) return 1;
+    v = cfg_get(c, "BFM_MODEL");
+    if (!v || !strcmp(v, "None")) s->bfm_model = BFM_NONE;
+    else if (!strcmp(v, "Hall")) s->bfm_model = BFM_HALL;
+    else if (!strcmp(v, "Hall-Thollet")) s->bfm_model = BFM_THOLLET;
+    else if (!strcmp(v, "Lift-Drag")) s->bfm_model = BFM_LIFT_DRAG;
+    else if (!strcmp(v, "Blockage")) s->bfm_model = BFM_BLOCKAGE;
+    else return fail("BFM_MODEL '%s' is outside the oracle's scope", v);
+    if (cfg_bool(c, "STALLED_BFM_ACTIVE", 0, &s->stalled)) return 1;
+    if (cfg_bool(c, "PERTURBATION_BODY_FORCE", 0, &s->perturb)) return 1;
+    if (cfg_float_def(c, "ROTATIONAL_SPEED_SCALING_FACTOR", 1.0, &s->speed_scale)) return 1;
+    if (cfg_bool(c, "ACCELERATION_ACTIVE", 0, &s->accel)) return 1;
+    if (s->accel) {
+        if (s->dt_method != DT_FIXED) return fail("Rotational speed scaling factor is only active for fixed time step method");
+        if (cfg_float(c, "ACCELERATION_INITIAL_TIME", &s->acc_t0) || cfg_float(c, "ACCELERATION_FINAL_TIME", &s->acc_t1) ||
+            cfg_float(c, "ROTATIONAL_SPEED_SCALING_FACTOR_INITIAL", &s->acc_s0) ||
+            cfg_float(c, "ROTATIONAL_SPEED_SCALING_FACTOR_FINAL", &s->acc_s1))
+            return 1;
+    }
+    if (s->perturb) {
+        char items[8][128];
+        if (cfg_list(c, "PERTURBATION_CENTER", items, 8) < 3) return fail("PERTURBATION_CENTER needs 3 values");
+        for (int q = 0; q < 3; q++) parse_double(items[q], &s->pert_center[q]);
+        if (cfg_float(c, "PERTURBATION_RADIAL_EXTENSION", &s->pert_radius) ||
+            cfg_float(c, "PERTURBATION_SCALING_FACTOR", &s->pert_scale) ||
+            cfg_float(c, "PERTURBATION_TIME_START", &s->pert_t0) ||
+            cfg_float(c, "PERTURBATION_TIME_DURATION", &s->pert_dur))
+            return 1;
+    }
+    if (s->bfm_model == BFM_THOLLET) {
+        if (cfg_float(c, "HALL_THOLLET_COEFFICIENT_KN", &s->kn) || cfg_float(c, "HALL_THOLLET_COEFFICIENT_KF", &s->kf) ||
+            cfg_float(c, "HALL_THOLLET_COEFFICIENT_KD", &s->kd))
+            return 1;
+        v = cfg_get(c, "HALL_THOLLET_OFF_DESIGN_ACTIVE");
+        if (!v) return fail("Not found value for key \"HALL_THOLLET_OFF_DESIGN_ACTIVE\" in configuration.");
+        if (!strcmp(v, "true") || !strcmp(v, "yes") || !strcmp(v, "1")) s->offdesign = 1;
+        else if (!strcmp(v, "false") || !strcmp(v, "no") || !strcmp(v, "0")) s->offdesign = 0;
+        else return fail("Invalid value for key \"HALL_THOLLET_OFF_DESIGN_ACTIVE\" in configuration.");
+        s->has_nu = cfg_get(c, "FLUID_KINEMATIC_VISCOSITY") != NULL;
+        if (!s->has_nu) return fail("Hall-Thollet without FLUID_KINEMATIC_VISCOSITY is outside the oracle's scope");
+        if (cfg_float(c, "FLUID_KINEMATIC_VISCOSITY", &s->nu)) return 1;
+    }
+    if (s->bfm_model == BFM_LIFT_DRAG) {
+        int le, te;
+        double d;
+        if (cfg_float(c, "LEADING_EDGE_INDEX", &d)) return 1;
+        le = (int)d;
+        if (cfg_float(c, "TRAILING_EDGE_INDEX", &d)) return 1;
+        te = (int)d;
+        s->le_idx = le; s->te_idx = te;
+    }
+    int turbo_out = 0;
+    if (cfg_bool(c, "TURBO_OUTPUT", 0, &turbo_out)) return 1;
+    if (cfg_bool(c, "ENABLE_GREITZER_MODELING", 0, &s->greitzer)) return 1;
+    if (s->greitzer && s->dt_method != DT_FIXED) return fail("Greitzer modeling is only compatible with fixed time step method");
+    if (s->greitzer) {
+        if (cfg_get(c, "GREITZER_PLENUM_VOLUME")) { if (cfg_float(c, "GREITZER_PLENUM_VOLUME", &s->plenum_volume)) return 1; }
+        else if (cfg_float(c, "GREITZER_PENUM_VOLUME", &s->plenum_volume)) return 1;
+        if (cfg_float_def(c, "GREITZER_AMBIENT_PRESSURE", 101325.0, &s->ambient_p)) return 1;
+    }
+    s->need_turbo = turbo_out || s->greitzer;
+    return 0;
+}
+
+/* Solver::updateTurboPerformance's inlet-orientation default
+ * (src/solver.cpp:1654-1680). */
+static void resolve_turbo_dir(oracle_solver* s) {
+    const char* v = cfg_get(&s->cfg, "TURBO_DIRECTION");
+    const char* d = v ? v : "i";
+    if (!v) {
+        for (int m = 0; m < s->npatches; m++)
+            if (s->patches[m].type == BC_INLET) {
+                if (s->patches[m].orientation == BI_JSTART) { d = "j"; break; }
+                if (s->patches[m].orientation == BI_JEND) { d = "-j"; break; }
+            }
+    }
+    if (!strcmp(d, "-i")) s->turbo_dir = 1;
+    else if (!strcmp(d, "j") || !strcmp(d, "+j")) s->turbo_dir = 2;
+    else if (!strcmp(d, "-j")) s->turbo_dir = 3;
+    else s->turbo_dir = 0;
+}
+
+/* FluidIdeal::computeInitFields (src/fluid_ideal.cpp:155-170) and
+ * Solver::initializeSolutionFromScratch (src/solver.cpp:777-836). */
+static int init_solution(oracle_solver* s) {
+    double M, T, p;
+    if (cfg_float(&s->cfg, "INIT_MACH_NUMBER", &M) || cfg_float(&s->cfg, "INIT_TEMPERATURE", &T) ||
+        cfg_float(&s->cfg, "INIT_PRESSURE", &p))
+        return 1;
+    int restart = 0;
+    if (cfg_bool(&s->cfg, "RESTART_SOLUTION", 0, &restart)) return 1;
+    if (restart) return fail("Restarts are outside the oracle's scope");
+    const char* raw = cfg_get(&s->cfg, "INIT_DIRECTION");
+    int adaptive = 0;
+    vec3 d0 = v3(0, 0, 0);
+    if (raw && !strcmp(raw, "adaptive")) adaptive = 1;
+    else {
+        char items[8][128];
+        int n = cfg_list(&s->cfg, "INIT_DIRECTION", items, 8);
+        if (n != 3) return fail("INIT_DIRECTION must have 3 components or be 'adaptive'");
+        parse_double(items[0], &d0.x); parse_double(items[1], &d0.y); parse_double(items[2], &d0.z);
+        if (d0.x == 0.0 && d0.y == 0.0 && d0.z == 0.0) adaptive = 1;
+    }
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                vec3 dir = d0;
+                if (adaptive) { /* Mesh::computeAdaptiveFlowDirection (src/mesh.cpp:637-661) */
+                    long ia = (i < s->ni - 1) ? i : s->ni - 2;
+                    dir = vnormalized(vsub(s->vert[idx3(s, ia + 1, j, k)], s->vert[idx3(s, ia, j, k)]));
+                }
+                double a = sqrt(s->gamma * s->rgas * T);
+                vec3 u = vmul(vmul(vdiv(dir, vmag(dir)), a), M);
+                double rho = p / (s->rgas * T);
+                double e = f_static_energy_p_rho(s, p, rho);
+                double um = vmag(u);
+                double et = e + 0.5 * (um * um);
+                long q = idx3(s, i, j, k);
+                s->U[0][q] = rho;
+                s->U[1][q] = rho * u.x;
+                s->U[2][q] = rho * u.y;
+                s->U[3][q] = rho * u.z;
+                s->U[4][q] = rho * et;
+            }
+    return 0;
+}
+
+int oracle_create(const char* ini_path, oracle_solver** out) {
+    *out = NULL;
+    oracle_solver* s = (oracle_solver*)calloc(1, sizeof(oracle_solver));
+    char base[4096], path[4096];
+    snprintf(base, sizeof base, "%s", ini_path);
+    char* slash = strrchr(base, '/');
+    if (slash) *slash = 0; else snprintf(base, sizeof base, ".");
+    if (cfg_load(&s->cfg, ini_path) || read_settings(s)) { oracle_destroy(s); return 1; }
+    const char* grid = cfg_get(&s->cfg, "GRID_FILE");
+    if (!grid) { fail("Not found value for key \"GRID_FILE\" in configuration."); oracle_destroy(s); return 1; }
+    dir_join(path, sizeof path, base, grid);
+    if (read_grid(s, path)) { oracle_destroy(s); return 1; }
+    if (s->ni < 3 || (s->topology != TOPO_1D && s->nj < 3) || (s->topology == TOPO_3D && s->nk < 3)) {
+        fail("the grid needs at least 3 nodes along every swept direction");
+        oracle_destroy(s);
+        return 1;
+    }
+    if ((s->topology == TOPO_3D) != (s->nk > 1)) {
+        fail("TOPOLOGY does not match the grid's NK");
+        oracle_destroy(s);
+        return 1;
+    }
+    long nd = (s->ni + 1) * (s->nj + 1) * (s->nk + 1);
+    s->dual = (vec3*)calloc(nd, sizeof(vec3));
+    long nI = (s->ni + 1) * s->nj * s->nk, nJ = s->ni * (s->nj + 1) * s->nk, nK = s->ni * s->nj * (s->nk + 1);
+    s->sI = (vec3*)calloc(nI, sizeof(vec3)); s->cI = (vec3*)calloc(nI, sizeof(vec3));
+    s->sJ = (vec3*)calloc(nJ, sizeof(vec3)); s->cJ = (vec3*)calloc(nJ, sizeof(vec3));
+    s->sK = (vec3*)calloc(nK, sizeof(vec3)); s->cK = (vec3*)calloc(nK, sizeof(vec3));
+    s->vol = (double*)calloc(s->n, sizeof(double));
+    if (s->topology == TOPO_3D) build_dual_3d(s);
+    else build_dual_2d(s);
+    build_interfaces(s);
+    build_volumes(s);
+    if (s->bfm_active) {
+        if (!s->field[F_BLOCKAGE]) { fail("blockage not found in the grid file"); oracle_destroy(s); return 1; }
+        build_blockage_gradient(s);
+        const int need[] = {F_NAX, F_NRAD, F_NTAN, F_RPM, F_BLADE_PRESENT, F_NBLADES};
+        for (unsigned q = 0; q < sizeof need / sizeof need[0]; q++)
+            if (!s->field[need[q]]) { fail("%s not found in the grid file", FIELD_NAMES[need[q]]); oracle_destroy(s); return 1; }
+    }
+    const char* bcf = cfg_get(&s->cfg, "BOUNDARY_CONDITIONS_FILEPATH");
+    if (!bcf) { fail("Not found value for key \"BOUNDARY_CONDITIONS_FILEPATH\" in configuration."); oracle_destroy(s); return 1; }
+    dir_join(path, sizeof path, base, bcf);
+    if (read_boundaries(s, path) || build_boundary_structures(s)) { oracle_destroy(s); return 1; }
+    resolve_turbo_dir(s);
+    for (int m = 0; m < s->npatches; m++)
+        if (s->patches[m].type == BC_THROTTLE) { s->need_turbo = 1; s->throttle_kt = s->patches[m].values[0]; }
+    if (s->greitzer && s->throttle_kt == 0.0) {
+        int found = 0;
+        for (int m = 0; m < s->npatches; m++) if (s->patches[m].type == BC_THROTTLE) found = 1;
+        if (!found) { fail("Greitzer modeling enabled but no throttle boundary condition found!"); oracle_destroy(s); return 1; }
+    }
+    for (int c = 0; c < 5; c++) {
+        s->U[c] = (double*)calloc(s->n, sizeof(double));
+        s->Utmp[c] = (double*)calloc(s->n, sizeof(double));
+        s->R[c] = (double*)calloc(s->n, sizeof(double));
+    }
+    s->dt = (double*)calloc(s->n, sizeof(double));
+    if (init_solution(s)) { oracle_destroy(s); return 1; }
+    /* Greitzer initial state (src/solver.cpp:752-765) */
+    if (s->greitzer) {
+        update_mass_flows(s, s->U);
+        update_turbo(s, s->U);
+        sv5 W = prim_of(state_at(s, s->U, s->ni - 1, 0, 0));
+        double ph = pressure_prim(s, W);
+        double Th = f_temperature_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
+        s->gz_p = ph; s->gz_min = s->turbo[0]; s->gz_mout = s->turbo[0]; s->gz_T = Th; s->gz_t = 0.0;
+    }
+    /* initial radial profiles (src/solver.cpp:767-776) */
+    for (int m = 0; m < s->nprofiles; m++) {
+        radial_profile* rp = &s->profiles[m];
+        const patch* p = &s->patches[rp->patch];
+        long i = p->i_min > 0 ? p->i_min - 1 : 0;
+        int kk = 0;
+        for (long j = p->j_min; j < p->j_max && kk < rp->n; j++) {
+            sv5 W = prim_of(state_at(s, s->U, i, j, 0));
+            rp->pressure[kk++] = pressure_prim(s, W);
+        }
+    }
+    *out = s;
+    return 0;
+}
+
+void oracle_destroy(oracle_solver* s) {
+    if (!s) return;
+    cfg_free(&s->cfg);
+    free(s->vert); free(s->dual);
+    free(s->sI); free(s->sJ); free(s->sK); free(s->cI); free(s->cJ); free(s->cK);
+    free(s->vol); free(s->gradb);
+    for (int f = 0; f < F_COUNT; f++) free(s->field[f]);
+    free(s->patches); free(s->mapI); free(s->mapJ); free(s->mapK);
+    for (int m = 0; m < s->nprofiles; m++) { free(s->profiles[m].pressure); free(s->profiles[m].radius); }
+    free(s->profiles);
+    for (int c = 0; c < 5; c++) { free(s->U[c]); free(s->Utmp[c]); free(s->R[c]); }
+    free(s->dt);
+    free(s->hist);
+    free(s);
+}
+
+void oracle_shape(const oracle_solver* s, long long out[3]) {
+    out[0] = s->ni; out[1] = s->nj; out[2] = s->nk;
+}
+
+#define HIST_W 16 /* 5 lognorm + 6 massflow + 4 turbo + 1 hub */
+
+static void hist_push(oracle_solver* s, const double lr[5]) {
+    if (s->nhist == s->hist_cap) {
+        s->hist_cap = s->hist_cap ? 2 * s->hist_cap : 1024;
+        s->hist = (double*)realloc(s->hist, sizeof(double) * HIST_W * s->hist_cap);
+    }
+    double* h = s->hist + HIST_W * s->nhist;
+    for (int v = 0; v < 5; v++) h[v] = lr[v];
+    for (int b = 0; b < 6; b++) h[5 + b] = s->massflow[b];
+    for (int b = 0; b < 4; b++) h[11 + b] = s->need_turbo ? s->turbo[b] : 0.0;
+    h[15] = s->hub_p;
+    s->nhist++;
+}
+
+/* The explicit branch of Solver::solve (src/solver.cpp:1296-1398). The
+ * state's first preprocessSolution(.., false) is a no-op for inviscid runs. */
+int oracle_run(oracle_solver* s, long n_iter, long* n_done, int* converged) {
+    *n_done = 0;
+    *converged = 0;
+    s->nhist = 0;
+    for (int c = 0; c < 5; c++) memcpy(s->Utmp[c], s->U[c], sizeof(double) * s->n);
+    for (long it = s->iter + 1; it <= s->iter + n_iter; it++) {
+        update_mass_flows(s, s->Utmp);
+        if (s->need_turbo) update_turbo(s, s->Utmp);
+        compute_timestep(s, s->Utmp);
+        if (s->nprofiles || s->greitzer) update_radial_profiles(s, s->Utmp);
+        for (int st = 0; st < s->nstages; st++) {
+            compute_residuals(s, s->Utmp, it);
+            update_solution(s, s->coeffs[st]);
+            periodic_solution(s);
+        }
+        for (int c = 0; c < 5; c++) memcpy(s->U[c], s->Utmp[c], sizeof(double) * s->n);
+        double m = s->dt[0];
+        for (long q = 1; q < s->n; q++) if (s->dt[q] < m) m = s->dt[q];
+        s->t += m;
+        double lr[5];
+        if (log_residual_norm(s, lr)) { *n_done = it - s->iter; s->iter = it; return 2; }
+        if (!s->has_init_log) {
+            for (int v = 0; v < 5; v++) s->init_log[v] = lr[v];
+            s->has_init_log = 1;
+        } else if (it <= 5) {
+            for (int v = 0; v < 5; v++) s->init_log[v] = dmax(s->init_log[v], lr[v]);
+        }
+        hist_push(s, lr);
+        *n_done = it - s->iter;
+        if (check_convergence(s, lr)) { *converged = 1; break; }
+    }
+    s->iter += *n_done;
+    return 0;
+}
+
+int oracle_residual(oracle_solver* s, double* dt, double* r0, double* r1, double* r2, double* r3,
+                    double* r4) {
+    for (int c = 0; c < 5; c++) memcpy(s->Utmp[c], s->U[c], sizeof(double) * s->n);
+    update_mass_flows(s, s->Utmp);
+    if (s->need_turbo) update_turbo(s, s->Utmp);
+    compute_timestep(s, s->Utmp);
+    if (s->nprofiles || s->greitzer) update_radial_profiles(s, s->Utmp);
+    compute_residuals(s, s->Utmp, s->iter + 1);
+    memcpy(dt, s->dt, sizeof(double) * s->n);
+    double* outs[5] = {r0, r1, r2, r3, r4};
+    for (int c = 0; c < 5; c++) memcpy(outs[c], s->R[c], sizeof(double) * s->n);
+    return 0;
+}
+
+void oracle_get_state(const oracle_solver* s, double* rho, double* rhou, double* rhov, double* rhow,
+                      double* rhoe) {
+    double* outs[5] = {rho, rhou, rhov, rhow, rhoe};
+    for (int c = 0; c < 5; c++) memcpy(outs[c], s->U[c], sizeof(double) * s->n);
+}
+
+void oracle_set_state(oracle_solver* s, const double* rho, const double* rhou, const double* rhov,
+                      const double* rhow, const double* rhoe) {
+    const double* ins[5] = {rho, rhou, rhov, rhow, rhoe};
+    for (int c = 0; c < 5; c++) memcpy(s->U[c], ins[c], sizeof(double) * s->n);
+}
+
+long oracle_history(const oracle_solver* s, double* lognorm, double* massflow, double* turbo,
+                    double* hub) {
+    for (long q = 0; q < s->nhist; q++) {
+        const double* h = s->hist + HIST_W * q;
+        if (lognorm) for (int v = 0; v < 5; v++) lognorm[5 * q + v] = h[v];
+        if (massflow) for (int b = 0; b < 6; b++) massflow[6 * q + b] = h[5 + b];
+        if (turbo) for (int b = 0; b < 4; b++) turbo[4 * q + b] = h[11 + b];
+        if (hub) hub[q] = h[15];
+    }
+    return s->nhist;
+}
+
+double oracle_time(const oracle_solver* s) { return s->t; }
