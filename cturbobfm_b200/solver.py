@@ -1,0 +1,214 @@
+"""Python binding of the C ABI in include/ctbfm.h (ctypes).
+
+``Solver`` mirrors the reference's ``Solver(Config&, Mesh&)`` + ``solve()``
+(include/solver.hpp:45-53) for one operating point given by an input.ini in the
+reference's format. All computation happens in libctbfm.so on the GPU; this
+module only moves host buffers across the C boundary. There is no CPU
+fallback: a missing library or device raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libctbfm.so")
+
+CTBFM_OK = 0
+CTBFM_E_CONFIG = 1
+CTBFM_E_CUDA = 2
+CTBFM_E_DIVERGED = 3
+CTBFM_E_ARGUMENT = 4
+CTBFM_E_UNSUPPORTED = 5
+
+STATUS_RUNNING, STATUS_CONVERGED, STATUS_DIVERGED = 0, 1, 2
+
+
+class CtbfmError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class SolverDiverged(CtbfmError):
+    pass
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("ni", ctypes.c_int64),
+        ("nj", ctypes.c_int64),
+        ("nk", ctypes.c_int64),
+        ("topology", ctypes.c_int32),
+        ("n_stages", ctypes.c_int32),
+        ("iteration", ctypes.c_int64),
+        ("max_iterations", ctypes.c_int64),
+        ("status", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("time", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+# Every symbol include/ctbfm.h declares, with its ctypes signature.
+_DP = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+_I64 = ctypes.c_int64
+SIGNATURES = {
+    "ctbfm_create_from_ini": ([ctypes.c_char_p, ctypes.POINTER(_VP)], ctypes.c_int),
+    "ctbfm_destroy": ([_VP], None),
+    "ctbfm_set_stream": ([_VP, _VP], ctypes.c_int),
+    "ctbfm_get_info": ([_VP, ctypes.POINTER(Info)], ctypes.c_int),
+    "ctbfm_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
+    "ctbfm_enqueue": ([_VP, _I64], ctypes.c_int),
+    "ctbfm_solve": ([_VP, ctypes.POINTER(_I64)], ctypes.c_int),
+    "ctbfm_compute_residual": ([_VP] + [_DP] * 6, ctypes.c_int),
+    "ctbfm_get_state": ([_VP] + [_DP] * 5, ctypes.c_int),
+    "ctbfm_set_state": ([_VP] + [_DP] * 5, ctypes.c_int),
+    "ctbfm_get_lognorm": ([_VP, _DP], ctypes.c_int),
+    "ctbfm_get_history": ([_VP, _I64, _DP, _DP, _DP, _DP, ctypes.POINTER(_I64)], ctypes.c_int),
+    "ctbfm_get_turbo": ([_VP, _DP, _DP], ctypes.c_int),
+    "ctbfm_profile_kernels": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
+    "ctbfm_last_error": ([], ctypes.c_char_p),
+    "ctbfm_version": ([], ctypes.c_char_p),
+}
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libctbfm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise CtbfmError(CTBFM_E_CUDA, f"{path} is missing: build it with cturbobfm_b200.build.build()")
+        lib = ctypes.CDLL(path)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+def _check(rc: int):
+    if rc != CTBFM_OK:
+        msg = load_library().ctbfm_last_error().decode()
+        if rc == CTBFM_E_DIVERGED:
+            raise SolverDiverged(rc, msg)
+        raise CtbfmError(rc, msg)
+
+
+class Solver:
+    """One operating point on the current CUDA device."""
+
+    def __init__(self, ini_path: str):
+        lib = load_library()
+        h = _VP()
+        _check(lib.ctbfm_create_from_ini(os.path.abspath(ini_path).encode(), ctypes.byref(h)))
+        self._h = h
+        inf = self.info()
+        self.shape = (int(inf.ni), int(inf.nj), int(inf.nk))
+        self.n = self.shape[0] * self.shape[1] * self.shape[2]
+        self.n_stages = int(inf.n_stages)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().ctbfm_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> Info:
+        inf = Info()
+        _check(load_library().ctbfm_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _check(load_library().ctbfm_set_stream(self._h, _VP(stream_ptr or 0)))
+
+    def step(self, n_iter: int) -> int:
+        done = _I64()
+        _check(load_library().ctbfm_step(self._h, int(n_iter), ctypes.byref(done)))
+        return int(done.value)
+
+    def enqueue(self, n_iter: int):
+        _check(load_library().ctbfm_enqueue(self._h, int(n_iter)))
+
+    def solve(self) -> int:
+        done = _I64()
+        _check(load_library().ctbfm_solve(self._h, ctypes.byref(done)))
+        return int(done.value)
+
+    def residual(self):
+        dt = np.zeros(self.n)
+        r = np.zeros((5, self.n))
+        _check(load_library().ctbfm_compute_residual(self._h, _ptr(dt), *[_ptr(r[v]) for v in range(5)]))
+        return dt, r
+
+    def state(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        u = np.zeros((5, self.n)) if out is None else out
+        _check(load_library().ctbfm_get_state(self._h, *[_ptr(u[v]) for v in range(5)]))
+        return u
+
+    def set_state(self, u: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        _check(load_library().ctbfm_set_state(self._h, *[_ptr(u[v]) for v in range(5)]))
+
+    def lognorm(self) -> np.ndarray:
+        out = np.zeros(5)
+        _check(load_library().ctbfm_get_lognorm(self._h, _ptr(out)))
+        return out
+
+    def history(self) -> Dict[str, np.ndarray]:
+        lib = load_library()
+        rows = _I64()
+        _check(lib.ctbfm_get_history(self._h, 0, None, None, None, None, ctypes.byref(rows)))
+        n = int(rows.value)
+        ln, mf, tp, hub = np.zeros((n, 5)), np.zeros((n, 6)), np.zeros((n, 4)), np.zeros(n)
+        if n:
+            _check(lib.ctbfm_get_history(self._h, n, _ptr(ln), _ptr(mf), _ptr(tp), _ptr(hub), ctypes.byref(rows)))
+        return {"lognorm": ln, "massflow": mf, "turbo": tp, "hub": hub}
+
+    def turbo(self):
+        mf, tp = np.zeros(6), np.zeros(4)
+        _check(load_library().ctbfm_get_turbo(self._h, _ptr(mf), _ptr(tp)))
+        return mf, tp
+
+    KERNELS = ("k_bint", "k_dt", "k_pre", "k_faces_I", "k_faces_J", "k_faces_K", "k_nodes", "k_periodic",
+               "k_finalize")
+
+    def profile_kernels(self, reps: int = 20) -> Dict[str, float]:
+        """Average device time per launch (ms) of each kernel kind, CUDA events."""
+        out = np.zeros(len(self.KERNELS))
+        _check(load_library().ctbfm_profile_kernels(self._h, int(reps), _ptr(out)))
+        return {k: float(v) for k, v in zip(self.KERNELS, out)}
+
+    @property
+    def iteration(self) -> int:
+        return int(self.info().iteration)
+
+    @property
+    def status(self) -> int:
+        return int(self.info().status)
+
+    @property
+    def time(self) -> float:
+        return float(self.info().time)

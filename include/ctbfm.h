@@ -1,0 +1,158 @@
+/* ctbfm.h — C ABI of the B200-native CTurboBFM explicit residual-and-update loop.
+ *
+ * The reference (Propulsion-Power-TU-Delft/CTurboBFM) has no FFI; its
+ * extension points are C++ classes driven per face / per node through virtual
+ * calls. This header is the drop-in boundary that replaces them with batched
+ * device execution. Each entry point names the reference interface it stands
+ * for:
+ *
+ *   ctbfm_create_from_ini   Config(input.ini) + Mesh(config) + Solver(config, mesh)
+ *                           (src/turbobfm.cpp:15-27, src/config.cpp:8-13,
+ *                            src/mesh.cpp:11-40, src/solver.cpp:18-31)
+ *   ctbfm_solve             Solver::solve() explicit branch (src/solver.cpp:1296-1424)
+ *   ctbfm_step              n iterations of that loop (src/solver.cpp:1337-1398)
+ *   ctbfm_compute_residual  Solver::computeTimestepArray + Solver::computeResiduals
+ *                           (src/solver.cpp:1531-1630, 1783-1833) on the current state
+ *   ctbfm_get_state /
+ *   ctbfm_set_state         Solver::_conservativeSolution (FlowSolution,
+ *                           include/types.hpp:763-1018), reference layout
+ *                           (i*NJ + j)*NK + k, five arrays of doubles
+ *   ctbfm_get_lognorm       Solver::computeLogResidualNorm (src/solver.cpp:1488-1508)
+ *   ctbfm_get_turbo         Solver::updateMassFlows / updateTurboPerformance
+ *                           (src/solver.cpp:1633-1781)
+ *   ctbfm_last_error        the std::runtime_error text the reference would throw
+ *
+ * Conventions
+ *   - every function returns 0 on success and a non-zero CTBFM_E* code on
+ *     error; no C++ exception crosses this boundary; ctbfm_last_error() gives
+ *     the message of the calling thread's last error;
+ *   - the library owns all device memory; the caller owns host buffers;
+ *   - divergence (NaN/Inf residual norm, the reference's "Solver diverged")
+ *     is reported as CTBFM_E_DIVERGED, never as a device fault;
+ *   - a handle is bound to one CUDA stream and is not thread safe; separate
+ *     handles may be driven from separate host threads.
+ */
+#ifndef CTBFM_H
+#define CTBFM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ctbfm_solver ctbfm_solver;
+
+enum {
+    CTBFM_OK = 0,
+    CTBFM_E_CONFIG = 1,      /* invalid or unsupported input.ini / grid / boundary file */
+    CTBFM_E_CUDA = 2,        /* CUDA runtime error (allocation, launch) */
+    CTBFM_E_DIVERGED = 3,    /* NaN or Inf in a residual norm */
+    CTBFM_E_ARGUMENT = 4,    /* bad argument (null pointer, wrong size) */
+    CTBFM_E_UNSUPPORTED = 5  /* feature outside this library's scope */
+};
+
+enum {
+    CTBFM_STATUS_RUNNING = 0,
+    CTBFM_STATUS_CONVERGED = 1,
+    CTBFM_STATUS_DIVERGED = 2
+};
+
+typedef struct {
+    int64_t ni, nj, nk;       /* nodes (= control volumes) per direction */
+    int32_t topology;         /* 0 = 2D, 1 = 3D, 2 = axisymmetric */
+    int32_t n_stages;         /* Runge-Kutta stages per iteration (4 or 3) */
+    int64_t iteration;        /* iterations performed so far */
+    int64_t max_iterations;   /* N_ITERATIONS */
+    int32_t status;           /* CTBFM_STATUS_* */
+    int32_t precision;        /* 0 = FP64 */
+    double time;              /* physical time sum of min(dt) */
+} ctbfm_info;
+
+/* Builds a solver from an input.ini in the reference's format (the grid CSV and
+ * boundaries.csv it names resolve relative to the ini's directory) and uploads
+ * everything to the current CUDA device. */
+int ctbfm_create_from_ini(const char* ini_path, ctbfm_solver** out);
+
+/* Releases device memory, graphs and streams owned by the solver. */
+void ctbfm_destroy(ctbfm_solver* s);
+
+/* Binds the solver to a caller-owned CUDA stream (a cudaStream_t passed as
+ * void*); NULL restores the solver's own stream. */
+int ctbfm_set_stream(ctbfm_solver* s, void* cuda_stream);
+
+int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out);
+
+/* Runs up to n_iter iterations (fewer if the convergence test fires or the
+ * solution diverges). *n_done receives the iterations performed. Returns
+ * CTBFM_E_DIVERGED when a residual norm is NaN/Inf. Synchronises the stream. */
+int ctbfm_step(ctbfm_solver* s, int64_t n_iter, int64_t* n_done);
+
+/* Enqueues exactly n_iter iterations on the solver's stream without any host
+ * synchronisation (kernels of iterations after convergence or divergence
+ * return immediately). For timing and CUDA-graph capture. */
+int ctbfm_enqueue(ctbfm_solver* s, int64_t n_iter);
+
+/* Runs the whole loop to N_ITERATIONS or convergence, like Solver::solve(). */
+int ctbfm_solve(ctbfm_solver* s, int64_t* n_done);
+
+/* One time-step + residual evaluation of the current state with the next
+ * iteration's number, without advancing anything but the boundary-profile
+ * and plenum state the reference also advances there. Outputs are NI*NJ*NK
+ * doubles each (dt) and 5 arrays (residual, reference layout). */
+int ctbfm_compute_residual(ctbfm_solver* s, double* dt, double* r_rho, double* r_rhou,
+                           double* r_rhov, double* r_rhow, double* r_rhoe);
+
+/* Conservative state U^n (host buffers of NI*NJ*NK doubles each). */
+int ctbfm_get_state(ctbfm_solver* s, double* rho, double* rhou, double* rhov, double* rhow,
+                    double* rhoe);
+int ctbfm_set_state(ctbfm_solver* s, const double* rho, const double* rhou, const double* rhov,
+                    const double* rhow, const double* rhoe);
+
+/* log10 residual norms of the last iteration (5 doubles). */
+int ctbfm_get_lognorm(ctbfm_solver* s, double out[5]);
+
+/* Per-iteration history of the last ctbfm_step / ctbfm_solve call:
+ * log10 residual norms (5 per iteration), boundary mass flows (6: I start,
+ * I end, J start, J end, K start, K end), turbo performance (4: mass flow,
+ * PRtt, TRtt, eta_tt) and hub static pressure (1). Returns the number of rows
+ * written in *n_rows; pass NULL arrays to query the count. */
+int ctbfm_get_history(ctbfm_solver* s, int64_t max_rows, double* lognorm, double* massflow,
+                      double* turbo, double* hub, int64_t* n_rows);
+
+/* Mass flows (6) and turbo performance (4) of the current state, computed on
+ * the device in FP64. */
+int ctbfm_get_turbo(ctbfm_solver* s, double massflow[6], double turbo[4]);
+
+/* Kernel kinds timed by ctbfm_profile_kernels, in output order. */
+enum {
+    CTBFM_K_BOUNDARY_INTEGRALS = 0, /* k_bint */
+    CTBFM_K_TIME_STEP = 1,          /* k_dt */
+    CTBFM_K_PRE_STAGE = 2,          /* k_pre */
+    CTBFM_K_FACES_I = 3,            /* k_faces<I> */
+    CTBFM_K_FACES_J = 4,            /* k_faces<J> */
+    CTBFM_K_FACES_K = 5,            /* k_faces<K> (3-D) */
+    CTBFM_K_NODES = 6,              /* k_nodes */
+    CTBFM_K_PERIODIC = 7,           /* k_periodic (periodic cases) */
+    CTBFM_K_FINALIZE = 8,           /* k_finalize */
+    CTBFM_K_COUNT = 9
+};
+
+/* Measurement hook (no counterpart in the reference): launches each kernel
+ * kind of one iteration `reps` times on the solver's stream, bracketed by
+ * CUDA events, and writes the average duration in milliseconds per launch to
+ * out_ms[CTBFM_K_COUNT] (0 for kinds this case does not launch). The state,
+ * time step and control block are restored afterwards. */
+int ctbfm_profile_kernels(ctbfm_solver* s, int reps, double* out_ms);
+
+/* Message of the calling thread's last error ("" if none). */
+const char* ctbfm_last_error(void);
+
+/* Library version string. */
+const char* ctbfm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,5 +1,5 @@
 // Test harness around the reference solver (CTurboBFM), compiled from the
-// reference's own sources by build_ref.sh. It is test infrastructure: it gives
+// reference's own sources by refbuild/Makefile. It is test infrastructure: it gives
 // the oracle restatement and the CUDA path a bit-exact target.
 //
 // Modes

@@ -1,0 +1,57 @@
+"""Small operating points shared by the oracle-pinning and GPU parity tests.
+Each entry: name -> (case factory, iterations). Sizes are chosen so the CPU
+oracle finishes in well under a second per case."""
+
+import dataclasses
+
+from cturbobfm_b200 import cases
+
+
+def _throttle(greitzer: bool):
+    c = cases.meridional(ni=48, nj=16, bfm_model="Hall-Thollet")
+    c.patches[1] = dataclasses.replace(c.patches[1], spec="throttle, 0.5")
+    kw = dict(TIME_STEP_METHOD="fixed", FIXED_TIME_STEP="2e-7")
+    if greitzer:
+        kw.update(ENABLE_GREITZER_MODELING="yes", GREITZER_PLENUM_VOLUME="0.05")
+    return c.with_settings(**kw)
+
+
+def _sector(angle_deg: float, nk: int = 9):
+    """3-D annular sector with periodic k faces at the given angle and a
+    cylindrical-frame swirling inlet (no BFM)."""
+    import math
+    import numpy as np
+
+    c = cases.annulus3d(ni=20, nj=8, nk=nk, scheme="JST", muscl=False, rk=4, bfm_model="None")
+    ni, nj = c.shape[0], c.shape[1]
+    th = np.linspace(0.0, math.radians(angle_deg), nk)
+    r = np.sqrt(c.y ** 2 + c.z ** 2)
+    c.y[:] = r * np.cos(th)[None, None, :]
+    c.z[:] = r * np.sin(th)[None, None, :]
+    c.fields.clear()
+    c.patches[0] = dataclasses.replace(c.patches[0], spec="inlet, 101325.0, 288.15, 1, 0, 0.3")
+    c.patches[1] = dataclasses.replace(c.patches[1], spec="radial_equilibrium, 95000")
+    c.patches[4] = dataclasses.replace(c.patches[4], spec=f"periodic, 0, 0, {angle_deg}")
+    c.patches[5] = dataclasses.replace(c.patches[5], spec=f"periodic, 1, 0, {angle_deg}")
+    s = dict(c.settings)
+    s["BFM_ACTIVE"] = "no"
+    s["INLET_REFERENCE_FRAME"] = "cylindrical"
+    return dataclasses.replace(c, settings=s)
+
+
+CASES = {
+    "bump_jst_rk4": (lambda: cases.bump2d(ni=24, nj=12), 20),
+    "bump_roe_vanalbada_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
+    "bump_roe_vanleer_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van leer", rk=3, cfl=0.8), 20),
+    "bump_roe_minmod_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="min mod", rk=3, cfl=0.8), 20),
+    "bump_roe_first_order": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", rk=4, cfl=0.8), 20),
+    "bump_global_dt": (lambda: cases.bump2d(ni=24, nj=12).with_settings(TIME_STEP_METHOD="global", CFL="1.0"), 20),
+    "bump_outlet_ramp": (lambda: cases.bump2d(ni=24, nj=12).with_settings(OUTLET_PRESSURE_RAMP_ITERATIONS="10"), 20),
+    "meridional_hall": (lambda: cases.meridional(ni=24, nj=10), 20),
+    "meridional_thollet_radial_eq": (lambda: cases.meridional(ni=48, nj=16, bfm_model="Hall-Thollet", outlet="radial_equilibrium", p_ratio=1.0), 20),
+    "meridional_throttle": (lambda: _throttle(False), 20),
+    "meridional_greitzer": (lambda: _throttle(True), 20),
+    "annulus_roe_hall": (lambda: cases.annulus3d(ni=20, nj=8, nk=9), 10),
+    "annulus_jst_thollet": (lambda: cases.annulus3d(ni=40, nj=12, nk=17, scheme="JST", muscl=False, rk=4, bfm_model="Hall-Thollet"), 5),
+    "sector45_jst_cylindrical_inlet": (lambda: _sector(45.0), 10),
+}
