@@ -1,0 +1,70 @@
+"""The C ABI boundary without a GPU: libctbfm.so loads, exports every function
+include/ctbfm.h declares (and the Python binding knows each signature), and
+configuration errors come back as status codes with the reference's messages
+before any device work."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "ctbfm.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ctbfm_[a-z_0-9]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from cturbobfm_b200 import build, solver
+
+    if not os.path.exists(solver.LIB_PATH):
+        build.build()
+    return solver.load_library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    from cturbobfm_b200 import solver
+
+    names = declared_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in solver.SIGNATURES, name
+
+
+def test_version(lib):
+    assert b"sm_100a" in lib.ctbfm_version()
+
+
+def test_missing_input_file_is_a_config_error(lib, tmp_path):
+    h = ctypes.c_void_p()
+    rc = lib.ctbfm_create_from_ini(str(tmp_path / "nope.ini").encode(), ctypes.byref(h))
+    assert rc == 1
+    assert b"Failed to load configuration file" in lib.ctbfm_last_error()
+    assert not h.value
+
+
+@pytest.mark.parametrize("key,value,message", [
+    ("TOPOLOGY", "4D", "Invalid value for key \"TOPOLOGY\""),
+    ("CONVECTION_SCHEME", "AUSM", "Invalid value for key \"CONVECTION_SCHEME\""),
+    ("FLUX_LIMITER", "vanalbada", "Invalid value for key \"FLUX_LIMITER\""),
+    ("TIME_INTEGRATION_TYPE", "2", "Implicit time integration"),
+])
+def test_invalid_settings_are_rejected(lib, tmp_path, key, value, message):
+    from cturbobfm_b200 import cases
+
+    ini = cases.bump2d(ni=12, nj=6).with_settings(**{key: value}).write(str(tmp_path))
+    h = ctypes.c_void_p()
+    rc = lib.ctbfm_create_from_ini(ini.encode(), ctypes.byref(h))
+    assert rc == 1
+    assert message.encode() in lib.ctbfm_last_error()
+
+
+def test_null_arguments(lib):
+    assert lib.ctbfm_create_from_ini(None, None) == 4
+    assert lib.ctbfm_step(None, 1, None) == 4

@@ -1,0 +1,68 @@
+"""GPU behaviour beyond the small parity cases: divergence at the same
+iteration as the oracle, full-size workloads against the oracle for a few
+iterations, determinism, and the stop-at-convergence contract."""
+
+import numpy as np
+import pytest
+
+from cturbobfm_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b):
+    scale = np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return (np.abs(a - b).max(axis=1) / scale).max()
+
+
+def test_divergence_is_reported_at_the_oracles_iteration(tmp_path, oracle_lib):
+    from cturbobfm_b200 import Solver, SolverDiverged
+
+    ini = cases.bump2d(ni=96, nj=32, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=1.2).write(str(tmp_path))
+    ro = oracle_lib.Oracle(ini).run(500)
+    assert ro["status"] == 2
+    with Solver(ini) as s:
+        with pytest.raises(SolverDiverged, match="Solver diverged"):
+            s.step(500)
+        assert s.iteration == ro["iterations"]
+        assert s.status == 2
+        assert s.step(10) == 0  # a diverged run stays stopped
+
+
+@pytest.mark.parametrize("which,n", [("bump2d_192x64", 20), ("annulus3d_160x48x64", 2)])
+def test_full_size_workloads_match_oracle(which, n, tmp_path, oracle_lib):
+    from cturbobfm_b200 import Solver
+
+    case = cases.bump2d() if which.startswith("bump") else cases.annulus3d()
+    ini = case.write(str(tmp_path))
+    o = oracle_lib.Oracle(ini)
+    o.run(n)
+    with Solver(ini) as s:
+        assert s.step(n) == n
+        assert rel_err(s.state(), o.state()) <= 1e-12
+        assert np.abs(s.lognorm() - o.history()["lognorm"][-1]).max() <= 1e-10
+
+
+def test_runs_are_deterministic(tmp_path):
+    from cturbobfm_b200 import Solver
+
+    ini = cases.annulus3d(ni=80, nj=24, nk=33, cfl=1.0).write(str(tmp_path))
+    out = []
+    for _ in range(2):
+        with Solver(ini) as s:
+            s.step(25)
+            out.append((s.state(), s.lognorm()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_step_chunks_equal_one_long_step(tmp_path):
+    from cturbobfm_b200 import Solver
+
+    ini = cases.meridional(ni=48, nj=16).write(str(tmp_path))
+    with Solver(ini) as a, Solver(ini) as b:
+        a.step(37)
+        for n in (1, 8, 3, 16, 9):
+            b.step(n)
+        assert np.array_equal(a.state(), b.state())
+        assert a.time == b.time
