@@ -26,7 +26,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["device/kernels.cu"]
+CU_SOURCES = ["device/kernels.cu", "device/noalloc.cu"]
 CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/solver.cpp", "capi.cpp"]
 
 

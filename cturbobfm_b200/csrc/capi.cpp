@@ -150,6 +150,17 @@ int ctbfm_compute_residual(ctbfm_solver* s, double* dt, double* r0, double* r1, 
     });
 }
 
+// See include/ctbfm.h: residual evaluation that allocates no device memory.
+int ctbfm_compute_residual_noalloc(ctbfm_solver* s, double* dt, double* r0, double* r1, double* r2, double* r3,
+                                   double* r4) {
+    if (!s || !dt || !r0 || !r1 || !r2 || !r3 || !r4) return setError(CTBFM_E_ARGUMENT, "null argument");
+    return guarded([&] {
+        double* const r[5] = {r0, r1, r2, r3, r4};
+        s->solver->computeResidualNoAlloc(dt, r);
+        return CTBFM_OK;
+    });
+}
+
 int ctbfm_get_state(ctbfm_solver* s, double* rho, double* rhou, double* rhov, double* rhow, double* rhoe) {
     if (!s || !rho || !rhou || !rhov || !rhow || !rhoe) return setError(CTBFM_E_ARGUMENT, "null argument");
     return guarded([&] {

@@ -30,4 +30,9 @@ cudaError_t launchPeriodic(const DevCase& c, P5 Uout, double alpha, bool last, i
 
 constexpr int kKernelKinds = 9;
 
+// Static device scratch of ctbfm_compute_residual_noalloc (noalloc.cu): its
+// device address on the current device (looked up once per device) and size.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+cudaError_t noallocScratch(double** ptr, size_t* bytes);
+
 }  // namespace ctbfm

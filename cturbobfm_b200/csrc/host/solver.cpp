@@ -702,6 +702,49 @@ void Solver::computeResidual(double* dt, double* const r[5]) {
         check(cudaMemcpy(r[v], c_.S2[v], N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
 }
 
+// The residual evaluation of computeResidual with its per-face flux
+// contributions kept in the static scratch array of noalloc.cu; nothing is
+// allocated on the device (the caller cannot, or must not, call cudaMalloc).
+void Solver::computeResidualNoAlloc(double* dt, double* const r[5]) {
+    double* scratch = nullptr;
+    size_t bytes = 0;
+    check(noallocScratch(&scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
+    const int dirs = c_.topo == 1 ? 3 : 2;
+    size_t faces = 0;
+    for (int d = 0; d < dirs; d++) faces += static_cast<size_t>(mesh_.faceCount(d));
+    if (faces * 5 * sizeof(double) > bytes)
+        throw ConfigError("ctbfm_compute_residual_noalloc: the case has " + std::to_string(faces) +
+                          " faces and needs " + std::to_string(faces * 5 * sizeof(double)) +
+                          " bytes of face scratch; the static array holds " + std::to_string(bytes) +
+                          " bytes (at most " + std::to_string(bytes / (5 * sizeof(double))) + " faces)");
+    const Control c0 = control();
+    itHost_ = c0.it;
+    DevCase fc = c_;
+    fc.force = 1;  // run even after convergence
+    size_t off = 0;
+    for (int d = 0; d < dirs; d++) {
+        const size_t nf = static_cast<size_t>(mesh_.faceCount(d));
+        for (int v = 0; v < 5; v++) fc.f[d].c[v] = scratch + off + v * nf;
+        off += 5 * nf;
+    }
+    const P5 U{{c_.U[0], c_.U[1], c_.U[2], c_.U[3], c_.U[4]}};
+    const P5 A{{c_.S1[0], c_.S1[1], c_.S1[2], c_.S1[3], c_.S1[4]}};
+    const P5 B{{c_.S2[0], c_.S2[1], c_.S2[2], c_.S2[3], c_.S2[4]}};
+    if (needTurbo_) check(launchBoundaryIntegrals(fc, U, true, stream_), "launch k_bint");
+    check(launchTimeStep(fc, U, stream_), "launch k_dt");
+    check(launchPre(fc, U, needTurbo_, profiles_, true, stream_), "launch k_pre");
+    check(launchStage(fc, U, A, 0.0, false, 1, B, stream_), "launch stage");
+    const Control c1 = control();
+    const long N = mesh_.nodes();
+    if (c_.dt_method == 0) {
+        check(cudaMemcpy(dt, c_.dt, N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    } else {
+        std::fill(dt, dt + N, c_.dt_method == 2 ? c_.fixed_dt : c1.dt_min);
+    }
+    for (int v = 0; v < 5; v++)
+        check(cudaMemcpy(r[v], c_.S2[v], N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+}
+
 // Copies run on the solver's stream (asynchronous when the host buffers are
 // pinned) and are complete when the call returns.
 void Solver::getState(double* const out[5]) {

@@ -52,6 +52,9 @@ public:
     long long step(long long n);
     long long solve();
     void computeResidual(double* dt, double* const r[5]);
+    // Same outputs as computeResidual, with the face-flux scratch in the
+    // library's static device array instead of the solver's face buffers.
+    void computeResidualNoAlloc(double* dt, double* const r[5]);
 
     void getState(double* const out[5]);
     void setState(const double* const in[5]);

@@ -68,6 +68,7 @@ SIGNATURES = {
     "ctbfm_enqueue": ([_VP, _I64], ctypes.c_int),
     "ctbfm_solve": ([_VP, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_compute_residual": ([_VP] + [_DP] * 6, ctypes.c_int),
+    "ctbfm_compute_residual_noalloc": ([_VP] + [_DP] * 6, ctypes.c_int),
     "ctbfm_get_state": ([_VP] + [_DP] * 5, ctypes.c_int),
     "ctbfm_set_state": ([_VP] + [_DP] * 5, ctypes.c_int),
     "ctbfm_get_lognorm": ([_VP, _DP], ctypes.c_int),
@@ -161,6 +162,14 @@ class Solver:
         dt = np.zeros(self.n)
         r = np.zeros((5, self.n))
         _check(load_library().ctbfm_compute_residual(self._h, _ptr(dt), *[_ptr(r[v]) for v in range(5)]))
+        return dt, r
+
+    def residual_noalloc(self):
+        """ctbfm_compute_residual_noalloc: the residual evaluation without any
+        device allocation (face-flux scratch in the library's static array)."""
+        dt = np.zeros(self.n)
+        r = np.zeros((5, self.n))
+        _check(load_library().ctbfm_compute_residual_noalloc(self._h, _ptr(dt), *[_ptr(r[v]) for v in range(5)]))
         return dt, r
 
     def state(self, out: Optional[np.ndarray] = None) -> np.ndarray:

@@ -104,6 +104,21 @@ int ctbfm_solve(ctbfm_solver* s, int64_t* n_done);
 int ctbfm_compute_residual(ctbfm_solver* s, double* dt, double* r_rho, double* r_rhou,
                            double* r_rhov, double* r_rhow, double* r_rhoe);
 
+/* Same outputs as ctbfm_compute_residual, for callers that cannot call
+ * cudaMalloc when they need a residual: processes whose device memory is
+ * owned by another allocator (a framework's caching allocator, or a pool
+ * reserved at start-up) and control loops that must not block in the
+ * driver's allocator mid-step. It allocates no device memory: the per-face
+ * flux contributions go to a static __device__ array of 16 MiB (5 doubles for
+ * at most 419430 faces summed over the swept directions; larger cases return
+ * CTBFM_E_CONFIG with the sizes in the message). Every GPU that loads the
+ * library holds that array until exit; all calls on a device share it, so
+ * calls that overlap on the GPU race. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture. No counterpart in the reference. */
+int ctbfm_compute_residual_noalloc(ctbfm_solver* s, double* dt, double* r_rho, double* r_rhou,
+                                   double* r_rhov, double* r_rhow, double* r_rhoe);
+
 /* Conservative state U^n (host buffers of NI*NJ*NK doubles each). */
 int ctbfm_get_state(ctbfm_solver* s, double* rho, double* rhou, double* rhov, double* rhow,
                     double* rhoe);

@@ -1,0 +1,48 @@
+"""ctbfm_compute_residual_noalloc against ctbfm_compute_residual.
+
+The no-allocation entry point serves callers that cannot call cudaMalloc when
+they need a residual (device memory owned by another allocator, or loops that
+must not block in the allocator); its face-flux scratch is a static device
+array. This file is collected last so that a run stopping at the first
+failure has already run every other test; it also passes on its own.
+"""
+
+import numpy as np
+import pytest
+
+from cturbobfm_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12  # the tolerance of the other GPU parity tests
+
+
+def rel_err(a, b):
+    a, b = np.atleast_2d(a), np.atleast_2d(b)
+    scale = np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return (np.abs(a - b).max(axis=1) / scale).max()
+
+
+@pytest.mark.parametrize("make", [lambda: cases.bump2d(ni=48, nj=24),
+                                  lambda: cases.annulus3d(ni=20, nj=8, nk=9)], ids=["bump2d", "annulus3d"])
+def test_noalloc_residual_matches_allocating_entry_point(make, tmp_path):
+    from cturbobfm_b200 import Solver
+
+    ini = make().write(str(tmp_path))
+    with Solver(ini) as s:
+        s.step(3)
+        dt_ref, r_ref = s.residual()
+        for _ in range(2):  # two calls in a row share the static scratch
+            dt, r = s.residual_noalloc()
+            assert rel_err(dt, dt_ref) <= REL_TOL
+            assert rel_err(r, r_ref) <= REL_TOL
+
+
+def test_noalloc_rejects_cases_beyond_the_scratch(tmp_path):
+    from cturbobfm_b200 import Solver
+    from cturbobfm_b200.solver import CtbfmError
+
+    ini = cases.annulus3d(ni=100, nj=40, nk=40).write(str(tmp_path))  # about 0.49 M faces > 419430
+    with Solver(ini) as s:
+        with pytest.raises(CtbfmError, match="static array holds"):
+            s.residual_noalloc()
