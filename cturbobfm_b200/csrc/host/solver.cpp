@@ -74,16 +74,63 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
         throw ConfigError("Rotational speed scaling factor is only active for fixed time step method");
     coeffs_ = config.getTimeIntegrationCoeffs();
     maxIter_ = config.getMaxIterations();
+    // every setting and input file is validated before the first CUDA call,
+    // so that input errors are reported as such on any machine
+    setupModels();
+    readBoundaries();
+    buildBoundaryStructures();
+    validateSettings();
     check(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = ownStream_;
     check(cudaMallocHost(reinterpret_cast<void**>(&hostCtl_), sizeof(Control)), "cudaMallocHost");
     std::memset(hostCtl_, 0, sizeof(Control));
-    setupModels();
-    readBoundaries();
-    buildBoundaryStructures();
+    uploadBoundaryStructures();
     upload();
     initializeSolution();
     initializeProfilesAndPlenum();
+}
+
+// Parses every key the device set-up reads (the reference's getters throw on
+// the same inputs).
+void Solver::validateSettings() {
+    const TimeStepMethod m = config_.getTimeStepMethod();
+    config_.getCFL();
+    if (m == TimeStepMethod::Fixed) config_.getFixedTimeStep();
+    config_.getFluidGamma();
+    config_.getFluidGasConstant();
+    config_.getInitMachNumber();
+    config_.getInitTemperature();
+    config_.getInitPressure();
+    const std::string raw = config_.has("INIT_DIRECTION") ? config_.get("INIT_DIRECTION") : "";
+    if (raw != "adaptive") {
+        const auto items = config_.parseList("INIT_DIRECTION");
+        if (items.size() != 3) throw ConfigError("INIT_DIRECTION must have 3 components or be 'adaptive'");
+        for (const auto& it : items) {
+            try {
+                (void)std::stod(it);
+            } catch (const std::exception&) {
+                throw ConfigError("Invalid vector element for key \"INIT_DIRECTION\": \"" + it + "\"");
+            }
+        }
+    }
+    config_.getResidualsDropConvergence();
+    config_.isSimulationSteady();
+    config_.isInletCylindrical();
+    config_.getOutletPressureRampMaxIterations();
+    config_.getRotationalSpeedScalingFactor();
+    if (config_.isAccelerationActive()) {
+        config_.parseFloat("ACCELERATION_INITIAL_TIME");
+        config_.parseFloat("ACCELERATION_FINAL_TIME");
+        config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_INITIAL");
+        config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_FINAL");
+    }
+    if (config_.isPerturbationBodyForceActive()) {
+        if (config_.parseList("PERTURBATION_CENTER").size() < 3) throw ConfigError("PERTURBATION_CENTER needs 3 values");
+        config_.parseFloat("PERTURBATION_RADIAL_EXTENSION");
+        config_.parseFloat("PERTURBATION_SCALING_FACTOR");
+        config_.parseFloat("PERTURBATION_TIME_START");
+        config_.parseFloat("PERTURBATION_TIME_DURATION");
+    }
 }
 
 Solver::~Solver() {
@@ -254,21 +301,11 @@ void Solver::buildBoundaryStructures() {
     // the K map is never read outside 3-D; keep it valid for the kernels
     for (auto& v : mapK)
         if (v < 0) v = 0;
-    auto up8 = [&](const std::vector<signed char>& v) {
-        void* d = nullptr;
-        check(cudaMalloc(&d, v.size()), "cudaMalloc");
-        allocations_.push_back(d);
-        check(cudaMemcpy(d, v.data(), v.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
-        return static_cast<const signed char*>(d);
-    };
-    c_.mapI = up8(mapI);
-    c_.mapJ = up8(mapJ);
-    c_.mapK = up8(mapK);
-    if (nprof) {
-        c_.prof_p = alloc(profP.size());
-        check(cudaMemcpy(c_.prof_p, profP.data(), profP.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
-        c_.prof_r = upload(profR);
-    }
+    mapI_ = std::move(mapI);
+    mapJ_ = std::move(mapJ);
+    mapK_ = std::move(mapK);
+    profP_ = std::move(profP);
+    profR_ = std::move(profR);
 
     // turbo performance, throttle and plenum (src/solver.cpp:1309-1321, 735-748)
     needTurbo_ = config_.saveTurboOutput();
@@ -303,6 +340,24 @@ void Solver::buildBoundaryStructures() {
                 if (b.orientation == 3) { dir = "-j"; break; }
             }
     c_.turbo_dir = dir == "-i" ? 1 : ((dir == "j" || dir == "+j") ? 2 : (dir == "-j" ? 3 : 0));
+}
+
+void Solver::uploadBoundaryStructures() {
+    auto up8 = [&](const std::vector<signed char>& v) {
+        void* d = nullptr;
+        check(cudaMalloc(&d, v.size()), "cudaMalloc");
+        allocations_.push_back(d);
+        check(cudaMemcpy(d, v.data(), v.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+        return static_cast<const signed char*>(d);
+    };
+    c_.mapI = up8(mapI_);
+    c_.mapJ = up8(mapJ_);
+    c_.mapK = up8(mapK_);
+    if (c_.nprofiles) {
+        c_.prof_p = alloc(profP_.size());
+        check(cudaMemcpy(c_.prof_p, profP_.data(), profP_.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+        c_.prof_r = upload(profR_);
+    }
 }
 
 void Solver::upload() {

@@ -74,6 +74,8 @@ public:
 private:
     void readBoundaries();
     void buildBoundaryStructures();
+    void uploadBoundaryStructures();
+    void validateSettings();
     void setupModels();
     void upload();
     void initializeSolution();
@@ -97,6 +99,8 @@ private:
     double periodicAngleDeg_ = 0.0, periodicAngleRad_ = 0.0, periodicTransl_ = 0.0;
 
     DevCase c_{};
+    std::vector<signed char> mapI_, mapJ_, mapK_;
+    std::vector<double> profP_, profR_;
     std::vector<void*> allocations_;
     Control* hostCtl_ = nullptr;  // pinned
     cudaStream_t ownStream_ = nullptr, stream_ = nullptr;
