@@ -192,7 +192,9 @@ def algorithmic_bytes(case, kernel: str) -> float:
     faces = {"I": (ni + 1) * nj * nk, "J": ni * (nj + 1) * nk, "K": ni * nj * (nk + 1)}
     if kernel.startswith("k_faces_"):
         f = faces[kernel[-1]]
-        return 8.0 * (5 * n + 4 * f + 5 * f)  # state once, normal + area, flux * |S|
+        return 8.0 * (5 * n + 4 * f + 5 * f)  # primitives once, normal + area, flux * |S|
+    if kernel == "k_prim":
+        return 8.0 * (5 * n + 5 * n)
     if kernel == "k_nodes":
         # face contributions of 3 directions, stage input, U^n, output, dt, volume,
         # rotation (cos, sin, r) and the BFM fields of the node (14)
@@ -204,8 +206,8 @@ def algorithmic_bytes(case, kernel: str) -> float:
 
 def launches_per_iteration(case, kernel: str) -> int:
     s = case.n_stages
-    return {"k_faces_I": s, "k_faces_J": s, "k_faces_K": s, "k_nodes": s, "k_periodic": s, "k_dt": 1, "k_pre": 1,
-            "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
+    return {"k_faces_I": s, "k_faces_J": s, "k_faces_K": s, "k_nodes": s, "k_periodic": s, "k_prim": s, "k_dt": 1,
+            "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
 
 
 def measured_peaks():

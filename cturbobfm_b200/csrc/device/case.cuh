@@ -129,6 +129,7 @@ struct DevCase {
     double* S1[5];  // stage buffers
     double* S2[5];
     double* Rp[5];  // periodic-plane residuals (2 * ni * nj)
+    double* W[5];   // primitives of the current stage input (k_prim)
     double* dt;
     double* partial;  // reduction partials
     int node_blocks;  // grid of the node kernel (fixed for deterministic sums)

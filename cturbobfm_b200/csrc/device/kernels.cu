@@ -135,44 +135,62 @@ __global__ void __launch_bounds__(256) k_faces(DevCase c, P5 Uin) {
         } else {
             const long long qR = nodeIdx(c, fi, fj, fk);
             const long long qL = qR - st;
-            const S5 Ul = load5(U, qL), Ur = load5(U, qR);
-            S5 Ull, Urr;
-            if (DIR == 2 && c.periodic) {
-                if (dface == 1) {
-                    Ull = rotState(load5(U, nodeIdx(c, fi, fj, c.nk - 2)), c.per_cos_m, c.per_sin_m);
-                    Urr = load5(U, qR + 1);
-                } else if (dface == nlast - 1) {
-                    Ull = load5(U, qR - 2);
-                    Urr = rotState(load5(U, nodeIdx(c, fi, fj, 1)), c.per_cos_p, c.per_sin_p);
+            // faces whose four stencil nodes are plain interior nodes read the
+            // primitives k_prim computed once per node (bitwise the same values
+            // as converting here); faces next to a boundary or a periodic seam
+            // extrapolate or rotate conservative states first
+            const bool plain = dface >= 2 && dface <= nlast - 2;
+            if (plain) {
+                if (SCHEME == 0) {
+                    flux = fluxJstW(gs, load5(U, qL - st), load5(U, qL), load5(U, qR), load5(U, qR + st),
+                                    load5(c.W, qL - st), load5(c.W, qL), load5(c.W, qR), load5(c.W, qR + st), n);
                 } else {
-                    Ull = load5(U, qL - st);
-                    Urr = load5(U, qR + st);
+                    flux = fluxRoeW(gs, c.muscl, c.limiter, c.muscl ? load5(c.W, qL - st) : zero5(), load5(c.W, qL),
+                                    load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5(), n);
                 }
             } else {
-                if (dface == 1) {
-                    Ull = Ul - (Ur - Ul);
-                    Urr = load5(U, qR + st);
-                } else if (dface == nlast - 1) {
-                    Ull = load5(U, qL - st);
-                    Urr = Ur + (Ur - Ul);
+                const S5 Ul = load5(U, qL), Ur = load5(U, qR);
+                S5 Ull, Urr;
+                if (DIR == 2 && c.periodic) {
+                    if (dface == 1) {
+                        Ull = rotState(load5(U, nodeIdx(c, fi, fj, c.nk - 2)), c.per_cos_m, c.per_sin_m);
+                        Urr = load5(U, qR + 1);
+                    } else {  // dface == nlast - 1
+                        Ull = load5(U, qR - 2);
+                        Urr = rotState(load5(U, nodeIdx(c, fi, fj, 1)), c.per_cos_p, c.per_sin_p);
+                    }
                 } else {
-                    Ull = load5(U, qL - st);
-                    Urr = load5(U, qR + st);
+                    if (dface == 1) {
+                        Ull = Ul - (Ur - Ul);
+                        Urr = load5(U, qR + st);
+                    } else {  // dface == nlast - 1
+                        Ull = load5(U, qL - st);
+                        Urr = Ur + (Ur - Ul);
+                    }
                 }
+                if (SCHEME == 0) flux = fluxJst(gs, Ull, Ul, Ur, Urr, n);
+                else flux = fluxRoe(gs, c.muscl, c.limiter, Ull, Ul, Ur, Urr, n);
             }
-            if (SCHEME == 0) flux = fluxJst(gs, Ull, Ul, Ur, Urr, n);
-            else flux = fluxRoe(gs, c.muscl, c.limiter, Ull, Ul, Ur, Urr, n);
         }
 #pragma unroll
         for (int v = 0; v < 5; v++) F.c[v][f] = flux.v[v] * area;
     }
 }
 
+// Primitives of the stage input (getPrimitiveVariablesFromConservative,
+// src/math_utils.cpp:49-57), once per node for the face kernels.
+__global__ void __launch_bounds__(256) k_prim(DevCase c, P5 Uin) {
+    if (halted(c)) return;
+    for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < c.n;
+         q += static_cast<long long>(gridDim.x) * blockDim.x)
+        store5(c.W, q, primOf(load5(Uin.p, q)));
+}
+
 // ------------------------------------------------------------------ nodes
 // Residual assembly in the reference's accumulation order (I faces, J faces,
 // K faces, then sources), then Solver::updateSolution (src/solver.cpp:2230-2249).
 // mode 0: U_out = U^n - R * (alpha*dt/V); mode 1: write R to Rout.
-__global__ void __launch_bounds__(256) k_nodes(DevCase c, P5 Uin, P5 Uout, double alpha, int last, int mode, P5 Rout) {
+__global__ void __launch_bounds__(256, 2) k_nodes(DevCase c, P5 Uin, P5 Uout, double alpha, int last, int mode, P5 Rout) {
     if (halted(c)) return;
     const Gas gs{c.gamma, c.rgas};
     const double t = c.ctl->t;
@@ -593,8 +611,14 @@ cudaError_t launchPeriodic(const DevCase& c, P5 Uout, double alpha, bool last, i
     return cudaGetLastError();
 }
 
+cudaError_t launchPrim(const DevCase& c, P5 Uin, cudaStream_t s) {
+    k_prim<<<c.node_blocks, 256, 0, s>>>(c, Uin);
+    return cudaGetLastError();
+}
+
 cudaError_t launchStage(const DevCase& c, P5 Uin, P5 Uout, double alpha, bool last, int mode, P5 Rout, cudaStream_t s) {
     const int dirs = c.topo == 1 ? 3 : 2;
+    k_prim<<<c.node_blocks, 256, 0, s>>>(c, Uin);
     for (int d = 0; d < dirs; d++) {
         const cudaError_t e = launchFaces(c, d, Uin, s);
         if (e != cudaSuccess) return e;

@@ -24,11 +24,12 @@ cudaError_t launchStage(const DevCase& c, P5 Uin, P5 Uout, double alpha, bool la
                         cudaStream_t s);
 cudaError_t launchFinalize(const DevCase& c, cudaStream_t s);
 // single kernels of a stage (profiling)
+cudaError_t launchPrim(const DevCase& c, P5 Uin, cudaStream_t s);
 cudaError_t launchFaces(const DevCase& c, int dir, P5 Uin, cudaStream_t s);
 cudaError_t launchNodes(const DevCase& c, P5 Uin, P5 Uout, double alpha, bool last, int mode, P5 Rout, cudaStream_t s);
 cudaError_t launchPeriodic(const DevCase& c, P5 Uout, double alpha, bool last, int mode, P5 Rout, cudaStream_t s);
 
-constexpr int kKernelKinds = 9;
+constexpr int kKernelKinds = 10;
 
 // Static device scratch of ctbfm_compute_residual_noalloc (noalloc.cu): its
 // device address on the current device (looked up once per device) and size.

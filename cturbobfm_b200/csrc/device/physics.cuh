@@ -151,8 +151,8 @@ CTBFM_DI double jstR(Gas gs, const S5& W) {
 CTBFM_DI double pressurePrim(Gas gs, const S5& W) { return pressure_rho_u_et(gs, W.v[0], velOf(W), W.v[4]); }
 CTBFM_DI double jstS(double p1, double p2, double p3) { return fabs((p1 - 2 * p2 + p3) / (p1 + 2 * p2 + p3)); }
 
-CTBFM_DI S5 fluxJst(Gas gs, const S5& Ull, const S5& Ul, const S5& Ur, const S5& Urr, D3 n) {
-    const S5 Wll = primOf(Ull), Wl = primOf(Ul), Wr = primOf(Ur), Wrr = primOf(Urr);
+CTBFM_DI S5 fluxJstW(Gas gs, const S5& Ull, const S5& Ul, const S5& Ur, const S5& Urr, const S5& Wll,
+                     const S5& Wl, const S5& Wr, const S5& Wrr, D3 n) {
     const S5 Wavg = (Wl + Wr) * 0.5;
     const double rL = jstR(gs, Wl), rR = jstR(gs, Wr);
     const double pll = pressurePrim(gs, Wll), pl = pressurePrim(gs, Wl), pr = pressurePrim(gs, Wr),
@@ -165,6 +165,10 @@ CTBFM_DI S5 fluxJst(Gas gs, const S5& Ull, const S5& Ul, const S5& Ur, const S5&
     const S5 F = advFlux(gs, Wavg, n);
     const S5 d = (Ur - Ul) * psi2 - (((Urr - Ur) - (Ur - Ul) * 2) + (Ul - Ull)) * psi4;
     return F - d;
+}
+
+CTBFM_DI S5 fluxJst(Gas gs, const S5& Ull, const S5& Ul, const S5& Ur, const S5& Urr, D3 n) {
+    return fluxJstW(gs, Ull, Ul, Ur, Urr, primOf(Ull), primOf(Ul), primOf(Ur), primOf(Urr), n);
 }
 
 // ------------------------------------------------------ Roe + MUSCL flux
@@ -189,10 +193,8 @@ CTBFM_DI double roeAvg(double sl, double sr, double pl, double pr) {  // roeAver
 
 // AdvectionRoe::computeFlux (src/advection_roe.cpp:6-220), entropy fix 0.01
 // (include/advection_roe.hpp:63).
-CTBFM_DI S5 fluxRoe(Gas gs, int muscl, int lim, const S5& Ull, const S5& Ul, const S5& Ur, const S5& Urr, D3 n1) {
-    S5 Wl = primOf(Ul), Wr = primOf(Ur);
+CTBFM_DI S5 fluxRoeW(Gas gs, int muscl, int lim, const S5& Wll, S5 Wl, S5 Wr, const S5& Wrr, D3 n1) {
     if (muscl) {
-        const S5 Wrr = primOf(Urr), Wll = primOf(Ull);
         S5 limL, limR;
 #pragma unroll
         for (int i = 0; i < 5; i++) {
@@ -291,6 +293,11 @@ CTBFM_DI S5 fluxRoe(Gas gs, int muscl, int lim, const S5& Ull, const S5& Ul, con
               Fr.v[1] * (dot(n1, ey)) + Fr.v[2] * (dot(n2, ey)) + Fr.v[3] * (dot(n3, ey)),
               Fr.v[1] * (dot(n1, ez)) + Fr.v[2] * (dot(n2, ez)) + Fr.v[3] * (dot(n3, ez)),
               Fr.v[4]);
+}
+
+CTBFM_DI S5 fluxRoe(Gas gs, int muscl, int lim, const S5& Ull, const S5& Ul, const S5& Ur, const S5& Urr, D3 n1) {
+    return fluxRoeW(gs, muscl, lim, muscl ? primOf(Ull) : zero5(), primOf(Ul), primOf(Ur),
+                    muscl ? primOf(Urr) : zero5(), n1);
 }
 
 // ----------------------------------------------------------- boundaries

@@ -542,6 +542,7 @@ void Solver::upload() {
         c_.S1[v] = alloc(N);
         c_.S2[v] = alloc(N);
         c_.Rp[v] = alloc(2 * NI * NJ);
+        c_.W[v] = alloc(N);
     }
     c_.dt = alloc(N);
     c_.node_blocks = nodeBlocks(N);
@@ -860,6 +861,7 @@ void Solver::profileKernels(int reps, double* outMs) {
     timeIt(6, [&] { check(launchNodes(fc, U, A, coeffs_.back(), true, 0, B, stream_), "k_nodes"); });
     if (c_.periodic) timeIt(7, [&] { check(launchPeriodic(fc, A, coeffs_.back(), true, 0, B, stream_), "k_periodic"); });
     timeIt(8, [&] { check(launchFinalize(fc, stream_), "k_finalize"); });
+    timeIt(9, [&] { check(launchPrim(fc, U, stream_), "k_prim"); });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     check(cudaMemcpy(c_.dt, dtSaved.data(), N * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");

@@ -202,7 +202,7 @@ class Solver:
         return mf, tp
 
     KERNELS = ("k_bint", "k_dt", "k_pre", "k_faces_I", "k_faces_J", "k_faces_K", "k_nodes", "k_periodic",
-               "k_finalize")
+               "k_finalize", "k_prim")
 
     def profile_kernels(self, reps: int = 20) -> Dict[str, float]:
         """Average device time per launch (ms) of each kernel kind, CUDA events."""

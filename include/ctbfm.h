@@ -151,7 +151,8 @@ enum {
     CTBFM_K_NODES = 6,              /* k_nodes */
     CTBFM_K_PERIODIC = 7,           /* k_periodic (periodic cases) */
     CTBFM_K_FINALIZE = 8,           /* k_finalize */
-    CTBFM_K_COUNT = 9
+    CTBFM_K_PRIMITIVES = 9,         /* k_prim */
+    CTBFM_K_COUNT = 10
 };
 
 /* Measurement hook (no counterpart in the reference): launches each kernel
