@@ -2,8 +2,11 @@
 C++ layer (g++), linked with the static CUDA runtime.
 
 Flags that carry the numerical contract:
-  * kernels: ``--fmad=false`` (no multiply-add contraction; IEEE double
-    division and square root are nvcc's defaults);
+  * double kernels (kernels.cu, noalloc.cu): ``--fmad=false`` (no
+    multiply-add contraction; IEEE double division and square root are
+    nvcc's defaults);
+  * float kernels (kernels_f32.cu): contraction allowed; the compensated
+    (Kahan) state update has no product to contract;
   * host code: ``-ffp-contract=off`` (mesh metrics bit-identical to the
     reference's).
 """
@@ -26,8 +29,9 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["device/kernels.cu", "device/noalloc.cu"]
-CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/solver.cpp", "capi.cpp"]
+# (source, contract multiply-adds)
+CU_SOURCES = [("device/kernels.cu", False), ("device/kernels_f32.cu", True), ("device/noalloc.cu", False)]
+CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/engine.cpp", "host/solver.cpp", "capi.cpp"]
 
 
 def _run(cmd: List[str]) -> None:
@@ -59,12 +63,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = _all_headers()
     objs = []
-    for src in CU_SOURCES:
+    for src, fmad in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, os.path.basename(src) + ".o")
         if force or _stale(o, [s] + headers):
-            _run([NVCC, *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-                  "-Xptxas", "-v" if verbose else "-O3", "-c", s, "-o", o])
+            _run([NVCC, *ARCH, "-lineinfo", "-O3", "--fmad=" + ("true" if fmad else "false"), "-std=c++17",
+                  "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3", "-c", s, "-o", o])
         objs.append(o)
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)

@@ -109,7 +109,7 @@ int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out) {
         out->iteration = c.it;
         out->max_iterations = s->solver->maxIterations();
         out->status = c.status;
-        out->precision = 0;
+        out->precision = s->solver->precision();
         out->time = c.t;
         return CTBFM_OK;
     });

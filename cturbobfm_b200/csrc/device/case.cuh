@@ -1,7 +1,10 @@
-// Device-side description of one solver instance: metric arrays, boundary
-// tables, BFM fields, state buffers and the device-resident control block that
-// carries the iteration counter, physical time, residual norms, turbo
-// performance and plenum state from kernel to kernel without host round trips.
+// Device-side description of one operating point (instance): metric arrays,
+// boundary tables, BFM fields, state buffers and the device-resident control
+// block that carries the iteration counter, physical time, residual norms,
+// turbo performance and plenum state from kernel to kernel without host round
+// trips. R is the working precision of the state and the metric arrays
+// (double for the plain path, float for the compensated path); reductions,
+// integrals, profiles and the control block are always double.
 #pragma once
 
 #include <cstdint>
@@ -32,12 +35,13 @@ struct DevPatch {
 // One face direction: unit normal n = S/|S| and area |S| per face of the face
 // grid (I: (ni+1, nj, nk), J: (ni, nj+1, nk), K: (ni, nj, nk+1)), plus the
 // per-face residual contribution flux * |S| written by the face kernel.
-struct DevFaces {
-    const double* nx;
-    const double* ny;
-    const double* nz;
-    const double* area;
-    double* c[5];
+template <typename R>
+struct DevFacesT {
+    const R* nx;
+    const R* ny;
+    const R* nz;
+    const R* area;
+    R* c[5];
 };
 
 // Iteration state living on the device.
@@ -60,7 +64,18 @@ struct Control {
     double gz_p, gz_min, gz_mout, gz_T, gz_t;  // Greitzer plenum
 };
 
-struct DevCase {
+// A block's share of a batched launch: `count` consecutive elements (nodes,
+// faces, periodic pairs, planes or instances) of instance `inst`, starting at
+// `start`; `local` numbers the tiles of that instance (reduction partials).
+struct Tile {
+    int inst;
+    int local;
+    long long start;
+    long long count;
+};
+
+template <typename R>
+struct alignas(16) DevCaseT {
     int ni, nj, nk;
     long long n;
     int topo;  // 0 2D, 1 3D, 2 axisymmetric
@@ -68,7 +83,8 @@ struct DevCase {
     int periodic, bfm, blockage, bfm_model, stalled, perturb, accel, offdesign;
     int need_turbo, greitzer, inlet_cyl, turbo_dir, nprofiles, npatches;
     int le_idx, te_idx;
-    int force;  // run even when the control block says the run has stopped
+    int compensated;  // the state carries a Kahan compensation term (float path)
+    int force;        // run even when the control block says the run has stopped
     double gamma, rgas, cp, cfl, fixed_dt;
     double coeffs[4];
     double per_cos_p, per_sin_p, per_cos_m, per_sin_m;  // cos/sin of +angle and -angle
@@ -78,66 +94,70 @@ struct DevCase {
     double plenum_volume, ambient_p, throttle_kt, inlet_pt;
     double pert_c[3], pert_r, pert_s, pert_t0, pert_dur;
 
-    DevFaces f[3];
+    DevFacesT<R> f[3];
     // per node
-    const double* vol;
-    const double* cost;  // cos(theta), theta = atan2(z, y) (host glibc)
-    const double* sint;
-    const double* radius;
-    const double* areaK0;  // |S_K(i, j, 0)| (axisymmetric source)
-    const double* edge[12];  // dI.xyz, dsI, dJ.xyz, dsJ, dK.xyz, dsK (time step)
+    const R* vol;
+    const R* cost;  // cos(theta), theta = atan2(z, y) (host glibc)
+    const R* sint;
+    const R* radius;
+    const R* areaK0;    // |S_K(i, j, 0)| (axisymmetric source)
+    const R* edge[12];  // dI.xyz, dsI, dJ.xyz, dsJ, dK.xyz, dsK (time step)
     const double* vx;
     const double* vy;
     const double* vz;
+    const double* cost64;  // double copies for the FP64 boundary integrals and profiles
+    const double* sint64;
     // boundary tables: patch index per boundary face
     const signed char* mapI;  // (2, nj, nk)
     const signed char* mapJ;  // (ni, 2, nk)
     const signed char* mapK;  // (ni, nj, 2)
     DevPatch patch[kMaxPatches];
     // radial profiles
-    double* prof_p;          // concatenated pressure profiles
-    const double* prof_r;    // concatenated radii
+    double* prof_p;        // concatenated pressure profiles
+    const double* prof_r;  // concatenated radii
     int prof_off[kMaxProfiles];
     int prof_n[kMaxProfiles];
     int prof_type[kMaxProfiles];
-    int prof_i[kMaxProfiles];     // node i of the sampled column
-    int prof_j0[kMaxProfiles];    // first j
-    double prof_kt[kMaxProfiles]; // throttle coefficient of the profile's patch
+    int prof_i[kMaxProfiles];      // node i of the sampled column
+    int prof_j0[kMaxProfiles];     // first j
+    double prof_kt[kMaxProfiles];  // throttle coefficient of the profile's patch
     // boundary planes for the surface integrals: raw S vectors
     const double* bsx[6];
     const double* bsy[6];
     const double* bsz[6];
     // BFM fields (nullptr when absent)
-    const double* blk;
-    const double* gbx;
-    const double* gby;
-    const double* gbz;
-    const double* nax;
-    const double* nrad;
-    const double* ntan;
-    const double* rpm;
-    const double* stwl;
-    const double* bpresent;
-    const double* nblades;
-    const double* cosmetal;
-    const double* devpivot;
-    const double* devstall;
-    const double* ldbeta0;
-    const double* ldkp;
+    const R* blk;
+    const R* gbx;
+    const R* gby;
+    const R* gbz;
+    const R* nax;
+    const R* nrad;
+    const R* ntan;
+    const R* rpm;
+    const R* stwl;
+    const R* bpresent;
+    const R* nblades;
+    const R* cosmetal;
+    const R* devpivot;
+    const R* devstall;
+    const R* ldbeta0;
+    const R* ldkp;
     // state
-    double* U[5];   // U^n
-    double* S1[5];  // stage buffers
-    double* S2[5];
-    double* Rp[5];  // periodic-plane residuals (2 * ni * nj)
-    double* W[5];   // primitives of the current stage input (k_prim)
-    double* dt;
-    double* partial;  // reduction partials
-    int node_blocks;  // grid of the node kernel (fixed for deterministic sums)
-    int per_blocks;
-    int dt_blocks;
+    R* U[5];   // U^n
+    R* Uc[5];  // Kahan compensation of U^n (compensated path; true state = U - Uc)
+    R* S1[5];  // stage buffers
+    R* S2[5];
+    R* Rp[5];  // periodic-plane residuals (2 * ni * nj)
+    R* W[5];   // primitives of the current stage input (k_prim)
+    R* dt;
+    double* partial;  // [node_tiles*5 | per_tiles*5 | node_tiles dt minima]
+    int node_tiles;   // tiles of this instance in the node kernels
+    int per_tiles;    // tiles of this instance in the periodic kernel
     Control* ctl;
     double* hist;  // 16 doubles per iteration row
     long long hist_cap;
 };
+
+using DevCase = DevCaseT<double>;
 
 }  // namespace ctbfm

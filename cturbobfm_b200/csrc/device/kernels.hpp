@@ -1,35 +1,58 @@
-// Host-side launchers of the FP64 loop kernels (kernels.cu).
+// Host-side launchers of the loop kernels (kernels_impl.cuh), instantiated for
+// double (kernels.cu, --fmad=false) and float (kernels_f32.cu).
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <cstddef>
 
 #include "case.cuh"
 
 namespace ctbfm {
 
-// Five state / residual arrays passed by value to a kernel.
-struct P5 {
-    double* p[5];
+// Device array of tiles for one kernel family.
+struct TileList {
+    const Tile* tiles = nullptr;
+    int n = 0;
 };
 
-int nodeBlocks(long long n);
-int periodicBlocks(long long np);
+// Everything a batched launch needs: the instances' descriptions on the
+// device and the tile lists of each kernel family.
+template <typename R>
+struct BatchView {
+    const DevCaseT<R>* cases = nullptr;  // m device-resident instance descriptions
+    int m = 0;
+    TileList node;        // nodes of every instance (k_prim, k_nodes, k_dt)
+    TileList face[3][2];  // faces per direction and scheme (0 JST, 1 Roe)
+    TileList per;         // periodic (i, j) pairs of periodic instances
+    TileList inst;        // one tile per instance (k_pre, k_finalize)
+    TileList bint;        // 8 plane tiles per instance that needs turbo performance
+    TileList bintAll;     // 8 plane tiles for every instance
+};
 
-cudaError_t launchBoundaryIntegrals(const DevCase& c, P5 Uin, bool turbo, cudaStream_t s);
-cudaError_t launchTimeStep(const DevCase& c, P5 Uin, cudaStream_t s);
-cudaError_t launchPre(const DevCase& c, P5 Uin, bool turbo, bool profiles, bool dtpart, cudaStream_t s);
-cudaError_t launchSetLimits(const DevCase& c, long long itStop, long long histBase, cudaStream_t s);
-// mode 0: Runge-Kutta stage update into Uout; mode 1: residual into Rout.
-cudaError_t launchStage(const DevCase& c, P5 Uin, P5 Uout, double alpha, bool last, int mode, P5 Rout,
-                        cudaStream_t s);
-cudaError_t launchFinalize(const DevCase& c, cudaStream_t s);
-// single kernels of a stage (profiling)
-cudaError_t launchPrim(const DevCase& c, P5 Uin, cudaStream_t s);
-cudaError_t launchFaces(const DevCase& c, int dir, P5 Uin, cudaStream_t s);
-cudaError_t launchNodes(const DevCase& c, P5 Uin, P5 Uout, double alpha, bool last, int mode, P5 Rout, cudaStream_t s);
-cudaError_t launchPeriodic(const DevCase& c, P5 Uout, double alpha, bool last, int mode, P5 Rout, cudaStream_t s);
+template <typename R>
+struct Launcher {
+    static cudaError_t setLimits(const BatchView<R>& b, long long n, cudaStream_t s);
+    static cudaError_t boundaryIntegrals(const BatchView<R>& b, bool all, int force, cudaStream_t s);
+    static cudaError_t timeStep(const BatchView<R>& b, int force, cudaStream_t s);
+    static cudaError_t pre(const BatchView<R>& b, bool forceTurbo, bool dtpart, bool profiles, int force,
+                           cudaStream_t s);
+    static cudaError_t prim(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    static cudaError_t faces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s);
+    static cudaError_t nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    static cudaError_t periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    static cudaError_t finalize(const BatchView<R>& b, int force, cudaStream_t s);
+    // k_prim, k_faces, k_nodes, k_periodic of one stage (stage -1: residual only)
+    static cudaError_t stage(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    // one whole iteration of every instance in the batch
+    static cudaError_t iteration(const BatchView<R>& b, int nstages, cudaStream_t s);
+};
+
+extern template struct Launcher<double>;
+extern template struct Launcher<float>;
 
 constexpr int kKernelKinds = 10;
+constexpr int kTileSize = 256;  // elements per tile (one per thread)
 
 // Static device scratch of ctbfm_compute_residual_noalloc (noalloc.cu): its
 // device address on the current device (looked up once per device) and size.

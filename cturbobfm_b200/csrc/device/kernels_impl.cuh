@@ -1,0 +1,768 @@
+// Kernels of the explicit residual-and-update loop (sm_100a), templated on the
+// working precision R and driven by tiles, so that one launch advances any set
+// of operating points (one, or a whole batch of uneven grids).
+//
+// A launch's grid has one block per Tile; a tile is a contiguous range of one
+// instance's elements (nodes, faces of one direction, periodic (i,j) pairs,
+// boundary planes or the instance itself). Each block first copies its
+// instance's DevCaseT into shared memory and returns at once when that
+// instance has converged, diverged or reached its iteration limit, so finished
+// instances cost nothing while the rest of the batch runs.
+//
+// One pseudo-time iteration, with no host synchronisation:
+//   k_set_limits (once per enqueue), k_bint (boundary integrals, when turbo
+//   performance is needed), k_dt, k_pre, then per Runge-Kutta stage k_prim,
+//   k_faces<I|J|K>, k_nodes, k_periodic, and finally k_finalize.
+//
+// The double instantiation (kernels.cu) is compiled with --fmad=false so that
+// each expression rounds as the reference's does; the float instantiation
+// (kernels_f32.cu) keeps a Kahan compensation term of the state.
+
+#include <cuda_runtime.h>
+
+#include "kernels.hpp"
+#include "sources.cuh"
+
+namespace ctbfm {
+
+namespace {
+
+// Copies the block's instance description into shared memory.
+template <typename R>
+__device__ __forceinline__ Tile stageCase(const DevCaseT<R>* cases, const Tile* tiles, DevCaseT<R>& sc) {
+    const Tile t = tiles[blockIdx.x];
+    const int4* src = reinterpret_cast<const int4*>(cases + t.inst);
+    int4* dst = reinterpret_cast<int4*>(&sc);
+    constexpr int n16 = static_cast<int>(sizeof(DevCaseT<R>) / 16);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+    __syncthreads();
+    return t;
+}
+
+template <typename R>
+__device__ __forceinline__ bool halted(const DevCaseT<R>& c, int force) {
+    return !force && (c.ctl->status != 0 || c.ctl->it >= c.ctl->it_stop);
+}
+
+// Stage buffers: RK4 U -> S1 -> S2 -> S1 -> U, RK3 U -> S1 -> S2 -> U (the
+// last stage updates U^n in place); stage -1 is a residual-only evaluation of
+// U^n into S2.
+template <typename R>
+__device__ __forceinline__ R* const* stageIn(const DevCaseT<R>& c, int s) {
+    if (s <= 0) return c.U;
+    if (s == 1) return c.S1;
+    if (s == 2) return c.S2;
+    return c.S1;
+}
+template <typename R>
+__device__ __forceinline__ R* const* stageOut(const DevCaseT<R>& c, int s) {
+    if (s < 0) return c.S2;
+    if (s == c.nstages - 1) return c.U;
+    if (s == 0) return c.S1;
+    if (s == 1) return c.S2;
+    return c.S1;
+}
+
+template <typename R>
+__device__ __forceinline__ S5<R> boundaryFlux(const DevCaseT<R>& c, Gas<R> gs, int pidx, const S5<R>& Uint, V3<R> n,
+                                              long long qtheta, int fj, long long it) {
+    const DevPatch& p = c.patch[pidx];
+    switch (p.type) {
+        case kBcInlet: return bcInlet(c, gs, p, Uint, n, c.cost[qtheta], c.sint[qtheta]);
+        case kBcOutlet: return bcOutlet(c, gs, Uint, n, R(p.v[0]), it);
+        case kBcRadialEq:
+        case kBcThrottle: {
+            // BoundaryOutletThrottle / RadialEquilibrium index the profile by the
+            // face's j (src/boundary_outlet_throttle.cpp:14).
+            const int m = p.profile;
+            const int jj = fj < c.prof_n[m] ? fj : c.prof_n[m] - 1;
+            return bcOutlet(c, gs, Uint, n, R(c.prof_p[c.prof_off[m] + jj]), it);
+        }
+        case kBcInviscidWall: return bcWall(gs, Uint, n);
+        default: return zero5<R>();  // periodic / wedge faces: BoundaryFake, zero flux
+    }
+}
+
+// Deterministic block sum of NV doubles per thread; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void blockSum(double (&v)[NV]) {
+    __shared__ double sh[NV][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < NV; c++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    if (lane == 0)
+#pragma unroll
+        for (int c = 0; c < NV; c++) sh[c][warp] = v[c];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int c = 0; c < NV; c++) {
+            v[c] = lane < nw ? sh[c][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double blockMin(double v) {
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? sh[lane] : INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    }
+    __syncthreads();
+    return v;
+}
+
+// The state in double, including the compensation term of the float path.
+template <typename R>
+__device__ __forceinline__ S5<double> state64(const DevCaseT<R>& c, R* const* U, long long q) {
+    S5<double> s;
+#pragma unroll
+    for (int v = 0; v < 5; v++) s.v[v] = static_cast<double>(U[v][q]);
+    if (c.compensated && U == c.U)
+#pragma unroll
+        for (int v = 0; v < 5; v++) s.v[v] -= static_cast<double>(c.Uc[v][q]);
+    return s;
+}
+
+// ------------------------------------------------------------------ faces
+// Solver::computeAdvectionFluxResidualsImpl (src/solver.cpp:1865-2040): one
+// thread per face of direction DIR; writes flux * |S|.
+template <int DIR, int SCHEME, typename R>
+__global__ void __launch_bounds__(256) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    const Tile tl = stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    const long long it = c.ctl->it + 1;
+    const Gas<R> gs{R(c.gamma), R(c.rgas)};
+    const int nfj = c.nj + (DIR == 1), nfk = c.nk + (DIR == 2);
+    const long long st = DIR == 0 ? static_cast<long long>(c.nj) * c.nk : (DIR == 1 ? c.nk : 1);
+    const int nlast = DIR == 0 ? c.ni : (DIR == 1 ? c.nj : c.nk);
+    const DevFacesT<R>& F = c.f[DIR];
+    R* const* U = stageIn(c, stage);
+    for (long long f = tl.start + threadIdx.x; f < tl.start + tl.count; f += blockDim.x) {
+        const int fk = static_cast<int>(f % nfk);
+        const long long t = f / nfk;
+        const int fj = static_cast<int>(t % nfj);
+        const int fi = static_cast<int>(t / nfj);
+        const int dface = DIR == 0 ? fi : (DIR == 1 ? fj : fk);
+        if (DIR == 2 && c.bfm && c.bpresent[nodeIdx(c, fi, fj, 0)] > R(0)) continue;  // blade rows: no K flux
+        V3<R> n = v3(__ldg(F.nx + f), __ldg(F.ny + f), __ldg(F.nz + f));
+        const R area = __ldg(F.area + f);
+        S5<R> flux;
+        if (dface == 0 || dface == nlast) {
+            const int side = dface == 0 ? 0 : 1;
+            const int ni_ = DIR == 0 ? (side ? c.ni - 1 : 0) : fi;
+            const int nj_ = DIR == 1 ? (side ? c.nj - 1 : 0) : fj;
+            const int nk_ = DIR == 2 ? (side ? c.nk - 1 : 0) : fk;
+            const long long q = nodeIdx(c, ni_, nj_, nk_);
+            if (side == 0) n = -n;  // outward normal of the start face
+            int pidx;
+            if (DIR == 0) pidx = c.mapI[(static_cast<long long>(side) * c.nj + fj) * c.nk + fk];
+            else if (DIR == 1) pidx = c.mapJ[(static_cast<long long>(fi) * 2 + side) * c.nk + fk];
+            else pidx = c.mapK[(static_cast<long long>(fi) * c.nj + fj) * 2 + side];
+            // theta of the face's (i, j, k) node for the cylindrical inlet frame
+            const long long qth =
+                nodeIdx(c, fi < c.ni ? fi : c.ni - 1, fj < c.nj ? fj : c.nj - 1, fk < c.nk ? fk : c.nk - 1);
+            flux = boundaryFlux(c, gs, pidx, load5(U, q), n, qth, fj, it);
+        } else {
+            const long long qR = nodeIdx(c, fi, fj, fk);
+            const long long qL = qR - st;
+            // faces whose four stencil nodes are plain interior nodes read the
+            // primitives k_prim computed once per node (bitwise the same values
+            // as converting here); faces next to a boundary or a periodic seam
+            // extrapolate or rotate conservative states first
+            const bool plain = dface >= 2 && dface <= nlast - 2;
+            if (plain) {
+                if (SCHEME == 0) {
+                    flux = fluxJstW(gs, load5(U, qL - st), load5(U, qL), load5(U, qR), load5(U, qR + st),
+                                    load5(c.W, qL - st), load5(c.W, qL), load5(c.W, qR), load5(c.W, qR + st), n);
+                } else {
+                    flux = fluxRoeW(gs, c.muscl, c.limiter, c.muscl ? load5(c.W, qL - st) : zero5<R>(),
+                                    load5(c.W, qL), load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5<R>(), n);
+                }
+            } else {
+                const S5<R> Ul = load5(U, qL), Ur = load5(U, qR);
+                S5<R> Ull, Urr;
+                if (DIR == 2 && c.periodic) {
+                    if (dface == 1) {
+                        Ull = rotState(load5(U, nodeIdx(c, fi, fj, c.nk - 2)), R(c.per_cos_m), R(c.per_sin_m));
+                        Urr = load5(U, qR + 1);
+                    } else {  // dface == nlast - 1
+                        Ull = load5(U, qR - 2);
+                        Urr = rotState(load5(U, nodeIdx(c, fi, fj, 1)), R(c.per_cos_p), R(c.per_sin_p));
+                    }
+                } else {
+                    if (dface == 1) {
+                        Ull = Ul - (Ur - Ul);
+                        Urr = load5(U, qR + st);
+                    } else {  // dface == nlast - 1
+                        Ull = load5(U, qL - st);
+                        Urr = Ur + (Ur - Ul);
+                    }
+                }
+                if (SCHEME == 0) flux = fluxJst(gs, Ull, Ul, Ur, Urr, n);
+                else flux = fluxRoe(gs, c.muscl, c.limiter, Ull, Ul, Ur, Urr, n);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) F.c[v][f] = flux.v[v] * area;
+    }
+}
+
+// Primitives of the stage input (getPrimitiveVariablesFromConservative,
+// src/math_utils.cpp:49-57), once per node for the face kernels.
+template <typename R>
+__global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    const Tile tl = stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    R* const* U = stageIn(c, stage);
+    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x)
+        store5(c.W, q, primOf(load5(U, q)));
+}
+
+// ------------------------------------------------------------------ nodes
+// Residual assembly in the reference's accumulation order (I faces, J faces,
+// K faces, then sources), then Solver::updateSolution (src/solver.cpp:2230-2249)
+// U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
+// Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
+template <typename R>
+__global__ void __launch_bounds__(256, 2) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    const Tile tl = stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    const Gas<R> gs{R(c.gamma), R(c.rgas)};
+    const double t = c.ctl->t;
+    const R dtg = R(c.ctl->dt_min);
+    const bool resOnly = stage < 0;
+    const bool last = !resOnly && stage == c.nstages - 1;
+    const R alpha = resOnly ? R(0) : R(c.coeffs[stage]);
+    R* const* Uin = stageIn(c, stage);
+    R* const* Uout = stageOut(c, stage);
+    double acc[5] = {0, 0, 0, 0, 0};
+    const int nj = c.nj, nk = c.nk;
+    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) {
+        const int k = static_cast<int>(q % nk);
+        const long long tq = q / nk;
+        const int j = static_cast<int>(tq % nj);
+        const int i = static_cast<int>(tq / nj);
+        S5<R> Res = zero5<R>();
+        {  // I faces: face i (node is right, or the start boundary) then face i+1
+            const long long f0 = (static_cast<long long>(i) * nj + j) * nk + k;
+            const long long f1 = f0 + static_cast<long long>(nj) * nk;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const R a = c.f[0].c[v][f0];
+                Res.v[v] = (i == 0) ? Res.v[v] + a : Res.v[v] - a;
+                Res.v[v] = Res.v[v] + c.f[0].c[v][f1];
+            }
+        }
+        {  // J faces
+            const long long f0 = (static_cast<long long>(i) * (nj + 1) + j) * nk + k;
+            const long long f1 = f0 + nk;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const R a = c.f[1].c[v][f0];
+                Res.v[v] = (j == 0) ? Res.v[v] + a : Res.v[v] - a;
+                Res.v[v] = Res.v[v] + c.f[1].c[v][f1];
+            }
+        }
+        if (c.topo == 1 && !(c.bfm && c.bpresent[nodeIdx(c, i, j, 0)] > R(0))) {  // K faces
+            const long long f0 = (static_cast<long long>(i) * nj + j) * (nk + 1) + k;
+            const long long f1 = f0 + 1;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const R a = c.f[2].c[v][f0];
+                Res.v[v] = (k == 0) ? Res.v[v] + a : Res.v[v] - a;
+                Res.v[v] = Res.v[v] + c.f[2].c[v][f1];
+            }
+        }
+        const S5<R> Unode = load5(Uin, q);
+        applySources(c, gs, Uin, i, j, k, q, Unode, t, Res);
+        if (c.periodic && (k == 0 || k == nk - 1)) {
+            const long long pq = (k == 0 ? 0 : c.n / nk) + static_cast<long long>(i) * nj + j;
+            store5(c.Rp, pq, Res);
+            continue;
+        }
+        if (resOnly) {
+            store5(Uout, q, Res);
+            continue;
+        }
+        const R dt = c.dt_method == 1 ? dtg : (c.dt_method == 2 ? R(c.fixed_dt) : c.dt[q]);
+        const R fac = alpha * dt / c.vol[q];
+        const S5<R> Un = load5(c.U, q);
+        S5<R> Un1;
+        if (c.compensated) {
+            const S5<R> Cn = load5(c.Uc, q);
+            S5<R> Cn1;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const R y = -(Res.v[v] * fac) - Cn.v[v];
+                const R s = Un.v[v] + y;
+                Cn1.v[v] = (s - Un.v[v]) - y;
+                Un1.v[v] = s;
+            }
+            if (last) store5(c.Uc, q, Cn1);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 5; v++) Un1.v[v] = Un.v[v] - Res.v[v] * fac;
+        }
+        store5(Uout, q, Un1);
+        if (last)
+#pragma unroll
+            for (int v = 0; v < 5; v++) acc[v] += static_cast<double>(Res.v[v]) * static_cast<double>(Res.v[v]);
+    }
+    if (last) {
+        blockSum<5>(acc);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int v = 0; v < 5; v++) c.partial[tl.local * 5 + v] = acc[v];
+    }
+}
+
+// Solver::enforcePeriodicityOnResiduals (src/solver.cpp:1836-1853), the update
+// of the two periodic planes and Solver::enforcePeriodicityOnSolution
+// (src/solver.cpp:2308-2327). One thread per (i, j) pair.
+template <typename R>
+__global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    const Tile tl = stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    const R dtg = R(c.ctl->dt_min);
+    const bool resOnly = stage < 0;
+    const bool last = !resOnly && stage == c.nstages - 1;
+    const R alpha = resOnly ? R(0) : R(c.coeffs[stage]);
+    R* const* Uout = stageOut(c, stage);
+    const R cm = R(c.per_cos_m), sm = R(c.per_sin_m), cp = R(c.per_cos_p), sp = R(c.per_sin_p);
+    const long long np = static_cast<long long>(c.ni) * c.nj;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long p = tl.start + threadIdx.x; p < tl.start + tl.count; p += blockDim.x) {
+        const S5<R> R1 = load5(c.Rp, p), R2 = load5(c.Rp, np + p);
+        const S5<R> Ra = (R1 + rotState(R2, cm, sm)) * R(0.5);
+        const S5<R> Rb = rotState(Ra, cp, sp);
+        const long long q0 = p * c.nk, q1 = p * c.nk + c.nk - 1;
+        if (resOnly) {
+            store5(Uout, q0, Ra);
+            store5(Uout, q1, Rb);
+            continue;
+        }
+        const R dt0 = c.dt_method == 1 ? dtg : (c.dt_method == 2 ? R(c.fixed_dt) : c.dt[q0]);
+        const R dt1 = c.dt_method == 1 ? dtg : (c.dt_method == 2 ? R(c.fixed_dt) : c.dt[q1]);
+        const R f0 = alpha * dt0 / c.vol[q0];
+        const R f1 = alpha * dt1 / c.vol[q1];
+        S5<R> U0, U1;
+        if (c.compensated) {
+            const S5<R> A0 = load5(c.U, q0), A1 = load5(c.U, q1);
+            const S5<R> C0 = load5(c.Uc, q0), C1 = load5(c.Uc, q1);
+            S5<R> D0, D1;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const R y0 = -(Ra.v[v] * f0) - C0.v[v];
+                U0.v[v] = A0.v[v] + y0;
+                D0.v[v] = (U0.v[v] - A0.v[v]) - y0;
+                const R y1 = -(Rb.v[v] * f1) - C1.v[v];
+                U1.v[v] = A1.v[v] + y1;
+                D1.v[v] = (U1.v[v] - A1.v[v]) - y1;
+            }
+            if (last) {
+                const S5<R> Da = (D0 + rotState(D1, cm, sm)) * R(0.5);
+                store5(c.Uc, q0, Da);
+                store5(c.Uc, q1, rotState(Da, cp, sp));
+            }
+        } else {
+            U0 = load5(c.U, q0) - Ra * f0;
+            U1 = load5(c.U, q1) - Rb * f1;
+        }
+        const S5<R> Ua = (U0 + rotState(U1, cm, sm)) * R(0.5);
+        store5(Uout, q0, Ua);
+        store5(Uout, q1, rotState(Ua, cp, sp));
+        if (last)
+#pragma unroll
+            for (int v = 0; v < 5; v++)
+                acc[v] += static_cast<double>(Ra.v[v]) * static_cast<double>(Ra.v[v]) +
+                          static_cast<double>(Rb.v[v]) * static_cast<double>(Rb.v[v]);
+    }
+    if (last) {
+        blockSum<5>(acc);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int v = 0; v < 5; v++) c.partial[(c.node_tiles + tl.local) * 5 + v] = acc[v];
+    }
+}
+
+// ------------------------------------------------------------- time step
+// Solver::computeTimestepArray (src/solver.cpp:1531-1630), inviscid:
+// dt = CFL / sum_d (|u . e_d| + a) / |e_d| over the dual-node edges.
+template <typename R>
+__global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile* tiles, int force) {
+    __shared__ DevCaseT<R> c;
+    const Tile tl = stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    if (c.dt_method == 2) return;
+    const Gas<R> gs{R(c.gamma), R(c.rgas)};
+    const R cfl = R(c.cfl);
+    double mn = INFINITY;
+    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) {
+        const S5<R> W = primOf(load5(c.U, q));
+        const V3<R> u = velOf(W);
+        const R a = soundSpeed_rho_u_et(gs, W.v[0], u, W.v[4]);
+        const V3<R> dI = v3(c.edge[0][q], c.edge[1][q], c.edge[2][q]);
+        const V3<R> dJ = v3(c.edge[4][q], c.edge[5][q], c.edge[6][q]);
+        const R ui = fabs(dot(u, dI)), uj = fabs(dot(u, dJ));
+        R lc = (ui + a) / c.edge[3][q];
+        lc += (uj + a) / c.edge[7][q];
+        if (c.topo == 1) {
+            const V3<R> dK = v3(c.edge[8][q], c.edge[9][q], c.edge[10][q]);
+            lc += (fabs(dot(u, dK)) + a) / c.edge[11][q];
+        }
+        const R dt = cfl / lc;
+        c.dt[q] = dt;
+        mn = fmin(mn, static_cast<double>(dt));
+    }
+    mn = blockMin(mn);
+    if (threadIdx.x == 0) c.partial[(c.node_tiles + c.per_tiles) * 5 + tl.local] = mn;
+}
+
+// ------------------------------------------------------ boundary integrals
+// Solver::updateMassFlows (src/solver.cpp:1633-1649) and the mass-weighted
+// total pressure / temperature integrals of Solver::updateTurboPerformance
+// (src/solver.cpp:1652-1781), in double. Tile.local = 0..5: mass flow through
+// plane `local`; 6, 7: Pt and Tt integrals over the inlet / outlet planes.
+template <typename R>
+__device__ __forceinline__ void planeExtent(const DevCaseT<R>& c, int b, int& na, int& nb) {
+    if (b <= 1) { na = c.nj; nb = c.nk; }
+    else if (b <= 3) { na = c.ni; nb = c.nk; }
+    else { na = c.ni; nb = c.nj; }
+}
+template <typename R>
+__device__ __forceinline__ long long planeNode(const DevCaseT<R>& c, int b, int a, int bb) {
+    switch (b) {
+        case 0: return nodeIdx(c, 0, a, bb);
+        case 1: return nodeIdx(c, c.ni - 1, a, bb);
+        case 2: return nodeIdx(c, a, 0, bb);
+        case 3: return nodeIdx(c, a, c.nj - 1, bb);
+        case 4: return nodeIdx(c, a, bb, 0);
+        default: return nodeIdx(c, a, bb, c.nk - 1);
+    }
+}
+template <typename R>
+__device__ __forceinline__ int turboPlane(const DevCaseT<R>& c, int m) {
+    switch (c.turbo_dir) {
+        case 1: return m == 0 ? 1 : 0;
+        case 2: return m == 0 ? 2 : 3;
+        case 3: return m == 0 ? 3 : 2;
+        default: return m == 0 ? 0 : 1;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Tile* tiles, int force) {
+    __shared__ DevCaseT<R> c;
+    const Tile tl = stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    const Gas<double> gs{c.gamma, c.rgas};
+    const int blk = tl.local;
+    const int plane = blk < 6 ? blk : turboPlane(c, blk - 6);
+    int na, nb;
+    planeExtent(c, plane, na, nb);
+    const long long cnt = static_cast<long long>(na) * nb;
+    double s[2] = {0.0, 0.0};
+    for (long long e = threadIdx.x; e < cnt; e += blockDim.x) {
+        const int a = static_cast<int>(e / nb), bb = static_cast<int>(e % nb);
+        const long long q = planeNode(c, plane, a, bb);
+        const double sx = c.bsx[plane][e], sy = c.bsy[plane][e], sz = c.bsz[plane][e];
+        const S5<double> Uq = state64(c, c.U, q);
+        if (blk < 6) {
+            s[0] += sx * Uq.v[1] + sy * Uq.v[2] + sz * Uq.v[3];
+        } else {
+            const S5<double> W = primOf(Uq);
+            const double rho = W.v[0];
+            const V3<double> u = velOf(W);
+            const double P = totalPressure_rho_u_et(gs, rho, u, W.v[4]);
+            const double T = totalTemperature_rho_u_et(gs, rho, u, W.v[4]);
+            s[0] += sx * (rho * u.x * P) + sy * (rho * u.y * P) + sz * (rho * u.z * P);
+            s[1] += sx * (rho * u.x * T) + sy * (rho * u.y * T) + sz * (rho * u.z * T);
+        }
+    }
+    blockSum<2>(s);
+    if (threadIdx.x == 0) {
+        if (blk < 6) c.ctl->massflow[blk] = s[0];
+        else {
+            c.ctl->pt_int[blk - 6] = s[0];
+            c.ctl->tt_int[blk - 6] = s[1];
+        }
+    }
+}
+
+// ------------------------------------------------------------ pre-stage
+// Global min(dt); turbo performance with FluidIdeal::computeTotalEfficiency_PRtt_TRt
+// (src/fluid_ideal.cpp:179-191); GreitzerModel::computePlenumPressure
+// (src/greitzer_model.cpp:36-56); Solver::updateRadialProfiles
+// (src/solver.cpp:2688-2787) with integrateRadialEquilibrium
+// (src/math_utils.cpp:141-170). All double. One block per instance.
+template <typename R>
+__global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Tile* tiles, int forceTurbo, int dtpart,
+                                             int profiles, int force) {
+    __shared__ DevCaseT<R> c;
+    stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    Control* ctl = c.ctl;
+    if (!dtpart) {
+    } else if (c.dt_method == 2) {
+        if (threadIdx.x == 0) ctl->dt_min = c.fixed_dt;
+    } else {
+        double mn = INFINITY;
+        const double* part = c.partial + (c.node_tiles + c.per_tiles) * 5;
+        for (int b = threadIdx.x; b < c.node_tiles; b += blockDim.x) mn = fmin(mn, part[b]);
+        mn = blockMin(mn);
+        if (threadIdx.x == 0) ctl->dt_min = mn;
+    }
+    if (threadIdx.x != 0) return;
+    if (c.need_turbo || forceTurbo) {
+        const int p0 = turboPlane(c, 0), p1 = turboPlane(c, 1);
+        double mflow = 0.5 * (fabs(ctl->massflow[p0]) + fabs(ctl->massflow[p1]));
+        if (c.topo == 2) mflow *= 2.0 * M_PI / c.wedge;
+        else if (c.per_angle_deg != 0.0) mflow *= 360.0 / c.per_angle_deg;
+        double pt[2], tt[2];
+        for (int m = 0; m < 2; m++) {
+            double mf = ctl->massflow[m == 0 ? p0 : p1];
+            if (fabs(mf) < 1e-12) mf = (mf >= 0.0 ? 1e-12 : -1e-12);
+            pt[m] = ctl->pt_int[m] / mf;
+            tt[m] = ctl->tt_int[m] / mf;
+        }
+        const double pr = (fabs(pt[0]) > 1e-12) ? pt[1] / pt[0] : 1.0;
+        const double tr = (fabs(tt[0]) > 1e-12) ? tt[1] / tt[0] : 1.0;
+        const double dT = tr - 1.0;
+        const double dTs = pow(pr, (c.gamma - 1.0) / c.gamma) - 1.0;
+        double eta;
+        if (fabs(dT) < 1e-12) eta = 1.0;
+        else if (dT >= 0.0) eta = dTs / dT;
+        else eta = (fabs(dTs) < 1e-12) ? 1.0 : dT / dTs;
+        ctl->turbo[0] = mflow;
+        ctl->turbo[1] = pr;
+        ctl->turbo[2] = tr;
+        ctl->turbo[3] = eta;
+        ctl->has_turbo = 1;
+    }
+    if (!profiles || (c.nprofiles == 0 && !c.greitzer)) return;
+    if (c.greitzer) {
+        ctl->gz_min = ctl->turbo[0];
+        ctl->gz_t += c.fixed_dt;
+        const double a = sqrt(c.gamma * c.rgas * ctl->gz_T);
+        const double np = ctl->gz_p + c.fixed_dt * a * a / c.plenum_volume * (ctl->gz_min - ctl->gz_mout);
+        ctl->gz_p = np;
+        const double dp = ctl->gz_p - c.ambient_p;
+        ctl->gz_mout = (dp > 0.0) ? sqrt(dp / c.throttle_kt) : 0.0;
+        ctl->hub_p = ctl->gz_p;
+    }
+    for (int m = 0; m < c.nprofiles; m++) {
+        double* p = c.prof_p + c.prof_off[m];
+        const double* r = c.prof_r + c.prof_off[m];
+        const int n = c.prof_n[m];
+        if (c.greitzer) {
+        } else if (c.prof_type[m] == kBcThrottle) {
+            ctl->hub_p = c.inlet_pt + c.prof_kt[m] * ctl->turbo[0] * ctl->turbo[0];
+        } else if (c.prof_type[m] == kBcRadialEq) {
+            ctl->hub_p = p[0];
+        }
+        // sample density and |u_theta| at (prof_i, j, 0) and integrate dp/dr
+        double rho1 = 0, ut1 = 0;
+        p[0] = ctl->hub_p;
+        for (int jj = 0; jj < n; jj++) {
+            const long long q = nodeIdx(c, c.prof_i[m], c.prof_j0[m] + jj, 0);
+            const S5<double> W = primOf(state64(c, c.U, q));
+            const V3<double> vc = cylOfCart(velOf(W), c.cost64[q], c.sint64[q]);
+            const double rho2 = W.v[0], ut2 = fabs(vc.z);
+            if (jj > 0) {
+                const double r1 = r[jj - 1], r2 = r[jj];
+                const double dr = r2 - r1;
+                const double d1 = rho1 * ut1 * ut1 / r1;
+                const double d2 = rho2 * ut2 * ut2 / r2;
+                p[jj] = p[jj - 1] + 0.5 * (d1 + d2) * dr;
+            }
+            rho1 = rho2;
+            ut1 = ut2;
+        }
+    }
+}
+
+// ------------------------------------------------------------- finalize
+// Solver::computeLogResidualNorm (src/solver.cpp:1488-1508),
+// printInfoResiduals' initial maximum (src/solver.cpp:1426-1439),
+// Solver::checkConvergence (src/solver.cpp:2985-3015) and the time advance
+// t += min(dt) (src/solver.cpp:1389). One block per instance.
+template <typename R>
+__global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, const Tile* tiles, int force) {
+    __shared__ DevCaseT<R> c;
+    stageCase(cases, tiles, c);
+    if (halted(c, force)) return;
+    Control* ctl = c.ctl;
+    const int nparts = c.node_tiles + (c.periodic ? c.per_tiles : 0);
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+#pragma unroll
+        for (int v = 0; v < 5; v++) s[v] += c.partial[b * 5 + v];
+    blockSum<5>(s);
+    if (threadIdx.x != 0) return;
+    const long long it = ctl->it + 1;
+    ctl->t += ctl->dt_min;
+    double lr[5];
+    bool diverged = false;
+    for (int v = 0; v < 5; v++) {
+        const double nrm = sqrt(s[v]);
+        if (isnan(nrm) || isinf(nrm)) diverged = true;
+        lr[v] = (nrm >= 2.2250738585072014e-308) ? log10(nrm / static_cast<double>(c.n)) : -16.0;
+        if (lr[v] < -16.0) lr[v] = -16.0;
+        ctl->lognorm[v] = lr[v];
+    }
+    ctl->it = it;
+    if (diverged) {
+        ctl->status = 2;
+        return;
+    }
+    if (!ctl->has_init) {
+        for (int v = 0; v < 5; v++) ctl->init_log[v] = lr[v];
+        ctl->has_init = 1;
+    } else if (it <= 5) {
+        for (int v = 0; v < 5; v++) ctl->init_log[v] = rmax(ctl->init_log[v], lr[v]);
+    }
+    const long long row = it - 1 - ctl->hist_base;
+    if (c.hist && row >= 0 && row < c.hist_cap) {
+        double* h = c.hist + row * 16;
+        for (int v = 0; v < 5; v++) h[v] = lr[v];
+        for (int b = 0; b < 6; b++) h[5 + b] = ctl->massflow[b];
+        for (int b = 0; b < 4; b++) h[11 + b] = c.need_turbo ? ctl->turbo[b] : 0.0;
+        h[15] = ctl->hub_p;
+    }
+    if (c.steady) {
+        bool conv = true;
+        for (int v = 0; v < 5; ++v) {
+            if (v == 3 && c.topo != 1 && c.topo != 2) continue;
+            if (ctl->init_log[v] <= -15.99) continue;
+            if (lr[v] <= -15.0) continue;
+            if (lr[v] >= ctl->init_log[v] - static_cast<double>(c.drop)) {
+                conv = false;
+                break;
+            }
+        }
+        if (conv) ctl->status = 1;
+    }
+}
+
+// Sets each instance's iteration limit (n more iterations) and history origin.
+template <typename R>
+__global__ void k_set_limits(const DevCaseT<R>* cases, int m, long long n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    Control* ctl = cases[i].ctl;
+    ctl->it_stop = ctl->it + n;
+    ctl->hist_base = ctl->it;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+
+template <typename R>
+cudaError_t Launcher<R>::setLimits(const BatchView<R>& b, long long n, cudaStream_t s) {
+    k_set_limits<R><<<(b.m + 127) / 128, 128, 0, s>>>(b.cases, b.m, n);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::boundaryIntegrals(const BatchView<R>& b, bool all, int force, cudaStream_t s) {
+    const TileList& t = all ? b.bintAll : b.bint;
+    if (t.n) k_bint<R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::timeStep(const BatchView<R>& b, int force, cudaStream_t s) {
+    if (b.node.n) k_dt<R><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::pre(const BatchView<R>& b, bool forceTurbo, bool dtpart, bool profiles, int force,
+                             cudaStream_t s) {
+    if (b.inst.n)
+        k_pre<R><<<b.inst.n, 256, 0, s>>>(b.cases, b.inst.tiles, forceTurbo ? 1 : 0, dtpart ? 1 : 0, profiles ? 1 : 0,
+                                          force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::prim(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    if (b.node.n) k_prim<R><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::faces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s) {
+    for (int sch = 0; sch < 2; sch++) {
+        const TileList& t = b.face[dir][sch];
+        if (!t.n) continue;
+        if (sch == 0) {
+            if (dir == 0) k_faces<0, 0, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else if (dir == 1) k_faces<1, 0, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else k_faces<2, 0, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+        } else {
+            if (dir == 0) k_faces<0, 1, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else if (dir == 1) k_faces<1, 1, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else k_faces<2, 1, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+        }
+    }
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    if (b.node.n) k_nodes<R><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    if (b.per.n) k_periodic<R><<<b.per.n, 256, 0, s>>>(b.cases, b.per.tiles, stage, force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::finalize(const BatchView<R>& b, int force, cudaStream_t s) {
+    if (b.inst.n) k_finalize<R><<<b.inst.n, 256, 0, s>>>(b.cases, b.inst.tiles, force);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::stage(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    cudaError_t e = prim(b, stage, force, s);
+    for (int d = 0; d < 3 && e == cudaSuccess; d++) e = faces(b, d, stage, force, s);
+    if (e == cudaSuccess) e = nodes(b, stage, force, s);
+    if (e == cudaSuccess) e = periodic(b, stage, force, s);
+    return e;
+}
+
+template <typename R>
+cudaError_t Launcher<R>::iteration(const BatchView<R>& b, int nstages, cudaStream_t s) {
+    cudaError_t e = boundaryIntegrals(b, false, 0, s);
+    if (e == cudaSuccess) e = timeStep(b, 0, s);
+    if (e == cudaSuccess) e = pre(b, false, true, true, 0, s);
+    for (int st = 0; st < nstages && e == cudaSuccess; st++) e = stage(b, st, 0, s);
+    if (e == cudaSuccess) e = finalize(b, 0, s);
+    return e;
+}
+
+}  // namespace ctbfm

@@ -1,0 +1,166 @@
+// Device-side engine: see engine.hpp.
+#include "engine.hpp"
+
+#include <algorithm>
+
+namespace ctbfm {
+
+// ---------------------------------------------------------------- InstanceT
+
+template <typename R>
+InstanceT<R>::~InstanceT() {
+    for (void* p : allocs_) cudaFree(p);
+}
+
+template <typename R>
+void* InstanceT<R>::allocBytes(size_t n) {
+    void* p = nullptr;
+    cudaCheck(cudaMalloc(&p, std::max<size_t>(n, 16)), "cudaMalloc");
+    allocs_.push_back(p);
+    bytes_ += std::max<size_t>(n, 16);
+    return p;
+}
+
+template <typename R>
+R* InstanceT<R>::allocR(size_t n) {
+    return static_cast<R*>(allocBytes(n * sizeof(R)));
+}
+
+template <typename R>
+double* InstanceT<R>::allocD(size_t n) {
+    return static_cast<double*>(allocBytes(n * sizeof(double)));
+}
+
+template <typename R>
+const R* InstanceT<R>::uploadR(const std::vector<double>& v) {
+    R* d = allocR(v.size());
+    if (sizeof(R) == sizeof(double)) {
+        cudaCheck(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    } else {
+        std::vector<R> tmp(v.begin(), v.end());
+        cudaCheck(cudaMemcpy(d, tmp.data(), tmp.size() * sizeof(R), cudaMemcpyHostToDevice), "cudaMemcpy");
+    }
+    return d;
+}
+
+template <typename R>
+const double* InstanceT<R>::uploadD(const std::vector<double>& v) {
+    double* d = allocD(v.size());
+    cudaCheck(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    return d;
+}
+
+// ------------------------------------------------------------------- GroupT
+
+template <typename R>
+GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(members)) {
+    if (members_.empty()) throw std::invalid_argument("empty group");
+    nstages_ = members_[0]->c.nstages;
+    for (auto* m : members_)
+        if (m->c.nstages != nstages_)
+            throw std::invalid_argument("all members of a group need the same number of Runge-Kutta stages");
+    const int M = static_cast<int>(members_.size());
+    // tile lists over the packed index of all members
+    std::vector<Tile> node, face[3][2], per, inst, bint, bintAll;
+    auto cover = [](std::vector<Tile>& out, int m, long long count) {
+        int local = 0;
+        for (long long s = 0; s < count; s += kTileSize) out.push_back({m, local++, s, std::min<long long>(kTileSize, count - s)});
+        return local;
+    };
+    for (int m = 0; m < M; m++) {
+        const DevCaseT<R>& c = members_[m]->c;
+        const int nt = cover(node, m, c.n);
+        if (nt != c.node_tiles) throw std::logic_error("node tile count mismatch");
+        for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++) {
+            const long long nf =
+                static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
+            cover(face[d][c.scheme], m, nf);
+        }
+        if (c.periodic) cover(per, m, static_cast<long long>(c.ni) * c.nj);
+        inst.push_back({m, 0, 0, 1});
+        for (int b = 0; b < 8; b++) {
+            bintAll.push_back({m, b, 0, 1});
+            if (c.need_turbo) bint.push_back({m, b, 0, 1});
+        }
+    }
+    std::vector<Tile> all;
+    std::vector<std::pair<TileList*, size_t>> offs;
+    auto add = [&](TileList& tl, const std::vector<Tile>& v) {
+        offs.push_back({&tl, all.size()});
+        tl.n = static_cast<int>(v.size());
+        all.insert(all.end(), v.begin(), v.end());
+    };
+    add(view_.node, node);
+    for (int d = 0; d < 3; d++)
+        for (int s = 0; s < 2; s++) add(view_.face[d][s], face[d][s]);
+    add(view_.per, per);
+    add(view_.inst, inst);
+    add(view_.bint, bint);
+    add(view_.bintAll, bintAll);
+    cudaCheck(cudaMalloc(&dTiles_, std::max<size_t>(all.size(), 1) * sizeof(Tile)), "cudaMalloc");
+    cudaCheck(cudaMemcpy(dTiles_, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice), "cudaMemcpy");
+    for (auto& [tl, off] : offs) tl->tiles = dTiles_ + off;
+    cudaCheck(cudaMalloc(&dCases_, M * sizeof(DevCaseT<R>)), "cudaMalloc");
+    view_.cases = dCases_;
+    view_.m = M;
+    refresh(nullptr);
+    cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+template <typename R>
+GroupT<R>::~GroupT() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (captureStream_) {
+        cudaStreamSynchronize(captureStream_);
+        cudaStreamDestroy(captureStream_);
+    }
+    cudaFree(dCases_);
+    cudaFree(dTiles_);
+}
+
+// One pageable host-to-device copy per member, ordered on s: each call returns
+// once its source is staged, so the host copy may change right after.
+template <typename R>
+void GroupT<R>::refresh(cudaStream_t s) {
+    for (size_t i = 0; i < members_.size(); i++)
+        cudaCheck(cudaMemcpyAsync(dCases_ + i, &members_[i]->c, sizeof(DevCaseT<R>), cudaMemcpyHostToDevice, s),
+                  "cudaMemcpyAsync");
+}
+
+template <typename R>
+void GroupT<R>::capture() {
+    if (graph_) return;
+    cudaGraph_t g = nullptr;
+    cudaCheck(cudaStreamBeginCapture(captureStream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < graphIters_ && e == cudaSuccess; i++) e = Launcher<R>::iteration(view_, nstages_, captureStream_);
+    const cudaError_t e2 = cudaStreamEndCapture(captureStream_, &g);
+    cudaCheck(e, "launch during graph capture");
+    cudaCheck(e2, "cudaStreamEndCapture");
+    const cudaError_t e3 = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    cudaCheck(e3, "cudaGraphInstantiate");
+}
+
+template <typename R>
+void GroupT<R>::enqueue(long long n, cudaStream_t s) {
+    if (n <= 0) return;
+    cudaCheck(Launcher<R>::setLimits(view_, n, s), "launch k_set_limits");
+    long long left = n;
+    if (left >= graphIters_) {
+        capture();
+        while (left >= graphIters_) {
+            cudaCheck(cudaGraphLaunch(graph_, s), "cudaGraphLaunch");
+            left -= graphIters_;
+        }
+    }
+    for (long long i = 0; i < left; i++) cudaCheck(Launcher<R>::iteration(view_, nstages_, s), "launch iteration");
+}
+
+template class InstanceT<double>;
+template class InstanceT<float>;
+template class GroupT<double>;
+template class GroupT<float>;
+
+}  // namespace ctbfm

@@ -1,0 +1,86 @@
+// Device-side engine: InstanceT<R> owns one operating point's device arrays
+// (working precision R); GroupT<R> advances any set of instances together —
+// it uploads their descriptions, builds the tile lists every kernel family
+// launches over (a packed index of all instances' nodes, faces and planes) and
+// captures CUDA graphs of whole iterations.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../device/case.cuh"
+#include "../device/kernels.hpp"
+
+namespace ctbfm {
+
+class CudaError : public std::runtime_error {
+public:
+    using std::runtime_error::runtime_error;
+};
+
+inline void cudaCheck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename R>
+class InstanceT {
+public:
+    InstanceT() = default;
+    ~InstanceT();
+    InstanceT(const InstanceT&) = delete;
+    InstanceT& operator=(const InstanceT&) = delete;
+
+    R* allocR(size_t n);
+    double* allocD(size_t n);
+    const R* uploadR(const std::vector<double>& v);
+    const double* uploadD(const std::vector<double>& v);
+    void* allocBytes(size_t n);
+    size_t deviceBytes() const { return bytes_; }
+
+    DevCaseT<R> c{};  // host copy of the description, pointers into this instance's device arrays
+
+private:
+    std::vector<void*> allocs_;
+    size_t bytes_ = 0;
+};
+
+template <typename R>
+class GroupT {
+public:
+    explicit GroupT(std::vector<InstanceT<R>*> members);
+    ~GroupT();
+    GroupT(const GroupT&) = delete;
+    GroupT& operator=(const GroupT&) = delete;
+
+    // n iterations of every member (fewer for members that converge or
+    // diverge), enqueued on s without host synchronisation.
+    void enqueue(long long n, cudaStream_t s);
+    const BatchView<R>& view() const { return view_; }
+    int stages() const { return nstages_; }
+    int size() const { return static_cast<int>(members_.size()); }
+    // Re-uploads the members' descriptions (after a member's host copy
+    // changed), ordered on stream s; allocates nothing.
+    void refresh(cudaStream_t s);
+
+private:
+    void capture();
+
+    std::vector<InstanceT<R>*> members_;
+    int nstages_ = 0;
+    DevCaseT<R>* dCases_ = nullptr;
+    Tile* dTiles_ = nullptr;
+    BatchView<R> view_;
+    cudaStream_t captureStream_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    int graphIters_ = 8;
+};
+
+extern template class InstanceT<double>;
+extern template class InstanceT<float>;
+extern template class GroupT<double>;
+extern template class GroupT<float>;
+
+}  // namespace ctbfm

@@ -45,24 +45,6 @@ struct HostGas {
 
 }  // namespace
 
-void Solver::check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-double* Solver::alloc(size_t count) {
-    void* p = nullptr;
-    check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(double)), "cudaMalloc");
-    allocations_.push_back(p);
-    deviceBytes_ += std::max<size_t>(count, 1) * sizeof(double);
-    return static_cast<double*>(p);
-}
-
-const double* Solver::upload(const std::vector<double>& v) {
-    double* d = alloc(v.size());
-    check(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
-    return d;
-}
-
 Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_(config.getTopology()) {
     if (config.isViscosityActive()) throw ConfigError("Viscous fluxes are outside this library's Euler path");
     if (config.parseBool("TURBULENCE_ACTIVE", false)) throw ConfigError("Turbulence models are outside this library's Euler path");
@@ -72,6 +54,11 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
         throw ConfigError("Only the ideal-gas fluid model is supported");
     if (config.isAccelerationActive() && config.getTimeStepMethod() != TimeStepMethod::Fixed)
         throw ConfigError("Rotational speed scaling factor is only active for fixed time step method");
+    // GPU_PRECISION (this library's key; the reference ignores unknown keys)
+    const std::string prec = config.has("GPU_PRECISION") ? config.get("GPU_PRECISION") : "fp64";
+    if (prec == "fp64") prec_ = kFP64;
+    else if (prec == "fp32_kahan") prec_ = kFP32Kahan;
+    else throw ConfigError("Invalid value for key \"GPU_PRECISION\" (fp64 or fp32_kahan)");
     coeffs_ = config.getTimeIntegrationCoeffs();
     maxIter_ = config.getMaxIterations();
     // every setting and input file is validated before the first CUDA call,
@@ -80,65 +67,22 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     readBoundaries();
     buildBoundaryStructures();
     validateSettings();
-    check(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    setupScalars();
+    cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = ownStream_;
-    check(cudaMallocHost(reinterpret_cast<void**>(&hostCtl_), sizeof(Control)), "cudaMallocHost");
+    cudaCheck(cudaMallocHost(reinterpret_cast<void**>(&hostCtl_), sizeof(Control)), "cudaMallocHost");
     std::memset(hostCtl_, 0, sizeof(Control));
-    uploadBoundaryStructures();
-    upload();
-    initializeSolution();
-    initializeProfilesAndPlenum();
-}
-
-// Parses every key the device set-up reads (the reference's getters throw on
-// the same inputs).
-void Solver::validateSettings() {
-    const TimeStepMethod m = config_.getTimeStepMethod();
-    config_.getCFL();
-    if (m == TimeStepMethod::Fixed) config_.getFixedTimeStep();
-    config_.getFluidGamma();
-    config_.getFluidGasConstant();
-    config_.getInitMachNumber();
-    config_.getInitTemperature();
-    config_.getInitPressure();
-    const std::string raw = config_.has("INIT_DIRECTION") ? config_.get("INIT_DIRECTION") : "";
-    if (raw != "adaptive") {
-        const auto items = config_.parseList("INIT_DIRECTION");
-        if (items.size() != 3) throw ConfigError("INIT_DIRECTION must have 3 components or be 'adaptive'");
-        for (const auto& it : items) {
-            try {
-                (void)std::stod(it);
-            } catch (const std::exception&) {
-                throw ConfigError("Invalid vector element for key \"INIT_DIRECTION\": \"" + it + "\"");
-            }
-        }
+    if (prec_ == kFP32Kahan) {
+        i32_ = std::make_unique<InstanceT<float>>();
+        uploadArrays(*i32_);
+        g32_ = std::make_unique<GroupT<float>>(std::vector<InstanceT<float>*>{i32_.get()});
+        initializeState(*i32_, *g32_);
+    } else {
+        i64_ = std::make_unique<InstanceT<double>>();
+        uploadArrays(*i64_);
+        g64_ = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{i64_.get()});
+        initializeState(*i64_, *g64_);
     }
-    config_.getResidualsDropConvergence();
-    config_.isSimulationSteady();
-    config_.isInletCylindrical();
-    config_.getOutletPressureRampMaxIterations();
-    config_.getRotationalSpeedScalingFactor();
-    if (config_.isAccelerationActive()) {
-        config_.parseFloat("ACCELERATION_INITIAL_TIME");
-        config_.parseFloat("ACCELERATION_FINAL_TIME");
-        config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_INITIAL");
-        config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_FINAL");
-    }
-    if (config_.isPerturbationBodyForceActive()) {
-        if (config_.parseList("PERTURBATION_CENTER").size() < 3) throw ConfigError("PERTURBATION_CENTER needs 3 values");
-        config_.parseFloat("PERTURBATION_RADIAL_EXTENSION");
-        config_.parseFloat("PERTURBATION_SCALING_FACTOR");
-        config_.parseFloat("PERTURBATION_TIME_START");
-        config_.parseFloat("PERTURBATION_TIME_DURATION");
-    }
-}
-
-Solver::~Solver() {
-    if (graph_) cudaGraphExecDestroy(graph_);
-    if (ownStream_) cudaStreamSynchronize(ownStream_);
-    for (void* p : allocations_) cudaFree(p);
-    if (hostCtl_) cudaFreeHost(hostCtl_);
-    if (ownStream_) cudaStreamDestroy(ownStream_);
 }
 
 // Solver::buildAdvectionModel / buildBfmInfo (src/solver.cpp:185-198, 701-749).
@@ -209,7 +153,7 @@ void Solver::buildBoundaryStructures() {
     const long NI = mesh_.ni(), NJ = mesh_.nj(), NK = mesh_.nk();
     std::vector<double> profP, profR;
     int nprof = 0;
-    c_.periodic = 0;
+    proto_.periodic = 0;
     for (size_t m = 0; m < boundaries_.size(); m++) {
         BoundaryPatch& b = boundaries_[m];
         if (b.type == kBcRadialEq || b.type == kBcThrottle) {
@@ -219,12 +163,12 @@ void Solver::buildBoundaryStructures() {
             if (b.j_min != 0) throw ConfigError("radial profiles must start at j = 0 (the profile is indexed by the face's j)");
             if (nprof >= kMaxProfiles) throw ConfigError("too many radial profiles");
             const int n = static_cast<int>(b.j_max - b.j_min);
-            c_.prof_off[nprof] = static_cast<int>(profP.size());
-            c_.prof_n[nprof] = n;
-            c_.prof_type[nprof] = b.type;
-            c_.prof_i[nprof] = static_cast<int>(b.i_min > 0 ? b.i_min - 1 : 0);
-            c_.prof_j0[nprof] = static_cast<int>(b.j_min);
-            c_.prof_kt[nprof] = b.type == kBcThrottle ? (b.values.empty() ? 0.0 : b.values[0]) : 0.0;
+            proto_.prof_off[nprof] = static_cast<int>(profP.size());
+            proto_.prof_n[nprof] = n;
+            proto_.prof_type[nprof] = b.type;
+            proto_.prof_i[nprof] = static_cast<int>(b.i_min > 0 ? b.i_min - 1 : 0);
+            proto_.prof_j0[nprof] = static_cast<int>(b.j_min);
+            proto_.prof_kt[nprof] = b.type == kBcThrottle ? (b.values.empty() ? 0.0 : b.values[0]) : 0.0;
             for (long j = b.j_min; j < b.j_max; j++) {
                 profR.push_back(mesh_.radius(b.i_max - 1, j, 0));
                 profP.push_back(0.0);
@@ -240,7 +184,7 @@ void Solver::buildBoundaryStructures() {
                 if (periodicAngleDeg_ == 360.0) periodicAngleDeg_ = 0.0;
                 periodicAngleRad_ = periodicAngleDeg_ * M_PI / 180.0;
                 mesh_.checkPeriodicity(periodicTransl_, periodicAngleRad_);
-                c_.periodic = 1;
+                proto_.periodic = 1;
             }
             if (b.k_min != b.k_max) throw ConfigError("Periodic boundary only supported on i-j patches");
             if (b.i_min != 0 || b.j_min != 0 || b.i_max != NI || b.j_max != NJ)
@@ -257,11 +201,10 @@ void Solver::buildBoundaryStructures() {
         } else {
             b.flux = std::make_unique<BoundaryFake>(b.type);
         }
-        c_.patch[m] = b.flux->toDevice();
+        proto_.patch[m] = b.flux->toDevice();
     }
-    c_.npatches = static_cast<int>(boundaries_.size());
-    c_.nprofiles = nprof;
-    profiles_ = nprof > 0;
+    proto_.npatches = static_cast<int>(boundaries_.size());
+    proto_.nprofiles = nprof;
 
     std::vector<signed char> mapI(2 * NJ * NK, -1), mapJ(NI * 2 * NK, -1), mapK(NI * NJ * 2, -1);
     for (size_t m = 0; m < boundaries_.size(); m++) {
@@ -309,28 +252,27 @@ void Solver::buildBoundaryStructures() {
 
     // turbo performance, throttle and plenum (src/solver.cpp:1309-1321, 735-748)
     needTurbo_ = config_.saveTurboOutput();
-    c_.inlet_pt = 0.0;
+    proto_.inlet_pt = 0.0;
     for (const auto& b : boundaries_)
         if (b.type == kBcInlet) {
-            c_.inlet_pt = b.values[0];
+            proto_.inlet_pt = b.values[0];
             break;
         }
-    c_.throttle_kt = 0.0;
+    proto_.throttle_kt = 0.0;
     bool hasThrottle = false;
     for (const auto& b : boundaries_)
         if (b.type == kBcThrottle) {
             hasThrottle = true;
-            c_.throttle_kt = b.values.empty() ? 0.0 : b.values[0];
+            proto_.throttle_kt = b.values.empty() ? 0.0 : b.values[0];
         }
-    c_.greitzer = config_.enableGreitzerModeling() ? 1 : 0;
-    if (c_.greitzer && !hasThrottle) throw ConfigError("Greitzer modeling enabled but no throttle boundary condition found!");
-    if (c_.greitzer || hasThrottle) needTurbo_ = true;
-    if (c_.greitzer) {
-        profiles_ = true;
-        c_.plenum_volume = config_.getGreitzerPlenumVolume();
-        c_.ambient_p = config_.getGreitzerAmbientPressure();
+    proto_.greitzer = config_.enableGreitzerModeling() ? 1 : 0;
+    if (proto_.greitzer && !hasThrottle) throw ConfigError("Greitzer modeling enabled but no throttle boundary condition found!");
+    if (proto_.greitzer || hasThrottle) needTurbo_ = true;
+    if (proto_.greitzer) {
+        proto_.plenum_volume = config_.getGreitzerPlenumVolume();
+        proto_.ambient_p = config_.getGreitzerAmbientPressure();
     }
-    c_.need_turbo = needTurbo_ ? 1 : 0;
+    proto_.need_turbo = needTurbo_ ? 1 : 0;
     // TURBO_DIRECTION or the inlet orientation (src/solver.cpp:1654-1680)
     std::string dir = config_.has("TURBO_DIRECTION") ? config_.get("TURBO_DIRECTION") : "i";
     if (!config_.has("TURBO_DIRECTION"))
@@ -339,74 +281,147 @@ void Solver::buildBoundaryStructures() {
                 if (b.orientation == 2) { dir = "j"; break; }
                 if (b.orientation == 3) { dir = "-j"; break; }
             }
-    c_.turbo_dir = dir == "-i" ? 1 : ((dir == "j" || dir == "+j") ? 2 : (dir == "-j" ? 3 : 0));
+    proto_.turbo_dir = dir == "-i" ? 1 : ((dir == "j" || dir == "+j") ? 2 : (dir == "-j" ? 3 : 0));
 }
 
-void Solver::uploadBoundaryStructures() {
-    auto up8 = [&](const std::vector<signed char>& v) {
-        void* d = nullptr;
-        check(cudaMalloc(&d, v.size()), "cudaMalloc");
-        allocations_.push_back(d);
-        check(cudaMemcpy(d, v.data(), v.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
-        return static_cast<const signed char*>(d);
-    };
-    c_.mapI = up8(mapI_);
-    c_.mapJ = up8(mapJ_);
-    c_.mapK = up8(mapK_);
-    if (c_.nprofiles) {
-        c_.prof_p = alloc(profP_.size());
-        check(cudaMemcpy(c_.prof_p, profP_.data(), profP_.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
-        c_.prof_r = upload(profR_);
+// Parses every key the device set-up reads (the reference's getters throw on
+// the same inputs).
+void Solver::validateSettings() {
+    const TimeStepMethod m = config_.getTimeStepMethod();
+    config_.getCFL();
+    if (m == TimeStepMethod::Fixed) config_.getFixedTimeStep();
+    config_.getFluidGamma();
+    config_.getFluidGasConstant();
+    config_.getInitMachNumber();
+    config_.getInitTemperature();
+    config_.getInitPressure();
+    const std::string raw = config_.has("INIT_DIRECTION") ? config_.get("INIT_DIRECTION") : "";
+    if (raw != "adaptive") {
+        const auto items = config_.parseList("INIT_DIRECTION");
+        if (items.size() != 3) throw ConfigError("INIT_DIRECTION must have 3 components or be 'adaptive'");
+        for (const auto& it : items) {
+            try {
+                (void)std::stod(it);
+            } catch (const std::exception&) {
+                throw ConfigError("Invalid vector element for key \"INIT_DIRECTION\": \"" + it + "\"");
+            }
+        }
+    }
+    config_.getResidualsDropConvergence();
+    config_.isSimulationSteady();
+    config_.isInletCylindrical();
+    config_.getOutletPressureRampMaxIterations();
+    config_.getRotationalSpeedScalingFactor();
+    if (config_.isAccelerationActive()) {
+        config_.parseFloat("ACCELERATION_INITIAL_TIME");
+        config_.parseFloat("ACCELERATION_FINAL_TIME");
+        config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_INITIAL");
+        config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_FINAL");
+    }
+    if (config_.isPerturbationBodyForceActive()) {
+        if (config_.parseList("PERTURBATION_CENTER").size() < 3) throw ConfigError("PERTURBATION_CENTER needs 3 values");
+        config_.parseFloat("PERTURBATION_RADIAL_EXTENSION");
+        config_.parseFloat("PERTURBATION_SCALING_FACTOR");
+        config_.parseFloat("PERTURBATION_TIME_START");
+        config_.parseFloat("PERTURBATION_TIME_DURATION");
     }
 }
 
-void Solver::upload() {
+
+Solver::~Solver() {
+    if (ownStream_) cudaStreamSynchronize(ownStream_);
+    g32_.reset();
+    g64_.reset();
+    i32_.reset();
+    i64_.reset();
+    if (hostCtl_) cudaFreeHost(hostCtl_);
+    if (ownStream_) cudaStreamDestroy(ownStream_);
+}
+
+size_t Solver::deviceBytes() const { return i64_ ? i64_->deviceBytes() : i32_->deviceBytes(); }
+
+// Scalar settings of the device description (both precisions).
+void Solver::setupScalars() {
+    DevCaseT<double>& c = proto_;
     const long NI = mesh_.ni(), NJ = mesh_.nj(), NK = mesh_.nk(), N = mesh_.nodes();
-    c_.ni = static_cast<int>(NI);
-    c_.nj = static_cast<int>(NJ);
-    c_.nk = static_cast<int>(NK);
-    c_.n = N;
-    c_.topo = static_cast<int>(topo_);
-    advection_->configure(c_);
-    c_.nstages = static_cast<int>(coeffs_.size());
-    for (size_t s = 0; s < coeffs_.size(); s++) c_.coeffs[s] = coeffs_[s];
-    c_.dt_method = static_cast<int>(config_.getTimeStepMethod());
-    c_.steady = config_.isSimulationSteady() ? 1 : 0;
-    c_.drop = config_.getResidualsDropConvergence();
-    c_.gamma = config_.getFluidGamma();
-    c_.rgas = config_.getFluidGasConstant();
-    c_.cp = (c_.gamma * c_.rgas) / (c_.gamma - 1);
-    c_.cfl = config_.getCFL();
-    c_.fixed_dt = c_.dt_method == 2 ? config_.getFixedTimeStep() : 0.0;
-    c_.per_angle_deg = periodicAngleDeg_;
-    c_.per_cos_p = std::cos(periodicAngleRad_);
-    c_.per_sin_p = std::sin(periodicAngleRad_);
-    c_.per_cos_m = std::cos(-periodicAngleRad_);
-    c_.per_sin_m = std::sin(-periodicAngleRad_);
-    c_.wedge = mesh_.wedgeAngle();
-    c_.ramp_iters = config_.getOutletPressureRampMaxIterations();
-    c_.init_p = config_.getInitPressure();
-    c_.inlet_cyl = config_.isInletCylindrical() ? 1 : 0;
-    c_.bfm = config_.isBFMActive() ? 1 : 0;
-    bfm_->configure(c_);
-    c_.speed_scale = config_.getRotationalSpeedScalingFactor();
-    c_.accel = config_.isAccelerationActive() ? 1 : 0;
-    if (c_.accel) {
-        c_.acc_t0 = config_.parseFloat("ACCELERATION_INITIAL_TIME");
-        c_.acc_t1 = config_.parseFloat("ACCELERATION_FINAL_TIME");
-        c_.acc_s0 = config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_INITIAL");
-        c_.acc_s1 = config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_FINAL");
+    c.ni = static_cast<int>(NI);
+    c.nj = static_cast<int>(NJ);
+    c.nk = static_cast<int>(NK);
+    c.n = N;
+    c.topo = static_cast<int>(topo_);
+    advection_->configure(c);
+    c.nstages = static_cast<int>(coeffs_.size());
+    for (size_t s = 0; s < coeffs_.size(); s++) c.coeffs[s] = coeffs_[s];
+    c.dt_method = static_cast<int>(config_.getTimeStepMethod());
+    c.steady = config_.isSimulationSteady() ? 1 : 0;
+    c.drop = config_.getResidualsDropConvergence();
+    c.gamma = config_.getFluidGamma();
+    c.rgas = config_.getFluidGasConstant();
+    c.cp = (c.gamma * c.rgas) / (c.gamma - 1);
+    c.cfl = config_.getCFL();
+    c.fixed_dt = c.dt_method == 2 ? config_.getFixedTimeStep() : 0.0;
+    c.per_angle_deg = periodicAngleDeg_;
+    c.per_cos_p = std::cos(periodicAngleRad_);
+    c.per_sin_p = std::sin(periodicAngleRad_);
+    c.per_cos_m = std::cos(-periodicAngleRad_);
+    c.per_sin_m = std::sin(-periodicAngleRad_);
+    c.wedge = mesh_.wedgeAngle();
+    c.ramp_iters = config_.getOutletPressureRampMaxIterations();
+    c.init_p = config_.getInitPressure();
+    c.inlet_cyl = config_.isInletCylindrical() ? 1 : 0;
+    c.bfm = config_.isBFMActive() ? 1 : 0;
+    bfm_->configure(c);
+    c.speed_scale = config_.getRotationalSpeedScalingFactor();
+    c.accel = config_.isAccelerationActive() ? 1 : 0;
+    if (c.accel) {
+        c.acc_t0 = config_.parseFloat("ACCELERATION_INITIAL_TIME");
+        c.acc_t1 = config_.parseFloat("ACCELERATION_FINAL_TIME");
+        c.acc_s0 = config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_INITIAL");
+        c.acc_s1 = config_.parseFloat("ROTATIONAL_SPEED_SCALING_FACTOR_FINAL");
     }
-    if (c_.perturb) {
+    if (c.perturb) {
         const auto pc = config_.parseList("PERTURBATION_CENTER");
         if (pc.size() < 3) throw ConfigError("PERTURBATION_CENTER needs 3 values");
-        for (int q = 0; q < 3; q++) c_.pert_c[q] = std::stod(pc[q]);
-        c_.pert_r = config_.parseFloat("PERTURBATION_RADIAL_EXTENSION");
-        c_.pert_s = config_.parseFloat("PERTURBATION_SCALING_FACTOR");
-        c_.pert_t0 = config_.parseFloat("PERTURBATION_TIME_START");
-        c_.pert_dur = config_.parseFloat("PERTURBATION_TIME_DURATION");
+        for (int q = 0; q < 3; q++) c.pert_c[q] = std::stod(pc[q]);
+        c.pert_r = config_.parseFloat("PERTURBATION_RADIAL_EXTENSION");
+        c.pert_s = config_.parseFloat("PERTURBATION_SCALING_FACTOR");
+        c.pert_t0 = config_.parseFloat("PERTURBATION_TIME_START");
+        c.pert_dur = config_.parseFloat("PERTURBATION_TIME_DURATION");
     }
+    if (c.bfm && c.bfm_model == 3) {
+        if (c.le_idx < 0 || c.le_idx >= NI || c.te_idx < 0 || c.te_idx >= NI)
+            throw ConfigError("LEADING_EDGE_INDEX / TRAILING_EDGE_INDEX outside the grid");
+    }
+    c.compensated = prec_ == kFP32Kahan ? 1 : 0;
+    c.node_tiles = static_cast<int>((N + kTileSize - 1) / kTileSize);
+    c.per_tiles = c.periodic ? static_cast<int>((NI * NJ + kTileSize - 1) / kTileSize) : 0;
+    c.hist_cap = std::min<long long>(std::max<long long>(maxIter_, 1024), 1 << 20);
+}
 
+// Device arrays of the operating point in precision R.
+template <typename R>
+void Solver::uploadArrays(InstanceT<R>& inst) {
+    DevCaseT<R>& c = inst.c;
+    static_assert(sizeof(DevCaseT<R>) == sizeof(DevCaseT<double>), "same layout for both precisions");
+    std::memcpy(static_cast<void*>(&c), &proto_, sizeof(c));  // scalars; every pointer is set below
+    const long NI = mesh_.ni(), NJ = mesh_.nj(), NK = mesh_.nk(), N = mesh_.nodes();
+    // boundary tables and radial profiles
+    auto up8 = [&](const std::vector<signed char>& v) {
+        void* d = inst.allocBytes(v.size());
+        cudaCheck(cudaMemcpy(d, v.data(), v.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+        return static_cast<const signed char*>(d);
+    };
+    c.mapI = up8(mapI_);
+    c.mapJ = up8(mapJ_);
+    c.mapK = up8(mapK_);
+    c.prof_p = nullptr;
+    c.prof_r = nullptr;
+    if (c.nprofiles) {
+        c.prof_p = inst.allocD(profP_.size());
+        cudaCheck(cudaMemcpy(c.prof_p, profP_.data(), profP_.size() * sizeof(double), cudaMemcpyHostToDevice),
+                  "cudaMemcpy");
+        c.prof_r = inst.uploadD(profR_);
+    }
     // face metrics: unit normal n = S/|S| and |S| (computeAdvectionFluxFromPrimitive)
     for (int d = 0; d < 3; d++) {
         const auto& S = mesh_.surfaces(d);
@@ -418,11 +433,11 @@ void Solver::upload() {
             nz[f] = S[f].z / m;
             ar[f] = m;
         }
-        c_.f[d].nx = upload(nx);
-        c_.f[d].ny = upload(ny);
-        c_.f[d].nz = upload(nz);
-        c_.f[d].area = upload(ar);
-        for (int v = 0; v < 5; v++) c_.f[d].c[v] = alloc(S.size());
+        c.f[d].nx = inst.uploadR(nx);
+        c.f[d].ny = inst.uploadR(ny);
+        c.f[d].nz = inst.uploadR(nz);
+        c.f[d].area = inst.uploadR(ar);
+        for (int v = 0; v < 5; v++) c.f[d].c[v] = inst.allocR(S.size());
     }
     // per node: volume, radius, theta rotation, edges of the dual cell
     std::vector<double> cst(N), snt(N), rad(N), aK(N, 0.0);
@@ -451,12 +466,14 @@ void Solver::upload() {
                     edge[4 * d + 3][q] = ds;
                 }
             }
-    c_.vol = upload(mesh_.volumes());
-    c_.cost = upload(cst);
-    c_.sint = upload(snt);
-    c_.radius = upload(rad);
-    c_.areaK0 = upload(aK);
-    for (int e = 0; e < 12; e++) c_.edge[e] = upload(edge[e]);
+    c.vol = inst.uploadR(mesh_.volumes());
+    c.cost = inst.uploadR(cst);
+    c.sint = inst.uploadR(snt);
+    c.radius = inst.uploadR(rad);
+    c.areaK0 = inst.uploadR(aK);
+    c.cost64 = inst.uploadD(cst);
+    c.sint64 = inst.uploadD(snt);
+    for (int e = 0; e < 12; e++) c.edge[e] = inst.uploadR(edge[e]);
     {
         std::vector<double> vx(N), vy(N), vz(N);
         for (long q = 0; q < N; q++) {
@@ -464,9 +481,9 @@ void Solver::upload() {
             vy[q] = mesh_.vertices()[q].y;
             vz[q] = mesh_.vertices()[q].z;
         }
-        c_.vx = upload(vx);
-        c_.vy = upload(vy);
-        c_.vz = upload(vz);
+        c.vx = inst.uploadD(vx);
+        c.vy = inst.uploadD(vy);
+        c.vz = inst.uploadD(vz);
     }
     // boundary planes (raw surface vectors) for the surface integrals
     for (int b = 0; b < 6; b++) {
@@ -487,17 +504,19 @@ void Solver::upload() {
                 sy.push_back(S[f].y);
                 sz.push_back(S[f].z);
             }
-        c_.bsx[b] = upload(sx);
-        c_.bsy[b] = upload(sy);
-        c_.bsz[b] = upload(sz);
+        c.bsx[b] = inst.uploadD(sx);
+        c.bsy[b] = inst.uploadD(sy);
+        c.bsz[b] = inst.uploadD(sz);
     }
     // BFM fields (include/types.hpp:1036-1078 names)
-    if (c_.bfm) {
-        auto need = [&](const char* name) { return upload(mesh_.field(name)); };
-        auto opt = [&](const char* name) -> const double* {
-            return mesh_.hasField(name) ? upload(mesh_.field(name)) : nullptr;
+    c.blk = c.gbx = c.gby = c.gbz = c.nax = c.nrad = c.ntan = c.rpm = c.stwl = c.bpresent = c.nblades = nullptr;
+    c.cosmetal = c.devpivot = c.devstall = c.ldbeta0 = c.ldkp = nullptr;
+    if (c.bfm) {
+        auto need = [&](const char* name) { return inst.uploadR(mesh_.field(name)); };
+        auto opt = [&](const char* name) -> const R* {
+            return mesh_.hasField(name) ? inst.uploadR(mesh_.field(name)) : nullptr;
         };
-        c_.blk = need("blockage");
+        c.blk = need("blockage");
         const auto& gb = mesh_.blockageGradient();
         std::vector<double> gx(N), gy(N), gz(N);
         for (long q = 0; q < N; q++) {
@@ -505,63 +524,58 @@ void Solver::upload() {
             gy[q] = gb[q].y;
             gz[q] = gb[q].z;
         }
-        c_.gbx = upload(gx);
-        c_.gby = upload(gy);
-        c_.gbz = upload(gz);
-        c_.bpresent = need("bladePresent");
-        c_.nblades = need("numberBlades");
-        if (c_.bfm_model != 0 && c_.bfm_model != 4) {
+        c.gbx = inst.uploadR(gx);
+        c.gby = inst.uploadR(gy);
+        c.gbz = inst.uploadR(gz);
+        c.bpresent = need("bladePresent");
+        c.nblades = need("numberBlades");
+        if (c.bfm_model != 0 && c.bfm_model != 4) {
             // SourceBFMBase::computeFlowState reads all of these (src/source_bfm_base.cpp:104-149)
-            c_.nax = need("normalAxial");
-            c_.nrad = need("normalRadial");
-            c_.ntan = need("normalTangential");
-            c_.rpm = need("rpm");
-            need("bladeLeanAngle");
-            need("bladeGasPathAngle");
+            c.nax = need("normalAxial");
+            c.nrad = need("normalRadial");
+            c.ntan = need("normalTangential");
+            c.rpm = need("rpm");
+            mesh_.field("bladeLeanAngle");
+            mesh_.field("bladeGasPathAngle");
             const auto& metal = mesh_.field("bladeMetalAngle");
             std::vector<double> cm(N);
             for (long q = 0; q < N; q++) cm[q] = std::cos(metal[q]);
-            c_.cosmetal = upload(cm);
+            c.cosmetal = inst.uploadR(cm);
         } else {
-            c_.rpm = opt("rpm");
+            c.rpm = opt("rpm");
         }
-        if (c_.bfm_model == 2 || c_.bfm_model == 3) c_.stwl = need("streamwiseLength");
-        if (c_.bfm_model == 2 && c_.offdesign) c_.devpivot = need("deviationAnglePivot");
-        if (c_.stalled) c_.devstall = need("deviationAngleStall");
-        if (c_.bfm_model == 3) {
-            c_.ldbeta0 = need("liftDragBeta0");
-            c_.ldkp = need("liftDragKpEtamax");
-            if (c_.le_idx < 0 || c_.le_idx >= NI || c_.te_idx < 0 || c_.te_idx >= NI)
-                throw ConfigError("LEADING_EDGE_INDEX / TRAILING_EDGE_INDEX outside the grid");
+        if (c.bfm_model == 2 || c.bfm_model == 3) c.stwl = need("streamwiseLength");
+        if (c.bfm_model == 2 && c.offdesign) c.devpivot = need("deviationAnglePivot");
+        if (c.stalled) c.devstall = need("deviationAngleStall");
+        if (c.bfm_model == 3) {
+            c.ldbeta0 = need("liftDragBeta0");
+            c.ldkp = need("liftDragKpEtamax");
         }
-        if (topo_ == Topology::ThreeD && !c_.rpm) c_.rpm = need("rpm");
+        if (topo_ == Topology::ThreeD && !c.rpm) c.rpm = need("rpm");
     }
     // state, stage buffers, reductions, control block, history
     for (int v = 0; v < 5; v++) {
-        c_.U[v] = alloc(N);
-        c_.S1[v] = alloc(N);
-        c_.S2[v] = alloc(N);
-        c_.Rp[v] = alloc(2 * NI * NJ);
-        c_.W[v] = alloc(N);
+        c.U[v] = inst.allocR(N);
+        c.Uc[v] = c.compensated ? inst.allocR(N) : nullptr;
+        c.S1[v] = inst.allocR(N);
+        c.S2[v] = inst.allocR(N);
+        c.Rp[v] = inst.allocR(2 * NI * NJ);
+        c.W[v] = inst.allocR(N);
     }
-    c_.dt = alloc(N);
-    c_.node_blocks = nodeBlocks(N);
-    c_.per_blocks = periodicBlocks(NI * NJ);
-    c_.dt_blocks = c_.node_blocks;
-    c_.partial = alloc(static_cast<size_t>(c_.node_blocks + c_.per_blocks) * 5 + c_.dt_blocks);
-    void* ctl = nullptr;
-    check(cudaMalloc(&ctl, sizeof(Control)), "cudaMalloc");
-    allocations_.push_back(ctl);
-    c_.ctl = static_cast<Control*>(ctl);
-    c_.hist_cap = std::min<long long>(std::max<long long>(maxIter_, 1024), 1 << 20);
-    c_.hist = alloc(static_cast<size_t>(c_.hist_cap) * kHistWidth);
+    c.dt = inst.allocR(N);
+    c.partial = inst.allocD(static_cast<size_t>(c.node_tiles + c.per_tiles) * 5 + c.node_tiles);
+    c.ctl = static_cast<Control*>(inst.allocBytes(sizeof(Control)));
+    c.hist = inst.allocD(static_cast<size_t>(c.hist_cap) * kHistWidth);
 }
 
-// FluidIdeal::computeInitFields (src/fluid_ideal.cpp:155-170) and
-// Solver::initializeSolutionFromScratch (src/solver.cpp:777-836).
-void Solver::initializeSolution() {
+// FluidIdeal::computeInitFields (src/fluid_ideal.cpp:155-170),
+// Solver::initializeSolutionFromScratch (src/solver.cpp:777-836), and the
+// Greitzer initial state and initial radial profiles of
+// Solver::initializeSolutionArrays (src/solver.cpp:750-776).
+template <typename R>
+void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
     const double M = config_.getInitMachNumber(), T = config_.getInitTemperature(), p = config_.getInitPressure();
-    const double g = c_.gamma, R = c_.rgas;
+    const double g = proto_.gamma, Rg = proto_.rgas;
     const std::string raw = config_.has("INIT_DIRECTION") ? config_.get("INIT_DIRECTION") : "";
     bool adaptive = raw == "adaptive";
     Vec3 d0;
@@ -585,9 +599,9 @@ void Solver::initializeSolution() {
                     const double m = dv.magnitude();
                     dir = (m == 0) ? Vec3(0, 0, 0) : dv / m;
                 }
-                const double a = std::sqrt(g * R * T);
+                const double a = std::sqrt(g * Rg * T);
                 const Vec3 u = (dir / dir.magnitude()) * a * M;
-                const double rho = p / (R * T);
+                const double rho = p / (Rg * T);
                 const double e = p / ((g - 1) * rho);
                 const double um = u.magnitude();
                 const double et = e + 0.5 * (um * um);
@@ -598,33 +612,22 @@ void Solver::initializeSolution() {
                 U[3][q] = rho * u.z;
                 U[4][q] = rho * et;
             }
-    for (int v = 0; v < 5; v++)
-        check(cudaMemcpy(c_.U[v], U[v].data(), N * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
     std::memset(hostCtl_, 0, sizeof(Control));
-    check(cudaMemcpy(c_.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
-}
-
-// Greitzer initial state and initial radial profiles
-// (Solver::initializeSolutionArrays, src/solver.cpp:750-776).
-void Solver::initializeProfilesAndPlenum() {
-    const long N = mesh_.nodes();
-    std::array<std::vector<double>, 5> U;
-    for (int v = 0; v < 5; v++) {
-        U[v].resize(N);
-        check(cudaMemcpy(U[v].data(), c_.U[v], N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
-    }
-    const HostGas gas{c_.gamma, c_.rgas};
+    cudaCheck(cudaMemcpy(inst.c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
+    const double* in[5] = {U[0].data(), U[1].data(), U[2].data(), U[3].data(), U[4].data()};
+    setState(in);
+    const HostGas gas{g, Rg};
     auto prim = [&](long q, double& rho, Vec3& u, double& et) {
         rho = U[0][q];
         u = Vec3(U[1][q] / U[0][q], U[2][q] / U[0][q], U[3][q] / U[0][q]);
         et = U[4][q] / U[0][q];
     };
-    if (c_.greitzer) {
+    if (proto_.greitzer) {
         double mf[6], tp[4];
         getTurbo(mf, tp);
         double rho, et;
         Vec3 u;
-        prim(mesh_.idx(mesh_.ni() - 1, 0, 0), rho, u, et);
+        prim(mesh_.idx(NI - 1, 0, 0), rho, u, et);
         Control ctl = control();
         ctl.gz_p = gas.pressure(rho, u, et);
         ctl.gz_T = gas.temperature(rho, u, et);
@@ -633,93 +636,43 @@ void Solver::initializeProfilesAndPlenum() {
         ctl.gz_t = 0.0;
         ctl.has_turbo = 0;
         *hostCtl_ = ctl;
-        check(cudaMemcpy(c_.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
+        cudaCheck(cudaMemcpy(inst.c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
     }
-    if (c_.nprofiles) {
-        std::vector<double> profP(c_.prof_off[c_.nprofiles - 1] + c_.prof_n[c_.nprofiles - 1]);
-        for (int m = 0; m < c_.nprofiles; m++)
-            for (int jj = 0; jj < c_.prof_n[m]; jj++) {
+    if (proto_.nprofiles) {
+        std::vector<double> profP(profP_.size());
+        for (int m = 0; m < proto_.nprofiles; m++)
+            for (int jj = 0; jj < proto_.prof_n[m]; jj++) {
                 double rho, et;
                 Vec3 u;
-                prim(mesh_.idx(c_.prof_i[m], c_.prof_j0[m] + jj, 0), rho, u, et);
-                profP[c_.prof_off[m] + jj] = gas.pressure(rho, u, et);
+                prim(mesh_.idx(proto_.prof_i[m], proto_.prof_j0[m] + jj, 0), rho, u, et);
+                profP[proto_.prof_off[m] + jj] = gas.pressure(rho, u, et);
             }
-        check(cudaMemcpy(c_.prof_p, profP.data(), profP.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+        cudaCheck(cudaMemcpy(inst.c.prof_p, profP.data(), profP.size() * sizeof(double), cudaMemcpyHostToDevice),
+                  "cudaMemcpy");
     }
+    (void)grp;
 }
 
-void Solver::setLimits(long long itStop, long long histBase) {
-    check(launchSetLimits(c_, itStop, histBase, stream_), "launch set-limits");
-}
-
-// One iteration of the explicit branch of Solver::solve (src/solver.cpp:1337-1398).
-void Solver::enqueueIteration() {
-    const P5 U{{c_.U[0], c_.U[1], c_.U[2], c_.U[3], c_.U[4]}};
-    const P5 A{{c_.S1[0], c_.S1[1], c_.S1[2], c_.S1[3], c_.S1[4]}};
-    const P5 B{{c_.S2[0], c_.S2[1], c_.S2[2], c_.S2[3], c_.S2[4]}};
-    if (needTurbo_) check(launchBoundaryIntegrals(c_, U, true, stream_), "launch k_bint");
-    check(launchTimeStep(c_, U, stream_), "launch k_dt");
-    check(launchPre(c_, U, needTurbo_, profiles_, true, stream_), "launch k_pre");
-    const int ns = static_cast<int>(coeffs_.size());
-    // stage buffers: RK4 U->A->B->A->U, RK3 U->A->B->U (the last stage updates U^n in place)
-    const P5 in4[4] = {U, A, B, A}, out4[4] = {A, B, A, U};
-    const P5 in3[3] = {U, A, B}, out3[3] = {A, B, U};
-    for (int s = 0; s < ns; s++) {
-        const P5& in = ns == 4 ? in4[s] : in3[s];
-        const P5& out = ns == 4 ? out4[s] : out3[s];
-        check(launchStage(c_, in, out, coeffs_[s], s == ns - 1, 0, B, stream_), "launch stage");
-    }
-    check(launchFinalize(c_, stream_), "launch k_finalize");
-}
-
-void Solver::captureGraph() {
-    if (graph_) return;
-    graphIters_ = 8;
-    cudaGraph_t g = nullptr;
-    check(cudaStreamBeginCapture(ownStream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-    cudaStream_t saved = stream_;
-    stream_ = ownStream_;
-    try {
-        for (int i = 0; i < graphIters_; i++) enqueueIteration();
-    } catch (...) {
-        stream_ = saved;
-        cudaStreamEndCapture(ownStream_, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-    }
-    stream_ = saved;
-    check(cudaStreamEndCapture(ownStream_, &g), "cudaStreamEndCapture");
-    const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
-    cudaGraphDestroy(g);
-    check(e, "cudaGraphInstantiate");
-}
+// ------------------------------------------------------------------ running
 
 void Solver::enqueue(long long n) {
-    if (n <= 0) return;
-    setLimits(itHost_ + n, itHost_);
-    captureGraph();
-    long long left = n;
-    while (left >= graphIters_) {
-        check(cudaGraphLaunch(graph_, stream_), "cudaGraphLaunch");
-        left -= graphIters_;
-    }
-    for (long long i = 0; i < left; i++) enqueueIteration();
-    itHost_ += n;
+    visit([&](auto& inst, auto& grp) { grp.enqueue(n, stream_); (void)inst; });
 }
 
 Control Solver::control() {
-    check(cudaMemcpyAsync(hostCtl_, c_.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream_), "cudaMemcpyAsync");
-    check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    visit([&](auto& inst, auto&) {
+        cudaCheck(cudaMemcpyAsync(hostCtl_, inst.c.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream_),
+                  "cudaMemcpyAsync");
+    });
+    cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
     return *hostCtl_;
 }
 
 long long Solver::step(long long n) {
     const Control before = control();
     if (before.status != 0) return 0;
-    itHost_ = before.it;
     enqueue(n);
     const Control after = control();
-    itHost_ = after.it;
     return after.it - before.it;
 }
 
@@ -729,33 +682,48 @@ long long Solver::solve() {
     while (true) {
         const Control c = control();
         if (c.status != 0 || c.it >= maxIter_) break;
-        const long long n = std::min<long long>(chunk, maxIter_ - c.it);
-        done += step(n);
+        done += step(std::min<long long>(chunk, maxIter_ - c.it));
     }
     return done;
 }
 
-void Solver::computeResidual(double* dt, double* const r[5]) {
-    const Control c0 = control();
-    itHost_ = c0.it;
-    DevCase fc = c_;
-    fc.force = 1;  // run even after convergence
-    const P5 U{{c_.U[0], c_.U[1], c_.U[2], c_.U[3], c_.U[4]}};
-    const P5 A{{c_.S1[0], c_.S1[1], c_.S1[2], c_.S1[3], c_.S1[4]}};
-    const P5 B{{c_.S2[0], c_.S2[1], c_.S2[2], c_.S2[3], c_.S2[4]}};
-    if (needTurbo_) check(launchBoundaryIntegrals(fc, U, true, stream_), "launch k_bint");
-    check(launchTimeStep(fc, U, stream_), "launch k_dt");
-    check(launchPre(fc, U, needTurbo_, profiles_, true, stream_), "launch k_pre");
-    check(launchStage(fc, U, A, 0.0, false, 1, B, stream_), "launch stage");
-    const Control c1 = control();
-    const long N = mesh_.nodes();
-    if (c_.dt_method == 0) {
-        check(cudaMemcpy(dt, c_.dt, N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
-    } else {
-        std::fill(dt, dt + N, c_.dt_method == 2 ? c_.fixed_dt : c1.dt_min);
+namespace {
+
+// One time-step + residual evaluation of U^n with the next iteration's number
+// (boundary integrals, time step, profiles, stage -1 into S2).
+template <typename R>
+void residualSequence(const BatchView<R>& v, cudaStream_t s) {
+    cudaCheck(Launcher<R>::boundaryIntegrals(v, false, 1, s), "launch k_bint");
+    cudaCheck(Launcher<R>::timeStep(v, 1, s), "launch k_dt");
+    cudaCheck(Launcher<R>::pre(v, false, true, true, 1, s), "launch k_pre");
+    cudaCheck(Launcher<R>::stage(v, -1, 1, s), "launch stage");
+}
+
+// Device array of R -> host doubles, without any allocation: a float array is
+// copied into the first half of the output buffer and widened in place from
+// the back (double q occupies bytes [8q, 8q+8), the floats still to be read
+// lie below byte 4q).
+template <typename R>
+void copyOut(const R* d, double* h, size_t n, cudaStream_t s) {
+    cudaCheck(cudaMemcpyAsync(h, d, n * sizeof(R), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    cudaCheck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (sizeof(R) != sizeof(double)) {
+        const R* f = reinterpret_cast<const R*>(h);
+        for (size_t q = n; q-- > 0;) h[q] = static_cast<double>(f[q]);
     }
-    for (int v = 0; v < 5; v++)
-        check(cudaMemcpy(r[v], c_.S2[v], N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+}
+
+}  // namespace
+
+void Solver::computeResidual(double* dt, double* const r[5]) {
+    const long N = mesh_.nodes();
+    visit([&](auto& inst, auto& grp) {
+        residualSequence(grp.view(), stream_);
+        const Control c1 = control();
+        if (inst.c.dt_method == 0) copyOut(inst.c.dt, dt, N, stream_);
+        else std::fill(dt, dt + N, inst.c.dt_method == 2 ? inst.c.fixed_dt : c1.dt_min);
+        for (int v = 0; v < 5; v++) copyOut(inst.c.S2[v], r[v], N, stream_);
+    });
 }
 
 // The residual evaluation of computeResidual with its per-face flux
@@ -764,65 +732,95 @@ void Solver::computeResidual(double* dt, double* const r[5]) {
 void Solver::computeResidualNoAlloc(double* dt, double* const r[5]) {
     double* scratch = nullptr;
     size_t bytes = 0;
-    check(noallocScratch(&scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
-    const int dirs = c_.topo == 1 ? 3 : 2;
-    size_t faces = 0;
-    for (int d = 0; d < dirs; d++) faces += static_cast<size_t>(mesh_.faceCount(d));
-    if (faces * 5 * sizeof(double) > bytes)
-        throw ConfigError("ctbfm_compute_residual_noalloc: the case has " + std::to_string(faces) +
-                          " faces and needs " + std::to_string(faces * 5 * sizeof(double)) +
-                          " bytes of face scratch; the static array holds " + std::to_string(bytes) +
-                          " bytes (at most " + std::to_string(bytes / (5 * sizeof(double))) + " faces)");
-    const Control c0 = control();
-    itHost_ = c0.it;
-    DevCase fc = c_;
-    fc.force = 1;  // run even after convergence
-    size_t off = 0;
-    for (int d = 0; d < dirs; d++) {
-        const size_t nf = static_cast<size_t>(mesh_.faceCount(d));
-        for (int v = 0; v < 5; v++) fc.f[d].c[v] = scratch + off + v * nf;
-        off += 5 * nf;
-    }
-    const P5 U{{c_.U[0], c_.U[1], c_.U[2], c_.U[3], c_.U[4]}};
-    const P5 A{{c_.S1[0], c_.S1[1], c_.S1[2], c_.S1[3], c_.S1[4]}};
-    const P5 B{{c_.S2[0], c_.S2[1], c_.S2[2], c_.S2[3], c_.S2[4]}};
-    if (needTurbo_) check(launchBoundaryIntegrals(fc, U, true, stream_), "launch k_bint");
-    check(launchTimeStep(fc, U, stream_), "launch k_dt");
-    check(launchPre(fc, U, needTurbo_, profiles_, true, stream_), "launch k_pre");
-    check(launchStage(fc, U, A, 0.0, false, 1, B, stream_), "launch stage");
-    const Control c1 = control();
+    cudaCheck(noallocScratch(&scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
     const long N = mesh_.nodes();
-    if (c_.dt_method == 0) {
-        check(cudaMemcpy(dt, c_.dt, N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
-    } else {
-        std::fill(dt, dt + N, c_.dt_method == 2 ? c_.fixed_dt : c1.dt_min);
-    }
-    for (int v = 0; v < 5; v++)
-        check(cudaMemcpy(r[v], c_.S2[v], N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    visit([&](auto& inst, auto& grp) {
+        using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+        const int dirs = inst.c.topo == 1 ? 3 : 2;
+        size_t faces = 0;
+        for (int d = 0; d < dirs; d++) faces += static_cast<size_t>(mesh_.faceCount(d));
+        if (faces * 5 * sizeof(R) > bytes)
+            throw ConfigError("ctbfm_compute_residual_noalloc: the case has " + std::to_string(faces) +
+                              " faces and needs " + std::to_string(faces * 5 * sizeof(R)) +
+                              " bytes of face scratch; the static array holds " + std::to_string(bytes) +
+                              " bytes (at most " + std::to_string(bytes / (5 * sizeof(R))) + " faces)");
+        const DevFacesT<R> saved[3] = {inst.c.f[0], inst.c.f[1], inst.c.f[2]};
+        R* base = reinterpret_cast<R*>(scratch);
+        size_t off = 0;
+        for (int d = 0; d < dirs; d++) {
+            const size_t nf = static_cast<size_t>(mesh_.faceCount(d));
+            for (int v = 0; v < 5; v++) inst.c.f[d].c[v] = base + off + v * nf;
+            off += 5 * nf;
+        }
+        grp.refresh(stream_);
+        residualSequence(grp.view(), stream_);
+        for (int d = 0; d < 3; d++) inst.c.f[d] = saved[d];
+        grp.refresh(stream_);
+        const Control c1 = control();
+        if (inst.c.dt_method == 0) copyOut(inst.c.dt, dt, N, stream_);
+        else std::fill(dt, dt + N, inst.c.dt_method == 2 ? inst.c.fixed_dt : c1.dt_min);
+        for (int v = 0; v < 5; v++) copyOut(inst.c.S2[v], r[v], N, stream_);
+    });
 }
 
-// Copies run on the solver's stream (asynchronous when the host buffers are
-// pinned) and are complete when the call returns.
+// The state as double (float path: U - Uc); copies run on the solver's stream
+// (asynchronous when the host buffers are pinned) and complete on return.
 void Solver::getState(double* const out[5]) {
-    for (int v = 0; v < 5; v++)
-        check(cudaMemcpyAsync(out[v], c_.U[v], mesh_.nodes() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
-              "cudaMemcpyAsync");
-    check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    const long N = mesh_.nodes();
+    visit([&](auto& inst, auto&) {
+        using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+        if (sizeof(R) == sizeof(double)) {
+            for (int v = 0; v < 5; v++)
+                cudaCheck(cudaMemcpyAsync(out[v], inst.c.U[v], N * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+                          "cudaMemcpyAsync");
+            cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+        } else {
+            std::vector<R> u(N), cc(N);
+            for (int v = 0; v < 5; v++) {
+                cudaCheck(cudaMemcpyAsync(u.data(), inst.c.U[v], N * sizeof(R), cudaMemcpyDeviceToHost, stream_),
+                          "cudaMemcpyAsync");
+                cudaCheck(cudaMemcpyAsync(cc.data(), inst.c.Uc[v], N * sizeof(R), cudaMemcpyDeviceToHost, stream_),
+                          "cudaMemcpyAsync");
+                cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+                for (long q = 0; q < N; q++) out[v][q] = static_cast<double>(u[q]) - static_cast<double>(cc[q]);
+            }
+        }
+    });
 }
 
 void Solver::setState(const double* const in[5]) {
-    for (int v = 0; v < 5; v++)
-        check(cudaMemcpyAsync(c_.U[v], in[v], mesh_.nodes() * sizeof(double), cudaMemcpyHostToDevice, stream_),
-              "cudaMemcpyAsync");
-    check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    const long N = mesh_.nodes();
+    visit([&](auto& inst, auto&) {
+        using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+        if (sizeof(R) == sizeof(double)) {
+            for (int v = 0; v < 5; v++)
+                cudaCheck(cudaMemcpyAsync(inst.c.U[v], in[v], N * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                          "cudaMemcpyAsync");
+            cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+        } else {
+            // U = float(x), Uc = U - x, so that U - Uc carries x beyond float precision
+            std::vector<R> u(N), cc(N);
+            for (int v = 0; v < 5; v++) {
+                for (long q = 0; q < N; q++) {
+                    u[q] = static_cast<R>(in[v][q]);
+                    cc[q] = static_cast<R>(static_cast<double>(u[q]) - in[v][q]);
+                }
+                cudaCheck(cudaMemcpyAsync(inst.c.U[v], u.data(), N * sizeof(R), cudaMemcpyHostToDevice, stream_),
+                          "cudaMemcpyAsync");
+                cudaCheck(cudaMemcpyAsync(inst.c.Uc[v], cc.data(), N * sizeof(R), cudaMemcpyHostToDevice, stream_),
+                          "cudaMemcpyAsync");
+                cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+            }
+        }
+    });
 }
 
 void Solver::getTurbo(double massflow[6], double turbo[4]) {
-    DevCase fc = c_;
-    fc.force = 1;
-    const P5 U{{c_.U[0], c_.U[1], c_.U[2], c_.U[3], c_.U[4]}};
-    check(launchBoundaryIntegrals(fc, U, true, stream_), "launch k_bint");
-    check(launchPre(fc, U, true, false, false, stream_), "launch k_pre");
+    visit([&](auto& inst, auto& grp) {
+        using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+        cudaCheck(Launcher<R>::boundaryIntegrals(grp.view(), true, 1, stream_), "launch k_bint");
+        cudaCheck(Launcher<R>::pre(grp.view(), true, false, false, 1, stream_), "launch k_pre");
+    });
     const Control c = control();
     for (int b = 0; b < 6; b++) massflow[b] = c.massflow[b];
     for (int b = 0; b < 4; b++) turbo[b] = c.turbo[b];
@@ -832,52 +830,56 @@ void Solver::profileKernels(int reps, double* outMs) {
     for (int k = 0; k < kKernelKinds; k++) outMs[k] = 0.0;
     if (reps <= 0) return;
     const Control saved = control();
-    const long N = mesh_.nodes();
-    std::vector<double> dtSaved(N);
-    check(cudaMemcpy(dtSaved.data(), c_.dt, N * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
-    DevCase fc = c_;
-    fc.force = 1;
-    const P5 U{{c_.U[0], c_.U[1], c_.U[2], c_.U[3], c_.U[4]}};
-    const P5 A{{c_.S1[0], c_.S1[1], c_.S1[2], c_.S1[3], c_.S1[4]}};
-    const P5 B{{c_.S2[0], c_.S2[1], c_.S2[2], c_.S2[3], c_.S2[4]}};
-    cudaEvent_t e0, e1;
-    check(cudaEventCreate(&e0), "cudaEventCreate");
-    check(cudaEventCreate(&e1), "cudaEventCreate");
-    auto timeIt = [&](int kind, auto&& launch) {
-        launch();  // warm
-        check(cudaEventRecord(e0, stream_), "cudaEventRecord");
-        for (int r = 0; r < reps; r++) launch();
-        check(cudaEventRecord(e1, stream_), "cudaEventRecord");
-        check(cudaEventSynchronize(e1), "cudaEventSynchronize");
-        float ms = 0.f;
-        check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-        outMs[kind] = static_cast<double>(ms) / reps;
-    };
-    if (needTurbo_) timeIt(0, [&] { check(launchBoundaryIntegrals(fc, U, true, stream_), "k_bint"); });
-    if (c_.dt_method != 2) timeIt(1, [&] { check(launchTimeStep(fc, U, stream_), "k_dt"); });
-    timeIt(2, [&] { check(launchPre(fc, U, needTurbo_, false, true, stream_), "k_pre"); });
-    const int dirs = c_.topo == 1 ? 3 : 2;
-    for (int d = 0; d < dirs; d++) timeIt(3 + d, [&] { check(launchFaces(fc, d, U, stream_), "k_faces"); });
-    timeIt(6, [&] { check(launchNodes(fc, U, A, coeffs_.back(), true, 0, B, stream_), "k_nodes"); });
-    if (c_.periodic) timeIt(7, [&] { check(launchPeriodic(fc, A, coeffs_.back(), true, 0, B, stream_), "k_periodic"); });
-    timeIt(8, [&] { check(launchFinalize(fc, stream_), "k_finalize"); });
-    timeIt(9, [&] { check(launchPrim(fc, U, stream_), "k_prim"); });
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    check(cudaMemcpy(c_.dt, dtSaved.data(), N * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
-    *hostCtl_ = saved;
-    check(cudaMemcpy(c_.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
+    visit([&](auto& inst, auto& grp) {
+        using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+        using L = Launcher<R>;
+        const BatchView<R>& v = grp.view();
+        const long N = mesh_.nodes();
+        std::vector<R> dtSaved(N);
+        cudaCheck(cudaMemcpy(dtSaved.data(), inst.c.dt, N * sizeof(R), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        cudaEvent_t e0, e1;
+        cudaCheck(cudaEventCreate(&e0), "cudaEventCreate");
+        cudaCheck(cudaEventCreate(&e1), "cudaEventCreate");
+        auto timeIt = [&](int kind, auto&& launch) {
+            launch();  // warm
+            cudaCheck(cudaEventRecord(e0, stream_), "cudaEventRecord");
+            for (int r = 0; r < reps; r++) launch();
+            cudaCheck(cudaEventRecord(e1, stream_), "cudaEventRecord");
+            cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            outMs[kind] = static_cast<double>(ms) / reps;
+        };
+        const int lastStage = inst.c.nstages - 1;
+        // stage 0 reads U^n and writes S1, leaving U^n untouched
+        if (inst.c.need_turbo) timeIt(0, [&] { cudaCheck(L::boundaryIntegrals(v, false, 1, stream_), "k_bint"); });
+        if (inst.c.dt_method != 2) timeIt(1, [&] { cudaCheck(L::timeStep(v, 1, stream_), "k_dt"); });
+        timeIt(2, [&] { cudaCheck(L::pre(v, false, true, false, 1, stream_), "k_pre"); });
+        const int dirs = inst.c.topo == 1 ? 3 : 2;
+        for (int d = 0; d < dirs; d++) timeIt(3 + d, [&] { cudaCheck(L::faces(v, d, 0, 1, stream_), "k_faces"); });
+        timeIt(6, [&] { cudaCheck(L::nodes(v, 0, 1, stream_), "k_nodes"); });
+        if (inst.c.periodic) timeIt(7, [&] { cudaCheck(L::periodic(v, 0, 1, stream_), "k_periodic"); });
+        timeIt(8, [&] { cudaCheck(L::finalize(v, 1, stream_), "k_finalize"); });
+        timeIt(9, [&] { cudaCheck(L::prim(v, 0, 1, stream_), "k_prim"); });
+        (void)lastStage;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaCheck(cudaMemcpy(inst.c.dt, dtSaved.data(), N * sizeof(R), cudaMemcpyHostToDevice), "cudaMemcpy");
+        *hostCtl_ = saved;
+        cudaCheck(cudaMemcpy(inst.c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
+    });
 }
 
 long long Solver::history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub) {
     const Control c = control();
-    long long rows = std::min<long long>(c.it - c.hist_base, c_.hist_cap);
+    const long long cap = proto_.hist_cap;
+    long long rows = std::min<long long>(c.it - c.hist_base, cap);
     if (rows < 0) rows = 0;
     if (!lognorm && !massflow && !turbo && !hub) return rows;
     rows = std::min(rows, maxRows);
     std::vector<double> h(static_cast<size_t>(rows) * kHistWidth);
-    if (rows)
-        check(cudaMemcpy(h.data(), c_.hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    const double* dh = i64_ ? i64_->c.hist : i32_->c.hist;
+    if (rows) cudaCheck(cudaMemcpy(h.data(), dh, h.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
     for (long long r = 0; r < rows; r++) {
         const double* row = h.data() + r * kHistWidth;
         if (lognorm) std::copy(row, row + 5, lognorm + 5 * r);
@@ -887,5 +889,10 @@ long long Solver::history(long long maxRows, double* lognorm, double* massflow, 
     }
     return rows;
 }
+
+template void Solver::uploadArrays<double>(InstanceT<double>&);
+template void Solver::uploadArrays<float>(InstanceT<float>&);
+template void Solver::initializeState<double>(InstanceT<double>&, GroupT<double>&);
+template void Solver::initializeState<float>(InstanceT<float>&, GroupT<float>&);
 
 }  // namespace ctbfm

@@ -1,9 +1,11 @@
 // Solver: the B200 counterpart of the reference's Solver(Config&, Mesh&) +
 // solve() (include/solver.hpp:45-388) for the explicit Runge-Kutta path. It
-// owns every device buffer of one operating point and runs the whole
-// iteration (time step, boundary profiles, stages, norms, convergence) as a
-// device-side sequence, captured in CUDA graphs, with no host round trip
-// inside a chunk of iterations.
+// validates the inputs exactly as the reference does, then owns the operating
+// point's device data (InstanceT) in the working precision chosen by the
+// GPU_PRECISION key (fp64, the default, or fp32_kahan), and runs whole
+// iterations (time step, boundary profiles, stages, norms, convergence) as a
+// device-side sequence captured in CUDA graphs, with no host round trip inside
+// a chunk of iterations.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,6 +18,7 @@
 #include "../device/case.cuh"
 #include "../device/kernels.hpp"
 #include "config.hpp"
+#include "engine.hpp"
 #include "mesh.hpp"
 #include "models.hpp"
 
@@ -30,10 +33,7 @@ struct BoundaryPatch {
     std::unique_ptr<BoundaryBase> flux;
 };
 
-class CudaError : public std::runtime_error {
-public:
-    using std::runtime_error::runtime_error;
-};
+enum Precision { kFP64 = 0, kFP32Kahan = 1 };
 
 class Solver {
 public:
@@ -44,6 +44,7 @@ public:
 
     void setStream(cudaStream_t s) { stream_ = s ? s : ownStream_; }
     cudaStream_t stream() const { return stream_; }
+    int precision() const { return prec_; }
 
     // Enqueues n iterations (no host sync). Kernels of iterations after
     // convergence / divergence return immediately.
@@ -61,8 +62,8 @@ public:
     void getTurbo(double massflow[6], double turbo[4]);
     Control control();  // synchronous copy of the control block
     void profileKernels(int reps, double* outMs);
-    size_t deviceBytes() const { return deviceBytes_; }
     long long history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub);
+    size_t deviceBytes() const;
 
     long ni() const { return mesh_.ni(); }
     long nj() const { return mesh_.nj(); }
@@ -71,43 +72,47 @@ public:
     int stages() const { return static_cast<int>(coeffs_.size()); }
     long maxIterations() const { return maxIter_; }
 
+    // device data for batches (nullptr when the solver runs the other precision)
+    InstanceT<double>* instance64() { return i64_.get(); }
+    InstanceT<float>* instance32() { return i32_.get(); }
+
 private:
     void readBoundaries();
     void buildBoundaryStructures();
-    void uploadBoundaryStructures();
-    void validateSettings();
+    void setupScalars();
     void setupModels();
-    void upload();
-    void initializeSolution();
-    void initializeProfilesAndPlenum();
-    void enqueueIteration();
-    void setLimits(long long itStop, long long histBase);
-    void captureGraph();
-    double* alloc(size_t count);
-    const double* upload(const std::vector<double>& v);
-    void check(cudaError_t e, const char* what);
+    void validateSettings();
+    template <typename R>
+    void uploadArrays(InstanceT<R>& inst);
+    template <typename R>
+    void initializeState(InstanceT<R>& inst, GroupT<R>& grp);
+    template <typename F>
+    auto visit(F&& f) {
+        if (prec_ == kFP32Kahan) return f(*i32_, *g32_);
+        return f(*i64_, *g64_);
+    }
 
     Config& config_;
     Mesh& mesh_;
     Topology topo_;
     std::vector<double> coeffs_;
     long maxIter_ = 0;
+    int prec_ = kFP64;
     std::unique_ptr<AdvectionBase> advection_;
     std::unique_ptr<SourceBFMBase> bfm_;
     std::vector<BoundaryPatch> boundaries_;
-    bool needTurbo_ = false, profiles_ = false;
+    bool needTurbo_ = false;
     double periodicAngleDeg_ = 0.0, periodicAngleRad_ = 0.0, periodicTransl_ = 0.0;
-
-    DevCase c_{};
+    DevCaseT<double> proto_{};  // scalar settings shared by both precisions
     std::vector<signed char> mapI_, mapJ_, mapK_;
     std::vector<double> profP_, profR_;
-    std::vector<void*> allocations_;
+
+    std::unique_ptr<InstanceT<double>> i64_;
+    std::unique_ptr<GroupT<double>> g64_;
+    std::unique_ptr<InstanceT<float>> i32_;
+    std::unique_ptr<GroupT<float>> g32_;
     Control* hostCtl_ = nullptr;  // pinned
     cudaStream_t ownStream_ = nullptr, stream_ = nullptr;
-    cudaGraphExec_t graph_ = nullptr;
-    int graphIters_ = 0;
-    long long itHost_ = 0;  // iteration counter as last seen by the host
-    size_t deviceBytes_ = 0;
 };
 
 }  // namespace ctbfm

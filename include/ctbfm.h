@@ -66,7 +66,7 @@ typedef struct {
     int64_t iteration;        /* iterations performed so far */
     int64_t max_iterations;   /* N_ITERATIONS */
     int32_t status;           /* CTBFM_STATUS_* */
-    int32_t precision;        /* 0 = FP64 */
+    int32_t precision;        /* GPU_PRECISION: 0 = fp64, 1 = fp32_kahan */
     double time;              /* physical time sum of min(dt) */
 } ctbfm_info;
 
