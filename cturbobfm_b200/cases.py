@@ -281,20 +281,33 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
     return Case(name, X, Y, Z, fields, patches, s)
 
 
+# Blade rows (x_le, x_te, kappa_hub_deg, kappa_tip_deg, rpm, n_blades,
+# max_blockage_loss) of the rotor/stator stage of annulus3d.
+STAGE_ROWS = [(0.2, 0.3, -50.0, -60.0, 10000.0, 24, 0.4),
+              (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
+# The compressor-map stage: the same rows with 30-40 degree rotor metal angles
+# and 0.1 blockage loss. The annulus3d stage diverges in axisymmetric form
+# (the oracle and the reference alike) at every back pressure of the map; this
+# one converges over p_out/pt_in 1.00-1.20 and speed 85-100 %.
+MAP_ROWS = [(0.2, 0.3, -30.0, -40.0, 10000.0, 24, 0.1),
+            (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.1)]
+
+
 def meridional(ni: int = 96, nj: int = 32, n_iter: int = 20000, cfl: float = 1.3,
                p_ratio: float = 1.15, speed: float = 1.0, bfm_model: str = "Hall",
                outlet: str = "outlet", drop: int = 8, mach: float = 0.3,
-               scheme: str = "JST", rk: int = 4, name: str = "meridional") -> Case:
-    """Axisymmetric meridional plane of the rotor/stator stage of annulus3d
-    (nk = 1; the solver builds a 1 degree wedge around it)."""
+               scheme: str = "JST", rk: int = 4, name: str = "meridional",
+               rows=None, ramp: Optional[int] = None, precision: Optional[str] = None) -> Case:
+    """Axisymmetric meridional plane of a rotor/stator stage (nk = 1; the
+    solver builds a 1 degree wedge around it). ``rows`` defaults to the
+    annulus3d stage; ``ramp`` sets OUTLET_PRESSURE_RAMP_ITERATIONS and
+    ``precision`` GPU_PRECISION."""
     xs = np.linspace(0.0, 0.6, ni)
     rs = np.linspace(0.20, 0.40, nj)
     X = np.broadcast_to(xs[:, None, None], (ni, nj, 1)).copy()
     Y = np.broadcast_to(rs[None, :, None], (ni, nj, 1)).copy()
     Z = np.zeros_like(X)
-    rows = [(0.2, 0.3, -50.0, -60.0, 10000.0, 24, 0.4),
-            (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
-    fields = _row_fields(xs, rs, rows, 1)
+    fields = _row_fields(xs, rs, STAGE_ROWS if rows is None else rows, 1)
     pt, tt = 101325.0, 288.15
     ps, ts = static_state(pt, tt, mach)
     s = _base_settings("axisymmetric")
@@ -319,6 +332,10 @@ def meridional(ni: int = 96, nj: int = 32, n_iter: int = 20000, cfl: float = 1.3
         "TURBO_OUTPUT": "yes",
         "TURBO_DIRECTION": "i",
     })
+    if ramp is not None:
+        s["OUTLET_PRESSURE_RAMP_ITERATIONS"] = str(ramp)
+    if precision is not None:
+        s["GPU_PRECISION"] = precision
     if outlet == "outlet":
         out_spec = f"outlet, {p_ratio * pt!r}"
     elif outlet == "radial_equilibrium":
@@ -335,12 +352,16 @@ def meridional(ni: int = 96, nj: int = 32, n_iter: int = 20000, cfl: float = 1.3
 
 
 def compressor_map(n: int = 256, seed: int = 20261203, ni_range=(64, 256),
-                   nj_range=(24, 96), p_ratio_range=(1.00, 1.35),
-                   speed_range=(0.70, 1.05), n_iter: int = 20000) -> List[Case]:
+                   nj_range=(24, 96), p_ratio_range=(1.00, 1.20),
+                   speed_range=(0.85, 1.00), n_iter: int = 40000, drop: int = 3,
+                   cfl: float = 2.2, ramp: int = 2000,
+                   precision: Optional[str] = "fp32_kahan") -> List[Case]:
     """The batched compressor-map workload: n axisymmetric meridional
-    instances with independently drawn grid sizes, back-pressure ratios and
-    shaft-speed scalings from a seeded PCG64 generator. Each runs JST + RK4 to
-    an 8-order residual drop."""
+    instances of the MAP_ROWS stage with independently drawn grid sizes,
+    back-pressure ratios and shaft-speed scalings from a seeded PCG64
+    generator (draw order per instance: NI, NJ, p_out/pt_in, speed). Each
+    runs JST + RK4 with local time steps at CFL 2.2, the outlet pressure
+    ramped over 2000 iterations, to a residual drop of 3 orders."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for m in range(n):
@@ -348,8 +369,9 @@ def compressor_map(n: int = 256, seed: int = 20261203, ni_range=(64, 256),
         nj = int(rng.integers(nj_range[0], nj_range[1] + 1))
         pr = float(rng.uniform(*p_ratio_range))
         sp = float(rng.uniform(*speed_range))
-        out.append(meridional(ni=ni, nj=nj, n_iter=n_iter, p_ratio=pr, speed=sp,
-                              drop=8, name=f"map{m:03d}"))
+        out.append(meridional(ni=ni, nj=nj, n_iter=n_iter, p_ratio=pr, speed=sp, cfl=cfl,
+                              drop=drop, name=f"map{m:03d}", rows=MAP_ROWS, ramp=ramp,
+                              precision=precision))
     return out
 
 

@@ -8,8 +8,11 @@
 
 #include <cmath>
 #include <memory>
+#include <stdexcept>
 #include <string>
+#include <vector>
 
+#include "host/batch.hpp"
 #include "host/config.hpp"
 #include "host/mesh.hpp"
 #include "host/solver.hpp"
@@ -18,6 +21,10 @@ struct ctbfm_solver {
     std::unique_ptr<ctbfm::Config> config;
     std::unique_ptr<ctbfm::Mesh> mesh;
     std::unique_ptr<ctbfm::Solver> solver;
+};
+
+struct ctbfm_batch {
+    std::unique_ptr<ctbfm::Batch> batch;
 };
 
 namespace {
@@ -38,6 +45,8 @@ int guarded(F&& f) {
         return setError(CTBFM_E_CONFIG, e.what());
     } catch (const ctbfm::CudaError& e) {
         return setError(CTBFM_E_CUDA, e.what());
+    } catch (const std::invalid_argument& e) {
+        return setError(CTBFM_E_ARGUMENT, e.what());
     } catch (const std::exception& e) {
         return setError(CTBFM_E_CONFIG, e.what());
     } catch (...) {
@@ -211,6 +220,79 @@ int ctbfm_profile_kernels(ctbfm_solver* s, int reps, double* out_ms) {
     if (!s || !out_ms || reps < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
     return guarded([&] {
         s->solver->profileKernels(reps, out_ms);
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_batch_create(ctbfm_solver* const* solvers, int32_t n, ctbfm_batch** out) {
+    if (!solvers || !out || n <= 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
+    *out = nullptr;
+    return guarded([&] {
+        std::vector<ctbfm::Solver*> members;
+        for (int32_t i = 0; i < n; i++) {
+            if (!solvers[i]) throw std::invalid_argument("null solver in batch");
+            members.push_back(solvers[i]->solver.get());
+        }
+        auto b = std::make_unique<ctbfm_batch>();
+        b->batch = std::make_unique<ctbfm::Batch>(members);
+        *out = b.release();
+        return CTBFM_OK;
+    });
+}
+
+void ctbfm_batch_destroy(ctbfm_batch* b) {
+    if (!b) return;
+    try {
+        delete b;
+    } catch (...) {
+    }
+}
+
+int ctbfm_batch_set_stream(ctbfm_batch* b, void* stream) {
+    if (!b) return setError(CTBFM_E_ARGUMENT, "null batch");
+    return guarded([&] {
+        b->batch->setStream(static_cast<cudaStream_t>(stream));
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_batch_enqueue(ctbfm_batch* b, int64_t n_iter) {
+    if (!b || n_iter < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
+    return guarded([&] {
+        b->batch->enqueue(n_iter);
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_batch_step(ctbfm_batch* b, int64_t n_iter, int64_t* n_done) {
+    if (!b || n_iter < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
+    return guarded([&] {
+        const long long d = b->batch->step(n_iter);
+        if (n_done) *n_done = d;
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_batch_status(ctbfm_batch* b, int32_t* status, int64_t* iterations, double* lognorm, double* best_drop) {
+    if (!b) return setError(CTBFM_E_ARGUMENT, "null batch");
+    return guarded([&] {
+        std::vector<ctbfm::Control> c(static_cast<size_t>(b->batch->size()));
+        b->batch->controls(c.data());
+        for (size_t i = 0; i < c.size(); i++) {
+            if (status) status[i] = c[i].status;
+            if (iterations) iterations[i] = c[i].it;
+            if (lognorm)
+                for (int v = 0; v < 5; v++) lognorm[5 * i + v] = c[i].lognorm[v];
+            if (best_drop) best_drop[i] = c[i].best_drop;
+        }
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_promote_fp64(ctbfm_solver* s) {
+    if (!s) return setError(CTBFM_E_ARGUMENT, "null solver");
+    return guarded([&] {
+        s->solver->promoteToFP64();
         return CTBFM_OK;
     });
 }

@@ -62,6 +62,13 @@ struct Control {
     double turbo[4];  // mass flow, PRtt, TRtt, eta_tt
     double pt_int[2], tt_int[2];
     double gz_p, gz_min, gz_mout, gz_T, gz_t;  // Greitzer plenum
+    // progress of the steady convergence test: the largest drop reached so
+    // far, min over the tested variables of (initial maximum - log norm);
+    // it_best is the last iteration at which it passed drop_mark + 0.05
+    // (drop_mark then moves up to it)
+    double best_drop;
+    double drop_mark;
+    long long it_best;
 };
 
 // A block's share of a batched launch: `count` consecutive elements (nodes,

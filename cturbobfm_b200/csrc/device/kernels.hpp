@@ -33,6 +33,8 @@ struct BatchView {
 template <typename R>
 struct Launcher {
     static cudaError_t setLimits(const BatchView<R>& b, long long n, cudaStream_t s);
+    // copies the m control blocks into out[0..m) (device memory)
+    static cudaError_t gatherControl(const BatchView<R>& b, Control* out, cudaStream_t s);
     static cudaError_t boundaryIntegrals(const BatchView<R>& b, bool all, int force, cudaStream_t s);
     static cudaError_t timeStep(const BatchView<R>& b, int force, cudaStream_t s);
     static cudaError_t pre(const BatchView<R>& b, bool forceTurbo, bool dtpart, bool profiles, int force,

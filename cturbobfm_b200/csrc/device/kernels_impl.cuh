@@ -4,10 +4,10 @@
 //
 // A launch's grid has one block per Tile; a tile is a contiguous range of one
 // instance's elements (nodes, faces of one direction, periodic (i,j) pairs,
-// boundary planes or the instance itself). Each block first copies its
-// instance's DevCaseT into shared memory and returns at once when that
-// instance has converged, diverged or reached its iteration limit, so finished
-// instances cost nothing while the rest of the batch runs.
+// boundary planes or the instance itself). Each block returns at once when
+// its instance has converged, diverged or reached its iteration limit, so
+// finished instances cost next to nothing while the rest of the batch runs,
+// and otherwise copies the instance's DevCaseT into shared memory.
 //
 // One pseudo-time iteration, with no host synchronisation:
 //   k_set_limits (once per enqueue), k_bint (boundary integrals, when turbo
@@ -27,21 +27,27 @@ namespace ctbfm {
 
 namespace {
 
-// Copies the block's instance description into shared memory.
+// Block entry: reads the block's tile, returns false (the whole block leaves
+// before touching anything else) when its instance has converged, diverged,
+// reached its iteration limit or has no such stage, and otherwise copies the
+// instance description into shared memory. Every thread reads the same
+// control words, which no kernel writes while others read them.
 template <typename R>
-__device__ __forceinline__ Tile stageCase(const DevCaseT<R>* cases, const Tile* tiles, DevCaseT<R>& sc) {
-    const Tile t = tiles[blockIdx.x];
-    const int4* src = reinterpret_cast<const int4*>(cases + t.inst);
+__device__ __forceinline__ bool enter(const DevCaseT<R>* cases, const Tile* tiles, DevCaseT<R>& sc, int stage,
+                                      int force, Tile& t) {
+    t = tiles[blockIdx.x];
+    const DevCaseT<R>* g = cases + t.inst;
+    if (!force) {
+        const Control* ctl = g->ctl;
+        if (ctl->status != 0 || ctl->it >= ctl->it_stop) return false;
+    }
+    if (stage >= g->nstages) return false;
+    const int4* src = reinterpret_cast<const int4*>(g);
     int4* dst = reinterpret_cast<int4*>(&sc);
     constexpr int n16 = static_cast<int>(sizeof(DevCaseT<R>) / 16);
     for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
     __syncthreads();
-    return t;
-}
-
-template <typename R>
-__device__ __forceinline__ bool halted(const DevCaseT<R>& c, int force) {
-    return !force && (c.ctl->status != 0 || c.ctl->it >= c.ctl->it_stop);
+    return true;
 }
 
 // Stage buffers: RK4 U -> S1 -> S2 -> S1 -> U, RK3 U -> S1 -> S2 -> U (the
@@ -143,8 +149,8 @@ __device__ __forceinline__ S5<double> state64(const DevCaseT<R>& c, R* const* U,
 template <int DIR, int SCHEME, typename R>
 __global__ void __launch_bounds__(256) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
-    const Tile tl = stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl)) return;
     const long long it = c.ctl->it + 1;
     const Gas<R> gs{R(c.gamma), R(c.rgas)};
     const int nfj = c.nj + (DIR == 1), nfk = c.nk + (DIR == 2);
@@ -227,8 +233,8 @@ __global__ void __launch_bounds__(256) k_faces(const DevCaseT<R>* cases, const T
 template <typename R>
 __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
-    const Tile tl = stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl)) return;
     R* const* U = stageIn(c, stage);
     for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x)
         store5(c.W, q, primOf(load5(U, q)));
@@ -242,8 +248,8 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 template <typename R>
 __global__ void __launch_bounds__(256, 2) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
-    const Tile tl = stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl)) return;
     const Gas<R> gs{R(c.gamma), R(c.rgas)};
     const double t = c.ctl->t;
     const R dtg = R(c.ctl->dt_min);
@@ -339,8 +345,8 @@ __global__ void __launch_bounds__(256, 2) k_nodes(const DevCaseT<R>* cases, cons
 template <typename R>
 __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
-    const Tile tl = stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl)) return;
     const R dtg = R(c.ctl->dt_min);
     const bool resOnly = stage < 0;
     const bool last = !resOnly && stage == c.nstages - 1;
@@ -409,8 +415,8 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
 template <typename R>
 __global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile* tiles, int force) {
     __shared__ DevCaseT<R> c;
-    const Tile tl = stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl)) return;
     if (c.dt_method == 2) return;
     const Gas<R> gs{R(c.gamma), R(c.rgas)};
     const R cfl = R(c.cfl);
@@ -471,8 +477,8 @@ __device__ __forceinline__ int turboPlane(const DevCaseT<R>& c, int m) {
 template <typename R>
 __global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Tile* tiles, int force) {
     __shared__ DevCaseT<R> c;
-    const Tile tl = stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl)) return;
     const Gas<double> gs{c.gamma, c.rgas};
     const int blk = tl.local;
     const int plane = blk < 6 ? blk : turboPlane(c, blk - 6);
@@ -517,8 +523,8 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Tile* tiles, int forceTurbo, int dtpart,
                                              int profiles, int force) {
     __shared__ DevCaseT<R> c;
-    stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl)) return;
     Control* ctl = c.ctl;
     if (!dtpart) {
     } else if (c.dt_method == 2) {
@@ -607,8 +613,8 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
 template <typename R>
 __global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, const Tile* tiles, int force) {
     __shared__ DevCaseT<R> c;
-    stageCase(cases, tiles, c);
-    if (halted(c, force)) return;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl)) return;
     Control* ctl = c.ctl;
     const int nparts = c.node_tiles + (c.periodic ? c.per_tiles : 0);
     double s[5] = {0, 0, 0, 0, 0};
@@ -649,17 +655,38 @@ __global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, cons
     }
     if (c.steady) {
         bool conv = true;
+        double drop = INFINITY;
         for (int v = 0; v < 5; ++v) {
             if (v == 3 && c.topo != 1 && c.topo != 2) continue;
             if (ctl->init_log[v] <= -15.99) continue;
             if (lr[v] <= -15.0) continue;
-            if (lr[v] >= ctl->init_log[v] - static_cast<double>(c.drop)) {
-                conv = false;
-                break;
-            }
+            drop = fmin(drop, ctl->init_log[v] - lr[v]);
+            if (lr[v] >= ctl->init_log[v] - static_cast<double>(c.drop)) conv = false;
         }
         if (conv) ctl->status = 1;
+        if (it <= 5) {
+            ctl->best_drop = 0.0;
+            ctl->drop_mark = 0.0;
+            ctl->it_best = it;
+        } else {
+            ctl->best_drop = fmax(ctl->best_drop, drop);
+            if (drop >= ctl->drop_mark + 0.05) {
+                ctl->drop_mark = drop;
+                ctl->it_best = it;
+            }
+        }
     }
+}
+
+// Copies every instance's control block into one array (one D2H copy for a
+// whole batch).
+template <typename R>
+__global__ void k_gather_control(const DevCaseT<R>* cases, int m, Control* out) {
+    const int i = blockIdx.x;
+    if (i >= m) return;
+    const int* src = reinterpret_cast<const int*>(cases[i].ctl);
+    int* dst = reinterpret_cast<int*>(out + i);
+    for (int w = threadIdx.x; w < static_cast<int>(sizeof(Control) / 4); w += blockDim.x) dst[w] = src[w];
 }
 
 // Sets each instance's iteration limit (n more iterations) and history origin.
@@ -679,6 +706,12 @@ __global__ void k_set_limits(const DevCaseT<R>* cases, int m, long long n) {
 template <typename R>
 cudaError_t Launcher<R>::setLimits(const BatchView<R>& b, long long n, cudaStream_t s) {
     k_set_limits<R><<<(b.m + 127) / 128, 128, 0, s>>>(b.cases, b.m, n);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launcher<R>::gatherControl(const BatchView<R>& b, Control* out, cudaStream_t s) {
+    if (b.m) k_gather_control<R><<<b.m, 64, 0, s>>>(b.cases, b.m, out);
     return cudaGetLastError();
 }
 

@@ -55,10 +55,10 @@ const double* InstanceT<R>::uploadD(const std::vector<double>& v) {
 template <typename R>
 GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(members)) {
     if (members_.empty()) throw std::invalid_argument("empty group");
-    nstages_ = members_[0]->c.nstages;
-    for (auto* m : members_)
-        if (m->c.nstages != nstages_)
-            throw std::invalid_argument("all members of a group need the same number of Runge-Kutta stages");
+    // stage kernels run the largest stage count; members with fewer stages
+    // skip the extra launches on the device
+    nstages_ = 0;
+    for (auto* m : members_) nstages_ = std::max(nstages_, m->c.nstages);
     const int M = static_cast<int>(members_.size());
     // tile lists over the packed index of all members
     std::vector<Tile> node, face[3][2], per, inst, bint, bintAll;

@@ -870,6 +870,39 @@ void Solver::profileKernels(int reps, double* outMs) {
     });
 }
 
+void Solver::promoteToFP64() {
+    if (prec_ == kFP64) return;
+    const long N = mesh_.nodes();
+    std::array<std::vector<double>, 5> U;
+    double* out[5];
+    for (int v = 0; v < 5; v++) {
+        U[v].resize(N);
+        out[v] = U[v].data();
+    }
+    getState(out);
+    const Control ctl = control();
+    proto_.compensated = 0;
+    auto inst = std::make_unique<InstanceT<double>>();
+    uploadArrays(*inst);
+    auto grp = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{inst.get()});
+    const DevCaseT<float>& f = i32_->c;
+    if (proto_.nprofiles)
+        cudaCheck(cudaMemcpy(inst->c.prof_p, f.prof_p, profP_.size() * sizeof(double), cudaMemcpyDeviceToDevice),
+                  "cudaMemcpy");
+    cudaCheck(cudaMemcpy(inst->c.hist, f.hist, static_cast<size_t>(proto_.hist_cap) * kHistWidth * sizeof(double),
+                         cudaMemcpyDeviceToDevice),
+              "cudaMemcpy");
+    i64_ = std::move(inst);
+    g64_ = std::move(grp);
+    prec_ = kFP64;
+    const double* in[5] = {U[0].data(), U[1].data(), U[2].data(), U[3].data(), U[4].data()};
+    setState(in);
+    *hostCtl_ = ctl;
+    cudaCheck(cudaMemcpy(i64_->c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
+    g32_.reset();
+    i32_.reset();
+}
+
 long long Solver::history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub) {
     const Control c = control();
     const long long cap = proto_.hist_cap;

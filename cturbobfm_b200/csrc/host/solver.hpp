@@ -62,6 +62,11 @@ public:
     void getTurbo(double massflow[6], double turbo[4]);
     Control control();  // synchronous copy of the control block
     void profileKernels(int reps, double* outMs);
+    // Continues a fp32_kahan solve in FP64: the state U - Uc, the control
+    // block (iteration, time, convergence reference, plenum), the radial
+    // profiles and the history move to a new FP64 instance; the float
+    // instance is released. No-op on an FP64 solver.
+    void promoteToFP64();
     long long history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub);
     size_t deviceBytes() const;
 

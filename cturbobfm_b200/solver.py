@@ -26,6 +26,7 @@ CTBFM_E_ARGUMENT = 4
 CTBFM_E_UNSUPPORTED = 5
 
 STATUS_RUNNING, STATUS_CONVERGED, STATUS_DIVERGED = 0, 1, 2
+PRECISION_FP64, PRECISION_FP32_KAHAN = 0, 1
 
 
 class CtbfmError(RuntimeError):
@@ -75,6 +76,13 @@ SIGNATURES = {
     "ctbfm_get_history": ([_VP, _I64, _DP, _DP, _DP, _DP, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_get_turbo": ([_VP, _DP, _DP], ctypes.c_int),
     "ctbfm_profile_kernels": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
+    "ctbfm_batch_create": ([ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(_VP)], ctypes.c_int),
+    "ctbfm_batch_destroy": ([_VP], None),
+    "ctbfm_batch_set_stream": ([_VP, _VP], ctypes.c_int),
+    "ctbfm_batch_enqueue": ([_VP, _I64], ctypes.c_int),
+    "ctbfm_batch_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
+    "ctbfm_batch_status": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_I64), _DP, _DP], ctypes.c_int),
+    "ctbfm_promote_fp64": ([_VP], ctypes.c_int),
     "ctbfm_last_error": ([], ctypes.c_char_p),
     "ctbfm_version": ([], ctypes.c_char_p),
 }
@@ -136,6 +144,10 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+    def promote_fp64(self):
+        """Continues a fp32_kahan solve in FP64 (no-op for FP64 solvers)."""
+        _check(load_library().ctbfm_promote_fp64(self._h))
 
     def info(self) -> Info:
         inf = Info()
@@ -221,3 +233,58 @@ class Solver:
     @property
     def time(self) -> float:
         return float(self.info().time)
+
+
+class Batch:
+    """Solvers of one GPU_PRECISION advanced together (ctbfm_batch_*): one
+    launch per kernel family for all members. The solvers stay usable for
+    queries between steps and must outlive the batch."""
+
+    def __init__(self, solvers):
+        lib = load_library()
+        self.solvers = list(solvers)
+        arr = (_VP * len(self.solvers))(*[s._h for s in self.solvers])
+        h = _VP()
+        _check(lib.ctbfm_batch_create(arr, len(self.solvers), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().ctbfm_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.solvers)
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _check(load_library().ctbfm_batch_set_stream(self._h, _VP(stream_ptr or 0)))
+
+    def enqueue(self, n_iter: int):
+        _check(load_library().ctbfm_batch_enqueue(self._h, int(n_iter)))
+
+    def step(self, n_iter: int) -> int:
+        done = _I64(0)
+        _check(load_library().ctbfm_batch_step(self._h, int(n_iter), ctypes.byref(done)))
+        return int(done.value)
+
+    def status(self) -> Dict[str, np.ndarray]:
+        m = len(self.solvers)
+        st = np.zeros(m, np.int32)
+        it = np.zeros(m, np.int64)
+        ln = np.zeros((m, 5))
+        bd = np.zeros(m)
+        _check(load_library().ctbfm_batch_status(self._h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                 it.ctypes.data_as(ctypes.POINTER(_I64)), _ptr(ln), _ptr(bd)))
+        return {"status": st, "iterations": it, "lognorm": ln, "best_drop": bd}

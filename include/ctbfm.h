@@ -162,6 +162,47 @@ enum {
  * time step and control block are restored afterwards. */
 int ctbfm_profile_kernels(ctbfm_solver* s, int reps, double* out_ms);
 
+/* ------------------------------------------------------------------------
+ * Batches of operating points. No counterpart in the reference, which runs
+ * one turbobfm process per operating point (python/Run_All_Cases.py:18-98).
+ * A batch advances its solvers together: each kernel family is one launch
+ * over a packed tile index of all members' nodes, faces and planes, so many
+ * small grids share the GPU. Every member computes exactly what it computes
+ * alone (per-member reductions in a fixed order).
+ * ------------------------------------------------------------------------ */
+typedef struct ctbfm_batch ctbfm_batch;
+
+/* Groups n solvers of the same GPU_PRECISION (Runge-Kutta stage counts may
+ * differ). The solvers stay owned by the caller, must outlive the batch and
+ * must not be stepped on their own while it exists; their state, turbo and
+ * history queries remain valid between batch steps. Duplicates, NULLs and
+ * mixed precisions are CTBFM_E_ARGUMENT. */
+int ctbfm_batch_create(ctbfm_solver* const* solvers, int32_t n, ctbfm_batch** out);
+void ctbfm_batch_destroy(ctbfm_batch* b);
+int ctbfm_batch_set_stream(ctbfm_batch* b, void* cuda_stream);
+
+/* Enqueues n_iter iterations of every member that is still running (members
+ * that converge or diverge stop on the device at that iteration). */
+int ctbfm_batch_enqueue(ctbfm_batch* b, int64_t n_iter);
+
+/* enqueue + synchronise. *n_done (nullable) receives the most iterations any
+ * member advanced. A diverged member is reported through
+ * ctbfm_batch_status, not as an error of the call. */
+int ctbfm_batch_step(ctbfm_batch* b, int64_t n_iter, int64_t* n_done);
+
+/* Per member (arrays of n, each nullable): CTBFM_STATUS_*, iterations done,
+ * the last log10 residual norms (5 per member), and the convergence progress
+ * best_drop = the largest min-over-variables drop of the log norm below its
+ * initial maximum reached so far (orders of magnitude). */
+int ctbfm_batch_status(ctbfm_batch* b, int32_t* status, int64_t* iterations, double* lognorm,
+                       double* best_drop);
+
+/* Continues a fp32_kahan solver in FP64 (state U - Uc, iteration count,
+ * time, convergence reference, plenum and profile state carried over); a
+ * no-op for FP64 solvers. A batch holding the solver must be destroyed
+ * first. No counterpart in the reference (FP64 only). */
+int ctbfm_promote_fp64(ctbfm_solver* s);
+
 /* Message of the calling thread's last error ("" if none). */
 const char* ctbfm_last_error(void);
 

@@ -59,6 +59,7 @@ def test_missing_input_file_is_a_config_error(lib, tmp_path):
     ("INIT_DIRECTION", "1, 0", "INIT_DIRECTION must have 3 components"),
     ("ENABLE_GREITZER_MODELING", "yes", "Greitzer modeling is only compatible with fixed time step method"),
     ("INLET_REFERENCE_FRAME", "polar", "Invalid value for key \"INLET_REFERENCE_FRAME\""),
+    ("GPU_PRECISION", "fp16", "Invalid value for key \"GPU_PRECISION\""),
 ])
 def test_invalid_settings_are_rejected(lib, tmp_path, key, value, message):
     from cturbobfm_b200 import cases
@@ -73,3 +74,13 @@ def test_invalid_settings_are_rejected(lib, tmp_path, key, value, message):
 def test_null_arguments(lib):
     assert lib.ctbfm_create_from_ini(None, None) == 4
     assert lib.ctbfm_step(None, 1, None) == 4
+    assert lib.ctbfm_batch_create(None, 0, None) == 4
+    assert lib.ctbfm_batch_step(None, 1, None) == 4
+    assert lib.ctbfm_batch_enqueue(None, 1) == 4
+    assert lib.ctbfm_batch_status(None, None, None, None, None) == 4
+    assert lib.ctbfm_promote_fp64(None) == 4
+    arr = (ctypes.c_void_p * 2)(None, None)
+    out = ctypes.c_void_p()
+    assert lib.ctbfm_batch_create(arr, 2, ctypes.byref(out)) == 4
+    assert out.value is None
+    lib.ctbfm_batch_destroy(None)
