@@ -278,6 +278,30 @@ def run_ours(args):
     ms_max = float(t.item())
     value = world * n * stages * args.steps / (ms_max / 1e3)
 
+    u64 = solver.state() if world == 1 else None
+
+    # the same workload in fp32_kahan (float fluxes and state + Kahan term,
+    # double norms and integrals), device-timed the same way
+    fp32 = None
+    if world == 1:
+        ini32 = case.with_settings(GPU_PRECISION="fp32_kahan").write(os.path.join(tmp.name, "fp32"))
+        with Solver(ini32) as s32:
+            s32.set_stream(stream.cuda_stream)
+            s32.enqueue(args.warmup)
+            stream.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            f0.record(stream)
+            s32.enqueue(args.steps)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            ms32 = f0.elapsed_time(f1)
+            u32 = s32.state()
+            rel = [float(np.abs(u32[v] - u64[v]).max() / np.abs(u64[v]).max()) for v in range(5)]
+            fp32 = {"value": n * stages * args.steps / (ms32 / 1e3), "unit": UNIT, "ms_per_step": ms32 / args.steps,
+                    "speedup_vs_fp64": ms_max / ms32,
+                    "state_rel_err_vs_fp64": {"after_iterations": args.warmup + args.steps, "per_field_max": rel}}
+
     # end to end through the C ABI with pinned host buffers: every step uploads
     # the state, runs one iteration and reads the state and residual norms back
     host = torch.empty((5, n), dtype=torch.float64, pin_memory=True)
@@ -338,11 +362,304 @@ def run_ours(args):
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "kernel_ms": prof, "kernel_share": {k: v / total for k, v in shares.items() if v > 0},
     }
+    if fp32:
+        line["fp32_kahan"] = fp32
     if world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(case, args.cpu_iters)
         line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
     solver.close()
+
+
+# ------------------------------------------------------------ compressor map
+MAP_METRIC = "converged op-points/hour"
+MAP_WORKLOAD = ("compressor map: 256 axisymmetric BFM instances (Hall, MAP_ROWS stage), NI x NJ ~ U{64..256} x "
+                "U{24..96}, p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], PCG64 seed 20261203, JST, RK4, local dt "
+                "CFL 2.2, outlet ramp 2000 its, residual drop 3 orders")
+
+
+def _map_launches_per_iteration(case) -> int:
+    # k_bint, k_dt, k_pre, per stage k_prim + k_faces I + k_faces J + k_nodes, k_finalize
+    return 3 + 4 * case.n_stages + 1
+
+
+def _solve_batched(solvers, stream, chunk: int, n_iter: int, per_iteration: int):
+    """Runs the batch to convergence (or N_ITERATIONS) in chunks, dropping
+    finished members from the batch whenever a quarter of it has finished.
+    Returns (per-member status, iterations, launches)."""
+    import numpy as np
+
+    from cturbobfm_b200 import Batch
+
+    m = len(solvers)
+    status = np.zeros(m, np.int32)
+    iters = np.zeros(m, np.int64)
+    active = list(range(m))
+    launches = 0
+    while active:
+        with Batch([solvers[i] for i in active]) as b:
+            b.set_stream(stream.cuda_stream)
+            start = len(active)
+            while True:
+                b.step(chunk)
+                st = b.status()
+                launches += chunk * per_iteration + 4  # + k_set_limits and three control gathers
+                for j, i in enumerate(active):
+                    status[i] = st["status"][j]
+                    iters[i] = st["iterations"][j]
+                done = [i for i in active if status[i] != 0 or iters[i] >= n_iter]
+                if len(done) * 4 >= start or len(done) == len(active):
+                    break
+        active = [i for i in active if not (status[i] != 0 or iters[i] >= n_iter)]
+    return status, iters, launches
+
+
+def map_cpu_baseline(inis, iterations, n_iter: int):
+    """Converged op-points/hour of the reference build on the host cores: one
+    single-threaded process per instance, all at once (the way the
+    reference's python/Run_All_Cases.py fans out), each timed over n_iter
+    iterations with set-up subtracted; points/hour then follows from the
+    iteration counts each instance needs to converge (the same algorithm,
+    measured on the GPU FP64 path)."""
+    from oracle import oracle
+
+    if not os.path.exists(oracle.REF_CLI):
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+
+    def launch(ini, n):
+        d = os.path.dirname(ini)
+        lines = [l for l in open(ini).read().splitlines() if not l.startswith("N_ITERATIONS")]
+        open(ini, "w").write("\n".join(lines + [f"N_ITERATIONS = {n}"]) + "\n")
+        return subprocess.Popen([oracle.REF_CLI, "input.ini"], cwd=d, stdout=subprocess.DEVNULL,
+                                stderr=subprocess.DEVNULL, env=env)
+
+    def wall(n):
+        t0 = time.perf_counter()
+        ps = [launch(ini, n) for ini in inis]
+        for p in ps:
+            p.wait(timeout=900)
+        return time.perf_counter() - t0
+
+    t1 = wall(1)
+    tn = wall(n_iter + 1)
+    per_round = (tn - t1) / n_iter  # seconds per iteration of all sampled instances at once
+    # all sampled instances run concurrently, one per core: the batch of them
+    # takes as long as the slowest, which needs max(iterations) iterations
+    cores = len(inis)
+    seconds = per_round * max(iterations)
+    return {"value": len(inis) / seconds * 3600.0, "unit": "points/hour", "cores": cores, "kind": "reference",
+            "sample": f"{len(inis)} map instances as concurrent single-threaded reference processes, "
+                      f"{n_iter} iterations timed (set-up subtracted), scaled to the iterations each needs to "
+                      f"converge"}
+
+
+def run_map(args):
+    import numpy as np
+    import torch
+
+    from cturbobfm_b200 import Solver, cases
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    cs32 = cases.compressor_map(n=args.map_n, precision="fp32_kahan")
+    per_iteration = _map_launches_per_iteration(cs32[0])
+    n_iter = int(cs32[0].settings["N_ITERATIONS"])
+    tmp = tempfile.TemporaryDirectory()
+
+    def write(cs, tag):
+        out = []
+        for c in cs:
+            d = os.path.join(tmp.name, tag, c.name)
+            os.makedirs(d)
+            out.append(c.write(d))
+        return out
+
+    inis32 = write(cs32, "fp32")
+    cs64 = [c.with_settings(GPU_PRECISION="fp64") for c in cs32]
+    inis64 = write(cs64, "fp64")
+    nodes = np.array([c.n_nodes for c in cs32])
+    stream = torch.cuda.Stream()
+    results = {}
+    with ClockSampler(local) as clocks:
+        for arm, inis in (("batched_fp32_kahan", inis32), ("batched_fp64", inis64)):
+            if arm == "batched_fp64" and args.map_skip_fp64_batch:
+                continue
+            w0 = time.perf_counter()
+            solvers = [Solver(p) for p in inis]
+            setup = time.perf_counter() - w0
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            status, iters, launches = _solve_batched(solvers, stream, args.map_chunk, n_iter, per_iteration)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sec = e0.elapsed_time(e1) / 1e3
+            w1 = time.perf_counter()
+            turbo = np.array([s.turbo()[1] for s in solvers])
+            readback = time.perf_counter() - w1
+            bytes_up = sum(int(s.info().device_bytes) for s in solvers)
+            for s in solvers:
+                s.close()
+            conv = int((status == 1).sum())
+            results[arm] = {"seconds": sec, "setup_seconds": setup, "readback_seconds": readback,
+                            "converged": conv, "diverged": int((status == 2).sum()),
+                            "points_per_hour": conv / sec * 3600.0,
+                            "e2e_points_per_hour": conv / (setup + sec + readback) * 3600.0,
+                            "iterations": iters.tolist(), "turbo": turbo, "status": status,
+                            "node_stage_per_s": float((nodes * iters).sum() * 4 / sec), "launches": launches,
+                            "device_bytes": bytes_up}
+        # the plain FP64 path: one drop-in solver at a time, to convergence
+        sample = list(range(min(args.map_plain, len(inis64))))
+        plain_sec, plain_conv, plain = 0.0, 0, []
+        for i in sample:
+            with Solver(inis64[i]) as s:
+                s.set_stream(stream.cuda_stream)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                try:
+                    s.solve()
+                except Exception:
+                    pass
+                e1.record(stream)
+                torch.cuda.synchronize()
+                plain_sec += e0.elapsed_time(e1) / 1e3
+                plain_conv += int(s.status == 1)
+                plain.append((s.status, s.iteration, s.turbo()[1]))
+    clk = clocks.summary()
+    r32 = results["batched_fp32_kahan"]
+    plain_pph = plain_conv / plain_sec * 3600.0 if plain_sec > 0 else None
+    # accuracy of the batched FP32 results against the plain FP64 solves of the same instances
+    err_mf, err_pr = [], []
+    for j, i in enumerate(sample):
+        st, it, tb = plain[j]
+        if st == 1 and r32["status"][i] == 1:
+            err_mf.append(abs(r32["turbo"][i][0] - tb[0]) / abs(tb[0]))
+            err_pr.append(abs(r32["turbo"][i][1] - tb[1]) / abs(tb[1]))
+    line = {
+        "metric": MAP_METRIC, "value": r32["points_per_hour"], "unit": "points/hour", "n_gpus": 1,
+        "steps": len(cs32), "warmup": 0, "ms_per_step": r32["seconds"] * 1e3 / max(1, len(cs32)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+kahan (f64 integrals)",
+        "data": "synthetic",
+        "config": {"workload": MAP_WORKLOAD, "instances": len(cs32), "nodes_total": int(nodes.sum()),
+                   "chunk_iterations": args.map_chunk, "l2": "inputs larger than L2 (working set > 126 MiB)"},
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "e2e": {"value": r32["e2e_points_per_hour"], "unit": "points/hour",
+                "h2d_bytes_per_step": r32["device_bytes"] / len(cs32), "d2h_bytes_per_step": 6 * 8 + 4 * 8},
+        "gpu_launches": r32["launches"],
+        "batched_fp32_kahan": {k: r32[k] for k in ("seconds", "setup_seconds", "converged", "diverged",
+                                                   "points_per_hour", "node_stage_per_s")},
+        "plain_fp64": {"points_per_hour": plain_pph, "instances": len(sample), "converged": plain_conv,
+                       "seconds": plain_sec, "iterations": [p[1] for p in plain]},
+        "speedup_vs_plain_fp64": (r32["points_per_hour"] / plain_pph) if plain_pph else None,
+        "fp32_vs_plain_fp64_rel_err": {"massflow_max": max(err_mf) if err_mf else None,
+                                       "pr_tt_max": max(err_pr) if err_pr else None, "instances": len(err_mf)},
+        "iterations_fp32": {"min": int(min(r32["iterations"])), "median": float(np.median(r32["iterations"])),
+                            "max": int(max(r32["iterations"]))},
+    }
+    if "batched_fp64" in results:
+        r64 = results["batched_fp64"]
+        line["batched_fp64"] = {k: r64[k] for k in ("seconds", "converged", "diverged", "points_per_hour",
+                                                    "node_stage_per_s")}
+        both = (r32["status"] == 1) & (r64["status"] == 1)
+        if both.any():
+            emf = np.abs(r32["turbo"][both, 0] - r64["turbo"][both, 0]) / np.abs(r64["turbo"][both, 0])
+            epr = np.abs(r32["turbo"][both, 1] - r64["turbo"][both, 1]) / np.abs(r64["turbo"][both, 1])
+            dit = np.abs(np.array(r32["iterations"])[both] - np.array(r64["iterations"])[both])
+            line["batched_fp32_vs_fp64_rel_err"] = {
+                "massflow": {"p50": float(np.median(emf)), "p90": float(np.percentile(emf, 90)),
+                             "max": float(emf.max()), "above_1e-4": int((emf > 1e-4).sum())},
+                "pr_tt": {"p50": float(np.median(epr)), "p90": float(np.percentile(epr, 90)),
+                          "max": float(epr.max()), "above_1e-4": int((epr > 1e-4).sum())},
+                "convergence_iteration_difference": {"median": float(np.median(dit)), "max": int(dit.max())},
+                "instances": int(both.sum())}
+    line["not_converged"] = [
+        {"name": cs32[i].name, "shape": list(cs32[i].shape[:2]),
+         "p_ratio": round(float(cs32[i].patches[1].values[0]) / 101325.0, 4),
+         "speed": float(cs32[i].settings["ROTATIONAL_SPEED_SCALING_FACTOR"]),
+         "status": int(r32["status"][i]), "iterations": int(r32["iterations"][i])}
+        for i in range(len(cs32)) if r32["status"][i] != 1]
+    if not args.no_cpu_baseline:
+        conv_plain = [j for j, p in enumerate(plain) if p[0] == 1]
+        if conv_plain:
+            base = map_cpu_baseline([inis64[sample[j]] for j in conv_plain], [plain[j][1] for j in conv_plain],
+                                    args.cpu_iters * 10)
+            if base:
+                line["cpu_baseline"] = base
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- serving
+SERVE_WORKLOAD = ("serving: Poisson arrivals, 70% axisymmetric compressor-map requests (NI x NJ ~ U{64..256} x "
+                  "U{24..96}) and 30% 3-D annuli (U{96..160} x U{32..48} x U{32..64}), MAP_ROWS stage, "
+                  "p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], JST RK4 CFL 2.2, drop 3 orders, fp32_kahan")
+
+
+def run_serve(args):
+    import numpy as np
+    import torch
+
+    from cturbobfm_b200 import Server, cases
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    tmp = tempfile.TemporaryDirectory()
+    per_rate = {}
+    with ClockSampler(local) as clocks:
+        for rate in args.serve_rates:
+            reqs = cases.serving_requests(args.serve_n, rate)
+            inis = []
+            for t, c in reqs:
+                d = os.path.join(tmp.name, f"r{rate}", c.name)
+                os.makedirs(d)
+                inis.append((t, c.write(d), c.n_nodes, c.shape[2] > 1))
+            res = {}
+            with Server(chunk=args.serve_chunk, stall_window=0, host_threads=8) as srv:
+                t0 = time.perf_counter()
+                nxt = 0
+                ids = {}
+                while len(res) < len(inis):
+                    now = time.perf_counter() - t0
+                    while nxt < len(inis) and inis[nxt][0] <= now:
+                        ids[srv.submit(inis[nxt][1])] = nxt
+                        nxt += 1
+                    active, waiting = srv.pump()
+                    for r in srv.results():
+                        res[ids[r["id"]]] = r
+                    if active == 0 and waiting == 0 and nxt < len(inis):
+                        time.sleep(max(0.0, min(0.01, inis[nxt][0] - (time.perf_counter() - t0))))
+                wall = time.perf_counter() - t0
+            lat = np.array([res[i]["t_done"] - res[i]["t_submit"] for i in range(len(inis))])
+            conv = np.array([res[i]["status"] == 1 for i in range(len(inis))])
+            its = np.array([res[i]["iterations"] for i in range(len(inis))])
+            nodes = np.array([x[2] for x in inis])
+            is3d = np.array([x[3] for x in inis])
+            per_rate[str(rate)] = {
+                "requests": len(inis), "converged": int(conv.sum()),
+                "diverged": int(sum(res[i]["status"] == 2 for i in range(len(inis)))),
+                "errors": int(sum(res[i]["error"] != 0 for i in range(len(inis)))),
+                "p50_s": float(np.percentile(lat[conv], 50)) if conv.any() else None,
+                "p99_s": float(np.percentile(lat[conv], 99)) if conv.any() else None,
+                "p50_s_axisymmetric": float(np.percentile(lat[conv & ~is3d], 50)) if (conv & ~is3d).any() else None,
+                "p50_s_3d": float(np.percentile(lat[conv & is3d], 50)) if (conv & is3d).any() else None,
+                "points_per_hour": float(conv.sum() / wall * 3600.0), "wall_s": wall,
+                "arrival_window_s": inis[-1][0],
+                "node_stage_per_s": float((nodes * its).sum() * 4 / wall),
+            }
+    clk = clocks.summary()
+    first = per_rate[str(args.serve_rates[0])]
+    line = {
+        "metric": "serving p50 time-to-converged", "value": first["p50_s"], "unit": "s", "n_gpus": 1,
+        "steps": first["requests"], "warmup": 0, "ms_per_step": first["wall_s"] * 1e3 / first["requests"],
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+kahan (f64 integrals)",
+        "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "rates_per_s": args.serve_rates, "requests_per_rate": args.serve_n,
+                   "chunk_iterations": args.serve_chunk, "clock": "host wall clock from submit to retirement"},
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "per_rate": per_rate,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def solver_bytes(solver, case) -> float:
@@ -361,11 +678,25 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["annulus", "map", "serve"], default="annulus",
+                    help="annulus: the 160x48x64 full-annulus loop (default); map: the batched compressor map; "
+                         "serve: continuous batching of arriving requests")
+    ap.add_argument("--map-n", type=int, default=256)
+    ap.add_argument("--map-chunk", type=int, default=250)
+    ap.add_argument("--map-plain", type=int, default=8, help="instances solved one at a time on the plain FP64 path")
+    ap.add_argument("--map-skip-fp64-batch", action="store_true")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[5.0, 20.0, 80.0])
+    ap.add_argument("--serve-n", type=int, default=48)
+    ap.add_argument("--serve-chunk", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "map":
+        run_map(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

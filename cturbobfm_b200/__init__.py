@@ -6,6 +6,6 @@ include/ctbfm.h); ``cturbobfm_b200.solver`` binds it for Python, and
 input formats.
 """
 
-from .solver import Batch, Solver, SolverDiverged, CtbfmError, load_library  # noqa: F401
+from .solver import Batch, Server, Solver, SolverDiverged, CtbfmError, load_library  # noqa: F401
 
-__all__ = ["Batch", "Solver", "SolverDiverged", "CtbfmError", "load_library"]
+__all__ = ["Batch", "Server", "Solver", "SolverDiverged", "CtbfmError", "load_library"]

@@ -230,12 +230,18 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
               cfl: float = 1.2, scheme: str = "Roe", muscl: bool = True,
               limiter: str = "van albada", rk: int = 3, bfm_model: str = "Hall",
               rpm: float = 10000.0, p_ratio: float = 1.15, mach: float = 0.3,
-              name: str = "annulus3d") -> Case:
+              name: str = "annulus3d", rows=None, speed: Optional[float] = None,
+              drop: Optional[int] = None, ramp: Optional[int] = None,
+              precision: Optional[str] = None) -> Case:
     """Full-annulus axial rotor + stator: hub radius 0.20 m, tip 0.40 m, axial
     length 0.6 m; rotor at 0.2-0.3 m (blockage loss 0.4, metal angle magnitude
     50 deg at hub to 60 deg at tip, negative in the solver's sign convention
     for positive rpm), stator at 0.35-0.45 m. k = 0 and k = nk - 1 are 360
-    degree periodic duplicates (identical coordinates)."""
+    degree periodic duplicates (identical coordinates). ``rows`` replaces the
+    blade rows (MAP_ROWS for the serving workload); ``speed``, ``drop``,
+    ``ramp`` and ``precision`` set ROTATIONAL_SPEED_SCALING_FACTOR,
+    RESIDUALS_DROP_CONVERGENCE, OUTLET_PRESSURE_RAMP_ITERATIONS and
+    GPU_PRECISION."""
     xs = np.linspace(0.0, 0.6, ni)
     rs = np.linspace(0.20, 0.40, nj)
     th = np.array([2.0 * math.pi * k / (nk - 1) for k in range(nk - 1)] + [0.0])
@@ -244,8 +250,9 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
     T = np.broadcast_to(th[None, None, :], (ni, nj, nk))
     Y = R * np.cos(T)
     Z = R * np.sin(T)
-    rows = [(0.2, 0.3, -50.0, -60.0, rpm, 24, 0.4),
-            (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
+    if rows is None:
+        rows = [(0.2, 0.3, -50.0, -60.0, rpm, 24, 0.4),
+                (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
     fields = _row_fields(xs, rs, rows, nk)
     pt, tt = 101325.0, 288.15
     ps, ts = static_state(pt, tt, mach)
@@ -270,6 +277,14 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
         "FLUX_LIMITER": limiter,
         "TURBO_DIRECTION": "i",
     })
+    if speed is not None:
+        s["ROTATIONAL_SPEED_SCALING_FACTOR"] = f"{speed!r}"
+    if drop is not None:
+        s["RESIDUALS_DROP_CONVERGENCE"] = str(drop)
+    if ramp is not None:
+        s["OUTLET_PRESSURE_RAMP_ITERATIONS"] = str(ramp)
+    if precision is not None:
+        s["GPU_PRECISION"] = precision
     patches = [
         Patch("INFLOW", 0, 0, 0, nj, 0, nk, f"inlet, {pt!r}, {tt!r}, 1, 0, 0"),
         Patch("OUTFLOW", ni, ni, 0, nj, 0, nk, f"outlet, {p_ratio * pt!r}"),
@@ -372,6 +387,39 @@ def compressor_map(n: int = 256, seed: int = 20261203, ni_range=(64, 256),
         out.append(meridional(ni=ni, nj=nj, n_iter=n_iter, p_ratio=pr, speed=sp, cfl=cfl,
                               drop=drop, name=f"map{m:03d}", rows=MAP_ROWS, ramp=ramp,
                               precision=precision))
+    return out
+
+
+def serving_requests(n: int, rate: float, seed: int = 20261203, frac_3d: float = 0.3,
+                     precision: Optional[str] = "fp32_kahan") -> List[Tuple[float, Case]]:
+    """The serving workload: n operating-point requests with Poisson arrival
+    times at `rate` per second, drawn from a seeded PCG64 generator (per
+    request: inter-arrival gap, kind, then sizes, back pressure and speed).
+    A fraction 1 - frac_3d are axisymmetric instances of the compressor map
+    (NI x NJ ~ U{64..256} x U{24..96}); the rest are 3-D annuli of the same
+    stage with NI x NJ x NK ~ U{96..160} x U{32..48} x U{32..64} (JST + RK4,
+    CFL 2.2). All: p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], outlet
+    ramp 2000 iterations, residual drop 3 orders."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    t = 0.0
+    for m in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        is3d = bool(rng.uniform() < frac_3d)
+        if is3d:
+            ni, nj, nk = int(rng.integers(96, 161)), int(rng.integers(32, 49)), int(rng.integers(32, 65))
+        else:
+            ni, nj, nk = int(rng.integers(64, 257)), int(rng.integers(24, 97)), 1
+        pr = float(rng.uniform(1.00, 1.20))
+        sp = float(rng.uniform(0.85, 1.00))
+        if is3d:
+            c = annulus3d(ni=ni, nj=nj, nk=nk, cfl=2.2, scheme="JST", muscl=False, limiter="None", rk=4,
+                          p_ratio=pr, rows=MAP_ROWS, speed=sp, drop=3, ramp=2000, precision=precision,
+                          n_iter=40000, name=f"req{m:04d}")
+        else:
+            c = meridional(ni=ni, nj=nj, n_iter=40000, p_ratio=pr, speed=sp, cfl=2.2, drop=3,
+                           name=f"req{m:04d}", rows=MAP_ROWS, ramp=2000, precision=precision)
+        out.append((t, c))
     return out
 
 

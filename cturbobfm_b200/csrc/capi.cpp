@@ -6,7 +6,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -15,6 +17,7 @@
 #include "host/batch.hpp"
 #include "host/config.hpp"
 #include "host/mesh.hpp"
+#include "host/server.hpp"
 #include "host/solver.hpp"
 
 struct ctbfm_solver {
@@ -25,6 +28,11 @@ struct ctbfm_solver {
 
 struct ctbfm_batch {
     std::unique_ptr<ctbfm::Batch> batch;
+};
+
+struct ctbfm_server {
+    std::unique_ptr<ctbfm::Server> server;
+    std::vector<ctbfm::ServerResult> pending;  // taken from the server, not yet returned
 };
 
 namespace {
@@ -120,6 +128,7 @@ int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out) {
         out->status = c.status;
         out->precision = s->solver->precision();
         out->time = c.t;
+        out->device_bytes = static_cast<int64_t>(s->solver->deviceBytes());
         return CTBFM_OK;
     });
 }
@@ -293,6 +302,80 @@ int ctbfm_promote_fp64(ctbfm_solver* s) {
     if (!s) return setError(CTBFM_E_ARGUMENT, "null solver");
     return guarded([&] {
         s->solver->promoteToFP64();
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t chunk_iterations,
+                        int64_t stall_window, int32_t host_threads, ctbfm_server** out) {
+    if (!out) return setError(CTBFM_E_ARGUMENT, "null argument");
+    *out = nullptr;
+    return guarded([&] {
+        ctbfm::ServerOptions o;
+        o.budget_bytes = static_cast<size_t>(device_budget_bytes);
+        o.max_active = max_active;
+        o.chunk = chunk_iterations;
+        o.stall_window = stall_window;
+        o.host_threads = host_threads;
+        auto s = std::make_unique<ctbfm_server>();
+        s->server = std::make_unique<ctbfm::Server>(o);
+        *out = s.release();
+        return CTBFM_OK;
+    });
+}
+
+void ctbfm_server_destroy(ctbfm_server* s) {
+    if (!s) return;
+    try {
+        delete s;
+    } catch (...) {
+    }
+}
+
+int ctbfm_server_submit(ctbfm_server* s, const char* ini_path, int64_t* request_id) {
+    if (!s || !ini_path) return setError(CTBFM_E_ARGUMENT, "null argument");
+    return guarded([&] {
+        const long long id = s->server->submit(ini_path);
+        if (request_id) *request_id = id;
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_server_pump(ctbfm_server* s, int32_t* n_active, int32_t* n_waiting) {
+    if (!s) return setError(CTBFM_E_ARGUMENT, "null server");
+    return guarded([&] {
+        int a = 0, w = 0;
+        s->server->pump(&a, &w);
+        if (n_active) *n_active = a;
+        if (n_waiting) *n_waiting = w;
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_server_results(ctbfm_server* s, ctbfm_result* out, int32_t max, int32_t* n_out) {
+    if (!s || (!out && max > 0) || max < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
+    return guarded([&] {
+        for (auto& r : s->server->take()) s->pending.push_back(std::move(r));
+        const int32_t n = std::min<int32_t>(max, static_cast<int32_t>(s->pending.size()));
+        for (int32_t i = 0; i < n; i++) {
+            const ctbfm::ServerResult& r = s->pending[i];
+            ctbfm_result& o = out[i];
+            o.id = r.id;
+            o.status = r.status;
+            o.precision = r.precision;
+            o.iterations = r.iterations;
+            o.t_submit = r.t_submit;
+            o.t_admit = r.t_admit;
+            o.t_done = r.t_done;
+            for (int b = 0; b < 6; b++) o.massflow[b] = r.massflow[b];
+            for (int b = 0; b < 4; b++) o.turbo[b] = r.turbo[b];
+            o.error = r.error;
+            const size_t len = std::min(r.message.size(), sizeof(o.message) - 1);
+            std::memcpy(o.message, r.message.data(), len);
+            o.message[len] = 0;
+        }
+        s->pending.erase(s->pending.begin(), s->pending.begin() + n);
+        if (n_out) *n_out = n;
         return CTBFM_OK;
     });
 }

@@ -1,0 +1,247 @@
+// Server: see server.hpp.
+#include "server.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+
+namespace ctbfm {
+
+namespace {
+double steadySeconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+Server::Server(const ServerOptions& o) : opt_(o), t0_(steadySeconds()) {
+    if (opt_.chunk <= 0) throw std::invalid_argument("chunk must be positive");
+    if (opt_.max_active <= 0) throw std::invalid_argument("max_active must be positive");
+    if (opt_.stall_window < 0) throw std::invalid_argument("stall_window must be >= 0");
+    const int nt = std::max(1, opt_.host_threads);
+    for (int t = 0; t < nt; t++) workers_.emplace_back([this] { worker(); });
+}
+
+Server::~Server() {
+    {
+        std::lock_guard<std::mutex> l(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& w : workers_) w.join();
+    b32_.reset();
+    b64_.reset();
+    active_.clear();
+}
+
+double Server::now() const { return steadySeconds() - t0_; }
+
+long long Server::submit(const std::string& iniPath) {
+    auto j = std::make_unique<Job>();
+    j->ini = iniPath;
+    j->t_submit = now();
+    std::lock_guard<std::mutex> l(mu_);
+    j->id = nextId_++;
+    prep_.push_back(j.get());
+    const long long id = j->id;
+    queue_.push_back(std::move(j));
+    cv_.notify_one();
+    return id;
+}
+
+// Host preparation: the Config and Mesh constructors (input file, grid, dual
+// grid, metrics, blockage gradient). No CUDA call happens here.
+void Server::worker() {
+    while (true) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> l(mu_);
+            cv_.wait(l, [this] { return stop_ || !prep_.empty(); });
+            if (stop_) return;
+            j = prep_.front();
+            prep_.pop_front();
+        }
+        std::unique_ptr<Config> cfg;
+        std::unique_ptr<Mesh> mesh;
+        int err = 0;
+        std::string msg;
+        try {
+            cfg = std::make_unique<Config>(j->ini);
+            mesh = std::make_unique<Mesh>(*cfg);
+        } catch (const std::exception& e) {
+            err = 1;  // CTBFM_E_CONFIG
+            msg = e.what();
+        }
+        std::lock_guard<std::mutex> l(mu_);
+        j->config = std::move(cfg);
+        j->mesh = std::move(mesh);
+        j->error = err;
+        j->message = msg;
+        j->nodes = j->mesh ? static_cast<long long>(j->mesh->nodes()) : 0;
+        j->prepared = true;
+    }
+}
+
+size_t Server::estimate(const Job& j) const {
+    const bool f32 = j.config && j.config->has("GPU_PRECISION") && j.config->get("GPU_PRECISION") == "fp32_kahan";
+    const double per = bytesPerNode_[f32 ? 1 : 0] > 0 ? bytesPerNode_[f32 ? 1 : 0] : (f32 ? 700.0 : 1200.0);
+    return static_cast<size_t>(per * static_cast<double>(j.nodes) * 1.05) + (size_t(1) << 20);
+}
+
+void Server::retire(std::unique_ptr<Job> job, const Control* ctl, int error, const std::string& msg) {
+    ServerResult r;
+    r.id = job->id;
+    r.t_submit = job->t_submit;
+    r.t_admit = job->t_admit;
+    r.error = error;
+    r.message = msg;
+    if (job->solver && ctl) {
+        r.status = ctl->status;
+        r.iterations = ctl->it;
+        r.precision = job->solver->precision();
+        try {
+            job->solver->getTurbo(r.massflow, r.turbo);
+        } catch (const std::exception& e) {
+            r.error = 2;  // CTBFM_E_CUDA
+            r.message = e.what();
+        }
+    }
+    job.reset();  // releases the solve's device memory
+    r.t_done = now();
+    done_.push_back(std::move(r));
+}
+
+void Server::rebuild() {
+    b32_.reset();
+    b64_.reset();
+    idx32_.clear();
+    idx64_.clear();
+    std::vector<Solver*> m32, m64;
+    for (size_t i = 0; i < active_.size(); i++) {
+        Solver* s = active_[i]->solver.get();
+        if (s->precision() == kFP32Kahan) {
+            m32.push_back(s);
+            idx32_.push_back(static_cast<int>(i));
+        } else {
+            m64.push_back(s);
+            idx64_.push_back(static_cast<int>(i));
+        }
+    }
+    if (!m32.empty()) b32_ = std::make_unique<Batch>(m32);
+    if (!m64.empty()) b64_ = std::make_unique<Batch>(m64);
+    dirty_ = false;
+}
+
+void Server::pump(int* nActive, int* nWaiting) {
+    // 1. admission, in arrival order, while slots and device memory allow
+    while (true) {
+        std::unique_ptr<Job> j;
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            if (queue_.empty() || !queue_.front()->prepared) break;
+            if (queue_.front()->error == 0) {
+                if (static_cast<int>(active_.size()) >= opt_.max_active) break;
+                const size_t need = estimate(*queue_.front());
+                size_t budget = opt_.budget_bytes;
+                if (budget == 0) {
+                    size_t freeB = 0, totalB = 0;
+                    cudaCheck(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
+                    budget = used_ + freeB * 9 / 10;
+                }
+                if (used_ + need > budget && !active_.empty()) break;
+            }
+            j = std::move(queue_.front());
+            queue_.pop_front();
+        }
+        if (j->error) {
+            const int err = j->error;
+            const std::string msg = j->message;
+            retire(std::move(j), nullptr, err, msg);
+            continue;
+        }
+        try {
+            j->solver = std::make_unique<Solver>(*j->config, *j->mesh);
+        } catch (const ConfigError& e) {
+            const std::string msg = e.what();
+            retire(std::move(j), nullptr, 1, msg);
+            continue;
+        } catch (const CudaError& e) {
+            const std::string msg = e.what();
+            retire(std::move(j), nullptr, 2, msg);
+            continue;
+        }
+        j->bytes = j->solver->deviceBytes();
+        const int p = j->solver->precision() == kFP32Kahan ? 1 : 0;
+        if (bytesPerNode_[p] == 0 && j->nodes > 0)
+            bytesPerNode_[p] = static_cast<double>(j->bytes) / static_cast<double>(j->nodes);
+        used_ += j->bytes;
+        j->t_admit = now();
+        active_.push_back(std::move(j));
+        dirty_ = true;
+    }
+    // 2. one chunk of iterations for every admitted solve; the two precision
+    //    groups run on their own streams and overlap on the device
+    if (!active_.empty()) {
+        if (dirty_) rebuild();
+        if (b32_) b32_->enqueue(opt_.chunk);
+        if (b64_) b64_->enqueue(opt_.chunk);
+        std::vector<Control> ctl(active_.size());
+        std::vector<Control> tmp;
+        if (b32_) {
+            tmp.resize(idx32_.size());
+            b32_->controls(tmp.data());
+            for (size_t m = 0; m < idx32_.size(); m++) ctl[idx32_[m]] = tmp[m];
+        }
+        if (b64_) {
+            tmp.resize(idx64_.size());
+            b64_->controls(tmp.data());
+            for (size_t m = 0; m < idx64_.size(); m++) ctl[idx64_[m]] = tmp[m];
+        }
+        // 3. retire finished solves, promote stalled float solves
+        std::vector<std::unique_ptr<Job>> keep;
+        std::vector<size_t> promote;
+        for (size_t i = 0; i < active_.size(); i++) {
+            const Control& c = ctl[i];
+            auto& j = active_[i];
+            if (c.status != 0 || c.it >= j->solver->maxIterations()) {
+                if (!dirty_) {
+                    b32_.reset();
+                    b64_.reset();
+                    dirty_ = true;
+                }
+                used_ -= std::min(used_, j->bytes);
+                retire(std::move(j), &c, 0, "");
+                continue;
+            }
+            if (opt_.stall_window > 0 && j->solver->precision() == kFP32Kahan && c.it - c.it_best >= opt_.stall_window)
+                promote.push_back(keep.size());
+            keep.push_back(std::move(j));
+        }
+        active_ = std::move(keep);
+        if (!promote.empty()) {
+            b32_.reset();
+            b64_.reset();
+            for (size_t k : promote) {
+                auto& j = active_[k];
+                used_ -= std::min(used_, j->bytes);
+                j->solver->promoteToFP64();
+                j->bytes = j->solver->deviceBytes();
+                used_ += j->bytes;
+            }
+            dirty_ = true;
+        }
+    }
+    if (nActive) *nActive = static_cast<int>(active_.size());
+    if (nWaiting) {
+        std::lock_guard<std::mutex> l(mu_);
+        *nWaiting = static_cast<int>(queue_.size());
+    }
+}
+
+std::vector<ServerResult> Server::take() {
+    std::vector<ServerResult> out;
+    out.swap(done_);
+    return out;
+}
+
+}  // namespace ctbfm

@@ -1,0 +1,100 @@
+// Server: continuous batching of operating-point solves. The reference runs
+// one process per operating point to the end (python/Run_All_Cases.py:18-98);
+// here requests arrive at any time, are prepared on host worker threads
+// (input parsing, grid metrics), admitted in arrival order while device
+// memory and slots allow, advance together with every other admitted solve
+// (one Batch per working precision, each on its own stream, so FP32 and FP64
+// work overlaps), and retire the moment they converge, diverge or reach
+// N_ITERATIONS. A fp32_kahan solve whose convergence progress stalls for
+// stall_window iterations continues in FP64.
+#pragma once
+
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "batch.hpp"
+#include "config.hpp"
+#include "mesh.hpp"
+#include "solver.hpp"
+
+namespace ctbfm {
+
+struct ServerResult {
+    long long id = 0;
+    int status = -1;  // CTBFM_STATUS_*, -1 when the request failed before running
+    int precision = 0;
+    long long iterations = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;  // seconds since the server started
+    double massflow[6] = {0, 0, 0, 0, 0, 0};
+    double turbo[4] = {0, 0, 0, 0};
+    int error = 0;  // CTBFM_OK or the request's error code
+    std::string message;
+};
+
+struct ServerOptions {
+    size_t budget_bytes = 0;      // device memory the admitted solves may hold (0: 90 % of free)
+    int max_active = 1024;        // admitted solves at most
+    long long chunk = 200;        // iterations between scheduling rounds
+    long long stall_window = 0;   // fp32_kahan -> FP64 after this many iterations without progress (0: never)
+    int host_threads = 4;         // workers preparing requests
+};
+
+class Server {
+public:
+    explicit Server(const ServerOptions& o);
+    ~Server();
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    // Queues a request (thread safe); its host preparation starts at once.
+    long long submit(const std::string& iniPath);
+    // One scheduling round: admit, advance every admitted solve by `chunk`
+    // iterations, retire and promote. Returns after the GPU work of the round.
+    void pump(int* active, int* waiting);
+    // Requests finished since the last call.
+    std::vector<ServerResult> take();
+    double now() const;
+
+private:
+    struct Job {
+        long long id = 0;
+        std::string ini;
+        double t_submit = 0, t_admit = 0;
+        bool prepared = false;
+        int error = 0;
+        std::string message;
+        long long nodes = 0;
+        std::unique_ptr<Config> config;
+        std::unique_ptr<Mesh> mesh;
+        std::unique_ptr<Solver> solver;  // declared last: released before the mesh and config it refers to
+        size_t bytes = 0;
+    };
+    void worker();
+    void rebuild();
+    void retire(std::unique_ptr<Job> job, const Control* ctl, int error, const std::string& msg);
+    size_t estimate(const Job& j) const;
+
+    ServerOptions opt_;
+    double t0_ = 0;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<Job*> prep_;                   // awaiting a worker
+    std::deque<std::unique_ptr<Job>> queue_;  // submitted, in arrival order
+    std::vector<std::thread> workers_;
+    bool stop_ = false;
+    long long nextId_ = 1;
+    std::vector<std::unique_ptr<Job>> active_;
+    std::unique_ptr<Batch> b64_, b32_;
+    std::vector<int> idx64_, idx32_;  // active_ index of each batch member
+    bool dirty_ = false;
+    size_t used_ = 0;
+    double bytesPerNode_[2] = {0, 0};  // measured per precision (0: not yet)
+    std::vector<ServerResult> done_;
+};
+
+}  // namespace ctbfm

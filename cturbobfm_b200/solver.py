@@ -51,6 +51,23 @@ class Info(ctypes.Structure):
         ("status", ctypes.c_int32),
         ("precision", ctypes.c_int32),
         ("time", ctypes.c_double),
+        ("device_bytes", ctypes.c_int64),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_int64),
+        ("status", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("iterations", ctypes.c_int64),
+        ("t_submit", ctypes.c_double),
+        ("t_admit", ctypes.c_double),
+        ("t_done", ctypes.c_double),
+        ("massflow", ctypes.c_double * 6),
+        ("turbo", ctypes.c_double * 4),
+        ("error", ctypes.c_int32),
+        ("message", ctypes.c_char * 240),
     ]
 
 
@@ -83,6 +100,13 @@ SIGNATURES = {
     "ctbfm_batch_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_batch_status": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_I64), _DP, _DP], ctypes.c_int),
     "ctbfm_promote_fp64": ([_VP], ctypes.c_int),
+    "ctbfm_server_create": ([ctypes.c_uint64, ctypes.c_int32, _I64, _I64, ctypes.c_int32, ctypes.POINTER(_VP)],
+                            ctypes.c_int),
+    "ctbfm_server_destroy": ([_VP], None),
+    "ctbfm_server_submit": ([_VP, ctypes.c_char_p, ctypes.POINTER(_I64)], ctypes.c_int),
+    "ctbfm_server_pump": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "ctbfm_server_results": ([_VP, ctypes.POINTER(Result), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
+                             ctypes.c_int),
     "ctbfm_last_error": ([], ctypes.c_char_p),
     "ctbfm_version": ([], ctypes.c_char_p),
 }
@@ -288,3 +312,53 @@ class Batch:
         _check(load_library().ctbfm_batch_status(self._h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                                  it.ctypes.data_as(ctypes.POINTER(_I64)), _ptr(ln), _ptr(bd)))
         return {"status": st, "iterations": it, "lognorm": ln, "best_drop": bd}
+
+
+class Server:
+    """Continuous batching of operating-point solves (ctbfm_server_*)."""
+
+    def __init__(self, budget_bytes: int = 0, max_active: int = 1024, chunk: int = 200, stall_window: int = 0,
+                 host_threads: int = 4):
+        h = _VP()
+        _check(load_library().ctbfm_server_create(int(budget_bytes), int(max_active), int(chunk), int(stall_window),
+                                                  int(host_threads), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().ctbfm_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, ini_path: str) -> int:
+        rid = _I64(0)
+        _check(load_library().ctbfm_server_submit(self._h, os.path.abspath(ini_path).encode(), ctypes.byref(rid)))
+        return int(rid.value)
+
+    def pump(self):
+        a, w = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(load_library().ctbfm_server_pump(self._h, ctypes.byref(a), ctypes.byref(w)))
+        return int(a.value), int(w.value)
+
+    def results(self, max_results: int = 4096):
+        buf = (Result * max_results)()
+        n = ctypes.c_int32(0)
+        _check(load_library().ctbfm_server_results(self._h, buf, max_results, ctypes.byref(n)))
+        out = []
+        for r in buf[: n.value]:
+            out.append({"id": r.id, "status": r.status, "precision": r.precision, "iterations": r.iterations,
+                        "t_submit": r.t_submit, "t_admit": r.t_admit, "t_done": r.t_done,
+                        "massflow": list(r.massflow), "turbo": list(r.turbo), "error": r.error,
+                        "message": r.message.decode(errors="replace")})
+        return out

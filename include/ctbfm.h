@@ -68,6 +68,7 @@ typedef struct {
     int32_t status;           /* CTBFM_STATUS_* */
     int32_t precision;        /* GPU_PRECISION: 0 = fp64, 1 = fp32_kahan */
     double time;              /* physical time sum of min(dt) */
+    int64_t device_bytes;     /* device memory the solver holds */
 } ctbfm_info;
 
 /* Builds a solver from an input.ini in the reference's format (the grid CSV and
@@ -202,6 +203,52 @@ int ctbfm_batch_status(ctbfm_batch* b, int32_t* status, int64_t* iterations, dou
  * no-op for FP64 solvers. A batch holding the solver must be destroyed
  * first. No counterpart in the reference (FP64 only). */
 int ctbfm_promote_fp64(ctbfm_solver* s);
+
+/* ------------------------------------------------------------------------
+ * Serving: continuous batching of operating-point solves. No counterpart in
+ * the reference (one process per operating point, run to the end). Requests
+ * are prepared on host worker threads, admitted in arrival order while slots
+ * and device memory allow, advance together with every other admitted solve
+ * (one batch per GPU_PRECISION, each on its own stream), and retire as soon
+ * as they converge, diverge or reach N_ITERATIONS. Each solve's state, BFM
+ * fields and plenum state stay on the device from admission to retirement.
+ * ------------------------------------------------------------------------ */
+typedef struct ctbfm_server ctbfm_server;
+
+typedef struct {
+    int64_t id;
+    int32_t status;      /* CTBFM_STATUS_*, -1 when the request failed before running */
+    int32_t precision;   /* precision the solve finished in (0 fp64, 1 fp32_kahan) */
+    int64_t iterations;
+    double t_submit;     /* seconds since the server was created */
+    double t_admit;
+    double t_done;
+    double massflow[6];  /* as ctbfm_get_turbo */
+    double turbo[4];
+    int32_t error;       /* CTBFM_OK or the request's error code */
+    char message[240];   /* error message, truncated */
+} ctbfm_result;
+
+/* device_budget_bytes: device memory the admitted solves may hold (0: 90 % of
+ * what is free at each admission); max_active: admitted solves at most;
+ * chunk_iterations: iterations per scheduling round; stall_window: a
+ * fp32_kahan solve whose convergence progress (best_drop of
+ * ctbfm_batch_status) has not grown by 0.05 for this many iterations
+ * continues in FP64 (0: never); host_threads: request-preparation workers. */
+int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t chunk_iterations,
+                        int64_t stall_window, int32_t host_threads, ctbfm_server** out);
+void ctbfm_server_destroy(ctbfm_server* s);
+
+/* Queues the operating point of an input.ini; thread safe. */
+int ctbfm_server_submit(ctbfm_server* s, const char* ini_path, int64_t* request_id);
+
+/* One scheduling round on the calling thread (admit, advance every admitted
+ * solve by chunk_iterations, retire, promote). n_active / n_waiting
+ * (nullable) receive the counts after the round. */
+int ctbfm_server_pump(ctbfm_server* s, int32_t* n_active, int32_t* n_waiting);
+
+/* Moves up to max finished requests into out; *n_out receives how many. */
+int ctbfm_server_results(ctbfm_server* s, ctbfm_result* out, int32_t max, int32_t* n_out);
 
 /* Message of the calling thread's last error ("" if none). */
 const char* ctbfm_last_error(void);

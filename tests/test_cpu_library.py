@@ -6,6 +6,7 @@ before any device work."""
 import ctypes
 import os
 import re
+import time
 
 import pytest
 
@@ -84,3 +85,25 @@ def test_null_arguments(lib):
     assert lib.ctbfm_batch_create(arr, 2, ctypes.byref(out)) == 4
     assert out.value is None
     lib.ctbfm_batch_destroy(None)
+    assert lib.ctbfm_server_submit(None, b"x", None) == 4
+    assert lib.ctbfm_server_pump(None, None, None) == 4
+    assert lib.ctbfm_server_results(None, None, 0, None) == 4
+    lib.ctbfm_server_destroy(None)
+
+
+def test_server_reports_a_bad_request_without_device_work(lib, tmp_path):
+    from cturbobfm_b200 import Server
+
+    with Server(chunk=10, host_threads=2) as s:
+        rid = s.submit(str(tmp_path / "missing" / "input.ini"))
+        res = []
+        for _ in range(2000):
+            active, waiting = s.pump()
+            res += s.results()
+            if res:
+                break
+            time.sleep(0.005)
+        assert active == 0 and waiting == 0
+    assert len(res) == 1 and res[0]["id"] == rid
+    assert res[0]["error"] == 1 and res[0]["status"] == -1
+    assert res[0]["message"]

@@ -1,0 +1,114 @@
+"""Serving (ctbfm_server_*): requests arriving while others run are admitted
+into the running batches, and each result is the same alone and in the mix
+(bit for bit: every member computes on its own, and scheduling decisions
+depend only on the member's own iteration count)."""
+
+import os
+
+import numpy as np
+import pytest
+
+from cturbobfm_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _req(name, ni, nj, pr, sp, prec="fp32_kahan", drop=3):
+    return cases.meridional(ni=ni, nj=nj, p_ratio=pr, speed=sp, cfl=2.2, drop=drop, rows=cases.MAP_ROWS,
+                            ramp=2000, precision=prec, n_iter=20000, name=name)
+
+
+def _write(c, root):
+    d = os.path.join(root, c.name)
+    os.makedirs(d)
+    return c.write(d)
+
+
+def _drain(server, expect):
+    out = {}
+    for _ in range(10000):
+        server.pump()
+        for r in server.results():
+            out[r["id"]] = r
+        if len(out) == expect:
+            return out
+    raise AssertionError("server did not finish")
+
+
+def test_results_are_the_same_alone_and_in_the_mix(tmp_path):
+    from cturbobfm_b200 import Server, Solver
+
+    a = _write(_req("a", 64, 24, 1.05, 0.95), str(tmp_path))
+    others = [_write(_req("b", 96, 32, 1.1, 0.9), str(tmp_path)),
+              _write(_req("c", 80, 28, 1.0, 1.0, prec="fp64"), str(tmp_path)),
+              _write(_req("d", 72, 40, 1.15, 0.92), str(tmp_path)),
+              _write(cases.bump2d(ni=48, nj=16, n_iter=3000, name="e").with_settings(GPU_PRECISION="fp32_kahan"),
+                     str(tmp_path))]
+    with Server(chunk=100) as s:
+        ida = s.submit(a)
+        alone = _drain(s, 1)[ida]
+    assert alone["status"] == 1 and alone["error"] == 0
+    # the same operating point on the plain drop-in path
+    with Solver(a) as p:
+        p.solve()
+        assert p.status == 1
+        assert p.iteration == alone["iterations"]
+        assert np.array_equal(p.turbo()[1], np.array(alone["turbo"]))
+    # in the mix: two requests first, A after two rounds, the rest later
+    with Server(chunk=100) as s:
+        ids = [s.submit(others[0]), s.submit(others[1])]
+        s.pump()
+        s.pump()
+        ida = s.submit(a)
+        s.pump()
+        ids += [s.submit(others[2]), s.submit(others[3])]
+        res = _drain(s, 5)
+    mixed = res[ida]
+    assert mixed["status"] == alone["status"]
+    assert mixed["iterations"] == alone["iterations"]
+    assert mixed["turbo"] == alone["turbo"] and mixed["massflow"] == alone["massflow"]
+    assert all(res[i]["error"] == 0 for i in ids)
+    assert res[ids[1]]["precision"] == 0  # the fp64 request stays fp64
+    assert all(r["t_admit"] >= r["t_submit"] and r["t_done"] >= r["t_admit"] for r in res.values())
+
+
+def test_budget_admits_one_solve_at_a_time(tmp_path):
+    from cturbobfm_b200 import Server, Solver
+
+    inis = [_write(_req(f"r{m}", 64, 24, 1.0 + 0.05 * m, 0.95), str(tmp_path)) for m in range(3)]
+    with Solver(inis[0]) as p:
+        one = int(p.info().device_bytes)
+    with Server(budget_bytes=int(one * 1.5), chunk=200) as s:
+        ids = [s.submit(i) for i in inis]
+        res = _drain(s, 3)
+    order = sorted(res.values(), key=lambda r: r["t_admit"])
+    assert [r["id"] for r in order] == ids  # arrival order
+    for prev, nxt in zip(order, order[1:]):
+        assert nxt["t_admit"] >= prev["t_done"]  # admitted only once the previous solve left
+
+
+def test_stalled_fp32_solve_continues_in_fp64_deterministically(tmp_path):
+    from cturbobfm_b200 import Server
+
+    ini = _write(_req("s", 64, 24, 1.05, 0.95), str(tmp_path))
+    out = []
+    for _ in range(2):
+        with Server(chunk=50, stall_window=50) as s:
+            rid = s.submit(ini)
+            out.append(_drain(s, 1)[rid])
+    assert out[0]["precision"] == 0  # promoted
+    assert out[0]["status"] == 1
+    assert out[0] == {**out[1], "t_submit": out[0]["t_submit"], "t_admit": out[0]["t_admit"],
+                      "t_done": out[0]["t_done"], "id": out[0]["id"]}
+
+
+def test_a_bad_request_fails_alone(tmp_path):
+    from cturbobfm_b200 import Server
+
+    good = _write(_req("g", 64, 24, 1.05, 0.95), str(tmp_path))
+    with Server(chunk=200) as s:
+        bad = s.submit(str(tmp_path / "missing" / "input.ini"))
+        ok = s.submit(good)
+        res = _drain(s, 2)
+    assert res[bad]["error"] == 1 and res[bad]["status"] == -1
+    assert res[ok]["error"] == 0 and res[ok]["status"] == 1
