@@ -72,6 +72,9 @@ class Case:
     fields: Dict[str, np.ndarray]
     patches: List[Patch]
     settings: Dict[str, str]
+    # keyword arguments of fluid_table.write for FLUID_MODEL = real (the table
+    # is written next to input.ini under FLUID_TABLE_FILE)
+    table: Optional[Dict] = None
 
     @property
     def shape(self) -> Tuple[int, int, int]:
@@ -114,6 +117,10 @@ class Case:
         settings["BOUNDARY_CONDITIONS_FILEPATH"] = "boundaries.csv"
         for p in self.patches:
             settings[p.name] = p.spec
+        if self.table is not None:
+            from . import fluid_table
+
+            fluid_table.write(os.path.join(directory, settings["FLUID_TABLE_FILE"]), **self.table)
         ini = os.path.join(directory, "input.ini")
         with open(ini, "w") as f:
             f.write("[CFD]\n")
@@ -421,6 +428,29 @@ def serving_requests(n: int, rate: float, seed: int = 20261203, frac_3d: float =
                            name=f"req{m:04d}", rows=MAP_ROWS, ramp=2000, precision=precision)
         out.append((t, c))
     return out
+
+
+def with_real_gas(case: Case, pt: float, tt: float, p_init: float, t_init: float, p_out: Optional[float] = None,
+                  table: Optional[Dict] = None) -> Case:
+    """The same operating point in FLUID_MODEL = real with the synthetic CO2
+    table of fluid_table (1e5-1e7 Pa, 200-600 K, 60 x 60 per section unless
+    `table` says otherwise): inlet total conditions (pt, tt), initial static
+    state (p_init, t_init), outlet static pressure p_out (default p_init)."""
+    s = dict(case.settings)
+    s.update({"FLUID_MODEL": "real", "FLUID_NAME": "CO2", "FLUID_TABLE_FILE": "fluid_table_CO2.lut",
+              "INIT_PRESSURE": f"{p_init!r}", "INIT_TEMPERATURE": f"{t_init!r}"})
+    for k in ("FLUID_GAMMA", "FLUID_R_CONSTANT"):
+        s.pop(k, None)
+    patches = []
+    for p in case.patches:
+        kind = p.kind
+        if kind == "inlet":
+            rest = p.spec.split(",")[3:]
+            p = dataclasses.replace(p, spec=", ".join([f"inlet, {pt!r}, {tt!r}"] + [r.strip() for r in rest]))
+        elif kind in ("outlet", "radial_equilibrium"):
+            p = dataclasses.replace(p, spec=f"{kind}, {(p_init if p_out is None else p_out)!r}")
+        patches.append(p)
+    return dataclasses.replace(case, settings=s, patches=patches, table=dict(table or {}))
 
 
 def read_grid_csv(path: str) -> Tuple[Tuple[int, int, int], Dict[str, np.ndarray]]:

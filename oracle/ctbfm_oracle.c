@@ -263,6 +263,9 @@ struct oracle_solver {
     int turbo_dir; /* bcIndices pair */
     int greitzer;
     double plenum_volume, ambient_p, gz_p, gz_min, gz_mout, gz_T, gz_t, throttle_kt;
+    /* FLUID_MODEL = real: the look-up table of FluidReal */
+    int real;
+    struct lut_s* lut;
     /* mesh */
     vec3* vert;  /* n */
     vec3* dual;  /* (ni+1)(nj+1)(nk+1) */
@@ -323,10 +326,192 @@ static void res_sub(oracle_solver* s, long i, long j, long k, sv5 d) {
     for (int c = 0; c < 5; c++) s->R[c][q] -= d.v[c];
 }
 
+/* ------------------------------------------------------- real-gas tables */
+/* Table2D (include/fluid_real.hpp:11-58): uniform grid, clamped bilinear
+ * interpolation, data[i * ny + j]. */
+typedef struct {
+    long nx, ny;
+    double xmin, xmax, ymin, ymax, dx, dy;
+    double* d;
+} table2d;
+
+static void table_init(table2d* t, long nx, long ny, double x0, double x1, double y0, double y1) {
+    t->nx = nx; t->ny = ny; t->xmin = x0; t->xmax = x1; t->ymin = y0; t->ymax = y1;
+    t->dx = (nx > 1) ? (x1 - x0) / (double)(nx - 1) : 1.0;
+    t->dy = (ny > 1) ? (y1 - y0) / (double)(ny - 1) : 1.0;
+    free(t->d);
+    t->d = (double*)calloc((size_t)(nx * ny > 0 ? nx * ny : 1), sizeof(double));
+}
+
+static double clampd(double v, double lo, double hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); } /* std::clamp */
+
+static double table_interp(const table2d* t, double x, double y) {
+    double xc = clampd(x, t->xmin, t->xmax);
+    double yc = clampd(y, t->ymin, t->ymax);
+    double rx = (xc - t->xmin) / t->dx;
+    double ry = (yc - t->ymin) / t->dy;
+    /* size_t conversion; a NaN coordinate lands on the last cell either way */
+    unsigned long i = (rx >= 0.0 && rx < 1e18) ? (unsigned long)rx : (unsigned long)t->nx;
+    unsigned long j = (ry >= 0.0 && ry < 1e18) ? (unsigned long)ry : (unsigned long)t->ny;
+    if (i >= (unsigned long)(t->nx - 1)) i = (t->nx >= 2) ? (unsigned long)(t->nx - 2) : 0;
+    if (j >= (unsigned long)(t->ny - 1)) j = (t->ny >= 2) ? (unsigned long)(t->ny - 2) : 0;
+    double wx = rx - (double)i;
+    double wy = ry - (double)j;
+    double f00 = t->d[i * t->ny + j];
+    double f10 = t->d[(i + 1) * t->ny + j];
+    double f01 = t->d[i * t->ny + (j + 1)];
+    double f11 = t->d[(i + 1) * t->ny + (j + 1)];
+    return (1.0 - wx) * (1.0 - wy) * f00 + wx * (1.0 - wy) * f10 + (1.0 - wx) * wy * f01 + wx * wy * f11;
+}
+
+typedef struct lut_s {
+    double molar, R, pcrit, Tcrit, rhocrit, gnom;
+    table2d p, T, a, s, mu, kappa, dpdrho, dpde; /* (rho, e) */
+    table2d rho_pt, e_pt, a_pt, s_pt;           /* (p, T) */
+    table2d rho_ps, T_ps, e_ps;                 /* (p, s) */
+} lut;
+
+static void lut_free(lut* L) {
+    if (!L) return;
+    table2d* all[15] = {&L->p, &L->T, &L->a, &L->s, &L->mu, &L->kappa, &L->dpdrho, &L->dpde,
+                        &L->rho_pt, &L->e_pt, &L->a_pt, &L->s_pt, &L->rho_ps, &L->T_ps, &L->e_ps};
+    for (int q = 0; q < 15; q++) free(all[q]->d);
+    free(L);
+}
+
+/* splits "KEY: value" with the reference's trimming; returns 0 without ':' */
+static int lut_keyval(const char* line, char* key, size_t nk, char* val, size_t nv) {
+    const char* colon = strchr(line, ':');
+    if (!colon) return 0;
+    size_t kl = (size_t)(colon - line);
+    if (kl >= nk) kl = nk - 1;
+    memcpy(key, line, kl);
+    key[kl] = 0;
+    trim(key, " \t\r\n");
+    snprintf(val, nv, "%s", colon + 1);
+    trim(val, " \t\r\n");
+    return 1;
+}
+
+/* reads the next data line (skipping empty, '#' and '\r' lines) into v[n] */
+static int lut_row(FILE* f, char* line, size_t cap, double* v, int n) {
+    do {
+        if (!fgets(line, (int)cap, f)) return 1;
+    } while (line[0] == '\n' || line[0] == '#' || line[0] == '\r' || line[0] == 0);
+    char* p = line;
+    for (int q = 0; q < n; q++) {
+        char* e = NULL;
+        v[q] = strtod(p, &e);
+        if (e == p) v[q] = 0.0;
+        p = e;
+    }
+    return 0;
+}
+
+/* FluidReal::loadTable (src/fluid_real.cpp:12-208). */
+static int lut_load(lut* L, const char* path) {
+    FILE* f = fopen(path, "r");
+    if (!f) return fail("FluidReal: Could not open table file at: %s", path);
+    L->R = 287.0; L->gnom = 1.3;
+    char line[4096], key[256], val[1024];
+    int sec = 0; /* 1 RHO_E, 2 P_T, 3 P_S */
+    long n1 = 0, n2 = 0;
+    double x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+    while (fgets(line, sizeof line, f)) {
+        size_t len = strlen(line);
+        if (len && line[len - 1] == '\n') line[--len] = 0;
+        if (len == 0 || line[0] == '\r') continue;
+        if (strstr(line, "# SECTION: RHO_E")) { sec = 1; continue; }
+        if (strstr(line, "# SECTION: P_T")) { sec = 2; continue; }
+        if (strstr(line, "# SECTION: P_S")) { sec = 3; continue; }
+        if (line[0] == '#') continue;
+        if (!lut_keyval(line, key, sizeof key, val, sizeof val)) continue;
+        if (sec == 0) {
+            if (!strcmp(key, "MOLAR_MASS")) L->molar = strtod(val, NULL);
+            else if (!strcmp(key, "GAS_CONSTANT")) L->R = strtod(val, NULL);
+            else if (!strcmp(key, "CRITICAL_PRESSURE")) L->pcrit = strtod(val, NULL);
+            else if (!strcmp(key, "CRITICAL_TEMPERATURE")) L->Tcrit = strtod(val, NULL);
+            else if (!strcmp(key, "CRITICAL_DENSITY")) L->rhocrit = strtod(val, NULL);
+            else if (!strcmp(key, "NOMINAL_GAMMA")) L->gnom = strtod(val, NULL);
+            continue;
+        }
+        const char* kn1 = sec == 1 ? "N_RHO" : "N_P";
+        const char* kn2 = sec == 1 ? "N_E" : (sec == 2 ? "N_T" : "N_S");
+        const char* kx0 = sec == 1 ? "RHO_MIN" : "P_MIN";
+        const char* kx1 = sec == 1 ? "RHO_MAX" : "P_MAX";
+        const char* ky0 = sec == 1 ? "E_MIN" : (sec == 2 ? "T_MIN" : "S_MIN");
+        const char* ky1 = sec == 1 ? "E_MAX" : (sec == 2 ? "T_MAX" : "S_MAX");
+        if (!strcmp(key, kn1)) n1 = strtol(val, NULL, 10);
+        else if (!strcmp(key, kn2)) n2 = strtol(val, NULL, 10);
+        else if (!strcmp(key, kx0)) x0 = strtod(val, NULL);
+        else if (!strcmp(key, kx1)) x1 = strtod(val, NULL);
+        else if (!strcmp(key, ky0)) y0 = strtod(val, NULL);
+        else if (!strcmp(key, ky1)) {
+            y1 = strtod(val, NULL);
+            table2d* t[8];
+            int nt;
+            if (sec == 1) {
+                table2d* q[8] = {&L->p, &L->T, &L->a, &L->s, &L->mu, &L->kappa, &L->dpdrho, &L->dpde};
+                memcpy(t, q, sizeof q); nt = 8;
+            } else if (sec == 2) {
+                table2d* q[4] = {&L->rho_pt, &L->e_pt, &L->a_pt, &L->s_pt};
+                memcpy(t, q, sizeof q); nt = 4;
+            } else {
+                table2d* q[3] = {&L->rho_ps, &L->T_ps, &L->e_ps};
+                memcpy(t, q, sizeof q); nt = 3;
+            }
+            for (int q = 0; q < nt; q++) table_init(t[q], n1, n2, x0, x1, y0, y1);
+            double v[8];
+            int stop = 0;
+            for (long i = 0; i < n1 && !stop; i++)
+                for (long j = 0; j < n2; j++) {
+                    if (lut_row(f, line, sizeof line, v, nt)) { stop = 1; break; }
+                    for (int q = 0; q < nt; q++) t[q]->d[i * n2 + j] = v[q];
+                }
+        }
+    }
+    fclose(f);
+    return 0;
+}
+
+/* FluidReal inversions (src/fluid_real.cpp:211-320). */
+static double lut_e_p_rho(const lut* L, double p, double rho) { /* computeStaticEnergy_p_rho :227-250 */
+    double eLo = L->p.ymin, eHi = L->p.ymax;
+    double pLo = table_interp(&L->p, rho, eLo);
+    double pHi = table_interp(&L->p, rho, eHi);
+    if (p <= pLo) return eLo;
+    if (p >= pHi) return eHi;
+    for (int it = 0; it < 30; ++it) {
+        double eMid = 0.5 * (eLo + eHi);
+        double pMid = table_interp(&L->p, rho, eMid);
+        if (fabs(pMid - p) <= 1e-4 * p) return eMid;
+        if (pMid < p) eLo = eMid; else eHi = eMid;
+    }
+    return 0.5 * (eLo + eHi);
+}
+static double lut_h_p_s(const lut* L, double p, double s) { /* FluidBase::computeEnthalpy_p_s */
+    return table_interp(&L->e_ps, p, s) + p / table_interp(&L->rho_ps, p, s);
+}
+static double lut_pt_rho_e_et(const lut* L, double rho, double e, double et) { /* :299-321 */
+    double p = table_interp(&L->p, rho, e);
+    double sv = table_interp(&L->s, rho, e);
+    double ht = et + p / rho;
+    double pLo = p, pHi = L->rho_ps.xmax;
+    for (int it = 0; it < 25; ++it) {
+        double pMid = 0.5 * (pLo + pHi);
+        double rhoMid = table_interp(&L->rho_ps, pMid, sv);
+        double eMid = table_interp(&L->e_ps, pMid, sv);
+        double hMid = eMid + pMid / rhoMid;
+        if (hMid < ht) pLo = pMid; else pHi = pMid;
+    }
+    return 0.5 * (pLo + pHi);
+}
+
 /* ------------------------------------------------------- fluid (ideal gas) */
 /* FluidIdeal (src/fluid_ideal.cpp). */
 
 static double f_pressure_rho_e(const oracle_solver* s, double rho, double e) { /* :14-16 */
+    if (s->real) return table_interp(&s->lut->p, rho, e); /* FluidReal :211-213 */
     return (s->gamma - 1) * rho * e;
 }
 static double f_static_energy_u_et(vec3 u, double et) { /* :74-77, pow(|u|,2) == |u|*|u| */
@@ -334,32 +519,41 @@ static double f_static_energy_u_et(vec3 u, double et) { /* :74-77, pow(|u|,2) ==
     double m2 = m * m;
     return et - 0.5 * m2;
 }
+/* FluidBase::computeStaticEnergy_u_et (include/fluid_base.hpp:78-80), used by
+ * FluidReal: et - 0.5 u.u */
+static double fb_static_energy_u_et(vec3 u, double et) { return et - 0.5 * vdot(u, u); }
 static double f_pressure_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :89-92 */
+    if (s->real) return table_interp(&s->lut->p, rho, fb_static_energy_u_et(u, et)); /* fluid_base.hpp:91-94 */
     double e = f_static_energy_u_et(u, et);
     return f_pressure_rho_e(s, rho, e);
 }
 static double f_sound_speed_p_rho(const oracle_solver* s, double p, double rho) { /* :70-72 */
+    if (s->real) return table_interp(&s->lut->a, rho, lut_e_p_rho(s->lut, p, rho)); /* FluidReal :252-255 */
     return sqrt(s->gamma * p / rho);
 }
 static double f_sound_speed_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :83-87 */
+    if (s->real) return table_interp(&s->lut->a, rho, fb_static_energy_u_et(u, et)); /* fluid_base.hpp:86-89 */
     double e = f_static_energy_u_et(u, et);
     double p = f_pressure_rho_e(s, rho, e);
     return f_sound_speed_p_rho(s, p, rho);
 }
 static double f_sound_speed_rho_e(const oracle_solver* s, double rho, double e) { /* :22-24 */
-    (void)rho;
+    if (s->real) return table_interp(&s->lut->a, rho, e); /* FluidReal :219-221 */
     return sqrt(s->gamma * (s->gamma - 1.0) * e);
 }
 static double f_total_enthalpy_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :114-118 */
+    if (s->real) return et + f_pressure_rho_u_et(s, rho, u, et) / rho; /* fluid_base.hpp:106-109 */
     double e = f_static_energy_u_et(u, et);
     double p = f_pressure_rho_e(s, rho, e);
     return et + p / rho;
 }
 static double f_temperature_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :109-112 */
+    if (s->real) return table_interp(&s->lut->T, rho, fb_static_energy_u_et(u, et)); /* fluid_base.hpp:96-99 */
     double p = f_pressure_rho_u_et(s, rho, u, et);
     return p / (rho * s->rgas);
 }
 static double f_static_energy_p_rho(const oracle_solver* s, double p, double rho) { /* :10-12 */
+    if (s->real) return lut_e_p_rho(s->lut, p, rho);
     return p / ((s->gamma - 1) * rho);
 }
 static double f_mach_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :137-141 */
@@ -368,11 +562,18 @@ static double f_mach_rho_u_et(const oracle_solver* s, double rho, vec3 u, double
     return um / a;
 }
 static double f_total_pressure_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :94-98 */
+    if (s->real) return lut_pt_rho_e_et(s->lut, rho, fb_static_energy_u_et(u, et), et);
     double p = f_pressure_rho_u_et(s, rho, u, et);
     double M = f_mach_rho_u_et(s, rho, u, et);
     return p * pow(1.0 + (s->gamma - 1.0) / 2.0 * M * M, s->gamma / (s->gamma - 1));
 }
 static double f_total_temperature_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :100-104 */
+    if (s->real) { /* FluidReal :323-328 */
+        double pt = lut_pt_rho_e_et(s->lut, rho, fb_static_energy_u_et(u, et), et);
+        double e = fb_static_energy_u_et(u, et);
+        double sv = table_interp(&s->lut->s, rho, e);
+        return table_interp(&s->lut->T_ps, pt, sv);
+    }
     double T = f_temperature_rho_u_et(s, rho, u, et);
     double M = f_mach_rho_u_et(s, rho, u, et);
     return T * (1.0 + (s->gamma - 1.0) / 2.0 * M * M);
@@ -381,6 +582,7 @@ static double f_entropy_p_T(const oracle_solver* s, double p, double T) { /* :19
     return s->cp * log(T / 288.15) - s->rgas * log(p / 101325);
 }
 static double f_entropy_rho_u_et(const oracle_solver* s, double rho, vec3 u, double et) { /* :128-135 */
+    if (s->real) return table_interp(&s->lut->s, rho, fb_static_energy_u_et(u, et)); /* fluid_base.hpp:101-104 */
     double p = f_pressure_rho_u_et(s, rho, u, et);
     double T = f_temperature_rho_u_et(s, rho, u, et);
     return f_entropy_p_T(s, p, T);
@@ -554,8 +756,14 @@ static sv5 flux_roe(const oracle_solver* s, sv5 Ull, sv5 Ul, sv5 Ur, sv5 Urr, ve
     double eR = etR - 0.5 * (u1R * u1R + u2R * u2R + u3R * u3R);
     double pL = f_pressure_rho_e(s, rhoL, eL);
     double pR = f_pressure_rho_e(s, rhoR, eR);
-    double chiL = (s->gamma - 1.0) * eL, kapL = (s->gamma - 1.0) * rhoL;
-    double chiR = (s->gamma - 1.0) * eR, kapR = (s->gamma - 1.0) * rhoR;
+    double chiL, kapL, chiR, kapR;
+    if (s->real) { /* FluidReal :410-416 */
+        chiL = table_interp(&s->lut->dpdrho, rhoL, eL); kapL = table_interp(&s->lut->dpde, rhoL, eL);
+        chiR = table_interp(&s->lut->dpdrho, rhoR, eR); kapR = table_interp(&s->lut->dpde, rhoR, eR);
+    } else {
+        chiL = (s->gamma - 1.0) * eL; kapL = (s->gamma - 1.0) * rhoL;
+        chiR = (s->gamma - 1.0) * eR; kapR = (s->gamma - 1.0) * rhoR;
+    }
     double barChi = 0.5 * (chiL + chiR);
     double barKap = 0.5 * (kapL + kapR);
     double barRho = 0.5 * (rhoL + rhoR);
@@ -646,8 +854,16 @@ static sv5 bc_outlet(const oracle_solver* s, sv5 Uint, vec3 S, double p_b, long 
     double a = f_sound_speed_p_rho(s, p, W.v[0]);
     if (vmag(u) >= a) return adv_flux(s, W, S);
     double pb = ramped_outlet_pressure(s, it, p_b);
-    double rhob = pb * rho / p;
-    double eb = f_static_energy_p_rho(s, pb, rhob);
+    double rhob, eb;
+    if (s->real) { /* isentropic extrapolation, src/boundary_base.cpp:206-211 */
+        double eInt = W.v[4] - 0.5 * vdot(u, u);
+        double sInt = table_interp(&s->lut->s, rho, eInt);
+        rhob = table_interp(&s->lut->rho_ps, pb, sInt);
+        eb = table_interp(&s->lut->e_ps, pb, sInt);
+    } else {
+        rhob = pb * rho / p;
+        eb = f_static_energy_p_rho(s, pb, rhob);
+    }
     double etb = eb + 0.5 * vdot(u, u);
     sv5 Wb = {{rhob, u.x, u.y, u.z, etb}};
     return adv_flux(s, Wb, S);
@@ -687,6 +903,30 @@ static sv5 bc_inlet(const oracle_solver* s, const patch* pt, sv5 Uint, vec3 S, l
     double Cg = vdot(dir, n);
     if (Cg >= 0.0) Cg = -1.0;
     double Rout = pInt + Z * unInt;
+    if (s->real) { /* src/boundary_base.cpp:78-111 */
+        const lut* L = s->lut;
+        double sIn = table_interp(&L->s_pt, Pt, Tt);
+        double htIn = lut_h_p_s(L, Pt, sIn);
+        double pLow = 0.05 * Pt, pHigh = 0.999999 * Pt;
+        double pB = 0.5 * (pLow + pHigh);
+        for (int iter = 0; iter < 30; ++iter) {
+            double pMid = 0.5 * (pLow + pHigh);
+            double hMid = lut_h_p_s(L, pMid, sIn);
+            double VMid = sqrt(2.0 * dmax(0.0, htIn - hMid));
+            double res = pMid + Z * Cg * VMid - Rout;
+            if (fabs(res) < 1e-4 * Pt) { pB = pMid; break; }
+            if (res < 0.0) pLow = pMid; else pHigh = pMid;
+            pB = pMid;
+        }
+        double hB = lut_h_p_s(L, pB, sIn);
+        double VB = sqrt(2.0 * dmax(0.0, htIn - hB));
+        vec3 uB = vmul(dir, VB);
+        double rhoB = table_interp(&L->rho_ps, pB, sIn);
+        double eB = table_interp(&L->e_ps, pB, sIn);
+        double etB = eB + 0.5 * vdot(uB, uB);
+        sv5 Wb = {{rhoB, uB.x, uB.y, uB.z, etB}};
+        return adv_flux(s, Wb, S);
+    }
     double g = s->gamma, Rg = s->rgas;
     double cp = g * Rg / (g - 1.0);
     double htIn = cp * Tt;
@@ -1189,12 +1429,12 @@ static void update_turbo(oracle_solver* s, double* const* U) {
     double mflow = 0.5 * (fabs(s->massflow[bci[0]]) + fabs(s->massflow[bci[1]]));
     if (s->topology == TOPO_AXI) mflow *= 2.0 * M_PI / s->wedge;
     else if (s->per_angle_deg != 0.0) mflow *= 360.0 / s->per_angle_deg;
-    double pt[2], tt[2];
+    double pt[2], tt[2], htot[2], ent[2];
     for (int m = 0; m < 2; m++) {
         int bi = bci[m];
         long na, nb;
         boundary_extent(s, bi, &na, &nb);
-        double sp = 0.0, stt = 0.0;
+        double sp = 0.0, stt = 0.0, sht = 0.0, ss = 0.0;
         for (long a = 0; a < na; a++)
             for (long b = 0; b < nb; b++) {
                 long q;
@@ -1211,18 +1451,37 @@ static void update_turbo(oracle_solver* s, double* const* U) {
                 vec3 S = boundary_surface(s, bi, a, b);
                 sp += S.x * (rho * u.x * P) + S.y * (rho * u.y * P) + S.z * (rho * u.z * P);
                 stt += S.x * (rho * u.x * T) + S.y * (rho * u.y * T) + S.z * (rho * u.z * T);
+                if (s->real) { /* total enthalpy and entropy integrals, src/solver.cpp:1732-1749 */
+                    double H = f_total_enthalpy_rho_u_et(s, rho, u, et);
+                    double Sv = f_entropy_rho_u_et(s, rho, u, et);
+                    sht += S.x * (rho * u.x * H) + S.y * (rho * u.y * H) + S.z * (rho * u.z * H);
+                    ss += S.x * (rho * u.x * Sv) + S.y * (rho * u.y * Sv) + S.z * (rho * u.z * Sv);
+                }
             }
         double mf = s->massflow[bi];
         if (fabs(mf) < 1e-12) mf = (mf >= 0.0 ? 1e-12 : -1e-12);
         pt[m] = sp / mf;
         tt[m] = stt / mf;
+        htot[m] = sht / mf;
+        ent[m] = ss / mf;
     }
     double pr = (fabs(pt[0]) > 1e-12) ? pt[1] / pt[0] : 1.0;
     double tr = (fabs(tt[0]) > 1e-12) ? tt[1] / tt[0] : 1.0;
     s->turbo[0] = mflow;
     s->turbo[1] = pr;
     s->turbo[2] = tr;
-    s->turbo[3] = f_efficiency(s, pr, tr);
+    if (s->real) { /* src/solver.cpp:1768-1776, FluidBase::computeTotalEfficiency_h */
+        double hIn = htot[0], sIn = ent[0], ptOut = pt[1], hOut = htot[1];
+        double hOutS = lut_h_p_s(s->lut, ptOut, sIn);
+        double dh = hOut - hIn, dhs = hOutS - hIn;
+        double eta;
+        if (fabs(dh) < 1e-12) eta = 1.0;
+        else if (dh >= 0.0) eta = dhs / dh;
+        else eta = (fabs(dhs) < 1e-12) ? 1.0 : dh / dhs;
+        s->turbo[3] = eta;
+    } else {
+        s->turbo[3] = f_efficiency(s, pr, tr);
+    }
     s->has_turbo = 1;
 }
 
@@ -1243,7 +1502,8 @@ static void integrate_radial_eq(const double* rho, const double* ut, const doubl
 static double greitzer_step(oracle_solver* s, double mflow) {
     s->gz_min = mflow;
     s->gz_t += s->fixed_dt;
-    double a = sqrt(s->gamma * s->rgas * s->gz_T);
+    /* computeSoundSpeed_p_T: FluidIdeal sqrt(gamma R T), FluidReal the (p, T) table */
+    double a = s->real ? table_interp(&s->lut->a_pt, s->gz_p, s->gz_T) : sqrt(s->gamma * s->rgas * s->gz_T);
     double np = s->gz_p + s->fixed_dt * a * a / s->plenum_volume * (s->gz_min - s->gz_mout);
     s->gz_p = np;
     double dp = s->gz_p - s->ambient_p;
@@ -1803,11 +2063,20 @@ static int read_settings(oracle_solver* s) {
     if (cfg_bool(c, "VISCOSITY_ACTIVE", 0, &visc)) return 1;
     if (visc) return fail("Viscous fluxes are outside the oracle's scope");
     v = cfg_get(c, "FLUID_MODEL");
-    if (v && strcmp(v, "None") && strcmp(v, "Ideal") && strcmp(v, "ideal") && strcmp(v, "IDEAL"))
-        return fail("Only the ideal-gas model is in the oracle's scope");
-    if (cfg_float(c, "FLUID_GAMMA", &s->gamma)) return 1;
-    if (cfg_float(c, "FLUID_R_CONSTANT", &s->rgas)) return 1;
-    s->cp = (s->gamma * s->rgas) / (s->gamma - 1);
+    if (v && (!strcmp(v, "real") || !strcmp(v, "Real") || !strcmp(v, "REAL"))) {
+        s->real = 1; /* the table is loaded by oracle_create, next to the ini */
+        int stop = 0, regen = 0;
+        if (cfg_bool(c, "STOP_ON_TABLE_OUT_OF_BOUNDS", 0, &stop)) return 1;
+        if (stop) return fail("STOP_ON_TABLE_OUT_OF_BOUNDS is outside the oracle's scope");
+        if (cfg_bool(c, "FLUID_TABLE_FORCE_REGENERATE", 0, &regen)) return 1;
+        if (regen) return fail("Table regeneration is outside the oracle's scope");
+    } else if (v && strcmp(v, "None") && strcmp(v, "Ideal") && strcmp(v, "ideal") && strcmp(v, "IDEAL")) {
+        return fail("Invalid value for key \"FLUID_MODEL\" in configuration.");
+    } else {
+        if (cfg_float(c, "FLUID_GAMMA", &s->gamma)) return 1;
+        if (cfg_float(c, "FLUID_R_CONSTANT", &s->rgas)) return 1;
+        s->cp = (s->gamma * s->rgas) / (s->gamma - 1);
+    }
 
     if (cfg_bool(c, "SIMULATION_IS_STEADY", 1, &s->steady)) return 1;
     if (cfg_int_def(c, "RESIDUALS_DROP_CONVERGENCE", 16, &s->drop)) return 1;
@@ -1931,6 +2200,23 @@ static int init_solution(oracle_solver* s) {
                     long ia = (i < s->ni - 1) ? i : s->ni - 2;
                     dir = vnormalized(vsub(s->vert[idx3(s, ia + 1, j, k)], s->vert[idx3(s, ia, j, k)]));
                 }
+                if (s->real) { /* FluidReal::computeInitFields (src/fluid_real.cpp:346-362) */
+                    const lut* L = s->lut;
+                    double rho = table_interp(&L->rho_pt, p, T);
+                    double e = table_interp(&L->e_pt, p, T);
+                    double a = table_interp(&L->a, rho, e);
+                    double dm = vmag(dir);
+                    vec3 dn = (dm > 1e-12) ? vdiv(dir, dm) : v3(1.0, 0.0, 0.0);
+                    vec3 u = vmul(vmul(dn, a), M);
+                    double et = e + 0.5 * vdot(u, u);
+                    long q = idx3(s, i, j, k);
+                    s->U[0][q] = rho;
+                    s->U[1][q] = rho * u.x;
+                    s->U[2][q] = rho * u.y;
+                    s->U[3][q] = rho * u.z;
+                    s->U[4][q] = rho * et;
+                    continue;
+                }
                 double a = sqrt(s->gamma * s->rgas * T);
                 vec3 u = vmul(vmul(vdiv(dir, vmag(dir)), a), M);
                 double rho = p / (s->rgas * T);
@@ -1957,6 +2243,21 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
     if (cfg_load(&s->cfg, ini_path) || read_settings(s)) { oracle_destroy(s); return 1; }
     const char* grid = cfg_get(&s->cfg, "GRID_FILE");
     if (!grid) { fail("Not found value for key \"GRID_FILE\" in configuration."); oracle_destroy(s); return 1; }
+    if (s->real) { /* Config::getFluidTableFile (src/config.cpp:492-497), relative to the ini */
+        char tname[1024];
+        const char* tf = cfg_get(&s->cfg, "FLUID_TABLE_FILE");
+        const char* fname = cfg_get(&s->cfg, "FLUID_NAME");
+        if (!fname) fname = cfg_get(&s->cfg, "FLUID");
+        if (tf) snprintf(tname, sizeof tname, "%s", tf);
+        else snprintf(tname, sizeof tname, "fluid_table_%s.lut", fname ? fname : "CO2");
+        char tpath[4096];
+        dir_join(tpath, sizeof tpath, base, tname);
+        s->lut = (lut*)calloc(1, sizeof(lut));
+        if (lut_load(s->lut, tpath)) { oracle_destroy(s); return 1; }
+        s->gamma = s->lut->gnom;
+        s->rgas = s->lut->R;
+        s->cp = (s->gamma * s->rgas) / (s->gamma - 1);
+    }
     dir_join(path, sizeof path, base, grid);
     if (read_grid(s, path)) { oracle_destroy(s); return 1; }
     if (s->ni < 3 || (s->topology != TOPO_1D && s->nj < 3) || (s->topology == TOPO_3D && s->nk < 3)) {
@@ -2033,6 +2334,7 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
 void oracle_destroy(oracle_solver* s) {
     if (!s) return;
     cfg_free(&s->cfg);
+    lut_free(s->lut);
     free(s->vert); free(s->dual);
     free(s->sI); free(s->sJ); free(s->sK); free(s->cI); free(s->cJ); free(s->cK);
     free(s->vol); free(s->gradb);

@@ -39,6 +39,12 @@ def _sector(angle_deg: float, nk: int = 9):
     return dataclasses.replace(c, settings=s)
 
 
+def _co2(case):
+    """The same operating point in CO2 from the synthetic real-gas table:
+    inlet 8 MPa / 320 K, initial and outlet 7.6 MPa / 315 K."""
+    return cases.with_real_gas(case, pt=8.0e6, tt=320.0, p_init=7.6e6, t_init=315.0, table={"n_rho": 24, "n_e": 24, "n_p": 20, "n_T": 20, "n_s": 20})
+
+
 CASES = {
     "bump_jst_rk4": (lambda: cases.bump2d(ni=24, nj=12), 20),
     "bump_roe_vanalbada_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
@@ -54,4 +60,9 @@ CASES = {
     "annulus_roe_hall": (lambda: cases.annulus3d(ni=20, nj=8, nk=9), 10),
     "annulus_jst_thollet": (lambda: cases.annulus3d(ni=40, nj=12, nk=17, scheme="JST", muscl=False, rk=4, bfm_model="Hall-Thollet"), 5),
     "sector45_jst_cylindrical_inlet": (lambda: _sector(45.0), 10),
+    "co2_bump_jst_rk4": (lambda: _co2(cases.bump2d(ni=24, nj=12, mach=0.3)), 20),
+    "co2_bump_roe_minmod_rk3": (lambda: _co2(cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="min mod", rk=3, cfl=0.8, mach=0.3)), 20),
+    "co2_meridional_hall": (lambda: _co2(cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS)), 20),
+    "co2_meridional_greitzer": (lambda: _co2(_throttle(True)), 20),
+    "co2_annulus_roe_hall": (lambda: _co2(cases.annulus3d(ni=20, nj=8, nk=9, rows=cases.MAP_ROWS)), 5),
 }
