@@ -590,6 +590,61 @@ def run_map(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- real gas
+REALGAS_WORKLOAD = ("real-gas CO2 annulus 256x96x128 (3.1M nodes), synthetic van der Waals table 60x60 per section "
+                    "(1e5-1e7 Pa, 200-600 K), inlet 8.0 MPa / 310 K, Hall 15000 rpm, Roe+MUSCL(min mod), RK3, "
+                    "CFL 1.0; fp32_kahan bulk with FP64 table inversions")
+
+
+def run_realgas(args):
+    import numpy as np
+    import torch
+
+    from cturbobfm_b200 import Solver, cases
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    tmp = tempfile.TemporaryDirectory()
+    stream = torch.cuda.Stream()
+    arms = {}
+    with ClockSampler(local) as clocks:
+        for prec in ("fp32_kahan", "fp64"):
+            c = cases.realgas_annulus(precision=prec)
+            ini = c.write(os.path.join(tmp.name, prec))
+            with Solver(ini) as s:
+                s.set_stream(stream.cuda_stream)
+                s.enqueue(args.warmup)
+                stream.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                s.enqueue(args.steps)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                if s.status != 0:
+                    raise RuntimeError(f"real-gas workload stopped (status {s.status})")
+                arms[prec] = {"ms": ms, "state": s.state(), "turbo": s.turbo()[1], "n": c.n_nodes,
+                              "stages": c.n_stages, "bytes": int(s.info().device_bytes)}
+    clk = clocks.summary()
+    a, b = arms["fp32_kahan"], arms["fp64"]
+    n, st, K = a["n"], a["stages"], args.steps
+    rel = [float(np.abs(a["state"][v] - b["state"][v]).max() / np.abs(b["state"][v]).max()) for v in range(5)]
+    line = {
+        "metric": METRIC, "value": n * st * K / (a["ms"] / 1e3), "unit": UNIT, "n_gpus": 1, "steps": K,
+        "warmup": args.warmup, "ms_per_step": a["ms"] / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+kahan (f64 table inversions, integrals)", "data": "synthetic",
+        "config": {"workload": REALGAS_WORKLOAD, "nodes": n, "stages_per_step": st,
+                   "l2": f"inputs larger than L2: device working set {a['bytes'] / 2**20:.0f} MiB > 126 MiB"},
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "fp64": {"value": n * st * K / (b["ms"] / 1e3), "ms_per_step": b["ms"] / K},
+        "fp32_vs_fp64": {"after_iterations": args.warmup + K, "state_rel_err_per_field": rel,
+                         "massflow_rel_err": float(abs(a["turbo"][0] - b["turbo"][0]) / abs(b["turbo"][0])),
+                         "pr_tt_rel_err": float(abs(a["turbo"][1] - b["turbo"][1]) / abs(b["turbo"][1]))},
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- serving
 SERVE_WORKLOAD = ("serving: Poisson arrivals, 70% axisymmetric compressor-map requests (NI x NJ ~ U{64..256} x "
                   "U{24..96}) and 30% 3-D annuli (U{96..160} x U{32..48} x U{32..64}), MAP_ROWS stage, "
@@ -678,7 +733,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["annulus", "map", "serve"], default="annulus",
+    ap.add_argument("--workload", choices=["annulus", "map", "serve", "realgas"], default="annulus",
                     help="annulus: the 160x48x64 full-annulus loop (default); map: the batched compressor map; "
                          "serve: continuous batching of arriving requests")
     ap.add_argument("--map-n", type=int, default=256)
@@ -697,6 +752,8 @@ def main():
         run_map(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "realgas":
+        run_realgas(args)
     else:
         run_ours(args)
 

@@ -31,7 +31,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 # (source, contract multiply-adds)
 CU_SOURCES = [("device/kernels.cu", False), ("device/kernels_f32.cu", True), ("device/noalloc.cu", False)]
-CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/engine.cpp", "host/solver.cpp", "host/batch.cpp", "host/server.cpp", "capi.cpp"]
+CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/engine.cpp", "host/fluid_table.cpp", "host/solver.cpp", "host/batch.cpp", "host/server.cpp", "capi.cpp"]
 
 
 def _run(cmd: List[str]) -> None:

@@ -239,7 +239,7 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
               rpm: float = 10000.0, p_ratio: float = 1.15, mach: float = 0.3,
               name: str = "annulus3d", rows=None, speed: Optional[float] = None,
               drop: Optional[int] = None, ramp: Optional[int] = None,
-              precision: Optional[str] = None) -> Case:
+              precision: Optional[str] = None, scale: float = 1.0) -> Case:
     """Full-annulus axial rotor + stator: hub radius 0.20 m, tip 0.40 m, axial
     length 0.6 m; rotor at 0.2-0.3 m (blockage loss 0.4, metal angle magnitude
     50 deg at hub to 60 deg at tip, negative in the solver's sign convention
@@ -248,9 +248,10 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
     blade rows (MAP_ROWS for the serving workload); ``speed``, ``drop``,
     ``ramp`` and ``precision`` set ROTATIONAL_SPEED_SCALING_FACTOR,
     RESIDUALS_DROP_CONVERGENCE, OUTLET_PRESSURE_RAMP_ITERATIONS and
-    GPU_PRECISION."""
-    xs = np.linspace(0.0, 0.6, ni)
-    rs = np.linspace(0.20, 0.40, nj)
+    GPU_PRECISION. ``scale`` multiplies every length (grid and blade-row
+    positions)."""
+    xs = np.linspace(0.0, 0.6, ni) * scale
+    rs = np.linspace(0.20, 0.40, nj) * scale
     th = np.array([2.0 * math.pi * k / (nk - 1) for k in range(nk - 1)] + [0.0])
     X = np.broadcast_to(xs[:, None, None], (ni, nj, nk)).copy()
     R = np.broadcast_to(rs[None, :, None], (ni, nj, nk))
@@ -260,6 +261,7 @@ def annulus3d(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
     if rows is None:
         rows = [(0.2, 0.3, -50.0, -60.0, rpm, 24, 0.4),
                 (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.3)]
+    rows = [(r[0] * scale, r[1] * scale) + tuple(r[2:]) for r in rows]
     fields = _row_fields(xs, rs, rows, nk)
     pt, tt = 101325.0, 288.15
     ps, ts = static_state(pt, tt, mach)
@@ -451,6 +453,21 @@ def with_real_gas(case: Case, pt: float, tt: float, p_init: float, t_init: float
             p = dataclasses.replace(p, spec=f"{kind}, {(p_init if p_out is None else p_out)!r}")
         patches.append(p)
     return dataclasses.replace(case, settings=s, patches=patches, table=dict(table or {}))
+
+
+def realgas_annulus(ni: int = 256, nj: int = 96, nk: int = 128, n_iter: int = 10000, cfl: float = 1.0,
+                    precision: Optional[str] = None, p_out: float = 8.2e6, table: Optional[Dict] = None) -> Case:
+    """The real-gas workload: a compact CO2 rotor/stator annulus (annulus3d
+    geometry scaled by 1/4: hub 0.05 m, tip 0.10 m, length 0.15 m; MAP_ROWS
+    blade rows with the rotor at 15000 rpm), Hall body force, Roe + MUSCL
+    min mod, RK3, local time step at CFL 1.0, on the synthetic CO2 table of
+    fluid_table (60 x 60 per section, 1e5-1e7 Pa, 200-600 K). Inlet total
+    8.0 MPa / 310 K, initial state 7.6 MPa / 305 K at Mach 0.3, outlet static
+    p_out."""
+    rows = [(0.2, 0.3, -30.0, -40.0, 15000.0, 24, 0.1), (0.35, 0.45, 10.0, 15.0, 0.0, 30, 0.1)]
+    c = annulus3d(ni=ni, nj=nj, nk=nk, n_iter=n_iter, cfl=cfl, scheme="Roe", muscl=True, limiter="min mod", rk=3,
+                  bfm_model="Hall", rows=rows, precision=precision, scale=0.25, name="realgas_annulus")
+    return with_real_gas(c, pt=8.0e6, tt=310.0, p_init=7.6e6, t_init=305.0, p_out=p_out, table=table)
 
 
 def read_grid_csv(path: str) -> Tuple[Tuple[int, int, int], Dict[str, np.ndarray]]:

@@ -44,6 +44,27 @@ struct DevFacesT {
     R* c[5];
 };
 
+// One uniform table of the real-gas look-up (Table2D, include/fluid_real.hpp:
+// 11-58): values d[i * ny + j] over x_i = xmin + i dx, y_j = ymin + j dy, in
+// double and as a float copy for the float path's bulk evaluations.
+struct DevTable {
+    double xmin, xmax, ymin, ymax, dx, dy;
+    float fxmin, fxmax, fymin, fymax, fdx, fdy;
+    int nx, ny;
+    const double* d;
+    const float* f;
+};
+
+// The tables of FluidReal (include/fluid_real.hpp:139-160).
+enum DevLutRhoE : int { kReP = 0, kReT, kReA, kReS, kReMu, kReKappa, kReDpDrho, kReDpDe };
+enum DevLutPT : int { kPtRho = 0, kPtE, kPtA, kPtS };
+enum DevLutPS : int { kPsRho = 0, kPsT, kPsE };
+struct DevLut {
+    DevTable re[8];  // over (rho, e)
+    DevTable pt[4];  // over (p, T)
+    DevTable ps[3];  // over (p, s)
+};
+
 // Iteration state living on the device.
 struct Control {
     long long it;       // iterations completed
@@ -69,6 +90,9 @@ struct Control {
     double best_drop;
     double drop_mark;
     long long it_best;
+    // real gas: mass-weighted total-enthalpy and entropy integrals over the
+    // inlet / outlet planes (enthalpy-based efficiency)
+    double ht_int[2], s_int[2];
 };
 
 // A block's share of a batched launch: `count` consecutive elements (nodes,
@@ -160,6 +184,7 @@ struct alignas(16) DevCaseT {
     double* partial;  // [node_tiles*5 | per_tiles*5 | node_tiles dt minima]
     int node_tiles;   // tiles of this instance in the node kernels
     int per_tiles;    // tiles of this instance in the periodic kernel
+    const DevLut* lut;  // FLUID_MODEL = real: the look-up tables; nullptr for the ideal gas
     Control* ctl;
     double* hist;  // 16 doubles per iteration row
     long long hist_cap;

@@ -22,6 +22,8 @@ template <typename R>
 struct BatchView {
     const DevCaseT<R>* cases = nullptr;  // m device-resident instance descriptions
     int m = 0;
+    bool ideal = true;  // some member uses the ideal gas
+    bool real = false;  // some member uses the real-gas look-up tables
     TileList node;        // nodes of every instance (k_prim, k_nodes, k_dt)
     TileList face[3][2];  // faces per direction and scheme (0 JST, 1 Roe)
     TileList per;         // periodic (i, j) pairs of periodic instances

@@ -29,14 +29,18 @@ namespace {
 
 // Block entry: reads the block's tile, returns false (the whole block leaves
 // before touching anything else) when its instance has converged, diverged,
-// reached its iteration limit or has no such stage, and otherwise copies the
+// reached its iteration limit, has no such stage or another fluid model than
+// the kernel was compiled for, and otherwise copies the
 // instance description into shared memory. Every thread reads the same
 // control words, which no kernel writes while others read them.
 template <typename R>
 __device__ __forceinline__ bool enter(const DevCaseT<R>* cases, const Tile* tiles, DevCaseT<R>& sc, int stage,
-                                      int force, Tile& t) {
+                                      int force, Tile& t, int fluid = -1) {
     t = tiles[blockIdx.x];
     const DevCaseT<R>* g = cases + t.inst;
+    // kernels compiled for one fluid model (0 ideal, 1 look-up table) take
+    // only the instances of that model
+    if (fluid >= 0 && (g->lut != nullptr) != (fluid != 0)) return false;
     if (!force) {
         const Control* ctl = g->ctl;
         if (ctl->status != 0 || ctl->it >= ctl->it_stop) return false;
@@ -146,13 +150,13 @@ __device__ __forceinline__ S5<double> state64(const DevCaseT<R>& c, R* const* U,
 // ------------------------------------------------------------------ faces
 // Solver::computeAdvectionFluxResidualsImpl (src/solver.cpp:1865-2040): one
 // thread per face of direction DIR; writes flux * |S|.
-template <int DIR, int SCHEME, typename R>
+template <int DIR, int SCHEME, typename R, int FL>
 __global__ void __launch_bounds__(256) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
-    if (!enter(cases, tiles, c, stage, force, tl)) return;
+    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
     const long long it = c.ctl->it + 1;
-    const Gas<R> gs{R(c.gamma), R(c.rgas)};
+    const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const int nfj = c.nj + (DIR == 1), nfk = c.nk + (DIR == 2);
     const long long st = DIR == 0 ? static_cast<long long>(c.nj) * c.nk : (DIR == 1 ? c.nk : 1);
     const int nlast = DIR == 0 ? c.ni : (DIR == 1 ? c.nj : c.nk);
@@ -245,12 +249,12 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 // K faces, then sources), then Solver::updateSolution (src/solver.cpp:2230-2249)
 // U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
 // Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
-template <typename R>
+template <typename R, int FL>
 __global__ void __launch_bounds__(256, 2) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
-    if (!enter(cases, tiles, c, stage, force, tl)) return;
-    const Gas<R> gs{R(c.gamma), R(c.rgas)};
+    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
+    const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const double t = c.ctl->t;
     const R dtg = R(c.ctl->dt_min);
     const bool resOnly = stage < 0;
@@ -412,13 +416,13 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
 // ------------------------------------------------------------- time step
 // Solver::computeTimestepArray (src/solver.cpp:1531-1630), inviscid:
 // dt = CFL / sum_d (|u . e_d| + a) / |e_d| over the dual-node edges.
-template <typename R>
+template <typename R, int FL>
 __global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile* tiles, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
-    if (!enter(cases, tiles, c, 0, force, tl)) return;
+    if (!enter(cases, tiles, c, 0, force, tl, FL)) return;
     if (c.dt_method == 2) return;
-    const Gas<R> gs{R(c.gamma), R(c.rgas)};
+    const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const R cfl = R(c.cfl);
     double mn = INFINITY;
     for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) {
@@ -474,18 +478,18 @@ __device__ __forceinline__ int turboPlane(const DevCaseT<R>& c, int m) {
     }
 }
 
-template <typename R>
+template <typename R, int FL>
 __global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Tile* tiles, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
-    if (!enter(cases, tiles, c, 0, force, tl)) return;
-    const Gas<double> gs{c.gamma, c.rgas};
+    if (!enter(cases, tiles, c, 0, force, tl, FL)) return;
+    const Gas<double> gs{c.gamma, c.rgas, FL ? c.lut : nullptr};
     const int blk = tl.local;
     const int plane = blk < 6 ? blk : turboPlane(c, blk - 6);
     int na, nb;
     planeExtent(c, plane, na, nb);
     const long long cnt = static_cast<long long>(na) * nb;
-    double s[2] = {0.0, 0.0};
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
     for (long long e = threadIdx.x; e < cnt; e += blockDim.x) {
         const int a = static_cast<int>(e / nb), bb = static_cast<int>(e % nb);
         const long long q = planeNode(c, plane, a, bb);
@@ -501,14 +505,22 @@ __global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Ti
             const double T = totalTemperature_rho_u_et(gs, rho, u, W.v[4]);
             s[0] += sx * (rho * u.x * P) + sy * (rho * u.y * P) + sz * (rho * u.z * P);
             s[1] += sx * (rho * u.x * T) + sy * (rho * u.y * T) + sz * (rho * u.z * T);
+            if (FL) {  // total enthalpy and entropy (src/solver.cpp:1732-1749)
+                const double H = totalEnthalpy_rho_u_et(gs, rho, u, W.v[4]);
+                const double S = entropy_rho_u_et(gs, rho, u, W.v[4]);
+                s[2] += sx * (rho * u.x * H) + sy * (rho * u.y * H) + sz * (rho * u.z * H);
+                s[3] += sx * (rho * u.x * S) + sy * (rho * u.y * S) + sz * (rho * u.z * S);
+            }
         }
     }
-    blockSum<2>(s);
+    blockSum<4>(s);
     if (threadIdx.x == 0) {
         if (blk < 6) c.ctl->massflow[blk] = s[0];
         else {
             c.ctl->pt_int[blk - 6] = s[0];
             c.ctl->tt_int[blk - 6] = s[1];
+            c.ctl->ht_int[blk - 6] = s[2];
+            c.ctl->s_int[blk - 6] = s[3];
         }
     }
 }
@@ -542,21 +554,33 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
         double mflow = 0.5 * (fabs(ctl->massflow[p0]) + fabs(ctl->massflow[p1]));
         if (c.topo == 2) mflow *= 2.0 * M_PI / c.wedge;
         else if (c.per_angle_deg != 0.0) mflow *= 360.0 / c.per_angle_deg;
-        double pt[2], tt[2];
+        double pt[2], tt[2], ht[2], en[2];
         for (int m = 0; m < 2; m++) {
             double mf = ctl->massflow[m == 0 ? p0 : p1];
             if (fabs(mf) < 1e-12) mf = (mf >= 0.0 ? 1e-12 : -1e-12);
             pt[m] = ctl->pt_int[m] / mf;
             tt[m] = ctl->tt_int[m] / mf;
+            ht[m] = ctl->ht_int[m] / mf;
+            en[m] = ctl->s_int[m] / mf;
         }
         const double pr = (fabs(pt[0]) > 1e-12) ? pt[1] / pt[0] : 1.0;
         const double tr = (fabs(tt[0]) > 1e-12) ? tt[1] / tt[0] : 1.0;
-        const double dT = tr - 1.0;
-        const double dTs = pow(pr, (c.gamma - 1.0) / c.gamma) - 1.0;
         double eta;
-        if (fabs(dT) < 1e-12) eta = 1.0;
-        else if (dT >= 0.0) eta = dTs / dT;
-        else eta = (fabs(dTs) < 1e-12) ? 1.0 : dT / dTs;
+        if (c.lut) {
+            // src/solver.cpp:1768-1776 with FluidBase::computeTotalEfficiency_h
+            // (include/fluid_base.hpp:145-157)
+            const double hOutS = lutEnthalpy_p_s(*c.lut, pt[1], en[0]);
+            const double dh = ht[1] - ht[0], dhs = hOutS - ht[0];
+            if (fabs(dh) < 1e-12) eta = 1.0;
+            else if (dh >= 0.0) eta = dhs / dh;
+            else eta = (fabs(dhs) < 1e-12) ? 1.0 : dh / dhs;
+        } else {
+            const double dT = tr - 1.0;
+            const double dTs = pow(pr, (c.gamma - 1.0) / c.gamma) - 1.0;
+            if (fabs(dT) < 1e-12) eta = 1.0;
+            else if (dT >= 0.0) eta = dTs / dT;
+            else eta = (fabs(dTs) < 1e-12) ? 1.0 : dT / dTs;
+        }
         ctl->turbo[0] = mflow;
         ctl->turbo[1] = pr;
         ctl->turbo[2] = tr;
@@ -567,7 +591,8 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
     if (c.greitzer) {
         ctl->gz_min = ctl->turbo[0];
         ctl->gz_t += c.fixed_dt;
-        const double a = sqrt(c.gamma * c.rgas * ctl->gz_T);
+        // computeSoundSpeed_p_T: FluidIdeal sqrt(gamma R T), FluidReal the (p, T) table
+        const double a = c.lut ? lutInterp(c.lut->pt[kPtA], ctl->gz_p, ctl->gz_T) : sqrt(c.gamma * c.rgas * ctl->gz_T);
         const double np = ctl->gz_p + c.fixed_dt * a * a / c.plenum_volume * (ctl->gz_min - ctl->gz_mout);
         ctl->gz_p = np;
         const double dp = ctl->gz_p - c.ambient_p;
@@ -718,13 +743,15 @@ cudaError_t Launcher<R>::gatherControl(const BatchView<R>& b, Control* out, cuda
 template <typename R>
 cudaError_t Launcher<R>::boundaryIntegrals(const BatchView<R>& b, bool all, int force, cudaStream_t s) {
     const TileList& t = all ? b.bintAll : b.bint;
-    if (t.n) k_bint<R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, force);
+    if (t.n && b.ideal) k_bint<R, 0><<<t.n, 256, 0, s>>>(b.cases, t.tiles, force);
+    if (t.n && b.real) k_bint<R, 1><<<t.n, 256, 0, s>>>(b.cases, t.tiles, force);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::timeStep(const BatchView<R>& b, int force, cudaStream_t s) {
-    if (b.node.n) k_dt<R><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, force);
+    if (b.node.n && b.ideal) k_dt<R, 0><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, force);
+    if (b.node.n && b.real) k_dt<R, 1><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, force);
     return cudaGetLastError();
 }
 
@@ -743,27 +770,36 @@ cudaError_t Launcher<R>::prim(const BatchView<R>& b, int stage, int force, cudaS
     return cudaGetLastError();
 }
 
-template <typename R>
-cudaError_t Launcher<R>::faces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s) {
+namespace {
+template <int FL, typename R>
+void launchFaces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s) {
     for (int sch = 0; sch < 2; sch++) {
         const TileList& t = b.face[dir][sch];
         if (!t.n) continue;
         if (sch == 0) {
-            if (dir == 0) k_faces<0, 0, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else if (dir == 1) k_faces<1, 0, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else k_faces<2, 0, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            if (dir == 0) k_faces<0, 0, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else if (dir == 1) k_faces<1, 0, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else k_faces<2, 0, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
         } else {
-            if (dir == 0) k_faces<0, 1, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else if (dir == 1) k_faces<1, 1, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else k_faces<2, 1, R><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            if (dir == 0) k_faces<0, 1, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else if (dir == 1) k_faces<1, 1, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
+            else k_faces<2, 1, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
         }
     }
+}
+}  // namespace
+
+template <typename R>
+cudaError_t Launcher<R>::faces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s) {
+    if (b.ideal) launchFaces<0>(b, dir, stage, force, s);
+    if (b.real) launchFaces<1>(b, dir, stage, force, s);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.node.n) k_nodes<R><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.ideal) k_nodes<R, 0><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.real) k_nodes<R, 1><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
     return cudaGetLastError();
 }
 

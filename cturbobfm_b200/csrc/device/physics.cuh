@@ -120,51 +120,159 @@ CTBFM_DI void store5(R* const* U, long long q, const S5<R>& s) {
     for (int c = 0; c < 5; c++) U[c][q] = s.v[c];
 }
 
-// ---------------------------------------------------------- ideal gas
-// FluidIdeal (src/fluid_ideal.cpp).
+// ------------------------------------------------------------- fluids
+// Gas: the ideal gas of FluidIdeal (src/fluid_ideal.cpp) when lut is null,
+// otherwise the look-up tables of FluidReal (src/fluid_real.cpp) with the
+// FluidBase defaults it inherits (include/fluid_base.hpp). Each function
+// below takes the ideal branch exactly as before for the ideal gas.
 template <typename R>
 struct Gas {
     R g, R_;
+    const DevLut* lut;
 };
 
+// Table2D::interpolate (include/fluid_real.hpp:35-57): clamp, cell index by
+// truncation (a NaN coordinate gives a NaN result on both sides), bilinear
+// weights summed in the reference's order. Double: the double tables; float:
+// the float copy, in float.
+CTBFM_DI double lutInterp(const DevTable& t, double x, double y) {
+    const double xc = (x < t.xmin) ? t.xmin : ((t.xmax < x) ? t.xmax : x);
+    const double yc = (y < t.ymin) ? t.ymin : ((t.ymax < y) ? t.ymax : y);
+    const double rx = (xc - t.xmin) / t.dx;
+    const double ry = (yc - t.ymin) / t.dy;
+    unsigned long long i = static_cast<unsigned long long>(rx);
+    unsigned long long j = static_cast<unsigned long long>(ry);
+    if (i >= static_cast<unsigned long long>(t.nx - 1)) i = (t.nx >= 2) ? t.nx - 2 : 0;
+    if (j >= static_cast<unsigned long long>(t.ny - 1)) j = (t.ny >= 2) ? t.ny - 2 : 0;
+    const double wx = rx - static_cast<double>(i);
+    const double wy = ry - static_cast<double>(j);
+    const double* d = t.d + i * t.ny + j;
+    const double f00 = __ldg(d), f01 = __ldg(d + 1), f10 = __ldg(d + t.ny), f11 = __ldg(d + t.ny + 1);
+    return (1.0 - wx) * (1.0 - wy) * f00 + wx * (1.0 - wy) * f10 + (1.0 - wx) * wy * f01 + wx * wy * f11;
+}
+CTBFM_DI float lutInterp(const DevTable& t, float x, float y) {
+    const float xc = (x < t.fxmin) ? t.fxmin : ((t.fxmax < x) ? t.fxmax : x);
+    const float yc = (y < t.fymin) ? t.fymin : ((t.fymax < y) ? t.fymax : y);
+    const float rx = (xc - t.fxmin) / t.fdx;
+    const float ry = (yc - t.fymin) / t.fdy;
+    unsigned int i = static_cast<unsigned int>(rx);
+    unsigned int j = static_cast<unsigned int>(ry);
+    if (i >= static_cast<unsigned int>(t.nx - 1)) i = (t.nx >= 2) ? t.nx - 2 : 0;
+    if (j >= static_cast<unsigned int>(t.ny - 1)) j = (t.ny >= 2) ? t.ny - 2 : 0;
+    const float wx = rx - static_cast<float>(i);
+    const float wy = ry - static_cast<float>(j);
+    const float* d = t.f + i * t.ny + j;
+    const float f00 = __ldg(d), f01 = __ldg(d + 1), f10 = __ldg(d + t.ny), f11 = __ldg(d + t.ny + 1);
+    return (1.0f - wx) * (1.0f - wy) * f00 + wx * (1.0f - wy) * f10 + (1.0f - wx) * wy * f01 + wx * wy * f11;
+}
+
+// FluidReal::computeStaticEnergy_p_rho (src/fluid_real.cpp:227-250): bisection
+// on e, always in double (the table inversion).
+CTBFM_DI double lutStaticEnergy_p_rho(const DevLut& L, double p, double rho) {
+    const DevTable& tp = L.re[kReP];
+    double eLo = tp.ymin, eHi = tp.ymax;
+    const double pLo = lutInterp(tp, rho, eLo);
+    const double pHi = lutInterp(tp, rho, eHi);
+    if (p <= pLo) return eLo;
+    if (p >= pHi) return eHi;
+    for (int it = 0; it < 30; ++it) {
+        const double eMid = 0.5 * (eLo + eHi);
+        const double pMid = lutInterp(tp, rho, eMid);
+        if (fabs(pMid - p) <= 1e-4 * p) return eMid;
+        if (pMid < p) eLo = eMid;
+        else eHi = eMid;
+    }
+    return 0.5 * (eLo + eHi);
+}
+// FluidBase::computeEnthalpy_p_s (include/fluid_base.hpp:73-75) on the (p, s) tables.
 template <typename R>
-CTBFM_DI R staticEnergy_u_et(V3<R> u, R et) {  // :74-77 (pow(|u|,2) == |u|*|u|)
+CTBFM_DI R lutEnthalpy_p_s(const DevLut& L, R p, R s) {
+    return lutInterp(L.ps[kPsE], p, s) + p / lutInterp(L.ps[kPsRho], p, s);
+}
+// FluidReal::computeTotalPressure_rho_u_et (src/fluid_real.cpp:299-321) given
+// the static energy: 25 bisection steps on the (p, s) tables, in double.
+CTBFM_DI double lutTotalPressure(const DevLut& L, double rho, double e, double et) {
+    const double p = lutInterp(L.re[kReP], rho, e);
+    const double s = lutInterp(L.re[kReS], rho, e);
+    const double ht = et + p / rho;
+    double pLo = p, pHi = L.ps[kPsRho].xmax;
+    for (int it = 0; it < 25; ++it) {
+        const double pMid = 0.5 * (pLo + pHi);
+        const double rhoMid = lutInterp(L.ps[kPsRho], pMid, s);
+        const double eMid = lutInterp(L.ps[kPsE], pMid, s);
+        const double hMid = eMid + pMid / rhoMid;
+        if (hMid < ht) pLo = pMid;
+        else pHi = pMid;
+    }
+    return 0.5 * (pLo + pHi);
+}
+
+template <typename R>
+CTBFM_DI R staticEnergy_u_et(V3<R> u, R et) {  // FluidIdeal :74-77 (pow(|u|,2) == |u|*|u|)
     const R m = mag(u);
     const R m2 = m * m;
     return et - R(0.5) * m2;
 }
 template <typename R>
-CTBFM_DI R pressure_rho_e(Gas<R> gs, R rho, R e) {  // :14-16
+CTBFM_DI R staticEnergy_u_et(Gas<R> gs, V3<R> u, R et) {
+    if (gs.lut) return et - R(0.5) * dot(u, u);  // FluidBase (include/fluid_base.hpp:78-80)
+    return staticEnergy_u_et(u, et);
+}
+template <typename R>
+CTBFM_DI R pressure_rho_e(Gas<R> gs, R rho, R e) {  // :14-16; FluidReal :211-213
+    if (gs.lut) return lutInterp(gs.lut->re[kReP], rho, e);
     return (gs.g - R(1)) * rho * e;
 }
 template <typename R>
-CTBFM_DI R pressure_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :89-92
-    return pressure_rho_e(gs, rho, staticEnergy_u_et(u, et));
+CTBFM_DI R pressure_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :89-92; fluid_base.hpp:91-94
+    return pressure_rho_e(gs, rho, staticEnergy_u_et(gs, u, et));
 }
 template <typename R>
-CTBFM_DI R soundSpeed_p_rho(Gas<R> gs, R p, R rho) {  // :70-72
+CTBFM_DI R soundSpeed_p_rho(Gas<R> gs, R p, R rho) {  // :70-72; FluidReal :252-255 (inversion in double)
+    if (gs.lut) {
+        const double e = lutStaticEnergy_p_rho(*gs.lut, static_cast<double>(p), static_cast<double>(rho));
+        return R(lutInterp(gs.lut->re[kReA], static_cast<double>(rho), e));
+    }
     return sqrt(gs.g * p / rho);
 }
 template <typename R>
-CTBFM_DI R soundSpeed_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :83-87
+CTBFM_DI R soundSpeed_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :83-87; fluid_base.hpp:86-89
+    if (gs.lut) return lutInterp(gs.lut->re[kReA], rho, staticEnergy_u_et(gs, u, et));
     const R p = pressure_rho_e(gs, rho, staticEnergy_u_et(u, et));
     return soundSpeed_p_rho(gs, p, rho);
 }
 template <typename R>
-CTBFM_DI R soundSpeed_rho_e(Gas<R> gs, R e) {  // :22-24
+CTBFM_DI R soundSpeed_rho_e(Gas<R> gs, R rho, R e) {  // :22-24; FluidReal :219-221
+    if (gs.lut) return lutInterp(gs.lut->re[kReA], rho, e);
     return sqrt(gs.g * (gs.g - R(1)) * e);
 }
 template <typename R>
-CTBFM_DI R totalEnthalpy_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :114-118
-    const R p = pressure_rho_e(gs, rho, staticEnergy_u_et(u, et));
+CTBFM_DI R dpdrho_e(Gas<R> gs, R rho, R e) {  // :50-52; FluidReal :410-412
+    if (gs.lut) return lutInterp(gs.lut->re[kReDpDrho], rho, e);
+    return (gs.g - R(1)) * e;
+}
+template <typename R>
+CTBFM_DI R dpde_rho(Gas<R> gs, R rho, R e) {  // :54-56; FluidReal :414-416
+    if (gs.lut) return lutInterp(gs.lut->re[kReDpDe], rho, e);
+    return (gs.g - R(1)) * rho;
+}
+template <typename R>
+CTBFM_DI R totalEnthalpy_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :114-118; fluid_base.hpp:106-109
+    const R p = pressure_rho_e(gs, rho, staticEnergy_u_et(gs, u, et));
     return et + p / rho;
 }
 template <typename R>
-CTBFM_DI R temperature_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :109-112
+CTBFM_DI R temperature_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :109-112; fluid_base.hpp:96-99
+    if (gs.lut) return lutInterp(gs.lut->re[kReT], rho, staticEnergy_u_et(gs, u, et));
     return pressure_rho_u_et(gs, rho, u, et) / (rho * gs.R_);
 }
 template <typename R>
-CTBFM_DI R staticEnergy_p_rho(Gas<R> gs, R p, R rho) {  // :10-12
+CTBFM_DI R entropy_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // real gas only: fluid_base.hpp:101-104
+    return lutInterp(gs.lut->re[kReS], rho, staticEnergy_u_et(gs, u, et));
+}
+template <typename R>
+CTBFM_DI R staticEnergy_p_rho(Gas<R> gs, R p, R rho) {  // :10-12; FluidReal :227-250 (double)
+    if (gs.lut) return R(lutStaticEnergy_p_rho(*gs.lut, static_cast<double>(p), static_cast<double>(rho)));
     return p / ((gs.g - R(1)) * rho);
 }
 template <typename R>
@@ -173,13 +281,20 @@ CTBFM_DI R mach_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :137-141
     return mag(u) / a;
 }
 template <typename R>
-CTBFM_DI R totalPressure_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :94-98
+CTBFM_DI R totalPressure_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :94-98; FluidReal :299-321
+    if (gs.lut) return R(lutTotalPressure(*gs.lut, rho, staticEnergy_u_et(gs, u, et), et));
     const R p = pressure_rho_u_et(gs, rho, u, et);
     const R M = mach_rho_u_et(gs, rho, u, et);
     return p * pow(R(1) + (gs.g - R(1)) / R(2) * M * M, gs.g / (gs.g - R(1)));
 }
 template <typename R>
-CTBFM_DI R totalTemperature_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :100-104
+CTBFM_DI R totalTemperature_rho_u_et(Gas<R> gs, R rho, V3<R> u, R et) {  // :100-104; FluidReal :323-328
+    if (gs.lut) {
+        const double pt = lutTotalPressure(*gs.lut, rho, staticEnergy_u_et(gs, u, et), et);
+        const double e = staticEnergy_u_et(gs, u, et);
+        const double s = lutInterp(gs.lut->re[kReS], static_cast<double>(rho), e);
+        return R(lutInterp(gs.lut->ps[kPsT], pt, s));
+    }
     const R T = temperature_rho_u_et(gs, rho, u, et);
     const R M = mach_rho_u_et(gs, rho, u, et);
     return T * (R(1) + (gs.g - R(1)) / R(2) * M * M);
@@ -323,8 +438,8 @@ CTBFM_DI S5<R> fluxRoeW(Gas<R> gs, int muscl, int lim, const S5<R>& Wll, S5<R> W
     const R eR = etR - R(0.5) * (u1R * u1R + u2R * u2R + u3R * u3R);
     const R pL = pressure_rho_e(gs, rhoL, eL);
     const R pR = pressure_rho_e(gs, rhoR, eR);
-    const R chiL = (gs.g - R(1)) * eL, kapL = (gs.g - R(1)) * rhoL;
-    const R chiR = (gs.g - R(1)) * eR, kapR = (gs.g - R(1)) * rhoR;
+    const R chiL = dpdrho_e(gs, rhoL, eL), kapL = dpde_rho(gs, rhoL, eL);
+    const R chiR = dpdrho_e(gs, rhoR, eR), kapR = dpde_rho(gs, rhoR, eR);
     const R barChi = R(0.5) * (chiL + chiR);
     const R barKap = R(0.5) * (kapL + kapR);
     const R barRho = R(0.5) * (rhoL + rhoR);
@@ -347,7 +462,7 @@ CTBFM_DI S5<R> fluxRoeW(Gas<R> gs, int muscl, int lim, const S5<R>& Wll, S5<R> W
     const R hA = htA - R(0.5) * q2;
     R a2 = chiP + kapP * hA;
     if (a2 <= R(0)) {
-        const R aL = soundSpeed_rho_e(gs, eL), aR = soundSpeed_rho_e(gs, eR);
+        const R aL = soundSpeed_rho_e(gs, rhoL, eL), aR = soundSpeed_rho_e(gs, rhoR, eR);
         a2 = R(0.5) * (aL * aL + aR * aR);
     }
     const R aA = sqrt(a2);
@@ -415,8 +530,16 @@ CTBFM_DI S5<R> bcOutlet(const DevCaseT<R>& c, Gas<R> gs, const S5<R>& Uint, V3<R
     const R a = soundSpeed_p_rho(gs, p, W.v[0]);
     if (mag(u) >= a) return advFlux(gs, W, n);
     const R pb = rampedOutletPressure(c, it, pOut);
-    const R rhob = pb * rho / p;
-    const R eb = staticEnergy_p_rho(gs, pb, rhob);
+    R rhob, eb;
+    if (gs.lut) {  // isentropic extrapolation (src/boundary_base.cpp:206-211)
+        const R eInt = W.v[4] - R(0.5) * dot(u, u);
+        const R sInt = lutInterp(gs.lut->re[kReS], rho, eInt);
+        rhob = lutInterp(gs.lut->ps[kPsRho], pb, sInt);
+        eb = lutInterp(gs.lut->ps[kPsE], pb, sInt);
+    } else {
+        rhob = pb * rho / p;
+        eb = staticEnergy_p_rho(gs, pb, rhob);
+    }
     const R etb = eb + R(0.5) * dot(u, u);
     return advFlux(gs, s5(rhob, u.x, u.y, u.z, etb), n);
 }
@@ -454,6 +577,35 @@ CTBFM_DI S5<R> bcInlet(const DevCaseT<R>& c, Gas<R> gs, const DevPatch& pt, cons
     R Cg = dot(dir, n);
     if (Cg >= R(0)) Cg = R(-1);
     const R Rout = pInt + Z * unInt;
+    if (gs.lut) {  // src/boundary_base.cpp:78-111, the search in double on the (p, s) tables
+        const DevLut& L = *gs.lut;
+        const double Ptd = pt.v[0], Ttd = pt.v[1];
+        const double Zd = Z, Cgd = Cg, Routd = Rout;
+        const double sIn = lutInterp(L.pt[kPtS], Ptd, Ttd);
+        const double htIn = lutEnthalpy_p_s(L, Ptd, sIn);
+        double pLow = 0.05 * Ptd, pHigh = 0.999999 * Ptd;
+        double pB = 0.5 * (pLow + pHigh);
+        for (int iter = 0; iter < 30; ++iter) {
+            const double pMid = 0.5 * (pLow + pHigh);
+            const double hMid = lutEnthalpy_p_s(L, pMid, sIn);
+            const double VMid = sqrt(2.0 * rmax(0.0, htIn - hMid));
+            const double res = pMid + Zd * Cgd * VMid - Routd;
+            if (fabs(res) < 1e-4 * Ptd) {
+                pB = pMid;
+                break;
+            }
+            if (res < 0.0) pLow = pMid;
+            else pHigh = pMid;
+            pB = pMid;
+        }
+        const double hB = lutEnthalpy_p_s(L, pB, sIn);
+        const R VB = R(sqrt(2.0 * rmax(0.0, htIn - hB)));
+        const V3<R> uB = dir * VB;
+        const R rhoB = R(lutInterp(L.ps[kPsRho], pB, sIn));
+        const R eB = R(lutInterp(L.ps[kPsE], pB, sIn));
+        const R etB = eB + R(0.5) * dot(uB, uB);
+        return advFlux(gs, s5(rhoB, uB.x, uB.y, uB.z, etB), n);
+    }
     const R g = gs.g, Rg = gs.R_;
     const R cp = g * Rg / (g - R(1));
     const R htIn = cp * Tt;

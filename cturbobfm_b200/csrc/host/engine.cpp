@@ -103,6 +103,8 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     cudaCheck(cudaMalloc(&dCases_, M * sizeof(DevCaseT<R>)), "cudaMalloc");
     view_.cases = dCases_;
     view_.m = M;
+    view_.ideal = view_.real = false;
+    for (auto* m : members_) (m->c.lut ? view_.real : view_.ideal) = true;
     refresh(nullptr);
     cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");

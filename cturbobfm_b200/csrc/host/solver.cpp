@@ -49,9 +49,18 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     if (config.isViscosityActive()) throw ConfigError("Viscous fluxes are outside this library's Euler path");
     if (config.parseBool("TURBULENCE_ACTIVE", false)) throw ConfigError("Turbulence models are outside this library's Euler path");
     if (config.parseBool("RESTART_SOLUTION", false)) throw ConfigError("Restart files are outside this library's scope");
+    // Config::getFluidModel (src/config.cpp:468-481)
     const std::string fluid = config.has("FLUID_MODEL") ? config.get("FLUID_MODEL") : "None";
-    if (fluid != "None" && fluid != "Ideal" && fluid != "ideal" && fluid != "IDEAL")
-        throw ConfigError("Only the ideal-gas fluid model is supported");
+    if (fluid == "real" || fluid == "Real" || fluid == "REAL") {
+        if (config.parseBool("STOP_ON_TABLE_OUT_OF_BOUNDS", false))
+            throw ConfigError("STOP_ON_TABLE_OUT_OF_BOUNDS is outside this library's scope");
+        if (config.parseBool("FLUID_TABLE_FORCE_REGENERATE", false))
+            throw ConfigError("Regenerating the fluid table is outside this library's scope (pass a .lut file)");
+        // Solver::buildFluidModel (src/solver.cpp:48-74) with an existing table
+        table_ = std::make_unique<FluidTable>(fluidTablePath(config));
+    } else if (fluid != "None" && fluid != "Ideal" && fluid != "ideal" && fluid != "IDEAL") {
+        throw ConfigError("Invalid value for key \"FLUID_MODEL\" in configuration.");
+    }
     if (config.isAccelerationActive() && config.getTimeStepMethod() != TimeStepMethod::Fixed)
         throw ConfigError("Rotational speed scaling factor is only active for fixed time step method");
     // GPU_PRECISION (this library's key; the reference ignores unknown keys)
@@ -290,8 +299,10 @@ void Solver::validateSettings() {
     const TimeStepMethod m = config_.getTimeStepMethod();
     config_.getCFL();
     if (m == TimeStepMethod::Fixed) config_.getFixedTimeStep();
-    config_.getFluidGamma();
-    config_.getFluidGasConstant();
+    if (!table_) {
+        config_.getFluidGamma();
+        config_.getFluidGasConstant();
+    }
     config_.getInitMachNumber();
     config_.getInitTemperature();
     config_.getInitPressure();
@@ -355,8 +366,10 @@ void Solver::setupScalars() {
     c.dt_method = static_cast<int>(config_.getTimeStepMethod());
     c.steady = config_.isSimulationSteady() ? 1 : 0;
     c.drop = config_.getResidualsDropConvergence();
-    c.gamma = config_.getFluidGamma();
-    c.rgas = config_.getFluidGasConstant();
+    // FluidReal::getGamma / getRconstant (include/fluid_real.hpp:100-101): the
+    // table's nominal values
+    c.gamma = table_ ? table_->gammaNominal() : config_.getFluidGamma();
+    c.rgas = table_ ? table_->gasConstant() : config_.getFluidGasConstant();
     c.cp = (c.gamma * c.rgas) / (c.gamma - 1);
     c.cfl = config_.getCFL();
     c.fixed_dt = c.dt_method == 2 ? config_.getFixedTimeStep() : 0.0;
@@ -564,6 +577,7 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
     }
     c.dt = inst.allocR(N);
     c.partial = inst.allocD(static_cast<size_t>(c.node_tiles + c.per_tiles) * 5 + c.node_tiles);
+    c.lut = table_ ? uploadLut(inst) : nullptr;
     c.ctl = static_cast<Control*>(inst.allocBytes(sizeof(Control)));
     c.hist = inst.allocD(static_cast<size_t>(c.hist_cap) * kHistWidth);
 }
@@ -599,13 +613,28 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
                     const double m = dv.magnitude();
                     dir = (m == 0) ? Vec3(0, 0, 0) : dv / m;
                 }
+                const long q = mesh_.idx(i, j, k);
+                if (table_) {  // FluidReal::computeInitFields (src/fluid_real.cpp:346-362)
+                    const double rho = table_->density_p_T(p, T);
+                    const double e = table_->energy_p_T(p, T);
+                    const double a = table_->soundSpeed_rho_e(rho, e);
+                    const double dm = dir.magnitude();
+                    const Vec3 dn = (dm > 1e-12) ? dir / dm : Vec3(1.0, 0.0, 0.0);
+                    const Vec3 u = (dn * a) * M;
+                    const double et = e + 0.5 * u.dot(u);
+                    U[0][q] = rho;
+                    U[1][q] = rho * u.x;
+                    U[2][q] = rho * u.y;
+                    U[3][q] = rho * u.z;
+                    U[4][q] = rho * et;
+                    continue;
+                }
                 const double a = std::sqrt(g * Rg * T);
                 const Vec3 u = (dir / dir.magnitude()) * a * M;
                 const double rho = p / (Rg * T);
                 const double e = p / ((g - 1) * rho);
                 const double um = u.magnitude();
                 const double et = e + 0.5 * (um * um);
-                const long q = mesh_.idx(i, j, k);
                 U[0][q] = rho;
                 U[1][q] = rho * u.x;
                 U[2][q] = rho * u.y;
@@ -629,8 +658,14 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
         Vec3 u;
         prim(mesh_.idx(NI - 1, 0, 0), rho, u, et);
         Control ctl = control();
-        ctl.gz_p = gas.pressure(rho, u, et);
-        ctl.gz_T = gas.temperature(rho, u, et);
+        if (table_) {  // FluidBase::computePressure_primitive / computeTemperature_rho_u_et
+            const double e = FluidTable::staticEnergy_u_et(u, et);
+            ctl.gz_p = table_->pressure_rho_e(rho, e);
+            ctl.gz_T = table_->temperature_rho_e(rho, e);
+        } else {
+            ctl.gz_p = gas.pressure(rho, u, et);
+            ctl.gz_T = gas.temperature(rho, u, et);
+        }
         ctl.gz_min = tp[0];
         ctl.gz_mout = tp[0];
         ctl.gz_t = 0.0;
@@ -645,7 +680,8 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
                 double rho, et;
                 Vec3 u;
                 prim(mesh_.idx(proto_.prof_i[m], proto_.prof_j0[m] + jj, 0), rho, u, et);
-                profP[proto_.prof_off[m] + jj] = gas.pressure(rho, u, et);
+                profP[proto_.prof_off[m] + jj] =
+                    table_ ? table_->pressure_rho_e(rho, FluidTable::staticEnergy_u_et(u, et)) : gas.pressure(rho, u, et);
             }
         cudaCheck(cudaMemcpy(inst.c.prof_p, profP.data(), profP.size() * sizeof(double), cudaMemcpyHostToDevice),
                   "cudaMemcpy");
@@ -921,6 +957,40 @@ long long Solver::history(long long maxRows, double* lognorm, double* massflow, 
         if (hub) hub[r] = row[15];
     }
     return rows;
+}
+
+// The look-up tables on the device: every table in double and as a float copy,
+// and the DevLut that points at them.
+template <typename R>
+const DevLut* Solver::uploadLut(InstanceT<R>& inst) {
+    DevLut h{};
+    auto fill = [&](DevTable& t, const HostTable& src) {
+        t.xmin = src.xmin;
+        t.xmax = src.xmax;
+        t.ymin = src.ymin;
+        t.ymax = src.ymax;
+        t.dx = src.dx;
+        t.dy = src.dy;
+        t.fxmin = static_cast<float>(src.xmin);
+        t.fxmax = static_cast<float>(src.xmax);
+        t.fymin = static_cast<float>(src.ymin);
+        t.fymax = static_cast<float>(src.ymax);
+        t.fdx = static_cast<float>(src.dx);
+        t.fdy = static_cast<float>(src.dy);
+        t.nx = static_cast<int>(src.nx);
+        t.ny = static_cast<int>(src.ny);
+        t.d = inst.uploadD(src.d);
+        std::vector<float> f(src.d.begin(), src.d.end());
+        float* df = static_cast<float*>(inst.allocBytes(f.size() * sizeof(float)));
+        cudaCheck(cudaMemcpy(df, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
+        t.f = df;
+    };
+    for (int q = 0; q < 8; q++) fill(h.re[q], table_->rhoE()[q]);
+    for (int q = 0; q < 4; q++) fill(h.pt[q], table_->pT()[q]);
+    for (int q = 0; q < 3; q++) fill(h.ps[q], table_->pS()[q]);
+    DevLut* d = static_cast<DevLut*>(inst.allocBytes(sizeof(DevLut)));
+    cudaCheck(cudaMemcpy(d, &h, sizeof(DevLut), cudaMemcpyHostToDevice), "cudaMemcpy");
+    return d;
 }
 
 template void Solver::uploadArrays<double>(InstanceT<double>&);

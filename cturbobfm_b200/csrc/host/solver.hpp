@@ -19,6 +19,7 @@
 #include "../device/kernels.hpp"
 #include "config.hpp"
 #include "engine.hpp"
+#include "fluid_table.hpp"
 #include "mesh.hpp"
 #include "models.hpp"
 
@@ -45,6 +46,7 @@ public:
     void setStream(cudaStream_t s) { stream_ = s ? s : ownStream_; }
     cudaStream_t stream() const { return stream_; }
     int precision() const { return prec_; }
+    bool realGas() const { return table_ != nullptr; }
 
     // Enqueues n iterations (no host sync). Kernels of iterations after
     // convergence / divergence return immediately.
@@ -91,6 +93,8 @@ private:
     void uploadArrays(InstanceT<R>& inst);
     template <typename R>
     void initializeState(InstanceT<R>& inst, GroupT<R>& grp);
+    template <typename R>
+    const DevLut* uploadLut(InstanceT<R>& inst);
     template <typename F>
     auto visit(F&& f) {
         if (prec_ == kFP32Kahan) return f(*i32_, *g32_);
@@ -105,6 +109,7 @@ private:
     int prec_ = kFP64;
     std::unique_ptr<AdvectionBase> advection_;
     std::unique_ptr<SourceBFMBase> bfm_;
+    std::unique_ptr<FluidTable> table_;  // FLUID_MODEL = real
     std::vector<BoundaryPatch> boundaries_;
     bool needTurbo_ = false;
     double periodicAngleDeg_ = 0.0, periodicAngleRad_ = 0.0, periodicTransl_ = 0.0;

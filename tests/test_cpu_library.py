@@ -61,6 +61,7 @@ def test_missing_input_file_is_a_config_error(lib, tmp_path):
     ("ENABLE_GREITZER_MODELING", "yes", "Greitzer modeling is only compatible with fixed time step method"),
     ("INLET_REFERENCE_FRAME", "polar", "Invalid value for key \"INLET_REFERENCE_FRAME\""),
     ("GPU_PRECISION", "fp16", "Invalid value for key \"GPU_PRECISION\""),
+    ("FLUID_MODEL", "vdw", "Invalid value for key \"FLUID_MODEL\""),
 ])
 def test_invalid_settings_are_rejected(lib, tmp_path, key, value, message):
     from cturbobfm_b200 import cases
@@ -107,3 +108,19 @@ def test_server_reports_a_bad_request_without_device_work(lib, tmp_path):
     assert len(res) == 1 and res[0]["id"] == rid
     assert res[0]["error"] == 1 and res[0]["status"] == -1
     assert res[0]["message"]
+
+
+def test_real_gas_table_errors_come_back_as_config_errors(lib, tmp_path):
+    import os
+    from cturbobfm_b200 import cases
+
+    c = cases.with_real_gas(cases.bump2d(ni=12, nj=6), pt=8.0e6, tt=320.0, p_init=7.6e6, t_init=315.0,
+                            table={"n_rho": 8, "n_e": 8, "n_p": 8, "n_T": 8, "n_s": 8})
+    ini = c.write(str(tmp_path / "a"))
+    os.remove(os.path.join(str(tmp_path / "a"), "fluid_table_CO2.lut"))
+    h = ctypes.c_void_p()
+    assert lib.ctbfm_create_from_ini(ini.encode(), ctypes.byref(h)) == 1
+    assert b"FluidReal: Could not open table file at:" in lib.ctbfm_last_error()
+    ini = c.with_settings(STOP_ON_TABLE_OUT_OF_BOUNDS="yes").write(str(tmp_path / "b"))
+    assert lib.ctbfm_create_from_ini(ini.encode(), ctypes.byref(h)) == 1
+    assert b"STOP_ON_TABLE_OUT_OF_BOUNDS" in lib.ctbfm_last_error()
