@@ -32,12 +32,16 @@ namespace {
 // B200 (bench workload and a 768 x 256 JST bump): double Roe faces 3 blocks
 // (85 registers, 69.6 us for the K faces against 76.3 us at 2 blocks and
 // 124 us unbounded), double JST faces 2 (3 spills more than it gains), nodes
-// 3 (63.6 us double, 39.7 us float, against 71.8 / 53.0 us at 2).
+// 3 in double (63.6 us against 71.8 us at 2) and 4 in float (the batched
+// compressor map 5 % faster than at 3).
 template <int SCHEME, typename R>
 constexpr int facesMinBlocks() {
     return (sizeof(R) == 8 && SCHEME == 0) ? 2 : 3;
 }
-constexpr int kNodesMinBlocks = 3;
+template <typename R>
+constexpr int nodesMinBlocks() {
+    return sizeof(R) == 8 ? 3 : 4;
+}
 
 // Block entry: reads the block's tile, returns false (the whole block leaves
 // before touching anything else) when its instance has converged, diverged,
@@ -262,7 +266,7 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 // U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
 // Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
 template <typename R, int FL>
-__global__ void __launch_bounds__(256, kNodesMinBlocks) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+__global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
