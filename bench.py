@@ -230,6 +230,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     from cturbobfm_b200 import Solver
+    from cturbobfm_b200.replicas import max_over_ranks, whole_job_rate
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
@@ -272,11 +273,8 @@ def run_ours(args):
     done = solver.iteration - it0
     if done != args.steps or solver.status != 0:
         raise RuntimeError(f"timed region ran {done} of {args.steps} iterations (status {solver.status})")
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * n * stages * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dev)
+    value = whole_job_rate(n * stages * args.steps, world, ms_max)
 
     u64 = solver.state() if world == 1 else None
 
@@ -319,10 +317,7 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * stages * args.steps / (float(te.item()) / 1e3)
+    e2e_value = whole_job_rate(n * stages * args.steps, world, max_over_ranks(e0.elapsed_time(e1), dev))
 
     # per-kernel device times (CUDA events on the launching stream)
     prof = solver.profile_kernels(reps=10)
