@@ -145,7 +145,7 @@ def port_iteration_seconds(ini_path: str, n_iter: int) -> float:
     return (time.perf_counter() - t0) / n_iter
 
 
-def cpu_baseline(case, n_iter: int):
+def cpu_baseline(case, n_iter: int, one_core_iters: int = 0):
     from oracle import oracle
 
     stages = case.n_stages
@@ -159,10 +159,17 @@ def cpu_baseline(case, n_iter: int):
             threads = 1
             sec = port_iteration_seconds(ini, n_iter)
             kind = "port"
+        one_core = None
+        if kind == "reference" and one_core_iters > 0:
+            one_core = case.n_nodes * stages / reference_iteration_seconds(d, one_core_iters, 1)
     value = case.n_nodes * stages / sec
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{n_iter} iterations of the same {case.shape[0]}x{case.shape[1]}x{case.shape[2]} case "
-                      f"({n_iter * stages} stages), set-up subtracted", "seconds_per_iteration": sec}
+    out = {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"{n_iter} iterations of the same {case.shape[0]}x{case.shape[1]}x{case.shape[2]} case "
+                     f"({n_iter * stages} stages), set-up subtracted", "seconds_per_iteration": sec}
+    if one_core is not None:
+        out["value_1_core"] = one_core
+        out["sample_1_core"] = f"{one_core_iters} iterations on 1 thread, set-up subtracted"
+    return out
 
 
 def run_reference_arm(args):
@@ -346,6 +353,7 @@ def run_ours(args):
             "workload": WORKLOAD, "nodes": n, "stages_per_step": stages,
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "l2": f"inputs larger than L2: device working set {solver_bytes(solver, case) / 2**20:.0f} MiB > 126 MiB",
+            "face_tiles_autotuned": list(solver.info().face_tile),
         },
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 5 * 8 * n,
@@ -357,11 +365,18 @@ def run_ours(args):
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "kernel_ms": prof, "kernel_share": {k: v / total for k, v in shares.items() if v > 0},
     }
+    # stage-level view: the compulsory bytes of a fused stage per cell-stage
+    # (5 words read U(k-1), 5 read U^n, 5 written, dt/V, 3 face vectors of
+    # 3 FP64 words) at the measured cell-stage rate
+    b_stage = 8.0 * 16 + 8.0 * 3 * 3
+    line["stage_roofline"] = {"bytes_per_cell_stage": b_stage, "achieved": value * b_stage / 1e9,
+                              "peak": peak, "unit": "GB/s", "frac": value * b_stage / 1e9 / peak}
     if fp32:
         line["fp32_kahan"] = fp32
     if world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(case, args.cpu_iters)
-        line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        base = cpu_baseline(case, args.cpu_iters, one_core_iters=3)
+        line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample", "value_1_core",
+                                                     "sample_1_core") if k in base}
     print(json.dumps(line), flush=True)
     solver.close()
 

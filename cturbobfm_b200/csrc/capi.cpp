@@ -129,6 +129,7 @@ int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out) {
         out->precision = s->solver->precision();
         out->time = c.t;
         out->device_bytes = static_cast<int64_t>(s->solver->deviceBytes());
+        for (int d = 0; d < 3; d++) out->face_tile[d] = s->solver->faceTile(d);
         return CTBFM_OK;
     });
 }

@@ -60,23 +60,40 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     nstages_ = 0;
     for (auto* m : members_) nstages_ = std::max(nstages_, m->c.nstages);
     const int M = static_cast<int>(members_.size());
-    // tile lists over the packed index of all members
+    buildTiles();
+    cudaCheck(cudaMalloc(&dCases_, M * sizeof(DevCaseT<R>)), "cudaMalloc");
+    view_.cases = dCases_;
+    view_.m = M;
+    view_.ideal = view_.real = false;
+    for (auto* m : members_) (m->c.lut ? view_.real : view_.ideal) = true;
+    refresh(nullptr);
+    cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+// Tile lists over the packed index of all members. Node tiles are kTileSize
+// elements (the per-tile reduction partials depend on it); face tiles take the
+// per-direction size the autotuner chose (any multiple of the block size: a
+// block loops over its tile).
+template <typename R>
+void GroupT<R>::buildTiles() {
+    const int M = static_cast<int>(members_.size());
     std::vector<Tile> node, face[3][2], per, inst, bint, bintAll;
-    auto cover = [](std::vector<Tile>& out, int m, long long count) {
+    auto cover = [](std::vector<Tile>& out, int m, long long count, long long size) {
         int local = 0;
-        for (long long s = 0; s < count; s += kTileSize) out.push_back({m, local++, s, std::min<long long>(kTileSize, count - s)});
+        for (long long s = 0; s < count; s += size) out.push_back({m, local++, s, std::min<long long>(size, count - s)});
         return local;
     };
     for (int m = 0; m < M; m++) {
         const DevCaseT<R>& c = members_[m]->c;
-        const int nt = cover(node, m, c.n);
+        const int nt = cover(node, m, c.n, kTileSize);
         if (nt != c.node_tiles) throw std::logic_error("node tile count mismatch");
         for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++) {
             const long long nf =
                 static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
-            cover(face[d][c.scheme], m, nf);
+            cover(face[d][c.scheme], m, nf, faceTile_[d]);
         }
-        if (c.periodic) cover(per, m, static_cast<long long>(c.ni) * c.nj);
+        if (c.periodic) cover(per, m, static_cast<long long>(c.ni) * c.nj, kTileSize);
         inst.push_back({m, 0, 0, 1});
         for (int b = 0; b < 8; b++) {
             bintAll.push_back({m, b, 0, 1});
@@ -97,17 +114,56 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     add(view_.inst, inst);
     add(view_.bint, bint);
     add(view_.bintAll, bintAll);
+    if (dTiles_) cudaCheck(cudaFree(dTiles_), "cudaFree");
+    dTiles_ = nullptr;
     cudaCheck(cudaMalloc(&dTiles_, std::max<size_t>(all.size(), 1) * sizeof(Tile)), "cudaMalloc");
     cudaCheck(cudaMemcpy(dTiles_, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice), "cudaMemcpy");
+    // a copy from pageable memory may still be in flight when cudaMemcpy
+    // returns, and the kernels run on non-blocking streams: wait for it
+    cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
     for (auto& [tl, off] : offs) tl->tiles = dTiles_ + off;
-    cudaCheck(cudaMalloc(&dCases_, M * sizeof(DevCaseT<R>)), "cudaMalloc");
-    view_.cases = dCases_;
-    view_.m = M;
-    view_.ideal = view_.real = false;
-    for (auto* m : members_) (m->c.lut ? view_.real : view_.ideal) = true;
-    refresh(nullptr);
-    cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
-    cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (graph_) {  // launches captured with the old lists
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+}
+
+// Autotuner of the face tiles: per direction, times the face kernels of the
+// current state (stage 0, forced; they only rewrite the face contributions,
+// which the next stage recomputes) with tiles of 256 to 2048 faces and keeps
+// the fastest, a larger tile only when it is at least 2 % faster. Results do
+// not depend on the tiling (every face is computed on its own).
+template <typename R>
+void GroupT<R>::tune(cudaStream_t s) {
+    tuned_ = true;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaCheck(cudaEventCreate(&e0), "cudaEventCreate");
+    cudaCheck(cudaEventCreate(&e1), "cudaEventCreate");
+    const int sizes[] = {256, 512, 1024, 2048};
+    for (int d = 0; d < 3; d++) {
+        if (!view_.face[d][0].n && !view_.face[d][1].n) continue;
+        float best = 0.f;
+        int bestSize = kTileSize;
+        for (int sz : sizes) {
+            faceTile_[d] = sz;
+            buildTiles();
+            cudaCheck(Launcher<R>::faces(view_, d, 0, 1, s), "launch k_faces (tuning)");
+            cudaCheck(cudaEventRecord(e0, s), "cudaEventRecord");
+            for (int r = 0; r < 3; r++) cudaCheck(Launcher<R>::faces(view_, d, 0, 1, s), "launch k_faces (tuning)");
+            cudaCheck(cudaEventRecord(e1, s), "cudaEventRecord");
+            cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (sz == sizes[0] || ms < 0.98f * best) {
+                best = ms;
+                bestSize = sz;
+            }
+        }
+        faceTile_[d] = bestSize;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    buildTiles();
 }
 
 template <typename R>
@@ -148,6 +204,7 @@ void GroupT<R>::capture() {
 template <typename R>
 void GroupT<R>::enqueue(long long n, cudaStream_t s) {
     if (n <= 0) return;
+    if (!tuned_ && autotune_ && n >= kTuneMinIterations) tune(s);
     cudaCheck(Launcher<R>::setLimits(view_, n, s), "launch k_set_limits");
     long long left = n;
     if (left >= graphIters_) {

@@ -64,9 +64,16 @@ public:
     // Re-uploads the members' descriptions (after a member's host copy
     // changed), ordered on stream s; allocates nothing.
     void refresh(cudaStream_t s);
+    // Chooses the face-tile size per direction by timing (done once, at the
+    // first enqueue of at least kTuneMinIterations iterations, when enabled).
+    void tune(cudaStream_t s);
+    void setAutotune(bool on) { autotune_ = on; }
+    int faceTile(int d) const { return faceTile_[d]; }
+    static constexpr long long kTuneMinIterations = 64;
 
 private:
     void capture();
+    void buildTiles();
 
     std::vector<InstanceT<R>*> members_;
     int nstages_ = 0;
@@ -76,6 +83,9 @@ private:
     cudaStream_t captureStream_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
     int graphIters_ = 8;
+    int faceTile_[3] = {kTileSize, kTileSize, kTileSize};
+    bool tuned_ = false;
+    bool autotune_ = true;
 };
 
 extern template class InstanceT<double>;

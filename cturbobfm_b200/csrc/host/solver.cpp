@@ -92,6 +92,9 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
         g64_ = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{i64_.get()});
         initializeState(*i64_, *g64_);
     }
+    // host-to-device copies from pageable memory may still be in flight when
+    // cudaMemcpy returns; the solver's kernels run on a non-blocking stream
+    cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
 }
 
 // Solver::buildAdvectionModel / buildBfmInfo (src/solver.cpp:185-198, 701-749).
@@ -903,6 +906,7 @@ void Solver::profileKernels(int reps, double* outMs) {
         cudaCheck(cudaMemcpy(inst.c.dt, dtSaved.data(), N * sizeof(R), cudaMemcpyHostToDevice), "cudaMemcpy");
         *hostCtl_ = saved;
         cudaCheck(cudaMemcpy(inst.c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
+        cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
     });
 }
 
@@ -937,6 +941,7 @@ void Solver::promoteToFP64() {
     cudaCheck(cudaMemcpy(i64_->c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
     g32_.reset();
     i32_.reset();
+    cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
 }
 
 long long Solver::history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub) {

@@ -47,6 +47,7 @@ public:
     cudaStream_t stream() const { return stream_; }
     int precision() const { return prec_; }
     bool realGas() const { return table_ != nullptr; }
+    int faceTile(int d) const { return g64_ ? g64_->faceTile(d) : g32_->faceTile(d); }
 
     // Enqueues n iterations (no host sync). Kernels of iterations after
     // convergence / divergence return immediately.

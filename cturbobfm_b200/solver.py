@@ -52,6 +52,7 @@ class Info(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("time", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
+        ("face_tile", ctypes.c_int32 * 3),
     ]
 
 

@@ -69,6 +69,7 @@ typedef struct {
     int32_t precision;        /* GPU_PRECISION: 0 = fp64, 1 = fp32_kahan */
     double time;              /* physical time sum of min(dt) */
     int64_t device_bytes;     /* device memory the solver holds */
+    int32_t face_tile[3];     /* faces per block chosen by the autotuner per direction (I, J, K) */
 } ctbfm_info;
 
 /* Builds a solver from an input.ini in the reference's format (the grid CSV and

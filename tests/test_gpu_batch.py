@@ -128,3 +128,21 @@ def test_promotion_carries_the_solve_over_to_fp64(tmp_path):
         assert s.iteration == 100
         assert len(s.history()["lognorm"]) == 40
         assert np.isfinite(s.state()).all()
+
+
+def test_autotuned_face_tiles_leave_results_unchanged(tmp_path, oracle_lib):
+    from cturbobfm_b200 import Solver
+
+    # 100 iterations trigger the face-tile autotuner at the first enqueue;
+    # the state must still match the oracle as closely as untuned runs do
+    ini = cases.bump2d(ni=96, nj=32).write(str(tmp_path))
+    o = oracle_lib.Oracle(ini)
+    o.run(100)
+    with Solver(ini) as s:
+        assert s.step(100) == 100
+        tiles = list(s.info().face_tile)
+        u = s.state()
+    assert all(t in (256, 512, 1024, 2048) for t in tiles)
+    ref = o.state()
+    err = (np.abs(u - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)).max()
+    assert err <= 1e-12
