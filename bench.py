@@ -680,7 +680,8 @@ def run_serve(args):
                 os.makedirs(d)
                 inis.append((t, c.write(d), c.n_nodes, c.shape[2] > 1))
             res = {}
-            with Server(chunk=args.serve_chunk, stall_window=0, host_threads=8) as srv:
+            with Server(chunk=args.serve_chunk, stall_window=0, host_threads=8,
+                        max_active_nodes=args.serve_max_nodes) as srv:
                 t0 = time.perf_counter()
                 nxt = 0
                 ids = {}
@@ -720,7 +721,8 @@ def run_serve(args):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+kahan (f64 integrals)",
         "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "rates_per_s": args.serve_rates, "requests_per_rate": args.serve_n,
-                   "chunk_iterations": args.serve_chunk, "clock": "host wall clock from submit to retirement"},
+                   "chunk_iterations": args.serve_chunk, "max_active_nodes": args.serve_max_nodes,
+                   "clock": "host wall clock from submit to retirement"},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "per_rate": per_rate,
     }
@@ -753,6 +755,9 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[5.0, 20.0, 80.0])
     ap.add_argument("--serve-n", type=int, default=48)
     ap.add_argument("--serve-chunk", type=int, default=100)
+    ap.add_argument("--serve-max-nodes", type=int, default=1500000,
+                    help="grid nodes admitted at once (about what fills the GPU; 0: no limit, every arrival "
+                         "shares the device at once)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -307,14 +307,15 @@ int ctbfm_promote_fp64(ctbfm_solver* s) {
     });
 }
 
-int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t chunk_iterations,
-                        int64_t stall_window, int32_t host_threads, ctbfm_server** out) {
+int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t max_active_nodes,
+                        int64_t chunk_iterations, int64_t stall_window, int32_t host_threads, ctbfm_server** out) {
     if (!out) return setError(CTBFM_E_ARGUMENT, "null argument");
     *out = nullptr;
     return guarded([&] {
         ctbfm::ServerOptions o;
         o.budget_bytes = static_cast<size_t>(device_budget_bytes);
         o.max_active = max_active;
+        o.max_active_nodes = max_active_nodes;
         o.chunk = chunk_iterations;
         o.stall_window = stall_window;
         o.host_threads = host_threads;

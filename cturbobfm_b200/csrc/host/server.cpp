@@ -17,6 +17,7 @@ double steadySeconds() {
 Server::Server(const ServerOptions& o) : opt_(o), t0_(steadySeconds()) {
     if (opt_.chunk <= 0) throw std::invalid_argument("chunk must be positive");
     if (opt_.max_active <= 0) throw std::invalid_argument("max_active must be positive");
+    if (opt_.max_active_nodes < 0) throw std::invalid_argument("max_active_nodes must be >= 0");
     if (opt_.stall_window < 0) throw std::invalid_argument("stall_window must be >= 0");
     const int nt = std::max(1, opt_.host_threads);
     for (int t = 0; t < nt; t++) workers_.emplace_back([this] { worker(); });
@@ -149,6 +150,9 @@ void Server::pump(int* nActive, int* nWaiting) {
                     budget = used_ + freeB * 9 / 10;
                 }
                 if (used_ + need > budget && !active_.empty()) break;
+                if (opt_.max_active_nodes > 0 && usedNodes_ + queue_.front()->nodes > opt_.max_active_nodes &&
+                    !active_.empty())
+                    break;
             }
             j = std::move(queue_.front());
             queue_.pop_front();
@@ -175,6 +179,7 @@ void Server::pump(int* nActive, int* nWaiting) {
         if (bytesPerNode_[p] == 0 && j->nodes > 0)
             bytesPerNode_[p] = static_cast<double>(j->bytes) / static_cast<double>(j->nodes);
         used_ += j->bytes;
+        usedNodes_ += j->nodes;
         j->t_admit = now();
         active_.push_back(std::move(j));
         dirty_ = true;
@@ -210,6 +215,7 @@ void Server::pump(int* nActive, int* nWaiting) {
                     dirty_ = true;
                 }
                 used_ -= std::min(used_, j->bytes);
+                usedNodes_ -= std::min(usedNodes_, j->nodes);
                 retire(std::move(j), &c, 0, "");
                 continue;
             }

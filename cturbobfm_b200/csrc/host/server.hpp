@@ -39,6 +39,7 @@ struct ServerResult {
 struct ServerOptions {
     size_t budget_bytes = 0;      // device memory the admitted solves may hold (0: 90 % of free)
     int max_active = 1024;        // admitted solves at most
+    long long max_active_nodes = 0;  // grid nodes of the admitted solves together at most (0: no limit)
     long long chunk = 200;        // iterations between scheduling rounds
     long long stall_window = 0;   // fp32_kahan -> FP64 after this many iterations without progress (0: never)
     int host_threads = 4;         // workers preparing requests
@@ -93,6 +94,7 @@ private:
     std::vector<int> idx64_, idx32_;  // active_ index of each batch member
     bool dirty_ = false;
     size_t used_ = 0;
+    long long usedNodes_ = 0;
     double bytesPerNode_[2] = {0, 0};  // measured per precision (0: not yet)
     std::vector<ServerResult> done_;
 };

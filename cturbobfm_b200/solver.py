@@ -101,8 +101,8 @@ SIGNATURES = {
     "ctbfm_batch_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_batch_status": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_I64), _DP, _DP], ctypes.c_int),
     "ctbfm_promote_fp64": ([_VP], ctypes.c_int),
-    "ctbfm_server_create": ([ctypes.c_uint64, ctypes.c_int32, _I64, _I64, ctypes.c_int32, ctypes.POINTER(_VP)],
-                            ctypes.c_int),
+    "ctbfm_server_create": ([ctypes.c_uint64, ctypes.c_int32, _I64, _I64, _I64, ctypes.c_int32,
+                             ctypes.POINTER(_VP)], ctypes.c_int),
     "ctbfm_server_destroy": ([_VP], None),
     "ctbfm_server_submit": ([_VP, ctypes.c_char_p, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_server_pump": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -319,10 +319,10 @@ class Server:
     """Continuous batching of operating-point solves (ctbfm_server_*)."""
 
     def __init__(self, budget_bytes: int = 0, max_active: int = 1024, chunk: int = 200, stall_window: int = 0,
-                 host_threads: int = 4):
+                 host_threads: int = 4, max_active_nodes: int = 0):
         h = _VP()
-        _check(load_library().ctbfm_server_create(int(budget_bytes), int(max_active), int(chunk), int(stall_window),
-                                                  int(host_threads), ctypes.byref(h)))
+        _check(load_library().ctbfm_server_create(int(budget_bytes), int(max_active), int(max_active_nodes), int(chunk),
+                                                  int(stall_window), int(host_threads), ctypes.byref(h)))
         self._h = h
 
     def close(self):

@@ -232,12 +232,15 @@ typedef struct {
 
 /* device_budget_bytes: device memory the admitted solves may hold (0: 90 % of
  * what is free at each admission); max_active: admitted solves at most;
- * chunk_iterations: iterations per scheduling round; stall_window: a
+ * max_active_nodes: grid nodes the admitted solves may hold together (0: no
+ * limit; about the node count that fills the GPU keeps early arrivals from
+ * sharing the device with every later one); chunk_iterations: iterations
+ * per scheduling round; stall_window: a
  * fp32_kahan solve whose convergence progress (best_drop of
  * ctbfm_batch_status) has not grown by 0.05 for this many iterations
  * continues in FP64 (0: never); host_threads: request-preparation workers. */
-int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t chunk_iterations,
-                        int64_t stall_window, int32_t host_threads, ctbfm_server** out);
+int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t max_active_nodes,
+                        int64_t chunk_iterations, int64_t stall_window, int32_t host_threads, ctbfm_server** out);
 void ctbfm_server_destroy(ctbfm_server* s);
 
 /* Queues the operating point of an input.ini; thread safe. */

@@ -112,3 +112,17 @@ def test_a_bad_request_fails_alone(tmp_path):
         res = _drain(s, 2)
     assert res[bad]["error"] == 1 and res[bad]["status"] == -1
     assert res[ok]["error"] == 0 and res[ok]["status"] == 1
+
+
+def test_node_limit_admits_in_arrival_order(tmp_path):
+    from cturbobfm_b200 import Server
+
+    inis = [_write(_req(f"n{m}", 64, 24, 1.0 + 0.05 * m, 0.95), str(tmp_path)) for m in range(3)]
+    with Server(chunk=200, max_active_nodes=int(64 * 24 * 1.5)) as s:
+        ids = [s.submit(i) for i in inis]
+        res = _drain(s, 3)
+    order = sorted(res.values(), key=lambda r: r["t_admit"])
+    assert [r["id"] for r in order] == ids
+    for prev, nxt in zip(order, order[1:]):
+        assert nxt["t_admit"] >= prev["t_done"]
+    assert all(r["status"] == 1 for r in res.values())
