@@ -25,7 +25,13 @@ struct BatchView {
     bool ideal = true;  // some member uses the ideal gas
     bool real = false;  // some member uses the real-gas look-up tables
     TileList node;        // nodes of every instance (k_prim, k_nodes, k_dt)
-    TileList face[3][2];  // faces per direction and scheme (0 JST, 1 Roe)
+    // faces per direction, scheme (0 JST, 1 Roe) and face set: 0 every face
+    // of the direction; for K lines of at least 3 nodes, and J lines of at
+    // least 3 nodes whose rows of nk faces do not fall on whole warps, 1 the
+    // faces two or more faces from both ends of each line (plain interior
+    // stencils) and 2 the four faces at the ends (boundary and next-to-
+    // boundary stencils), so that no warp mixes the two code paths
+    TileList face[3][2][3];
     TileList per;         // periodic (i, j) pairs of periodic instances
     TileList inst;        // one tile per instance (k_pre, k_finalize)
     TileList bint;        // 8 plane tiles per instance that needs turbo performance

@@ -165,8 +165,12 @@ __device__ __forceinline__ S5<double> state64(const DevCaseT<R>& c, R* const* U,
 
 // ------------------------------------------------------------------ faces
 // Solver::computeAdvectionFluxResidualsImpl (src/solver.cpp:1865-2040): one
-// thread per face of direction DIR; writes flux * |S|.
-template <int DIR, int SCHEME, typename R, int FL>
+// thread per face of direction DIR; writes flux * |S|. SET 0 enumerates every
+// face of the direction in storage order; for J and K, SET 1 enumerates the
+// faces at positions 2 .. n-2 along each line and SET 2 the faces at 0, 1,
+// n-1 and n (n = nj or nk, at least 3), the k index fastest where the line
+// is not along k, so that warps of one launch take one code path.
+template <int DIR, int SCHEME, typename R, int FL, int SET>
 __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
@@ -178,11 +182,43 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
     const int nlast = DIR == 0 ? c.ni : (DIR == 1 ? c.nj : c.nk);
     const DevFacesT<R>& F = c.f[DIR];
     R* const* U = stageIn(c, stage);
-    for (long long f = tl.start + threadIdx.x; f < tl.start + tl.count; f += blockDim.x) {
-        const int fk = static_cast<int>(f % nfk);
-        const long long t = f / nfk;
-        const int fj = static_cast<int>(t % nfj);
-        const int fi = static_cast<int>(t / nfj);
+    for (long long p = tl.start + threadIdx.x; p < tl.start + tl.count; p += blockDim.x) {
+        long long f;
+        int fi, fj, fk;
+        if (SET == 0 || DIR == 0) {
+            f = p;
+            fk = static_cast<int>(f % nfk);
+            const long long t = f / nfk;
+            fj = static_cast<int>(t % nfj);
+            fi = static_cast<int>(t / nfj);
+        } else if (DIR == 1) {
+            fk = static_cast<int>(p % c.nk);
+            const long long t = p / c.nk;
+            if (SET == 1) {
+                const int m = c.nj - 3;
+                fj = 2 + static_cast<int>(t % m);
+                fi = static_cast<int>(t / m);
+            } else {
+                const int s4 = static_cast<int>(t % 4);
+                fj = s4 < 2 ? s4 : c.nj - 3 + s4;
+                fi = static_cast<int>(t / 4);
+            }
+            f = (static_cast<long long>(fi) * nfj + fj) * c.nk + fk;
+        } else {
+            long long t;
+            if (SET == 1) {
+                const int m = c.nk - 3;
+                fk = 2 + static_cast<int>(p % m);
+                t = p / m;
+            } else {
+                const int s4 = static_cast<int>(p % 4);
+                fk = s4 < 2 ? s4 : c.nk - 3 + s4;
+                t = p / 4;
+            }
+            fj = static_cast<int>(t % c.nj);
+            fi = static_cast<int>(t / c.nj);
+            f = (static_cast<long long>(fi) * c.nj + fj) * nfk + fk;
+        }
         const int dface = DIR == 0 ? fi : (DIR == 1 ? fj : fk);
         if (DIR == 2 && c.bfm && c.bpresent[nodeIdx(c, fi, fj, 0)] > R(0)) continue;  // blade rows: no K flux
         V3<R> n = v3(__ldg(F.nx + f), __ldg(F.ny + f), __ldg(F.nz + f));
@@ -787,20 +823,24 @@ cudaError_t Launcher<R>::prim(const BatchView<R>& b, int stage, int force, cudaS
 }
 
 namespace {
+template <int DIR, int SCHEME, int FL, typename R>
+void launchFaceSets(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    const TileList* t = b.face[DIR][SCHEME];
+    if (t[0].n) k_faces<DIR, SCHEME, R, FL, 0><<<t[0].n, 256, 0, s>>>(b.cases, t[0].tiles, stage, force);
+    if (t[1].n) k_faces<DIR, SCHEME, R, FL, 1><<<t[1].n, 256, 0, s>>>(b.cases, t[1].tiles, stage, force);
+    if (t[2].n) k_faces<DIR, SCHEME, R, FL, 2><<<t[2].n, 256, 0, s>>>(b.cases, t[2].tiles, stage, force);
+}
 template <int FL, typename R>
 void launchFaces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s) {
-    for (int sch = 0; sch < 2; sch++) {
-        const TileList& t = b.face[dir][sch];
-        if (!t.n) continue;
-        if (sch == 0) {
-            if (dir == 0) k_faces<0, 0, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else if (dir == 1) k_faces<1, 0, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else k_faces<2, 0, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-        } else {
-            if (dir == 0) k_faces<0, 1, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else if (dir == 1) k_faces<1, 1, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-            else k_faces<2, 1, R, FL><<<t.n, 256, 0, s>>>(b.cases, t.tiles, stage, force);
-        }
+    if (dir == 0) {
+        launchFaceSets<0, 0, FL>(b, stage, force, s);
+        launchFaceSets<0, 1, FL>(b, stage, force, s);
+    } else if (dir == 1) {
+        launchFaceSets<1, 0, FL>(b, stage, force, s);
+        launchFaceSets<1, 1, FL>(b, stage, force, s);
+    } else {
+        launchFaceSets<2, 0, FL>(b, stage, force, s);
+        launchFaceSets<2, 1, FL>(b, stage, force, s);
     }
 }
 }  // namespace

@@ -78,7 +78,7 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
 template <typename R>
 void GroupT<R>::buildTiles() {
     const int M = static_cast<int>(members_.size());
-    std::vector<Tile> node, face[3][2], per, inst, bint, bintAll;
+    std::vector<Tile> node, face[3][2][3], per, inst, bint, bintAll;
     auto cover = [](std::vector<Tile>& out, int m, long long count, long long size) {
         int local = 0;
         for (long long s = 0; s < count; s += size) out.push_back({m, local++, s, std::min<long long>(size, count - s)});
@@ -91,7 +91,18 @@ void GroupT<R>::buildTiles() {
         for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++) {
             const long long nf =
                 static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
-            cover(face[d][c.scheme], m, nf, faceTile_[d]);
+            const int nline = d == 1 ? c.nj : c.nk;  // nodes along a J or K line
+            // J rows of nk faces fall on whole warps when nk is a multiple of
+            // 32: no warp mixes end and plain faces, one launch is cheaper
+            const bool aligned = d == 1 && c.nk % 32 == 0;
+            if (d == 0 || nline < 3 || aligned) {
+                cover(face[d][c.scheme][0], m, nf, faceTile_[d]);
+            } else {
+                // plain faces 2 .. n-2 and the four end faces of every line
+                const long long lines = d == 1 ? static_cast<long long>(c.ni) * c.nk : static_cast<long long>(c.ni) * c.nj;
+                cover(face[d][c.scheme][1], m, lines * (nline - 3), faceTile_[d]);
+                cover(face[d][c.scheme][2], m, lines * 4, faceTile_[d]);
+            }
         }
         if (c.periodic) cover(per, m, static_cast<long long>(c.ni) * c.nj, kTileSize);
         inst.push_back({m, 0, 0, 1});
@@ -109,7 +120,8 @@ void GroupT<R>::buildTiles() {
     };
     add(view_.node, node);
     for (int d = 0; d < 3; d++)
-        for (int s = 0; s < 2; s++) add(view_.face[d][s], face[d][s]);
+        for (int s = 0; s < 2; s++)
+            for (int k = 0; k < 3; k++) add(view_.face[d][s][k], face[d][s][k]);
     add(view_.per, per);
     add(view_.inst, inst);
     add(view_.bint, bint);
@@ -141,7 +153,10 @@ void GroupT<R>::tune(cudaStream_t s) {
     cudaCheck(cudaEventCreate(&e1), "cudaEventCreate");
     const int sizes[] = {256, 512, 1024, 2048};
     for (int d = 0; d < 3; d++) {
-        if (!view_.face[d][0].n && !view_.face[d][1].n) continue;
+        int nt = 0;
+        for (int sc = 0; sc < 2; sc++)
+            for (int k = 0; k < 3; k++) nt += view_.face[d][sc][k].n;
+        if (!nt) continue;
         float best = 0.f;
         int bestSize = kTileSize;
         for (int sz : sizes) {
