@@ -657,8 +657,10 @@ def run_realgas(args):
 
 # ---------------------------------------------------------------- serving
 SERVE_WORKLOAD = ("serving: Poisson arrivals, 70% axisymmetric compressor-map requests (NI x NJ ~ U{64..256} x "
-                  "U{24..96}) and 30% 3-D annuli (U{96..160} x U{32..48} x U{32..64}), MAP_ROWS stage, "
-                  "p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], JST RK4 CFL 2.2, drop 3 orders, fp32_kahan")
+                  "U{24..96}; a fifth of them throttle + Greitzer plenum requests on U{64..128} x U{24..48}, "
+                  "kt ~ U[0.8,1.0], B ~ U[0.1,0.5] mapped to GREITZER_PLENUM_VOLUME, fixed dt) and 30% 3-D annuli "
+                  "(U{96..160} x U{32..48} x U{32..64}), MAP_ROWS stage, static outlets p_out/pt_in ~ U[1.00,1.20], "
+                  "speed ~ U[0.85,1.00], JST RK4 CFL 2.2, drop 3 orders, fp32_kahan")
 
 
 def run_serve(args):

@@ -399,16 +399,49 @@ def compressor_map(n: int = 256, seed: int = 20261203, ni_range=(64, 256),
     return out
 
 
+def greitzer_plenum_volume(B: float, speed: float, r_hub: float = 0.20, r_tip: float = 0.40, length: float = 0.6,
+                           rpm: float = 10000.0, tt: float = 288.15, gamma: float = 1.4, rgas: float = 287.05) -> float:
+    """GREITZER_PLENUM_VOLUME for a Greitzer B parameter. The reference has no
+    B key; this library maps B = U / (2 a) sqrt(V_p / (A_c L_c)) with U the
+    blade speed at the mean radius, a the inlet stagnation sound speed, A_c
+    the annulus area and L_c the machine length, so
+    V_p = (2 a B / U)^2 A_c L_c."""
+    U = rpm * speed * 2.0 * math.pi / 60.0 * 0.5 * (r_hub + r_tip)
+    a = math.sqrt(gamma * rgas * tt)
+    Ac = math.pi * (r_tip ** 2 - r_hub ** 2)
+    return (2.0 * a * B / U) ** 2 * Ac * length
+
+
+def throttle_request(ni: int, nj: int, kt: float, B: float, speed: float, name: str = "throttle",
+                     precision: Optional[str] = "fp32_kahan", n_iter: int = 40000) -> Case:
+    """An axisymmetric compressor-map request on a throttle with the Greitzer
+    plenum (ENABLE_GREITZER_MODELING, fixed time step): throttle coefficient
+    kt, B parameter mapped by greitzer_plenum_volume, time step
+    dt = 1.2 / ((u + a) / dx + a / dr) with u + a = 440 m/s, a = 340 m/s on the
+    grid's spacings; JST, RK4, residual drop 3 orders."""
+    c = meridional(ni=ni, nj=nj, p_ratio=1.0, speed=speed, cfl=2.2, drop=3, rows=MAP_ROWS, n_iter=n_iter,
+                   name=name, precision=precision)
+    c.patches[1] = dataclasses.replace(c.patches[1], spec=f"throttle, {kt!r}")
+    dx, dr = 0.6 / (ni - 1), 0.2 / (nj - 1)
+    dt = 1.2 / (440.0 / dx + 340.0 / dr)
+    return c.with_settings(TIME_STEP_METHOD="fixed", FIXED_TIME_STEP=repr(dt), ENABLE_GREITZER_MODELING="yes",
+                           GREITZER_PLENUM_VOLUME=repr(greitzer_plenum_volume(B, speed)))
+
+
 def serving_requests(n: int, rate: float, seed: int = 20261203, frac_3d: float = 0.3,
-                     precision: Optional[str] = "fp32_kahan") -> List[Tuple[float, Case]]:
+                     precision: Optional[str] = "fp32_kahan", frac_throttle: float = 0.2) -> List[Tuple[float, Case]]:
     """The serving workload: n operating-point requests with Poisson arrival
     times at `rate` per second, drawn from a seeded PCG64 generator (per
     request: inter-arrival gap, kind, then sizes, back pressure and speed).
     A fraction 1 - frac_3d are axisymmetric instances of the compressor map
-    (NI x NJ ~ U{64..256} x U{24..96}); the rest are 3-D annuli of the same
-    stage with NI x NJ x NK ~ U{96..160} x U{32..48} x U{32..64} (JST + RK4,
-    CFL 2.2). All: p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], outlet
-    ramp 2000 iterations, residual drop 3 orders."""
+    (NI x NJ ~ U{64..256} x U{24..96}), of which a fraction frac_throttle are
+    throttle requests with the Greitzer plenum (throttle_request on NI x NJ ~
+    U{64..128} x U{24..48}: kt ~ U[0.8, 1.0], B ~ U[0.1, 0.5]; finer grids
+    and kt 1.2 diverge from the impulsive throttled start at any time step);
+    the rest are 3-D annuli of the same stage
+    with NI x NJ x NK ~ U{96..160} x U{32..48} x U{32..64} (JST + RK4, CFL
+    2.2). Static-outlet requests: p_out/pt_in ~ U[1.00,1.20], outlet ramp 2000
+    iterations. All: speed ~ U[0.85,1.00], residual drop 3 orders."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     t = 0.0
@@ -421,6 +454,12 @@ def serving_requests(n: int, rate: float, seed: int = 20261203, frac_3d: float =
             ni, nj, nk = int(rng.integers(64, 257)), int(rng.integers(24, 97)), 1
         pr = float(rng.uniform(1.00, 1.20))
         sp = float(rng.uniform(0.85, 1.00))
+        throttle = (not is3d) and bool(rng.uniform() < frac_throttle)
+        if throttle:
+            kt, B = float(rng.uniform(0.8, 1.0)), float(rng.uniform(0.1, 0.5))
+            ni, nj = 64 + (ni - 64) // 3, 24 + (nj - 24) // 3  # U{64..128} x U{24..48}
+            out.append((t, throttle_request(ni, nj, kt, B, sp, name=f"req{m:04d}", precision=precision)))
+            continue
         if is3d:
             c = annulus3d(ni=ni, nj=nj, nk=nk, cfl=2.2, scheme="JST", muscl=False, limiter="None", rk=4,
                           p_ratio=pr, rows=MAP_ROWS, speed=sp, drop=3, ramp=2000, precision=precision,
