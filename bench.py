@@ -680,7 +680,8 @@ def run_serve(args):
             for t, c in reqs:
                 d = os.path.join(tmp.name, f"r{rate}", c.name)
                 os.makedirs(d)
-                inis.append((t, c.write(d), c.n_nodes, c.shape[2] > 1))
+                kind = "3d" if c.shape[2] > 1 else ("throttle" if "ENABLE_GREITZER_MODELING" in c.settings else "axisymmetric")
+                inis.append((t, c.write(d), c.n_nodes, c.shape[2] > 1, kind))
             res = {}
             with Server(chunk=args.serve_chunk, stall_window=0, host_threads=8,
                         max_active_nodes=args.serve_max_nodes) as srv:
@@ -714,6 +715,10 @@ def run_serve(args):
                 "points_per_hour": float(conv.sum() / wall * 3600.0), "wall_s": wall,
                 "arrival_window_s": inis[-1][0],
                 "node_stage_per_s": float((nodes * its).sum() * 4 / wall),
+                "by_kind": {k: {"requests": int(sum(x[4] == k for x in inis)),
+                                "converged": int(sum(conv[i] for i in range(len(inis)) if inis[i][4] == k)),
+                                "diverged": int(sum(res[i]["status"] == 2 for i in range(len(inis)) if inis[i][4] == k))}
+                            for k in ("axisymmetric", "throttle", "3d")},
             }
     clk = clocks.summary()
     first = per_rate[str(args.serve_rates[0])]
