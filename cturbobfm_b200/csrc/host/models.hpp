@@ -3,7 +3,9 @@
 // (include/advection_base.hpp:21-25, include/boundary_base.hpp:26-32,
 // include/source_bfm_base.hpp:20-31). Here they are parameter carriers: each
 // one validates its settings and writes the parameters the batched device
-// kernels read; the arithmetic itself runs on the GPU.
+// kernels read; the arithmetic itself runs on the GPU. They fill the
+// double-typed scalar description (DevCase) that the solver copies into the
+// instance of either working precision.
 #pragma once
 
 #include <memory>
