@@ -68,3 +68,16 @@ def test_step_chunks_equal_one_long_step(tmp_path):
             b.step(n)
         assert np.array_equal(a.state(), b.state())
         assert a.time == b.time
+
+
+def test_full_size_real_gas_workload_matches_oracle(tmp_path, oracle_lib):
+    from cturbobfm_b200 import Solver
+
+    # the 256 x 96 x 128 CO2 annulus (3.1 M nodes): one iteration, FP64
+    ini = cases.realgas_annulus().write(str(tmp_path))
+    o = oracle_lib.Oracle(ini)
+    o.run(1)
+    with Solver(ini) as s:
+        assert s.step(1) == 1
+        assert rel_err(s.state(), o.state()) <= 1e-12
+        assert np.abs(s.lognorm() - o.history()["lognorm"][-1]).max() <= 1e-10
