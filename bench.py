@@ -213,7 +213,15 @@ def algorithmic_bytes(case, kernel: str) -> float:
 
 def launches_per_iteration(case, kernel: str) -> int:
     s = case.n_stages
-    return {"k_faces_I": s, "k_faces_J": s, "k_faces_K": s, "k_nodes": s, "k_periodic": s, "k_prim": s, "k_dt": 1,
+    ni, nj, nk = case.shape
+    # the end faces of K lines (and of J lines whose rows do not fill whole
+    # warps) run in a launch of their own
+    if kernel == "k_faces_K" and nk >= 3:
+        return 2 * s
+    if kernel == "k_faces_J" and nj >= 3 and nk % 32 != 0:
+        return 2 * s
+    return {"k_faces_I": s, "k_faces_J": s, "k_faces_K": s, "k_nodes": s, "k_periodic": s, "k_prim": s,
+            "k_dt": 1,
             "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
 
 
