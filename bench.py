@@ -1,8 +1,11 @@
 """Benchmark of the explicit residual-and-update loop on the full-annulus
 rotor/stator workload (160 x 48 x 64 nodes, Roe + MUSCL van Albada, RK3,
-local time step at CFL 1.2, Hall body force, FP64).
+local time step at CFL 1.0 -- the configuration's 1.2 diverges at iteration
+53 in the reference build too -- Hall body force, FP64, with the fp32_kahan
+arm beside it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload annulus|map|serve|realgas]
 
 One step = one pseudo-time iteration (all Runge-Kutta stages) of the whole
 operating point. The metric is cell-stage updates per second (nodes x stages x
@@ -211,18 +214,25 @@ def algorithmic_bytes(case, kernel: str) -> float:
     return 0.0
 
 
-def launches_per_iteration(case, kernel: str) -> int:
+def calls_per_iteration(case, kernel: str) -> int:
+    """How often per iteration each kernel kind of ctbfm_profile_kernels runs
+    (its timing covers all launches of one call)."""
     s = case.n_stages
-    ni, nj, nk = case.shape
-    # the end faces of K lines (and of J lines whose rows do not fill whole
-    # warps) run in a launch of their own
-    if kernel == "k_faces_K" and nk >= 3:
-        return 2 * s
-    if kernel == "k_faces_J" and nj >= 3 and nk % 32 != 0:
-        return 2 * s
     return {"k_faces_I": s, "k_faces_J": s, "k_faces_K": s, "k_nodes": s, "k_periodic": s, "k_prim": s,
-            "k_dt": 1,
-            "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
+            "k_dt": 1, "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
+
+
+def launches_per_iteration(case, kernel: str) -> int:
+    """Kernel launches per iteration of each kind: the end faces of K lines
+    (and of J lines whose rows do not fill whole warps) run in a launch of
+    their own."""
+    ni, nj, nk = case.shape
+    n = calls_per_iteration(case, kernel)
+    if kernel == "k_faces_K" and nk >= 3:
+        return 2 * n
+    if kernel == "k_faces_J" and nj >= 3 and nk % 32 != 0:
+        return 2 * n
+    return n
 
 
 def measured_peaks():
@@ -336,7 +346,7 @@ def run_ours(args):
 
     # per-kernel device times (CUDA events on the launching stream)
     prof = solver.profile_kernels(reps=10)
-    shares = {k: prof[k] * launches_per_iteration(case, k) for k in prof}
+    shares = {k: prof[k] * calls_per_iteration(case, k) for k in prof}
     total = sum(shares.values()) or 1.0
     dominant = max(shares, key=shares.get)
     peaks = measured_peaks()
