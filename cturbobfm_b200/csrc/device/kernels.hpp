@@ -63,6 +63,10 @@ extern template struct Launcher<float>;
 
 constexpr int kKernelKinds = 10;
 constexpr int kTileSize = 256;  // elements per tile (one per thread)
+// periodic (i, j) pairs per tile, one block of as many threads each: the
+// periodic planes hold few pairs with much work each (7 680 on the bench
+// workload: 120 blocks instead of 30)
+constexpr int kPeriodicTile = 64;
 
 // Static device scratch of ctbfm_compute_residual_noalloc (noalloc.cu): its
 // device address on the current device (looked up once per device) and size.

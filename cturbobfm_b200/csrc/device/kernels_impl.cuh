@@ -861,7 +861,7 @@ cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cuda
 
 template <typename R>
 cudaError_t Launcher<R>::periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.per.n) k_periodic<R><<<b.per.n, 256, 0, s>>>(b.cases, b.per.tiles, stage, force);
+    if (b.per.n) k_periodic<R><<<b.per.n, kPeriodicTile, 0, s>>>(b.cases, b.per.tiles, stage, force);
     return cudaGetLastError();
 }
 

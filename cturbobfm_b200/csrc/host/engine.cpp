@@ -104,7 +104,8 @@ void GroupT<R>::buildTiles() {
                 cover(face[d][c.scheme][2], m, lines * 4, faceTile_[d]);
             }
         }
-        if (c.periodic) cover(per, m, static_cast<long long>(c.ni) * c.nj, kTileSize);
+        if (c.periodic && cover(per, m, static_cast<long long>(c.ni) * c.nj, kPeriodicTile) != c.per_tiles)
+            throw std::logic_error("periodic tile count mismatch");
         inst.push_back({m, 0, 0, 1});
         for (int b = 0; b < 8; b++) {
             bintAll.push_back({m, b, 0, 1});

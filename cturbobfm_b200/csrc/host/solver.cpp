@@ -410,7 +410,7 @@ void Solver::setupScalars() {
     }
     c.compensated = prec_ == kFP32Kahan ? 1 : 0;
     c.node_tiles = static_cast<int>((N + kTileSize - 1) / kTileSize);
-    c.per_tiles = c.periodic ? static_cast<int>((NI * NJ + kTileSize - 1) / kTileSize) : 0;
+    c.per_tiles = c.periodic ? static_cast<int>((NI * NJ + kPeriodicTile - 1) / kPeriodicTile) : 0;
     c.hist_cap = std::min<long long>(std::max<long long>(maxIter_, 1024), 1 << 20);
 }
 
