@@ -139,6 +139,10 @@ void GroupT<R>::buildTiles() {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
     }
+    if (graph1_) {
+        cudaGraphExecDestroy(graph1_);
+        graph1_ = nullptr;
+    }
 }
 
 // Autotuner of the face tiles: per direction, times the face kernels of the
@@ -185,6 +189,7 @@ void GroupT<R>::tune(cudaStream_t s) {
 template <typename R>
 GroupT<R>::~GroupT() {
     if (graph_) cudaGraphExecDestroy(graph_);
+    if (graph1_) cudaGraphExecDestroy(graph1_);
     if (captureStream_) {
         cudaStreamSynchronize(captureStream_);
         cudaStreamDestroy(captureStream_);
@@ -202,21 +207,25 @@ void GroupT<R>::refresh(cudaStream_t s) {
                   "cudaMemcpyAsync");
 }
 
+// Captures `iters` whole iterations into one executable graph.
 template <typename R>
-void GroupT<R>::capture() {
-    if (graph_) return;
+cudaGraphExec_t GroupT<R>::captureIterations(int iters) {
     cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
     cudaCheck(cudaStreamBeginCapture(captureStream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < graphIters_ && e == cudaSuccess; i++) e = Launcher<R>::iteration(view_, nstages_, captureStream_);
+    for (int i = 0; i < iters && e == cudaSuccess; i++) e = Launcher<R>::iteration(view_, nstages_, captureStream_);
     const cudaError_t e2 = cudaStreamEndCapture(captureStream_, &g);
     cudaCheck(e, "launch during graph capture");
     cudaCheck(e2, "cudaStreamEndCapture");
-    const cudaError_t e3 = cudaGraphInstantiate(&graph_, g, 0);
+    const cudaError_t e3 = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     cudaCheck(e3, "cudaGraphInstantiate");
+    return exec;
 }
 
+// n iterations as graphs of graphIters_ iterations plus single-iteration
+// graphs for the rest (one graph launch instead of 20-30 kernel launches).
 template <typename R>
 void GroupT<R>::enqueue(long long n, cudaStream_t s) {
     if (n <= 0) return;
@@ -224,13 +233,14 @@ void GroupT<R>::enqueue(long long n, cudaStream_t s) {
     cudaCheck(Launcher<R>::setLimits(view_, n, s), "launch k_set_limits");
     long long left = n;
     if (left >= graphIters_) {
-        capture();
+        if (!graph_) graph_ = captureIterations(graphIters_);
         while (left >= graphIters_) {
             cudaCheck(cudaGraphLaunch(graph_, s), "cudaGraphLaunch");
             left -= graphIters_;
         }
     }
-    for (long long i = 0; i < left; i++) cudaCheck(Launcher<R>::iteration(view_, nstages_, s), "launch iteration");
+    if (left > 0 && !graph1_) graph1_ = captureIterations(1);
+    for (long long i = 0; i < left; i++) cudaCheck(cudaGraphLaunch(graph1_, s), "cudaGraphLaunch");
 }
 
 template class InstanceT<double>;

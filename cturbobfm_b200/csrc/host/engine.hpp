@@ -72,7 +72,7 @@ public:
     static constexpr long long kTuneMinIterations = 64;
 
 private:
-    void capture();
+    cudaGraphExec_t captureIterations(int iters);
     void buildTiles();
 
     std::vector<InstanceT<R>*> members_;
@@ -81,7 +81,8 @@ private:
     Tile* dTiles_ = nullptr;
     BatchView<R> view_;
     cudaStream_t captureStream_ = nullptr;
-    cudaGraphExec_t graph_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;   // graphIters_ iterations
+    cudaGraphExec_t graph1_ = nullptr;  // one iteration
     int graphIters_ = 8;
     int faceTile_[3] = {kTileSize, kTileSize, kTileSize};
     bool tuned_ = false;
