@@ -436,8 +436,10 @@ def serving_requests(n: int, rate: float, seed: int = 20261203, frac_3d: float =
     A fraction 1 - frac_3d are axisymmetric instances of the compressor map
     (NI x NJ ~ U{64..256} x U{24..96}), of which a fraction frac_throttle are
     throttle requests with the Greitzer plenum (throttle_request on NI x NJ ~
-    U{64..128} x U{24..48}: kt ~ U[0.8, 1.0], B ~ U[0.1, 0.5]; finer grids
-    and kt 1.2 diverge from the impulsive throttled start at any time step);
+    U{64..128} x U{24..48}: kt ~ U[0.8, 1.0], B ~ U[0.1, 0.5], speed ~
+    U[0.85, 0.90]; finer grids, kt 1.2 and speeds from about 0.93 on the
+    finer of these grids diverge from the impulsive throttled start at any
+    time step, in the oracle as on the GPU);
     the rest are 3-D annuli of the same stage
     with NI x NJ x NK ~ U{96..160} x U{32..48} x U{32..64} (JST + RK4, CFL
     2.2). Static-outlet requests: p_out/pt_in ~ U[1.00,1.20], outlet ramp 2000
@@ -458,6 +460,7 @@ def serving_requests(n: int, rate: float, seed: int = 20261203, frac_3d: float =
         if throttle:
             kt, B = float(rng.uniform(0.8, 1.0)), float(rng.uniform(0.1, 0.5))
             ni, nj = 64 + (ni - 64) // 3, 24 + (nj - 24) // 3  # U{64..128} x U{24..48}
+            sp = 0.85 + (sp - 0.85) / 3.0  # U[0.85, 0.90]
             out.append((t, throttle_request(ni, nj, kt, B, sp, name=f"req{m:04d}", precision=precision)))
             continue
         if is3d:
