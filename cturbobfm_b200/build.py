@@ -35,7 +35,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # (source, float kernels: contraction and approximate division / square root)
 CU_SOURCES = [("device/kernels.cu", False), ("device/kernels_f32.cu", True), ("device/noalloc.cu", False)]
 FAST_F32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
-CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/engine.cpp", "host/fluid_table.cpp", "host/solver.cpp", "host/batch.cpp", "host/server.cpp", "capi.cpp"]
+CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/engine.cpp", "host/fluid_table.cpp", "host/restart.cpp",
+               "host/output.cpp", "host/solver.cpp", "host/batch.cpp", "host/server.cpp", "capi.cpp"]
 
 
 def _run(cmd: List[str]) -> None:

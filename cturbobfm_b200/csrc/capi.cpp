@@ -199,6 +199,14 @@ int ctbfm_set_state(ctbfm_solver* s, const double* rho, const double* rhou, cons
     });
 }
 
+int ctbfm_write_solution(ctbfm_solver* s, const char* path) {
+    if (!s || !path) return setError(CTBFM_E_ARGUMENT, "null argument");
+    return guarded([&] {
+        s->solver->writeSolution(path);
+        return CTBFM_OK;
+    });
+}
+
 int ctbfm_get_lognorm(ctbfm_solver* s, double out[5]) {
     if (!s || !out) return setError(CTBFM_E_ARGUMENT, "null argument");
     return guarded([&] {

@@ -1,6 +1,7 @@
 // FluidTable: see fluid_table.hpp.
 #include "fluid_table.hpp"
 
+#include <cmath>
 #include <cstdlib>
 #include <fstream>
 #include <sstream>
@@ -122,6 +123,50 @@ FluidTable::FluidTable(const std::string& path) {
     }
     for (const auto* tabs : {&re_[0], &pt_[0], &ps_[0]})
         if (tabs->nx < 2 || tabs->ny < 2) throw ConfigError("FluidReal: table " + path + " lacks a section");
+}
+
+double FluidTable::staticEnergy_p_rho(double p, double rho) const {
+    const HostTable& tp = re_[kReP];
+    double eLo = tp.ymin, eHi = tp.ymax;
+    const double pLo = tp.interpolate(rho, eLo);
+    const double pHi = tp.interpolate(rho, eHi);
+    if (p <= pLo) return eLo;
+    if (p >= pHi) return eHi;
+    for (int it = 0; it < 30; ++it) {
+        const double eMid = 0.5 * (eLo + eHi);
+        const double pMid = tp.interpolate(rho, eMid);
+        if (std::abs(pMid - p) <= 1e-4 * p) return eMid;
+        if (pMid < p) eLo = eMid;
+        else eHi = eMid;
+    }
+    return 0.5 * (eLo + eHi);
+}
+
+double FluidTable::pressure_rho_T(double rho, double T) const {
+    const HostTable& tT = re_[kReT];
+    double eLo = tT.ymin, eHi = tT.ymax;
+    for (int it = 0; it < 25; ++it) {
+        const double eMid = 0.5 * (eLo + eHi);
+        if (tT.interpolate(rho, eMid) < T) eLo = eMid;
+        else eHi = eMid;
+    }
+    return pressure_rho_e(rho, 0.5 * (eLo + eHi));
+}
+
+double FluidTable::totalPressure_rho_e_et(double rho, double e, double et) const {
+    const double p = pressure_rho_e(rho, e);
+    const double s = entropy_rho_e(rho, e);
+    const double ht = et + p / rho;
+    double pLo = p, pHi = ps_[kPsRho].xmax;
+    for (int it = 0; it < 25; ++it) {
+        const double pMid = 0.5 * (pLo + pHi);
+        const double rhoMid = ps_[kPsRho].interpolate(pMid, s);
+        const double eMid = ps_[kPsE].interpolate(pMid, s);
+        const double hMid = eMid + pMid / rhoMid;
+        if (hMid < ht) pLo = pMid;
+        else pHi = pMid;
+    }
+    return 0.5 * (pLo + pHi);
 }
 
 std::string fluidTablePath(const Config& config) {

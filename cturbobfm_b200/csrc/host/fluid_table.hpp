@@ -42,6 +42,15 @@ public:
     double soundSpeed_rho_e(double rho, double e) const { return re_[kReA].interpolate(rho, e); }
     double density_p_T(double p, double T) const { return pt_[kPtRho].interpolate(p, T); }
     double energy_p_T(double p, double T) const { return pt_[kPtE].interpolate(p, T); }
+    double entropy_rho_e(double rho, double e) const { return re_[kReS].interpolate(rho, e); }
+    double temperature_p_s(double p, double s) const { return ps_[kPsT].interpolate(p, s); }
+    // FluidReal::computeStaticEnergy_p_rho (src/fluid_real.cpp:227-250)
+    double staticEnergy_p_rho(double p, double rho) const;
+    // FluidReal::computePressure_rho_T (src/fluid_real.cpp:262-277)
+    double pressure_rho_T(double rho, double T) const;
+    // FluidReal::computeTotalPressure_rho_u_et (src/fluid_real.cpp:299-321)
+    // with e = e(u, et) already formed
+    double totalPressure_rho_e_et(double rho, double e, double et) const;
 
 private:
     std::array<HostTable, 8> re_;

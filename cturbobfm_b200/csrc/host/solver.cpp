@@ -1,6 +1,10 @@
 // Solver: see solver.hpp.
 #include "solver.hpp"
 
+#include "host_fluid.hpp"
+#include "output.hpp"
+#include "restart.hpp"
+
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -48,7 +52,6 @@ struct HostGas {
 Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_(config.getTopology()) {
     if (config.isViscosityActive()) throw ConfigError("Viscous fluxes are outside this library's Euler path");
     if (config.parseBool("TURBULENCE_ACTIVE", false)) throw ConfigError("Turbulence models are outside this library's Euler path");
-    if (config.parseBool("RESTART_SOLUTION", false)) throw ConfigError("Restart files are outside this library's scope");
     // Config::getFluidModel (src/config.cpp:468-481)
     const std::string fluid = config.has("FLUID_MODEL") ? config.get("FLUID_MODEL") : "None";
     if (fluid == "real" || fluid == "Real" || fluid == "REAL") {
@@ -606,7 +609,10 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
     std::array<std::vector<double>, 5> U;
     for (auto& a : U) a.resize(N);
     const auto& V = mesh_.vertices();
-    for (long i = 0; i < NI; i++)
+    // Solver::initializeSolutionArrays (src/solver.cpp:783-789)
+    const bool restart = config_.parseBool("RESTART_SOLUTION", false);
+    if (restart) restartState(config_, mesh_, topo_, proto_.periodic != 0, *hostFluid(), U);
+    for (long i = 0; i < NI && !restart; i++)
         for (long j = 0; j < NJ; j++)
             for (long k = 0; k < NK; k++) {
                 Vec3 dir = d0;
@@ -825,6 +831,24 @@ void Solver::getState(double* const out[5]) {
             }
         }
     });
+}
+
+std::unique_ptr<HostFluid> Solver::hostFluid() const {
+    if (table_) return std::make_unique<RealFluid>(*table_);
+    return std::make_unique<IdealFluid>(proto_.gamma, proto_.rgas);
+}
+
+void Solver::writeSolution(const std::string& path) {
+    const long N = mesh_.nodes();
+    std::array<std::vector<double>, 5> U;
+    double* out[5];
+    for (int v = 0; v < 5; v++) {
+        U[v].resize(N);
+        out[v] = U[v].data();
+    }
+    getState(out);
+    const double* in[5] = {out[0], out[1], out[2], out[3], out[4]};
+    writeSolutionCsv(path, config_, mesh_, *hostFluid(), in);
 }
 
 void Solver::setState(const double* const in[5]) {

@@ -25,6 +25,8 @@
 
 namespace ctbfm {
 
+class HostFluid;
+
 struct BoundaryPatch {
     std::string name;
     int type = kBcEmpty;
@@ -62,6 +64,9 @@ public:
 
     void getState(double* const out[5]);
     void setState(const double* const in[5]);
+    // The current state as a volume CSV in the reference's format
+    // (Output::writeSolution, src/output.cpp:384-398), at `path`.
+    void writeSolution(const std::string& path);
     void getTurbo(double massflow[6], double turbo[4]);
     Control control();  // synchronous copy of the control block
     void profileKernels(int reps, double* outMs);
@@ -96,6 +101,7 @@ private:
     void initializeState(InstanceT<R>& inst, GroupT<R>& grp);
     template <typename R>
     const DevLut* uploadLut(InstanceT<R>& inst);
+    std::unique_ptr<HostFluid> hostFluid() const;
     template <typename F>
     auto visit(F&& f) {
         if (prec_ == kFP32Kahan) return f(*i32_, *g32_);

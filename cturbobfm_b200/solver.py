@@ -91,6 +91,7 @@ SIGNATURES = {
     "ctbfm_get_state": ([_VP] + [_DP] * 5, ctypes.c_int),
     "ctbfm_set_state": ([_VP] + [_DP] * 5, ctypes.c_int),
     "ctbfm_get_lognorm": ([_VP, _DP], ctypes.c_int),
+    "ctbfm_write_solution": ([_VP, ctypes.c_char_p], ctypes.c_int),
     "ctbfm_get_history": ([_VP, _I64, _DP, _DP, _DP, _DP, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_get_turbo": ([_VP, _DP, _DP], ctypes.c_int),
     "ctbfm_profile_kernels": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
@@ -217,6 +218,13 @@ class Solver:
     def set_state(self, u: np.ndarray):
         u = np.ascontiguousarray(u, dtype=np.float64)
         _check(load_library().ctbfm_set_state(self._h, *[_ptr(u[v]) for v in range(5)]))
+
+    def write_solution(self, path: str) -> str:
+        """ctbfm_write_solution: the current state as a volume CSV in the
+        reference's format (Output::writeSolution, src/output.cpp:384-447),
+        readable back as a restart file. Returns the path."""
+        _check(load_library().ctbfm_write_solution(self._h, os.fspath(path).encode()))
+        return os.fspath(path)
 
     def lognorm(self) -> np.ndarray:
         out = np.zeros(5)

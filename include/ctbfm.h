@@ -20,6 +20,10 @@
  *   ctbfm_get_lognorm       Solver::computeLogResidualNorm (src/solver.cpp:1488-1508)
  *   ctbfm_get_turbo         Solver::updateMassFlows / updateTurboPerformance
  *                           (src/solver.cpp:1633-1781)
+ *   ctbfm_write_solution    Output::writeSolution (src/output.cpp:384-447): the
+ *                           volume CSV that RESTART_SOLUTION reads back
+ *                           (Solver::initializeSolutionFromRestart,
+ *                           src/solver.cpp:890-1295, done at create time)
  *   ctbfm_last_error        the std::runtime_error text the reference would throw
  *
  * Conventions
@@ -126,6 +130,14 @@ int ctbfm_get_state(ctbfm_solver* s, double* rho, double* rhou, double* rhov, do
                     double* rhoe);
 int ctbfm_set_state(ctbfm_solver* s, const double* rho, const double* rhou, const double* rhov,
                     const double* rhow, const double* rhoe);
+
+/* Writes the current state as a volume CSV in the reference's format
+ * (NI/NJ/NK lines, "x,y,z,<fields sorted by name>", 16 significant digits;
+ * OUTPUT_FIELDS_TYPE primary or secondary, the default). The file is a valid
+ * restart file (RESTART_SOLUTION = yes, RESTART_SOLUTION_FILEPATH, RESTART_TYPE
+ * standard / axisymmetric / nearest_neighbor / nearest_neighbor_axisymmetric).
+ * CTBFM_E_CONFIG for OUTPUT_FIELDS_TYPE = turbo_bfm on a body-force case. */
+int ctbfm_write_solution(ctbfm_solver* s, const char* path);
 
 /* log10 residual norms of the last iteration (5 doubles). */
 int ctbfm_get_lognorm(ctbfm_solver* s, double out[5]);

@@ -11,7 +11,8 @@
  * throttle / radial-equilibrium / inviscid-wall / periodic / wedge boundaries,
  * axisymmetric, blade-row geometric, Gong and BFM (Hall, Hall-Thollet,
  * Lift-Drag, blockage) sources, local / global / fixed time steps, residual
- * norms, convergence test, turbo performance and the Greitzer plenum.
+ * norms, convergence test, turbo performance and the Greitzer plenum, and
+ * the restart initialisations (standard, axisymmetric, nearest neighbour).
  */
 #define _GNU_SOURCE
 #include "ctbfm_oracle.h"
@@ -2171,16 +2172,205 @@ static void resolve_turbo_dir(oracle_solver* s) {
     else s->turbo_dir = 0;
 }
 
+/* ------------------------------------------------------------------ restart */
+/* Solver::initializeSolutionFromRestart (src/solver.cpp:890-966) with
+ * readRestartFile (:1155-1295), standardRestart (:968-1000),
+ * axisymmetricRestart (:1002-1035) and nearestNeighborRestart (:1037-1153).
+ * The nearest node is found by exhaustive search, the first of equal
+ * distances in file order; the reference's k-d tree may pick another of
+ * several exactly equidistant nodes, so the oracle meets the reference on
+ * inputs without such ties (tie resolution is pinned by the golden fixtures
+ * made with the reference build). */
+typedef struct {
+    long ni, nj, nk;
+    vec3* xyz;
+    double *rho, *vx, *vy, *vz, *T;
+} restart_data;
+
+static void restart_free(restart_data* r) {
+    free(r->xyz); free(r->rho); free(r->vx); free(r->vy); free(r->vz); free(r->T);
+    memset(r, 0, sizeof *r);
+}
+
+static char* trim_ws(char* t) {
+    while (*t == ' ' || *t == '\t' || *t == '\r' || *t == '\n') t++;
+    size_t n = strlen(t);
+    while (n && (t[n - 1] == ' ' || t[n - 1] == '\t' || t[n - 1] == '\r' || t[n - 1] == '\n')) t[--n] = 0;
+    return t;
+}
+
+/* FluidIdeal::computePressure_rho_T (src/fluid_ideal.cpp:66-68),
+ * FluidReal::computePressure_rho_T (src/fluid_real.cpp:262-277) */
+static double f_pressure_rho_T(const oracle_solver* s, double rho, double T) {
+    if (s->real) {
+        const table2d* tT = &s->lut->T;
+        double eLo = tT->ymin, eHi = tT->ymax;
+        for (int it = 0; it < 25; ++it) {
+            double eMid = 0.5 * (eLo + eHi);
+            if (table_interp(tT, rho, eMid) < T) eLo = eMid; else eHi = eMid;
+        }
+        return table_interp(&s->lut->p, rho, 0.5 * (eLo + eHi));
+    }
+    return rho * s->rgas * T;
+}
+
+static int restart_read(const oracle_solver* s, const char* path, restart_data* r) {
+    memset(r, 0, sizeof *r);
+    FILE* f = fopen(path, "r");
+    if (!f) return fail("Failed to open restart file: %s", path);
+    char* line = NULL;
+    size_t cap = 0;
+    long* dims[3] = {&r->ni, &r->nj, &r->nk};
+    for (int d = 0; d < 3; d++) {
+        char* eq;
+        if (getline(&line, &cap, f) < 0 || !(eq = strchr(line, '='))) {
+            free(line); fclose(f);
+            return fail("Restart file %s lacks its NI/NJ/NK lines", path);
+        }
+        *dims[d] = strtol(eq + 1, NULL, 10);
+    }
+    if (getline(&line, &cap, f) < 0) { free(line); fclose(f); return fail("Restart file %s lacks its header", path); }
+    long ix = -1, iy = -1, iz = -1, need[5] = {-1, -1, -1, -1, -1};
+    const char* names[5] = {"Density", "Velocity X", "Velocity Y", "Velocity Z", "Total Energy"};
+    {
+        long c = 0;
+        char* save = NULL;
+        for (char* tok = strtok_r(line, ",", &save); tok; tok = strtok_r(NULL, ",", &save), c++) {
+            char* t = trim_ws(tok);
+            if (!strcmp(t, "x") || (!strcmp(t, "X") && ix < 0)) ix = c;
+            if (!strcmp(t, "y") || (!strcmp(t, "Y") && iy < 0)) iy = c;
+            if (!strcmp(t, "z") || (!strcmp(t, "Z") && iz < 0)) iz = c;
+            for (int v = 0; v < 5; v++) if (!strcmp(t, names[v])) need[v] = c;
+        }
+    }
+    for (int v = 0; v < 5; v++)
+        if (need[v] < 0) { free(line); fclose(f); return fail("Restart file %s has no \"%s\" column", path, names[v]); }
+    long n = r->ni * r->nj * r->nk;
+    r->xyz = (vec3*)calloc(n > 0 ? n : 1, sizeof(vec3));
+    double** arr[5] = {&r->rho, &r->vx, &r->vy, &r->vz, &r->T};
+    for (int v = 0; v < 5; v++) *arr[v] = (double*)calloc(n > 0 ? n : 1, sizeof(double));
+    long row = 0, i = 0, j = 0, k = 0;
+    double vals[256];
+    while (getline(&line, &cap, f) >= 0) {
+        if (!*trim_ws(line)) continue;
+        if (row >= n) { free(line); fclose(f); return fail("Restart file %s has more rows than NI*NJ*NK", path); }
+        long nv = 0;
+        char* save = NULL;
+        for (char* tok = strtok_r(line, ",", &save); tok && nv < 256; tok = strtok_r(NULL, ",", &save)) {
+            double v = strtod(tok, NULL);
+            if (isnan(v) || isinf(v)) {
+                free(line); fclose(f);
+                return fail("Corrupted restart file '%s': NaN or Inf encountered at row index (%ld,%ld,%ld).", path, i, j, k);
+            }
+            vals[nv++] = v;
+        }
+        for (int v = 0; v < 5; v++) if (need[v] >= nv) { free(line); fclose(f); return fail("short restart row"); }
+        if (ix >= 0 && iy >= 0 && iz >= 0 && ix < nv && iy < nv && iz < nv) r->xyz[row] = v3(vals[ix], vals[iy], vals[iz]);
+        double rho = vals[need[0]];
+        vec3 u = v3(vals[need[1]], vals[need[2]], vals[need[3]]);
+        r->rho[row] = rho; r->vx[row] = u.x; r->vy[row] = u.y; r->vz[row] = u.z;
+        r->T[row] = f_temperature_rho_u_et(s, rho, u, vals[need[4]]);
+        row++;
+        if (++k == r->nk) { k = 0; if (++j == r->nj) { j = 0; ++i; } }
+    }
+    free(line);
+    fclose(f);
+    if (row != n) return fail("Restart file %s has %ld rows, NI*NJ*NK = %ld", path, row, n);
+    return 0;
+}
+
+static vec3 rotate_x(vec3 v, double th) { /* rotateVectorAlongXAxis (src/math_utils.cpp:109-115) */
+    return v3(v.x, v.y * cos(th) - v.z * sin(th), v.y * sin(th) + v.z * cos(th));
+}
+
+static void restart_node(oracle_solver* s, long q, double rho, vec3 v, double T) {
+    s->U[0][q] = rho;
+    s->U[1][q] = rho * v.x;
+    s->U[2][q] = rho * v.y;
+    s->U[3][q] = rho * v.z;
+    double p = f_pressure_rho_T(s, rho, T);
+    double e = f_static_energy_p_rho(s, p, rho);
+    double et = e + 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z);
+    s->U[4][q] = rho * et;
+}
+
+static int restart_solution(oracle_solver* s, const char* base) {
+    const char* file = cfg_get(&s->cfg, "RESTART_SOLUTION_FILEPATH");
+    if (!file) return fail("Not found value for key \"RESTART_SOLUTION_FILEPATH\" in configuration.");
+    char path[4096];
+    dir_join(path, sizeof path, base, file);
+    restart_data r;
+    if (restart_read(s, path, &r)) { restart_free(&r); return 1; }
+    const char* type = cfg_get(&s->cfg, "RESTART_TYPE");
+    if (!type) type = "None";
+    int nearest = !strcmp(type, "nearest_neighbor") || !strcmp(type, "nearest_neighbor_axisymmetric");
+    if (!nearest && (r.ni != s->ni || r.nj != s->nj || r.nk != s->nk)) {
+        if (r.ni == s->ni && r.nj == s->nj && !strcmp(type, "axisymmetric")) {
+            for (long i = 0; i < s->ni; i++)
+                for (long j = 0; j < s->nj; j++)
+                    for (long k = 0; k < s->nk; k++) {
+                        vec3 a = s->vert[idx3(s, i, j, 0)], b = s->vert[idx3(s, i, j, k)];
+                        double rot = atan2_0_2pi(b.z, b.y) - atan2_0_2pi(a.z, a.y);
+                        long src = (i * r.nj + j) * r.nk;
+                        vec3 vel = rotate_x(v3(r.vx[src], r.vy[src], r.vz[src]), rot);
+                        restart_node(s, idx3(s, i, j, k), r.rho[src], vel, r.T[src]);
+                    }
+            restart_free(&r);
+            return 0;
+        }
+        if (!strcmp(type, "standard")) {
+            fail("Restart file dimensions (%ld,%ld,%ld) do not match solver dimensions (%ld,%ld,%ld) and "
+                 "RESTART_TYPE=standard was requested.", r.ni, r.nj, r.nk, s->ni, s->nj, s->nk);
+            restart_free(&r);
+            return 1;
+        }
+        nearest = 1;
+    }
+    if (!nearest) {
+        for (long q = 0; q < s->n; q++) restart_node(s, q, r.rho[q], v3(r.vx[q], r.vy[q], r.vz[q]), r.T[q]);
+        restart_free(&r);
+        return 0;
+    }
+    long n = r.ni * r.nj * r.nk;
+    if (n == 0) { restart_free(&r); return fail("Cannot perform nearest-neighbor restart: restart data is empty."); }
+    int axi = !strcmp(type, "axisymmetric") || !strcmp(type, "nearest_neighbor_axisymmetric") ||
+              s->topology == TOPO_AXI || (r.nk == 1 && s->nk > 1 && s->periodic);
+    for (long q = 0; q < s->n; q++) {
+        vec3 p = s->vert[q];
+        double x0 = p.x, x1 = axi ? sqrt(p.y * p.y + p.z * p.z) : p.y, x2 = p.z;
+        long best = 0;
+        double bd = DBL_MAX;
+        for (long m = 0; m < n; m++) {
+            vec3 c = r.xyz[m];
+            double c1 = axi ? sqrt(c.y * c.y + c.z * c.z) : c.y;
+            double d0 = x0 - c.x, d1 = x1 - c1, d2 = 0.0;
+            double dd = 0.0;
+            dd += d0 * d0;
+            dd += d1 * d1;
+            if (!axi) { d2 = x2 - c.z; dd += d2 * d2; }
+            if (dd < bd) { bd = dd; best = m; }
+        }
+        vec3 vel = v3(r.vx[best], r.vy[best], r.vz[best]);
+        if (axi) {
+            vec3 c = r.xyz[best];
+            vel = rotate_x(vel, atan2_0_2pi(p.z, p.y) - atan2_0_2pi(c.z, c.y));
+        }
+        restart_node(s, q, r.rho[best], vel, r.T[best]);
+    }
+    restart_free(&r);
+    return 0;
+}
+
 /* FluidIdeal::computeInitFields (src/fluid_ideal.cpp:155-170) and
  * Solver::initializeSolutionFromScratch (src/solver.cpp:777-836). */
-static int init_solution(oracle_solver* s) {
+static int init_solution(oracle_solver* s, const char* base) {
     double M, T, p;
     if (cfg_float(&s->cfg, "INIT_MACH_NUMBER", &M) || cfg_float(&s->cfg, "INIT_TEMPERATURE", &T) ||
         cfg_float(&s->cfg, "INIT_PRESSURE", &p))
         return 1;
     int restart = 0;
     if (cfg_bool(&s->cfg, "RESTART_SOLUTION", 0, &restart)) return 1;
-    if (restart) return fail("Restarts are outside the oracle's scope");
+    if (restart) return restart_solution(s, base); /* Solver::initializeSolutionArrays (src/solver.cpp:783-789) */
     const char* raw = cfg_get(&s->cfg, "INIT_DIRECTION");
     int adaptive = 0;
     vec3 d0 = v3(0, 0, 0);
@@ -2306,7 +2496,7 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
         s->R[c] = (double*)calloc(s->n, sizeof(double));
     }
     s->dt = (double*)calloc(s->n, sizeof(double));
-    if (init_solution(s)) { oracle_destroy(s); return 1; }
+    if (init_solution(s, base)) { oracle_destroy(s); return 1; }
     /* Greitzer initial state (src/solver.cpp:752-765) */
     if (s->greitzer) {
         update_mass_flows(s, s->U);

@@ -56,3 +56,42 @@ def primitive_fields(u, gamma, rgas):
 def l2_relative(a, b):
     """The regression tests' error measure (test/regression_tests/test_cases.py:82-88)."""
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+RESTART = os.path.join(GOLDEN, "restart")
+
+
+def restart_fixture_names(prefix=""):
+    """Fixtures of tests/golden/restart/ (made by make_restart_golden.py)."""
+    return sorted(n for n in (os.path.splitext(os.path.basename(p))[0]
+                              for p in glob.glob(os.path.join(RESTART, "*.npz"))) if n.startswith(prefix))
+
+
+def load_restart(name):
+    return dict(np.load(os.path.join(RESTART, name + ".npz"), allow_pickle=False))
+
+
+def restart_case(fx):
+    """The fixture's target case as a cases.Case."""
+    import json
+
+    from cturbobfm_b200 import cases
+
+    names = [str(n) for n in fx["field_names"] if str(n)]
+    patches = [cases.Patch(**p) for p in json.loads(str(fx["patches"]))]
+    return cases.Case(name=str(fx["name"]), x=fx["x"], y=fx["y"], z=fx["z"],
+                      fields={n: fx["field_" + n] for n in names}, patches=patches,
+                      settings=json.loads(str(fx["settings"])))
+
+
+def write_restart_case(fx, directory, **settings):
+    """Writes the fixture's case (and its restart.csv, if any); returns the
+    ini path. Extra settings override the fixture's."""
+    case = restart_case(fx)
+    if settings:
+        case = case.with_settings(**settings)
+    ini = case.write(directory)
+    if "restart_csv" in fx:
+        with open(os.path.join(directory, "restart.csv"), "w") as f:
+            f.write(str(fx["restart_csv"]))
+    return ini
