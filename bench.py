@@ -676,9 +676,10 @@ def run_realgas(args):
 # ---------------------------------------------------------------- serving
 SERVE_WORKLOAD = ("serving: Poisson arrivals, 70% axisymmetric compressor-map requests (NI x NJ ~ U{64..256} x "
                   "U{24..96}; a fifth of them throttle + Greitzer plenum requests on U{64..128} x U{24..48}, "
-                  "kt ~ U[0.8,1.0], B ~ U[0.1,0.5] mapped to GREITZER_PLENUM_VOLUME, fixed dt) and 30% 3-D annuli "
-                  "(U{96..160} x U{32..48} x U{32..64}), MAP_ROWS stage, static outlets p_out/pt_in ~ U[1.00,1.20], "
-                  "speed ~ U[0.85,1.00], JST RK4 CFL 2.2, drop 3 orders, fp32_kahan")
+                  "kt ~ U[0.8,1.0], B ~ U[0.1,0.5] mapped to GREITZER_PLENUM_VOLUME, speed ~ U[0.85,0.90], fixed dt) "
+                  "and 30% 3-D annuli (U{96..160} x U{32..48} x U{32..64}), MAP_ROWS stage, static outlets "
+                  "p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], JST RK4 CFL 2.2, drop 3 orders, fp32_kahan "
+                  "(float solves move to FP64 only with --serve-stall-window > 0)")
 
 
 def run_serve(args):
@@ -701,7 +702,7 @@ def run_serve(args):
                 kind = "3d" if c.shape[2] > 1 else ("throttle" if "ENABLE_GREITZER_MODELING" in c.settings else "axisymmetric")
                 inis.append((t, c.write(d), c.n_nodes, c.shape[2] > 1, kind))
             res = {}
-            with Server(chunk=args.serve_chunk, stall_window=0, host_threads=8,
+            with Server(chunk=args.serve_chunk, stall_window=args.serve_stall_window, host_threads=8,
                         max_active_nodes=args.serve_max_nodes) as srv:
                 t0 = time.perf_counter()
                 nxt = 0
@@ -726,6 +727,7 @@ def run_serve(args):
                 "requests": len(inis), "converged": int(conv.sum()),
                 "diverged": int(sum(res[i]["status"] == 2 for i in range(len(inis)))),
                 "errors": int(sum(res[i]["error"] != 0 for i in range(len(inis)))),
+                "rerun_fp64": int(sum(res[i]["precision"] == 0 for i in range(len(inis)))),
                 "p50_s": float(np.percentile(lat[conv], 50)) if conv.any() else None,
                 "p99_s": float(np.percentile(lat[conv], 99)) if conv.any() else None,
                 "p50_s_axisymmetric": float(np.percentile(lat[conv & ~is3d], 50)) if (conv & ~is3d).any() else None,
@@ -735,7 +737,9 @@ def run_serve(args):
                 "node_stage_per_s": float((nodes * its).sum() * 4 / wall),
                 "by_kind": {k: {"requests": int(sum(x[4] == k for x in inis)),
                                 "converged": int(sum(conv[i] for i in range(len(inis)) if inis[i][4] == k)),
-                                "diverged": int(sum(res[i]["status"] == 2 for i in range(len(inis)) if inis[i][4] == k))}
+                                "diverged": int(sum(res[i]["status"] == 2 for i in range(len(inis)) if inis[i][4] == k)),
+                                "rerun_fp64": int(sum(res[i]["precision"] == 0 for i in range(len(inis))
+                                                      if inis[i][4] == k))}
                             for k in ("axisymmetric", "throttle", "3d")},
             }
     clk = clocks.summary()
@@ -747,6 +751,7 @@ def run_serve(args):
         "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "rates_per_s": args.serve_rates, "requests_per_rate": args.serve_n,
                    "chunk_iterations": args.serve_chunk, "max_active_nodes": args.serve_max_nodes,
+                   "stall_window": args.serve_stall_window,
                    "clock": "host wall clock from submit to retirement"},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "per_rate": per_rate,
@@ -780,6 +785,8 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[5.0, 20.0, 80.0])
     ap.add_argument("--serve-n", type=int, default=48)
     ap.add_argument("--serve-chunk", type=int, default=100)
+    ap.add_argument("--serve-stall-window", type=int, default=0,
+                    help="serve: > 0 lets the server move stalled float solves to FP64 and re-run diverged ones in FP64")
     ap.add_argument("--serve-max-nodes", type=int, default=1500000,
                     help="grid nodes admitted at once (about what fills the GPU; 0: no limit, every arrival "
                          "shares the device at once)")

@@ -49,9 +49,20 @@ constexpr int nodesMinBlocks() {
 // the kernel was compiled for, and otherwise copies the
 // instance description into shared memory. Every thread reads the same
 // control words, which no kernel writes while others read them.
+// Programmatic dependent launch: kernels are launched with programmatic
+// stream serialization, so a grid's launch is processed while its
+// predecessor's blocks drain, and each kernel waits here, before touching any
+// memory, until the previous grid on its stream has completed and its writes
+// are visible. The predecessor signals only by exiting (an explicit early
+// launch_dependents measured 1.5-4 % slower per iteration on the
+// 160 x 48 x 64 annulus). Without the launch attribute the wait does
+// nothing.
+__device__ __forceinline__ void gridDependency() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename R>
 __device__ __forceinline__ bool enter(const DevCaseT<R>* cases, const Tile* tiles, DevCaseT<R>& sc, int stage,
                                       int force, Tile& t, int fluid = -1) {
+    gridDependency();
     t = tiles[blockIdx.x];
     const DevCaseT<R>* g = cases + t.inst;
     // kernels compiled for one fluid model (0 ideal, 1 look-up table) take
@@ -759,6 +770,7 @@ __global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, cons
 // whole batch).
 template <typename R>
 __global__ void k_gather_control(const DevCaseT<R>* cases, int m, Control* out) {
+    gridDependency();
     const int i = blockIdx.x;
     if (i >= m) return;
     const int* src = reinterpret_cast<const int*>(cases[i].ctl);
@@ -769,6 +781,7 @@ __global__ void k_gather_control(const DevCaseT<R>* cases, int m, Control* out) 
 // Sets each instance's iteration limit (n more iterations) and history origin.
 template <typename R>
 __global__ void k_set_limits(const DevCaseT<R>* cases, int m, long long n) {
+    gridDependency();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     Control* ctl = cases[i].ctl;
@@ -780,30 +793,51 @@ __global__ void k_set_limits(const DevCaseT<R>* cases, int m, long long n) {
 
 // ------------------------------------------------------------- launchers
 
+#ifndef CTBFM_PDL
+#define CTBFM_PDL 1
+#endif
+
+// Every kernel is launched with programmatic stream serialization (see
+// gridDependency); launch errors surface through cudaGetLastError.
+template <typename... P, typename... A>
+void launchK(void (*k)(P...), unsigned grid, unsigned block, cudaStream_t s, A... a) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = CTBFM_PDL;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, k, static_cast<P>(a)...);
+}
+
 template <typename R>
 cudaError_t Launcher<R>::setLimits(const BatchView<R>& b, long long n, cudaStream_t s) {
-    k_set_limits<R><<<(b.m + 127) / 128, 128, 0, s>>>(b.cases, b.m, n);
+    launchK(k_set_limits<R>, (b.m + 127) / 128, 128, s, b.cases, b.m, n);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::gatherControl(const BatchView<R>& b, Control* out, cudaStream_t s) {
-    if (b.m) k_gather_control<R><<<b.m, 64, 0, s>>>(b.cases, b.m, out);
+    if (b.m) launchK(k_gather_control<R>, b.m, 64, s, b.cases, b.m, out);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::boundaryIntegrals(const BatchView<R>& b, bool all, int force, cudaStream_t s) {
     const TileList& t = all ? b.bintAll : b.bint;
-    if (t.n && b.ideal) k_bint<R, 0><<<t.n, 256, 0, s>>>(b.cases, t.tiles, force);
-    if (t.n && b.real) k_bint<R, 1><<<t.n, 256, 0, s>>>(b.cases, t.tiles, force);
+    if (t.n && b.ideal) launchK(k_bint<R, 0>, t.n, 256, s, b.cases, t.tiles, force);
+    if (t.n && b.real) launchK(k_bint<R, 1>, t.n, 256, s, b.cases, t.tiles, force);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::timeStep(const BatchView<R>& b, int force, cudaStream_t s) {
-    if (b.node.n && b.ideal) k_dt<R, 0><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, force);
-    if (b.node.n && b.real) k_dt<R, 1><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, force);
+    if (b.node.n && b.ideal) launchK(k_dt<R, 0>, b.node.n, 256, s, b.cases, b.node.tiles, force);
+    if (b.node.n && b.real) launchK(k_dt<R, 1>, b.node.n, 256, s, b.cases, b.node.tiles, force);
     return cudaGetLastError();
 }
 
@@ -811,14 +845,14 @@ template <typename R>
 cudaError_t Launcher<R>::pre(const BatchView<R>& b, bool forceTurbo, bool dtpart, bool profiles, int force,
                              cudaStream_t s) {
     if (b.inst.n)
-        k_pre<R><<<b.inst.n, 256, 0, s>>>(b.cases, b.inst.tiles, forceTurbo ? 1 : 0, dtpart ? 1 : 0, profiles ? 1 : 0,
+        launchK(k_pre<R>, b.inst.n, 256, s, b.cases, b.inst.tiles, forceTurbo ? 1 : 0, dtpart ? 1 : 0, profiles ? 1 : 0,
                                           force);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::prim(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.node.n) k_prim<R><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
+    if (b.node.n) launchK(k_prim<R>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
     return cudaGetLastError();
 }
 
@@ -826,9 +860,9 @@ namespace {
 template <int DIR, int SCHEME, int FL, typename R>
 void launchFaceSets(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
     const TileList* t = b.face[DIR][SCHEME];
-    if (t[0].n) k_faces<DIR, SCHEME, R, FL, 0><<<t[0].n, 256, 0, s>>>(b.cases, t[0].tiles, stage, force);
-    if (t[1].n) k_faces<DIR, SCHEME, R, FL, 1><<<t[1].n, 256, 0, s>>>(b.cases, t[1].tiles, stage, force);
-    if (t[2].n) k_faces<DIR, SCHEME, R, FL, 2><<<t[2].n, 256, 0, s>>>(b.cases, t[2].tiles, stage, force);
+    if (t[0].n) launchK(k_faces<DIR, SCHEME, R, FL, 0>, t[0].n, 256, s, b.cases, t[0].tiles, stage, force);
+    if (t[1].n) launchK(k_faces<DIR, SCHEME, R, FL, 1>, t[1].n, 256, s, b.cases, t[1].tiles, stage, force);
+    if (t[2].n) launchK(k_faces<DIR, SCHEME, R, FL, 2>, t[2].n, 256, s, b.cases, t[2].tiles, stage, force);
 }
 template <int FL, typename R>
 void launchFaces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s) {
@@ -854,20 +888,20 @@ cudaError_t Launcher<R>::faces(const BatchView<R>& b, int dir, int stage, int fo
 
 template <typename R>
 cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.node.n && b.ideal) k_nodes<R, 0><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
-    if (b.node.n && b.real) k_nodes<R, 1><<<b.node.n, 256, 0, s>>>(b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.ideal) launchK(k_nodes<R, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.real) launchK(k_nodes<R, 1>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.per.n) k_periodic<R><<<b.per.n, kPeriodicTile, 0, s>>>(b.cases, b.per.tiles, stage, force);
+    if (b.per.n) launchK(k_periodic<R>, b.per.n, kPeriodicTile, s, b.cases, b.per.tiles, stage, force);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t Launcher<R>::finalize(const BatchView<R>& b, int force, cudaStream_t s) {
-    if (b.inst.n) k_finalize<R><<<b.inst.n, 256, 0, s>>>(b.cases, b.inst.tiles, force);
+    if (b.inst.n) launchK(k_finalize<R>, b.inst.n, 256, s, b.cases, b.inst.tiles, force);
     return cudaGetLastError();
 }
 

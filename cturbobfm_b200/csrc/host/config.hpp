@@ -27,6 +27,8 @@ public:
 
     bool has(const std::string& key) const { return data_.count(key) > 0; }
     std::string get(const std::string& key) const;
+    // Overrides one key (the server's FP64 re-run of a diverged float solve).
+    void set(const std::string& key, const std::string& value) { data_[key] = value; }
     const std::string& directory() const { return dir_; }
 
     // typed getters, same names and defaults as the reference's Config

@@ -202,12 +202,18 @@ void Server::pump(int* nActive, int* nWaiting) {
             b64_->controls(tmp.data());
             for (size_t m = 0; m < idx64_.size(); m++) ctl[idx64_[m]] = tmp[m];
         }
-        // 3. retire finished solves, promote stalled float solves
+        // 3. retire finished solves, re-run diverged float solves in FP64,
+        //    promote stalled float solves
         std::vector<std::unique_ptr<Job>> keep;
-        std::vector<size_t> promote;
+        std::vector<size_t> promote, rerun;
         for (size_t i = 0; i < active_.size(); i++) {
             const Control& c = ctl[i];
             auto& j = active_[i];
+            if (opt_.stall_window > 0 && c.status == 2 && j->solver->precision() == kFP32Kahan && !j->rerun) {
+                rerun.push_back(keep.size());
+                keep.push_back(std::move(j));
+                continue;
+            }
             if (c.status != 0 || c.it >= j->solver->maxIterations()) {
                 if (!dirty_) {
                     b32_.reset();
@@ -224,6 +230,38 @@ void Server::pump(int* nActive, int* nWaiting) {
             keep.push_back(std::move(j));
         }
         active_ = std::move(keep);
+        if (!rerun.empty()) {
+            // A float solve whose residual became NaN/Inf starts again from its
+            // initial state in FP64; the outcome depends on the request alone.
+            b32_.reset();
+            b64_.reset();
+            dirty_ = true;
+            std::vector<size_t> failed;
+            for (size_t k : rerun) {
+                auto& j = active_[k];
+                used_ -= std::min(used_, j->bytes);
+                j->solver.reset();
+                j->rerun = true;
+                j->config->set("GPU_PRECISION", "fp64");
+                try {
+                    j->solver = std::make_unique<Solver>(*j->config, *j->mesh);
+                    j->bytes = j->solver->deviceBytes();
+                    used_ += j->bytes;
+                } catch (const std::exception& e) {
+                    j->message = e.what();
+                    failed.push_back(k);
+                }
+            }
+            for (auto it = failed.rbegin(); it != failed.rend(); ++it) {
+                auto j = std::move(active_[*it]);
+                active_.erase(active_.begin() + static_cast<long>(*it));
+                usedNodes_ -= std::min(usedNodes_, j->nodes);
+                const std::string msg = j->message;
+                retire(std::move(j), nullptr, 2, msg);
+            }
+            for (size_t& k : promote)  // indices after the erased entries shift down
+                k -= static_cast<size_t>(std::count_if(failed.begin(), failed.end(), [k](size_t f) { return f < k; }));
+        }
         if (!promote.empty()) {
             b32_.reset();
             b64_.reset();

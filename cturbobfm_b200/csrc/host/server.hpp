@@ -41,7 +41,8 @@ struct ServerOptions {
     int max_active = 1024;        // admitted solves at most
     long long max_active_nodes = 0;  // grid nodes of the admitted solves together at most (0: no limit)
     long long chunk = 200;        // iterations between scheduling rounds
-    long long stall_window = 0;   // fp32_kahan -> FP64 after this many iterations without progress (0: never)
+    long long stall_window = 0;   // fp32_kahan -> FP64 after this many iterations without progress, and
+                                  // diverged fp32_kahan solves re-run in FP64 (0: neither)
     int host_threads = 4;         // workers preparing requests
 };
 
@@ -74,6 +75,7 @@ private:
         std::unique_ptr<Mesh> mesh;
         std::unique_ptr<Solver> solver;  // declared last: released before the mesh and config it refers to
         size_t bytes = 0;
+        bool rerun = false;  // a diverged float solve restarted in FP64
     };
     void worker();
     void rebuild();

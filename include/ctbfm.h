@@ -250,7 +250,11 @@ typedef struct {
  * per scheduling round; stall_window: a
  * fp32_kahan solve whose convergence progress (best_drop of
  * ctbfm_batch_status) has not grown by 0.05 for this many iterations
- * continues in FP64 (0: never); host_threads: request-preparation workers. */
+ * continues in FP64, and a fp32_kahan solve whose residual becomes NaN/Inf
+ * is run again once, from its initial state, in FP64 (0: neither; a moved
+ * solve's result reports precision 0); host_threads: request-preparation
+ * workers. A result depends on its own request only, never on the rest of
+ * the mix. */
 int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_t max_active_nodes,
                         int64_t chunk_iterations, int64_t stall_window, int32_t host_threads, ctbfm_server** out);
 void ctbfm_server_destroy(ctbfm_server* s);

@@ -126,3 +126,35 @@ def test_node_limit_admits_in_arrival_order(tmp_path):
     for prev, nxt in zip(order, order[1:]):
         assert nxt["t_admit"] >= prev["t_done"]
     assert all(r["status"] == 1 for r in res.values())
+
+
+def test_diverged_fp32_solve_is_run_again_in_fp64(tmp_path):
+    """A 3-D request of the serving mix (JST, RK4, CFL 2.2) whose fp32_kahan
+    solve blows up in its start-up transient while the FP64 solve converges:
+    a server allowed to move float solves to FP64 (stall_window > 0) runs it
+    again from its initial state in FP64, and the result is that of the
+    plain FP64 solve."""
+    from cturbobfm_b200 import Server, SolverDiverged, Solver
+
+    c = [c for _, c in cases.serving_requests(48, 5.0) if c.shape[2] > 1][1]
+    ini32 = _write(c, str(tmp_path / "f32"))
+    with Solver(ini32) as s:
+        with pytest.raises(SolverDiverged):
+            s.solve()
+    ini64 = _write(c.with_settings(GPU_PRECISION="fp64"), str(tmp_path / "f64"))
+    with Solver(ini64) as s:
+        s.solve()
+        assert s.status == 1
+        it64 = s.iteration
+        mf64, tp64 = s.turbo()
+    with Server(chunk=200) as srv:  # stall_window 0: the divergence is the result
+        rid = srv.submit(ini32)
+        r = _drain(srv, 1)[rid]
+    assert r["status"] == 2 and r["precision"] == 1
+    with Server(chunk=200, stall_window=100000) as srv:
+        rid = srv.submit(ini32)
+        r = _drain(srv, 1)[rid]
+    assert r["status"] == 1 and r["precision"] == 0
+    assert r["iterations"] == it64
+    assert np.array_equal(np.array(r["turbo"]), tp64)
+    assert np.array_equal(np.array(r["massflow"]), mf64)
