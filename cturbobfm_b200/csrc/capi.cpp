@@ -226,6 +226,15 @@ int ctbfm_get_history(ctbfm_solver* s, int64_t max_rows, double* lognorm, double
     });
 }
 
+int ctbfm_get_history_time(ctbfm_solver* s, int64_t max_rows, double* time, int64_t* n_rows) {
+    if (!s) return setError(CTBFM_E_ARGUMENT, "null solver");
+    return guarded([&] {
+        const long long r = s->solver->history(max_rows, nullptr, nullptr, nullptr, nullptr, time);
+        if (n_rows) *n_rows = r;
+        return CTBFM_OK;
+    });
+}
+
 int ctbfm_get_turbo(ctbfm_solver* s, double massflow[6], double turbo[4]) {
     if (!s || !massflow || !turbo) return setError(CTBFM_E_ARGUMENT, "null argument");
     return guarded([&] {

@@ -105,6 +105,10 @@ struct Tile {
     long long count;
 };
 
+// History row: log10 norms (5), boundary mass flows (6), turbo performance
+// (4), hub static pressure (1), physical time after the iteration (1).
+constexpr int kHistWidth = 17;
+
 template <typename R>
 struct alignas(16) DevCaseT {
     int ni, nj, nk;
@@ -186,8 +190,9 @@ struct alignas(16) DevCaseT {
     int per_tiles;    // tiles of this instance in the periodic kernel
     const DevLut* lut;  // FLUID_MODEL = real: the look-up tables; nullptr for the ideal gas
     Control* ctl;
-    double* hist;  // 16 doubles per iteration row
+    double* hist;  // kHistWidth doubles per iteration row
     long long hist_cap;
+    long long max_it;  // N_ITERATIONS: no enqueue runs an instance past it
 };
 
 using DevCase = DevCaseT<double>;

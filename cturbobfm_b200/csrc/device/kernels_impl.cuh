@@ -735,11 +735,12 @@ __global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, cons
     }
     const long long row = it - 1 - ctl->hist_base;
     if (c.hist && row >= 0 && row < c.hist_cap) {
-        double* h = c.hist + row * 16;
+        double* h = c.hist + row * kHistWidth;
         for (int v = 0; v < 5; v++) h[v] = lr[v];
         for (int b = 0; b < 6; b++) h[5 + b] = ctl->massflow[b];
         for (int b = 0; b < 4; b++) h[11 + b] = c.need_turbo ? ctl->turbo[b] : 0.0;
         h[15] = ctl->hub_p;
+        h[16] = ctl->t;
     }
     if (c.steady) {
         bool conv = true;
@@ -778,14 +779,16 @@ __global__ void k_gather_control(const DevCaseT<R>* cases, int m, Control* out) 
     for (int w = threadIdx.x; w < static_cast<int>(sizeof(Control) / 4); w += blockDim.x) dst[w] = src[w];
 }
 
-// Sets each instance's iteration limit (n more iterations) and history origin.
+// Sets each instance's iteration limit (n more iterations, at most its
+// N_ITERATIONS, like the reference's loop bound) and history origin.
 template <typename R>
 __global__ void k_set_limits(const DevCaseT<R>* cases, int m, long long n) {
     gridDependency();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     Control* ctl = cases[i].ctl;
-    ctl->it_stop = ctl->it + n;
+    const long long stop = ctl->it + n;
+    ctl->it_stop = stop < cases[i].max_it ? stop : cases[i].max_it;
     ctl->hist_base = ctl->it;
 }
 

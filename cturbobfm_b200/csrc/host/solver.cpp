@@ -16,7 +16,6 @@ namespace ctbfm {
 
 namespace {
 
-constexpr int kHistWidth = 16;
 
 int boundaryTypeFromString(std::string s) {  // include/types.hpp:202-232, path subset
     std::transform(s.begin(), s.end(), s.begin(), [](unsigned char ch) { return std::tolower(ch); });
@@ -415,6 +414,7 @@ void Solver::setupScalars() {
     c.node_tiles = static_cast<int>((N + kTileSize - 1) / kTileSize);
     c.per_tiles = c.periodic ? static_cast<int>((NI * NJ + kPeriodicTile - 1) / kPeriodicTile) : 0;
     c.hist_cap = std::min<long long>(std::max<long long>(maxIter_, 1024), 1 << 20);
+    c.max_it = maxIter_;
 }
 
 // Device arrays of the operating point in precision R.
@@ -968,12 +968,13 @@ void Solver::promoteToFP64() {
     cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
 }
 
-long long Solver::history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub) {
+long long Solver::history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub,
+                          double* time) {
     const Control c = control();
     const long long cap = proto_.hist_cap;
     long long rows = std::min<long long>(c.it - c.hist_base, cap);
     if (rows < 0) rows = 0;
-    if (!lognorm && !massflow && !turbo && !hub) return rows;
+    if (!lognorm && !massflow && !turbo && !hub && !time) return rows;
     rows = std::min(rows, maxRows);
     std::vector<double> h(static_cast<size_t>(rows) * kHistWidth);
     const double* dh = i64_ ? i64_->c.hist : i32_->c.hist;
@@ -984,6 +985,7 @@ long long Solver::history(long long maxRows, double* lognorm, double* massflow, 
         if (massflow) std::copy(row + 5, row + 11, massflow + 6 * r);
         if (turbo) std::copy(row + 11, row + 15, turbo + 4 * r);
         if (hub) hub[r] = row[15];
+        if (time) time[r] = row[16];
     }
     return rows;
 }

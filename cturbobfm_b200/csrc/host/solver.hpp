@@ -75,7 +75,8 @@ public:
     // profiles and the history move to a new FP64 instance; the float
     // instance is released. No-op on an FP64 solver.
     void promoteToFP64();
-    long long history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub);
+    long long history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub,
+                      double* time = nullptr);
     size_t deviceBytes() const;
 
     long ni() const { return mesh_.ni(); }

@@ -94,6 +94,7 @@ SIGNATURES = {
     "ctbfm_write_solution": ([_VP, ctypes.c_char_p], ctypes.c_int),
     "ctbfm_get_history": ([_VP, _I64, _DP, _DP, _DP, _DP, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_get_turbo": ([_VP, _DP, _DP], ctypes.c_int),
+    "ctbfm_get_history_time": ([_VP, _I64, _DP, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_profile_kernels": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
     "ctbfm_batch_create": ([ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(_VP)], ctypes.c_int),
     "ctbfm_batch_destroy": ([_VP], None),
@@ -237,9 +238,11 @@ class Solver:
         _check(lib.ctbfm_get_history(self._h, 0, None, None, None, None, ctypes.byref(rows)))
         n = int(rows.value)
         ln, mf, tp, hub = np.zeros((n, 5)), np.zeros((n, 6)), np.zeros((n, 4)), np.zeros(n)
+        t = np.zeros(n)
         if n:
             _check(lib.ctbfm_get_history(self._h, n, _ptr(ln), _ptr(mf), _ptr(tp), _ptr(hub), ctypes.byref(rows)))
-        return {"lognorm": ln, "massflow": mf, "turbo": tp, "hub": hub}
+            _check(lib.ctbfm_get_history_time(self._h, n, _ptr(t), ctypes.byref(rows)))
+        return {"lognorm": ln, "massflow": mf, "turbo": tp, "hub": hub, "time": t}
 
     def turbo(self):
         mf, tp = np.zeros(6), np.zeros(4)

@@ -10,7 +10,8 @@
  *                           (src/turbobfm.cpp:15-27, src/config.cpp:8-13,
  *                            src/mesh.cpp:11-40, src/solver.cpp:18-31)
  *   ctbfm_solve             Solver::solve() explicit branch (src/solver.cpp:1296-1424)
- *   ctbfm_step              n iterations of that loop (src/solver.cpp:1337-1398)
+ *   ctbfm_step              n iterations of that loop (src/solver.cpp:1337-1398),
+ *                           never past N_ITERATIONS
  *   ctbfm_compute_residual  Solver::computeTimestepArray + Solver::computeResiduals
  *                           (src/solver.cpp:1531-1630, 1783-1833) on the current state
  *   ctbfm_get_state /
@@ -90,8 +91,9 @@ int ctbfm_set_stream(ctbfm_solver* s, void* cuda_stream);
 
 int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out);
 
-/* Runs up to n_iter iterations (fewer if the convergence test fires or the
- * solution diverges). *n_done receives the iterations performed. Returns
+/* Runs up to n_iter iterations (fewer if the convergence test fires, the
+ * solution diverges or N_ITERATIONS is reached). *n_done receives the
+ * iterations performed. Returns
  * CTBFM_E_DIVERGED when a residual norm is NaN/Inf. Synchronises the stream. */
 int ctbfm_step(ctbfm_solver* s, int64_t n_iter, int64_t* n_done);
 
@@ -149,6 +151,10 @@ int ctbfm_get_lognorm(ctbfm_solver* s, double out[5]);
  * written in *n_rows; pass NULL arrays to query the count. */
 int ctbfm_get_history(ctbfm_solver* s, int64_t max_rows, double* lognorm, double* massflow,
                       double* turbo, double* hub, int64_t* n_rows);
+
+/* Physical time after each iteration of the same history (Solver::_time,
+ * src/solver.cpp:1389-1390; the time column of turbo.csv). */
+int ctbfm_get_history_time(ctbfm_solver* s, int64_t max_rows, double* time, int64_t* n_rows);
 
 /* Mass flows (6) and turbo performance (4) of the current state, computed on
  * the device in FP64. */
