@@ -14,7 +14,8 @@ namespace ctbfm {
 constexpr int kMaxPatches = 16;
 constexpr int kMaxProfiles = 4;
 
-// Boundary types on the path (include/types.hpp:178-194 restricted).
+// Boundary types (include/types.hpp:178-194; the 2-D inlet file and the
+// no-slip wall of the viscous path are not among them).
 enum DevBc : int {
     kBcInlet = 0,
     kBcOutlet = 1,
@@ -23,7 +24,12 @@ enum DevBc : int {
     kBcWedge = 4,
     kBcPeriodic = 5,
     kBcThrottle = 6,
-    kBcEmpty = 7
+    kBcEmpty = 7,
+    kBcInletSupersonic = 8,
+    kBcOutletSupersonic = 9,
+    kBcMassFlow = 10,
+    kBcTransparent = 11,
+    kBcFarfield = 12
 };
 
 struct DevPatch {
@@ -156,6 +162,14 @@ struct alignas(16) DevCaseT {
     int prof_i[kMaxProfiles];      // node i of the sampled column
     int prof_j0[kMaxProfiles];     // first j
     double prof_kt[kMaxProfiles];  // throttle coefficient of the profile's patch
+    // mass-flow outlets (src/solver.cpp:2734-2770): target mass flow, relaxation,
+    // boundary plane of the patch (0..5); a profile without radial
+    // equilibrium is filled with the hub value instead of integrated
+    double prof_mf[kMaxProfiles];
+    double prof_relax[kMaxProfiles];
+    int prof_plane[kMaxProfiles];
+    int prof_fill[kMaxProfiles];
+    double mf_max_change;  // MASS_FLOW_MAX_PRESSURE_CHANGE
     // boundary planes for the surface integrals: raw S vectors
     const double* bsx[6];
     const double* bsy[6];

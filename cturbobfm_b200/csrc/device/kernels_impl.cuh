@@ -100,13 +100,24 @@ __device__ __forceinline__ R* const* stageOut(const DevCaseT<R>& c, int s) {
     return c.S1;
 }
 
-template <typename R>
-__device__ __forceinline__ S5<R> boundaryFlux(const DevCaseT<R>& c, Gas<R> gs, int pidx, const S5<R>& Uint, V3<R> n,
+// Not inlined: the boundary faces are few, and keeping their many flux
+// variants out of the face kernels' bodies halves the kernels' spills.
+template <int SCHEME, typename R>
+__device__ __noinline__ S5<R> boundaryFlux(const DevCaseT<R>& c, Gas<R> gs, int pidx, const S5<R>& Uint, V3<R> n,
                                               long long qtheta, int fj, long long it) {
     const DevPatch& p = c.patch[pidx];
     switch (p.type) {
         case kBcInlet: return bcInlet(c, gs, p, Uint, n, c.cost[qtheta], c.sint[qtheta]);
         case kBcOutlet: return bcOutlet(c, gs, Uint, n, R(p.v[0]), it);
+        case kBcInletSupersonic: return bcInletSupersonic(gs, p, n);
+        case kBcOutletSupersonic: return bcOutletSupersonic(gs, Uint, n);
+        case kBcFarfield: return bcFarfield(gs, p, Uint, n);
+        case kBcTransparent:
+            // BoundaryTransparent (src/boundary_transparent.cpp:5-16): the
+            // scheme's own flux with the interior state on both sides
+            if (SCHEME == 0) return fluxJst(gs, Uint, Uint, Uint, Uint, n);
+            return fluxRoe(gs, c.muscl, c.limiter, Uint, Uint, Uint, Uint, n);
+        case kBcMassFlow:  // BoundaryOutletMassFlow (src/boundary_outlet_mass_flow.cpp:4-19)
         case kBcRadialEq:
         case kBcThrottle: {
             // BoundaryOutletThrottle / RadialEquilibrium index the profile by the
@@ -197,7 +208,17 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
         long long f;
         int fi, fj, fk;
         if (SET == 0 || DIR == 0) {
-            f = p;
+            if (SET == 0) {
+                f = p;
+            } else {  // I faces: the planes fi = 2 .. ni-2 are contiguous, the end planes 0, 1, ni-1, ni
+                const long long plane = static_cast<long long>(c.nj) * c.nk;
+                if (SET == 1) {
+                    f = 2 * plane + p;
+                } else {
+                    const int s4 = static_cast<int>(p / plane);
+                    f = static_cast<long long>(s4 < 2 ? s4 : c.ni - 3 + s4) * plane + p % plane;
+                }
+            }
             fk = static_cast<int>(f % nfk);
             const long long t = f / nfk;
             fj = static_cast<int>(t % nfj);
@@ -235,7 +256,9 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
         V3<R> n = v3(__ldg(F.nx + f), __ldg(F.ny + f), __ldg(F.nz + f));
         const R area = __ldg(F.area + f);
         S5<R> flux;
-        if (dface == 0 || dface == nlast) {
+        // SET 1 holds plain interior faces only, SET 2 only the four end faces
+        // of a line: each launch compiles only the paths it can take
+        if (SET != 1 && (dface == 0 || dface == nlast)) {
             const int side = dface == 0 ? 0 : 1;
             const int ni_ = DIR == 0 ? (side ? c.ni - 1 : 0) : fi;
             const int nj_ = DIR == 1 ? (side ? c.nj - 1 : 0) : fj;
@@ -249,7 +272,7 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
             // theta of the face's (i, j, k) node for the cylindrical inlet frame
             const long long qth =
                 nodeIdx(c, fi < c.ni ? fi : c.ni - 1, fj < c.nj ? fj : c.nj - 1, fk < c.nk ? fk : c.nk - 1);
-            flux = boundaryFlux(c, gs, pidx, load5(U, q), n, qth, fj, it);
+            flux = boundaryFlux<SCHEME>(c, gs, pidx, load5(U, q), n, qth, fj, it);
         } else {
             const long long qR = nodeIdx(c, fi, fj, fk);
             const long long qL = qR - st;
@@ -257,7 +280,7 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
             // primitives k_prim computed once per node (bitwise the same values
             // as converting here); faces next to a boundary or a periodic seam
             // extrapolate or rotate conservative states first
-            const bool plain = dface >= 2 && dface <= nlast - 2;
+            const bool plain = SET == 1 || (SET == 0 && dface >= 2 && dface <= nlast - 2);
             if (plain) {
                 if (SCHEME == 0) {
                     flux = fluxJstW(gs, load5(U, qL - st), load5(U, qL), load5(U, qR), load5(U, qR + st),
@@ -669,8 +692,25 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
         if (c.greitzer) {
         } else if (c.prof_type[m] == kBcThrottle) {
             ctl->hub_p = c.inlet_pt + c.prof_kt[m] * ctl->turbo[0] * ctl->turbo[0];
+        } else if (c.prof_type[m] == kBcMassFlow) {
+            // mass-flow controller (src/solver.cpp:2734-2770): relax the hub
+            // pressure by the relative mass-flow error, clamped
+            double cur = fabs(ctl->massflow[c.prof_plane[m]]);
+            if (c.topo == 2) cur *= 2.0 * M_PI / c.wedge;
+            else if (c.per_angle_deg != 0.0) cur *= 360.0 / c.per_angle_deg;
+            const double err = (cur - c.prof_mf[m]) / c.prof_mf[m];
+            double dp = c.prof_relax[m] * err;
+            dp = dp < -c.mf_max_change ? -c.mf_max_change : (c.mf_max_change < dp ? c.mf_max_change : dp);
+            double p0 = p[0];
+            if (p0 <= 0.0) p0 = c.init_p > 0.0 ? c.init_p : 101325.0;
+            const double hub = p0 * (1.0 + dp);
+            ctl->hub_p = hub < 100.0 ? 100.0 : hub;
         } else if (c.prof_type[m] == kBcRadialEq) {
             ctl->hub_p = p[0];
+        }
+        if (c.prof_fill[m]) {  // no radial equilibrium: the hub value everywhere
+            for (int jj = 0; jj < n; jj++) p[jj] = ctl->hub_p;
+            continue;
         }
         // sample density and |u_theta| at (prof_i, j, 0) and integrate dp/dr
         double rho1 = 0, ut1 = 0;

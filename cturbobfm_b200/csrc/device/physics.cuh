@@ -557,6 +557,106 @@ CTBFM_DI S5<R> bcWall(Gas<R> gs, const S5<R>& Uint, V3<R> n) {
     return s5(R(0), pw * n.x, pw * n.y, pw * n.z, R(0));
 }
 
+template <typename R>
+CTBFM_DI R density_p_T(Gas<R> gs, R p, R T) {  // :134-136; FluidReal::computeDensity_p_T (the (p, T) table)
+    if (gs.lut) return lutInterp(gs.lut->pt[kPtRho], p, T);
+    return p / (gs.R_ * T);
+}
+
+// BoundaryOutletSupersonic::computeBoundaryFlux (src/boundary_outlet_supersonic.cpp:4-14).
+template <typename R>
+CTBFM_DI S5<R> bcOutletSupersonic(Gas<R> gs, const S5<R>& Uint, V3<R> n) {
+    return advFlux(gs, primOf(Uint), n);
+}
+
+// BoundaryInletSupersonic::computeBoundaryFlux (src/boundary_inlet_supersonic.cpp:4-34):
+// the state of the patch values (p, T, u, v, w).
+template <typename R>
+CTBFM_DI S5<R> bcInletSupersonic(Gas<R> gs, const DevPatch& pt, V3<R> n) {
+    const R p = R(pt.v[0]), T = R(pt.v[1]);
+    const V3<R> u = v3(R(pt.v[2]), R(pt.v[3]), R(pt.v[4]));
+    const R rho = density_p_T(gs, p, T);
+    const R e = staticEnergy_p_rho(gs, p, rho);
+    const R et = e + R(0.5) * dot(u, u);
+    return advFlux(gs, s5(rho, u.x, u.y, u.z, et), n);
+}
+
+// BoundaryFarfield::computeBoundaryFlux (src/boundary_farfield.cpp:5-144):
+// freestream (Mach, p, T, direction) from the patch values; supersonic
+// outflow takes the interior state, supersonic inflow the freestream, and
+// subsonic faces combine the outgoing and incoming characteristics, with
+// Riemann invariants for the ideal gas and acoustic impedance plus (p, s)
+// tables for the real gas.
+template <typename R>
+CTBFM_DI S5<R> bcFarfield(Gas<R> gs, const DevPatch& pt, const S5<R>& Uint, V3<R> n) {
+    const R g = gs.g;
+    const R machInf = R(pt.v[0]), pInf = R(pt.v[1]), TInf = R(pt.v[2]);
+    V3<R> dir = v3(R(pt.v[3]), R(pt.v[4]), R(pt.v[5]));
+    dir = dir / mag(dir);
+    const R rhoInf = density_p_T(gs, pInf, TInf);
+    const R aInf = soundSpeed_p_rho(gs, pInf, rhoInf);
+    const V3<R> uInf = dir * (machInf * aInf);
+    const S5<R> W = primOf(Uint);
+    const R rhoI = W.v[0];
+    const V3<R> uI = velOf(W);
+    const R pI = pressure_rho_u_et(gs, rhoI, uI, W.v[4]);
+    const R aI = soundSpeed_p_rho(gs, pI, rhoI);
+    const R unI = dot(uI, n);
+    const R unInf = dot(uInf, n);
+    if (unI >= aI) return advFlux(gs, W, n);
+    if (unI <= -aI) {
+        const R eInf = staticEnergy_p_rho(gs, pInf, rhoInf);
+        const R etInf = eInf + R(0.5) * dot(uInf, uInf);
+        return advFlux(gs, s5(rhoInf, uInf.x, uInf.y, uInf.z, etInf), n);
+    }
+    R rhoB, eB;
+    R unB;
+    V3<R> uRef;
+    if (!gs.lut) {
+        const R Rp = unI + R(2) * aI / (g - R(1));
+        const R Rm = unInf - R(2) * aInf / (g - R(1));
+        unB = R(0.5) * (Rp + Rm);
+        const R aB = R(0.25) * (g - R(1)) * (Rp - Rm);
+        R rhoRef, pRef;
+        if (unB > R(0)) {
+            rhoRef = rhoI;
+            pRef = pI;
+            uRef = uI;
+        } else {
+            rhoRef = rhoInf;
+            pRef = pInf;
+            uRef = uInf;
+        }
+        const R ent = pRef / pow(rhoRef, g);
+        rhoB = pow(aB * aB / (g * ent), R(1) / (g - R(1)));
+        const R pB = rhoB * aB * aB / g;
+        eB = staticEnergy_p_rho(gs, pB, rhoB);
+    } else {
+        const R rhoAvg = R(0.5) * (rhoI + rhoInf);
+        const R aAvg = R(0.5) * (aI + aInf);
+        const R Z = rhoAvg * aAvg;
+        const R Rp = unI + pI / Z;
+        const R Rm = unInf - pInf / Z;
+        unB = R(0.5) * (Rp + Rm);
+        const R pB = R(0.5) * (Rp - Rm) * Z;
+        R sRef;
+        if (unB > R(0)) {
+            const R eI = W.v[4] - R(0.5) * dot(uI, uI);
+            sRef = lutInterp(gs.lut->re[kReS], rhoI, eI);
+            uRef = uI;
+        } else {
+            sRef = lutInterp(gs.lut->pt[kPtS], pInf, TInf);
+            uRef = uInf;
+        }
+        rhoB = lutInterp(gs.lut->ps[kPsRho], pB, sRef);
+        eB = lutInterp(gs.lut->ps[kPsE], pB, sRef);
+    }
+    const V3<R> ut = uRef - n * dot(uRef, n);
+    const V3<R> uB = ut + n * unB;
+    const R etB = eB + R(0.5) * dot(uB, uB);
+    return advFlux(gs, s5(rhoB, uB.x, uB.y, uB.z, etB), n);
+}
+
 // BoundaryInlet::computeBoundaryFlux (src/boundary_inlet.cpp:4-43) and
 // BoundaryBase::computeSubsonicInletFlux (src/boundary_base.cpp:7-124);
 // cth/sth are cos/sin of the node's theta for the cylindrical frame.

@@ -91,15 +91,20 @@ void GroupT<R>::buildTiles() {
         for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++) {
             const long long nf =
                 static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
-            const int nline = d == 1 ? c.nj : c.nk;  // nodes along a J or K line
-            // J rows of nk faces fall on whole warps when nk is a multiple of
-            // 32: no warp mixes end and plain faces, one launch is cheaper
-            const bool aligned = d == 1 && c.nk % 32 == 0;
-            if (d == 0 || nline < 3 || aligned) {
+            const int nline = d == 0 ? c.ni : (d == 1 ? c.nj : c.nk);  // nodes along a line of direction d
+            // K lines (and J lines whose rows of nk faces do not fill whole
+            // warps) run as two launches, plain faces 2 .. n-2 and the four
+            // end faces of every line, so the plain launch carries no boundary
+            // or extrapolation code; I faces and warp-aligned J rows run as one
+            // launch (splitting them measured slower: the four end planes of I
+            // make a large launch of boundary code)
+            const bool split = nline >= 3 && (d == 2 || (d == 1 && c.nk % 32 != 0));
+            if (!split) {
                 cover(face[d][c.scheme][0], m, nf, faceTile_[d]);
             } else {
-                // plain faces 2 .. n-2 and the four end faces of every line
-                const long long lines = d == 1 ? static_cast<long long>(c.ni) * c.nk : static_cast<long long>(c.ni) * c.nj;
+                const long long lines = d == 0 ? static_cast<long long>(c.nj) * c.nk
+                                               : (d == 1 ? static_cast<long long>(c.ni) * c.nk
+                                                         : static_cast<long long>(c.ni) * c.nj);
                 cover(face[d][c.scheme][1], m, lines * (nline - 3), faceTile_[d]);
                 cover(face[d][c.scheme][2], m, lines * 4, faceTile_[d]);
             }

@@ -92,6 +92,25 @@ private:
     int type_, profile_;
 };
 
+// BoundaryInletSupersonic (fixed p, T, velocity) and BoundaryFarfield
+// (Mach, p, T, direction): the patch values, at least `need` of them.
+class BoundaryWithValues : public BoundaryBase {
+public:
+    BoundaryWithValues(int type, const std::vector<double>& values, size_t need, const char* what)
+        : type_(type), values_(values) {
+        if (values_.size() < need) throw ConfigError(what);
+    }
+    DevPatch toDevice() const override {
+        DevPatch p{type_, -1, {}};
+        for (size_t i = 0; i < values_.size() && i < 8; i++) p.v[i] = values_[i];
+        return p;
+    }
+
+private:
+    int type_;
+    std::vector<double> values_;
+};
+
 class BoundaryInviscidWall : public BoundaryBase {
 public:
     DevPatch toDevice() const override { return DevPatch{kBcInviscidWall, -1, {}}; }

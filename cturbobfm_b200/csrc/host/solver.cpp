@@ -27,9 +27,12 @@ int boundaryTypeFromString(std::string s) {  // include/types.hpp:202-232, path 
     if (s == "periodic") return kBcPeriodic;
     if (s == "throttle") return kBcThrottle;
     if (s == "empty") return kBcEmpty;
-    if (s == "inlet_supersonic" || s == "outlet_supersonic" || s == "mass_flow" || s == "outlet_mass_flow" ||
-        s == "massflow" || s == "mass_flow_rate" || s == "inlet_2d" || s == "no_slip_wall" || s == "transparent" ||
-        s == "farfield")
+    if (s == "inlet_supersonic") return kBcInletSupersonic;
+    if (s == "outlet_supersonic") return kBcOutletSupersonic;
+    if (s == "mass_flow" || s == "outlet_mass_flow" || s == "massflow" || s == "mass_flow_rate") return kBcMassFlow;
+    if (s == "transparent") return kBcTransparent;
+    if (s == "farfield") return kBcFarfield;
+    if (s == "inlet_2d" || s == "no_slip_wall")
         throw ConfigError("BoundaryType " + s + " is outside this library's scope");
     throw ConfigError("Unknown BoundaryType: " + s);
 }
@@ -170,7 +173,21 @@ void Solver::buildBoundaryStructures() {
     proto_.periodic = 0;
     for (size_t m = 0; m < boundaries_.size(); m++) {
         BoundaryPatch& b = boundaries_[m];
-        if (b.type == kBcRadialEq || b.type == kBcThrottle) {
+        if (b.type == kBcRadialEq || b.type == kBcThrottle || b.type == kBcMassFlow) {
+            // Solver::buildBoundaryDataStructures (src/solver.cpp:296-345): a
+            // mass-flow outlet uses radial equilibrium when its 4th value says
+            // so (or, without one, in axisymmetric or body-force cases) and the
+            // patch is an i-end face; otherwise one pressure for the patch
+            bool radial = true;
+            if (b.type == kBcMassFlow) {
+                const bool canDoRadial = b.i_min == b.i_max && b.i_min != 0 && b.j_max > b.j_min;
+                if (b.values.size() >= 4) radial = b.values[3] > 0.5 && canDoRadial;
+                else radial = canDoRadial && (topo_ == Topology::Axisymmetric || config_.isBFMActive());
+                if (b.values.empty() || b.values[0] <= 0.0)
+                    throw ConfigError("Target mass flow for boundary patch " + b.name + " must be specified and positive.");
+                if (b.i_min != b.i_max || b.i_min == 0)
+                    throw ConfigError("mass-flow outlets on other than the i-end face are outside this library's scope");
+            }
             if (b.i_min != b.i_max) throw ConfigError("Radial equilibrium only supported on j-k patches");
             if (b.i_min == 0) throw ConfigError("Radial equilibrium only supported to the last i-position");
             if (b.j_max <= b.j_min) throw ConfigError("Invalid boundary indices for radial equilibrium patch: " + b.name);
@@ -183,6 +200,13 @@ void Solver::buildBoundaryStructures() {
             proto_.prof_i[nprof] = static_cast<int>(b.i_min > 0 ? b.i_min - 1 : 0);
             proto_.prof_j0[nprof] = static_cast<int>(b.j_min);
             proto_.prof_kt[nprof] = b.type == kBcThrottle ? (b.values.empty() ? 0.0 : b.values[0]) : 0.0;
+            proto_.prof_fill[nprof] = radial ? 0 : 1;
+            proto_.prof_mf[nprof] = b.type == kBcMassFlow ? b.values[0] : 0.0;
+            proto_.prof_plane[nprof] = b.orientation;
+            // Config::getMassFlowRelaxation (include/config.hpp:291) or the patch's 3rd value
+            double relax = config_.parseFloat("MASS_FLOW_RELAXATION", 0.05);
+            if (b.type == kBcMassFlow && b.values.size() >= 3 && b.values[2] > 0.0) relax = b.values[2];
+            proto_.prof_relax[nprof] = relax;
             for (long j = b.j_min; j < b.j_max; j++) {
                 profR.push_back(mesh_.radius(b.i_max - 1, j, 0));
                 profP.push_back(0.0);
@@ -212,6 +236,12 @@ void Solver::buildBoundaryStructures() {
             b.flux = std::make_unique<BoundaryOutlet>(b.values[0]);
         } else if (b.type == kBcInviscidWall) {
             b.flux = std::make_unique<BoundaryInviscidWall>();
+        } else if (b.type == kBcInletSupersonic) {
+            b.flux = std::make_unique<BoundaryWithValues>(kBcInletSupersonic, b.values, 5,
+                                                          "inlet_supersonic needs pressure, temperature and 3 velocity components");
+        } else if (b.type == kBcFarfield) {
+            b.flux = std::make_unique<BoundaryWithValues>(kBcFarfield, b.values, 6,
+                                                          "farfield needs Mach number, pressure, temperature and a 3-component direction");
         } else {
             b.flux = std::make_unique<BoundaryFake>(b.type);
         }
@@ -282,6 +312,10 @@ void Solver::buildBoundaryStructures() {
     proto_.greitzer = config_.enableGreitzerModeling() ? 1 : 0;
     if (proto_.greitzer && !hasThrottle) throw ConfigError("Greitzer modeling enabled but no throttle boundary condition found!");
     if (proto_.greitzer || hasThrottle) needTurbo_ = true;
+    for (const auto& b : boundaries_)
+        if (b.type == kBcMassFlow) needTurbo_ = true;  // src/solver.cpp:1311-1316
+    // Config::getMassFlowMaxPressureChange (include/config.hpp:293)
+    proto_.mf_max_change = config_.parseFloat("MASS_FLOW_MAX_PRESSURE_CHANGE", 0.02);
     if (proto_.greitzer) {
         proto_.plenum_volume = config_.getGreitzerPlenumVolume();
         proto_.ambient_p = config_.getGreitzerAmbientPressure();
@@ -683,8 +717,19 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
         cudaCheck(cudaMemcpy(inst.c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
     }
     if (proto_.nprofiles) {
+        // Solver::initializeSolutionArrays (src/solver.cpp:819-834): a mass-flow
+        // outlet with a positive 2nd value starts from it, every other profile
+        // from the state's static pressure at i_max - 1
+        std::vector<const BoundaryPatch*> profPatch;
+        for (const auto& b : boundaries_)
+            if (b.type == kBcRadialEq || b.type == kBcThrottle || b.type == kBcMassFlow) profPatch.push_back(&b);
         std::vector<double> profP(profP_.size());
-        for (int m = 0; m < proto_.nprofiles; m++)
+        for (int m = 0; m < proto_.nprofiles; m++) {
+            const BoundaryPatch& b = *profPatch[static_cast<size_t>(m)];
+            if (b.type == kBcMassFlow && b.values.size() >= 2 && b.values[1] > 0.0) {
+                for (int jj = 0; jj < proto_.prof_n[m]; jj++) profP[proto_.prof_off[m] + jj] = b.values[1];
+                continue;
+            }
             for (int jj = 0; jj < proto_.prof_n[m]; jj++) {
                 double rho, et;
                 Vec3 u;
@@ -692,6 +737,7 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
                 profP[proto_.prof_off[m] + jj] =
                     table_ ? table_->pressure_rho_e(rho, FluidTable::staticEnergy_u_et(u, et)) : gas.pressure(rho, u, et);
             }
+        }
         cudaCheck(cudaMemcpy(inst.c.prof_p, profP.data(), profP.size() * sizeof(double), cudaMemcpyHostToDevice),
                   "cudaMemcpy");
     }

@@ -212,7 +212,7 @@ enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE };
 /* BoundaryType (include/types.hpp:178-194), restricted to the types on the path. */
 enum {
     BC_INLET = 0, BC_OUTLET, BC_RADIAL_EQ, BC_INVISCID_WALL, BC_WEDGE, BC_PERIODIC, BC_THROTTLE,
-    BC_EMPTY
+    BC_EMPTY, BC_INLET_SUPERSONIC, BC_OUTLET_SUPERSONIC, BC_MASS_FLOW, BC_TRANSPARENT, BC_FARFIELD
 };
 enum { BI_ISTART = 0, BI_IEND, BI_JSTART, BI_JEND, BI_KSTART, BI_KEND };
 
@@ -260,6 +260,7 @@ struct oracle_solver {
     long le_idx, te_idx;
     int inlet_cyl;
     double ramp_iters, init_p;
+    double mf_relax, mf_max_change; /* mass-flow outlet controller */
     int need_turbo;
     int turbo_dir; /* bcIndices pair */
     int greitzer;
@@ -954,12 +955,109 @@ static sv5 bc_inlet(const oracle_solver* s, const patch* pt, sv5 Uint, vec3 S, l
     return adv_flux(s, Wb, S);
 }
 
+/* FluidIdeal::computeDensity_p_T (src/fluid_ideal.cpp:134-136),
+ * FluidReal::computeDensity_p_T (src/fluid_real.cpp:279-281). */
+static double f_density_p_T(const oracle_solver* s, double p, double T) {
+    if (s->real) return table_interp(&s->lut->rho_pt, p, T);
+    return p / (s->rgas * T);
+}
+
+/* BoundaryInletSupersonic::computeBoundaryFlux (src/boundary_inlet_supersonic.cpp:4-34). */
+static sv5 bc_inlet_supersonic(const oracle_solver* s, const patch* pt, vec3 S) {
+    double p = pt->values[0], T = pt->values[1];
+    vec3 u = v3(pt->values[2], pt->values[3], pt->values[4]);
+    double rho = f_density_p_T(s, p, T);
+    double e = f_static_energy_p_rho(s, p, rho);
+    double et = e + 0.5 * vdot(u, u);
+    sv5 W = {{rho, u.x, u.y, u.z, et}};
+    return adv_flux(s, W, S);
+}
+
+/* BoundaryFarfield::computeBoundaryFlux (src/boundary_farfield.cpp:5-144). */
+static sv5 bc_farfield(const oracle_solver* s, const patch* pt, sv5 Uint, vec3 S) {
+    double g = s->gamma;
+    double machInf = pt->values[0], pInf = pt->values[1], TInf = pt->values[2];
+    vec3 dir = v3(pt->values[3], pt->values[4], pt->values[5]);
+    dir = vdiv(dir, vmag(dir));
+    double rhoInf = f_density_p_T(s, pInf, TInf);
+    double aInf = f_sound_speed_p_rho(s, pInf, rhoInf);
+    vec3 uInf = vmul(dir, machInf * aInf);
+    sv5 W = prim_of(Uint);
+    double rhoI = W.v[0];
+    vec3 uI = vel_of(W);
+    double pI = f_pressure_rho_u_et(s, rhoI, uI, W.v[4]);
+    double aI = f_sound_speed_p_rho(s, pI, rhoI);
+    vec3 n = vdiv(S, vmag(S));
+    double unI = vdot(uI, n), unInf = vdot(uInf, n);
+    sv5 Wb;
+    if (unI >= aI) {
+        Wb = W;
+    } else if (unI <= -aI) {
+        double eInf = f_static_energy_p_rho(s, pInf, rhoInf);
+        double etInf = eInf + 0.5 * vdot(uInf, uInf);
+        sv5 t = {{rhoInf, uInf.x, uInf.y, uInf.z, etInf}};
+        Wb = t;
+    } else {
+        double rhoB, eB, unB;
+        vec3 uRef;
+        if (!s->real) {
+            double Rp = unI + 2.0 * aI / (g - 1.0);
+            double Rm = unInf - 2.0 * aInf / (g - 1.0);
+            unB = 0.5 * (Rp + Rm);
+            double aB = 0.25 * (g - 1.0) * (Rp - Rm);
+            double rhoRef, pRef;
+            if (unB > 0.0) { rhoRef = rhoI; pRef = pI; uRef = uI; }
+            else { rhoRef = rhoInf; pRef = pInf; uRef = uInf; }
+            double ent = pRef / pow(rhoRef, g);
+            rhoB = pow(aB * aB / (g * ent), 1.0 / (g - 1.0));
+            double pB = rhoB * aB * aB / g;
+            eB = f_static_energy_p_rho(s, pB, rhoB);
+        } else {
+            double rhoAvg = 0.5 * (rhoI + rhoInf);
+            double aAvg = 0.5 * (aI + aInf);
+            double Z = rhoAvg * aAvg;
+            double Rp = unI + pI / Z;
+            double Rm = unInf - pInf / Z;
+            unB = 0.5 * (Rp + Rm);
+            double pB = 0.5 * (Rp - Rm) * Z;
+            double sRef;
+            if (unB > 0.0) {
+                double eI = W.v[4] - 0.5 * vdot(uI, uI);
+                sRef = table_interp(&s->lut->s, rhoI, eI);
+                uRef = uI;
+            } else {
+                sRef = table_interp(&s->lut->s_pt, pInf, TInf);
+                uRef = uInf;
+            }
+            rhoB = table_interp(&s->lut->rho_ps, pB, sRef);
+            eB = table_interp(&s->lut->e_ps, pB, sRef);
+        }
+        vec3 ut = vsub(uRef, vmul(n, vdot(uRef, n)));
+        vec3 uB = vadd(ut, vmul(n, unB));
+        double etB = eB + 0.5 * vdot(uB, uB);
+        sv5 t = {{rhoB, uB.x, uB.y, uB.z, etB}};
+        Wb = t;
+    }
+    return adv_flux(s, Wb, S);
+}
+
 static sv5 boundary_flux(oracle_solver* s, int pidx, sv5 Uint, vec3 S, long fi, long fj, long fk,
                          long it) {
     const patch* p = &s->patches[pidx];
     switch (p->type) {
         case BC_INLET: return bc_inlet(s, p, Uint, S, fi, fj, fk);
         case BC_OUTLET: return bc_outlet(s, Uint, S, p->values[0], it);
+        case BC_INLET_SUPERSONIC: return bc_inlet_supersonic(s, p, S);
+        case BC_OUTLET_SUPERSONIC: /* src/boundary_outlet_supersonic.cpp:4-14 */
+            return adv_flux(s, prim_of(Uint), S);
+        case BC_FARFIELD: return bc_farfield(s, p, Uint, S);
+        case BC_TRANSPARENT: /* src/boundary_transparent.cpp:5-16 */
+            return flux_interior(s, Uint, Uint, Uint, Uint, S);
+        case BC_MASS_FLOW: { /* src/boundary_outlet_mass_flow.cpp:4-19 */
+            const radial_profile* rp = &s->profiles[p->profile];
+            long idx = fj < rp->n ? fj : rp->n - 1;
+            return bc_outlet(s, Uint, S, rp->pressure[idx], it);
+        }
         case BC_RADIAL_EQ:
         case BC_THROTTLE: /* src/boundary_outlet_throttle.cpp:5-16, radial_equilibrium.cpp:5-16 */
             return bc_outlet(s, Uint, S, s->profiles[p->profile].pressure[fj], it);
@@ -1542,6 +1640,21 @@ static void update_radial_profiles(oracle_solver* s, double* const* U) {
             for (int b = 0; b < s->npatches; b++)
                 if (s->patches[b].type == BC_INLET) { ptin = s->patches[b].values[0]; break; }
             s->hub_p = ptin + kt * mf * mf;
+        } else if (bp->type == BC_MASS_FLOW) { /* src/solver.cpp:2734-2770 */
+            double target = bp->values[0];
+            double cur = fabs(s->massflow[bp->orientation]);
+            if (s->topology == TOPO_AXI) cur *= 2.0 * M_PI / s->wedge;
+            else if (s->per_angle_deg != 0.0) cur *= 360.0 / s->per_angle_deg;
+            double relax = s->mf_relax;
+            if (bp->nvalues >= 3 && bp->values[2] > 0.0) relax = bp->values[2];
+            double err = (cur - target) / target;
+            double dp = relax * err;
+            if (dp < -s->mf_max_change) dp = -s->mf_max_change;
+            else if (s->mf_max_change < dp) dp = s->mf_max_change;
+            double p0 = rp->pressure[0];
+            if (p0 <= 0.0) p0 = s->init_p > 0.0 ? s->init_p : 101325.0;
+            s->hub_p = p0 * (1.0 + dp);
+            if (s->hub_p < 100.0) s->hub_p = 100.0;
         } else if (bp->type == BC_RADIAL_EQ) {
             s->hub_p = rp->pressure[0];
         }
@@ -1879,6 +1992,12 @@ static int bc_type_of(const char* name, int* out) { /* boundaryTypeFromString, i
     else if (!strcmp(low, "periodic")) *out = BC_PERIODIC;
     else if (!strcmp(low, "throttle")) *out = BC_THROTTLE;
     else if (!strcmp(low, "empty")) *out = BC_EMPTY;
+    else if (!strcmp(low, "inlet_supersonic")) *out = BC_INLET_SUPERSONIC;
+    else if (!strcmp(low, "outlet_supersonic")) *out = BC_OUTLET_SUPERSONIC;
+    else if (!strcmp(low, "mass_flow") || !strcmp(low, "outlet_mass_flow") || !strcmp(low, "massflow") ||
+             !strcmp(low, "mass_flow_rate")) *out = BC_MASS_FLOW;
+    else if (!strcmp(low, "transparent")) *out = BC_TRANSPARENT;
+    else if (!strcmp(low, "farfield")) *out = BC_FARFIELD;
     else return fail("Boundary type '%s' is not supported by the oracle", name);
     return 0;
 }
@@ -1939,14 +2058,25 @@ static int read_boundaries(oracle_solver* s, const char* path) {
 static int build_boundary_structures(oracle_solver* s) {
     for (int m = 0; m < s->npatches; m++) {
         patch* p = &s->patches[m];
-        if (p->type == BC_RADIAL_EQ || p->type == BC_THROTTLE) {
+        if (p->type == BC_RADIAL_EQ || p->type == BC_THROTTLE || p->type == BC_MASS_FLOW) {
+            /* Solver::buildBoundaryDataStructures (src/solver.cpp:296-345) */
+            int radial = 1;
+            if (p->type == BC_MASS_FLOW) {
+                int can = p->i_min == p->i_max && p->i_min != 0 && p->j_max > p->j_min;
+                if (p->nvalues >= 4) radial = p->values[3] > 0.5 && can;
+                else radial = can && (s->topology == TOPO_AXI || s->bfm_active);
+                if (p->nvalues < 1 || p->values[0] <= 0.0)
+                    return fail("Target mass flow for boundary patch %s must be specified and positive.", p->name);
+                if (p->i_min != p->i_max || p->i_min == 0)
+                    return fail("mass-flow outlets on other than the i-end face are outside the oracle's scope");
+            }
             if (p->i_min != p->i_max) return fail("Radial equilibrium only supported on j-k patches");
             if (p->i_min == 0) return fail("Radial equilibrium only supported to the last i-position");
             if (p->j_max <= p->j_min) return fail("Invalid boundary indices for radial equilibrium patch: %s", p->name);
             radial_profile rp;
             memset(&rp, 0, sizeof rp);
             rp.n = (int)(p->j_max - p->j_min);
-            rp.nradius = rp.n;
+            rp.nradius = radial ? rp.n : 0;
             rp.pressure = (double*)calloc(rp.n, sizeof(double));
             rp.radius = (double*)calloc(rp.n, sizeof(double));
             for (long j = p->j_min; j < p->j_max; j++) rp.radius[j - p->j_min] = node_radius(s, p->i_max - 1, j, 0);
@@ -2483,8 +2613,22 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
     dir_join(path, sizeof path, base, bcf);
     if (read_boundaries(s, path) || build_boundary_structures(s)) { oracle_destroy(s); return 1; }
     resolve_turbo_dir(s);
-    for (int m = 0; m < s->npatches; m++)
+    for (int m = 0; m < s->npatches; m++) {
         if (s->patches[m].type == BC_THROTTLE) { s->need_turbo = 1; s->throttle_kt = s->patches[m].values[0]; }
+        if (s->patches[m].type == BC_MASS_FLOW) s->need_turbo = 1; /* src/solver.cpp:1311-1316 */
+        if (s->patches[m].type == BC_INLET_SUPERSONIC && s->patches[m].nvalues < 5)
+            { fail("inlet_supersonic needs pressure, temperature and 3 velocity components"); oracle_destroy(s); return 1; }
+        if (s->patches[m].type == BC_FARFIELD && s->patches[m].nvalues < 6)
+            { fail("farfield needs Mach number, pressure, temperature and a 3-component direction"); oracle_destroy(s); return 1; }
+    }
+    /* Config::getMassFlowRelaxation / getMassFlowMaxPressureChange (include/config.hpp:291-293) */
+    s->mf_relax = 0.05;
+    s->mf_max_change = 0.02;
+    if (cfg_get(&s->cfg, "MASS_FLOW_RELAXATION") && cfg_float(&s->cfg, "MASS_FLOW_RELAXATION", &s->mf_relax))
+        { oracle_destroy(s); return 1; }
+    if (cfg_get(&s->cfg, "MASS_FLOW_MAX_PRESSURE_CHANGE") &&
+        cfg_float(&s->cfg, "MASS_FLOW_MAX_PRESSURE_CHANGE", &s->mf_max_change))
+        { oracle_destroy(s); return 1; }
     if (s->greitzer && s->throttle_kt == 0.0) {
         int found = 0;
         for (int m = 0; m < s->npatches; m++) if (s->patches[m].type == BC_THROTTLE) found = 1;
@@ -2506,10 +2650,14 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
         double Th = f_temperature_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
         s->gz_p = ph; s->gz_min = s->turbo[0]; s->gz_mout = s->turbo[0]; s->gz_T = Th; s->gz_t = 0.0;
     }
-    /* initial radial profiles (src/solver.cpp:767-776) */
+    /* initial radial profiles (src/solver.cpp:818-834) */
     for (int m = 0; m < s->nprofiles; m++) {
         radial_profile* rp = &s->profiles[m];
         const patch* p = &s->patches[rp->patch];
+        if (p->type == BC_MASS_FLOW && p->nvalues >= 2 && p->values[1] > 0.0) {
+            for (int q = 0; q < rp->n; q++) rp->pressure[q] = p->values[1];
+            continue;
+        }
         long i = p->i_min > 0 ? p->i_min - 1 : 0;
         int kk = 0;
         for (long j = p->j_min; j < p->j_max && kk < rp->n; j++) {

@@ -45,6 +45,52 @@ def _co2(case):
     return cases.with_real_gas(case, pt=8.0e6, tt=320.0, p_init=7.6e6, t_init=315.0, table={"n_rho": 24, "n_e": 24, "n_p": 20, "n_T": 20, "n_s": 20})
 
 
+def _bump_bc(inlet: str, outlet: str, **kw):
+    """The bump channel with other inlet / outlet boundary conditions."""
+    c = cases.bump2d(ni=24, nj=12, **kw)
+    c.patches[0] = dataclasses.replace(c.patches[0], spec=inlet)
+    c.patches[1] = dataclasses.replace(c.patches[1], spec=outlet)
+    return c
+
+
+def _bump_farfield():
+    ps, ts = cases.static_state(101325.0, 288.15, 0.5)
+    ff = f"farfield, 0.5, {ps!r}, {ts!r}, 1, 0, 0"
+    return _bump_bc(ff, ff)
+
+
+def _bump_farfield_supersonic():
+    ps, ts = cases.static_state(101325.0, 288.15, 1.6)
+    ff = f"farfield, 1.6, {ps!r}, {ts!r}, 1, 0, 0"
+    return _bump_bc(ff, ff, mach=1.6, cfl=1.0)
+
+
+def _bump_supersonic():
+    ps, ts = cases.static_state(101325.0, 288.15, 1.6)
+    u = 1.6 * (1.4 * 287.05 * ts) ** 0.5
+    return _bump_bc(f"inlet_supersonic, {ps!r}, {ts!r}, {u!r}, 0, 0", "outlet_supersonic", mach=1.6, cfl=1.0)
+
+
+def _mass_flow(spec: str, **settings):
+    c = cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS)
+    c.patches[1] = dataclasses.replace(c.patches[1], spec=spec)
+    return c.with_settings(**settings) if settings else c
+
+
+def _sector_mass_flow():
+    c = _sector(45.0)
+    c.patches[1] = dataclasses.replace(c.patches[1], spec="mass_flow, 8.0")
+    return c
+
+
+def _co2_farfield():
+    ff = "farfield, 0.3, 7600000.0, 315.0, 1, 0, 0"
+    c = _co2(cases.bump2d(ni=24, nj=12, mach=0.3))
+    c.patches[0] = dataclasses.replace(c.patches[0], spec=ff)
+    c.patches[1] = dataclasses.replace(c.patches[1], spec=ff)
+    return c
+
+
 CASES = {
     "bump_jst_rk4": (lambda: cases.bump2d(ni=24, nj=12), 20),
     "bump_roe_vanalbada_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
@@ -65,4 +111,15 @@ CASES = {
     "co2_meridional_hall": (lambda: _co2(cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS)), 20),
     "co2_meridional_greitzer": (lambda: _co2(_throttle(True)), 20),
     "co2_annulus_roe_hall": (lambda: _co2(cases.annulus3d(ni=20, nj=8, nk=9, rows=cases.MAP_ROWS)), 5),
+    "bump_farfield": (_bump_farfield, 20),
+    "bump_farfield_supersonic": (_bump_farfield_supersonic, 20),
+    "bump_supersonic_in_out": (_bump_supersonic, 20),
+    "bump_transparent_jst": (lambda: _bump_bc("inlet, 101325.0, 288.15, 1, 0, 0", "transparent"), 20),
+    "bump_transparent_roe_muscl": (lambda: _bump_bc("inlet, 101325.0, 288.15, 1, 0, 0", "transparent", scheme="Roe",
+                                                    muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
+    "meridional_mass_flow_radial": (lambda: _mass_flow("mass_flow, 70.0"), 20),
+    "meridional_mass_flow_uniform": (lambda: _mass_flow("mass_flow, 70.0, 101325.0, 0.1, 0",
+                                                        MASS_FLOW_MAX_PRESSURE_CHANGE="0.05"), 20),
+    "sector45_mass_flow": (_sector_mass_flow, 10),
+    "co2_bump_farfield": (_co2_farfield, 20),
 }
