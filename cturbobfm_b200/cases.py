@@ -75,6 +75,9 @@ class Case:
     # keyword arguments of fluid_table.write for FLUID_MODEL = real (the table
     # is written next to input.ini under FLUID_TABLE_FILE)
     table: Optional[Dict] = None
+    # further input files written next to input.ini (name -> text), e.g. the
+    # Chima scaling functions
+    files: Optional[Dict[str, str]] = None
 
     @property
     def shape(self) -> Tuple[int, int, int]:
@@ -117,6 +120,9 @@ class Case:
         settings["BOUNDARY_CONDITIONS_FILEPATH"] = "boundaries.csv"
         for p in self.patches:
             settings[p.name] = p.spec
+        for name, text in (self.files or {}).items():
+            with open(os.path.join(directory, name), "w") as f:
+                f.write(text)
         if self.table is not None:
             from . import fluid_table
 

@@ -99,6 +99,8 @@ struct Control {
     // real gas: mass-weighted total-enthalpy and entropy integrals over the
     // inlet / outlet planes (enthalpy-based efficiency)
     double ht_int[2], s_int[2];
+    // Chima: turning and loss scaling at the iteration's mass flow
+    double chima_turn, chima_loss;
 };
 
 // A block's share of a batched launch: `count` consecutive elements (nodes,
@@ -191,6 +193,12 @@ struct alignas(16) DevCaseT {
     const R* devstall;
     const R* ldbeta0;
     const R* ldkp;
+    const R* dangmom;   // Chima: deltaAngularMomentum
+    const R* dentropy;  // Chima: deltaEntropy
+    const double* chima_mf;    // Chima scaling functions over the mass flow
+    const double* chima_turn;
+    const double* chima_loss;
+    int chima_n;
     // state
     R* U[5];   // U^n
     R* Uc[5];  // Kahan compensation of U^n (compensated path; true state = U - Uc)

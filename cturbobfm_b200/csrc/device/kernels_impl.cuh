@@ -131,6 +131,17 @@ __device__ __noinline__ S5<R> boundaryFlux(const DevCaseT<R>& c, Gas<R> gs, int 
     }
 }
 
+// linearInterpolation (src/math_utils.cpp:487-514): constant beyond the ends,
+// otherwise linear in the interval [x_i, x_i+1) that holds xp (x ascending).
+__device__ __forceinline__ double linearInterpolation(const double* x, const double* y, int n, double xp) {
+    if (xp <= x[0]) return y[0];
+    if (xp >= x[n - 1]) return y[n - 1];
+    int i = 0;
+    while (i + 1 < n && x[i + 1] <= xp) i++;  // last x_i <= xp: std::upper_bound - 1
+    const double t = (xp - x[i]) / (x[i + 1] - x[i]);
+    return (1.0 - t) * y[i] + t * y[i + 1];
+}
+
 // Deterministic block sum of NV doubles per thread; result valid in thread 0.
 template <int NV>
 __device__ __forceinline__ void blockSum(double (&v)[NV]) {
@@ -672,6 +683,10 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
         ctl->turbo[2] = tr;
         ctl->turbo[3] = eta;
         ctl->has_turbo = 1;
+        if (c.bfm_model == 5) {  // SourceBFMChima::computeBodyForceSource (src/source_bfm_chima.cpp:33-41)
+            ctl->chima_turn = linearInterpolation(c.chima_mf, c.chima_turn, c.chima_n, mflow);
+            ctl->chima_loss = linearInterpolation(c.chima_mf, c.chima_loss, c.chima_n, mflow);
+        }
     }
     if (!profiles || (c.nprofiles == 0 && !c.greitzer)) return;
     if (c.greitzer) {

@@ -50,7 +50,7 @@ CTBFM_DI S5<R> gongSource(const DevCaseT<R>& c, R* const* U, R omega, int i, int
 // SourceBFMBase::computeFlowState (src/source_bfm_base.cpp:104-149).
 template <typename R>
 struct BfmState {
-    R radius, omega, pitch, staggered, blockage, flowAngle, dev, cth, sth;
+    R radius, omega, pitch, staggered, blockage, flowAngle, dev, cth, sth, vmer;
     V3<R> relCyl, relCart, nCyl, invDirCyl, viscDirCyl;
 };
 
@@ -91,6 +91,7 @@ CTBFM_DI void bfmFlowState(const DevCaseT<R>& c, long long q, const S5<R>& W, do
     b.relCyl = velCyl - drag;
     b.relCart = cartOfCyl(b.relCyl, b.cth, b.sth);
     const R vmer = sqrt(velCyl.x * velCyl.x + velCyl.y * velCyl.y);
+    b.vmer = vmer;
     const R nb = c.nblades[q];
     b.pitch = R(2) * R(M_PI) * b.radius / nb;
     b.nCyl = v3(c.nax[q], c.nrad[q], c.ntan[q]);
@@ -133,10 +134,29 @@ template <typename R>
 CTBFM_DI S5<R> bfmBodyForce(const DevCaseT<R>& c, Gas<R> gs, int i, int j, int k, long long q, const S5<R>& W,
                             double t) {
     // SourceBFMBase::computeBodyForceSource: no force for "None" / "Blockage"
-    if (c.bfm_model != 1 && c.bfm_model != 2 && c.bfm_model != 3) return zero5<R>();
+    if (c.bfm_model != 1 && c.bfm_model != 2 && c.bfm_model != 3 && c.bfm_model != 5) return zero5<R>();
     BfmState<R> b;
     bfmFlowState(c, q, W, t, b);
     const R vol = c.vol[q];
+    if (c.bfm_model == 5) {  // Chima (src/source_bfm_chima.cpp:16-190)
+        // SourceBFMChima::computeDerivativeFunction (:180-190): parabolic
+        auto deriv = [](R yF, R xL, R xF) { return R(-2.0) * yF * xL / (xF * xF) + R(2.0) * yF / xF; };
+        const R sLoc = c.stwl[q];
+        const R sTe = c.stwl[nodeIdx(c, c.te_idx, j, k)];
+        const V3<R> u = velOf(W);
+        // viscous component first (:146-178); its tangential force enters the inviscid one
+        const R dSdM = deriv(c.dentropy[q], sLoc, sTe) * R(c.ctl->chima_loss);
+        const R T = temperature_rho_u_et(gs, W.v[0], u, W.v[4]);
+        const R fv = T * b.vmer / mag(b.relCyl) * dSdM;
+        const V3<R> fvCyl = b.viscDirCyl * fv;
+        const S5<R> visc = forceSource(fvCyl, b, vol, W.v[0]);
+        // inviscid component (:51-83)
+        const R dLdM = deriv(c.dangmom[q], sLoc, sTe) * R(c.ctl->chima_turn);
+        const R ftan = dLdM * b.vmer / b.radius;
+        const R fi = (ftan - fvCyl.z) / b.invDirCyl.z;
+        const S5<R> inv = forceSource(b.invDirCyl * fi, b, vol, W.v[0]);
+        return inv + visc;
+    }
     const R w2 = dot(b.relCyl, b.relCyl);
     if (c.bfm_model == 1) {  // Hall
         const R fm = w2 * R(M_PI) * b.dev / b.pitch / fabs(b.nCyl.z);

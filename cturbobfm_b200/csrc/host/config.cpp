@@ -173,7 +173,8 @@ BfmModel Config::getBFMModel() const {
     if (v == "None") return BfmModel::None;
     if (v == "Blockage") return BfmModel::Blockage;
     if (v == "Lift-Drag") return BfmModel::LiftDrag;
-    if (v == "Chima" || v == "Correlations")
+    if (v == "Chima") return BfmModel::Chima;
+    if (v == "Correlations")
         throw ConfigError("BFM_MODEL \"" + v + "\" is outside this library's scope");
     throw ConfigError("Invalid value for key \"BFM_MODEL\" in configuration.");
 }

@@ -196,4 +196,26 @@ private:
     int le_, te_;
 };
 
+// SourceBFMChima (src/source_bfm_chima.cpp:3-13): leading / trailing edge
+// indices and the scaling functions of turning and loss over the mass flow,
+// read from CHIMA_SCALING_FUNCTIONS_FILEPATH (a CSV table with the columns
+// MassFlow, PhiTurn, PhiLoss; InputTable, src/input_table.cpp:8-55).
+class SourceBFMChima : public SourceBFMBase {
+public:
+    explicit SourceBFMChima(const Config& config);
+    BfmModel model() const override { return BfmModel::Chima; }
+    void configure(DevCase& c) const override {
+        SourceBFMBase::configure(c);
+        c.le_idx = le_;
+        c.te_idx = te_;
+    }
+    const std::vector<double>& massFlow() const { return mf_; }
+    const std::vector<double>& turning() const { return turn_; }
+    const std::vector<double>& loss() const { return loss_; }
+
+private:
+    int le_, te_;
+    std::vector<double> mf_, turn_, loss_;
+};
+
 }  // namespace ctbfm

@@ -51,6 +51,68 @@ struct HostGas {
 
 }  // namespace
 
+// The input-field names a CSV table may carry (FieldNameMapper,
+// include/types.hpp:1083-1127); an unknown name is an error.
+static bool knownFieldName(const std::string& n) {
+    static const char* names[] = {
+        "x", "y", "z", "rho", "rho_u", "rho_v", "rho_w", "rho_e", "blockage", "normalAxial", "normalRadial",
+        "normalTangential", "rpm", "streamwiseLength", "bladePresent", "numberBlades", "spanwiseLength", "Dht_Dm",
+        "Ds_Dm", "MassFlow", "PhiTurn", "PhiLoss", "PhiDev", "bladeMetalAngle", "bladeGasPathAngle", "bladeLeanAngle",
+        "bladeCamberCurvature", "Pt", "Tt", "nx", "ny", "nz", "dbladeMetalAngle_dm", "deviationAnglePivot",
+        "deltaAngularMomentum", "deltaEntropy", "deltaFlowAngle", "deviationAngleStall", "liftDragBeta0",
+        "liftDragBetaEtamax", "liftDragKpEtamax"};
+    for (const char* k : names)
+        if (n == k) return true;
+    return false;
+}
+
+SourceBFMChima::SourceBFMChima(const Config& config) : SourceBFMBase(config), le_(0), te_(0) {
+    // InputTable::readCsvFile (src/input_table.cpp:14-55): a header line of
+    // field names, then rows of values, column by column
+    if (!config.has("CHIMA_SCALING_FUNCTIONS_FILEPATH"))
+        throw ConfigError("Not found value for key \"CHIMA_SCALING_FUNCTIONS_FILEPATH\" in configuration.");
+    std::string path = config.get("CHIMA_SCALING_FUNCTIONS_FILEPATH");
+    if (!path.empty() && path[0] != '/' && !config.directory().empty()) path = config.directory() + "/" + path;
+    std::ifstream f(path);
+    if (!f) throw ConfigError("Error opening file: " + path);
+    std::string line;
+    std::vector<std::string> head;
+    if (std::getline(f, line)) {
+        std::stringstream hs(line);
+        std::string col;
+        while (std::getline(hs, col, ',')) {
+            if (!knownFieldName(col)) throw ConfigError("Unknown field name: " + col);
+            head.push_back(col);
+        }
+    }
+    std::vector<std::vector<double>> cols(head.size());
+    while (std::getline(f, line)) {
+        std::stringstream ss(line);
+        std::string tok;
+        size_t idx = 0;
+        while (std::getline(ss, tok, ',') && idx < head.size()) {
+            try {
+                cols[idx].push_back(std::stod(tok));
+            } catch (const std::exception&) {
+            }
+            ++idx;
+        }
+    }
+    auto column = [&](const char* name) -> const std::vector<double>& {
+        for (size_t q = 0; q < head.size(); q++)
+            if (head[q] == name) return cols[q];
+        throw ConfigError(std::string("Chima scaling functions file ") + path + " has no " + name + " column");
+    };
+    mf_ = column("MassFlow");
+    turn_ = column("PhiTurn");
+    loss_ = column("PhiLoss");
+    if (mf_.empty() || turn_.size() != mf_.size() || loss_.size() != mf_.size())
+        throw ConfigError("Chima scaling functions file " + path + " needs equally long MassFlow, PhiTurn, PhiLoss columns");
+    // the table member is initialised before the edge indices (include/source_bfm_chima.hpp:48-52)
+    le_ = static_cast<int>(config.parseFloat("LEADING_EDGE_INDEX"));
+    te_ = static_cast<int>(config.parseFloat("TRAILING_EDGE_INDEX"));
+}
+
 Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_(config.getTopology()) {
     if (config.isViscosityActive()) throw ConfigError("Viscous fluxes are outside this library's Euler path");
     if (config.parseBool("TURBULENCE_ACTIVE", false)) throw ConfigError("Turbulence models are outside this library's Euler path");
@@ -110,6 +172,7 @@ void Solver::setupModels() {
         case BfmModel::Hall: bfm_ = std::make_unique<SourceBFMHall>(config_); break;
         case BfmModel::HallThollet: bfm_ = std::make_unique<SourceBFMThollet>(config_); break;
         case BfmModel::LiftDrag: bfm_ = std::make_unique<SourceBFMLiftDrag>(config_); break;
+        case BfmModel::Chima: bfm_ = std::make_unique<SourceBFMChima>(config_); break;
         default: bfm_ = std::make_unique<SourceBFMBase>(config_); break;
     }
 }
@@ -314,6 +377,8 @@ void Solver::buildBoundaryStructures() {
     if (proto_.greitzer || hasThrottle) needTurbo_ = true;
     for (const auto& b : boundaries_)
         if (b.type == kBcMassFlow) needTurbo_ = true;  // src/solver.cpp:1311-1316
+    // the Chima model scales its forces by the current mass flow (src/solver.cpp:1319-1321)
+    if (config_.isBFMActive() && config_.getBFMModel() == BfmModel::Chima) needTurbo_ = true;
     // Config::getMassFlowMaxPressureChange (include/config.hpp:293)
     proto_.mf_max_change = config_.parseFloat("MASS_FLOW_MAX_PRESSURE_CHANGE", 0.02);
     if (proto_.greitzer) {
@@ -440,7 +505,7 @@ void Solver::setupScalars() {
         c.pert_t0 = config_.parseFloat("PERTURBATION_TIME_START");
         c.pert_dur = config_.parseFloat("PERTURBATION_TIME_DURATION");
     }
-    if (c.bfm && c.bfm_model == 3) {
+    if (c.bfm && (c.bfm_model == 3 || c.bfm_model == 5)) {
         if (c.le_idx < 0 || c.le_idx >= NI || c.te_idx < 0 || c.te_idx >= NI)
             throw ConfigError("LEADING_EDGE_INDEX / TRAILING_EDGE_INDEX outside the grid");
     }
@@ -563,7 +628,9 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
     }
     // BFM fields (include/types.hpp:1036-1078 names)
     c.blk = c.gbx = c.gby = c.gbz = c.nax = c.nrad = c.ntan = c.rpm = c.stwl = c.bpresent = c.nblades = nullptr;
-    c.cosmetal = c.devpivot = c.devstall = c.ldbeta0 = c.ldkp = nullptr;
+    c.cosmetal = c.devpivot = c.devstall = c.ldbeta0 = c.ldkp = c.dangmom = c.dentropy = nullptr;
+    c.chima_mf = c.chima_turn = c.chima_loss = nullptr;
+    c.chima_n = 0;
     if (c.bfm) {
         auto need = [&](const char* name) { return inst.uploadR(mesh_.field(name)); };
         auto opt = [&](const char* name) -> const R* {
@@ -597,7 +664,16 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         } else {
             c.rpm = opt("rpm");
         }
-        if (c.bfm_model == 2 || c.bfm_model == 3) c.stwl = need("streamwiseLength");
+        if (c.bfm_model == 2 || c.bfm_model == 3 || c.bfm_model == 5) c.stwl = need("streamwiseLength");
+        if (c.bfm_model == 5) {  // SourceBFMChima::computeInviscid/ViscousComponent
+            c.dangmom = need("deltaAngularMomentum");
+            c.dentropy = need("deltaEntropy");
+            const auto* chima = static_cast<const SourceBFMChima*>(bfm_.get());
+            c.chima_n = static_cast<int>(chima->massFlow().size());
+            c.chima_mf = inst.uploadD(chima->massFlow());
+            c.chima_turn = inst.uploadD(chima->turning());
+            c.chima_loss = inst.uploadD(chima->loss());
+        }
         if (c.bfm_model == 2 && c.offdesign) c.devpivot = need("deviationAnglePivot");
         if (c.stalled) c.devstall = need("deviationAngleStall");
         if (c.bfm_model == 3) {

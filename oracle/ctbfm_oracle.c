@@ -208,7 +208,7 @@ enum { TOPO_2D = 0, TOPO_3D = 1, TOPO_AXI = 2, TOPO_1D = 3 };
 enum { SCHEME_JST = 0, SCHEME_ROE = 1 };
 enum { LIM_NONE = 0, LIM_VAN_ALBADA, LIM_VAN_LEER, LIM_MIN_MOD };
 enum { DT_LOCAL = 0, DT_GLOBAL, DT_FIXED };
-enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE };
+enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE, BFM_CHIMA };
 /* BoundaryType (include/types.hpp:178-194), restricted to the types on the path. */
 enum {
     BC_INLET = 0, BC_OUTLET, BC_RADIAL_EQ, BC_INVISCID_WALL, BC_WEDGE, BC_PERIODIC, BC_THROTTLE,
@@ -237,12 +237,13 @@ typedef struct {
 
 enum {
     F_BLOCKAGE = 0, F_NAX, F_NRAD, F_NTAN, F_RPM, F_STWL, F_BLADE_PRESENT, F_NBLADES, F_METAL,
-    F_GASPATH, F_LEAN, F_DEV_PIVOT, F_DEV_STALL, F_LD_BETA0, F_LD_KP, F_COUNT
+    F_GASPATH, F_LEAN, F_DEV_PIVOT, F_DEV_STALL, F_LD_BETA0, F_LD_KP, F_DANGMOM, F_DENTROPY, F_COUNT
 };
 static const char* FIELD_NAMES[F_COUNT] = {
     "blockage", "normalAxial", "normalRadial", "normalTangential", "rpm", "streamwiseLength",
     "bladePresent", "numberBlades", "bladeMetalAngle", "bladeGasPathAngle", "bladeLeanAngle",
-    "deviationAnglePivot", "deviationAngleStall", "liftDragBeta0", "liftDragKpEtamax"};
+    "deviationAnglePivot", "deviationAngleStall", "liftDragBeta0", "liftDragKpEtamax",
+    "deltaAngularMomentum", "deltaEntropy"};
 
 struct oracle_solver {
     config cfg;
@@ -258,6 +259,8 @@ struct oracle_solver {
     int accel; double acc_t0, acc_t1, acc_s0, acc_s1;
     double pert_center[3], pert_radius, pert_scale, pert_t0, pert_dur;
     long le_idx, te_idx;
+    double *chima_mf, *chima_turn, *chima_loss; /* Chima scaling functions */
+    int chima_n;
     int inlet_cyl;
     double ramp_iters, init_p;
     double mf_relax, mf_max_change; /* mass-flow outlet controller */
@@ -1248,12 +1251,104 @@ static double thollet_kmach(const oracle_solver* s, vec3 rel, sv5 W) {
     return dmin(3.0, kp);
 }
 
+/* InputTable::readCsvFile (src/input_table.cpp:14-55) for the Chima scaling
+ * functions: a header line of field names, then rows of values appended
+ * column by column; the MassFlow, PhiTurn and PhiLoss columns. */
+static int read_chima_table(oracle_solver* s, const char* path) {
+    FILE* f = fopen(path, "r");
+    if (!f) return fail("Error opening file: %s", path);
+    char* line = NULL;
+    size_t cap = 0;
+    char names[64][64];
+    int nh = 0;
+    if (getline(&line, &cap, f) >= 0) {
+        size_t L = strlen(line);
+        if (L && line[L - 1] == '\n') line[--L] = 0;
+        char* p = line;
+        while (nh < 64) {
+            char* c = strchr(p, ',');
+            if (c) *c = 0;
+            snprintf(names[nh++], 64, "%s", p);
+            if (!c) break;
+            p = c + 1;
+        }
+    }
+    int im = -1, it = -1, il = -1;
+    for (int h = 0; h < nh; h++) {
+        if (!strcmp(names[h], "MassFlow")) im = h;
+        if (!strcmp(names[h], "PhiTurn")) it = h;
+        if (!strcmp(names[h], "PhiLoss")) il = h;
+    }
+    if (im < 0 || it < 0 || il < 0) { free(line); fclose(f); return fail("Chima scaling functions file %s lacks a column", path); }
+    int cap_rows = 16;
+    s->chima_mf = (double*)malloc(cap_rows * sizeof(double));
+    s->chima_turn = (double*)malloc(cap_rows * sizeof(double));
+    s->chima_loss = (double*)malloc(cap_rows * sizeof(double));
+    s->chima_n = 0;
+    while (getline(&line, &cap, f) >= 0) {
+        double v[64];
+        int nv = 0;
+        char* save = NULL;
+        for (char* t = strtok_r(line, ",\n", &save); t && nv < 64; t = strtok_r(NULL, ",\n", &save)) v[nv++] = strtod(t, NULL);
+        if (nv <= im || nv <= it || nv <= il) continue;
+        if (s->chima_n == cap_rows) {
+            cap_rows *= 2;
+            s->chima_mf = (double*)realloc(s->chima_mf, cap_rows * sizeof(double));
+            s->chima_turn = (double*)realloc(s->chima_turn, cap_rows * sizeof(double));
+            s->chima_loss = (double*)realloc(s->chima_loss, cap_rows * sizeof(double));
+        }
+        s->chima_mf[s->chima_n] = v[im];
+        s->chima_turn[s->chima_n] = v[it];
+        s->chima_loss[s->chima_n] = v[il];
+        s->chima_n++;
+    }
+    free(line);
+    fclose(f);
+    if (s->chima_n == 0) return fail("Chima scaling functions file %s has no data rows", path);
+    return 0;
+}
+
+/* linearInterpolation (src/math_utils.cpp:487-514). */
+static double linear_interp(const double* x, const double* y, int n, double xp) {
+    if (xp <= x[0]) return y[0];
+    if (xp >= x[n - 1]) return y[n - 1];
+    int i = 0;
+    while (i + 1 < n && x[i + 1] <= xp) i++;
+    double t = (xp - x[i]) / (x[i + 1] - x[i]);
+    return (1.0 - t) * y[i] + t * y[i + 1];
+}
+
+/* SourceBFMChima::computeDerivativeFunction (src/source_bfm_chima.cpp:180-190). */
+static double chima_derivative(double yF, double xL, double xF) {
+    return -2.0 * yF * xL / (xF * xF) + 2.0 * yF / xF;
+}
+
 static sv5 bfm_body_force(const oracle_solver* s, long i, long j, long k, sv5 W, double t) {
     long q = idx3(s, i, j, k);
     bfm_state b;
     bfm_flow_state(s, i, j, k, W, t, &b);
     double vol = s->vol[q];
     double w2 = vdot(b.relCyl, b.relCyl);
+    if (s->bfm_model == BFM_CHIMA) { /* src/source_bfm_chima.cpp:16-190 */
+        double mf = s->turbo[0];
+        double scTurn = linear_interp(s->chima_mf, s->chima_turn, s->chima_n, mf);
+        double scLoss = linear_interp(s->chima_mf, s->chima_loss, s->chima_n, mf);
+        double sLoc = s->field[F_STWL][q];
+        double sTe = s->field[F_STWL][idx3(s, s->te_idx, j, k)];
+        double dSdM = chima_derivative(s->field[F_DENTROPY][q], sLoc, sTe);
+        dSdM *= scLoss;
+        double T = f_temperature_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
+        double vmer = sqrt(b.velCyl.x * b.velCyl.x + b.velCyl.y * b.velCyl.y);
+        double fv = T * vmer / vmag(b.relCyl) * dSdM;
+        vec3 fvCyl = vmul(b.viscDirCyl, fv);
+        sv5 visc = force_source(fvCyl, &b, vol, W.v[0]);
+        double dLdM = chima_derivative(s->field[F_DANGMOM][q], sLoc, sTe);
+        dLdM *= scTurn;
+        double ftan = dLdM * vmer / b.radius;
+        double fi = (ftan - fvCyl.z) / b.invDirCyl.z;
+        sv5 inv = force_source(vmul(b.invDirCyl, fi), &b, vol, W.v[0]);
+        return sadd(inv, visc);
+    }
     if (s->bfm_model == BFM_HALL) { /* src/source_bfm_hall.cpp:3-34 */
         double fm = w2 * M_PI * b.dev / b.pitch / fabs(b.nCyl.z);
         return force_source(vmul(b.invDirCyl, fm), &b, vol, W.v[0]);
@@ -2227,6 +2322,7 @@ static int read_settings(oracle_solver* s) {
     else if (!strcmp(v, "Hall-Thollet")) s->bfm_model = BFM_THOLLET;
     else if (!strcmp(v, "Lift-Drag")) s->bfm_model = BFM_LIFT_DRAG;
     else if (!strcmp(v, "Blockage")) s->bfm_model = BFM_BLOCKAGE;
+    else if (!strcmp(v, "Chima")) s->bfm_model = BFM_CHIMA;
     else return fail("BFM_MODEL '%s' is outside the oracle's scope", v);
     if (cfg_bool(c, "STALLED_BFM_ACTIVE", 0, &s->stalled)) return 1;
     if (cfg_bool(c, "PERTURBATION_BODY_FORCE", 0, &s->perturb)) return 1;
@@ -2262,7 +2358,7 @@ static int read_settings(oracle_solver* s) {
         if (!s->has_nu) return fail("Hall-Thollet without FLUID_KINEMATIC_VISCOSITY is outside the oracle's scope");
         if (cfg_float(c, "FLUID_KINEMATIC_VISCOSITY", &s->nu)) return 1;
     }
-    if (s->bfm_model == BFM_LIFT_DRAG) {
+    if (s->bfm_model == BFM_LIFT_DRAG || s->bfm_model == BFM_CHIMA) {
         int le, te;
         double d;
         if (cfg_float(c, "LEADING_EDGE_INDEX", &d)) return 1;
@@ -2607,6 +2703,18 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
         const int need[] = {F_NAX, F_NRAD, F_NTAN, F_RPM, F_BLADE_PRESENT, F_NBLADES};
         for (unsigned q = 0; q < sizeof need / sizeof need[0]; q++)
             if (!s->field[need[q]]) { fail("%s not found in the grid file", FIELD_NAMES[need[q]]); oracle_destroy(s); return 1; }
+        if (s->bfm_model == BFM_CHIMA) {
+            const int needc[] = {F_STWL, F_DANGMOM, F_DENTROPY};
+            for (unsigned q = 0; q < 3; q++)
+                if (!s->field[needc[q]]) { fail("%s not found in the grid file", FIELD_NAMES[needc[q]]); oracle_destroy(s); return 1; }
+        }
+    }
+    if (s->bfm_model == BFM_CHIMA) { /* SourceBFMChima::SourceBFMChima (src/source_bfm_chima.cpp:3-13) */
+        const char* cf = cfg_get(&s->cfg, "CHIMA_SCALING_FUNCTIONS_FILEPATH");
+        if (!cf) { fail("Not found value for key \"CHIMA_SCALING_FUNCTIONS_FILEPATH\" in configuration."); oracle_destroy(s); return 1; }
+        dir_join(path, sizeof path, base, cf);
+        if (read_chima_table(s, path)) { oracle_destroy(s); return 1; }
+        s->need_turbo = 1; /* src/solver.cpp:1319-1321 */
     }
     const char* bcf = cfg_get(&s->cfg, "BOUNDARY_CONDITIONS_FILEPATH");
     if (!bcf) { fail("Not found value for key \"BOUNDARY_CONDITIONS_FILEPATH\" in configuration."); oracle_destroy(s); return 1; }
@@ -2676,6 +2784,7 @@ void oracle_destroy(oracle_solver* s) {
     free(s->vert); free(s->dual);
     free(s->sI); free(s->sJ); free(s->sK); free(s->cI); free(s->cJ); free(s->cK);
     free(s->vol); free(s->gradb);
+    free(s->chima_mf); free(s->chima_turn); free(s->chima_loss);
     for (int f = 0; f < F_COUNT; f++) free(s->field[f]);
     free(s->patches); free(s->mapI); free(s->mapJ); free(s->mapK);
     for (int m = 0; m < s->nprofiles; m++) { free(s->profiles[m].pressure); free(s->profiles[m].radius); }

@@ -91,6 +91,24 @@ def _co2_farfield():
     return c
 
 
+def _chima():
+    """Chima body force on the rotor row alone, with synthetic angular-momentum
+    and entropy rises and scaling functions over the mass flow."""
+    import numpy as np
+
+    c = cases.meridional(ni=24, nj=10, rows=[cases.MAP_ROWS[0]], bfm_model="Chima")
+    inside = c.fields["bladePresent"][:, 0, 0] > 0
+    idx = np.nonzero(inside)[0]
+    blade = c.fields["bladePresent"] > 0
+    c.fields["deltaAngularMomentum"] = np.where(blade, 40.0 * c.y / 0.3, 0.0)
+    c.fields["deltaEntropy"] = np.where(blade, 6.0, 0.0)
+    table = "MassFlow,PhiTurn,PhiLoss\n" + "".join(
+        f"{m!r},{t!r},{l!r}\n" for m, t, l in ((20.0, 0.8, 1.2), (40.0, 1.0, 1.0), (60.0, 1.1, 0.9), (90.0, 1.2, 0.8)))
+    c = c.with_settings(LEADING_EDGE_INDEX=str(int(idx[0])), TRAILING_EDGE_INDEX=str(int(idx[-1])),
+                        CHIMA_SCALING_FUNCTIONS_FILEPATH="chima.csv")
+    return dataclasses.replace(c, files={"chima.csv": table})
+
+
 CASES = {
     "bump_jst_rk4": (lambda: cases.bump2d(ni=24, nj=12), 20),
     "bump_roe_vanalbada_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
@@ -122,4 +140,5 @@ CASES = {
                                                         MASS_FLOW_MAX_PRESSURE_CHANGE="0.05"), 20),
     "sector45_mass_flow": (_sector_mass_flow, 10),
     "co2_bump_farfield": (_co2_farfield, 20),
+    "meridional_chima": (_chima, 20),
 }
