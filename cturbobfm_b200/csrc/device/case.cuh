@@ -189,6 +189,7 @@ struct alignas(16) DevCaseT {
     const R* bpresent;
     const R* nblades;
     const R* cosmetal;
+    const R* metal;  // Correlations: bladeMetalAngle
     const R* devpivot;
     const R* devstall;
     const R* ldbeta0;
@@ -218,5 +219,17 @@ struct alignas(16) DevCaseT {
 };
 
 using DevCase = DevCaseT<double>;
+
+// The Chima and Correlations body forces run in their own node-kernel
+// variant, so the common one carries none of their code.
+#ifdef __CUDACC__
+#define CTBFM_HD __host__ __device__
+#else
+#define CTBFM_HD
+#endif
+template <typename R>
+CTBFM_HD inline bool bfmRareModel(const DevCaseT<R>& c) {
+    return c.bfm && (c.bfm_model == 5 || c.bfm_model == 6);
+}
 
 }  // namespace ctbfm

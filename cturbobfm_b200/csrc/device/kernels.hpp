@@ -24,6 +24,8 @@ struct BatchView {
     int m = 0;
     bool ideal = true;  // some member uses the ideal gas
     bool real = false;  // some member uses the real-gas look-up tables
+    bool bfmCommon = true;  // some member uses no BFM or Hall / Hall-Thollet / Lift-Drag / blockage
+    bool bfmRare = false;   // some member uses the Chima or Correlations body force
     TileList node;        // nodes of every instance (k_prim, k_nodes, k_dt)
     // faces per direction, scheme (0 JST, 1 Roe) and face set: 0 every face
     // of the direction; for K lines of at least 3 nodes, and J lines of at

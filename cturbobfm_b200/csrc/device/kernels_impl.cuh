@@ -61,13 +61,15 @@ __device__ __forceinline__ void gridDependency() { asm volatile("griddepcontrol.
 
 template <typename R>
 __device__ __forceinline__ bool enter(const DevCaseT<R>* cases, const Tile* tiles, DevCaseT<R>& sc, int stage,
-                                      int force, Tile& t, int fluid = -1) {
+                                      int force, Tile& t, int fluid = -1, int bfmx = -1) {
     gridDependency();
     t = tiles[blockIdx.x];
     const DevCaseT<R>* g = cases + t.inst;
     // kernels compiled for one fluid model (0 ideal, 1 look-up table) take
     // only the instances of that model
     if (fluid >= 0 && (g->lut != nullptr) != (fluid != 0)) return false;
+    // node kernels compiled with (1) or without (0) the Chima / Correlations forces
+    if (bfmx >= 0 && bfmRareModel(*g) != (bfmx != 0)) return false;
     if (!force) {
         const Control* ctl = g->ctl;
         if (ctl->status != 0 || ctl->it >= ctl->it_stop) return false;
@@ -346,11 +348,11 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 // K faces, then sources), then Solver::updateSolution (src/solver.cpp:2230-2249)
 // U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
 // Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
-template <typename R, int FL>
+template <typename R, int FL, int BX>
 __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
-    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
+    if (!enter(cases, tiles, c, stage, force, tl, FL, BX)) return;
     const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const double t = c.ctl->t;
     const R dtg = R(c.ctl->dt_min);
@@ -398,7 +400,7 @@ __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevC
             }
         }
         const S5<R> Unode = load5(Uin, q);
-        applySources(c, gs, Uin, i, j, k, q, Unode, t, Res);
+        applySources<BX>(c, gs, Uin, i, j, k, q, Unode, t, Res);
         if (c.periodic && (k == 0 || k == nk - 1)) {
             const long long pq = (k == 0 ? 0 : c.n / nk) + static_cast<long long>(i) * nj + j;
             store5(c.Rp, pq, Res);
@@ -946,8 +948,10 @@ cudaError_t Launcher<R>::faces(const BatchView<R>& b, int dir, int stage, int fo
 
 template <typename R>
 cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.node.n && b.ideal) launchK(k_nodes<R, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
-    if (b.node.n && b.real) launchK(k_nodes<R, 1>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.ideal && b.bfmCommon) launchK(k_nodes<R, 0, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.real && b.bfmCommon) launchK(k_nodes<R, 1, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.ideal && b.bfmRare) launchK(k_nodes<R, 0, 1>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    if (b.node.n && b.real && b.bfmRare) launchK(k_nodes<R, 1, 1>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
     return cudaGetLastError();
 }
 

@@ -127,35 +127,125 @@ CTBFM_DI R tholletKmach(Gas<R> gs, V3<R> rel, const S5<R>& W) {
     return rmin(R(3), kp);
 }
 
+// SourceBFMChima::computeBodyForceSource (src/source_bfm_chima.cpp:16-190).
+// Not inlined, like correlationsForce: the rarely used models stay out of
+// the node kernel's registers.
+template <typename R>
+__device__ __noinline__ S5<R> chimaForce(const DevCaseT<R>& c, Gas<R> gs, int j, int k, long long q, const S5<R>& W,
+                                         const BfmState<R>& b, R vol) {
+    // SourceBFMChima::computeDerivativeFunction (:180-190): parabolic
+    auto deriv = [](R yF, R xL, R xF) { return R(-2.0) * yF * xL / (xF * xF) + R(2.0) * yF / xF; };
+    const R sLoc = c.stwl[q];
+    const R sTe = c.stwl[nodeIdx(c, c.te_idx, j, k)];
+    const V3<R> u = velOf(W);
+    // viscous component first (:146-178); its tangential force enters the inviscid one
+    const R dSdM = deriv(c.dentropy[q], sLoc, sTe) * R(c.ctl->chima_loss);
+    const R T = temperature_rho_u_et(gs, W.v[0], u, W.v[4]);
+    const R fv = T * b.vmer / mag(b.relCyl) * dSdM;
+    const V3<R> fvCyl = b.viscDirCyl * fv;
+    const S5<R> visc = forceSource(fvCyl, b, vol, W.v[0]);
+    // inviscid component (:51-83)
+    const R dLdM = deriv(c.dangmom[q], sLoc, sTe) * R(c.ctl->chima_turn);
+    const R ftan = dLdM * b.vmer / b.radius;
+    const R fi = (ftan - fvCyl.z) / b.invDirCyl.z;
+    const S5<R> inv = forceSource(b.invDirCyl * fi, b, vol, W.v[0]);
+    return inv + visc;
+}
+
+// SourceBFMCorrelations (src/source_bfm_correlations.cpp:12-236): the
+// turning force from incidence / deviation correlations evaluated between the
+// leading and trailing edge of the node's (j, k) line, on the stage state U;
+// the viscous component is zero.
+template <typename R>
+__device__ __noinline__ S5<R> correlationsForce(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int j, int k, long long q,
+                                 const S5<R>& W, const BfmState<R>& b, R vol) {
+    const long long qle = nodeIdx(c, c.le_idx, j, k), qte = nodeIdx(c, c.te_idx, j, k);
+    // computeCorrelationParameters (:33-85)
+    const R sle = c.stwl[qle], ste = c.stwl[qte];
+    const R sol = (ste - sle) / b.pitch;
+    const S5<R> Wi = primOf(load5(U, qle)), Wo = primOf(load5(U, qte));
+    const V3<R> vic = cylOfCart(velOf(Wi), b.cth, b.sth), voc = cylOfCart(velOf(Wo), b.cth, b.sth);
+    const R rIn = c.radius[qle], rOut = c.radius[qte];
+    const V3<R> relIn = vic - v3(R(0), R(0), b.omega * rIn);
+    const V3<R> relOut = voc - v3(R(0), R(0), b.omega * rOut);
+    const R vmIn = sqrt(relIn.x * relIn.x + relIn.y * relIn.y);
+    const R flowInDeg = atan2(relIn.z, vmIn) * R(180.0) / R(M_PI);
+    const R chordM = ste - sle;
+    const R camberAbs = fabs(c.metal[qte] - c.metal[qle]) * R(180) / R(M_PI);
+    // computeInviscidComponent (:88-210)
+    const R k1 = c.metal[qle] * R(180) / R(M_PI);
+    const R k2 = c.metal[qte] * R(180) / R(M_PI);
+    const R inc = flowInDeg - k1;
+    const R aAbs = fabs(flowInDeg);
+    const R n = R(0.025) * sol - R(0.06) - (pow(aAbs / R(90.0), R(1.0) + R(1.2) * sol)) / (R(1.5) + R(0.43) * sol);
+    const R p = R(0.914) + sol * sol * sol / R(160.0);
+    const R i0 = pow(aAbs, p) / (R(5.0) + R(46.0) * exp(R(-2.3) * sol)) -
+                 R(0.1) * pow(sol, R(3.0)) * exp((aAbs - R(70.0)) / R(4.0));
+    R thk = R(0);
+    for (int s = c.le_idx; s <= c.te_idx; ++s) {
+        const long long qs = nodeIdx(c, s, j, k);
+        const R pitch = R(2.0) * R(M_PI) * c.radius[qs] / c.nblades[q];
+        const R t = pitch * (R(1.0) - c.blk[qs]);
+        if (t > thk) thk = t;
+    }
+    const R tc = thk / chordM;
+    const R Kti = pow(R(10.0) * tc, R(0.28) / (R(0.1) + pow(tc, R(0.3))));
+    const R Ksh = R(0.8);
+    const R istar = Ksh * Kti * i0 + n * camberAbs;
+    const R a = soundSpeed_rho_u_et(gs, W.v[0], velOf(W), W.v[4]);
+    const R mach = mag(b.relCart) / a;
+    const R istarC = istar + R(1.3026) * mach + R(5.7380);
+    const R dev10 = R(0.01) * sol * aAbs +
+                    (R(0.74) * pow(sol, R(1.9)) + R(3.0) * sol) * pow(aAbs / R(90.0), R(1.67) + R(1.09) * sol);
+    const R Ktd = R(6.25) * tc + R(37.5) * tc * tc;
+    const R ac = R(0.3);
+    const R devStar = (R(0.92) * ac * ac + R(0.002) * fabs(k2)) / (R(1) - R(0.002) * camberAbs / sqrt(sol)) *
+                          camberAbs / sqrt(sol) +
+                      (Ksh * Ktd - R(1.0)) * dev10;
+    const R devStarC = R(-1.099379) + R(3.0186) * devStar - R(0.1988) * devStar * devStar;
+    const R ddi = (R(1.0) + (sol + R(0.25) * pow(sol, R(4.0))) * pow((aAbs / R(53.0)), R(2.5))) / exp(R(3.1) * sol);
+    const R umIn = sqrt(relIn.x * relIn.x + relIn.y * relIn.y);
+    const R umOut = sqrt(relOut.x * relOut.x + relOut.y * relOut.y);
+    const R incMag = b.omega > R(0.0) ? inc * R(-1.0) : inc;
+    const R devOut = devStarC + ddi * (incMag - istarC) + R(10.0) * (R(1.0) - umOut / umIn);
+    const R loc = (c.stwl[q] - sle) / (ste - sle);
+    const R devExpDeg = incMag + loc * (devOut - incMag);
+    const R devExp = devExpDeg * R(M_PI) / R(180.0);
+    const R uth = b.relCyl.z;
+    const R kappa = c.metal[q];
+    R Wn;
+    if (b.omega > R(0.0)) {
+        const R uexp = b.vmer * tan(-devExp + kappa);
+        Wn = uexp - uth;
+    } else {
+        const R uexp = b.vmer * tan(devExp + kappa);
+        Wn = -uexp + uth;
+    }
+    const R fn = R(c.kn) * b.vmer * Wn / (b.pitch * fabs(c.cosmetal[q]));
+    const V3<R> dirCart = cartOfCyl(b.invDirCyl, b.cth, b.sth);
+    const V3<R> fc = dirCart * fn;
+    const V3<R> fy = b.invDirCyl * fn;
+    const S5<R> inv = (s5(R(0), fc.x, fc.y, fc.z, fy.z * b.omega * b.radius) * vol) * W.v[0];
+    const R zero = R(0);
+    const S5<R> visc = (s5(R(0), zero, zero, zero, zero * b.omega * b.radius) * vol) * W.v[0];
+    return inv + visc;
+}
+
 // computeBodyForceSource of SourceBFMHall (src/source_bfm_hall.cpp:3-34),
 // SourceBFMThollet (src/source_bfm_thollet.cpp:3-138) and SourceBFMLiftDrag
 // (src/source_bfm_lift_drag.cpp:3-88).
-template <typename R>
-CTBFM_DI S5<R> bfmBodyForce(const DevCaseT<R>& c, Gas<R> gs, int i, int j, int k, long long q, const S5<R>& W,
-                            double t) {
+template <int BX, typename R>
+CTBFM_DI S5<R> bfmBodyForce(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
+                            const S5<R>& W, double t) {
     // SourceBFMBase::computeBodyForceSource: no force for "None" / "Blockage"
-    if (c.bfm_model != 1 && c.bfm_model != 2 && c.bfm_model != 3 && c.bfm_model != 5) return zero5<R>();
+    if (c.bfm_model != 1 && c.bfm_model != 2 && c.bfm_model != 3 && c.bfm_model != 5 && c.bfm_model != 6)
+        return zero5<R>();
     BfmState<R> b;
     bfmFlowState(c, q, W, t, b);
     const R vol = c.vol[q];
-    if (c.bfm_model == 5) {  // Chima (src/source_bfm_chima.cpp:16-190)
-        // SourceBFMChima::computeDerivativeFunction (:180-190): parabolic
-        auto deriv = [](R yF, R xL, R xF) { return R(-2.0) * yF * xL / (xF * xF) + R(2.0) * yF / xF; };
-        const R sLoc = c.stwl[q];
-        const R sTe = c.stwl[nodeIdx(c, c.te_idx, j, k)];
-        const V3<R> u = velOf(W);
-        // viscous component first (:146-178); its tangential force enters the inviscid one
-        const R dSdM = deriv(c.dentropy[q], sLoc, sTe) * R(c.ctl->chima_loss);
-        const R T = temperature_rho_u_et(gs, W.v[0], u, W.v[4]);
-        const R fv = T * b.vmer / mag(b.relCyl) * dSdM;
-        const V3<R> fvCyl = b.viscDirCyl * fv;
-        const S5<R> visc = forceSource(fvCyl, b, vol, W.v[0]);
-        // inviscid component (:51-83)
-        const R dLdM = deriv(c.dangmom[q], sLoc, sTe) * R(c.ctl->chima_turn);
-        const R ftan = dLdM * b.vmer / b.radius;
-        const R fi = (ftan - fvCyl.z) / b.invDirCyl.z;
-        const S5<R> inv = forceSource(b.invDirCyl * fi, b, vol, W.v[0]);
-        return inv + visc;
+    if (BX) {  // the node-kernel variant of the Chima and Correlations models
+        if (c.bfm_model == 5) return chimaForce(c, gs, j, k, q, W, b, vol);
+        return correlationsForce(c, gs, U, j, k, q, W, b, vol);
     }
     const R w2 = dot(b.relCyl, b.relCyl);
     if (c.bfm_model == 1) {  // Hall
@@ -221,9 +311,9 @@ CTBFM_DI R bfmPerturbation(const DevCaseT<R>& c, long long q, double t) {
 }
 
 // SourceBFMBase::computeTotalSource (src/source_bfm_base.cpp:25-84).
-template <typename R>
-CTBFM_DI S5<R> bfmTotalSource(const DevCaseT<R>& c, Gas<R> gs, int i, int j, int k, long long q, const S5<R>& W,
-                              double t) {
+template <int BX, typename R>
+CTBFM_DI S5<R> bfmTotalSource(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
+                              const S5<R>& W, double t) {
     S5<R> blk = zero5<R>();
     if (c.blockage) {
         const V3<R> u = velOf(W);
@@ -233,14 +323,14 @@ CTBFM_DI S5<R> bfmTotalSource(const DevCaseT<R>& c, Gas<R> gs, int i, int j, int
         blk = s5(ct, ct * u.x, ct * u.y, ct * u.z, ct * ht) * c.vol[q];
     }
     if (c.nblades[q] == R(0)) return blk;
-    const S5<R> bf = bfmBodyForce(c, gs, i, j, k, q, W, t);
+    const S5<R> bf = bfmBodyForce<BX>(c, gs, U, i, j, k, q, W, t);
     const R pf = bfmPerturbation(c, q, t);
     return blk + bf * (R(1) + pf);
 }
 
 // Solver::computeSourceResiduals (src/solver.cpp:2790-2924) applied to one
 // node's residual R.
-template <typename R>
+template <int BX, typename R>
 CTBFM_DI void applySources(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
                            const S5<R>& Unode, double t, S5<R>& Res) {
     if (c.topo == 1 && !c.bfm) return;
@@ -277,7 +367,7 @@ CTBFM_DI void applySources(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, 
     }
     if (c.bfm) {
         const V3<R> gb = v3(c.gbx[q], c.gby[q], c.gbz[q]);
-        if (mag(gb) > R(1E-10)) Res = Res - bfmTotalSource(c, gs, i, j, k, q, W, t);
+        if (mag(gb) > R(1E-10)) Res = Res - bfmTotalSource<BX>(c, gs, U, i, j, k, q, W, t);
     }
 }
 

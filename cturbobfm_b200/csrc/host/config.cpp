@@ -174,8 +174,7 @@ BfmModel Config::getBFMModel() const {
     if (v == "Blockage") return BfmModel::Blockage;
     if (v == "Lift-Drag") return BfmModel::LiftDrag;
     if (v == "Chima") return BfmModel::Chima;
-    if (v == "Correlations")
-        throw ConfigError("BFM_MODEL \"" + v + "\" is outside this library's scope");
+    if (v == "Correlations") return BfmModel::Correlations;
     throw ConfigError("Invalid value for key \"BFM_MODEL\" in configuration.");
 }
 

@@ -14,7 +14,7 @@ enum class Topology { TwoD = 0, ThreeD = 1, Axisymmetric = 2, OneD = 3 };
 enum class Scheme { JST = 0, Roe = 1 };
 enum class Limiter { None = 0, VanAlbada = 1, VanLeer = 2, MinMod = 3 };
 enum class TimeStepMethod { Local = 0, Global = 1, Fixed = 2 };
-enum class BfmModel { None = 0, Hall = 1, HallThollet = 2, LiftDrag = 3, Blockage = 4, Chima = 5 };
+enum class BfmModel { None = 0, Hall = 1, HallThollet = 2, LiftDrag = 3, Blockage = 4, Chima = 5, Correlations = 6 };
 
 class ConfigError : public std::runtime_error {
 public:

@@ -66,6 +66,8 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     view_.m = M;
     view_.ideal = view_.real = false;
     for (auto* m : members_) (m->c.lut ? view_.real : view_.ideal) = true;
+    view_.bfmCommon = view_.bfmRare = false;
+    for (auto* m : members_) (bfmRareModel(m->c) ? view_.bfmRare : view_.bfmCommon) = true;
     refresh(nullptr);
     cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");

@@ -218,4 +218,23 @@ private:
     std::vector<double> mf_, turn_, loss_;
 };
 
+// SourceBFMCorrelations (src/source_bfm_correlations.cpp:3-10,
+// include/config.hpp:345): leading / trailing edge indices and KN.
+class SourceBFMCorrelations : public SourceBFMBase {
+public:
+    explicit SourceBFMCorrelations(const Config& config)
+        : SourceBFMBase(config),
+          le_(static_cast<int>(config.parseFloat("LEADING_EDGE_INDEX"))),
+          te_(static_cast<int>(config.parseFloat("TRAILING_EDGE_INDEX"))) {}
+    BfmModel model() const override { return BfmModel::Correlations; }
+    void configure(DevCase& c) const override {
+        SourceBFMBase::configure(c);
+        c.le_idx = le_;
+        c.te_idx = te_;
+    }
+
+private:
+    int le_, te_;
+};
+
 }  // namespace ctbfm

@@ -173,6 +173,7 @@ void Solver::setupModels() {
         case BfmModel::HallThollet: bfm_ = std::make_unique<SourceBFMThollet>(config_); break;
         case BfmModel::LiftDrag: bfm_ = std::make_unique<SourceBFMLiftDrag>(config_); break;
         case BfmModel::Chima: bfm_ = std::make_unique<SourceBFMChima>(config_); break;
+        case BfmModel::Correlations: bfm_ = std::make_unique<SourceBFMCorrelations>(config_); break;
         default: bfm_ = std::make_unique<SourceBFMBase>(config_); break;
     }
 }
@@ -505,7 +506,9 @@ void Solver::setupScalars() {
         c.pert_t0 = config_.parseFloat("PERTURBATION_TIME_START");
         c.pert_dur = config_.parseFloat("PERTURBATION_TIME_DURATION");
     }
-    if (c.bfm && (c.bfm_model == 3 || c.bfm_model == 5)) {
+    if (c.bfm && c.bfm_model == 6)  // Config::getKnCorrelationBfmCoefficient (include/config.hpp:345)
+        c.kn = config_.parseFloat("KN_CORRELATION_BFM_COEFFICIENT");
+    if (c.bfm && (c.bfm_model == 3 || c.bfm_model == 5 || c.bfm_model == 6)) {
         if (c.le_idx < 0 || c.le_idx >= NI || c.te_idx < 0 || c.te_idx >= NI)
             throw ConfigError("LEADING_EDGE_INDEX / TRAILING_EDGE_INDEX outside the grid");
     }
@@ -630,6 +633,7 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
     c.blk = c.gbx = c.gby = c.gbz = c.nax = c.nrad = c.ntan = c.rpm = c.stwl = c.bpresent = c.nblades = nullptr;
     c.cosmetal = c.devpivot = c.devstall = c.ldbeta0 = c.ldkp = c.dangmom = c.dentropy = nullptr;
     c.chima_mf = c.chima_turn = c.chima_loss = nullptr;
+    c.metal = nullptr;
     c.chima_n = 0;
     if (c.bfm) {
         auto need = [&](const char* name) { return inst.uploadR(mesh_.field(name)); };
@@ -664,7 +668,12 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         } else {
             c.rpm = opt("rpm");
         }
-        if (c.bfm_model == 2 || c.bfm_model == 3 || c.bfm_model == 5) c.stwl = need("streamwiseLength");
+        if (c.bfm_model == 2 || c.bfm_model == 3 || c.bfm_model == 5 || c.bfm_model == 6)
+            c.stwl = need("streamwiseLength");
+        if (c.bfm_model == 6) {  // SourceBFMCorrelations reads the metal angle and the camber curvature
+            c.metal = need("bladeMetalAngle");
+            mesh_.field("bladeCamberCurvature");
+        }
         if (c.bfm_model == 5) {  // SourceBFMChima::computeInviscid/ViscousComponent
             c.dangmom = need("deltaAngularMomentum");
             c.dentropy = need("deltaEntropy");

@@ -208,7 +208,7 @@ enum { TOPO_2D = 0, TOPO_3D = 1, TOPO_AXI = 2, TOPO_1D = 3 };
 enum { SCHEME_JST = 0, SCHEME_ROE = 1 };
 enum { LIM_NONE = 0, LIM_VAN_ALBADA, LIM_VAN_LEER, LIM_MIN_MOD };
 enum { DT_LOCAL = 0, DT_GLOBAL, DT_FIXED };
-enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE, BFM_CHIMA };
+enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE, BFM_CHIMA, BFM_CORRELATIONS };
 /* BoundaryType (include/types.hpp:178-194), restricted to the types on the path. */
 enum {
     BC_INLET = 0, BC_OUTLET, BC_RADIAL_EQ, BC_INVISCID_WALL, BC_WEDGE, BC_PERIODIC, BC_THROTTLE,
@@ -237,13 +237,13 @@ typedef struct {
 
 enum {
     F_BLOCKAGE = 0, F_NAX, F_NRAD, F_NTAN, F_RPM, F_STWL, F_BLADE_PRESENT, F_NBLADES, F_METAL,
-    F_GASPATH, F_LEAN, F_DEV_PIVOT, F_DEV_STALL, F_LD_BETA0, F_LD_KP, F_DANGMOM, F_DENTROPY, F_COUNT
+    F_GASPATH, F_LEAN, F_DEV_PIVOT, F_DEV_STALL, F_LD_BETA0, F_LD_KP, F_DANGMOM, F_DENTROPY, F_CAMBER_CURV, F_COUNT
 };
 static const char* FIELD_NAMES[F_COUNT] = {
     "blockage", "normalAxial", "normalRadial", "normalTangential", "rpm", "streamwiseLength",
     "bladePresent", "numberBlades", "bladeMetalAngle", "bladeGasPathAngle", "bladeLeanAngle",
     "deviationAnglePivot", "deviationAngleStall", "liftDragBeta0", "liftDragKpEtamax",
-    "deltaAngularMomentum", "deltaEntropy"};
+    "deltaAngularMomentum", "deltaEntropy", "bladeCamberCurvature"};
 
 struct oracle_solver {
     config cfg;
@@ -1308,6 +1308,71 @@ static int read_chima_table(oracle_solver* s, const char* path) {
     return 0;
 }
 
+/* SourceBFMCorrelations::computeCorrelationParameters and
+ * computeInviscidComponent (src/source_bfm_correlations.cpp:33-210); the
+ * viscous component is zero (:213-236). */
+static sv5 correlations_force(const oracle_solver* s, double* const* U, long j, long k, long q, sv5 W,
+                              const bfm_state* b, double vol) {
+    long qle = idx3(s, s->le_idx, j, k), qte = idx3(s, s->te_idx, j, k);
+    const double* stwl = s->field[F_STWL];
+    const double* metal = s->field[F_METAL];
+    double sol = (stwl[qte] - stwl[qle]) / b->pitch;
+    sv5 Wi = prim_of(state_at(s, U, s->le_idx, j, k)), Wo = prim_of(state_at(s, U, s->te_idx, j, k));
+    vec3 vic = cyl_of_cart(vel_of(Wi), b->theta), voc = cyl_of_cart(vel_of(Wo), b->theta);
+    double rIn = node_radius(s, s->le_idx, j, k), rOut = node_radius(s, s->te_idx, j, k);
+    vec3 relIn = vsub(vic, v3(0.0, 0.0, b->omega * rIn));
+    vec3 relOut = vsub(voc, v3(0.0, 0.0, b->omega * rOut));
+    double vmIn = sqrt(relIn.x * relIn.x + relIn.y * relIn.y);
+    double flowInDeg = atan2(relIn.z, vmIn) * 180.0 / M_PI;
+    double chordM = stwl[qte] - stwl[qle];
+    double camberAbs = fabs(metal[qte] - metal[qle]) * 180 / M_PI;
+    double k1 = metal[qle] * 180 / M_PI, k2 = metal[qte] * 180 / M_PI;
+    double inc = flowInDeg - k1;
+    double aAbs = fabs(flowInDeg);
+    double n = 0.025 * sol - 0.06 - (pow(aAbs / 90.0, 1.0 + 1.2 * sol)) / (1.5 + 0.43 * sol);
+    double p = 0.914 + sol * sol * sol / 160.0;
+    double i0 = pow(aAbs, p) / (5.0 + 46.0 * exp(-2.3 * sol)) - 0.1 * pow(sol, 3.0) * exp((aAbs - 70.0) / 4.0);
+    double thk = 0.0;
+    for (long st = s->le_idx; st <= s->te_idx; ++st) {
+        double r = node_radius(s, st, j, k);
+        double pitch = 2.0 * M_PI * r / b->nblades;
+        double t = pitch * (1.0 - s->field[F_BLOCKAGE][idx3(s, st, j, k)]);
+        if (t > thk) thk = t;
+    }
+    double tc = thk / chordM;
+    double Kti = pow(10.0 * tc, 0.28 / (0.1 + pow(tc, 0.3)));
+    double Ksh = 0.8;
+    double istar = Ksh * Kti * i0 + n * camberAbs;
+    double a = f_sound_speed_rho_u_et(s, W.v[0], vel_of(W), W.v[4]);
+    double mach = vmag(b->relCart) / a;
+    double istarC = istar + 1.3026 * mach + 5.7380;
+    double dev10 = 0.01 * sol * aAbs + (0.74 * pow(sol, 1.9) + 3.0 * sol) * pow(aAbs / 90.0, 1.67 + 1.09 * sol);
+    double Ktd = 6.25 * tc + 37.5 * tc * tc;
+    double ac = 0.3;
+    double devStar = (0.92 * ac * ac + 0.002 * fabs(k2)) / (1 - 0.002 * camberAbs / sqrt(sol)) * camberAbs / sqrt(sol) +
+                     (Ksh * Ktd - 1.0) * dev10;
+    double devStarC = -1.099379 + 3.0186 * devStar - 0.1988 * devStar * devStar;
+    double ddi = (1.0 + (sol + 0.25 * pow(sol, 4.0)) * pow((aAbs / 53.0), 2.5)) / exp(3.1 * sol);
+    double umIn = sqrt(relIn.x * relIn.x + relIn.y * relIn.y);
+    double umOut = sqrt(relOut.x * relOut.x + relOut.y * relOut.y);
+    double incMag = b->omega > 0.0 ? inc * (-1.0) : inc;
+    double devOut = devStarC + ddi * (incMag - istarC) + 10.0 * (1.0 - umOut / umIn);
+    double loc = (stwl[q] - stwl[qle]) / (stwl[qte] - stwl[qle]);
+    double devExpDeg = incMag + loc * (devOut - incMag);
+    double devExp = devExpDeg * M_PI / 180.0;
+    double uth = b->relCyl.z, kappa = metal[q];
+    double vmer = sqrt(b->velCyl.x * b->velCyl.x + b->velCyl.y * b->velCyl.y);
+    double Wn;
+    if (b->omega > 0.0) Wn = vmer * tan(-devExp + kappa) - uth;
+    else Wn = -(vmer * tan(devExp + kappa)) + uth;
+    double fn = s->kn * vmer * Wn / (b->pitch * fabs(cos(metal[q])));
+    vec3 dirCart = cart_of_cyl(b->invDirCyl, b->theta);
+    vec3 fc = vmul(dirCart, fn), fy = vmul(b->invDirCyl, fn);
+    sv5 inv = {{0.0, fc.x, fc.y, fc.z, fy.z * b->omega * b->radius}};
+    sv5 visc = {{0.0, 0.0, 0.0, 0.0, 0.0 * b->omega * b->radius}};
+    return sadd(smul(smul(inv, vol), W.v[0]), smul(smul(visc, vol), W.v[0]));
+}
+
 /* linearInterpolation (src/math_utils.cpp:487-514). */
 static double linear_interp(const double* x, const double* y, int n, double xp) {
     if (xp <= x[0]) return y[0];
@@ -1323,12 +1388,13 @@ static double chima_derivative(double yF, double xL, double xF) {
     return -2.0 * yF * xL / (xF * xF) + 2.0 * yF / xF;
 }
 
-static sv5 bfm_body_force(const oracle_solver* s, long i, long j, long k, sv5 W, double t) {
+static sv5 bfm_body_force(const oracle_solver* s, double* const* U, long i, long j, long k, sv5 W, double t) {
     long q = idx3(s, i, j, k);
     bfm_state b;
     bfm_flow_state(s, i, j, k, W, t, &b);
     double vol = s->vol[q];
     double w2 = vdot(b.relCyl, b.relCyl);
+    if (s->bfm_model == BFM_CORRELATIONS) return correlations_force(s, U, j, k, q, W, &b, vol);
     if (s->bfm_model == BFM_CHIMA) { /* src/source_bfm_chima.cpp:16-190 */
         double mf = s->turbo[0];
         double scTurn = linear_interp(s->chima_mf, s->chima_turn, s->chima_n, mf);
@@ -1416,7 +1482,7 @@ static double bfm_perturbation(const oracle_solver* s, long i, long j, long k, d
 }
 
 /* SourceBFMBase::computeTotalSource (src/source_bfm_base.cpp:25-84). */
-static sv5 bfm_total_source(const oracle_solver* s, long i, long j, long k, sv5 W, double t) {
+static sv5 bfm_total_source(const oracle_solver* s, double* const* U, long i, long j, long k, sv5 W, double t) {
     long q = idx3(s, i, j, k);
     sv5 blk = szero();
     if (s->blockage_active) {
@@ -1430,7 +1496,7 @@ static sv5 bfm_total_source(const oracle_solver* s, long i, long j, long k, sv5 
         blk = smul(src, vol);
     }
     if (s->field[F_NBLADES][q] == 0) return blk;
-    sv5 bf = bfm_body_force(s, i, j, k, W, t);
+    sv5 bf = bfm_body_force(s, U, i, j, k, W, t);
     double pf = bfm_perturbation(s, i, j, k, t);
     return sadd(blk, smul(bf, 1.0 + pf));
 }
@@ -1480,7 +1546,7 @@ static void source_residuals(oracle_solver* s, double* const* U) {
                     res_sub(s, i, j, k, gong_source(s, U, om, i, j, k, vol));
                 }
                 if (s->bfm_active) {
-                    if (vmag(s->gradb[q]) > 1E-10) res_sub(s, i, j, k, bfm_total_source(s, i, j, k, W, s->t));
+                    if (vmag(s->gradb[q]) > 1E-10) res_sub(s, i, j, k, bfm_total_source(s, U, i, j, k, W, s->t));
                 }
             }
 }
@@ -2323,6 +2389,7 @@ static int read_settings(oracle_solver* s) {
     else if (!strcmp(v, "Lift-Drag")) s->bfm_model = BFM_LIFT_DRAG;
     else if (!strcmp(v, "Blockage")) s->bfm_model = BFM_BLOCKAGE;
     else if (!strcmp(v, "Chima")) s->bfm_model = BFM_CHIMA;
+    else if (!strcmp(v, "Correlations")) s->bfm_model = BFM_CORRELATIONS;
     else return fail("BFM_MODEL '%s' is outside the oracle's scope", v);
     if (cfg_bool(c, "STALLED_BFM_ACTIVE", 0, &s->stalled)) return 1;
     if (cfg_bool(c, "PERTURBATION_BODY_FORCE", 0, &s->perturb)) return 1;
@@ -2358,7 +2425,8 @@ static int read_settings(oracle_solver* s) {
         if (!s->has_nu) return fail("Hall-Thollet without FLUID_KINEMATIC_VISCOSITY is outside the oracle's scope");
         if (cfg_float(c, "FLUID_KINEMATIC_VISCOSITY", &s->nu)) return 1;
     }
-    if (s->bfm_model == BFM_LIFT_DRAG || s->bfm_model == BFM_CHIMA) {
+    if (s->bfm_model == BFM_CORRELATIONS && cfg_float(c, "KN_CORRELATION_BFM_COEFFICIENT", &s->kn)) return 1;
+    if (s->bfm_model == BFM_LIFT_DRAG || s->bfm_model == BFM_CHIMA || s->bfm_model == BFM_CORRELATIONS) {
         int le, te;
         double d;
         if (cfg_float(c, "LEADING_EDGE_INDEX", &d)) return 1;
@@ -2703,6 +2771,11 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
         const int need[] = {F_NAX, F_NRAD, F_NTAN, F_RPM, F_BLADE_PRESENT, F_NBLADES};
         for (unsigned q = 0; q < sizeof need / sizeof need[0]; q++)
             if (!s->field[need[q]]) { fail("%s not found in the grid file", FIELD_NAMES[need[q]]); oracle_destroy(s); return 1; }
+        if (s->bfm_model == BFM_CORRELATIONS) {
+            const int needc[] = {F_STWL, F_METAL, F_CAMBER_CURV};
+            for (unsigned q = 0; q < 3; q++)
+                if (!s->field[needc[q]]) { fail("%s not found in the grid file", FIELD_NAMES[needc[q]]); oracle_destroy(s); return 1; }
+        }
         if (s->bfm_model == BFM_CHIMA) {
             const int needc[] = {F_STWL, F_DANGMOM, F_DENTROPY};
             for (unsigned q = 0; q < 3; q++)

@@ -109,6 +109,17 @@ def _chima():
     return dataclasses.replace(c, files={"chima.csv": table})
 
 
+def _correlations():
+    """Correlations body force on the rotor row alone."""
+    import numpy as np
+
+    c = cases.meridional(ni=24, nj=10, rows=[cases.MAP_ROWS[0]], bfm_model="Correlations")
+    idx = np.nonzero(c.fields["bladePresent"][:, 0, 0] > 0)[0]
+    c.fields["bladeCamberCurvature"] = np.full_like(c.x, 2.0)
+    return c.with_settings(LEADING_EDGE_INDEX=str(int(idx[0])), TRAILING_EDGE_INDEX=str(int(idx[-1])),
+                           KN_CORRELATION_BFM_COEFFICIENT="0.8")
+
+
 CASES = {
     "bump_jst_rk4": (lambda: cases.bump2d(ni=24, nj=12), 20),
     "bump_roe_vanalbada_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
@@ -141,4 +152,5 @@ CASES = {
     "sector45_mass_flow": (_sector_mass_flow, 10),
     "co2_bump_farfield": (_co2_farfield, 20),
     "meridional_chima": (_chima, 20),
+    "meridional_correlations": (_correlations, 20),
 }

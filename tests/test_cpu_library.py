@@ -56,7 +56,7 @@ def test_missing_input_file_is_a_config_error(lib, tmp_path):
     ("FLUX_LIMITER", "vanalbada", "Invalid value for key \"FLUX_LIMITER\""),
     ("TIME_INTEGRATION_TYPE", "2", "Implicit time integration"),
     ("TIME_STEP_METHOD", "adaptive", "Invalid value for key \"TIME_STEP_METHOD\""),
-    ("BFM_MODEL", "Correlations", "outside this library's scope"),
+    ("BFM_MODEL", "Correlations", "Not found value for key \"LEADING_EDGE_INDEX\""),
     ("BFM_MODEL", "Chima", "Not found value for key \"CHIMA_SCALING_FUNCTIONS_FILEPATH\""),
     ("INIT_DIRECTION", "1, 0", "INIT_DIRECTION must have 3 components"),
     ("ENABLE_GREITZER_MODELING", "yes", "Greitzer modeling is only compatible with fixed time step method"),
