@@ -32,8 +32,11 @@ int boundaryTypeFromString(std::string s) {  // include/types.hpp:202-232, path 
     if (s == "mass_flow" || s == "outlet_mass_flow" || s == "massflow" || s == "mass_flow_rate") return kBcMassFlow;
     if (s == "transparent") return kBcTransparent;
     if (s == "farfield") return kBcFarfield;
-    if (s == "inlet_2d" || s == "no_slip_wall")
-        throw ConfigError("BoundaryType " + s + " is outside this library's scope");
+    // the reference never assigns the 2-D inlet file's path (Solver::_inlet2DfilePath
+    // stays empty, include/solver.hpp:345), so its inlet_2d cannot run
+    if (s == "inlet_2d")
+        throw ConfigError("BoundaryType inlet_2d: the reference reads its 2-D inlet file from an empty path; not supported");
+    if (s == "no_slip_wall") throw ConfigError("BoundaryType no_slip_wall belongs to the viscous path, outside this library's scope");
     throw ConfigError("Unknown BoundaryType: " + s);
 }
 
@@ -391,7 +394,7 @@ void Solver::buildBoundaryStructures() {
     std::string dir = config_.has("TURBO_DIRECTION") ? config_.get("TURBO_DIRECTION") : "i";
     if (!config_.has("TURBO_DIRECTION"))
         for (const auto& b : boundaries_)
-            if (b.type == kBcInlet) {
+            if (b.type == kBcInlet || b.type == kBcInletSupersonic) {
                 if (b.orientation == 2) { dir = "j"; break; }
                 if (b.orientation == 3) { dir = "-j"; break; }
             }

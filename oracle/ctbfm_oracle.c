@@ -2455,7 +2455,7 @@ static void resolve_turbo_dir(oracle_solver* s) {
     const char* d = v ? v : "i";
     if (!v) {
         for (int m = 0; m < s->npatches; m++)
-            if (s->patches[m].type == BC_INLET) {
+            if (s->patches[m].type == BC_INLET || s->patches[m].type == BC_INLET_SUPERSONIC) {
                 if (s->patches[m].orientation == BI_JSTART) { d = "j"; break; }
                 if (s->patches[m].orientation == BI_JEND) { d = "-j"; break; }
             }
