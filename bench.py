@@ -682,6 +682,23 @@ SERVE_WORKLOAD = ("serving: Poisson arrivals, 70% axisymmetric compressor-map re
                   "(float solves move to FP64 only with --serve-stall-window > 0)")
 
 
+def warm_start_solution(root):
+    """The converged nominal operating point of the serving mix (the map stage
+    on a 128 x 48 meridional grid, p_out/pt_in 1.10, speed 0.925, FP64), as a
+    volume CSV for the requests' restarts. Solved before the timed region."""
+    from cturbobfm_b200 import Solver, cases
+
+    c = cases.meridional(ni=128, nj=48, p_ratio=1.10, speed=0.925, cfl=2.2, drop=3, rows=cases.MAP_ROWS,
+                         ramp=2000, n_iter=40000, name="nominal")
+    d = os.path.join(root, "nominal")
+    t0 = time.perf_counter()
+    with Solver(c.write(d)) as s:
+        s.solve()
+        status, its = s.status, s.iteration
+        path = s.write_solution(os.path.join(d, "nominal.csv"))
+    return {"path": path, "status": status, "iterations": its, "seconds": time.perf_counter() - t0}
+
+
 def run_serve(args):
     import numpy as np
     import torch
@@ -692,6 +709,9 @@ def run_serve(args):
     torch.cuda.set_device(local)
     tmp = tempfile.TemporaryDirectory()
     per_rate = {}
+    warm = None
+    if args.serve_warm:
+        warm = warm_start_solution(tmp.name)
     with ClockSampler(local) as clocks:
         for rate in args.serve_rates:
             reqs = cases.serving_requests(args.serve_n, rate)
@@ -699,6 +719,12 @@ def run_serve(args):
             for t, c in reqs:
                 d = os.path.join(tmp.name, f"r{rate}", c.name)
                 os.makedirs(d)
+                if warm:
+                    # start from the converged nominal operating point, mapped onto the
+                    # request's grid by the reference's nearest-neighbour restart
+                    c = c.with_settings(RESTART_SOLUTION="yes", RESTART_SOLUTION_FILEPATH=warm["path"],
+                                        RESTART_TYPE="nearest_neighbor_axisymmetric",
+                                        OUTLET_PRESSURE_RAMP_ITERATIONS="0")
                 kind = "3d" if c.shape[2] > 1 else ("throttle" if "ENABLE_GREITZER_MODELING" in c.settings else "axisymmetric")
                 inis.append((t, c.write(d), c.n_nodes, c.shape[2] > 1, kind))
             res = {}
@@ -752,6 +778,11 @@ def run_serve(args):
         "config": {"workload": SERVE_WORKLOAD, "rates_per_s": args.serve_rates, "requests_per_rate": args.serve_n,
                    "chunk_iterations": args.serve_chunk, "max_active_nodes": args.serve_max_nodes,
                    "stall_window": args.serve_stall_window,
+                   "warm_start": (None if not warm else
+                                  {"from": "converged nominal point, 128x48 meridional, p_out/pt_in 1.10, speed 0.925",
+                                   "restart_type": "nearest_neighbor_axisymmetric", "outlet_ramp": 0,
+                                   "nominal_iterations": warm["iterations"], "nominal_status": warm["status"],
+                                   "nominal_seconds_untimed": warm["seconds"]}),
                    "clock": "host wall clock from submit to retirement"},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "per_rate": per_rate,
@@ -785,6 +816,8 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[5.0, 20.0, 80.0])
     ap.add_argument("--serve-n", type=int, default=48)
     ap.add_argument("--serve-chunk", type=int, default=100)
+    ap.add_argument("--serve-warm", action="store_true",
+                    help="serve: every request restarts from one converged nominal operating point")
     ap.add_argument("--serve-stall-window", type=int, default=0,
                     help="serve: > 0 lets the server move stalled float solves to FP64 and re-run diverged ones in FP64")
     ap.add_argument("--serve-max-nodes", type=int, default=1500000,
