@@ -158,3 +158,44 @@ def test_diverged_fp32_solve_is_run_again_in_fp64(tmp_path):
     assert r["iterations"] == it64
     assert np.array_equal(np.array(r["turbo"]), tp64)
     assert np.array_equal(np.array(r["massflow"]), mf64)
+
+
+def test_warm_started_request_is_the_same_alone_and_in_the_mix(tmp_path):
+    """A request that restarts from another operating point's converged
+    solution (RESTART_SOLUTION, nearest-neighbour mapping onto its own grid)
+    converges faster than cold and gives the same result alone, in a mix, and
+    on the plain drop-in path."""
+    from cturbobfm_b200 import Server, Solver
+
+    nominal = _req("n", 64, 24, 1.1, 0.95, prec="fp64")
+    with Solver(_write(nominal, str(tmp_path))) as s:
+        s.solve()
+        assert s.status == 1
+        csv = s.write_solution(str(tmp_path / "nominal.csv"))
+    cold = _req("w", 80, 28, 1.05, 0.95)
+    warm = cold.with_settings(RESTART_SOLUTION="yes", RESTART_SOLUTION_FILEPATH=csv,
+                              RESTART_TYPE="nearest_neighbor_axisymmetric", OUTLET_PRESSURE_RAMP_ITERATIONS="0")
+    ini_cold = _write(cold, str(tmp_path / "cold"))
+    ini = _write(warm, str(tmp_path / "warm"))
+    with Solver(ini_cold) as p:
+        p.solve()
+        cold_its = p.iteration
+    with Solver(ini) as p:
+        p.solve()
+        assert p.status == 1
+        plain = (p.iteration, list(p.turbo()[1]))
+    assert plain[0] < cold_its
+    with Server(chunk=100) as s:
+        rid = s.submit(ini)
+        alone = _drain(s, 1)[rid]
+    other = _write(_req("o", 96, 32, 1.1, 0.9), str(tmp_path))
+    with Server(chunk=100) as s:
+        first = s.submit(other)
+        s.pump()
+        rid = s.submit(ini)
+        mixed = _drain(s, 2)[rid]
+    for r in (alone, mixed):
+        assert r["status"] == 1
+        assert r["iterations"] == plain[0]
+        assert r["turbo"] == plain[1]
+    assert first >= 0
