@@ -212,7 +212,8 @@ enum { BFM_NONE = 0, BFM_HALL, BFM_THOLLET, BFM_LIFT_DRAG, BFM_BLOCKAGE, BFM_CHI
 /* BoundaryType (include/types.hpp:178-194), restricted to the types on the path. */
 enum {
     BC_INLET = 0, BC_OUTLET, BC_RADIAL_EQ, BC_INVISCID_WALL, BC_WEDGE, BC_PERIODIC, BC_THROTTLE,
-    BC_EMPTY, BC_INLET_SUPERSONIC, BC_OUTLET_SUPERSONIC, BC_MASS_FLOW, BC_TRANSPARENT, BC_FARFIELD
+    BC_EMPTY, BC_INLET_SUPERSONIC, BC_OUTLET_SUPERSONIC, BC_MASS_FLOW, BC_TRANSPARENT, BC_FARFIELD,
+    BC_NO_SLIP_WALL
 };
 enum { BI_ISTART = 0, BI_IEND, BI_JSTART, BI_JEND, BI_KSTART, BI_KEND };
 
@@ -290,6 +291,14 @@ struct oracle_solver {
     radial_profile* profiles;
     int nprofiles;
     double hub_p;
+    /* VISCOSITY_ACTIVE: laminar transport (constant or Sutherland viscosity,
+     * conductivity cp mu / Pr), stationary no-slip walls, Green-Gauss
+     * gradients of u, v, w and T per node */
+    int viscous, visc_const;
+    double mu_const, suth_mu, suth_T, suth_S, vcp, vpr;
+    unsigned char* wall;
+    vec3* grad[4];
+    double* gfield[4];
     /* state */
     double *U[5], *Utmp[5], *R[5], *dt;
     double t;
@@ -1044,9 +1053,28 @@ static sv5 bc_farfield(const oracle_solver* s, const patch* pt, sv5 Uint, vec3 S
     return adv_flux(s, Wb, S);
 }
 
+/* BoundaryBase::isNodeOnNoSlipWall (include/boundary_base.hpp:44-49): the
+ * boundary face's own indices read as node indices, so the end faces of a
+ * direction (index n) never count. */
+static int node_on_wall(const oracle_solver* s, long i, long j, long k) {
+    if (!s->viscous || !s->wall) return 0;
+    if (i >= s->ni || j >= s->nj || k >= s->nk) return 0;
+    return s->wall[idx3(s, i, j, k)] != 0;
+}
+
+/* BoundaryBase::computeStagnationWallFlux (src/boundary_base.cpp:126-178) for
+ * a wall at rest: the boundary pressure is the patch's first value. */
+static sv5 stagnation_wall_flux(double pB, vec3 S) {
+    vec3 n = vdiv(S, vmag(S));
+    sv5 F = {{0.0, pB * n.x, pB * n.y, pB * n.z, 0.0}};
+    return F;
+}
+
 static sv5 boundary_flux(oracle_solver* s, int pidx, sv5 Uint, vec3 S, long fi, long fj, long fk,
                          long it) {
     const patch* p = &s->patches[pidx];
+    if ((p->type == BC_INLET || p->type == BC_INLET_SUPERSONIC) && node_on_wall(s, fi, fj, fk))
+        return stagnation_wall_flux(p->values[0], S);
     switch (p->type) {
         case BC_INLET: return bc_inlet(s, p, Uint, S, fi, fj, fk);
         case BC_OUTLET: return bc_outlet(s, Uint, S, p->values[0], it);
@@ -1064,7 +1092,8 @@ static sv5 boundary_flux(oracle_solver* s, int pidx, sv5 Uint, vec3 S, long fi, 
         case BC_RADIAL_EQ:
         case BC_THROTTLE: /* src/boundary_outlet_throttle.cpp:5-16, radial_equilibrium.cpp:5-16 */
             return bc_outlet(s, Uint, S, s->profiles[p->profile].pressure[fj], it);
-        case BC_INVISCID_WALL: return bc_wall(s, Uint, S);
+        case BC_INVISCID_WALL:
+        case BC_NO_SLIP_WALL: return bc_wall(s, Uint, S); /* src/solver.cpp:393-398 */
         default: return szero(); /* BoundaryFake (src/boundary_fake.cpp:4-13) */
     }
 }
@@ -1564,14 +1593,153 @@ static void periodic_residuals(oracle_solver* s) {
         }
 }
 
+/* ------------------------------------------------------- viscous path */
+
+/* FluidIdeal::computeMolecularDynamicViscosity (src/fluid_ideal.cpp:224-231);
+ * FluidReal's (src/fluid_real.cpp:387-393) is a constant in both models. */
+static double f_mu(const oracle_solver* s, double T) {
+    if (s->visc_const) return s->mu_const;
+    return s->suth_mu * pow(T / s->suth_T, 1.5) * ((s->suth_T + s->suth_S) / (T + s->suth_S));
+}
+
+/* Solver::computeSolutionGradient (src/solver.cpp:3033-3058): node
+ * temperature of FluidIdeal::computeTemperature_conservative
+ * (src/fluid_ideal.cpp:198-207) or FluidBase's (include/fluid_base.hpp:163-177),
+ * then computeGradientsGreenGauss4 (src/math_utils.cpp:237-392): face values
+ * interpolated by the distances of the face centre to the two nodes, the
+ * node value on boundary faces, summed W, E, N, S, B, T and scaled by 1/V. */
+static void solution_gradient(oracle_solver* s, double* const* U) {
+    if (!s->viscous) return;
+    for (long q = 0; q < s->n; q++) {
+        double rho = U[0][q];
+        double ux = U[1][q] / rho, uy = U[2][q] / rho, uz = U[3][q] / rho, et = U[4][q] / rho;
+        double T;
+        if (s->real) {
+            double e = et - 0.5 * (ux * ux + uy * uy + uz * uz);
+            T = table_interp(&s->lut->T, rho, e);
+        } else {
+            T = (et - (ux * ux + uy * uy + uz * uz) * 0.5) * ((s->gamma - 1.0) / s->rgas);
+        }
+        s->gfield[0][q] = ux;
+        s->gfield[1][q] = uy;
+        s->gfield[2][q] = uz;
+        s->gfield[3][q] = T;
+    }
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                long q = idx3(s, i, j, k);
+                vec3 p0 = s->vert[q];
+                long nb[6];
+                vec3 mid[6];
+                int has[6];
+                has[0] = i > 0;          nb[0] = has[0] ? idx3(s, i - 1, j, k) : q; mid[0] = s->cI[sIi(s, i, j, k)];
+                has[1] = i < s->ni - 1;  nb[1] = has[1] ? idx3(s, i + 1, j, k) : q; mid[1] = has[1] ? s->cI[sIi(s, i + 1, j, k)] : p0;
+                has[2] = j < s->nj - 1;  nb[2] = has[2] ? idx3(s, i, j + 1, k) : q; mid[2] = has[2] ? s->cJ[sJi(s, i, j + 1, k)] : p0;
+                has[3] = j > 0;          nb[3] = has[3] ? idx3(s, i, j - 1, k) : q; mid[3] = s->cJ[sJi(s, i, j, k)];
+                has[4] = k > 0;          nb[4] = has[4] ? idx3(s, i, j, k - 1) : q; mid[4] = s->cK[sKi(s, i, j, k)];
+                has[5] = k < s->nk - 1;  nb[5] = has[5] ? idx3(s, i, j, k + 1) : q; mid[5] = has[5] ? s->cK[sKi(s, i, j, k + 1)] : p0;
+                vec3 sf[6] = {vneg(s->sI[sIi(s, i, j, k)]), s->sI[sIi(s, i + 1, j, k)], s->sJ[sJi(s, i, j + 1, k)],
+                              vneg(s->sJ[sJi(s, i, j, k)]), vneg(s->sK[sKi(s, i, j, k)]), s->sK[sKi(s, i, j, k + 1)]};
+                for (int v = 0; v < 4; v++) {
+                    double fc = s->gfield[v][q];
+                    vec3 g = v3(0.0, 0.0, 0.0);
+                    for (int f = 0; f < 6; f++) {
+                        double sv = fc;
+                        if (has[f]) {
+                            double d0 = vmag(vsub(mid[f], p0));
+                            double d1 = vmag(vsub(mid[f], s->vert[nb[f]]));
+                            double w = d0 / (d0 + d1);
+                            sv = fc + (s->gfield[v][nb[f]] - fc) * w;
+                        }
+                        g = vadd(g, vmul(sf[f], sv));
+                    }
+                    double inv = 1.0 / s->vol[q];
+                    s->grad[v][q] = vmul(g, inv);
+                }
+            }
+}
+
+/* Solver::computeViscousFlux (src/solver.cpp:2174-2226) with
+ * computeViscousStressTensor (src/math_utils.cpp:593-608); laminar, so the
+ * eddy viscosity and conductivity of TurbulenceModelNone are 0. */
+static sv5 viscous_flux(const oracle_solver* s, sv5 Uc, vec3 gu, vec3 gv, vec3 gw, vec3 gT, vec3 S,
+                        double muEddy) {
+    sv5 W = prim_of(Uc);
+    vec3 vel = vel_of(W);
+    double T = f_temperature_rho_u_et(s, W.v[0], vel, W.v[4]);
+    double muL = f_mu(s, T);
+    double kappaL = s->vcp * muL / s->vpr;
+    double kappaEddy = 0.0;
+    double muT = muL + muEddy;
+    double kT = kappaL + kappaEddy;
+    double lam = -2.0 / 3.0 * muT;
+    double xx = lam * (gu.x + gv.y + gw.z) + 2.0 * muT * gu.x;
+    double yy = lam * (gu.x + gv.y + gw.z) + 2.0 * muT * gv.y;
+    double zz = lam * (gu.x + gv.y + gw.z) + 2.0 * muT * gw.z;
+    double xy = muT * (gu.y + gv.x);
+    double xz = muT * (gu.z + gw.x);
+    double yz = muT * (gv.z + gw.y);
+    vec3 tX = v3(xx, xy, xz), tY = v3(xy, yy, yz), tZ = v3(xz, yz, zz);
+    double thX = vdot(tX, vel) + kT * gT.x;
+    double thY = vdot(tY, vel) + kT * gT.y;
+    double thZ = vdot(tZ, vel) + kT * gT.z;
+    vec3 n = vdiv(S, vmag(S));
+    sv5 F = {{0.0, vdot(tX, n), vdot(tY, n), vdot(tZ, n), thX * n.x + thY * n.y + thZ * n.z}};
+    return F;
+}
+
+/* Solver::computeViscousFluxResiduals (src/solver.cpp:2060-2171): interior
+ * faces only, states and gradients averaged over the two nodes. */
+static void viscous_residuals(oracle_solver* s, int dir, double* const* U) {
+    long nf[3] = {s->ni, s->nj, s->nk};
+    nf[dir] += 1;
+    const vec3* surf = dir == 0 ? s->sI : (dir == 1 ? s->sJ : s->sK);
+    const long st[3] = {dir == 0, dir == 1, dir == 2};
+    for (long fi = 0; fi < nf[0]; fi++)
+        for (long fj = 0; fj < nf[1]; fj++)
+            for (long fk = 0; fk < nf[2]; fk++) {
+                long dface = dir == 0 ? fi : (dir == 1 ? fj : fk);
+                if (dface == 0 || dface == nf[dir] - 1) continue;
+                long ql = idx3(s, fi - st[0], fj - st[1], fk - st[2]);
+                long qr = idx3(s, fi, fj, fk);
+                vec3 S = surf[dir == 0 ? sIi(s, fi, fj, fk) : (dir == 1 ? sJi(s, fi, fj, fk) : sKi(s, fi, fj, fk))];
+                sv5 Ua = smul(sadd(state_at(s, U, fi - st[0], fj - st[1], fk - st[2]), state_at(s, U, fi, fj, fk)), 0.5);
+                vec3 g[4];
+                for (int v = 0; v < 4; v++) g[v] = vmul(vadd(s->grad[v][ql], s->grad[v][qr]), 0.5);
+                double muEddy = (0.0 + 0.0) * 0.5;
+                sv5 F = viscous_flux(s, Ua, g[0], g[1], g[2], g[3], S, muEddy);
+                sv5 c = smul(smul(F, vmag(S)), -1.0);
+                res_add(s, fi - st[0], fj - st[1], fk - st[2], c);
+                res_sub(s, fi, fj, fk, c);
+            }
+}
+
+/* Solver::setMomentumSolutionOnViscousWalls (src/solver.cpp:3147-3186) for a
+ * wall at rest: the momentum of every wall node becomes density * 0, on the
+ * state (preprocessSolution, :3189-3203) and on the residuals
+ * (enforceNoSlipWallsOnResiduals, :1856-1863). */
+static void no_slip_momentum(const oracle_solver* s, double* const* X) {
+    if (!s->viscous) return;
+    for (long q = 0; q < s->n; q++)
+        if (s->wall[q])
+            for (int c = 1; c <= 3; c++) X[c][q] = X[0][q] * 0.0;
+}
+
 /* Solver::computeResiduals (src/solver.cpp:1783-1833). */
 static void compute_residuals(oracle_solver* s, double* const* U, long it) {
     for (int c = 0; c < 5; c++) memset(s->R[c], 0, sizeof(double) * s->n);
     advection_residuals(s, 0, U, it);
     if (s->topology != TOPO_1D) advection_residuals(s, 1, U, it);
     if (s->topology == TOPO_3D) advection_residuals(s, 2, U, it);
+    if (s->viscous) {
+        viscous_residuals(s, 0, U);
+        viscous_residuals(s, 1, U);
+        if (s->topology == TOPO_3D) viscous_residuals(s, 2, U);
+    }
     source_residuals(s, U);
     if (s->periodic) periodic_residuals(s);
+    no_slip_momentum(s, s->R);
 }
 
 /* Solver::computeTimestepArray (src/solver.cpp:1531-1630). */
@@ -1594,6 +1762,7 @@ static void compute_timestep(oracle_solver* s, double* const* U) {
                 double rho = W.v[0];
                 double a = f_sound_speed_rho_u_et(s, W.v[0], u, W.v[4]);
                 double mu = 0.0, mut = 0.0;
+                if (s->viscous) mu = f_mu(s, f_temperature_rho_u_et(s, W.v[0], u, W.v[4]));
                 double nu = mu / rho, nut = mut / rho;
                 double ui = fabs(vdot(u, dI)), uj = fabs(vdot(u, dJ)), uk = fabs(vdot(u, dK));
                 double lc = (ui + a) / dsI;
@@ -2159,6 +2328,7 @@ static int bc_type_of(const char* name, int* out) { /* boundaryTypeFromString, i
              !strcmp(low, "mass_flow_rate")) *out = BC_MASS_FLOW;
     else if (!strcmp(low, "transparent")) *out = BC_TRANSPARENT;
     else if (!strcmp(low, "farfield")) *out = BC_FARFIELD;
+    else if (!strcmp(low, "no_slip_wall")) *out = BC_NO_SLIP_WALL;
     else return fail("Boundary type '%s' is not supported by the oracle", name);
     return 0;
 }
@@ -2293,6 +2463,73 @@ static int build_boundary_structures(oracle_solver* s) {
     return 0;
 }
 
+/* setTransportProperties of FluidIdeal (src/fluid_ideal.cpp:209-222) and
+ * FluidReal (src/fluid_real.cpp:378-385) with Config::getViscosityModel and
+ * getFluidMuConstant (src/config.cpp:575-598); FluidReal's viscosity stays at
+ * its 2.0e-5 default unless the model is constant. The Spalart-Allmaras
+ * model is outside the oracle. */
+static int read_transport(oracle_solver* s) {
+    config* c = &s->cfg;
+    int turb = 0;
+    if (cfg_bool(c, "TURBULENCE_ACTIVE", 0, &turb)) return 1;
+    if (turb) return fail("TURBULENCE_ACTIVE: the Spalart-Allmaras model is outside the oracle's scope");
+    const char* m = cfg_get(c, "FLUID_VISCOSITY_MODEL");
+    int has_mu = cfg_get(c, "FLUID_MU_CONSTANT") || cfg_get(c, "FLUID_CONSTANT_MU");
+    if (!m || !strcmp(m, "None")) s->visc_const = has_mu;
+    else {
+        char low[128];
+        snprintf(low, sizeof low, "%s", m);
+        for (char* q = low; *q; q++) *q = (char)tolower((unsigned char)*q);
+        if (!strcmp(low, "sutherland")) s->visc_const = 0;
+        else if (!strcmp(low, "constant")) s->visc_const = 1;
+        else return fail("Unknown ViscosityModel: %s. Supported options: Sutherland, Constant.", m);
+    }
+    if (s->visc_const) {
+        const char* k = cfg_get(c, "FLUID_MU_CONSTANT") ? "FLUID_MU_CONSTANT"
+                        : cfg_get(c, "FLUID_CONSTANT_MU") ? "FLUID_CONSTANT_MU"
+                        : cfg_get(c, "FLUID_SUTHERLAND_MU_REF") ? "FLUID_SUTHERLAND_MU_REF" : NULL;
+        if (!k) return fail("Missing constant viscosity value: please specify \"FLUID_MU_CONSTANT\" in configuration.");
+        if (cfg_float(c, k, &s->mu_const)) return 1;
+    } else if (s->real) {
+        s->visc_const = 1;
+        s->mu_const = 2.0e-5;
+    } else if (cfg_float(c, "FLUID_SUTHERLAND_MU_REF", &s->suth_mu) || cfg_float(c, "FLUID_SUTHERLAND_T_REF", &s->suth_T) ||
+               cfg_float(c, "FLUID_SUTHERLAND_S", &s->suth_S)) {
+        return 1;
+    }
+    if (cfg_float(c, "FLUID_CP", &s->vcp) || cfg_float(c, "FLUID_PRANDTL_NUMBER", &s->vpr)) return 1;
+    return 0;
+}
+
+/* Solver::buildBoundaryFluxes (src/solver.cpp:369-388) with
+ * fetchBoundaryNodesIndexRange (src/boundary_base.cpp:227-267): the nodes of
+ * every no-slip wall patch; a moving wall is outside the oracle. */
+static int build_wall_mask(oracle_solver* s) {
+    s->wall = (unsigned char*)calloc(s->n, 1);
+    for (int m = 0; m < s->npatches; m++) {
+        const patch* p = &s->patches[m];
+        if (p->type != BC_NO_SLIP_WALL) continue;
+        if (p->nvalues > 0 && (p->nvalues < 3 || p->values[0] != 0.0 || p->values[1] != 0.0 || p->values[2] != 0.0))
+            return fail("moving no-slip walls are outside the oracle's scope (patch %s)", p->name);
+        long i0 = p->i_min, i1 = p->i_max, j0 = p->j_min, j1 = p->j_max, k0 = p->k_min, k1 = p->k_max;
+        if (i0 == i1 && i0 == 0) i1 = 1;
+        else if (i0 == i1 && i0 == s->ni) { i0 = s->ni - 1; i1 = i0 + 1; }
+        else if (j0 == j1 && j0 == 0) j1 = 1;
+        else if (j0 == j1 && j0 == s->nj) { j0 = s->nj - 1; j1 = j0 + 1; }
+        else if (k0 == k1 && k0 == 0) k1 = 1;
+        else if (k0 == k1 && k0 == s->nk) { k0 = s->nk - 1; k1 = k0 + 1; }
+        else return fail("Invalid indexing on boundary condition specs for patch %s", p->name);
+        for (long i = i0; i < i1; i++)
+            for (long j = j0; j < j1; j++)
+                for (long k = k0; k < k1; k++) s->wall[idx3(s, i, j, k)] = 1;
+    }
+    for (int v = 0; v < 4; v++) {
+        s->grad[v] = (vec3*)calloc(s->n, sizeof(vec3));
+        s->gfield[v] = (double*)calloc(s->n, sizeof(double));
+    }
+    return 0;
+}
+
 static int read_settings(oracle_solver* s) {
     config* c = &s->cfg;
     const char* v;
@@ -2351,9 +2588,7 @@ static int read_settings(oracle_solver* s) {
     else if (cfg_float(c, "CFL", &s->cfl)) return 1;
     if (s->dt_method == DT_FIXED && cfg_float(c, "FIXED_TIME_STEP", &s->fixed_dt)) return 1;
 
-    int visc = 0;
-    if (cfg_bool(c, "VISCOSITY_ACTIVE", 0, &visc)) return 1;
-    if (visc) return fail("Viscous fluxes are outside the oracle's scope");
+    if (cfg_bool(c, "VISCOSITY_ACTIVE", 0, &s->viscous)) return 1;
     v = cfg_get(c, "FLUID_MODEL");
     if (v && (!strcmp(v, "real") || !strcmp(v, "Real") || !strcmp(v, "REAL"))) {
         s->real = 1; /* the table is loaded by oracle_create, next to the ini */
@@ -2369,6 +2604,7 @@ static int read_settings(oracle_solver* s) {
         if (cfg_float(c, "FLUID_R_CONSTANT", &s->rgas)) return 1;
         s->cp = (s->gamma * s->rgas) / (s->gamma - 1);
     }
+    if (s->viscous && read_transport(s)) return 1;
 
     if (cfg_bool(c, "SIMULATION_IS_STEADY", 1, &s->steady)) return 1;
     if (cfg_int_def(c, "RESIDUALS_DROP_CONVERGENCE", 16, &s->drop)) return 1;
@@ -2794,6 +3030,7 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
     dir_join(path, sizeof path, base, bcf);
     if (read_boundaries(s, path) || build_boundary_structures(s)) { oracle_destroy(s); return 1; }
     resolve_turbo_dir(s);
+    if (s->viscous && build_wall_mask(s)) { oracle_destroy(s); return 1; }
     for (int m = 0; m < s->npatches; m++) {
         if (s->patches[m].type == BC_THROTTLE) { s->need_turbo = 1; s->throttle_kt = s->patches[m].values[0]; }
         if (s->patches[m].type == BC_MASS_FLOW) s->need_turbo = 1; /* src/solver.cpp:1311-1316 */
@@ -2864,6 +3101,8 @@ void oracle_destroy(oracle_solver* s) {
     free(s->profiles);
     for (int c = 0; c < 5; c++) { free(s->U[c]); free(s->Utmp[c]); free(s->R[c]); }
     free(s->dt);
+    free(s->wall);
+    for (int v = 0; v < 4; v++) { free(s->grad[v]); free(s->gfield[v]); }
     free(s->hist);
     free(s);
 }
@@ -2893,13 +3132,16 @@ int oracle_run(oracle_solver* s, long n_iter, long* n_done, int* converged) {
     *n_done = 0;
     *converged = 0;
     s->nhist = 0;
+    no_slip_momentum(s, s->U);
     for (int c = 0; c < 5; c++) memcpy(s->Utmp[c], s->U[c], sizeof(double) * s->n);
     for (long it = s->iter + 1; it <= s->iter + n_iter; it++) {
         update_mass_flows(s, s->Utmp);
         if (s->need_turbo) update_turbo(s, s->Utmp);
         compute_timestep(s, s->Utmp);
         if (s->nprofiles || s->greitzer) update_radial_profiles(s, s->Utmp);
+        no_slip_momentum(s, s->Utmp);
         for (int st = 0; st < s->nstages; st++) {
+            solution_gradient(s, s->Utmp);
             compute_residuals(s, s->Utmp, it);
             update_solution(s, s->coeffs[st]);
             periodic_solution(s);
@@ -2926,11 +3168,14 @@ int oracle_run(oracle_solver* s, long n_iter, long* n_done, int* converged) {
 
 int oracle_residual(oracle_solver* s, double* dt, double* r0, double* r1, double* r2, double* r3,
                     double* r4) {
+    no_slip_momentum(s, s->U);
     for (int c = 0; c < 5; c++) memcpy(s->Utmp[c], s->U[c], sizeof(double) * s->n);
     update_mass_flows(s, s->Utmp);
     if (s->need_turbo) update_turbo(s, s->Utmp);
     compute_timestep(s, s->Utmp);
     if (s->nprofiles || s->greitzer) update_radial_profiles(s, s->Utmp);
+    no_slip_momentum(s, s->Utmp);
+    solution_gradient(s, s->Utmp);
     compute_residuals(s, s->Utmp, s->iter + 1);
     memcpy(dt, s->dt, sizeof(double) * s->n);
     double* outs[5] = {r0, r1, r2, r3, r4};

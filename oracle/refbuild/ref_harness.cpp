@@ -108,6 +108,7 @@ int main(int argc, char** argv) {
             if (needTurbo) solver.updateTurboPerformance(solutionTmp);
             solver.computeTimestepArray(solutionTmp, timestep);
             solver.preprocessSolution(solutionTmp);
+            solver.computeSolutionGradient(solutionTmp, gradTmp);
             solver.computeResiduals(solutionTmp, gradTmp, 1, solver._currentTime, timestep, residuals);
             std::ofstream f(argv[3], std::ios::binary);
             writeI64(f, ni); writeI64(f, nj); writeI64(f, nk);

@@ -120,6 +120,28 @@ def _correlations():
                            KN_CORRELATION_BFM_COEFFICIENT="0.8")
 
 
+def _viscous(c, mu=None, walls=(2, 3), **settings):
+    """Laminar viscous run (VISCOSITY_ACTIVE) with the J-face walls made
+    no-slip walls at rest: Sutherland's law for air when mu is None, else a
+    constant viscosity (large, so that the viscous terms weigh in after a few
+    iterations on these coarse grids)."""
+    for m in walls:
+        c.patches[m] = dataclasses.replace(c.patches[m], spec="no_slip_wall, 0, 0, 0")
+    kw = dict(VISCOSITY_ACTIVE="yes", FLUID_CP="1004.675", FLUID_PRANDTL_NUMBER="0.72")
+    if mu is None:
+        kw.update(FLUID_VISCOSITY_MODEL="Sutherland", FLUID_SUTHERLAND_MU_REF="1.716e-5",
+                  FLUID_SUTHERLAND_T_REF="273.15", FLUID_SUTHERLAND_S="110.4")
+    else:
+        kw.update(FLUID_MU_CONSTANT=repr(mu))
+    kw.update(settings)
+    return c.with_settings(**kw)
+
+
+def _co2_viscous():
+    c = _co2(cases.bump2d(ni=24, nj=12, mach=0.3))
+    return _viscous(c, mu=5e-3, FLUID_CP="1200.0", FLUID_PRANDTL_NUMBER="0.9")
+
+
 CASES = {
     "bump_jst_rk4": (lambda: cases.bump2d(ni=24, nj=12), 20),
     "bump_roe_vanalbada_rk3": (lambda: cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada", rk=3, cfl=0.8), 20),
@@ -153,4 +175,15 @@ CASES = {
     "co2_bump_farfield": (_co2_farfield, 20),
     "meridional_chima": (_chima, 20),
     "meridional_correlations": (_correlations, 20),
+    "bump_viscous_sutherland": (lambda: _viscous(cases.bump2d(ni=24, nj=12)), 20),
+    "bump_viscous_roe_muscl": (lambda: _viscous(cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True, limiter="van albada",
+                                                             rk=3, cfl=0.8), mu=0.02), 20),
+    "bump_viscous_supersonic_inlet": (lambda: _viscous(_bump_supersonic(), mu=0.01), 20),
+    "bump_viscous_global_dt": (lambda: _viscous(cases.bump2d(ni=24, nj=12), mu=0.05, TIME_STEP_METHOD="global", CFL="1.0"), 20),
+    "meridional_viscous_duct": (lambda: _viscous(cases.meridional(ni=24, nj=10, p_ratio=0.95), mu=0.01,
+                                                 BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no"), 20),
+    "sector45_viscous": (lambda: _viscous(_sector(45.0), mu=0.01), 10),
+    "annulus_viscous_roe": (lambda: _viscous(cases.annulus3d(ni=20, nj=8, nk=9, bfm_model="None"),
+                                             BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no"), 10),
+    "co2_bump_viscous": (_co2_viscous, 20),
 }

@@ -80,3 +80,22 @@ def test_oracle_diverges_where_the_reference_does(tmp_path, oracle_lib):
     if oracle_lib.ref_available():
         ref = oracle_lib.ref_harness("steps", ini, 500)
         assert ref["converged"] == 2 and ref["iterations"] == 71  # the diverged iteration is not recorded
+
+
+def test_viscous_blade_rows_diverge_at_the_first_iteration_like_the_reference(tmp_path, oracle_lib):
+    """No-slip walls through Hall blade rows: the body force of a wall node at
+    rest is 0/0, so the reference's first iteration already has a NaN energy
+    residual; the oracle stops at the same iteration with the same NaN nodes."""
+    import numpy as np
+    from parity_cases import _viscous
+    from cturbobfm_b200 import cases
+
+    ini = _viscous(cases.meridional(ni=24, nj=10), mu=0.01).write(str(tmp_path))
+    r = oracle_lib.Oracle(ini).run(5)
+    assert r["status"] == 2 and r["iterations"] == 1
+    _, res = oracle_lib.Oracle(ini).residual()
+    bad = np.isnan(res)
+    assert bad[4].any() and not bad[:4].any()
+    if oracle_lib.ref_available():
+        assert oracle_lib.ref_harness("steps", ini, 5)["converged"] == 2
+        assert np.array_equal(np.isnan(oracle_lib.ref_harness("residual", ini)["residual"]), bad)
