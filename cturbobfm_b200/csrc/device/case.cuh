@@ -14,8 +14,8 @@ namespace ctbfm {
 constexpr int kMaxPatches = 16;
 constexpr int kMaxProfiles = 4;
 
-// Boundary types (include/types.hpp:178-194; the 2-D inlet file and the
-// no-slip wall of the viscous path are not among them).
+// Boundary types (include/types.hpp:178-194; the 2-D inlet file is not among
+// them).
 enum DevBc : int {
     kBcInlet = 0,
     kBcOutlet = 1,
@@ -29,7 +29,8 @@ enum DevBc : int {
     kBcOutletSupersonic = 9,
     kBcMassFlow = 10,
     kBcTransparent = 11,
-    kBcFarfield = 12
+    kBcFarfield = 12,
+    kBcNoSlipWall = 13
 };
 
 struct DevPatch {
@@ -212,6 +213,21 @@ struct alignas(16) DevCaseT {
     int node_tiles;   // tiles of this instance in the node kernels
     int per_tiles;    // tiles of this instance in the periodic kernel
     const DevLut* lut;  // FLUID_MODEL = real: the look-up tables; nullptr for the ideal gas
+    // VISCOSITY_ACTIVE (laminar): viscosity constant (visc_const) or
+    // Sutherland's law, conductivity vcp * mu / vpr; nodes of the no-slip
+    // walls (at rest); per face of each direction the raw surface vector S
+    // and the Green-Gauss interpolation weights of its left and right node;
+    // per node the gradients of u, v, w and T (G[3 * field + component]);
+    // per face the viscous contribution flux * |S| of the momentum and
+    // energy equations
+    int viscous, visc_const;
+    double mu_const, suth_mu, suth_T, suth_S, vcp, vpr;
+    const unsigned char* wall;
+    const R* sraw[3][3];
+    const R* gwL[3];
+    const R* gwR[3];
+    R* G[12];
+    R* V[3][4];
     Control* ctl;
     double* hist;  // kHistWidth doubles per iteration row
     long long hist_cap;

@@ -35,6 +35,9 @@ struct BatchView {
     // boundary stencils), so that no warp mixes the two code paths
     TileList face[3][2][3];
     TileList per;         // periodic (i, j) pairs of periodic instances
+    bool viscous = false;  // some member is viscous (VISCOSITY_ACTIVE)
+    TileList vnode;        // nodes of the viscous instances (k_grad)
+    TileList vface[3];     // every face of each swept direction of the viscous instances (k_vfaces)
     TileList inst;        // one tile per instance (k_pre, k_finalize)
     TileList bint;        // 8 plane tiles per instance that needs turbo performance
     TileList bintAll;     // 8 plane tiles for every instance
@@ -51,10 +54,12 @@ struct Launcher {
                            cudaStream_t s);
     static cudaError_t prim(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t faces(const BatchView<R>& b, int dir, int stage, int force, cudaStream_t s);
+    // k_grad and k_vfaces of the viscous members
+    static cudaError_t viscous(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t finalize(const BatchView<R>& b, int force, cudaStream_t s);
-    // k_prim, k_faces, k_nodes, k_periodic of one stage (stage -1: residual only)
+    // k_prim, k_faces, (k_grad, k_vfaces), k_nodes, k_periodic of one stage (stage -1: residual only)
     static cudaError_t stage(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     // one whole iteration of every instance in the batch
     static cudaError_t iteration(const BatchView<R>& b, int nstages, cudaStream_t s);

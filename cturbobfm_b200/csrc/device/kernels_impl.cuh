@@ -22,6 +22,7 @@
 
 #include "kernels.hpp"
 #include "sources.cuh"
+#include "viscous.cuh"
 
 namespace ctbfm {
 
@@ -104,10 +105,15 @@ __device__ __forceinline__ R* const* stageOut(const DevCaseT<R>& c, int s) {
 
 // Not inlined: the boundary faces are few, and keeping their many flux
 // variants out of the face kernels' bodies halves the kernels' spills.
+// onWall: the face's own (i, j, k), read as a node, lies on a no-slip wall of
+// a viscous instance (BoundaryBase::isNodeOnNoSlipWall,
+// include/boundary_base.hpp:44-49): inlet faces there take the stagnation
+// flux (src/boundary_inlet.cpp:16-19, src/boundary_inlet_supersonic.cpp:15-18).
 template <int SCHEME, typename R>
 __device__ __noinline__ S5<R> boundaryFlux(const DevCaseT<R>& c, Gas<R> gs, int pidx, const S5<R>& Uint, V3<R> n,
-                                              long long qtheta, int fj, long long it) {
+                                              long long qtheta, int fj, long long it, bool onWall) {
     const DevPatch& p = c.patch[pidx];
+    if (onWall && (p.type == kBcInlet || p.type == kBcInletSupersonic)) return stagnationWallFlux(R(p.v[0]), n);
     switch (p.type) {
         case kBcInlet: return bcInlet(c, gs, p, Uint, n, c.cost[qtheta], c.sint[qtheta]);
         case kBcOutlet: return bcOutlet(c, gs, Uint, n, R(p.v[0]), it);
@@ -128,7 +134,8 @@ __device__ __noinline__ S5<R> boundaryFlux(const DevCaseT<R>& c, Gas<R> gs, int 
             const int jj = fj < c.prof_n[m] ? fj : c.prof_n[m] - 1;
             return bcOutlet(c, gs, Uint, n, R(c.prof_p[c.prof_off[m] + jj]), it);
         }
-        case kBcInviscidWall: return bcWall(gs, Uint, n);
+        case kBcInviscidWall:
+        case kBcNoSlipWall: return bcWall(gs, Uint, n);  // BoundaryInviscidWall for both (src/solver.cpp:393-398)
         default: return zero5<R>();  // periodic / wedge faces: BoundaryFake, zero flux
     }
 }
@@ -196,6 +203,164 @@ __device__ __forceinline__ S5<double> state64(const DevCaseT<R>& c, R* const* U,
 #pragma unroll
         for (int v = 0; v < 5; v++) s.v[v] -= static_cast<double>(c.Uc[v][q]);
     return s;
+}
+
+// Viscous face contributions of node (i, j, k) (Solver::computeViscousFluxResiduals,
+// src/solver.cpp:2060-2171): interior faces only; the reference adds
+// -flux*|S| to the left node and subtracts it from the right one, so a node
+// takes +V of its start face, then -V of its end face, direction by direction
+// (K only in 3-D). The mass residual receives zeros, which change nothing.
+template <typename R>
+__device__ __forceinline__ void addViscousResidual(const DevCaseT<R>& c, int i, int j, int k, S5<R>& Res) {
+    const int nj = c.nj, nk = c.nk;
+    {
+        const long long f0 = (static_cast<long long>(i) * nj + j) * nk + k;
+        const long long f1 = f0 + static_cast<long long>(nj) * nk;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            if (i >= 1) Res.v[v + 1] = Res.v[v + 1] + c.V[0][v][f0];
+            if (i + 1 <= c.ni - 1) Res.v[v + 1] = Res.v[v + 1] - c.V[0][v][f1];
+        }
+    }
+    {
+        const long long f0 = (static_cast<long long>(i) * (nj + 1) + j) * nk + k;
+        const long long f1 = f0 + nk;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            if (j >= 1) Res.v[v + 1] = Res.v[v + 1] + c.V[1][v][f0];
+            if (j + 1 <= nj - 1) Res.v[v + 1] = Res.v[v + 1] - c.V[1][v][f1];
+        }
+    }
+    if (c.topo == 1) {
+        const long long f0 = (static_cast<long long>(i) * nj + j) * (nk + 1) + k;
+        const long long f1 = f0 + 1;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            if (k >= 1) Res.v[v + 1] = Res.v[v + 1] + c.V[2][v][f0];
+            if (k + 1 <= nk - 1) Res.v[v + 1] = Res.v[v + 1] - c.V[2][v][f1];
+        }
+    }
+}
+
+// Solver::setMomentumSolutionOnViscousWalls (src/solver.cpp:3147-3186) on the
+// residual of a wall node (enforceNoSlipWallsOnResiduals, :1856-1863): the
+// momentum residual becomes the mass residual times the zero wall velocity.
+template <typename R>
+__device__ __forceinline__ void noSlipResidual(S5<R>& Res) {
+    Res.v[1] = Res.v[0] * R(0);
+    Res.v[2] = Res.v[0] * R(0);
+    Res.v[3] = Res.v[0] * R(0);
+}
+
+// ----------------------------------------------------------- viscous terms
+// Solver::computeSolutionGradient (src/solver.cpp:3033-3058) with
+// computeGradientsGreenGauss4 (src/math_utils.cpp:237-392): per node the
+// gradients of u, v, w and T over the six dual faces, W E N S B T, each face
+// value interpolated between the node and its neighbour with the face
+// centre's distance weights (the node's own value on boundary faces), summed
+// in that order and multiplied by 1/V. Reads the primitives of k_prim.
+template <typename R, int FL>
+__global__ void __launch_bounds__(256) k_grad(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
+    const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
+    const int ni = c.ni, nj = c.nj, nk = c.nk;
+    const long long sI = static_cast<long long>(nj) * nk;
+    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) {
+        const int k = static_cast<int>(q % nk);
+        const long long tq = q / nk;
+        const int j = static_cast<int>(tq % nj);
+        const int i = static_cast<int>(tq / nj);
+        auto fields = [&](long long n, R (&f)[4]) {
+            const S5<R> W = load5(c.W, n);
+            f[0] = W.v[1];
+            f[1] = W.v[2];
+            f[2] = W.v[3];
+            f[3] = gradientTemperature(c, gs, W);
+        };
+        R fc[4];
+        fields(q, fc);
+        R g[4][3];
+#pragma unroll
+        for (int v = 0; v < 4; v++) g[v][0] = g[v][1] = g[v][2] = R(0);
+        // face f of the node: neighbour (or -1), face index in its direction's
+        // grid, sign of S, and whether the node is the face's left node
+        auto face = [&](int d, long long fidx, long long nb, bool neg, bool left) {
+            R sv[4];
+            if (nb >= 0) {
+                const R w = left ? __ldg(c.gwL[d] + fidx) : __ldg(c.gwR[d] + fidx);
+                R fn[4];
+                fields(nb, fn);
+#pragma unroll
+                for (int v = 0; v < 4; v++) sv[v] = fc[v] + (fn[v] - fc[v]) * w;
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; v++) sv[v] = fc[v];
+            }
+            R S[3] = {__ldg(c.sraw[d][0] + fidx), __ldg(c.sraw[d][1] + fidx), __ldg(c.sraw[d][2] + fidx)};
+            if (neg) S[0] = -S[0], S[1] = -S[1], S[2] = -S[2];
+#pragma unroll
+            for (int v = 0; v < 4; v++)
+#pragma unroll
+                for (int x = 0; x < 3; x++) g[v][x] = addRn(g[v][x], mulRn(S[x], sv[v]));
+        };
+        const long long fI = (static_cast<long long>(i) * nj + j) * nk + k;        // I face i
+        const long long fJ = (static_cast<long long>(i) * (nj + 1) + j) * nk + k;  // J face j
+        const long long fK = (static_cast<long long>(i) * nj + j) * (nk + 1) + k;  // K face k
+        face(0, fI, i > 0 ? q - sI : -1, true, false);             // west: face i, node on its right
+        face(0, fI + sI, i < ni - 1 ? q + sI : -1, false, true);   // east: face i+1, node on its left
+        face(1, fJ + nk, j < nj - 1 ? q + nk : -1, false, true);   // north: face j+1
+        face(1, fJ, j > 0 ? q - nk : -1, true, false);             // south: face j
+        face(2, fK, k > 0 ? q - 1 : -1, true, false);              // bottom: face k
+        face(2, fK + 1, k < nk - 1 ? q + 1 : -1, false, true);     // top: face k+1
+        const R inv = R(1) / c.vol[q];
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+#pragma unroll
+            for (int x = 0; x < 3; x++) c.G[3 * v + x][q] = g[v][x] * inv;
+    }
+}
+
+// Solver::computeViscousFluxResiduals (src/solver.cpp:2060-2171): one thread
+// per face of direction DIR in storage order; interior faces write
+// flux * |S| of the momentum and energy equations from the averaged node
+// states and gradients (boundary faces carry no viscous flux and are not
+// read).
+template <int DIR, typename R, int FL>
+__global__ void __launch_bounds__(256) k_vfaces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
+    const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
+    const int nfj = c.nj + (DIR == 1), nfk = c.nk + (DIR == 2);
+    const int nlast = DIR == 0 ? c.ni : (DIR == 1 ? c.nj : c.nk);
+    const long long st = DIR == 0 ? static_cast<long long>(c.nj) * c.nk : (DIR == 1 ? c.nk : 1);
+    const DevFacesT<R>& F = c.f[DIR];
+    R* const* U = stageIn(c, stage);
+    for (long long f = tl.start + threadIdx.x; f < tl.start + tl.count; f += blockDim.x) {
+        const int fk = static_cast<int>(f % nfk);
+        const long long t = f / nfk;
+        const int fj = static_cast<int>(t % nfj);
+        const int fi = static_cast<int>(t / nfj);
+        const int dface = DIR == 0 ? fi : (DIR == 1 ? fj : fk);
+        if (dface == 0 || dface == nlast) continue;
+        const long long qR = nodeIdx(c, fi, fj, fk);
+        const long long qL = qR - st;
+        const S5<R> Ua = (load5(U, qL) + load5(U, qR)) * R(0.5);
+        V3<R> gr[4];
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+            gr[v] = v3((c.G[3 * v][qL] + c.G[3 * v][qR]) * R(0.5), (c.G[3 * v + 1][qL] + c.G[3 * v + 1][qR]) * R(0.5),
+                       (c.G[3 * v + 2][qL] + c.G[3 * v + 2][qR]) * R(0.5));
+        const R muEddy = (R(0) + R(0)) * R(0.5);
+        const V3<R> n = v3(__ldg(F.nx + f), __ldg(F.ny + f), __ldg(F.nz + f));
+        const R area = __ldg(F.area + f);
+        R flux[4];
+        viscousFlux(c, gs, Ua, gr[0], gr[1], gr[2], gr[3], n, muEddy, flux);
+#pragma unroll
+        for (int v = 0; v < 4; v++) c.V[DIR][v][f] = flux[v] * area;
+    }
 }
 
 // ------------------------------------------------------------------ faces
@@ -285,7 +450,8 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
             // theta of the face's (i, j, k) node for the cylindrical inlet frame
             const long long qth =
                 nodeIdx(c, fi < c.ni ? fi : c.ni - 1, fj < c.nj ? fj : c.nj - 1, fk < c.nk ? fk : c.nk - 1);
-            flux = boundaryFlux<SCHEME>(c, gs, pidx, load5(U, q), n, qth, fj, it);
+            const bool onWall = c.viscous && fi < c.ni && fj < c.nj && fk < c.nk && c.wall[nodeIdx(c, fi, fj, fk)];
+            flux = boundaryFlux<SCHEME>(c, gs, pidx, load5(U, q), n, qth, fj, it, onWall);
         } else {
             const long long qR = nodeIdx(c, fi, fj, fk);
             const long long qL = qR - st;
@@ -345,7 +511,8 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 
 // ------------------------------------------------------------------ nodes
 // Residual assembly in the reference's accumulation order (I faces, J faces,
-// K faces, then sources), then Solver::updateSolution (src/solver.cpp:2230-2249)
+// K faces, viscous I, J, K faces, then sources; no-slip wall nodes lose their
+// momentum residual last), then Solver::updateSolution (src/solver.cpp:2230-2249)
 // U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
 // Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
 template <typename R, int FL, int BX>
@@ -399,6 +566,7 @@ __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevC
                 Res.v[v] = Res.v[v] + c.f[2].c[v][f1];
             }
         }
+        if (c.viscous) addViscousResidual(c, i, j, k, Res);
         const S5<R> Unode = load5(Uin, q);
         applySources<BX>(c, gs, Uin, i, j, k, q, Unode, t, Res);
         if (c.periodic && (k == 0 || k == nk - 1)) {
@@ -406,6 +574,7 @@ __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevC
             store5(c.Rp, pq, Res);
             continue;
         }
+        if (c.viscous && c.wall[q]) noSlipResidual(Res);
         if (resOnly) {
             store5(Uout, q, Res);
             continue;
@@ -442,7 +611,8 @@ __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevC
     }
 }
 
-// Solver::enforcePeriodicityOnResiduals (src/solver.cpp:1836-1853), the update
+// Solver::enforcePeriodicityOnResiduals (src/solver.cpp:1836-1853), the
+// no-slip walls on the averaged residuals (:1856-1863), the update
 // of the two periodic planes and Solver::enforcePeriodicityOnSolution
 // (src/solver.cpp:2308-2327). One thread per (i, j) pair.
 template <typename R>
@@ -460,9 +630,13 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
     double acc[5] = {0, 0, 0, 0, 0};
     for (long long p = tl.start + threadIdx.x; p < tl.start + tl.count; p += blockDim.x) {
         const S5<R> R1 = load5(c.Rp, p), R2 = load5(c.Rp, np + p);
-        const S5<R> Ra = (R1 + rotState(R2, cm, sm)) * R(0.5);
-        const S5<R> Rb = rotState(Ra, cp, sp);
+        S5<R> Ra = (R1 + rotState(R2, cm, sm)) * R(0.5);
+        S5<R> Rb = rotState(Ra, cp, sp);
         const long long q0 = p * c.nk, q1 = p * c.nk + c.nk - 1;
+        if (c.viscous) {  // Solver::enforceNoSlipWallsOnResiduals after the periodic average
+            if (c.wall[q0]) noSlipResidual(Ra);
+            if (c.wall[q1]) noSlipResidual(Rb);
+        }
         if (resOnly) {
             store5(Uout, q0, Ra);
             store5(Uout, q1, Rb);
@@ -513,8 +687,9 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
 }
 
 // ------------------------------------------------------------- time step
-// Solver::computeTimestepArray (src/solver.cpp:1531-1630), inviscid:
-// dt = CFL / sum_d (|u . e_d| + a) / |e_d| over the dual-node edges.
+// Solver::computeTimestepArray (src/solver.cpp:1531-1630):
+// dt = CFL / (sum_d (|u . e_d| + a) / |e_d| + 4 nu sum_d 1 / |e_d|^2) over the
+// dual-node edges, the viscous term only for viscous instances.
 template <typename R, int FL>
 __global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile* tiles, int force) {
     __shared__ DevCaseT<R> c;
@@ -537,7 +712,18 @@ __global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile
             const V3<R> dK = v3(c.edge[8][q], c.edge[9][q], c.edge[10][q]);
             lc += (fabs(dot(u, dK)) + a) / c.edge[11][q];
         }
-        const R dt = cfl / lc;
+        R dt;
+        if (c.viscous) {  // 4 (nu + nu_t) sum_d 1/|e_d|^2, nu_t = 0
+            const R mu = molecularViscosity(c, temperature_rho_u_et(gs, W.v[0], u, W.v[4]));
+            const R nu = mu / W.v[0], nut = R(0) / W.v[0];
+            const R dsI = c.edge[3][q], dsJ = c.edge[7][q];
+            R ih2 = R(1) / (dsI * dsI);
+            ih2 += R(1) / (dsJ * dsJ);
+            if (c.topo == 1) ih2 += R(1) / (c.edge[11][q] * c.edge[11][q]);
+            dt = cfl / (lc + R(4) * (nu + nut) * ih2);
+        } else {
+            dt = cfl / lc;
+        }
         c.dt[q] = dt;
         mn = fmin(mn, static_cast<double>(dt));
     }
@@ -947,6 +1133,24 @@ cudaError_t Launcher<R>::faces(const BatchView<R>& b, int dir, int stage, int fo
 }
 
 template <typename R>
+cudaError_t Launcher<R>::viscous(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    if (!b.viscous) return cudaSuccess;
+    if (b.vnode.n && b.ideal) launchK(k_grad<R, 0>, b.vnode.n, 256, s, b.cases, b.vnode.tiles, stage, force);
+    if (b.vnode.n && b.real) launchK(k_grad<R, 1>, b.vnode.n, 256, s, b.cases, b.vnode.tiles, stage, force);
+    if (b.ideal) {
+        if (b.vface[0].n) launchK(k_vfaces<0, R, 0>, b.vface[0].n, 256, s, b.cases, b.vface[0].tiles, stage, force);
+        if (b.vface[1].n) launchK(k_vfaces<1, R, 0>, b.vface[1].n, 256, s, b.cases, b.vface[1].tiles, stage, force);
+        if (b.vface[2].n) launchK(k_vfaces<2, R, 0>, b.vface[2].n, 256, s, b.cases, b.vface[2].tiles, stage, force);
+    }
+    if (b.real) {
+        if (b.vface[0].n) launchK(k_vfaces<0, R, 1>, b.vface[0].n, 256, s, b.cases, b.vface[0].tiles, stage, force);
+        if (b.vface[1].n) launchK(k_vfaces<1, R, 1>, b.vface[1].n, 256, s, b.cases, b.vface[1].tiles, stage, force);
+        if (b.vface[2].n) launchK(k_vfaces<2, R, 1>, b.vface[2].n, 256, s, b.cases, b.vface[2].tiles, stage, force);
+    }
+    return cudaGetLastError();
+}
+
+template <typename R>
 cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
     if (b.node.n && b.ideal && b.bfmCommon) launchK(k_nodes<R, 0, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
     if (b.node.n && b.real && b.bfmCommon) launchK(k_nodes<R, 1, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
@@ -971,6 +1175,7 @@ template <typename R>
 cudaError_t Launcher<R>::stage(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
     cudaError_t e = prim(b, stage, force, s);
     for (int d = 0; d < 3 && e == cudaSuccess; d++) e = faces(b, d, stage, force, s);
+    if (e == cudaSuccess) e = viscous(b, stage, force, s);
     if (e == cudaSuccess) e = nodes(b, stage, force, s);
     if (e == cudaSuccess) e = periodic(b, stage, force, s);
     return e;

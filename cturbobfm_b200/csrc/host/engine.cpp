@@ -68,6 +68,8 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     for (auto* m : members_) (m->c.lut ? view_.real : view_.ideal) = true;
     view_.bfmCommon = view_.bfmRare = false;
     for (auto* m : members_) (bfmRareModel(m->c) ? view_.bfmRare : view_.bfmCommon) = true;
+    view_.viscous = false;
+    for (auto* m : members_) view_.viscous = view_.viscous || m->c.viscous;
     refresh(nullptr);
     cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -80,7 +82,7 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
 template <typename R>
 void GroupT<R>::buildTiles() {
     const int M = static_cast<int>(members_.size());
-    std::vector<Tile> node, face[3][2][3], per, inst, bint, bintAll;
+    std::vector<Tile> node, face[3][2][3], per, inst, bint, bintAll, vnode, vface[3];
     auto cover = [](std::vector<Tile>& out, int m, long long count, long long size) {
         int local = 0;
         for (long long s = 0; s < count; s += size) out.push_back({m, local++, s, std::min<long long>(size, count - s)});
@@ -111,6 +113,12 @@ void GroupT<R>::buildTiles() {
                 cover(face[d][c.scheme][2], m, lines * 4, faceTile_[d]);
             }
         }
+        if (c.viscous) {
+            cover(vnode, m, c.n, kTileSize);
+            for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++)
+                cover(vface[d], m, static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2)),
+                      kTileSize);
+        }
         if (c.periodic && cover(per, m, static_cast<long long>(c.ni) * c.nj, kPeriodicTile) != c.per_tiles)
             throw std::logic_error("periodic tile count mismatch");
         inst.push_back({m, 0, 0, 1});
@@ -131,6 +139,8 @@ void GroupT<R>::buildTiles() {
         for (int s = 0; s < 2; s++)
             for (int k = 0; k < 3; k++) add(view_.face[d][s][k], face[d][s][k]);
     add(view_.per, per);
+    add(view_.vnode, vnode);
+    for (int d = 0; d < 3; d++) add(view_.vface[d], vface[d]);
     add(view_.inst, inst);
     add(view_.bint, bint);
     add(view_.bintAll, bintAll);

@@ -36,7 +36,7 @@ int boundaryTypeFromString(std::string s) {  // include/types.hpp:202-232, path 
     // stays empty, include/solver.hpp:345), so its inlet_2d cannot run
     if (s == "inlet_2d")
         throw ConfigError("BoundaryType inlet_2d: the reference reads its 2-D inlet file from an empty path; not supported");
-    if (s == "no_slip_wall") throw ConfigError("BoundaryType no_slip_wall belongs to the viscous path, outside this library's scope");
+    if (s == "no_slip_wall") return kBcNoSlipWall;
     throw ConfigError("Unknown BoundaryType: " + s);
 }
 
@@ -117,8 +117,8 @@ SourceBFMChima::SourceBFMChima(const Config& config) : SourceBFMBase(config), le
 }
 
 Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_(config.getTopology()) {
-    if (config.isViscosityActive()) throw ConfigError("Viscous fluxes are outside this library's Euler path");
-    if (config.parseBool("TURBULENCE_ACTIVE", false)) throw ConfigError("Turbulence models are outside this library's Euler path");
+    if (config.parseBool("TURBULENCE_ACTIVE", false))
+        throw ConfigError("TURBULENCE_ACTIVE: the Spalart-Allmaras model is outside this library's scope");
     // Config::getFluidModel (src/config.cpp:468-481)
     const std::string fluid = config.has("FLUID_MODEL") ? config.get("FLUID_MODEL") : "None";
     if (fluid == "real" || fluid == "Real" || fluid == "REAL") {
@@ -131,6 +131,7 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     } else if (fluid != "None" && fluid != "Ideal" && fluid != "ideal" && fluid != "IDEAL") {
         throw ConfigError("Invalid value for key \"FLUID_MODEL\" in configuration.");
     }
+    if (config.isViscosityActive()) setupTransport();
     if (config.isAccelerationActive() && config.getTimeStepMethod() != TimeStepMethod::Fixed)
         throw ConfigError("Rotational speed scaling factor is only active for fixed time step method");
     // GPU_PRECISION (this library's key; the reference ignores unknown keys)
@@ -145,6 +146,7 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     setupModels();
     readBoundaries();
     buildBoundaryStructures();
+    buildWallMask();
     validateSettings();
     setupScalars();
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -179,6 +181,77 @@ void Solver::setupModels() {
         case BfmModel::Correlations: bfm_ = std::make_unique<SourceBFMCorrelations>(config_); break;
         default: bfm_ = std::make_unique<SourceBFMBase>(config_); break;
     }
+}
+
+// setTransportProperties of FluidIdeal (src/fluid_ideal.cpp:209-222) and
+// FluidReal (src/fluid_real.cpp:378-385), called when the fluid is built
+// (src/solver.cpp:72-74), with Config::getViscosityModel and getFluidMuConstant
+// (src/config.cpp:575-598). FluidReal's viscosity stays at its 2.0e-5 default
+// (include/fluid_real.hpp:168-171) unless the model is constant.
+void Solver::setupTransport() {
+    DevCaseT<double>& c = proto_;
+    c.viscous = 1;
+    const std::string raw = config_.has("FLUID_VISCOSITY_MODEL") ? config_.get("FLUID_VISCOSITY_MODEL") : "None";
+    bool constant;
+    if (raw == "None") {
+        constant = config_.has("FLUID_MU_CONSTANT") || config_.has("FLUID_CONSTANT_MU");
+    } else {
+        std::string key = raw;
+        std::transform(key.begin(), key.end(), key.begin(), [](unsigned char ch) { return std::tolower(ch); });
+        if (key == "sutherland") constant = false;
+        else if (key == "constant") constant = true;
+        else throw ConfigError("Unknown ViscosityModel: " + raw + ". Supported options: Sutherland, Constant.");
+    }
+    auto muConstant = [&]() {
+        if (config_.has("FLUID_MU_CONSTANT")) return config_.parseFloat("FLUID_MU_CONSTANT");
+        if (config_.has("FLUID_CONSTANT_MU")) return config_.parseFloat("FLUID_CONSTANT_MU");
+        if (config_.has("FLUID_SUTHERLAND_MU_REF")) return config_.parseFloat("FLUID_SUTHERLAND_MU_REF");
+        throw ConfigError("Missing constant viscosity value: please specify \"FLUID_MU_CONSTANT\" in configuration.");
+    };
+    c.visc_const = 1;
+    if (constant) {
+        c.mu_const = muConstant();
+    } else if (table_) {
+        c.mu_const = 2.0e-5;
+    } else {
+        c.visc_const = 0;
+        c.suth_mu = config_.parseFloat("FLUID_SUTHERLAND_MU_REF");
+        c.suth_T = config_.parseFloat("FLUID_SUTHERLAND_T_REF");
+        c.suth_S = config_.parseFloat("FLUID_SUTHERLAND_S");
+    }
+    c.vcp = config_.parseFloat("FLUID_CP");
+    c.vpr = config_.parseFloat("FLUID_PRANDTL_NUMBER");
+}
+
+// The nodes of every no-slip wall patch (Solver::buildBoundaryFluxes,
+// src/solver.cpp:369-388, with fetchBoundaryNodesIndexRange,
+// src/boundary_base.cpp:227-267). With viscosity on, the reference reads the
+// wall velocity from the patch's first three values at every iteration
+// (src/solver.cpp:3189-3203), so they must be there; walls at rest only.
+void Solver::buildWallMask() {
+    const long NI = mesh_.ni(), NJ = mesh_.nj(), NK = mesh_.nk();
+    wall_.clear();
+    for (const auto& b : boundaries_) {
+        if (b.type != kBcNoSlipWall) continue;
+        long i0 = b.i_min, i1 = b.i_max, j0 = b.j_min, j1 = b.j_max, k0 = b.k_min, k1 = b.k_max;
+        if (i0 == i1 && i0 == 0) i1 = 1;
+        else if (i0 == i1 && i0 == NI) { i0 = NI - 1; i1 = i0 + 1; }
+        else if (j0 == j1 && j0 == 0) j1 = 1;
+        else if (j0 == j1 && j0 == NJ) { j0 = NJ - 1; j1 = j0 + 1; }
+        else if (k0 == k1 && k0 == 0) k1 = 1;
+        else if (k0 == k1 && k0 == NK) { k0 = NK - 1; k1 = k0 + 1; }
+        else throw ConfigError("Invalid indexing on boundary condition specs for patch " + b.name);
+        if (!proto_.viscous) continue;
+        if (b.values.size() < 3)
+            throw ConfigError("no_slip_wall patch " + b.name + " needs the wall velocity (3 values) when VISCOSITY_ACTIVE");
+        if (b.values[0] != 0.0 || b.values[1] != 0.0 || b.values[2] != 0.0)
+            throw ConfigError("no_slip_wall patch " + b.name + ": moving walls are outside this library's scope");
+        if (wall_.empty()) wall_.assign(static_cast<size_t>(mesh_.nodes()), 0);
+        for (long i = std::max(i0, 0L); i < std::min(i1, NI); i++)
+            for (long j = std::max(j0, 0L); j < std::min(j1, NJ); j++)
+                for (long k = std::max(k0, 0L); k < std::min(k1, NK); k++) wall_[static_cast<size_t>(mesh_.idx(i, j, k))] = 1;
+    }
+    if (proto_.viscous && wall_.empty()) wall_.assign(static_cast<size_t>(mesh_.nodes()), 0);
 }
 
 // Solver::readBoundaryFile (src/solver.cpp:232-294).
@@ -557,6 +630,42 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
             nz[f] = S[f].z / m;
             ar[f] = m;
         }
+        if (c.viscous) {  // raw S and the Green-Gauss weights of the face's left and right node
+            std::vector<double> sx(S.size()), sy(S.size()), sz(S.size()), wl(S.size(), 0.0), wr(S.size(), 0.0);
+            const auto& C = mesh_.centers(d);
+            const auto& P = mesh_.vertices();
+            const long nfi = NI + (d == 0), nfj = NJ + (d == 1), nfk = NK + (d == 2);
+            const long nlast = d == 0 ? NI : (d == 1 ? NJ : NK);
+            const long st = d == 0 ? NJ * NK : (d == 1 ? NK : 1);
+            for (long fi = 0; fi < nfi; fi++)
+                for (long fj = 0; fj < nfj; fj++)
+                    for (long fk = 0; fk < nfk; fk++) {
+                        const long f = (fi * nfj + fj) * nfk + fk;
+                        sx[f] = S[f].x;
+                        sy[f] = S[f].y;
+                        sz[f] = S[f].z;
+                        const long df = d == 0 ? fi : (d == 1 ? fj : fk);
+                        if (df == 0 || df == nlast) continue;
+                        const long qr = mesh_.idx(fi, fj, fk), ql = qr - st;
+                        // computeGradientsGreenGauss4 (src/math_utils.cpp:270-353): w = d0 / (d0 + d1)
+                        // with d0 the face centre's distance to the node itself
+                        {
+                            const double d0 = (C[f] - P[qr]).magnitude(), d1 = (C[f] - P[ql]).magnitude();
+                            wr[f] = d0 / (d0 + d1);
+                        }
+                        {
+                            const double d0 = (C[f] - P[ql]).magnitude(), d1 = (C[f] - P[qr]).magnitude();
+                            wl[f] = d0 / (d0 + d1);
+                        }
+                    }
+            c.sraw[d][0] = inst.uploadR(sx);
+            c.sraw[d][1] = inst.uploadR(sy);
+            c.sraw[d][2] = inst.uploadR(sz);
+            c.gwL[d] = inst.uploadR(wl);
+            c.gwR[d] = inst.uploadR(wr);
+            if (d < 2 || topo_ == Topology::ThreeD)
+                for (int v = 0; v < 4; v++) c.V[d][v] = inst.allocR(S.size());
+        }
         c.f[d].nx = inst.uploadR(nx);
         c.f[d].ny = inst.uploadR(ny);
         c.f[d].nz = inst.uploadR(nz);
@@ -608,6 +717,12 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         c.vx = inst.uploadD(vx);
         c.vy = inst.uploadD(vy);
         c.vz = inst.uploadD(vz);
+    }
+    if (c.viscous) {  // no-slip wall nodes and the node gradients
+        void* d = inst.allocBytes(wall_.size());
+        cudaCheck(cudaMemcpy(d, wall_.data(), wall_.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+        c.wall = static_cast<const unsigned char*>(d);
+        for (int g = 0; g < 12; g++) c.G[g] = inst.allocR(N);
     }
     // boundary planes (raw surface vectors) for the surface integrals
     for (int b = 0; b < 6; b++) {
@@ -775,7 +890,7 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
     std::memset(hostCtl_, 0, sizeof(Control));
     cudaCheck(cudaMemcpy(inst.c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
     const double* in[5] = {U[0].data(), U[1].data(), U[2].data(), U[3].data(), U[4].data()};
-    setState(in);
+    uploadState(in);  // the plenum and the profiles start from the state before the wall preprocessing
     const HostGas gas{g, Rg};
     auto prim = [&](long q, double& rho, Vec3& u, double& et) {
         rho = U[0][q];
@@ -829,6 +944,7 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
         cudaCheck(cudaMemcpy(inst.c.prof_p, profP.data(), profP.size() * sizeof(double), cudaMemcpyHostToDevice),
                   "cudaMemcpy");
     }
+    if (proto_.viscous) setState(in);
     (void)grp;
 }
 
@@ -985,7 +1101,28 @@ void Solver::writeSolution(const std::string& path) {
     writeSolutionCsv(path, config_, mesh_, *hostFluid(), in);
 }
 
+// Solver::solve starts with preprocessSolution (src/solver.cpp:1323, :3189-3203):
+// with viscosity on, the momentum of every no-slip wall node becomes
+// density * 0 (walls at rest). Every iteration keeps it there, so doing it
+// whenever a state is set gives the reference's states.
 void Solver::setState(const double* const in[5]) {
+    if (!proto_.viscous) {
+        uploadState(in);
+        return;
+    }
+    const long N = mesh_.nodes();
+    std::array<std::vector<double>, 3> mom;
+    const double* u[5] = {in[0], nullptr, nullptr, nullptr, in[4]};
+    for (int v = 0; v < 3; v++) {
+        mom[v].assign(in[v + 1], in[v + 1] + N);
+        for (long q = 0; q < N; q++)
+            if (wall_[static_cast<size_t>(q)]) mom[v][q] = in[0][q] * 0.0;
+        u[v + 1] = mom[v].data();
+    }
+    uploadState(u);
+}
+
+void Solver::uploadState(const double* const in[5]) {
     const long N = mesh_.nodes();
     visit([&](auto& inst, auto&) {
         using R = std::remove_reference_t<decltype(*inst.c.U[0])>;

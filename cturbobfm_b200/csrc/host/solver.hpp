@@ -95,6 +95,11 @@ private:
     void buildBoundaryStructures();
     void setupScalars();
     void setupModels();
+    void setupTransport();
+    void buildWallMask();
+    // copies a state to the device as it is (setState adds the no-slip wall
+    // preprocessing of viscous runs)
+    void uploadState(const double* const in[5]);
     void validateSettings();
     template <typename R>
     void uploadArrays(InstanceT<R>& inst);
@@ -123,6 +128,7 @@ private:
     double periodicAngleDeg_ = 0.0, periodicAngleRad_ = 0.0, periodicTransl_ = 0.0;
     DevCaseT<double> proto_{};  // scalar settings shared by both precisions
     std::vector<signed char> mapI_, mapJ_, mapK_;
+    std::vector<unsigned char> wall_;  // viscous runs: 1 on no-slip wall nodes
     std::vector<double> profP_, profR_;
 
     std::unique_ptr<InstanceT<double>> i64_;
