@@ -10,7 +10,7 @@
 namespace ctbfm {
 
 void writeSolutionCsv(const std::string& path, const Config& config, const Mesh& mesh, const HostFluid& fluid,
-                      const double* const U[5]) {
+                      const double* const U[5], const std::map<std::string, std::vector<double>>* extra) {
     // Config::getOutputFieldsType (src/config.cpp:629-647)
     const std::string t = config.has("OUTPUT_FIELDS_TYPE") ? config.get("OUTPUT_FIELDS_TYPE") : "None";
     const bool primaryOnly = t == "primary" || t == "Primary" || t == "PRIMARY";
@@ -57,6 +57,9 @@ void writeSolutionCsv(const std::string& path, const Config& config, const Mesh&
             s[q] = fluid.entropy_rho_u_et(rho[q], u, et[q]);
         }
     }
+
+    if (extra)
+        for (const auto& kv : *extra) fields[kv.first] = kv.second;
 
     std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path.c_str(), "w"), &std::fclose);
     if (!f) throw std::runtime_error("Failed to open file: " + path);

@@ -12,7 +12,9 @@
 // reference.
 #pragma once
 
+#include <map>
 #include <string>
+#include <vector>
 
 #include "config.hpp"
 #include "host_fluid.hpp"
@@ -22,8 +24,10 @@ namespace ctbfm {
 
 // Throws ConfigError for OUTPUT_FIELDS_TYPE = turbo_bfm on a body-force case
 // (its force and deviation-angle fields are not kept by this library) and
-// std::runtime_error when the file cannot be written.
+// std::runtime_error when the file cannot be written. `extra` adds named
+// node fields (the viscous fields of Output::updateViscousFields,
+// src/output.cpp:240-306) to the sorted set.
 void writeSolutionCsv(const std::string& path, const Config& config, const Mesh& mesh, const HostFluid& fluid,
-                      const double* const U[5]);
+                      const double* const U[5], const std::map<std::string, std::vector<double>>* extra = nullptr);
 
 }  // namespace ctbfm

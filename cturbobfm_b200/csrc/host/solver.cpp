@@ -722,7 +722,10 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         void* d = inst.allocBytes(wall_.size());
         cudaCheck(cudaMemcpy(d, wall_.data(), wall_.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
         c.wall = static_cast<const unsigned char*>(d);
-        for (int g = 0; g < 12; g++) c.G[g] = inst.allocR(N);
+        for (int g = 0; g < 12; g++) {
+            c.G[g] = inst.allocR(N);
+            cudaCheck(cudaMemset(c.G[g], 0, N * sizeof(R)), "cudaMemset");
+        }
     }
     // boundary planes (raw surface vectors) for the surface integrals
     for (int b = 0; b < 6; b++) {
@@ -1098,7 +1101,126 @@ void Solver::writeSolution(const std::string& path) {
     }
     getState(out);
     const double* in[5] = {out[0], out[1], out[2], out[3], out[4]};
-    writeSolutionCsv(path, config_, mesh_, *hostFluid(), in);
+    if (!proto_.viscous) {
+        writeSolutionCsv(path, config_, mesh_, *hostFluid(), in);
+        return;
+    }
+    std::map<std::string, std::vector<double>> extra;
+    viscousOutputFields(in, extra);
+    writeSolutionCsv(path, config_, mesh_, *hostFluid(), in, &extra);
+}
+
+// Output::updateViscousFields (src/output.cpp:240-306) with
+// computeWallShearStress (:308-367): molecular viscosity of every node's
+// temperature, eddy viscosity 0 (no turbulence model), and on the nodes of
+// each no-slip wall (patch order; a later patch overwrites a shared node)
+// the wall shear stress from the latest stage's velocity gradients and
+// y+ = sqrt(|tau_w| rho) d / mu, d the wall-distance step to the next node
+// off the wall (Solver::computeWallDistance, src/solver.cpp:657-700: the
+// smallest node-to-node distance to any no-slip wall). Before the first
+// iteration the gradients are zero (the reference has its start-up
+// gradients there).
+void Solver::viscousOutputFields(const double* const U[5], std::map<std::string, std::vector<double>>& out) {
+    const long N = mesh_.nodes(), NI = mesh_.ni(), NJ = mesh_.nj(), NK = mesh_.nk();
+    const auto fluid = hostFluid();
+    const DevCaseT<double>& c = proto_;
+    auto mu = [&](double T) {  // FluidIdeal / FluidReal::computeMolecularDynamicViscosity
+        if (c.visc_const) return c.mu_const;
+        return c.suth_mu * std::pow(T / c.suth_T, 1.5) * ((c.suth_T + c.suth_S) / (T + c.suth_S));
+    };
+    auto& muL = out["Molecular Viscosity"];
+    out["Eddy Viscosity"].assign(static_cast<size_t>(N), 0.0);
+    auto& wx = out["Wall Shear Stress X"];
+    auto& wy = out["Wall Shear Stress Y"];
+    auto& wz = out["Wall Shear Stress Z"];
+    auto& yp = out["Y Plus"];
+    muL.resize(static_cast<size_t>(N));
+    for (auto* a : {&wx, &wy, &wz, &yp}) a->assign(static_cast<size_t>(N), 0.0);
+    for (long q = 0; q < N; q++) {
+        const Vec3 u(U[1][q] / U[0][q], U[2][q] / U[0][q], U[3][q] / U[0][q]);
+        muL[q] = mu(fluid->temperature_rho_u_et(U[0][q], u, U[4][q] / U[0][q]));
+    }
+    std::array<std::vector<double>, 12> G;
+    visit([&](auto& inst, auto&) {
+        using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+        std::vector<R> tmp(static_cast<size_t>(N));
+        for (int g = 0; g < 12; g++) {
+            cudaCheck(cudaMemcpyAsync(tmp.data(), inst.c.G[g], N * sizeof(R), cudaMemcpyDeviceToHost, stream_),
+                      "cudaMemcpyAsync");
+            cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+            G[g].assign(tmp.begin(), tmp.end());
+        }
+    });
+    struct Range { long i0, i1, j0, j1, k0, k1; };
+    std::vector<std::pair<const BoundaryPatch*, Range>> walls;
+    for (const auto& b : boundaries_) {
+        if (b.type != kBcNoSlipWall) continue;
+        Range r{b.i_min, b.i_max, b.j_min, b.j_max, b.k_min, b.k_max};
+        if (r.i0 == r.i1 && r.i0 == 0) r.i1 = 1;
+        else if (r.i0 == r.i1 && r.i0 == NI) { r.i0 = NI - 1; r.i1 = NI; }
+        else if (r.j0 == r.j1 && r.j0 == 0) r.j1 = 1;
+        else if (r.j0 == r.j1 && r.j0 == NJ) { r.j0 = NJ - 1; r.j1 = NJ; }
+        else if (r.k0 == r.k1 && r.k0 == 0) r.k1 = 1;
+        else { r.k0 = NK - 1; r.k1 = NK; }  // buildWallMask has checked the indices
+        walls.push_back({&b, r});
+    }
+    const auto& P = mesh_.vertices();
+    std::map<long, double> memo;
+    auto wallDistance = [&](long q) {
+        const auto hit = memo.find(q);
+        if (hit != memo.end()) return hit->second;
+        double best = 1.0E9;
+        for (const auto& w : walls) {
+            double m = 1.0E9;
+            for (long i = w.second.i0; i < w.second.i1; i++)
+                for (long j = w.second.j0; j < w.second.j1; j++)
+                    for (long k = w.second.k0; k < w.second.k1; k++) {
+                        const Vec3& b = P[mesh_.idx(i, j, k)];
+                        const double dx = P[q].x - b.x, dy = P[q].y - b.y, dz = P[q].z - b.z;
+                        const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+                        if (d < m) m = d;
+                    }
+            if (m < best) best = m;
+        }
+        memo[q] = best;
+        return best;
+    };
+    for (const auto& w : walls) {
+        const BoundaryPatch& b = *w.first;
+        const int o = b.orientation;
+        const long si = o == 0 ? 1 : (o == 1 ? -1 : 0), sj = o == 2 ? 1 : (o == 3 ? -1 : 0),
+                   sk = o == 4 ? 1 : (o == 5 ? -1 : 0);
+        for (long i = w.second.i0; i < w.second.i1; i++)
+            for (long j = w.second.j0; j < w.second.j1; j++)
+                for (long k = w.second.k0; k < w.second.k1; k++) {
+                    const long q = mesh_.idx(i, j, k);
+                    const Vec3 gu(G[0][q], G[1][q], G[2][q]), gv(G[3][q], G[4][q], G[5][q]), gw(G[6][q], G[7][q], G[8][q]);
+                    const double me = muL[q] + 0.0;
+                    const double lam = -2.0 * me / 3.0;
+                    const double xx = lam * (gu.x + gv.y + gw.z) + 2.0 * me * gu.x;
+                    const double yy = lam * (gu.x + gv.y + gw.z) + 2.0 * me * gv.y;
+                    const double zz = lam * (gu.x + gv.y + gw.z) + 2.0 * me * gw.z;
+                    const double xy = me * (gu.y + gv.x), xz = me * (gu.z + gw.x), yz = me * (gv.z + gw.y);
+                    Vec3 s;
+                    switch (o) {
+                        case 0: s = mesh_.surfaces(0)[mesh_.faceIdx(0, 0, j, k)]; break;
+                        case 1: s = -mesh_.surfaces(0)[mesh_.faceIdx(0, b.i_max, j, k)]; break;
+                        case 2: s = mesh_.surfaces(1)[mesh_.faceIdx(1, i, 0, k)]; break;
+                        case 3: s = -mesh_.surfaces(1)[mesh_.faceIdx(1, i, b.j_max, k)]; break;
+                        case 4: s = mesh_.surfaces(2)[mesh_.faceIdx(2, i, j, 0)]; break;
+                        default: s = -mesh_.surfaces(2)[mesh_.faceIdx(2, i, j, b.k_max)]; break;
+                    }
+                    const double sm = s.magnitude();
+                    s = (sm == 0.0) ? Vec3(0, 0, 0) : s / sm;  // Vector3D::normalized
+                    Vec3 t(xx * s.x + xy * s.y + xz * s.z, xy * s.x + yy * s.y + yz * s.z, xz * s.x + yz * s.y + zz * s.z);
+                    t = t - s * t.dot(s);
+                    wx[q] = t.x;
+                    wy[q] = t.y;
+                    wz[q] = t.z;
+                    const double d = wallDistance(mesh_.idx(i + si, j + sj, k + sk)) - wallDistance(q);
+                    yp[q] = std::sqrt(t.magnitude() * U[0][q]) * d / muL[q];
+                }
+    }
 }
 
 // Solver::solve starts with preprocessSolution (src/solver.cpp:1323, :3189-3203):

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -97,6 +98,7 @@ private:
     void setupModels();
     void setupTransport();
     void buildWallMask();
+    void viscousOutputFields(const double* const U[5], std::map<std::string, std::vector<double>>& out);
     // copies a state to the device as it is (setState adds the no-slip wall
     // preprocessing of viscous runs)
     void uploadState(const double* const in[5]);

@@ -13,7 +13,8 @@ source nodes, so the fixtures also pin how the nearest-neighbour search
 resolves equal distances.
 
 Output fixtures: the reference's volume CSV of a small case after a few
-iterations, with the state it was written from.
+iterations, with the state it was written from (two of them viscous, with
+the viscosity, wall shear stress and y+ columns).
 
 Each <name>.npz holds the target case (coordinates, grid fields, patches and
 settings as JSON), the restart file text, and the reference's results.
@@ -91,6 +92,14 @@ def output_fixture(name, case, n_iter, fields):
     print(name, case.shape, fields, flush=True)
 
 
+def viscous(case, mu):
+    """Laminar viscous run with the J-face walls as no-slip walls at rest."""
+    for m in (2, 3):
+        case.patches[m] = dataclasses.replace(case.patches[m], spec="no_slip_wall, 0, 0, 0")
+    return case.with_settings(VISCOSITY_ACTIVE="yes", FLUID_CP="1004.675", FLUID_PRANDTL_NUMBER="0.72",
+                              FLUID_MU_CONSTANT=repr(mu))
+
+
 def main():
     bump = cases.bump2d(ni=24, nj=10, name="bump_src")
     restart_fixture("bump_standard", bump, 40, cases.bump2d(ni=24, nj=10, name="bump_same"), None, 10)
@@ -108,6 +117,10 @@ def main():
     output_fixture("output_bump_secondary", cases.bump2d(ni=24, nj=10, name="bump_out"), 20, "secondary")
     output_fixture("output_meridional_primary", cases.meridional(ni=16, nj=7, rows=cases.MAP_ROWS, name="mer_out"),
                    20, "primary")
+    output_fixture("output_bump_viscous", viscous(cases.bump2d(ni=24, nj=10, name="bump_visc"), 0.02), 20, "secondary")
+    sector = cases.annulus3d(ni=16, nj=7, nk=5, scheme="JST", muscl=False, rk=4, bfm_model="None", name="ann_visc")
+    sector = sector.with_settings(BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no")
+    output_fixture("output_annulus_viscous_primary", viscous(sector, 0.01), 10, "primary")
 
 
 if __name__ == "__main__":
