@@ -5,7 +5,7 @@ local time step at CFL 1.0 -- the configuration's 1.2 diverges at iteration
 arm beside it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload annulus|map|serve|realgas]
+                    [--workload annulus|map|serve|realgas|viscous]
 
 One step = one pseudo-time iteration (all Runge-Kutta stages) of the whole
 operating point. The metric is cell-stage updates per second (nodes x stages x
@@ -624,6 +624,77 @@ REALGAS_WORKLOAD = ("real-gas CO2 annulus 256x96x128 (3.1M nodes), synthetic van
                     "CFL 1.0; fp32_kahan bulk with FP64 table inversions")
 
 
+VISCOUS_WORKLOAD = ("laminar viscous annulus duct 160x48x64 (491520 nodes, no blade rows), hub and shroud no-slip "
+                    "walls, Sutherland air, Roe+MUSCL(van albada), RK3, CFL 1.2; the same duct with inviscid walls "
+                    "timed beside it")
+
+
+def run_viscous(args):
+    """The viscous path: the duct with no-slip walls against the same duct
+    with inviscid walls (FP64 and fp32_kahan), device-timed with CUDA events
+    on the solver's stream. The per-stage time difference is the cost of the
+    viscous kernels (k_grad, three k_vfaces) plus the viscous terms of
+    k_nodes / k_dt; its roofline fraction counts only the two new kernels'
+    algorithmic bytes, so it is a lower bound for them."""
+    import torch
+
+    from cturbobfm_b200 import Solver, cases
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    tmp = tempfile.TemporaryDirectory()
+    stream = torch.cuda.Stream()
+    arms = {}
+    with ClockSampler(local) as clocks:
+        for prec in ("fp64", "fp32_kahan"):
+            for visc in (True, False):
+                c = cases.viscous_annulus(precision=prec, viscous=visc)
+                ini = c.write(os.path.join(tmp.name, f"{prec}_{visc}"))
+                with Solver(ini) as s:
+                    s.set_stream(stream.cuda_stream)
+                    s.enqueue(args.warmup)
+                    stream.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    torch.cuda.synchronize()
+                    e0.record(stream)
+                    s.enqueue(args.steps)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    ms = e0.elapsed_time(e1)
+                    if s.status != 0:
+                        raise RuntimeError(f"viscous workload stopped (status {s.status})")
+                    arms[(prec, visc)] = {"ms": ms / args.steps, "n": c.n_nodes, "stages": c.n_stages,
+                                          "bytes": int(s.info().device_bytes)}
+    clk = clocks.summary()
+    a = arms[("fp64", True)]
+    n, st, K = a["n"], a["stages"], args.steps
+    ni, nj, nk = 160, 48, 64
+    nf = (ni + 1) * nj * nk + ni * (nj + 1) * nk + ni * nj * (nk + 1)
+    # k_grad 8*(5N + 9N + 6N + N + 12N) + k_vfaces 8*(3*(5N + 12N) + 8F) bytes per stage (FP64)
+    alg = 8 * (33 * n) + 8 * (3 * 17 * n + 8 * nf)
+    extra_s = (a["ms"] - arms[("fp64", False)]["ms"]) / st / 1e3
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_kind = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = alg / extra_s / 1e9 if extra_s > 0 else None
+    line = {
+        "metric": METRIC, "value": n * st / (a["ms"] / 1e3), "unit": UNIT, "n_gpus": 1, "steps": K,
+        "warmup": args.warmup, "ms_per_step": a["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": VISCOUS_WORKLOAD, "nodes": n, "stages_per_step": st,
+                   "l2": f"inputs larger than L2: device working set {a['bytes'] / 2**20:.0f} MiB > 126 MiB"},
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "inviscid_duct_fp64": {"ms_per_step": arms[("fp64", False)]["ms"]},
+        "fp32_kahan": {"viscous_ms_per_step": arms[("fp32_kahan", True)]["ms"],
+                       "inviscid_ms_per_step": arms[("fp32_kahan", False)]["ms"]},
+        "viscous_terms_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
+                                   "algorithmic_bytes_per_stage": alg,
+                                   "note": "k_grad + k_vfaces bytes over the viscous-minus-inviscid stage time"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_realgas(args):
     import numpy as np
     import torch
@@ -806,7 +877,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["annulus", "map", "serve", "realgas"], default="annulus",
+    ap.add_argument("--workload", choices=["annulus", "map", "serve", "realgas", "viscous"], default="annulus",
                     help="annulus: the 160x48x64 full-annulus loop (default); map: the batched compressor map; "
                          "serve: continuous batching of arriving requests")
     ap.add_argument("--map-n", type=int, default=256)
@@ -834,6 +905,8 @@ def main():
         run_serve(args)
     elif args.workload == "realgas":
         run_realgas(args)
+    elif args.workload == "viscous":
+        run_viscous(args)
     else:
         run_ours(args)
 

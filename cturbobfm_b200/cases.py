@@ -518,6 +518,25 @@ def realgas_annulus(ni: int = 256, nj: int = 96, nk: int = 128, n_iter: int = 10
     return with_real_gas(c, pt=8.0e6, tt=310.0, p_init=7.6e6, t_init=305.0, p_out=p_out, table=table)
 
 
+def viscous_annulus(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 10000,
+                    precision: Optional[str] = None, viscous: bool = True) -> Case:
+    """The laminar viscous workload: the annulus3d duct (hub 0.20 m, tip
+    0.40 m, length 0.6 m, 360 degree periodic; Roe + MUSCL van Albada, RK3,
+    CFL 1.2) without blade rows, hub and shroud as no-slip walls at rest,
+    Sutherland's law for air (mu_ref 1.716e-5 Pa s at 273.15 K, S 110.4 K),
+    cp 1004.675 J/(kg K), Pr 0.72. ``viscous=False`` gives the same duct with
+    inviscid walls (the baseline of the viscous terms' cost)."""
+    c = annulus3d(ni=ni, nj=nj, nk=nk, n_iter=n_iter, bfm_model="None", precision=precision, name="viscous_annulus")
+    c = c.with_settings(BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no")
+    if not viscous:
+        return c
+    for m in (2, 3):
+        c.patches[m] = dataclasses.replace(c.patches[m], spec="no_slip_wall, 0, 0, 0")
+    return c.with_settings(VISCOSITY_ACTIVE="yes", FLUID_VISCOSITY_MODEL="Sutherland",
+                           FLUID_SUTHERLAND_MU_REF="1.716e-5", FLUID_SUTHERLAND_T_REF="273.15",
+                           FLUID_SUTHERLAND_S="110.4", FLUID_CP="1004.675", FLUID_PRANDTL_NUMBER="0.72")
+
+
 def read_grid_csv(path: str) -> Tuple[Tuple[int, int, int], Dict[str, np.ndarray]]:
     """Reads a grid CSV in the reference's format (src/input.cpp:14-82)."""
     ni = nj = nk = None
