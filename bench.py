@@ -624,8 +624,8 @@ REALGAS_WORKLOAD = ("real-gas CO2 annulus 256x96x128 (3.1M nodes), synthetic van
                     "CFL 1.0; fp32_kahan bulk with FP64 table inversions")
 
 
-VISCOUS_WORKLOAD = ("laminar viscous annulus duct 160x48x64 (491520 nodes, no blade rows), hub and shroud no-slip "
-                    "walls, Sutherland air, Roe+MUSCL(van albada), RK3, CFL 1.2; the same duct with inviscid walls "
+VISCOUS_WORKLOAD = ("laminar viscous annulus duct 160x48x64 (491520 nodes, no blade rows), outlet 0.95 pt, hub and "
+                    "shroud no-slip walls, Sutherland air, Roe+MUSCL(van albada), RK3, CFL 1.2; the same duct with inviscid walls "
                     "timed beside it")
 
 

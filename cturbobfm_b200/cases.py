@@ -522,11 +522,13 @@ def viscous_annulus(ni: int = 160, nj: int = 48, nk: int = 64, n_iter: int = 100
                     precision: Optional[str] = None, viscous: bool = True) -> Case:
     """The laminar viscous workload: the annulus3d duct (hub 0.20 m, tip
     0.40 m, length 0.6 m, 360 degree periodic; Roe + MUSCL van Albada, RK3,
-    CFL 1.2) without blade rows, hub and shroud as no-slip walls at rest,
+    CFL 1.2) without blade rows, static outlet at 0.95 of the inlet total
+    pressure, hub and shroud as no-slip walls at rest,
     Sutherland's law for air (mu_ref 1.716e-5 Pa s at 273.15 K, S 110.4 K),
     cp 1004.675 J/(kg K), Pr 0.72. ``viscous=False`` gives the same duct with
     inviscid walls (the baseline of the viscous terms' cost)."""
-    c = annulus3d(ni=ni, nj=nj, nk=nk, n_iter=n_iter, bfm_model="None", precision=precision, name="viscous_annulus")
+    c = annulus3d(ni=ni, nj=nj, nk=nk, n_iter=n_iter, bfm_model="None", p_ratio=0.95, precision=precision,
+                  name="viscous_annulus")
     c = c.with_settings(BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no")
     if not viscous:
         return c
