@@ -625,7 +625,7 @@ REALGAS_WORKLOAD = ("real-gas CO2 annulus 256x96x128 (3.1M nodes), synthetic van
 
 
 VISCOUS_WORKLOAD = ("laminar viscous annulus duct 160x48x64 (491520 nodes, no blade rows), outlet 0.95 pt, hub and "
-                    "shroud no-slip walls, Sutherland air, Roe+MUSCL(van albada), RK3, CFL 1.2; the same duct with inviscid walls "
+                    "shroud no-slip walls, Sutherland air, JST, RK4, CFL 1.2; the same duct with inviscid walls "
                     "timed beside it")
 
 
