@@ -323,12 +323,14 @@ __global__ void __launch_bounds__(256) k_grad(const DevCaseT<R>* cases, const Ti
 }
 
 // Solver::computeViscousFluxResiduals (src/solver.cpp:2060-2171): one thread
-// per face of direction DIR in storage order; interior faces write
+// per face of direction DIR in storage order (3 blocks of 256 per SM: 80
+// registers with a few spills, 3 % faster in FP64 and 12 % in float than 90
+// registers at 2 blocks on the viscous duct); interior faces write
 // flux * |S| of the momentum and energy equations from the averaged node
 // states and gradients (boundary faces carry no viscous flux and are not
 // read).
 template <int DIR, typename R, int FL>
-__global__ void __launch_bounds__(256) k_vfaces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+__global__ void __launch_bounds__(256, 3) k_vfaces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
