@@ -125,3 +125,39 @@ def test_real_gas_table_errors_come_back_as_config_errors(lib, tmp_path):
     ini = c.with_settings(STOP_ON_TABLE_OUT_OF_BOUNDS="yes").write(str(tmp_path / "b"))
     assert lib.ctbfm_create_from_ini(ini.encode(), ctypes.byref(h)) == 1
     assert b"STOP_ON_TABLE_OUT_OF_BOUNDS" in lib.ctbfm_last_error()
+
+
+def _viscous_bump(walls="no_slip_wall, 0, 0, 0", **settings):
+    import dataclasses
+
+    from cturbobfm_b200 import cases
+
+    c = cases.bump2d(ni=12, nj=6)
+    for m in (2, 3):
+        c.patches[m] = dataclasses.replace(c.patches[m], spec=walls)
+    kw = dict(VISCOSITY_ACTIVE="yes", FLUID_MU_CONSTANT="1e-3", FLUID_CP="1004.675", FLUID_PRANDTL_NUMBER="0.72")
+    kw.update(settings)
+    return c.with_settings(**{k: v for k, v in kw.items() if v is not None})
+
+
+@pytest.mark.parametrize("walls,settings,message", [
+    ("no_slip_wall, 0, 0, 0", {"TURBULENCE_ACTIVE": "yes"}, "Spalart-Allmaras"),
+    ("no_slip_wall, 0, 0, 0", {"FLUID_VISCOSITY_MODEL": "Power"}, "Unknown ViscosityModel: Power"),
+    ("no_slip_wall, 0, 0, 0", {"FLUID_CP": None}, "Not found value for key \"FLUID_CP\""),
+    ("no_slip_wall, 0, 0, 0", {"FLUID_PRANDTL_NUMBER": None}, "Not found value for key \"FLUID_PRANDTL_NUMBER\""),
+    ("no_slip_wall, 0, 0, 0", {"FLUID_VISCOSITY_MODEL": "Sutherland", "FLUID_MU_CONSTANT": None},
+     "Not found value for key \"FLUID_SUTHERLAND_MU_REF\""),
+    ("no_slip_wall, 0, 0, 0", {"FLUID_VISCOSITY_MODEL": "Constant", "FLUID_MU_CONSTANT": None},
+     "Missing constant viscosity value"),
+    ("no_slip_wall", {}, "needs the wall velocity"),
+    ("no_slip_wall, 10, 0, 0", {}, "moving walls"),
+])
+def test_viscous_settings_are_checked_before_device_work(lib, tmp_path, walls, settings, message):
+    """Viscous runs: the transport keys and the no-slip walls are read with
+    the reference's keys and messages when the solver is created, before any
+    device call."""
+    ini = _viscous_bump(walls, **settings).write(str(tmp_path))
+    h = ctypes.c_void_p()
+    rc = lib.ctbfm_create_from_ini(ini.encode(), ctypes.byref(h))
+    assert rc == 1
+    assert message.encode() in lib.ctbfm_last_error()

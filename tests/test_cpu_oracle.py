@@ -99,3 +99,23 @@ def test_viscous_blade_rows_diverge_at_the_first_iteration_like_the_reference(tm
     if oracle_lib.ref_available():
         assert oracle_lib.ref_harness("steps", ini, 5)["converged"] == 2
         assert np.array_equal(np.isnan(oracle_lib.ref_harness("residual", ini)["residual"]), bad)
+
+
+def test_no_slip_wall_without_viscosity_is_an_inviscid_wall(tmp_path, oracle_lib):
+    """Without VISCOSITY_ACTIVE the reference builds an inviscid-wall flux for
+    a no_slip_wall patch and never touches its nodes."""
+    import dataclasses
+    from cturbobfm_b200 import cases
+
+    base = cases.bump2d(ni=24, nj=12)
+    ns = cases.bump2d(ni=24, nj=12)
+    for m in (2, 3):
+        ns.patches[m] = dataclasses.replace(ns.patches[m], spec="no_slip_wall")
+    a = oracle_lib.Oracle(base.write(str(tmp_path / "a")))
+    ini = ns.write(str(tmp_path / "b"))
+    b = oracle_lib.Oracle(ini)
+    a.run(10)
+    b.run(10)
+    assert np.array_equal(a.state(), b.state())
+    if oracle_lib.ref_available():
+        assert np.array_equal(oracle_lib.ref_harness("steps", ini, 10)["state"], b.state())
