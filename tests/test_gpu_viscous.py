@@ -74,3 +74,22 @@ def test_viscous_channel_converges_like_the_oracle(tmp_path, oracle_lib):
     # no-slip: zero momentum on the wall nodes (j = 0 and j = nj - 1)
     m = u[1:4].reshape(3, 24, 12)
     assert np.all(m[:, :, 0] == 0.0) and np.all(m[:, :, -1] == 0.0)
+
+
+def test_no_slip_wall_without_viscosity_matches_the_inviscid_wall(tmp_path):
+    """Without VISCOSITY_ACTIVE a no_slip_wall patch is an inviscid wall, as
+    in the reference: the same states bit for bit."""
+    import dataclasses
+
+    from cturbobfm_b200 import Solver
+
+    base = cases.bump2d(ni=40, nj=16)
+    ns = cases.bump2d(ni=40, nj=16)
+    for m in (2, 3):
+        ns.patches[m] = dataclasses.replace(ns.patches[m], spec="no_slip_wall")
+    out = []
+    for k, c in enumerate((base, ns)):
+        with Solver(c.write(str(tmp_path / str(k)))) as s:
+            assert s.step(50) == 50
+            out.append(s.state())
+    assert np.array_equal(out[0], out[1])
