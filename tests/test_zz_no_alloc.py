@@ -24,7 +24,9 @@ def rel_err(a, b):
 
 
 @pytest.mark.parametrize("make", [lambda: cases.bump2d(ni=48, nj=24),
-                                  lambda: cases.annulus3d(ni=20, nj=8, nk=9)], ids=["bump2d", "annulus3d"])
+                                  lambda: cases.annulus3d(ni=20, nj=8, nk=9),
+                                  lambda: cases.viscous_annulus(ni=20, nj=8, nk=9)],
+                         ids=["bump2d", "annulus3d", "viscous_annulus"])
 def test_noalloc_residual_matches_allocating_entry_point(make, tmp_path):
     from cturbobfm_b200 import Solver
 
