@@ -76,8 +76,9 @@ constexpr int kTileSize = 256;  // elements per tile (one per thread)
 constexpr int kPeriodicTile = 64;
 
 // Static device scratch of ctbfm_compute_residual_noalloc (noalloc.cu): its
-// device address on the current device (looked up once per device) and size.
+// device address on device dev, which must be current (looked up once per
+// device), and its size.
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
-cudaError_t noallocScratch(double** ptr, size_t* bytes);
+cudaError_t noallocScratch(int dev, double** ptr, size_t* bytes);
 
 }  // namespace ctbfm

@@ -9,9 +9,14 @@
 // file-scope array below instead of in memory the solver allocates.
 //
 // Limits and sharing rules:
-//   * the array holds kNoAllocScratchBytes (16 MiB), i.e. 5 doubles for at most
-//     419430 faces summed over the swept directions; larger cases are rejected;
-//   * every GPU that loads the library holds the array until the process exits;
+//   * the array holds kNoAllocScratchBytes (16 MiB), i.e. 5 words per face for
+//     at most 419430 faces summed over the swept directions in FP64 and
+//     838860 in fp32_kahan; larger cases are rejected;
+//   * every GPU on which a solver is created holds the array until the
+//     process exits: with lazy module loading (CUDA_MODULE_LOADING=LAZY, the
+//     CUDA 12 default) the driver backs the array when its address is first
+//     looked up, so the solver constructor does that look-up, and the
+//     no-allocation entry point itself never triggers the reservation;
 //   * all calls on a device share the one array, which keeps the last call's
 //     contents; nothing in it has to start at zero, because each call writes
 //     every slot it later reads;
@@ -21,8 +26,8 @@
 // The array's name in host code is a host-side stand-in, not a device address:
 // host code obtains the device address once per device with
 // cudaGetSymbolAddress (with that device current) and passes it to the kernels.
-// The first call of the entry point on a device performs that set-up, so it
-// should come before any stream capture.
+// Creating a solver performs that set-up for the solver's device, before any
+// stream capture the caller may start.
 
 #include <cuda_runtime.h>
 
@@ -40,11 +45,12 @@ std::mutex g_scratchMutex;
 double* g_scratchAddress[kMaxDevices] = {};
 }  // namespace
 
-cudaError_t noallocScratch(double** ptr, size_t* bytes) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
+cudaError_t noallocScratch(int dev, double** ptr, size_t* bytes) {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    if (cur != dev) return cudaErrorInvalidDevice;  // the look-up must run with dev current
     std::lock_guard<std::mutex> lock(g_scratchMutex);
     if (!g_scratchAddress[dev]) {
         void* p = nullptr;

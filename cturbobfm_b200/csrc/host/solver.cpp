@@ -149,8 +149,17 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     buildWallMask();
     validateSettings();
     setupScalars();
+    cudaCheck(cudaGetDevice(&device_), "cudaGetDevice");
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = ownStream_;
+    // back the static scratch of computeResidualNoAlloc on this device now
+    // (under lazy module loading the driver reserves it at the first address
+    // look-up), so that the no-allocation entry point never reserves memory
+    {
+        double* scratch = nullptr;
+        size_t bytes = 0;
+        cudaCheck(noallocScratch(device_, &scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
+    }
     cudaCheck(cudaMallocHost(reinterpret_cast<void**>(&hostCtl_), sizeof(Control)), "cudaMallocHost");
     std::memset(hostCtl_, 0, sizeof(Control));
     if (prec_ == kFP32Kahan) {
@@ -1027,10 +1036,22 @@ void Solver::computeResidual(double* dt, double* const r[5]) {
 // The residual evaluation of computeResidual with its per-face flux
 // contributions kept in the static scratch array of noalloc.cu; nothing is
 // allocated on the device (the caller cannot, or must not, call cudaMalloc).
+// Runs on the solver's own device (restoring the caller's current device on
+// return) and always points the solver back at its own face buffers, also
+// when an error is thrown.
 void Solver::computeResidualNoAlloc(double* dt, double* const r[5]) {
+    int callerDevice = -1;
+    cudaCheck(cudaGetDevice(&callerDevice), "cudaGetDevice");
+    if (callerDevice != device_) cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    struct DeviceGuard {
+        int dev, own;
+        ~DeviceGuard() {
+            if (dev != own) cudaSetDevice(dev);
+        }
+    } deviceGuard{callerDevice, device_};
     double* scratch = nullptr;
     size_t bytes = 0;
-    cudaCheck(noallocScratch(&scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
+    cudaCheck(noallocScratch(device_, &scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
     const long N = mesh_.nodes();
     visit([&](auto& inst, auto& grp) {
         using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
@@ -1041,10 +1062,29 @@ void Solver::computeResidualNoAlloc(double* dt, double* const r[5]) {
             throw ConfigError("ctbfm_compute_residual_noalloc: the case has " + std::to_string(faces) +
                               " faces and needs " + std::to_string(faces * 5 * sizeof(R)) +
                               " bytes of face scratch; the static array holds " + std::to_string(bytes) +
-                              " bytes (at most " + std::to_string(bytes / (5 * sizeof(R))) + " faces)");
-        const DevFacesT<R> saved[3] = {inst.c.f[0], inst.c.f[1], inst.c.f[2]};
+                              " bytes (at most " + std::to_string(bytes / (5 * sizeof(R))) + " faces in " +
+                              (sizeof(R) == 8 ? "fp64" : "fp32_kahan") + ")");
+        // restores the solver's own face buffers on every exit: a solver left
+        // pointing at the shared array would race with other callers' noalloc
+        // evaluations and could write past the array in its next step
+        struct FaceGuard {
+            decltype(inst)& in;
+            decltype(grp)& g;
+            cudaStream_t st;
+            DevFacesT<R> saved[3];
+            bool active = false;
+            ~FaceGuard() {
+                if (!active) return;
+                for (int d = 0; d < 3; d++) in.c.f[d] = saved[d];
+                try {
+                    g.refresh(st);
+                } catch (...) {
+                }
+            }
+        } guard{inst, grp, stream_, {inst.c.f[0], inst.c.f[1], inst.c.f[2]}};
         R* base = reinterpret_cast<R*>(scratch);
         size_t off = 0;
+        guard.active = true;
         for (int d = 0; d < dirs; d++) {
             const size_t nf = static_cast<size_t>(mesh_.faceCount(d));
             for (int v = 0; v < 5; v++) inst.c.f[d].c[v] = base + off + v * nf;
@@ -1052,7 +1092,8 @@ void Solver::computeResidualNoAlloc(double* dt, double* const r[5]) {
         }
         grp.refresh(stream_);
         residualSequence(grp.view(), stream_);
-        for (int d = 0; d < 3; d++) inst.c.f[d] = saved[d];
+        guard.active = false;
+        for (int d = 0; d < 3; d++) inst.c.f[d] = guard.saved[d];
         grp.refresh(stream_);
         const Control c1 = control();
         if (inst.c.dt_method == 0) copyOut(inst.c.dt, dt, N, stream_);

@@ -139,6 +139,7 @@ private:
     std::unique_ptr<GroupT<float>> g32_;
     Control* hostCtl_ = nullptr;  // pinned
     cudaStream_t ownStream_ = nullptr, stream_ = nullptr;
+    int device_ = 0;  // the CUDA device current when the solver was created
 };
 
 }  // namespace ctbfm

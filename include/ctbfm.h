@@ -117,13 +117,16 @@ int ctbfm_compute_residual(ctbfm_solver* s, double* dt, double* r_rho, double* r
  * owned by another allocator (a framework's caching allocator, or a pool
  * reserved at start-up) and control loops that must not block in the
  * driver's allocator mid-step. It allocates no device memory: the per-face
- * flux contributions go to a static __device__ array of 16 MiB (5 doubles for
- * at most 419430 faces summed over the swept directions; larger cases return
- * CTBFM_E_CONFIG with the sizes in the message). Every GPU that loads the
- * library holds that array until exit; all calls on a device share it, so
- * calls that overlap on the GPU race. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture. No counterpart in the reference. */
+ * flux contributions go to a static __device__ array of 16 MiB, 5 words per
+ * face summed over the swept directions, i.e. at most 419430 faces in fp64
+ * and 838860 in fp32_kahan (larger cases return CTBFM_E_CONFIG with the
+ * sizes in the message). Every GPU on which a solver is created holds that
+ * array until exit: solver creation looks up its device address
+ * (cudaGetSymbolAddress), which also makes the driver back it under lazy
+ * module loading, so this call never reserves memory. All calls on a device
+ * share the array, so calls that overlap on the GPU race. The call runs on
+ * the device the solver was created on and restores the caller's current
+ * device. No counterpart in the reference. */
 int ctbfm_compute_residual_noalloc(ctbfm_solver* s, double* dt, double* r_rho, double* r_rhou,
                                    double* r_rhov, double* r_rhow, double* r_rhoe);
 

@@ -120,6 +120,67 @@ def _correlations():
                            KN_CORRELATION_BFM_COEFFICIENT="0.8")
 
 
+def _edges(c):
+    """LEADING_EDGE_INDEX / TRAILING_EDGE_INDEX of the first blade row."""
+    import numpy as np
+
+    idx = np.nonzero(c.fields["bladePresent"][:, 0, 0] > 0)[0]
+    return dict(LEADING_EDGE_INDEX=str(int(idx[0])), TRAILING_EDGE_INDEX=str(int(idx[-1])))
+
+
+def _lift_drag(c):
+    """Lift-Drag body force (src/source_bfm_lift_drag.cpp:3-88): design
+    relative flow angle beta0 and profile-loss coefficient Kp0 per node,
+    varying over the span so that both signs of (beta0 - beta) occur."""
+    import numpy as np
+
+    blade = c.fields["bladePresent"] > 0
+    span = (c.fields["bladeMetalAngle"] - c.fields["bladeMetalAngle"].min())
+    c.fields["liftDragBeta0"] = np.where(blade, np.deg2rad(-62.0) + 0.8 * span, 0.0)
+    c.fields["liftDragKpEtamax"] = np.where(blade, 0.02 + 0.01 * span, 0.0)
+    s = dict(BFM_MODEL="Lift-Drag")
+    s.update(_edges(c))
+    return c.with_settings(**s)
+
+
+def _stall_fields(c, name, lo, hi):
+    """A per-node deviation-angle field varying linearly over j from lo to
+    hi (radians) inside the blade rows, so that some nodes are beyond it."""
+    import numpy as np
+
+    nj = c.shape[1]
+    ramp = np.linspace(lo, hi, nj)[None, :, None]
+    c.fields[name] = np.where(c.fields["bladePresent"] > 0, np.broadcast_to(ramp, c.x.shape), 0.0)
+
+
+def _stalled(bfm_model):
+    """STALLED_BFM_ACTIVE (src/source_bfm_base.cpp:178-185,
+    src/source_bfm_thollet.cpp:79-84): nodes whose deviation exceeds
+    deviationAngleStall take the camber normal as force direction (and no
+    Thollet viscous force)."""
+    c = cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS, bfm_model=bfm_model)
+    _stall_fields(c, "deviationAngleStall", -0.05, 0.05)
+    return c.with_settings(STALLED_BFM_ACTIVE="yes")
+
+
+def _thollet_off_design():
+    """HALL_THOLLET_OFF_DESIGN_ACTIVE (src/source_bfm_thollet.cpp:85-110):
+    the off-design loss pi K_mach |delta - delta_pivot|^(2 K_d), together with
+    the stalled-node rule."""
+    c = _stalled("Hall-Thollet")
+    _stall_fields(c, "deviationAnglePivot", -0.1, 0.1)
+    return c.with_settings(HALL_THOLLET_OFF_DESIGN_ACTIVE="yes", HALL_THOLLET_COEFFICIENT_KD="1.3")
+
+
+def _perturbation(c, center, radius):
+    """PERTURBATION_BODY_FORCE (src/source_bfm_base.cpp:215-243): a Gaussian
+    bump of the body force in space and time around `center`, active over the
+    physical time the run covers."""
+    return c.with_settings(PERTURBATION_BODY_FORCE="yes", PERTURBATION_CENTER=", ".join(repr(v) for v in center),
+                           PERTURBATION_RADIAL_EXTENSION=repr(radius), PERTURBATION_SCALING_FACTOR="0.5",
+                           PERTURBATION_TIME_START="0.0", PERTURBATION_TIME_DURATION="0.002")
+
+
 def _viscous(c, mu=None, walls=(2, 3), **settings):
     """Laminar viscous run (VISCOSITY_ACTIVE) with the J-face walls made
     no-slip walls at rest: Sutherland's law for air when mu is None, else a
@@ -186,4 +247,12 @@ CASES = {
     "annulus_viscous_roe": (lambda: _viscous(cases.annulus3d(ni=20, nj=8, nk=9, bfm_model="None"),
                                              BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no"), 10),
     "co2_bump_viscous": (_co2_viscous, 20),
+    "meridional_lift_drag": (lambda: _lift_drag(cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS)), 20),
+    "meridional_hall_stalled": (lambda: _stalled("Hall"), 20),
+    "meridional_thollet_off_design_stalled": (_thollet_off_design, 20),
+    "meridional_hall_perturbation": (lambda: _perturbation(cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS),
+                                                           (0.25, 0.3, 0.0), 0.06), 20),
+    "annulus_lift_drag_perturbation": (lambda: _perturbation(_lift_drag(cases.annulus3d(ni=20, nj=8, nk=9,
+                                                                                        rows=cases.MAP_ROWS)),
+                                                             (0.25, 0.0, 0.3), 0.08), 10),
 }

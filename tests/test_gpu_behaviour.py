@@ -31,7 +31,28 @@ def test_divergence_is_reported_at_the_oracles_iteration(tmp_path, oracle_lib):
         assert s.iteration == ro["iterations"]
 
 
-@pytest.mark.parametrize("which,n", [("bump2d_192x64", 20), ("annulus3d_160x48x64", 2)])
+def test_bump_192x64_matches_the_reference_after_5000_iterations(tmp_path):
+    """The 192 x 64 bump channel (JST, RK4, local dt at CFL 2.0, uniform
+    inlet start) after 5000 iterations against the reference solver's own
+    run (fixture tests/golden/c1/bump2d_c1_5000.npz, made by
+    tests/golden/c1/make_c1_golden.py): 1e-12 relative per field, 1e-10 on every
+    log10 residual norm of the history."""
+    import os
+
+    from cturbobfm_b200 import Solver
+
+    fx = np.load(os.path.join(os.path.dirname(__file__), "golden", "c1", "bump2d_c1_5000.npz"))
+    n = int(fx["n_iter"])
+    ini = cases.bump2d().write(str(tmp_path))
+    with Solver(ini) as s:
+        assert s.step(n) == n
+        assert rel_err(s.state(), fx["state"]) <= 1e-12
+        h = s.history()
+        assert np.abs(h["lognorm"] - fx["lognorm"]).max() <= 1e-10
+        assert abs(s.time - float(fx["time"])) <= 1e-12 * float(fx["time"])
+
+
+@pytest.mark.parametrize("which,n", [("bump2d_192x64", 20), ("annulus3d_160x48x64", 10)])
 def test_full_size_workloads_match_oracle(which, n, tmp_path, oracle_lib):
     from cturbobfm_b200 import Solver
 

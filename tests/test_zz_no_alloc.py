@@ -40,6 +40,25 @@ def test_noalloc_residual_matches_allocating_entry_point(make, tmp_path):
             assert rel_err(r, r_ref) <= REL_TOL
 
 
+def test_noalloc_reserves_no_device_memory(tmp_path):
+    """The defining property: after one warm-up call (which loads the kernels
+    the evaluation launches), further calls leave the free device memory
+    unchanged; the static array was backed when the solver was created."""
+    import torch
+
+    from cturbobfm_b200 import Solver
+
+    torch.cuda.mem_get_info(0)  # the runtime behind the measurement is initialised before the first reading
+    ini = cases.annulus3d(ni=20, nj=8, nk=9).write(str(tmp_path))
+    with Solver(ini) as s:
+        s.residual_noalloc()
+        free0, _ = torch.cuda.mem_get_info(0)
+        for _ in range(3):
+            s.residual_noalloc()
+        free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+
+
 def test_noalloc_rejects_cases_beyond_the_scratch(tmp_path):
     from cturbobfm_b200 import Solver
     from cturbobfm_b200.solver import CtbfmError
