@@ -209,9 +209,19 @@ struct alignas(16) DevCaseT {
     R* Rp[5];  // periodic-plane residuals (2 * ni * nj)
     R* W[5];   // primitives of the current stage input (k_prim)
     R* dt;
-    double* partial;  // [node_tiles*5 | per_tiles*5 | node_tiles dt minima]
+    // per-tile partials: [node_tiles*5 norms of the split stage |
+    // per_tiles*5 periodic norms | node_tiles dt minima | nboxes*5 norms of
+    // the fused stage kernel]
+    double* partial;
     int node_tiles;   // tiles of this instance in the node kernels
     int per_tiles;    // tiles of this instance in the periodic kernel
+    // fused stage kernel (k_stage): whether the instance can run it
+    // (inviscid, no Chima / Correlations force), its box of nodes per block
+    // (extent along i, j, k) and the number of boxes along i, j, k
+    int fuse_ok;
+    int nboxes;
+    int fbox[3];
+    int fnb[3];
     const DevLut* lut;  // FLUID_MODEL = real: the look-up tables; nullptr for the ideal gas
     // VISCOSITY_ACTIVE (laminar): viscosity constant (visc_const) or
     // Sutherland's law, conductivity vcp * mu / vpr; nodes of the no-slip

@@ -16,6 +16,19 @@ struct TileList {
     int n = 0;
 };
 
+// Tile lists of the split stage (k_prim, k_faces, k_nodes) for one set of
+// members.
+struct SplitLists {
+    TileList node;  // nodes (k_prim, k_nodes)
+    // faces per direction, scheme (0 JST, 1 Roe) and face set: 0 every face
+    // of the direction; for K lines of at least 3 nodes, and J lines of at
+    // least 3 nodes whose rows of nk faces do not fall on whole warps, 1 the
+    // faces two or more faces from both ends of each line (plain interior
+    // stencils) and 2 the four faces at the ends (boundary and next-to-
+    // boundary stencils), so that no warp mixes the two code paths
+    TileList face[3][2][3];
+};
+
 // Everything a batched launch needs: the instances' descriptions on the
 // device and the tile lists of each kernel family.
 template <typename R>
@@ -26,14 +39,15 @@ struct BatchView {
     bool real = false;  // some member uses the real-gas look-up tables
     bool bfmCommon = true;  // some member uses no BFM or Hall / Hall-Thollet / Lift-Drag / blockage
     bool bfmRare = false;   // some member uses the Chima or Correlations body force
-    TileList node;        // nodes of every instance (k_prim, k_nodes, k_dt)
-    // faces per direction, scheme (0 JST, 1 Roe) and face set: 0 every face
-    // of the direction; for K lines of at least 3 nodes, and J lines of at
-    // least 3 nodes whose rows of nk faces do not fall on whole warps, 1 the
-    // faces two or more faces from both ends of each line (plain interior
-    // stencils) and 2 the four faces at the ends (boundary and next-to-
-    // boundary stencils), so that no warp mixes the two code paths
-    TileList face[3][2][3];
+    TileList node;        // nodes of every instance (k_dt)
+    // stage kernels: fusedMode 0 runs every member through the split stage
+    // (split[0]); fusedMode 1 runs the members that can (fuse_ok) through the
+    // fused stage kernel k_stage (one tile per box of nodes, by scheme, in
+    // fbox) and the others through the split stage (split[1])
+    int fusedMode = 0;
+    SplitLists split[2];
+    TileList fbox[2];
+    size_t fusedSmem = 0;  // dynamic shared memory of a k_stage block (largest member box)
     TileList per;         // periodic (i, j) pairs of periodic instances
     bool viscous = false;  // some member is viscous (VISCOSITY_ACTIVE)
     TileList vnode;        // nodes of the viscous instances (k_grad)
@@ -58,8 +72,14 @@ struct Launcher {
     static cudaError_t viscous(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    // k_stage over the fused members' boxes (fusedMode 1)
+    static cudaError_t fused(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    // dynamic shared memory of a k_stage block of an instance with box
+    // (bi, bj, bk) in topology topo and scheme (0 JST, 1 Roe)
+    static size_t fusedSmemBytes(int bi, int bj, int bk, int topo, int scheme);
     static cudaError_t finalize(const BatchView<R>& b, int force, cudaStream_t s);
-    // k_prim, k_faces, (k_grad, k_vfaces), k_nodes, k_periodic of one stage (stage -1: residual only)
+    // k_prim, k_faces, (k_grad, k_vfaces), k_nodes, k_stage, k_periodic of one
+    // stage (stage -1: residual only)
     static cudaError_t stage(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     // one whole iteration of every instance in the batch
     static cudaError_t iteration(const BatchView<R>& b, int nstages, cudaStream_t s);
@@ -68,8 +88,12 @@ struct Launcher {
 extern template struct Launcher<double>;
 extern template struct Launcher<float>;
 
-constexpr int kKernelKinds = 10;
+constexpr int kKernelKinds = 11;
 constexpr int kTileSize = 256;  // elements per tile (one per thread)
+// fused stage kernel: nodes per box (one per thread) and the faces of one
+// direction a box may hold in shared memory
+constexpr int kFusedBoxNodes = 256;
+constexpr int kFusedFaceCap = 384;
 // periodic (i, j) pairs per tile, one block of as many threads each: the
 // periodic planes hold few pairs with much work each (7 680 on the bench
 // workload: 120 blocks instead of 30)

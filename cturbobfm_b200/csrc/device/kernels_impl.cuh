@@ -20,6 +20,8 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "kernels.hpp"
 #include "sources.cuh"
 #include "viscous.cuh"
@@ -688,6 +690,9 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
     }
 }
 
+// ------------------------------------------------------------ fused stage
+#include "stage_fused.cuh"
+
 // ------------------------------------------------------------- time step
 // Solver::computeTimestepArray (src/solver.cpp:1531-1630):
 // dt = CFL / (sum_d (|u . e_d| + a) / |e_d| + 4 nu sum_d 1 / |e_d|^2) over the
@@ -943,17 +948,27 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
 // printInfoResiduals' initial maximum (src/solver.cpp:1426-1439),
 // Solver::checkConvergence (src/solver.cpp:2985-3015) and the time advance
 // t += min(dt) (src/solver.cpp:1389). One block per instance.
+// fusedMode 1: instances that ran the fused stage kernel have their norm
+// partials in its region (one per box) instead of the node tiles'.
 template <typename R>
-__global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, const Tile* tiles, int force) {
+__global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, const Tile* tiles, int force,
+                                                  int fusedMode) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, 0, force, tl)) return;
     Control* ctl = c.ctl;
-    const int nparts = c.node_tiles + (c.periodic ? c.per_tiles : 0);
+    const bool fz = fusedMode && c.fuse_ok;
+    const int na = fz ? c.nboxes : c.node_tiles;
+    const double* pa =
+        fz ? c.partial + (static_cast<long long>(c.node_tiles) + c.per_tiles) * 5 + c.node_tiles : c.partial;
+    const double* pp = c.partial + static_cast<long long>(c.node_tiles) * 5;  // periodic planes
+    const int nparts = na + (c.periodic ? c.per_tiles : 0);
     double s[5] = {0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+        const double* src = b < na ? pa + b * 5 : pp + (b - na) * 5;
 #pragma unroll
-        for (int v = 0; v < 5; v++) s[v] += c.partial[b * 5 + v];
+        for (int v = 0; v < 5; v++) s[v] += src[v];
+    }
     blockSum<5>(s);
     if (threadIdx.x != 0) return;
     const long long it = ctl->it + 1;
@@ -1100,14 +1115,15 @@ cudaError_t Launcher<R>::pre(const BatchView<R>& b, bool forceTurbo, bool dtpart
 
 template <typename R>
 cudaError_t Launcher<R>::prim(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.node.n) launchK(k_prim<R>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    const TileList& t = b.split[b.fusedMode].node;
+    if (t.n) launchK(k_prim<R>, t.n, 256, s, b.cases, t.tiles, stage, force);
     return cudaGetLastError();
 }
 
 namespace {
 template <int DIR, int SCHEME, int FL, typename R>
 void launchFaceSets(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    const TileList* t = b.face[DIR][SCHEME];
+    const TileList* t = b.split[b.fusedMode].face[DIR][SCHEME];
     if (t[0].n) launchK(k_faces<DIR, SCHEME, R, FL, 0>, t[0].n, 256, s, b.cases, t[0].tiles, stage, force);
     if (t[1].n) launchK(k_faces<DIR, SCHEME, R, FL, 1>, t[1].n, 256, s, b.cases, t[1].tiles, stage, force);
     if (t[2].n) launchK(k_faces<DIR, SCHEME, R, FL, 2>, t[2].n, 256, s, b.cases, t[2].tiles, stage, force);
@@ -1154,11 +1170,73 @@ cudaError_t Launcher<R>::viscous(const BatchView<R>& b, int stage, int force, cu
 
 template <typename R>
 cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    if (b.node.n && b.ideal && b.bfmCommon) launchK(k_nodes<R, 0, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
-    if (b.node.n && b.real && b.bfmCommon) launchK(k_nodes<R, 1, 0>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
-    if (b.node.n && b.ideal && b.bfmRare) launchK(k_nodes<R, 0, 1>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
-    if (b.node.n && b.real && b.bfmRare) launchK(k_nodes<R, 1, 1>, b.node.n, 256, s, b.cases, b.node.tiles, stage, force);
+    const TileList& t = b.split[b.fusedMode].node;
+    if (t.n && b.ideal && b.bfmCommon) launchK(k_nodes<R, 0, 0>, t.n, 256, s, b.cases, t.tiles, stage, force);
+    if (t.n && b.real && b.bfmCommon) launchK(k_nodes<R, 1, 0>, t.n, 256, s, b.cases, t.tiles, stage, force);
+    if (t.n && b.ideal && b.bfmRare) launchK(k_nodes<R, 0, 1>, t.n, 256, s, b.cases, t.tiles, stage, force);
+    if (t.n && b.real && b.bfmRare) launchK(k_nodes<R, 1, 1>, t.n, 256, s, b.cases, t.tiles, stage, force);
     return cudaGetLastError();
+}
+
+template <typename R>
+size_t Launcher<R>::fusedSmemBytes(int bi, int bj, int bk, int topo, int scheme) {
+    const int hk = topo == 1 ? 2 : 0;
+    const size_t np = static_cast<size_t>(bi + 4) * (bj + 4) * (bk + 2 * hk);
+    return ((scheme == 0 ? 7 : 5) * np + 5 * static_cast<size_t>(kFusedFaceCap)) * sizeof(R);
+}
+
+namespace {
+// Dynamic shared memory beyond the default 48 KB must be allowed per kernel
+// and device (its largest size so far; k_stage blocks of smaller instances
+// use less).
+template <typename R, int SCHEME, int FL>
+cudaError_t launchStage(const BatchView<R>& b, const TileList& t, int stage, int force, cudaStream_t s) {
+    constexpr int kDevices = 64;
+    static std::mutex mu;
+    static size_t allowed[kDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kDevices) return cudaErrorInvalidDevice;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (b.fusedSmem > allowed[dev]) {
+            e = cudaFuncSetAttribute(k_stage<R, SCHEME, FL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(b.fusedSmem));
+            if (e != cudaSuccess) return e;
+            allowed[dev] = b.fusedSmem;
+        }
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(t.n);
+    cfg.blockDim = dim3(kFusedBoxNodes);
+    cfg.dynamicSmemBytes = b.fusedSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = CTBFM_PDL;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_stage<R, SCHEME, FL>, b.cases, t.tiles, stage, force);
+}
+}  // namespace
+
+template <typename R>
+cudaError_t Launcher<R>::fused(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
+    if (!b.fusedMode) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int sc = 0; sc < 2 && e == cudaSuccess; sc++) {
+        const TileList& t = b.fbox[sc];
+        if (!t.n) continue;
+        if (sc == 0) {
+            if (b.ideal && e == cudaSuccess) e = launchStage<R, 0, 0>(b, t, stage, force, s);
+            if (b.real && e == cudaSuccess) e = launchStage<R, 0, 1>(b, t, stage, force, s);
+        } else {
+            if (b.ideal && e == cudaSuccess) e = launchStage<R, 1, 0>(b, t, stage, force, s);
+            if (b.real && e == cudaSuccess) e = launchStage<R, 1, 1>(b, t, stage, force, s);
+        }
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename R>
@@ -1169,7 +1247,7 @@ cudaError_t Launcher<R>::periodic(const BatchView<R>& b, int stage, int force, c
 
 template <typename R>
 cudaError_t Launcher<R>::finalize(const BatchView<R>& b, int force, cudaStream_t s) {
-    if (b.inst.n) launchK(k_finalize<R>, b.inst.n, 256, s, b.cases, b.inst.tiles, force);
+    if (b.inst.n) launchK(k_finalize<R>, b.inst.n, 256, s, b.cases, b.inst.tiles, force, b.fusedMode);
     return cudaGetLastError();
 }
 
@@ -1179,6 +1257,7 @@ cudaError_t Launcher<R>::stage(const BatchView<R>& b, int stage, int force, cuda
     for (int d = 0; d < 3 && e == cudaSuccess; d++) e = faces(b, d, stage, force, s);
     if (e == cudaSuccess) e = viscous(b, stage, force, s);
     if (e == cudaSuccess) e = nodes(b, stage, force, s);
+    if (e == cudaSuccess) e = fused(b, stage, force, s);
     if (e == cudaSuccess) e = periodic(b, stage, force, s);
     return e;
 }

@@ -354,13 +354,13 @@ CTBFM_DI R jstS(R p1, R p2, R p3) {
     return fabs((p1 - R(2) * p2 + p3) / (p1 + R(2) * p2 + p3));
 }
 
+// The JST flux given the nodes' pressures p and spectral radii r = |u| + a,
+// which depend on one node each: the fused stage kernel evaluates them once
+// per node, the face kernels once per face (the same values either way).
 template <typename R>
-CTBFM_DI S5<R> fluxJstW(Gas<R> gs, const S5<R>& Ull, const S5<R>& Ul, const S5<R>& Ur, const S5<R>& Urr,
-                        const S5<R>& Wll, const S5<R>& Wl, const S5<R>& Wr, const S5<R>& Wrr, V3<R> n) {
+CTBFM_DI S5<R> fluxJstPR(Gas<R> gs, const S5<R>& Ull, const S5<R>& Ul, const S5<R>& Ur, const S5<R>& Urr,
+                         const S5<R>& Wl, const S5<R>& Wr, R pll, R pl, R pr, R prr, R rL, R rR, V3<R> n) {
     const S5<R> Wavg = (Wl + Wr) * R(0.5);
-    const R rL = jstR(gs, Wl), rR = jstR(gs, Wr);
-    const R pll = pressurePrim(gs, Wll), pl = pressurePrim(gs, Wl), pr = pressurePrim(gs, Wr),
-            prr = pressurePrim(gs, Wrr);
     const R sL = jstS(pll, pl, pr), sR = jstS(pl, pr, prr);
     const R r = rmax(rL, rR);
     const R sf = rmax(sL, sR);
@@ -369,6 +369,13 @@ CTBFM_DI S5<R> fluxJstW(Gas<R> gs, const S5<R>& Ull, const S5<R>& Ul, const S5<R
     const S5<R> F = advFlux(gs, Wavg, n);
     const S5<R> d = (Ur - Ul) * psi2 - (((Urr - Ur) - (Ur - Ul) * R(2)) + (Ul - Ull)) * psi4;
     return F - d;
+}
+
+template <typename R>
+CTBFM_DI S5<R> fluxJstW(Gas<R> gs, const S5<R>& Ull, const S5<R>& Ul, const S5<R>& Ur, const S5<R>& Urr,
+                        const S5<R>& Wll, const S5<R>& Wl, const S5<R>& Wr, const S5<R>& Wrr, V3<R> n) {
+    return fluxJstPR(gs, Ull, Ul, Ur, Urr, Wl, Wr, pressurePrim(gs, Wll), pressurePrim(gs, Wl), pressurePrim(gs, Wr),
+                     pressurePrim(gs, Wrr), jstR(gs, Wl), jstR(gs, Wr), n);
 }
 
 template <typename R>

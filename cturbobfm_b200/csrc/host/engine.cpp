@@ -70,6 +70,7 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     for (auto* m : members_) (bfmRareModel(m->c) ? view_.bfmRare : view_.bfmCommon) = true;
     view_.viscous = false;
     for (auto* m : members_) view_.viscous = view_.viscous || m->c.viscous;
+    view_.fusedMode = 1;
     refresh(nullptr);
     cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -82,36 +83,47 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
 template <typename R>
 void GroupT<R>::buildTiles() {
     const int M = static_cast<int>(members_.size());
-    std::vector<Tile> node, face[3][2][3], per, inst, bint, bintAll, vnode, vface[3];
+    std::vector<Tile> node, snode[2], face[2][3][2][3], fbox[2], per, inst, bint, bintAll, vnode, vface[3];
     auto cover = [](std::vector<Tile>& out, int m, long long count, long long size) {
         int local = 0;
         for (long long s = 0; s < count; s += size) out.push_back({m, local++, s, std::min<long long>(size, count - s)});
         return local;
     };
+    size_t smem = 0;
     for (int m = 0; m < M; m++) {
         const DevCaseT<R>& c = members_[m]->c;
         const int nt = cover(node, m, c.n, kTileSize);
         if (nt != c.node_tiles) throw std::logic_error("node tile count mismatch");
-        for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++) {
-            const long long nf =
-                static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
-            const int nline = d == 0 ? c.ni : (d == 1 ? c.nj : c.nk);  // nodes along a line of direction d
-            // K lines (and J lines whose rows of nk faces do not fill whole
-            // warps) run as two launches, plain faces 2 .. n-2 and the four
-            // end faces of every line, so the plain launch carries no boundary
-            // or extrapolation code; I faces and warp-aligned J rows run as one
-            // launch (splitting them measured slower: the four end planes of I
-            // make a large launch of boundary code)
-            const bool split = nline >= 3 && (d == 2 || (d == 1 && c.nk % 32 != 0));
-            if (!split) {
-                cover(face[d][c.scheme][0], m, nf, faceTile_[d]);
-            } else {
-                const long long lines = d == 0 ? static_cast<long long>(c.nj) * c.nk
-                                               : (d == 1 ? static_cast<long long>(c.ni) * c.nk
-                                                         : static_cast<long long>(c.ni) * c.nj);
-                cover(face[d][c.scheme][1], m, lines * (nline - 3), faceTile_[d]);
-                cover(face[d][c.scheme][2], m, lines * 4, faceTile_[d]);
+        // split-stage lists: [0] every member, [1] the members outside the
+        // fused stage kernel
+        for (int mode = 0; mode < 2; mode++) {
+            if (mode == 1 && c.fuse_ok) continue;
+            cover(snode[mode], m, c.n, kTileSize);
+            for (int d = 0; d < (c.topo == 1 ? 3 : 2); d++) {
+                const long long nf =
+                    static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
+                const int nline = d == 0 ? c.ni : (d == 1 ? c.nj : c.nk);  // nodes along a line of direction d
+                // K lines (and J lines whose rows of nk faces do not fill whole
+                // warps) run as two launches, plain faces 2 .. n-2 and the four
+                // end faces of every line, so the plain launch carries no
+                // boundary or extrapolation code; I faces and warp-aligned J rows
+                // run as one launch (splitting them measured slower: the four end
+                // planes of I make a large launch of boundary code)
+                const bool split = nline >= 3 && (d == 2 || (d == 1 && c.nk % 32 != 0));
+                if (!split) {
+                    cover(face[mode][d][c.scheme][0], m, nf, faceTile_[d]);
+                } else {
+                    const long long lines = d == 0 ? static_cast<long long>(c.nj) * c.nk
+                                                   : (d == 1 ? static_cast<long long>(c.ni) * c.nk
+                                                             : static_cast<long long>(c.ni) * c.nj);
+                    cover(face[mode][d][c.scheme][1], m, lines * (nline - 3), faceTile_[d]);
+                    cover(face[mode][d][c.scheme][2], m, lines * 4, faceTile_[d]);
+                }
             }
+        }
+        if (c.fuse_ok) {  // one tile per box; Tile.local and Tile.start are the box index
+            for (int bx = 0; bx < c.nboxes; bx++) fbox[c.scheme].push_back({m, bx, bx, 1});
+            smem = std::max(smem, Launcher<R>::fusedSmemBytes(c.fbox[0], c.fbox[1], c.fbox[2], c.topo, c.scheme));
         }
         if (c.viscous) {
             cover(vnode, m, c.n, kTileSize);
@@ -127,6 +139,7 @@ void GroupT<R>::buildTiles() {
             if (c.need_turbo) bint.push_back({m, b, 0, 1});
         }
     }
+    view_.fusedSmem = smem;
     std::vector<Tile> all;
     std::vector<std::pair<TileList*, size_t>> offs;
     auto add = [&](TileList& tl, const std::vector<Tile>& v) {
@@ -135,9 +148,13 @@ void GroupT<R>::buildTiles() {
         all.insert(all.end(), v.begin(), v.end());
     };
     add(view_.node, node);
-    for (int d = 0; d < 3; d++)
-        for (int s = 0; s < 2; s++)
-            for (int k = 0; k < 3; k++) add(view_.face[d][s][k], face[d][s][k]);
+    for (int mode = 0; mode < 2; mode++) {
+        add(view_.split[mode].node, snode[mode]);
+        for (int d = 0; d < 3; d++)
+            for (int s = 0; s < 2; s++)
+                for (int k = 0; k < 3; k++) add(view_.split[mode].face[d][s][k], face[mode][d][s][k]);
+    }
+    for (int s = 0; s < 2; s++) add(view_.fbox[s], fbox[s]);
     add(view_.per, per);
     add(view_.vnode, vnode);
     for (int d = 0; d < 3; d++) add(view_.vface[d], vface[d]);
@@ -174,10 +191,12 @@ void GroupT<R>::tune(cudaStream_t s) {
     cudaCheck(cudaEventCreate(&e0), "cudaEventCreate");
     cudaCheck(cudaEventCreate(&e1), "cudaEventCreate");
     const int sizes[] = {256, 512, 1024, 2048};
+    const int mode = view_.fusedMode;
+    view_.fusedMode = 0;  // the face tiles of every member
     for (int d = 0; d < 3; d++) {
         int nt = 0;
         for (int sc = 0; sc < 2; sc++)
-            for (int k = 0; k < 3; k++) nt += view_.face[d][sc][k].n;
+            for (int k = 0; k < 3; k++) nt += view_.split[0].face[d][sc][k].n;
         if (!nt) continue;
         float best = 0.f;
         int bestSize = kTileSize;
@@ -198,9 +217,24 @@ void GroupT<R>::tune(cudaStream_t s) {
         }
         faceTile_[d] = bestSize;
     }
+    view_.fusedMode = mode;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     buildTiles();
+}
+
+template <typename R>
+void GroupT<R>::setFusedMode(int mode) {
+    if ((mode != 0) == (view_.fusedMode != 0)) return;
+    view_.fusedMode = mode != 0 ? 1 : 0;
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    if (graph1_) {
+        cudaGraphExecDestroy(graph1_);
+        graph1_ = nullptr;
+    }
 }
 
 template <typename R>

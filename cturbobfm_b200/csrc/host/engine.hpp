@@ -68,6 +68,11 @@ public:
     // first enqueue of at least kTuneMinIterations iterations, when enabled).
     void tune(cudaStream_t s);
     void setAutotune(bool on) { autotune_ = on; }
+    // Stage kernels: 0 the split stage for every member, 1 the fused stage
+    // kernel for the members that can run it (the others split). Results are
+    // the same either way; the captured graphs are rebuilt.
+    void setFusedMode(int mode);
+    int fusedMode() const { return view_.fusedMode; }
     int faceTile(int d) const { return faceTile_[d]; }
     static constexpr long long kTuneMinIterations = 64;
 

@@ -602,6 +602,33 @@ void Solver::setupScalars() {
     c.per_tiles = c.periodic ? static_cast<int>((NI * NJ + kPeriodicTile - 1) / kPeriodicTile) : 0;
     c.hist_cap = std::min<long long>(std::max<long long>(maxIter_, 1024), 1 << 20);
     c.max_it = maxIter_;
+    // fused stage kernel: inviscid instances without the Chima / Correlations
+    // forces; box of at most kFusedBoxNodes nodes, k (the contiguous index)
+    // up to 16 wide in 3-D, j up to 32 wide in 2-D (where j is contiguous),
+    // no direction holding more than kFusedFaceCap faces
+    c.fuse_ok = (!c.viscous && !bfmRareModel(c)) ? 1 : 0;
+    int bi, bj, bk;
+    if (c.topo == 1) {
+        bk = std::min(c.nk, 16);
+        bj = std::min(c.nj, 4);
+    } else {
+        bk = 1;
+        bj = std::min(c.nj, 32);
+    }
+    bi = std::max(1, std::min(c.ni, kFusedBoxNodes / (bj * bk)));
+    auto facesFit = [&] {
+        return (bi + 1) * bj * bk <= kFusedFaceCap && bi * (bj + 1) * bk <= kFusedFaceCap &&
+               bi * bj * (bk + 1) <= kFusedFaceCap;
+    };
+    while (bi > 1 && !facesFit()) bi--;
+    if (!facesFit()) c.fuse_ok = 0;
+    c.fbox[0] = bi;
+    c.fbox[1] = bj;
+    c.fbox[2] = bk;
+    c.fnb[0] = (c.ni + bi - 1) / bi;
+    c.fnb[1] = (c.nj + bj - 1) / bj;
+    c.fnb[2] = (c.nk + bk - 1) / bk;
+    c.nboxes = c.fnb[0] * c.fnb[1] * c.fnb[2];
 }
 
 // Device arrays of the operating point in precision R.
@@ -831,7 +858,8 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         c.W[v] = inst.allocR(N);
     }
     c.dt = inst.allocR(N);
-    c.partial = inst.allocD(static_cast<size_t>(c.node_tiles + c.per_tiles) * 5 + c.node_tiles);
+    c.partial = inst.allocD(static_cast<size_t>(c.node_tiles + c.per_tiles) * 5 + c.node_tiles +
+                            static_cast<size_t>(c.nboxes) * 5);
     c.lut = table_ ? uploadLut(inst) : nullptr;
     c.ctl = static_cast<Control*>(inst.allocBytes(sizeof(Control)));
     c.hist = inst.allocD(static_cast<size_t>(c.hist_cap) * kHistWidth);
