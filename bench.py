@@ -194,40 +194,77 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ ours
+def blade_fraction(case) -> float:
+    """Share of the nodes inside blade rows (bladePresent > 0)."""
+    import numpy as np
+
+    bp = case.fields.get("bladePresent")
+    return 0.0 if bp is None else float(np.count_nonzero(bp > 0)) / bp.size
+
+
+def stage_bytes_per_cell(case, word: int = 8) -> float:
+    """Algorithmic bytes of one cell-stage update as the survey's measurement
+    section defines them: w * (5 read U(k-1) + 5 read U^n + 5 written U(k) + 1
+    read dt/V) + 8 * 3 * d bytes of face vectors (d face directions owned per
+    node), plus 14 BFM fields of w bytes at blade-row nodes; the float path
+    adds 40 bytes to read and write the Kahan compensation."""
+    d = 3 if case.shape[2] > 1 else 2
+    b = word * 16 + 8 * 3 * d + 14 * word * blade_fraction(case)
+    if word == 4:
+        b += 40
+    return b
+
+
 def algorithmic_bytes(case, kernel: str) -> float:
-    """Compulsory DRAM bytes of one launch of a kernel kind (FP64): every input
-    read once, every output written once."""
+    """Compulsory DRAM bytes of one launch of a kernel kind (FP64). k_stage
+    (one fused stage) takes the survey's per-cell-stage figure times the nodes;
+    the split kernels count every input read once and every output written
+    once."""
     ni, nj, nk = case.shape
     n = ni * nj * nk
     faces = {"I": (ni + 1) * nj * nk, "J": ni * (nj + 1) * nk, "K": ni * nj * (nk + 1)}
+    if kernel == "k_stage":
+        return stage_bytes_per_cell(case) * n
     if kernel.startswith("k_faces_"):
         f = faces[kernel[-1]]
+        if kernel == "k_faces_K":
+            f = int(round(f * (1.0 - blade_fraction(case))))  # blade rows have no K flux
         return 8.0 * (5 * n + 4 * f + 5 * f)  # primitives once, normal + area, flux * |S|
     if kernel == "k_prim":
         return 8.0 * (5 * n + 5 * n)
     if kernel == "k_nodes":
-        # face contributions of 3 directions, stage input, U^n, output, dt, volume,
-        # rotation (cos, sin, r) and the BFM fields of the node (14)
-        return 8.0 * (5 * sum(faces.values()) + 3 * 5 * n + 2 * n + 3 * n + 14 * n)
+        # face contributions of I and J, of K outside the blade rows; stage
+        # input, output, dt, volume, bladePresent and the blockage gradient (3)
+        # at every node; rotation (cos, sin, r) and the BFM fields (9 of Hall)
+        # at blade-row nodes only (the stage input is U^n: read once)
+        bf = blade_fraction(case)
+        contrib = faces["I"] + faces["J"] + (faces["K"] * (1.0 - bf) if nk > 1 else 0.0)
+        return 8.0 * (5 * contrib + 2 * 5 * n + 2 * n + 4 * n + (3 + 9) * n * bf)
     if kernel == "k_dt":
         return 8.0 * (5 * n + 12 * n + n)
     return 0.0
 
 
-def calls_per_iteration(case, kernel: str) -> int:
+SPLIT_STAGE = ("k_prim", "k_faces_I", "k_faces_J", "k_faces_K", "k_nodes", "k_periodic")
+FUSED_STAGE = ("k_stage", "k_periodic")
+
+
+def calls_per_iteration(case, kernel: str, fused: bool = False) -> int:
     """How often per iteration each kernel kind of ctbfm_profile_kernels runs
-    (its timing covers all launches of one call)."""
+    (its timing covers all launches of one call), for the fused or the split
+    stage."""
     s = case.n_stages
-    return {"k_faces_I": s, "k_faces_J": s, "k_faces_K": s, "k_nodes": s, "k_periodic": s, "k_prim": s,
-            "k_dt": 1, "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
+    if kernel in SPLIT_STAGE + FUSED_STAGE:
+        return s if kernel in (FUSED_STAGE if fused else SPLIT_STAGE) else 0
+    return {"k_dt": 1, "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
 
 
-def launches_per_iteration(case, kernel: str) -> int:
+def launches_per_iteration(case, kernel: str, fused: bool = False) -> int:
     """Kernel launches per iteration of each kind: the end faces of K lines
     (and of J lines whose rows do not fill whole warps) run in a launch of
     their own."""
     ni, nj, nk = case.shape
-    n = calls_per_iteration(case, kernel)
+    n = calls_per_iteration(case, kernel, fused)
     if kernel == "k_faces_K" and nk >= 3:
         return 2 * n
     if kernel == "k_faces_J" and nj >= 3 and nk % 32 != 0:
@@ -321,7 +358,12 @@ def run_ours(args):
             ms32 = f0.elapsed_time(f1)
             u32 = s32.state()
             rel = [float(np.abs(u32[v] - u64[v]).max() / np.abs(u64[v]).max()) for v in range(5)]
-            fp32 = {"value": n * stages * args.steps / (ms32 / 1e3), "unit": UNIT, "ms_per_step": ms32 / args.steps,
+            v32 = n * stages * args.steps / (ms32 / 1e3)
+            b32 = stage_bytes_per_cell(case, 4)
+            pk = measured_peaks().get("hbm_gbs", 6650.0)
+            fp32 = {"value": v32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "status": s32.status,
+                    "stage_roofline": {"bytes_per_cell_stage": b32, "achieved": v32 * b32 / 1e9, "peak": pk,
+                                       "unit": "GB/s", "frac": v32 * b32 / 1e9 / pk},
                     "speedup_vs_fp64": ms_max / ms32,
                     "state_rel_err_vs_fp64": {"after_iterations": args.warmup + args.steps, "per_field_max": rel}}
 
@@ -346,7 +388,8 @@ def run_ours(args):
 
     # per-kernel device times (CUDA events on the launching stream)
     prof = solver.profile_kernels(reps=10)
-    shares = {k: prof[k] * calls_per_iteration(case, k) for k in prof}
+    fused = bool(solver.info().fused_stage)
+    shares = {k: prof[k] * calls_per_iteration(case, k, fused) for k in prof}
     total = sum(shares.values()) or 1.0
     dominant = max(shares, key=shares.get)
     peaks = measured_peaks()
@@ -354,7 +397,7 @@ def run_ours(args):
     alg = algorithmic_bytes(case, dominant)
     achieved = alg / (prof[dominant] / 1e3) / 1e9 if prof[dominant] > 0 else 0.0
     traffic = traffic_table().get(dominant)
-    launches = args.steps * (1 + sum(launches_per_iteration(case, k) for k in prof if prof[k] > 0))
+    launches = args.steps * (1 + sum(launches_per_iteration(case, k, fused) for k in prof if prof[k] > 0))
     clk = clocks.summary()
 
     if world > 1:
@@ -382,11 +425,13 @@ def run_ours(args):
                      "algorithmic_bytes_per_launch": alg, "launch_ms": prof[dominant],
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "kernel_ms": prof, "kernel_share": {k: v / total for k, v in shares.items() if v > 0},
+        "stage_kernels": "fused (k_stage)" if fused else "split (k_prim, k_faces, k_nodes)",
     }
     # stage-level view: the compulsory bytes of a fused stage per cell-stage
     # (5 words read U(k-1), 5 read U^n, 5 written, dt/V, 3 face vectors of
-    # 3 FP64 words) at the measured cell-stage rate
-    b_stage = 8.0 * 16 + 8.0 * 3 * 3
+    # 3 FP64 words, 14 BFM words at blade-row nodes) at the measured
+    # cell-stage rate
+    b_stage = stage_bytes_per_cell(case)
     line["stage_roofline"] = {"bytes_per_cell_stage": b_stage, "achieved": value * b_stage / 1e9,
                               "peak": peak, "unit": "GB/s", "frac": value * b_stage / 1e9 / peak}
     if fp32:

@@ -130,6 +130,7 @@ int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out) {
         out->time = c.t;
         out->device_bytes = static_cast<int64_t>(s->solver->deviceBytes());
         for (int d = 0; d < 3; d++) out->face_tile[d] = s->solver->faceTile(d);
+        out->fused_stage = s->solver->fusedStage() ? 1 : 0;
         return CTBFM_OK;
     });
 }

@@ -90,10 +90,10 @@ extern template struct Launcher<float>;
 
 constexpr int kKernelKinds = 11;
 constexpr int kTileSize = 256;  // elements per tile (one per thread)
-// fused stage kernel: nodes per box (one per thread) and the faces of one
-// direction a box may hold in shared memory
+// fused stage kernel: nodes per box (one per thread) and the faces (all
+// directions) a box may hold in shared memory
 constexpr int kFusedBoxNodes = 256;
-constexpr int kFusedFaceCap = 384;
+constexpr int kFusedFaceCap = 1024;
 // periodic (i, j) pairs per tile, one block of as many threads each: the
 // periodic planes hold few pairs with much work each (7 680 on the bench
 // workload: 120 blocks instead of 30)

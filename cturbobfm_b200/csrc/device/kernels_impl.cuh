@@ -1180,9 +1180,10 @@ cudaError_t Launcher<R>::nodes(const BatchView<R>& b, int stage, int force, cuda
 
 template <typename R>
 size_t Launcher<R>::fusedSmemBytes(int bi, int bj, int bk, int topo, int scheme) {
-    const int hk = topo == 1 ? 2 : 0;
-    const size_t np = static_cast<size_t>(bi + 4) * (bj + 4) * (bk + 2 * hk);
-    return ((scheme == 0 ? 7 : 5) * np + 5 * static_cast<size_t>(kFusedFaceCap)) * sizeof(R);
+    FusedBox b;
+    fusedLayout(bi, bj, bk, topo == 1, b);
+    return (static_cast<size_t>(fusedNodeFields(scheme)) * b.nW + 5 * static_cast<size_t>(b.nfI + b.nfJ + b.nfK)) *
+           sizeof(R);
 }
 
 namespace {

@@ -26,6 +26,11 @@ Batch::Batch(const std::vector<Solver*>& members) : members_(members) {
         for (Solver* m : members_) v.push_back(m->instance64());
         g64_ = std::make_unique<GroupT<double>>(v);
     }
+    // the fused stage kernel unless a member asks for the split stage
+    int fusion = 1;
+    for (Solver* m : members_) fusion = std::min(fusion, m->stageFusion());
+    if (g32_) g32_->setFusedMode(fusion);
+    else g64_->setFusedMode(fusion);
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = ownStream_;
     cudaCheck(cudaMalloc(reinterpret_cast<void**>(&dCtl_), members_.size() * sizeof(Control)), "cudaMalloc");

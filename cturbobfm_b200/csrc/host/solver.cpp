@@ -139,6 +139,13 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     if (prec == "fp64") prec_ = kFP64;
     else if (prec == "fp32_kahan") prec_ = kFP32Kahan;
     else throw ConfigError("Invalid value for key \"GPU_PRECISION\" (fp64 or fp32_kahan)");
+    // GPU_STAGE_FUSION (this library's key): the fused stage kernel
+    // ("fused", the default) or the split stage kernels ("split"); results
+    // are the same
+    const std::string fusion = config.has("GPU_STAGE_FUSION") ? config.get("GPU_STAGE_FUSION") : "fused";
+    if (fusion == "fused") fusion_ = 1;
+    else if (fusion == "split") fusion_ = 0;
+    else throw ConfigError("Invalid value for key \"GPU_STAGE_FUSION\" (fused or split)");
     coeffs_ = config.getTimeIntegrationCoeffs();
     maxIter_ = config.getMaxIterations();
     // every setting and input file is validated before the first CUDA call,
@@ -166,11 +173,13 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
         i32_ = std::make_unique<InstanceT<float>>();
         uploadArrays(*i32_);
         g32_ = std::make_unique<GroupT<float>>(std::vector<InstanceT<float>*>{i32_.get()});
+        g32_->setFusedMode(fusion_);
         initializeState(*i32_, *g32_);
     } else {
         i64_ = std::make_unique<InstanceT<double>>();
         uploadArrays(*i64_);
         g64_ = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{i64_.get()});
+        g64_->setFusedMode(fusion_);
         initializeState(*i64_, *g64_);
     }
     // host-to-device copies from pageable memory may still be in flight when
@@ -603,31 +612,51 @@ void Solver::setupScalars() {
     c.hist_cap = std::min<long long>(std::max<long long>(maxIter_, 1024), 1 << 20);
     c.max_it = maxIter_;
     // fused stage kernel: inviscid instances without the Chima / Correlations
-    // forces; box of at most kFusedBoxNodes nodes, k (the contiguous index)
-    // up to 16 wide in 3-D, j up to 32 wide in 2-D (where j is contiguous),
-    // no direction holding more than kFusedFaceCap faces
+    // forces. The box (at most kFusedBoxNodes nodes, one per thread) is
+    // chosen to carry the most nodes per round of face evaluations (a block's
+    // faces are a pool of 256 per round; the primitives and the node phase
+    // weigh in less), counting the nodes the grid's ragged last boxes leave
+    // out, with k (the contiguous index) 16 or 32 wide in 3-D, within
+    // kFusedFaceCap faces and the shared memory of 3 (Roe) or 2 (JST) blocks
+    // per SM in FP64
     c.fuse_ok = (!c.viscous && !bfmRareModel(c)) ? 1 : 0;
-    int bi, bj, bk;
-    if (c.topo == 1) {
-        bk = std::min(c.nk, 16);
-        bj = std::min(c.nj, 4);
-    } else {
-        bk = 1;
-        bj = std::min(c.nj, 32);
+    {
+        const bool three = c.topo == 1;
+        const int fields = c.scheme == 0 ? 7 : 5;
+        const size_t smemMax = size_t(c.scheme == 0 ? 104 : 70) << 10;
+        double best = -1.0;
+        int bb[3] = {1, 1, 1};
+        std::vector<int> bks;
+        if (three) {
+            for (int w : {16, 32}) bks.push_back(std::min(c.nk, w));
+        } else {
+            bks.push_back(1);
+        }
+        for (int bk : bks)
+            for (int bj = 1; bj <= std::min(c.nj, 64); bj++)
+                for (int bi = 1; bi <= std::min(c.ni, kFusedBoxNodes / (bj * bk)); bi++) {
+                    const int nodes = bi * bj * bk;
+                    const int faces = (bi + 1) * bj * bk + bi * (bj + 1) * bk + (three ? bi * bj * (bk + 1) : 0);
+                    const int nW = nodes + 4 * bj * bk + 4 * bi * bk + (three ? 4 * bi * bj : 0);
+                    if (nodes > kFusedBoxNodes || faces > kFusedFaceCap) continue;
+                    if ((static_cast<size_t>(fields) * nW + 5 * static_cast<size_t>(faces)) * 8 > smemMax) continue;
+                    const double boxes = std::ceil(double(c.ni) / bi) * std::ceil(double(c.nj) / bj) *
+                                         std::ceil(double(c.nk) / bk);
+                    const double cost = std::ceil(faces / 256.0) + 0.15 * std::ceil(nW / 256.0) + 0.5;
+                    const double score = double(c.n) / boxes / cost;
+                    if (score > best + 1e-9) {
+                        best = score;
+                        bb[0] = bi;
+                        bb[1] = bj;
+                        bb[2] = bk;
+                    }
+                }
+        if (best < 0) c.fuse_ok = 0;
+        for (int d = 0; d < 3; d++) c.fbox[d] = bb[d];
     }
-    bi = std::max(1, std::min(c.ni, kFusedBoxNodes / (bj * bk)));
-    auto facesFit = [&] {
-        return (bi + 1) * bj * bk <= kFusedFaceCap && bi * (bj + 1) * bk <= kFusedFaceCap &&
-               bi * bj * (bk + 1) <= kFusedFaceCap;
-    };
-    while (bi > 1 && !facesFit()) bi--;
-    if (!facesFit()) c.fuse_ok = 0;
-    c.fbox[0] = bi;
-    c.fbox[1] = bj;
-    c.fbox[2] = bk;
-    c.fnb[0] = (c.ni + bi - 1) / bi;
-    c.fnb[1] = (c.nj + bj - 1) / bj;
-    c.fnb[2] = (c.nk + bk - 1) / bk;
+    c.fnb[0] = (c.ni + c.fbox[0] - 1) / c.fbox[0];
+    c.fnb[1] = (c.nj + c.fbox[1] - 1) / c.fbox[1];
+    c.fnb[2] = (c.nk + c.fbox[2] - 1) / c.fbox[2];
     c.nboxes = c.fnb[0] * c.fnb[1] * c.fnb[2];
 }
 
@@ -1119,7 +1148,12 @@ void Solver::computeResidualNoAlloc(double* dt, double* const r[5]) {
             off += 5 * nf;
         }
         grp.refresh(stream_);
-        residualSequence(grp.view(), stream_);
+        // the split stage, whose face kernels write the per-face flux
+        // contributions the scratch holds (the fused stage kernel keeps them
+        // in shared memory and would leave the scratch unused)
+        BatchView<R> split = grp.view();
+        split.fusedMode = 0;
+        residualSequence(split, stream_);
         guard.active = false;
         for (int d = 0; d < 3; d++) inst.c.f[d] = guard.saved[d];
         grp.refresh(stream_);
@@ -1358,7 +1392,9 @@ void Solver::profileKernels(int reps, double* outMs) {
     visit([&](auto& inst, auto& grp) {
         using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
         using L = Launcher<R>;
-        const BatchView<R>& v = grp.view();
+        const BatchView<R>& fv = grp.view();
+        BatchView<R> v = fv;  // the split stage kernels of every member
+        v.fusedMode = 0;
         const long N = mesh_.nodes();
         std::vector<R> dtSaved(N);
         cudaCheck(cudaMemcpy(dtSaved.data(), inst.c.dt, N * sizeof(R), cudaMemcpyDeviceToHost), "cudaMemcpy");
@@ -1386,6 +1422,11 @@ void Solver::profileKernels(int reps, double* outMs) {
         if (inst.c.periodic) timeIt(7, [&] { cudaCheck(L::periodic(v, 0, 1, stream_), "k_periodic"); });
         timeIt(8, [&] { cudaCheck(L::finalize(v, 1, stream_), "k_finalize"); });
         timeIt(9, [&] { cudaCheck(L::prim(v, 0, 1, stream_), "k_prim"); });
+        if (inst.c.fuse_ok) {
+            BatchView<R> f = fv;
+            f.fusedMode = 1;
+            timeIt(10, [&] { cudaCheck(L::fused(f, 0, 1, stream_), "k_stage"); });
+        }
         (void)lastStage;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -1411,6 +1452,7 @@ void Solver::promoteToFP64() {
     auto inst = std::make_unique<InstanceT<double>>();
     uploadArrays(*inst);
     auto grp = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{inst.get()});
+    grp->setFusedMode(fusion_);
     const DevCaseT<float>& f = i32_->c;
     if (proto_.nprofiles)
         cudaCheck(cudaMemcpy(inst->c.prof_p, f.prof_p, profP_.size() * sizeof(double), cudaMemcpyDeviceToDevice),

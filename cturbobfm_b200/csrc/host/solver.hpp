@@ -49,8 +49,13 @@ public:
     void setStream(cudaStream_t s) { stream_ = s ? s : ownStream_; }
     cudaStream_t stream() const { return stream_; }
     int precision() const { return prec_; }
+    int stageFusion() const { return fusion_; }
     bool realGas() const { return table_ != nullptr; }
     int faceTile(int d) const { return g64_ ? g64_->faceTile(d) : g32_->faceTile(d); }
+    // the group runs the fused stage kernel and this instance can run it
+    bool fusedStage() const {
+        return g64_ ? (g64_->fusedMode() && i64_->c.fuse_ok) : (g32_->fusedMode() && i32_->c.fuse_ok);
+    }
 
     // Enqueues n iterations (no host sync). Kernels of iterations after
     // convergence / divergence return immediately.
@@ -122,6 +127,7 @@ private:
     std::vector<double> coeffs_;
     long maxIter_ = 0;
     int prec_ = kFP64;
+    int fusion_ = 1;  // GPU_STAGE_FUSION: 1 fused stage kernel, 0 split stage kernels
     std::unique_ptr<AdvectionBase> advection_;
     std::unique_ptr<SourceBFMBase> bfm_;
     std::unique_ptr<FluidTable> table_;  // FLUID_MODEL = real

@@ -53,6 +53,7 @@ class Info(ctypes.Structure):
         ("time", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
         ("face_tile", ctypes.c_int32 * 3),
+        ("fused_stage", ctypes.c_int32),
     ]
 
 
@@ -250,7 +251,7 @@ class Solver:
         return mf, tp
 
     KERNELS = ("k_bint", "k_dt", "k_pre", "k_faces_I", "k_faces_J", "k_faces_K", "k_nodes", "k_periodic",
-               "k_finalize", "k_prim")
+               "k_finalize", "k_prim", "k_stage")
 
     def profile_kernels(self, reps: int = 20) -> Dict[str, float]:
         """Average device time per launch (ms) of each kernel kind, CUDA events."""

@@ -75,6 +75,8 @@ typedef struct {
     double time;              /* physical time sum of min(dt) */
     int64_t device_bytes;     /* device memory the solver holds */
     int32_t face_tile[3];     /* faces per block chosen by the autotuner per direction (I, J, K) */
+    int32_t fused_stage;      /* 1: each Runge-Kutta stage runs as the fused kernel k_stage;
+                                 0: as the split kernels k_prim, k_faces, k_nodes */
 } ctbfm_info;
 
 /* Builds a solver from an input.ini in the reference's format (the grid CSV and
@@ -175,7 +177,8 @@ enum {
     CTBFM_K_PERIODIC = 7,           /* k_periodic (periodic cases) */
     CTBFM_K_FINALIZE = 8,           /* k_finalize */
     CTBFM_K_PRIMITIVES = 9,         /* k_prim */
-    CTBFM_K_COUNT = 10
+    CTBFM_K_STAGE = 10,             /* k_stage, the fused stage kernel (GPU_STAGE_FUSION = fused) */
+    CTBFM_K_COUNT = 11
 };
 
 /* Measurement hook (no counterpart in the reference): launches each kernel

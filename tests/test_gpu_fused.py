@@ -1,0 +1,77 @@
+"""The fused stage kernel (k_stage, GPU_STAGE_FUSION = fused, the default)
+against the split stage kernels (k_prim, k_faces, k_nodes; GPU_STAGE_FUSION =
+split) on the same case files. In FP64 every face flux and every node
+residual is the same value in both, so states, time steps and residuals agree
+bit for bit; only the residual-norm partials are summed over other tiles (one
+per box of nodes instead of one per 256 consecutive nodes), so the log10
+norms agree to rounding."""
+
+import numpy as np
+import pytest
+
+from cturbobfm_b200 import cases
+from parity_cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b):
+    scale = np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return (np.abs(a - b).max(axis=1) / scale).max()
+
+
+def _run(case, n, fusion, tmp_path, tag):
+    from cturbobfm_b200 import Solver
+
+    ini = case.with_settings(GPU_STAGE_FUSION=fusion).write(str(tmp_path / tag))
+    with Solver(ini) as s:
+        if fusion == "split":
+            assert s.info().fused_stage == 0
+        done = s.step(n)
+        return done, s.state(), s.history(), s.time, s.residual()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fused_stage_equals_split_stage(name, tmp_path):
+    make, n = CASES[name]
+    a = _run(make(), n, "split", tmp_path, "split")
+    b = _run(make(), n, "fused", tmp_path, "fused")
+    assert a[0] == b[0]
+    assert np.array_equal(a[1], b[1])
+    assert a[3] == b[3]
+    assert np.abs(a[2]["lognorm"] - b[2]["lognorm"]).max() <= 1e-12
+    assert np.array_equal(a[4][0], b[4][0])  # time step of the residual evaluation
+    assert np.array_equal(a[4][1], b[4][1])  # residual
+
+
+RAGGED = [(lambda: cases.annulus3d(ni=48, nj=20, nk=33, cfl=1.0), 6),
+          (lambda: cases.annulus3d(ni=30, nj=9, nk=17, scheme="JST", muscl=False, rk=4, bfm_model="Hall-Thollet"), 6),
+          (lambda: cases.meridional(ni=70, nj=37, rows=cases.MAP_ROWS), 12),
+          (lambda: cases.bump2d(ni=50, nj=33, scheme="Roe", muscl=True, limiter="min mod", rk=3, cfl=0.8), 12)]
+RAGGED_IDS = ["annulus_roe", "annulus_jst_thollet", "meridional_jst", "bump_roe_minmod"]
+
+
+@pytest.mark.parametrize("make,n", RAGGED, ids=RAGGED_IDS)
+def test_fused_stage_equals_split_stage_on_ragged_boxes_fp64(make, n, tmp_path):
+    """Grids whose extents are not multiples of the box (the last boxes along
+    each direction are clipped): bit for bit in FP64."""
+    a = _run(make(), n, "split", tmp_path, "split")
+    b = _run(make(), n, "fused", tmp_path, "fused")
+    assert a[0] == b[0]
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[4][1], b[4][1])
+
+
+@pytest.mark.parametrize("make,n", RAGGED, ids=RAGGED_IDS)
+def test_fused_stage_matches_split_stage_in_float(make, n, tmp_path):
+    """fp32_kahan: the float kernels are compiled with multiply-add contraction
+    and approximate division and square root, and the compiler may contract
+    the same expression differently in the two kernel bodies, so the two
+    float runs differ by rounding that the solver then carries along. The
+    bound is the float path's stated tolerance against the FP64 oracle (1e-3
+    relative per field; tests/test_gpu_precision.py)."""
+    c = make().with_settings(GPU_PRECISION="fp32_kahan")
+    a = _run(c, n, "split", tmp_path, "split")
+    b = _run(c, n, "fused", tmp_path, "fused")
+    assert a[0] == b[0]
+    assert rel_err(b[1], a[1]) <= 1e-3
