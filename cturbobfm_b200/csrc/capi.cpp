@@ -131,6 +131,7 @@ int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out) {
         out->device_bytes = static_cast<int64_t>(s->solver->deviceBytes());
         for (int d = 0; d < 3; d++) out->face_tile[d] = s->solver->faceTile(d);
         out->fused_stage = s->solver->fusedStage() ? 1 : 0;
+        for (int m = 0; m < 2; m++) out->tuned_stage_ms[m] = s->solver->tunedStageMs(m);
         return CTBFM_OK;
     });
 }
@@ -148,6 +149,14 @@ int ctbfm_enqueue(ctbfm_solver* s, int64_t n_iter) {
     if (!s || n_iter < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
     return guarded([&] {
         s->solver->enqueue(n_iter);
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_autotune(ctbfm_solver* s) {
+    if (!s) return setError(CTBFM_E_ARGUMENT, "null solver");
+    return guarded([&] {
+        s->solver->autotune();
         return CTBFM_OK;
     });
 }
@@ -288,6 +297,14 @@ int ctbfm_batch_enqueue(ctbfm_batch* b, int64_t n_iter) {
     if (!b || n_iter < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
     return guarded([&] {
         b->batch->enqueue(n_iter);
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_batch_autotune(ctbfm_batch* b) {
+    if (!b) return setError(CTBFM_E_ARGUMENT, "null batch");
+    return guarded([&] {
+        b->batch->autotune();
         return CTBFM_OK;
     });
 }

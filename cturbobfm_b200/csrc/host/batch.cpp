@@ -26,9 +26,10 @@ Batch::Batch(const std::vector<Solver*>& members) : members_(members) {
         for (Solver* m : members_) v.push_back(m->instance64());
         g64_ = std::make_unique<GroupT<double>>(v);
     }
-    // the fused stage kernel unless a member asks for the split stage
-    int fusion = 1;
-    for (Solver* m : members_) fusion = std::min(fusion, m->stageFusion());
+    // the split stage if a member asks for it, else the fused stage if a
+    // member asks for it, else autotuned
+    int fusion = 2;
+    for (Solver* m : members_) fusion = std::min(fusion, m->stageFusion() == 0 ? 0 : (m->stageFusion() == 1 ? 1 : 2));
     if (g32_) g32_->setFusedMode(fusion);
     else g64_->setFusedMode(fusion);
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -50,6 +51,12 @@ Batch::~Batch() {
 void Batch::enqueue(long long n) {
     if (g32_) g32_->enqueue(n, stream_);
     else g64_->enqueue(n, stream_);
+}
+
+void Batch::autotune() {
+    if (g32_ && !g32_->tuned()) g32_->tune(stream_);
+    if (g64_ && !g64_->tuned()) g64_->tune(stream_);
+    cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
 }
 
 void Batch::controls(Control* out) {

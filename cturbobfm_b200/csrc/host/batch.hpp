@@ -31,6 +31,8 @@ public:
 
     // n iterations of every member still running, no host synchronisation
     void enqueue(long long n);
+    // runs the group's autotuner now (face tiles, stage fusion) unless it has run
+    void autotune();
     // enqueue + synchronise; returns the most iterations any member advanced
     long long step(long long n);
     // every member's control block (synchronous), out[0..size())

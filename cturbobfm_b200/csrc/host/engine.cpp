@@ -218,13 +218,44 @@ void GroupT<R>::tune(cudaStream_t s) {
         faceTile_[d] = bestSize;
     }
     view_.fusedMode = mode;
+    buildTiles();
+    // stage fusion: forced stage-0 evaluations (they rewrite only the first
+    // stage buffer and the periodic residuals, which the next stage 0
+    // recomputes) with the split and with the fused stage kernels; the fused
+    // kernel is kept when at least 2 % faster
+    bool anyFused = false;
+    for (auto* m : members_) anyFused = anyFused || m->c.fuse_ok;
+    if (fusionAuto_ && anyFused) {
+        float ms[2] = {0.f, 0.f};
+        for (int mode2 = 0; mode2 < 2; mode2++) {
+            view_.fusedMode = mode2;
+            cudaCheck(Launcher<R>::stage(view_, 0, 1, s), "launch stage (tuning)");
+            cudaCheck(cudaEventRecord(e0, s), "cudaEventRecord");
+            for (int r = 0; r < 3; r++) cudaCheck(Launcher<R>::stage(view_, 0, 1, s), "launch stage (tuning)");
+            cudaCheck(cudaEventRecord(e1, s), "cudaEventRecord");
+            cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            cudaCheck(cudaEventElapsedTime(&ms[mode2], e0, e1), "cudaEventElapsedTime");
+        }
+        stageMs_[0] = ms[0] / 3;
+        stageMs_[1] = ms[1] / 3;
+        view_.fusedMode = ms[1] < 0.98f * ms[0] ? 1 : 0;
+        if (graph_) {
+            cudaGraphExecDestroy(graph_);
+            graph_ = nullptr;
+        }
+        if (graph1_) {
+            cudaGraphExecDestroy(graph1_);
+            graph1_ = nullptr;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    buildTiles();
 }
 
 template <typename R>
 void GroupT<R>::setFusedMode(int mode) {
+    fusionAuto_ = mode == 2;
+    if (mode == 2) mode = sizeof(R) == sizeof(float) ? 1 : 0;  // until the autotuner has timed both
     if ((mode != 0) == (view_.fusedMode != 0)) return;
     view_.fusedMode = mode != 0 ? 1 : 0;
     if (graph_) {

@@ -69,11 +69,16 @@ public:
     void tune(cudaStream_t s);
     void setAutotune(bool on) { autotune_ = on; }
     // Stage kernels: 0 the split stage for every member, 1 the fused stage
-    // kernel for the members that can run it (the others split). Results are
-    // the same either way; the captured graphs are rebuilt.
+    // kernel for the members that can run it (the others split), 2 chosen by
+    // the autotuner (until it has run: fused in float, split in double, the
+    // faster ones on the workloads measured). FP64 results are the same
+    // either way; the captured graphs are rebuilt.
     void setFusedMode(int mode);
+    bool tuned() const { return tuned_; }
     int fusedMode() const { return view_.fusedMode; }
     int faceTile(int d) const { return faceTile_[d]; }
+    // the autotuner's stage timings (ms per stage: split, fused; 0 untimed)
+    float stageMs(int mode) const { return stageMs_[mode]; }
     static constexpr long long kTuneMinIterations = 64;
 
 private:
@@ -90,8 +95,10 @@ private:
     cudaGraphExec_t graph1_ = nullptr;  // one iteration
     int graphIters_ = 8;
     int faceTile_[3] = {kTileSize, kTileSize, kTileSize};
+    float stageMs_[2] = {0.f, 0.f};
     bool tuned_ = false;
     bool autotune_ = true;
+    bool fusionAuto_ = false;
 };
 
 extern template class InstanceT<double>;

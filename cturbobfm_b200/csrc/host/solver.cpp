@@ -140,12 +140,14 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     else if (prec == "fp32_kahan") prec_ = kFP32Kahan;
     else throw ConfigError("Invalid value for key \"GPU_PRECISION\" (fp64 or fp32_kahan)");
     // GPU_STAGE_FUSION (this library's key): the fused stage kernel
-    // ("fused", the default) or the split stage kernels ("split"); results
-    // are the same
-    const std::string fusion = config.has("GPU_STAGE_FUSION") ? config.get("GPU_STAGE_FUSION") : "fused";
+    // ("fused"), the split stage kernels ("split") or the faster of the two
+    // as the autotuner measures them ("auto", the default); FP64 results are
+    // the same either way
+    const std::string fusion = config.has("GPU_STAGE_FUSION") ? config.get("GPU_STAGE_FUSION") : "auto";
     if (fusion == "fused") fusion_ = 1;
     else if (fusion == "split") fusion_ = 0;
-    else throw ConfigError("Invalid value for key \"GPU_STAGE_FUSION\" (fused or split)");
+    else if (fusion == "auto") fusion_ = 2;
+    else throw ConfigError("Invalid value for key \"GPU_STAGE_FUSION\" (auto, fused or split)");
     coeffs_ = config.getTimeIntegrationCoeffs();
     maxIter_ = config.getMaxIterations();
     // every setting and input file is validated before the first CUDA call,
@@ -1021,6 +1023,14 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
 
 void Solver::enqueue(long long n) {
     visit([&](auto& inst, auto& grp) { grp.enqueue(n, stream_); (void)inst; });
+}
+
+void Solver::autotune() {
+    visit([&](auto& inst, auto& grp) {
+        (void)inst;
+        if (!grp.tuned()) grp.tune(stream_);
+    });
+    cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
 }
 
 Control Solver::control() {

@@ -52,6 +52,7 @@ public:
     int stageFusion() const { return fusion_; }
     bool realGas() const { return table_ != nullptr; }
     int faceTile(int d) const { return g64_ ? g64_->faceTile(d) : g32_->faceTile(d); }
+    double tunedStageMs(int mode) const { return g64_ ? g64_->stageMs(mode) : g32_->stageMs(mode); }
     // the group runs the fused stage kernel and this instance can run it
     bool fusedStage() const {
         return g64_ ? (g64_->fusedMode() && i64_->c.fuse_ok) : (g32_->fusedMode() && i32_->c.fuse_ok);
@@ -60,6 +61,8 @@ public:
     // Enqueues n iterations (no host sync). Kernels of iterations after
     // convergence / divergence return immediately.
     void enqueue(long long n);
+    // runs the group's autotuner now (face tiles, stage fusion) unless it has run
+    void autotune();
     // Runs up to n iterations; returns iterations done; syncs.
     long long step(long long n);
     long long solve();
@@ -127,7 +130,7 @@ private:
     std::vector<double> coeffs_;
     long maxIter_ = 0;
     int prec_ = kFP64;
-    int fusion_ = 1;  // GPU_STAGE_FUSION: 1 fused stage kernel, 0 split stage kernels
+    int fusion_ = 2;  // GPU_STAGE_FUSION: 0 split stage kernels, 1 fused stage kernel, 2 autotuned
     std::unique_ptr<AdvectionBase> advection_;
     std::unique_ptr<SourceBFMBase> bfm_;
     std::unique_ptr<FluidTable> table_;  // FLUID_MODEL = real

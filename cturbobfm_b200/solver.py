@@ -54,6 +54,7 @@ class Info(ctypes.Structure):
         ("device_bytes", ctypes.c_int64),
         ("face_tile", ctypes.c_int32 * 3),
         ("fused_stage", ctypes.c_int32),
+        ("tuned_stage_ms", ctypes.c_double * 2),
     ]
 
 
@@ -86,6 +87,7 @@ SIGNATURES = {
     "ctbfm_get_info": ([_VP, ctypes.POINTER(Info)], ctypes.c_int),
     "ctbfm_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_enqueue": ([_VP, _I64], ctypes.c_int),
+    "ctbfm_autotune": ([_VP], ctypes.c_int),
     "ctbfm_solve": ([_VP, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_compute_residual": ([_VP] + [_DP] * 6, ctypes.c_int),
     "ctbfm_compute_residual_noalloc": ([_VP] + [_DP] * 6, ctypes.c_int),
@@ -101,6 +103,7 @@ SIGNATURES = {
     "ctbfm_batch_destroy": ([_VP], None),
     "ctbfm_batch_set_stream": ([_VP, _VP], ctypes.c_int),
     "ctbfm_batch_enqueue": ([_VP, _I64], ctypes.c_int),
+    "ctbfm_batch_autotune": ([_VP], ctypes.c_int),
     "ctbfm_batch_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_batch_status": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_I64), _DP, _DP], ctypes.c_int),
     "ctbfm_promote_fp64": ([_VP], ctypes.c_int),
@@ -192,6 +195,10 @@ class Solver:
 
     def enqueue(self, n_iter: int):
         _check(load_library().ctbfm_enqueue(self._h, int(n_iter)))
+
+    def autotune(self):
+        """ctbfm_autotune: face tiles and stage fusion, timed now."""
+        _check(load_library().ctbfm_autotune(self._h))
 
     def solve(self) -> int:
         done = _I64()
@@ -310,6 +317,10 @@ class Batch:
 
     def enqueue(self, n_iter: int):
         _check(load_library().ctbfm_batch_enqueue(self._h, int(n_iter)))
+
+    def autotune(self):
+        """ctbfm_batch_autotune: face tiles and stage fusion, timed now."""
+        _check(load_library().ctbfm_batch_autotune(self._h))
 
     def step(self, n_iter: int) -> int:
         done = _I64(0)

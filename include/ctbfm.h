@@ -77,6 +77,7 @@ typedef struct {
     int32_t face_tile[3];     /* faces per block chosen by the autotuner per direction (I, J, K) */
     int32_t fused_stage;      /* 1: each Runge-Kutta stage runs as the fused kernel k_stage;
                                  0: as the split kernels k_prim, k_faces, k_nodes */
+    double tuned_stage_ms[2]; /* the autotuner's time of one stage, split and fused (0: not timed) */
 } ctbfm_info;
 
 /* Builds a solver from an input.ini in the reference's format (the grid CSV and
@@ -103,6 +104,13 @@ int ctbfm_step(ctbfm_solver* s, int64_t n_iter, int64_t* n_done);
  * synchronisation (kernels of iterations after convergence or divergence
  * return immediately). For timing and CUDA-graph capture. */
 int ctbfm_enqueue(ctbfm_solver* s, int64_t n_iter);
+
+/* Runs the autotuner now unless it has run (otherwise it runs at the first
+ * enqueue of at least 64 iterations): face tiles per direction, and with
+ * GPU_STAGE_FUSION = auto whether the fused or the split stage kernels are
+ * faster, timed on forced first-stage evaluations that leave the state
+ * unchanged. Synchronises the stream. No counterpart in the reference. */
+int ctbfm_autotune(ctbfm_solver* s);
 
 /* Runs the whole loop to N_ITERATIONS or convergence, like Solver::solve(). */
 int ctbfm_solve(ctbfm_solver* s, int64_t* n_done);
@@ -210,6 +218,9 @@ int ctbfm_batch_set_stream(ctbfm_batch* b, void* cuda_stream);
 /* Enqueues n_iter iterations of every member that is still running (members
  * that converge or diverge stop on the device at that iteration). */
 int ctbfm_batch_enqueue(ctbfm_batch* b, int64_t n_iter);
+
+/* ctbfm_autotune for the batch's group. */
+int ctbfm_batch_autotune(ctbfm_batch* b);
 
 /* enqueue + synchronise. *n_done (nullable) receives the most iterations any
  * member advanced. A diverged member is reported through
