@@ -442,6 +442,15 @@ def run_ours(args):
                               "peak": peak, "unit": "GB/s", "frac": value * b_stage / 1e9 / peak}
     if fp32:
         line["fp32_kahan"] = fp32
+    if world == 1 and not args.no_map:
+        # the north-star workload beside the annulus line: converged
+        # op-points/hour of the batched compressor map (fp32_kahan and FP64),
+        # the plain FP64 path and the reference build on the host cores
+        m = map_line(args)
+        nc = m.pop("not_converged")
+        m["not_converged_count"] = len(nc)
+        m["not_converged_first"] = nc[:5]
+        line["map"] = m
     if world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(case, args.cpu_iters, one_core_iters=3)
         line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample", "value_1_core",
@@ -454,18 +463,21 @@ def run_ours(args):
 MAP_METRIC = "converged op-points/hour"
 MAP_WORKLOAD = ("compressor map: 256 axisymmetric BFM instances (Hall, MAP_ROWS stage), NI x NJ ~ U{64..256} x "
                 "U{24..96}, p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], PCG64 seed 20261203, JST, RK4, local dt "
-                "CFL 2.2, outlet ramp 2000 its, residual drop 3 orders")
+                "CFL 2.2, outlet ramp 2000 its, residual drop {drop} orders")
 
 
-def _map_launches_per_iteration(case) -> int:
-    # k_bint, k_dt, k_pre, per stage k_prim + k_faces I + k_faces J + k_nodes, k_finalize
-    return 3 + 4 * case.n_stages + 1
+def _map_launches_per_iteration(case, fused: bool) -> int:
+    # k_bint, k_dt, k_pre, per stage k_stage (fused) or k_prim + k_faces I +
+    # k_faces J + k_nodes (split), k_finalize
+    return 3 + (1 if fused else 4) * case.n_stages + 1
 
 
-def _solve_batched(solvers, stream, chunk: int, n_iter: int, per_iteration: int):
+def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
     """Runs the batch to convergence (or N_ITERATIONS) in chunks, dropping
-    finished members from the batch whenever a quarter of it has finished.
-    Returns (per-member status, iterations, launches)."""
+    finished members from the batch whenever a quarter of it has finished;
+    each batch is autotuned (face tiles, stage fusion) before it runs.
+    Returns (per-member status, iterations, launches, the first batch's
+    stage kernels and tuned stage times)."""
     import numpy as np
 
     from cturbobfm_b200 import Batch
@@ -475,9 +487,16 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, per_iteration: int)
     iters = np.zeros(m, np.int64)
     active = list(range(m))
     launches = 0
+    first = None
     while active:
         with Batch([solvers[i] for i in active]) as b:
             b.set_stream(stream.cuda_stream)
+            b.autotune()
+            fused, stage_ms = b.stage_kernels()
+            if first is None:
+                first = {"stage_kernels": "fused (k_stage)" if fused else "split (k_prim, k_faces, k_nodes)",
+                         "stage_autotuned_ms": {"split": stage_ms[0], "fused": stage_ms[1]}}
+            per_iteration = _map_launches_per_iteration(case, fused)
             start = len(active)
             while True:
                 b.step(chunk)
@@ -490,7 +509,7 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, per_iteration: int)
                 if len(done) * 4 >= start or len(done) == len(active):
                     break
         active = [i for i in active if not (status[i] != 0 or iters[i] >= n_iter)]
-    return status, iters, launches
+    return status, iters, launches, first
 
 
 def map_cpu_baseline(inis, iterations, n_iter: int):
@@ -534,6 +553,13 @@ def map_cpu_baseline(inis, iterations, n_iter: int):
 
 
 def run_map(args):
+    print(json.dumps(map_line(args)), flush=True)
+
+
+def map_line(args):
+    """The compressor-map measurement (batched fp32_kahan, batched FP64, the
+    plain FP64 path one instance at a time, the reference build on the host
+    cores) as one JSON-ready dict."""
     import numpy as np
     import torch
 
@@ -541,8 +567,7 @@ def run_map(args):
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
-    cs32 = cases.compressor_map(n=args.map_n, precision="fp32_kahan")
-    per_iteration = _map_launches_per_iteration(cs32[0])
+    cs32 = cases.compressor_map(n=args.map_n, precision="fp32_kahan", drop=args.map_drop)
     n_iter = int(cs32[0].settings["N_ITERATIONS"])
     tmp = tempfile.TemporaryDirectory()
 
@@ -570,7 +595,7 @@ def run_map(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            status, iters, launches = _solve_batched(solvers, stream, args.map_chunk, n_iter, per_iteration)
+            status, iters, launches, kern = _solve_batched(solvers, stream, args.map_chunk, n_iter, cs32[0])
             e1.record(stream)
             torch.cuda.synchronize()
             sec = e0.elapsed_time(e1) / 1e3
@@ -587,7 +612,7 @@ def run_map(args):
                             "e2e_points_per_hour": conv / (setup + sec + readback) * 3600.0,
                             "iterations": iters.tolist(), "turbo": turbo, "status": status,
                             "node_stage_per_s": float((nodes * iters).sum() * 4 / sec), "launches": launches,
-                            "device_bytes": bytes_up}
+                            "device_bytes": bytes_up, **kern}
         # the plain FP64 path: one drop-in solver at a time, to convergence
         sample = list(range(min(args.map_plain, len(inis64))))
         plain_sec, plain_conv, plain = 0.0, 0, []
@@ -621,14 +646,16 @@ def run_map(args):
         "steps": len(cs32), "warmup": 0, "ms_per_step": r32["seconds"] * 1e3 / max(1, len(cs32)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+kahan (f64 integrals)",
         "data": "synthetic",
-        "config": {"workload": MAP_WORKLOAD, "instances": len(cs32), "nodes_total": int(nodes.sum()),
+        "config": {"workload": MAP_WORKLOAD.format(drop=args.map_drop), "instances": len(cs32),
+                   "nodes_total": int(nodes.sum()),
                    "chunk_iterations": args.map_chunk, "l2": "inputs larger than L2 (working set > 126 MiB)"},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "e2e": {"value": r32["e2e_points_per_hour"], "unit": "points/hour",
                 "h2d_bytes_per_step": r32["device_bytes"] / len(cs32), "d2h_bytes_per_step": 6 * 8 + 4 * 8},
         "gpu_launches": r32["launches"],
         "batched_fp32_kahan": {k: r32[k] for k in ("seconds", "setup_seconds", "converged", "diverged",
-                                                   "points_per_hour", "node_stage_per_s")},
+                                                   "points_per_hour", "node_stage_per_s", "stage_kernels",
+                                                   "stage_autotuned_ms")},
         "plain_fp64": {"points_per_hour": plain_pph, "instances": len(sample), "converged": plain_conv,
                        "seconds": plain_sec, "iterations": [p[1] for p in plain]},
         "speedup_vs_plain_fp64": (r32["points_per_hour"] / plain_pph) if plain_pph else None,
@@ -640,7 +667,7 @@ def run_map(args):
     if "batched_fp64" in results:
         r64 = results["batched_fp64"]
         line["batched_fp64"] = {k: r64[k] for k in ("seconds", "converged", "diverged", "points_per_hour",
-                                                    "node_stage_per_s")}
+                                                    "node_stage_per_s", "stage_kernels", "stage_autotuned_ms")}
         both = (r32["status"] == 1) & (r64["status"] == 1)
         if both.any():
             emf = np.abs(r32["turbo"][both, 0] - r64["turbo"][both, 0]) / np.abs(r64["turbo"][both, 0])
@@ -666,7 +693,7 @@ def run_map(args):
                                     args.cpu_iters * 10)
             if base:
                 line["cpu_baseline"] = base
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # --------------------------------------------------------------- real gas
@@ -932,6 +959,8 @@ def main():
                     help="annulus: the 160x48x64 full-annulus loop (default); map: the batched compressor map; "
                          "serve: continuous batching of arriving requests")
     ap.add_argument("--map-n", type=int, default=256)
+    ap.add_argument("--map-drop", type=int, default=4, help="RESIDUALS_DROP_CONVERGENCE of the map instances")
+    ap.add_argument("--no-map", action="store_true", help="leave the compressor-map object out of the default line")
     ap.add_argument("--map-chunk", type=int, default=250)
     ap.add_argument("--map-plain", type=int, default=8, help="instances solved one at a time on the plain FP64 path")
     ap.add_argument("--map-skip-fp64-batch", action="store_true")

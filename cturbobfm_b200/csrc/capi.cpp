@@ -309,6 +309,15 @@ int ctbfm_batch_autotune(ctbfm_batch* b) {
     });
 }
 
+int ctbfm_batch_stage_kernels(ctbfm_batch* b, int32_t* fused, double stage_ms[2]) {
+    if (!b || !fused || !stage_ms) return setError(CTBFM_E_ARGUMENT, "bad argument");
+    return guarded([&] {
+        *fused = b->batch->fusedMode();
+        for (int m = 0; m < 2; m++) stage_ms[m] = b->batch->stageMs(m);
+        return CTBFM_OK;
+    });
+}
+
 int ctbfm_batch_step(ctbfm_batch* b, int64_t n_iter, int64_t* n_done) {
     if (!b || n_iter < 0) return setError(CTBFM_E_ARGUMENT, "bad argument");
     return guarded([&] {

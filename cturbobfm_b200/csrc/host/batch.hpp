@@ -33,6 +33,8 @@ public:
     void enqueue(long long n);
     // runs the group's autotuner now (face tiles, stage fusion) unless it has run
     void autotune();
+    int fusedMode() const { return g32_ ? g32_->fusedMode() : g64_->fusedMode(); }
+    double stageMs(int mode) const { return g32_ ? g32_->stageMs(mode) : g64_->stageMs(mode); }
     // enqueue + synchronise; returns the most iterations any member advanced
     long long step(long long n);
     // every member's control block (synchronous), out[0..size())

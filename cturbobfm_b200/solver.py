@@ -104,6 +104,7 @@ SIGNATURES = {
     "ctbfm_batch_set_stream": ([_VP, _VP], ctypes.c_int),
     "ctbfm_batch_enqueue": ([_VP, _I64], ctypes.c_int),
     "ctbfm_batch_autotune": ([_VP], ctypes.c_int),
+    "ctbfm_batch_stage_kernels": ([_VP, ctypes.POINTER(ctypes.c_int32), _DP], ctypes.c_int),
     "ctbfm_batch_step": ([_VP, _I64, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_batch_status": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_I64), _DP, _DP], ctypes.c_int),
     "ctbfm_promote_fp64": ([_VP], ctypes.c_int),
@@ -321,6 +322,14 @@ class Batch:
     def autotune(self):
         """ctbfm_batch_autotune: face tiles and stage fusion, timed now."""
         _check(load_library().ctbfm_batch_autotune(self._h))
+
+    def stage_kernels(self):
+        """(fused, (split ms, fused ms)): the batch's stage kernels and the
+        autotuner's stage timings (ctbfm_batch_stage_kernels)."""
+        f = ctypes.c_int32(0)
+        ms = np.zeros(2)
+        _check(load_library().ctbfm_batch_stage_kernels(self._h, ctypes.byref(f), _ptr(ms)))
+        return bool(f.value), (float(ms[0]), float(ms[1]))
 
     def step(self, n_iter: int) -> int:
         done = _I64(0)

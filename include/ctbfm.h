@@ -222,6 +222,12 @@ int ctbfm_batch_enqueue(ctbfm_batch* b, int64_t n_iter);
 /* ctbfm_autotune for the batch's group. */
 int ctbfm_batch_autotune(ctbfm_batch* b);
 
+/* The batch's stage kernels: *fused = 1 when its members that can run the
+ * fused stage kernel k_stage do, and the autotuner's time of one stage of the
+ * whole batch with the split and with the fused kernels (0 when not timed).
+ * No counterpart in the reference. */
+int ctbfm_batch_stage_kernels(ctbfm_batch* b, int32_t* fused, double stage_ms[2]);
+
 /* enqueue + synchronise. *n_done (nullable) receives the most iterations any
  * member advanced. A diverged member is reported through
  * ctbfm_batch_status, not as an error of the call. */
