@@ -646,7 +646,7 @@ def map_line(args):
         "steps": len(cs32), "warmup": 0, "ms_per_step": r32["seconds"] * 1e3 / max(1, len(cs32)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+kahan (f64 integrals)",
         "data": "synthetic",
-        "config": {"workload": MAP_WORKLOAD.format(drop=args.map_drop), "instances": len(cs32),
+        "config": {"workload": MAP_WORKLOAD.replace("{drop}", str(args.map_drop)), "instances": len(cs32),
                    "nodes_total": int(nodes.sum()),
                    "chunk_iterations": args.map_chunk, "l2": "inputs larger than L2 (working set > 126 MiB)"},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
