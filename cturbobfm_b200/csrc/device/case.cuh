@@ -208,6 +208,10 @@ struct alignas(16) DevCaseT {
     R* S2[5];
     R* Rp[5];  // periodic-plane residuals (2 * ni * nj)
     R* W[5];   // primitives of the current stage input (k_prim)
+    // JST: pressure and spectral radius |u| + a of each node of the current
+    // stage input (k_prim; nullptr for Roe), read by the plain face stencils
+    R* Wp;
+    R* Wr;
     R* dt;
     // per-tile partials: [node_tiles*5 norms of the split stage |
     // per_tiles*5 periodic norms | node_tiles dt minima | nboxes*5 norms of

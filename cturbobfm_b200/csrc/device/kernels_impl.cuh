@@ -466,8 +466,9 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
             const bool plain = SET == 1 || (SET == 0 && dface >= 2 && dface <= nlast - 2);
             if (plain) {
                 if (SCHEME == 0) {
-                    flux = fluxJstW(gs, load5(U, qL - st), load5(U, qL), load5(U, qR), load5(U, qR + st),
-                                    load5(c.W, qL - st), load5(c.W, qL), load5(c.W, qR), load5(c.W, qR + st), n);
+                    flux = fluxJstPR(gs, load5(U, qL - st), load5(U, qL), load5(U, qR), load5(U, qR + st),
+                                     load5(c.W, qL), load5(c.W, qR), __ldg(c.Wp + qL - st), __ldg(c.Wp + qL),
+                                     __ldg(c.Wp + qR), __ldg(c.Wp + qR + st), __ldg(c.Wr + qL), __ldg(c.Wr + qR), n);
                 } else {
                     flux = fluxRoeW(gs, c.muscl, c.limiter, c.muscl ? load5(c.W, qL - st) : zero5<R>(),
                                     load5(c.W, qL), load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5<R>(), n);
@@ -502,15 +503,25 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
 }
 
 // Primitives of the stage input (getPrimitiveVariablesFromConservative,
-// src/math_utils.cpp:49-57), once per node for the face kernels.
+// src/math_utils.cpp:49-57), once per node for the face kernels; for JST
+// also each node's pressure and spectral radius |u| + a, which the JST flux
+// of every face reads at its four (pressure) and two (radius) stencil nodes
+// (the same values the flux computed per face before).
 template <typename R>
 __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, stage, force, tl)) return;
     R* const* U = stageIn(c, stage);
-    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x)
-        store5(c.W, q, primOf(load5(U, q)));
+    const Gas<R> gs{R(c.gamma), R(c.rgas), c.lut};
+    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) {
+        const S5<R> W = primOf(load5(U, q));
+        store5(c.W, q, W);
+        if (c.Wp) {
+            c.Wp[q] = pressurePrim(gs, W);
+            c.Wr[q] = jstR(gs, W);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ nodes

@@ -888,6 +888,8 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         c.Rp[v] = inst.allocR(2 * NI * NJ);
         c.W[v] = inst.allocR(N);
     }
+    c.Wp = c.scheme == 0 ? inst.allocR(N) : nullptr;
+    c.Wr = c.scheme == 0 ? inst.allocR(N) : nullptr;
     c.dt = inst.allocR(N);
     c.partial = inst.allocD(static_cast<size_t>(c.node_tiles + c.per_tiles) * 5 + c.node_tiles +
                             static_cast<size_t>(c.nboxes) * 5);
