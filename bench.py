@@ -512,6 +512,71 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
     return status, iters, launches, first
 
 
+def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: int, stall: int):
+    """The precision pattern on the map: every member runs batched in
+    fp32_kahan until it is within one order of its residual drop (best_drop
+    >= drop - 1), stops progressing (best_drop grew by less than 0.05 orders
+    in `stall` iterations) or finishes; the members that stopped without
+    finishing then continue from their current state in FP64
+    (ctbfm_promote_fp64), batched, to convergence. Float carries the bulk of
+    the iterations; FP64 takes the last order, where the float residual
+    reaches its rounding floor, so the convergence test and the converged
+    state are FP64's. Returns (status, iterations, launches, stage kernels,
+    promoted count, FP64 iterations)."""
+    import numpy as np
+
+    from cturbobfm_b200 import Batch
+
+    m = len(solvers)
+    status = np.zeros(m, np.int32)
+    iters = np.zeros(m, np.int64)
+    mark = np.zeros(m)       # best_drop at the last 0.05-order progress
+    mark_it = np.zeros(m, np.int64)
+    ready = np.zeros(m, bool)
+    launches = 0
+    first = None
+    active = list(range(m))
+    # phase A: float
+    while active:
+        with Batch([solvers[i] for i in active]) as b:
+            b.set_stream(stream.cuda_stream)
+            b.autotune()
+            fused, stage_ms = b.stage_kernels()
+            if first is None:
+                first = {"stage_kernels": "fused (k_stage)" if fused else "split (k_prim, k_faces, k_nodes)",
+                         "stage_autotuned_ms": {"split": stage_ms[0], "fused": stage_ms[1]}}
+            per_iteration = _map_launches_per_iteration(case, fused)
+            start = len(active)
+            while True:
+                b.step(chunk)
+                st = b.status()
+                launches += chunk * per_iteration + 4
+                for j, i in enumerate(active):
+                    status[i] = st["status"][j]
+                    iters[i] = st["iterations"][j]
+                    bd = st["best_drop"][j]
+                    if bd >= mark[i] + 0.05:
+                        mark[i], mark_it[i] = bd, iters[i]
+                    if bd >= drop - 1 or iters[i] - mark_it[i] >= stall:
+                        ready[i] = True
+                out = [i for i in active if status[i] != 0 or iters[i] >= n_iter or ready[i]]
+                if len(out) * 4 >= start or len(out) == len(active):
+                    break
+        active = [i for i in active if not (status[i] != 0 or iters[i] >= n_iter or ready[i])]
+    # phase B: FP64 to convergence
+    promote = [i for i in range(m) if status[i] == 0 and iters[i] < n_iter]
+    it_a = iters.copy()
+    for i in promote:
+        solvers[i].promote_fp64()
+    if promote:
+        s_b, i_b, l_b, _ = _solve_batched([solvers[i] for i in promote], stream, chunk, n_iter, case)
+        for j, i in enumerate(promote):
+            status[i], iters[i] = s_b[j], i_b[j]
+        launches += l_b
+    fp64_iters = int(sum(iters[i] - it_a[i] for i in promote))
+    return status, iters, launches, first, len(promote), fp64_iters
+
+
 def map_cpu_baseline(inis, iterations, n_iter: int):
     """Converged op-points/hour of the reference build on the host cores: one
     single-threaded process per instance, all at once (the way the
@@ -586,7 +651,10 @@ def map_line(args):
     stream = torch.cuda.Stream()
     results = {}
     with ClockSampler(local) as clocks:
-        for arm, inis in (("batched_fp32_kahan", inis32), ("batched_fp64", inis64)):
+        arms = [("batched_fp32_kahan", inis32), ("batched_fp64", inis64)]
+        if args.map_pure_fp32:
+            arms.append(("batched_fp32_only", inis32))
+        for arm, inis in arms:
             if arm == "batched_fp64" and args.map_skip_fp64_batch:
                 continue
             w0 = time.perf_counter()
@@ -595,7 +663,12 @@ def map_line(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            status, iters, launches, kern = _solve_batched(solvers, stream, args.map_chunk, n_iter, cs32[0])
+            promoted, fp64_iters = 0, 0
+            if arm == "batched_fp32_kahan":
+                status, iters, launches, kern, promoted, fp64_iters = _solve_fp32_then_fp64(
+                    solvers, stream, args.map_chunk, n_iter, cs32[0], args.map_drop, args.map_stall)
+            else:
+                status, iters, launches, kern = _solve_batched(solvers, stream, args.map_chunk, n_iter, cs32[0])
             e1.record(stream)
             torch.cuda.synchronize()
             sec = e0.elapsed_time(e1) / 1e3
@@ -612,7 +685,8 @@ def map_line(args):
                             "e2e_points_per_hour": conv / (setup + sec + readback) * 3600.0,
                             "iterations": iters.tolist(), "turbo": turbo, "status": status,
                             "node_stage_per_s": float((nodes * iters).sum() * 4 / sec), "launches": launches,
-                            "device_bytes": bytes_up, **kern}
+                            "device_bytes": bytes_up, "promoted_to_fp64": promoted,
+                            "fp64_iteration_share": fp64_iters / max(1, int(iters.sum())), **kern}
         # the plain FP64 path: one drop-in solver at a time, to convergence
         sample = list(range(min(args.map_plain, len(inis64))))
         plain_sec, plain_conv, plain = 0.0, 0, []
@@ -655,15 +729,25 @@ def map_line(args):
         "gpu_launches": r32["launches"],
         "batched_fp32_kahan": {k: r32[k] for k in ("seconds", "setup_seconds", "converged", "diverged",
                                                    "points_per_hour", "node_stage_per_s", "stage_kernels",
-                                                   "stage_autotuned_ms")},
+                                                   "stage_autotuned_ms", "promoted_to_fp64",
+                                                   "fp64_iteration_share")},
+        "precision_pattern": ("fp32_kahan for every instance until it is within one order of the residual drop or "
+                              f"stalls for {args.map_stall} iterations, then the same solve continued in FP64 from "
+                              "its current state to convergence (FP64 convergence test and converged state)"),
         "plain_fp64": {"points_per_hour": plain_pph, "instances": len(sample), "converged": plain_conv,
                        "seconds": plain_sec, "iterations": [p[1] for p in plain]},
         "speedup_vs_plain_fp64": (r32["points_per_hour"] / plain_pph) if plain_pph else None,
+        "speedup_batched_fp64_vs_plain_fp64": ((results["batched_fp64"]["points_per_hour"] / plain_pph)
+                                               if plain_pph and "batched_fp64" in results else None),
         "fp32_vs_plain_fp64_rel_err": {"massflow_max": max(err_mf) if err_mf else None,
                                        "pr_tt_max": max(err_pr) if err_pr else None, "instances": len(err_mf)},
         "iterations_fp32": {"min": int(min(r32["iterations"])), "median": float(np.median(r32["iterations"])),
                             "max": int(max(r32["iterations"]))},
     }
+    if "batched_fp32_only" in results:
+        r = results["batched_fp32_only"]
+        line["batched_fp32_only"] = {k: r[k] for k in ("seconds", "converged", "diverged", "points_per_hour",
+                                                        "node_stage_per_s")}
     if "batched_fp64" in results:
         r64 = results["batched_fp64"]
         line["batched_fp64"] = {k: r64[k] for k in ("seconds", "converged", "diverged", "points_per_hour",
@@ -960,6 +1044,10 @@ def main():
                          "serve: continuous batching of arriving requests")
     ap.add_argument("--map-n", type=int, default=256)
     ap.add_argument("--map-drop", type=int, default=4, help="RESIDUALS_DROP_CONVERGENCE of the map instances")
+    ap.add_argument("--map-stall", type=int, default=3000,
+                    help="float members without 0.05 orders of progress for this many iterations move to FP64")
+    ap.add_argument("--map-pure-fp32", action="store_true",
+                    help="also run the map in fp32_kahan alone (no FP64 finish)")
     ap.add_argument("--no-map", action="store_true", help="leave the compressor-map object out of the default line")
     ap.add_argument("--map-chunk", type=int, default=250)
     ap.add_argument("--map-plain", type=int, default=8, help="instances solved one at a time on the plain FP64 path")
