@@ -34,6 +34,12 @@ public:
     // runs the group's autotuner now (face tiles, stage fusion) unless it has run
     void autotune();
     int fusedMode() const { return g32_ ? g32_->fusedMode() : g64_->fusedMode(); }
+    GroupTuning tuning() const { return g32_ ? g32_->tuning() : g64_->tuning(); }
+    void adopt(const GroupTuning& t) {
+        if (g32_) g32_->adopt(t);
+        else g64_->adopt(t);
+    }
+    long long nodes() const { return g32_ ? g32_->nodes() : g64_->nodes(); }
     double stageMs(int mode) const { return g32_ ? g32_->stageMs(mode) : g64_->stageMs(mode); }
     // enqueue + synchronise; returns the most iterations any member advanced
     long long step(long long n);

@@ -166,8 +166,10 @@ void GroupT<R>::buildTiles() {
     cudaCheck(cudaMalloc(&dTiles_, std::max<size_t>(all.size(), 1) * sizeof(Tile)), "cudaMalloc");
     cudaCheck(cudaMemcpy(dTiles_, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice), "cudaMemcpy");
     // a copy from pageable memory may still be in flight when cudaMemcpy
-    // returns, and the kernels run on non-blocking streams: wait for it
-    cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    // returns, and the kernels run on non-blocking streams: wait for it (the
+    // legacy default stream holds the copy and does not wait for the
+    // non-blocking streams, so other groups' work on the device runs on)
+    cudaCheck(cudaStreamSynchronize(cudaStreamLegacy), "cudaStreamSynchronize");
     for (auto& [tl, off] : offs) tl->tiles = dTiles_ + off;
     if (graph_) {  // launches captured with the old lists
         cudaGraphExecDestroy(graph_);
@@ -187,6 +189,7 @@ void GroupT<R>::buildTiles() {
 template <typename R>
 void GroupT<R>::tune(cudaStream_t s) {
     tuned_ = true;
+    selfTuned_ = true;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaCheck(cudaEventCreate(&e0), "cudaEventCreate");
     cudaCheck(cudaEventCreate(&e1), "cudaEventCreate");
@@ -250,6 +253,36 @@ void GroupT<R>::tune(cudaStream_t s) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+template <typename R>
+long long GroupT<R>::nodes() const {
+    long long n = 0;
+    for (auto* m : members_) n += m->c.n;
+    return n;
+}
+
+template <typename R>
+GroupTuning GroupT<R>::tuning() const {
+    GroupTuning t;
+    t.valid = selfTuned_;
+    for (int d = 0; d < 3; d++) t.faceTile[d] = faceTile_[d];
+    t.fusedMode = view_.fusedMode;
+    t.stageMs[0] = stageMs_[0];
+    t.stageMs[1] = stageMs_[1];
+    t.nodes = nodes();
+    return t;
+}
+
+template <typename R>
+void GroupT<R>::adopt(const GroupTuning& t) {
+    if (!t.valid) return;
+    for (int d = 0; d < 3; d++) faceTile_[d] = t.faceTile[d];
+    stageMs_[0] = t.stageMs[0];
+    stageMs_[1] = t.stageMs[1];
+    buildTiles();  // also drops captured graphs
+    if (fusionAuto_) view_.fusedMode = t.fusedMode;
+    tuned_ = true;
 }
 
 template <typename R>

@@ -47,6 +47,17 @@ private:
     size_t bytes_ = 0;
 };
 
+// What a group's autotuner chose (face tiles, stage fusion) and on how many
+// nodes, so that a later group of similar size can adopt it instead of
+// timing again.
+struct GroupTuning {
+    bool valid = false;
+    int faceTile[3] = {kTileSize, kTileSize, kTileSize};
+    int fusedMode = 0;
+    float stageMs[2] = {0.f, 0.f};
+    long long nodes = 0;
+};
+
 template <typename R>
 class GroupT {
 public:
@@ -79,6 +90,12 @@ public:
     int faceTile(int d) const { return faceTile_[d]; }
     // the autotuner's stage timings (ms per stage: split, fused; 0 untimed)
     float stageMs(int mode) const { return stageMs_[mode]; }
+    long long nodes() const;
+    // the autotuner's choices (valid once this group's own autotuner has run)
+    GroupTuning tuning() const;
+    // takes another group's tuning (face tiles; stage fusion when this group
+    // has GPU_STAGE_FUSION = auto) and marks this group tuned
+    void adopt(const GroupTuning& t);
     static constexpr long long kTuneMinIterations = 64;
 
 private:
@@ -99,6 +116,7 @@ private:
     bool tuned_ = false;
     bool autotune_ = true;
     bool fusionAuto_ = false;
+    bool selfTuned_ = false;  // this group's own autotuner ran (not adopted)
 };
 
 extern template class InstanceT<double>;

@@ -33,6 +33,7 @@ Server::~Server() {
     b32_.reset();
     b64_.reset();
     active_.clear();
+    pending_.clear();
 }
 
 double Server::now() const { return steadySeconds() - t0_; }
@@ -128,20 +129,32 @@ void Server::rebuild() {
             idx64_.push_back(static_cast<int>(i));
         }
     }
-    if (!m32.empty()) b32_ = std::make_unique<Batch>(m32);
-    if (!m64.empty()) b64_ = std::make_unique<Batch>(m64);
+    // a batch of about the size an earlier batch was tuned on takes that
+    // tuning; otherwise it times its own at its first chunk
+    auto build = [this](std::vector<Solver*>& m, int p) {
+        auto b = std::make_unique<Batch>(m);
+        const GroupTuning& t = tuned_[p];
+        const long long n = b->nodes();
+        if (t.valid && n * 4 >= t.nodes && n <= 4 * t.nodes) b->adopt(t);
+        return b;
+    };
+    if (!m32.empty()) b32_ = build(m32, 1);
+    if (!m64.empty()) b64_ = build(m64, 0);
     dirty_ = false;
 }
 
-void Server::pump(int* nActive, int* nWaiting) {
-    // 1. admission, in arrival order, while slots and device memory allow
+// Admission in arrival order while slots, device memory and the node limit
+// allow (the solves built but not yet running count too); a request whose
+// preparation failed retires at once.
+void Server::admit() {
     while (true) {
         std::unique_ptr<Job> j;
         {
             std::lock_guard<std::mutex> l(mu_);
             if (queue_.empty() || !queue_.front()->prepared) break;
             if (queue_.front()->error == 0) {
-                if (static_cast<int>(active_.size()) >= opt_.max_active) break;
+                const bool idle = active_.empty() && pending_.empty();
+                if (static_cast<int>(active_.size() + pending_.size()) >= opt_.max_active) break;
                 const size_t need = estimate(*queue_.front());
                 size_t budget = opt_.budget_bytes;
                 if (budget == 0) {
@@ -149,9 +162,8 @@ void Server::pump(int* nActive, int* nWaiting) {
                     cudaCheck(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
                     budget = used_ + freeB * 9 / 10;
                 }
-                if (used_ + need > budget && !active_.empty()) break;
-                if (opt_.max_active_nodes > 0 && usedNodes_ + queue_.front()->nodes > opt_.max_active_nodes &&
-                    !active_.empty())
+                if (used_ + need > budget && !idle) break;
+                if (opt_.max_active_nodes > 0 && usedNodes_ + queue_.front()->nodes > opt_.max_active_nodes && !idle)
                     break;
             }
             j = std::move(queue_.front());
@@ -180,102 +192,140 @@ void Server::pump(int* nActive, int* nWaiting) {
             bytesPerNode_[p] = static_cast<double>(j->bytes) / static_cast<double>(j->nodes);
         used_ += j->bytes;
         usedNodes_ += j->nodes;
-        j->t_admit = now();
+        pending_.push_back(std::move(j));
+    }
+}
+
+void Server::joinPending() {
+    if (pending_.empty()) return;
+    const double t = now();
+    for (auto& j : pending_) {
+        j->t_admit = t;
         active_.push_back(std::move(j));
+    }
+    pending_.clear();
+    dirty_ = true;
+}
+
+std::vector<Control> Server::gather() {
+    std::vector<Control> ctl(active_.size());
+    std::vector<Control> tmp;
+    if (b32_) {
+        tmp.resize(idx32_.size());
+        b32_->controls(tmp.data());
+        for (size_t m = 0; m < idx32_.size(); m++) ctl[idx32_[m]] = tmp[m];
+    }
+    if (b64_) {
+        tmp.resize(idx64_.size());
+        b64_->controls(tmp.data());
+        for (size_t m = 0; m < idx64_.size(); m++) ctl[idx64_[m]] = tmp[m];
+    }
+    return ctl;
+}
+
+void Server::process(const std::vector<Control>& ctl) {
+    std::vector<std::unique_ptr<Job>> keep;
+    std::vector<size_t> promote, rerun;
+    for (size_t i = 0; i < active_.size(); i++) {
+        const Control& c = ctl[i];
+        auto& j = active_[i];
+        if (opt_.stall_window > 0 && c.status == 2 && j->solver->precision() == kFP32Kahan && !j->rerun) {
+            rerun.push_back(keep.size());
+            keep.push_back(std::move(j));
+            continue;
+        }
+        if (c.status != 0 || c.it >= j->solver->maxIterations()) {
+            if (!dirty_) {
+                b32_.reset();
+                b64_.reset();
+                dirty_ = true;
+            }
+            used_ -= std::min(used_, j->bytes);
+            usedNodes_ -= std::min(usedNodes_, j->nodes);
+            retire(std::move(j), &c, 0, "");
+            continue;
+        }
+        if (opt_.stall_window > 0 && j->solver->precision() == kFP32Kahan && c.it - c.it_best >= opt_.stall_window)
+            promote.push_back(keep.size());
+        keep.push_back(std::move(j));
+    }
+    active_ = std::move(keep);
+    if (!rerun.empty()) {
+        // A float solve whose residual became NaN/Inf starts again from its
+        // initial state in FP64; the outcome depends on the request alone.
+        b32_.reset();
+        b64_.reset();
+        dirty_ = true;
+        std::vector<size_t> failed;
+        for (size_t k : rerun) {
+            auto& j = active_[k];
+            used_ -= std::min(used_, j->bytes);
+            j->solver.reset();
+            j->rerun = true;
+            j->config->set("GPU_PRECISION", "fp64");
+            try {
+                j->solver = std::make_unique<Solver>(*j->config, *j->mesh);
+                j->bytes = j->solver->deviceBytes();
+                used_ += j->bytes;
+            } catch (const std::exception& e) {
+                j->message = e.what();
+                failed.push_back(k);
+            }
+        }
+        for (auto it = failed.rbegin(); it != failed.rend(); ++it) {
+            auto j = std::move(active_[*it]);
+            active_.erase(active_.begin() + static_cast<long>(*it));
+            usedNodes_ -= std::min(usedNodes_, j->nodes);
+            const std::string msg = j->message;
+            retire(std::move(j), nullptr, 2, msg);
+        }
+        for (size_t& k : promote)  // indices after the erased entries shift down
+            k -= static_cast<size_t>(std::count_if(failed.begin(), failed.end(), [k](size_t f) { return f < k; }));
+    }
+    if (!promote.empty()) {
+        b32_.reset();
+        b64_.reset();
+        for (size_t k : promote) {
+            auto& j = active_[k];
+            used_ -= std::min(used_, j->bytes);
+            j->solver->promoteToFP64();
+            j->bytes = j->solver->deviceBytes();
+            used_ += j->bytes;
+        }
         dirty_ = true;
     }
-    // 2. one chunk of iterations for every admitted solve; the two precision
-    //    groups run on their own streams and overlap on the device
+}
+
+void Server::pump(int* nActive, int* nWaiting) {
+    // 1. the chunk in flight: wait for it, then retire / re-run / promote
+    //    with the batches idle
+    if (inflight_) {
+        const std::vector<Control> ctl = gather();
+        inflight_ = false;
+        process(ctl);
+    }
+    // 2. the solves built during that chunk join; with nothing on the device,
+    //    requests are admitted right away
+    joinPending();
+    if (active_.empty()) {
+        admit();
+        joinPending();
+    }
+    // 3. the next chunk for every admitted solve; the two precision groups
+    //    run on their own streams and overlap on the device
     if (!active_.empty()) {
         if (dirty_) rebuild();
         if (b32_) b32_->enqueue(opt_.chunk);
         if (b64_) b64_->enqueue(opt_.chunk);
-        std::vector<Control> ctl(active_.size());
-        std::vector<Control> tmp;
-        if (b32_) {
-            tmp.resize(idx32_.size());
-            b32_->controls(tmp.data());
-            for (size_t m = 0; m < idx32_.size(); m++) ctl[idx32_[m]] = tmp[m];
-        }
-        if (b64_) {
-            tmp.resize(idx64_.size());
-            b64_->controls(tmp.data());
-            for (size_t m = 0; m < idx64_.size(); m++) ctl[idx64_[m]] = tmp[m];
-        }
-        // 3. retire finished solves, re-run diverged float solves in FP64,
-        //    promote stalled float solves
-        std::vector<std::unique_ptr<Job>> keep;
-        std::vector<size_t> promote, rerun;
-        for (size_t i = 0; i < active_.size(); i++) {
-            const Control& c = ctl[i];
-            auto& j = active_[i];
-            if (opt_.stall_window > 0 && c.status == 2 && j->solver->precision() == kFP32Kahan && !j->rerun) {
-                rerun.push_back(keep.size());
-                keep.push_back(std::move(j));
-                continue;
-            }
-            if (c.status != 0 || c.it >= j->solver->maxIterations()) {
-                if (!dirty_) {
-                    b32_.reset();
-                    b64_.reset();
-                    dirty_ = true;
-                }
-                used_ -= std::min(used_, j->bytes);
-                usedNodes_ -= std::min(usedNodes_, j->nodes);
-                retire(std::move(j), &c, 0, "");
-                continue;
-            }
-            if (opt_.stall_window > 0 && j->solver->precision() == kFP32Kahan && c.it - c.it_best >= opt_.stall_window)
-                promote.push_back(keep.size());
-            keep.push_back(std::move(j));
-        }
-        active_ = std::move(keep);
-        if (!rerun.empty()) {
-            // A float solve whose residual became NaN/Inf starts again from its
-            // initial state in FP64; the outcome depends on the request alone.
-            b32_.reset();
-            b64_.reset();
-            dirty_ = true;
-            std::vector<size_t> failed;
-            for (size_t k : rerun) {
-                auto& j = active_[k];
-                used_ -= std::min(used_, j->bytes);
-                j->solver.reset();
-                j->rerun = true;
-                j->config->set("GPU_PRECISION", "fp64");
-                try {
-                    j->solver = std::make_unique<Solver>(*j->config, *j->mesh);
-                    j->bytes = j->solver->deviceBytes();
-                    used_ += j->bytes;
-                } catch (const std::exception& e) {
-                    j->message = e.what();
-                    failed.push_back(k);
-                }
-            }
-            for (auto it = failed.rbegin(); it != failed.rend(); ++it) {
-                auto j = std::move(active_[*it]);
-                active_.erase(active_.begin() + static_cast<long>(*it));
-                usedNodes_ -= std::min(usedNodes_, j->nodes);
-                const std::string msg = j->message;
-                retire(std::move(j), nullptr, 2, msg);
-            }
-            for (size_t& k : promote)  // indices after the erased entries shift down
-                k -= static_cast<size_t>(std::count_if(failed.begin(), failed.end(), [k](size_t f) { return f < k; }));
-        }
-        if (!promote.empty()) {
-            b32_.reset();
-            b64_.reset();
-            for (size_t k : promote) {
-                auto& j = active_[k];
-                used_ -= std::min(used_, j->bytes);
-                j->solver->promoteToFP64();
-                j->bytes = j->solver->deviceBytes();
-                used_ += j->bytes;
-            }
-            dirty_ = true;
-        }
+        inflight_ = true;
+        // a batch that timed its own tuning hands it on to later batches
+        if (b32_ && b32_->tuning().valid) tuned_[1] = b32_->tuning();
+        if (b64_ && b64_->tuning().valid) tuned_[0] = b64_->tuning();
     }
-    if (nActive) *nActive = static_cast<int>(active_.size());
+    // 4. while the chunk runs, build the next requests that fit (device
+    //    allocation and upload); they join at the next round
+    admit();
+    if (nActive) *nActive = static_cast<int>(active_.size() + pending_.size());
     if (nWaiting) {
         std::lock_guard<std::mutex> l(mu_);
         *nWaiting = static_cast<int>(queue_.size());

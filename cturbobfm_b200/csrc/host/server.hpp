@@ -55,8 +55,13 @@ public:
 
     // Queues a request (thread safe); its host preparation starts at once.
     long long submit(const std::string& iniPath);
-    // One scheduling round: admit, advance every admitted solve by `chunk`
-    // iterations, retire and promote. Returns after the GPU work of the round.
+    // One scheduling round: waits for the chunk the previous round enqueued
+    // and retires, promotes and re-runs from its results; the solves built
+    // during that chunk join the batches; the next chunk of `chunk`
+    // iterations of every admitted solve is enqueued; and while it runs on
+    // the device the next requests that fit are built (device memory and
+    // upload), to join at the next round. Returns without waiting for the
+    // chunk it enqueued.
     void pump(int* active, int* waiting);
     // Requests finished since the last call.
     std::vector<ServerResult> take();
@@ -79,6 +84,16 @@ private:
     };
     void worker();
     void rebuild();
+    // builds the Solvers of queued requests that fit the slots, memory and
+    // node limits, in arrival order, into pending_
+    void admit();
+    // the pending solves join the active ones (next chunk)
+    void joinPending();
+    // every active solve's control block after the chunk in flight
+    std::vector<Control> gather();
+    // retire finished solves, re-run diverged float solves in FP64, promote
+    // stalled float solves (batches idle)
+    void process(const std::vector<Control>& ctl);
     void retire(std::unique_ptr<Job> job, const Control* ctl, int error, const std::string& msg);
     size_t estimate(const Job& j) const;
 
@@ -92,6 +107,11 @@ private:
     bool stop_ = false;
     long long nextId_ = 1;
     std::vector<std::unique_ptr<Job>> active_;
+    std::vector<std::unique_ptr<Job>> pending_;  // built during the chunk in flight, join at the next round
+    bool inflight_ = false;                      // a chunk of the current batches is enqueued
+    // autotuner results per precision (0 fp64, 1 fp32_kahan), adopted by
+    // later batches whose node count is within 4x of the tuned one
+    GroupTuning tuned_[2];
     std::unique_ptr<Batch> b64_, b32_;
     std::vector<int> idx64_, idx32_;  // active_ index of each batch member
     bool dirty_ = false;

@@ -185,8 +185,12 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
         initializeState(*i64_, *g64_);
     }
     // host-to-device copies from pageable memory may still be in flight when
-    // cudaMemcpy returns; the solver's kernels run on a non-blocking stream
-    cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    // cudaMemcpy returns; the solver's kernels run on a non-blocking stream.
+    // Only the legacy default stream (the copies) and the solver's own stream
+    // are waited for, so a solver can be built while other solvers' batches
+    // run on the device (continuous batching).
+    cudaCheck(cudaStreamSynchronize(cudaStreamLegacy), "cudaStreamSynchronize");
+    cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
 }
 
 // Solver::buildAdvectionModel / buildBfmInfo (src/solver.cpp:185-198, 701-749).
@@ -1481,7 +1485,8 @@ void Solver::promoteToFP64() {
     cudaCheck(cudaMemcpy(i64_->c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
     g32_.reset();
     i32_.reset();
-    cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    cudaCheck(cudaStreamSynchronize(cudaStreamLegacy), "cudaStreamSynchronize");
+    cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
 }
 
 long long Solver::history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub,
