@@ -128,6 +128,20 @@ class Oracle:
         return _load().oracle_time(self._h)
 
 
+def reference_root() -> str:
+    """Where the reference's sources are read for the reference build: the
+    CTBFM_REFERENCE environment variable, else the REF default of the build
+    recipe (oracle/refbuild/Makefile)."""
+    env = os.environ.get("CTBFM_REFERENCE")
+    if env:
+        return env
+    mk = os.path.join(os.path.dirname(os.path.abspath(__file__)), "refbuild", "Makefile")
+    for line in open(mk):
+        if line.startswith("REF ?="):
+            return line.split("=", 1)[1].strip()
+    return ""
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_HARNESS)
 

@@ -117,4 +117,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    from oracle.oracle import reference_root
+
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_root())

@@ -4,7 +4,8 @@
   * against the regression cases' shipped reference.csv with the reference's
     own gate (relative L2 <= 3e-2, test/regression_tests/test_cases.py:82-88);
   * bit for bit against the reference build on every parity case, when that
-    build is present (it is on the development machine).
+    build is present (oracle/_ref, built from the reference's sources when
+    they are available).
 """
 
 import numpy as np
