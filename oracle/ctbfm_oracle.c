@@ -299,6 +299,13 @@ struct oracle_solver {
     unsigned char* wall;
     vec3* grad[4];
     double* gfield[4];
+    /* TURBULENCE_ACTIVE with TURBULENCE_MODEL = SA (TurbulenceModelSA): the
+     * working variable nu hat, the laminar kinematic viscosity of its last
+     * solve, the wall distance and the work arrays of its implicit update */
+    int sa;
+    double sa_init_nu, sa_ff_scale, sa_init_scale, sa_relax, sa_prt;
+    double *nuhat, *nul, *wdist, *sa_res, *sa_diag, *sa_dstar, *sa_dnu;
+    vec3 *nuhat_grad, *sa_vel;
     /* state */
     double *U[5], *Utmp[5], *R[5], *dt;
     double t;
@@ -1602,6 +1609,27 @@ static double f_mu(const oracle_solver* s, double T) {
     return s->suth_mu * pow(T / s->suth_T, 1.5) * ((s->suth_T + s->suth_S) / (T + s->suth_S));
 }
 
+/* SA constants (include/turbulence_model_sa.hpp:80-93). */
+static const double SA_CB1 = 0.1355, SA_CB2 = 0.622, SA_SIGMA = 2.0 / 3.0, SA_KAPPA = 0.41, SA_CW2 = 0.3,
+                    SA_CW3 = 2.0, SA_CV1 = 7.1, SA_CT3 = 0.0, SA_CT4 = 0.5, SA_CN1 = 16.0, SA_C2 = 0.7, SA_C3 = 0.9;
+static double sa_cw1(void) { return SA_CB1 / (SA_KAPPA * SA_KAPPA) + (1.0 + SA_CB2) / SA_SIGMA; }
+
+/* TurbulenceModelSA::getEddyViscosity (src/turbulence_model_sa.cpp:843-858),
+ * with the laminar viscosity of the model's last solve (0 before the first:
+ * no eddy viscosity). TurbulenceModelNone's is 0. */
+static double sa_mut(const oracle_solver* s, double rho, long q) {
+    if (!s->sa) return 0.0;
+    double nuHat = s->nuhat[q];
+    if (nuHat <= 0.0) return 0.0;
+    double nuL = s->nul[q];
+    if (nuL <= 0.0) return 0.0;
+    double chi = nuHat / nuL;
+    double chi3 = chi * chi * chi;
+    double cv1_3 = SA_CV1 * SA_CV1 * SA_CV1;
+    double fv1 = chi3 / (chi3 + cv1_3);
+    return fv1 * rho * nuHat;
+}
+
 /* Solver::computeSolutionGradient (src/solver.cpp:3033-3058): node
  * temperature of FluidIdeal::computeTemperature_conservative
  * (src/fluid_ideal.cpp:198-207) or FluidBase's (include/fluid_base.hpp:163-177),
@@ -1661,8 +1689,9 @@ static void solution_gradient(oracle_solver* s, double* const* U) {
 }
 
 /* Solver::computeViscousFlux (src/solver.cpp:2174-2226) with
- * computeViscousStressTensor (src/math_utils.cpp:593-608); laminar, so the
- * eddy viscosity and conductivity of TurbulenceModelNone are 0. */
+ * computeViscousStressTensor (src/math_utils.cpp:593-608); the eddy
+ * conductivity is mu_t cp / Pr_t with SA (getEddyThermalConductivity,
+ * include/turbulence_model_sa.hpp:73) and 0 with TurbulenceModelNone. */
 static sv5 viscous_flux(const oracle_solver* s, sv5 Uc, vec3 gu, vec3 gv, vec3 gw, vec3 gT, vec3 S,
                         double muEddy) {
     sv5 W = prim_of(Uc);
@@ -1670,7 +1699,7 @@ static sv5 viscous_flux(const oracle_solver* s, sv5 Uc, vec3 gu, vec3 gv, vec3 g
     double T = f_temperature_rho_u_et(s, W.v[0], vel, W.v[4]);
     double muL = f_mu(s, T);
     double kappaL = s->vcp * muL / s->vpr;
-    double kappaEddy = 0.0;
+    double kappaEddy = s->sa ? muEddy * s->vcp / s->sa_prt : 0.0;
     double muT = muL + muEddy;
     double kT = kappaL + kappaEddy;
     double lam = -2.0 / 3.0 * muT;
@@ -1707,7 +1736,7 @@ static void viscous_residuals(oracle_solver* s, int dir, double* const* U) {
                 sv5 Ua = smul(sadd(state_at(s, U, fi - st[0], fj - st[1], fk - st[2]), state_at(s, U, fi, fj, fk)), 0.5);
                 vec3 g[4];
                 for (int v = 0; v < 4; v++) g[v] = vmul(vadd(s->grad[v][ql], s->grad[v][qr]), 0.5);
-                double muEddy = (0.0 + 0.0) * 0.5;
+                double muEddy = (sa_mut(s, U[0][ql], ql) + sa_mut(s, U[0][qr], qr)) * 0.5;
                 sv5 F = viscous_flux(s, Ua, g[0], g[1], g[2], g[3], S, muEddy);
                 sv5 c = smul(smul(F, vmag(S)), -1.0);
                 res_add(s, fi - st[0], fj - st[1], fk - st[2], c);
@@ -1724,6 +1753,305 @@ static void no_slip_momentum(const oracle_solver* s, double* const* X) {
     for (long q = 0; q < s->n; q++)
         if (s->wall[q])
             for (int c = 1; c <= 3; c++) X[c][q] = X[0][q] * 0.0;
+}
+
+/* ------------------------------------------------------ Spalart-Allmaras */
+/* fetchBoundaryNodesIndexRange (src/boundary_base.cpp:227-267) and
+ * Boundary::computeOrientation (include/boundary_base.hpp:109-119): the
+ * patch's node range [r0, r1) x [r2, r3) x [r4, r5) and the step from a
+ * boundary node to its interior donor. */
+static void patch_nodes(const oracle_solver* s, const patch* p, long r[6], long step[3]) {
+    r[0] = p->i_min; r[1] = p->i_max; r[2] = p->j_min; r[3] = p->j_max; r[4] = p->k_min; r[5] = p->k_max;
+    if (r[0] == r[1] && r[0] == 0) r[1] = 1;
+    else if (r[0] == r[1] && r[0] == s->ni) { r[0] = s->ni - 1; r[1] = r[0] + 1; }
+    else if (r[2] == r[3] && r[2] == 0) r[3] = 1;
+    else if (r[2] == r[3] && r[2] == s->nj) { r[2] = s->nj - 1; r[3] = r[2] + 1; }
+    else if (r[4] == r[5] && r[4] == 0) r[5] = 1;
+    else if (r[4] == r[5] && r[4] == s->nk) { r[4] = s->nk - 1; r[5] = r[4] + 1; }
+    step[0] = step[1] = step[2] = 0;
+    if (p->i_min == p->i_max) step[0] = p->i_min == 0 ? 1 : -1;
+    else if (p->j_min == p->j_max) step[1] = p->j_min == 0 ? 1 : -1;
+    else if (p->k_min == p->k_max) step[2] = p->k_min == 0 ? 1 : -1;
+}
+
+/* TurbulenceModelSA::updateBoundaryValues (src/turbulence_model_sa.cpp:250-345):
+ * patch by patch in the boundary file's order, nu hat 0 on no-slip walls,
+ * the free-stream value on inlets and farfields, the interior donor's value
+ * on outlets, inviscid walls and transparent patches. */
+static void sa_boundary_values(oracle_solver* s) {
+    for (int m = 0; m < s->npatches; m++) {
+        const patch* p = &s->patches[m];
+        int kind;
+        if (p->type == BC_NO_SLIP_WALL) kind = 0;
+        else if (p->type == BC_INLET || p->type == BC_INLET_SUPERSONIC || p->type == BC_FARFIELD) kind = 1;
+        else if (p->type == BC_OUTLET || p->type == BC_RADIAL_EQ || p->type == BC_THROTTLE || p->type == BC_MASS_FLOW ||
+                 p->type == BC_OUTLET_SUPERSONIC || p->type == BC_INVISCID_WALL || p->type == BC_TRANSPARENT)
+            kind = 2;
+        else continue;
+        long r[6], st[3];
+        patch_nodes(s, p, r, st);
+        for (long i = r[0]; i < r[1]; i++)
+            for (long j = r[2]; j < r[3]; j++)
+                for (long k = r[4]; k < r[5]; k++) {
+                    long q = idx3(s, i, j, k);
+                    if (kind == 0) s->nuhat[q] = 0.0;
+                    else if (kind == 1) s->nuhat[q] = s->sa_init_nu * s->sa_ff_scale;
+                    else s->nuhat[q] = s->nuhat[idx3(s, i + st[0], j + st[1], k + st[2])];
+                }
+    }
+}
+
+/* computeGradientGreenGauss (src/math_utils.cpp:173-234) of nu hat with
+ * interpolateScalar (:395-466) and computeGreenGaussDivergence
+ * (include/math_utils.hpp:95-106): face values (f1 - f0) d0 / (d0 + d1) from
+ * the node, the node's own value on boundary faces, W E N S B T, divided by
+ * the volume. */
+static void sa_gradient(oracle_solver* s) {
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                long q = idx3(s, i, j, k);
+                vec3 p0 = s->vert[q];
+                double f0 = s->nuhat[q];
+                long nb[6];
+                int has[6];
+                vec3 mid[6];
+                has[0] = i > 0;         nb[0] = has[0] ? idx3(s, i - 1, j, k) : q; mid[0] = s->cI[sIi(s, i, j, k)];
+                has[1] = i < s->ni - 1; nb[1] = has[1] ? idx3(s, i + 1, j, k) : q; mid[1] = s->cI[sIi(s, i + 1, j, k)];
+                has[2] = j < s->nj - 1; nb[2] = has[2] ? idx3(s, i, j + 1, k) : q; mid[2] = s->cJ[sJi(s, i, j + 1, k)];
+                has[3] = j > 0;         nb[3] = has[3] ? idx3(s, i, j - 1, k) : q; mid[3] = s->cJ[sJi(s, i, j, k)];
+                has[4] = k > 0;         nb[4] = has[4] ? idx3(s, i, j, k - 1) : q; mid[4] = s->cK[sKi(s, i, j, k)];
+                has[5] = k < s->nk - 1; nb[5] = has[5] ? idx3(s, i, j, k + 1) : q; mid[5] = s->cK[sKi(s, i, j, k + 1)];
+                vec3 sf[6] = {vneg(s->sI[sIi(s, i, j, k)]), s->sI[sIi(s, i + 1, j, k)], s->sJ[sJi(s, i, j + 1, k)],
+                              vneg(s->sJ[sJi(s, i, j, k)]), vneg(s->sK[sKi(s, i, j, k)]), s->sK[sKi(s, i, j, k + 1)]};
+                vec3 g = v3(0.0, 0.0, 0.0);
+                for (int f = 0; f < 6; f++) {
+                    double sc = f0;
+                    if (has[f]) {
+                        double d0 = vmag(vsub(mid[f], p0));
+                        double d1 = vmag(vsub(mid[f], s->vert[nb[f]]));
+                        sc = f0 + (s->nuhat[nb[f]] - f0) * d0 / (d0 + d1);
+                    }
+                    g = vadd(g, vmul(sf[f], sc));
+                }
+                s->nuhat_grad[q] = vdiv(g, s->vol[q]);
+            }
+}
+
+/* TurbulenceModelSA::updateMeanFlowTerms (src/turbulence_model_sa.cpp:370-390):
+ * laminar kinematic viscosity mu(T) / rho from rho, rho u / rho, rho E / rho. */
+static void sa_mean_flow(oracle_solver* s, double* const* U) {
+    for (long q = 0; q < s->n; q++) {
+        double rho = U[0][q];
+        vec3 u = v3(U[1][q] / rho, U[2][q] / rho, U[3][q] / rho);
+        double T = f_temperature_rho_u_et(s, rho, u, U[4][q] / rho);
+        s->nul[q] = f_mu(s, T) / rho;
+    }
+}
+
+/* nu + nu hat fn of one node (computeViscousFlux, :513-545). */
+static double sa_nu_total(const oracle_solver* s, long q) {
+    double nuL = s->nul[q], nuHat = s->nuhat[q];
+    if (nuHat >= 0.0) return nuL + nuHat;
+    double chi = (nuL > 0.0) ? (nuHat / nuL) : 0.0;
+    double chi3 = chi * chi * chi;
+    double fn = (SA_CN1 + chi3) / (SA_CN1 - chi3);
+    return nuL + nuHat * fn;
+}
+
+/* TurbulenceModelSA::computeFluxContribution / computeAdvectionFlux /
+ * computeViscousFlux (src/turbulence_model_sa.cpp:406-558): interior faces of
+ * direction dir in storage order, first-order upwind advection of nu hat by
+ * the mean face-normal velocity, diffusion (nu + nu hat fn) grad nu hat /
+ * sigma averaged over the two nodes; the left node gains and the right node
+ * loses (adv - visc) |S|. */
+static void sa_flux_dir(oracle_solver* s, int dir, double* const* U) {
+    long nf[3] = {s->ni, s->nj, s->nk};
+    nf[dir] += 1;
+    const vec3* surf = dir == 0 ? s->sI : (dir == 1 ? s->sJ : s->sK);
+    const long st[3] = {dir == 0, dir == 1, dir == 2};
+    for (long fi = 0; fi < nf[0]; fi++)
+        for (long fj = 0; fj < nf[1]; fj++)
+            for (long fk = 0; fk < nf[2]; fk++) {
+                long dface = dir == 0 ? fi : (dir == 1 ? fj : fk);
+                if (dface == 0 || dface == nf[dir] - 1) continue;
+                long ql = idx3(s, fi - st[0], fj - st[1], fk - st[2]);
+                long qr = idx3(s, fi, fj, fk);
+                vec3 S = surf[dir == 0 ? sIi(s, fi, fj, fk) : (dir == 1 ? sJi(s, fi, fj, fk) : sKi(s, fi, fj, fk))];
+                vec3 n = vnormalized(S);
+                sv5 Wl = prim_of(state_at(s, U, fi - st[0], fj - st[1], fk - st[2]));
+                sv5 Wr = prim_of(state_at(s, U, fi, fj, fk));
+                double un = 0.5 * vdot(vadd(vel_of(Wl), vel_of(Wr)), n);
+                double phi = (un >= 0.0) ? s->nuhat[ql] : s->nuhat[qr];
+                double adv = phi * un;
+                vec3 tl = vmul(vdiv(s->nuhat_grad[ql], SA_SIGMA), sa_nu_total(s, ql));
+                vec3 tr = vmul(vdiv(s->nuhat_grad[qr], SA_SIGMA), sa_nu_total(s, qr));
+                double visc = 0.5 * vdot(vadd(tl, tr), n);
+                double c = (adv - visc) * vmag(S);
+                s->sa_res[ql] += c;
+                s->sa_res[qr] -= c;
+            }
+}
+
+/* TurbulenceModelSA::computeSource (src/turbulence_model_sa.cpp:578-647):
+ * production, destruction and cross diffusion of one node (SA-neg branch
+ * for negative nu hat), with the rotation-rate magnitude of
+ * computeRotationRateMagnitude (src/math_utils.cpp:620-639) from the
+ * velocity gradients of the solution gradient. */
+static double sa_source(const oracle_solver* s, long q) {
+    double d = s->wdist[q];
+    if (d <= 0.0) return 0.0;
+    double nuHat = s->nuhat[q];
+    double nuL = s->nul[q];
+    if (nuL <= 0.0) nuL = 1e-14;
+    vec3 gu = s->grad[0][q], gv = s->grad[1][q], gw = s->grad[2][q];
+    double o12 = 0.5 * (gu.y - gv.x), o13 = 0.5 * (gu.z - gw.x), o23 = 0.5 * (gv.z - gw.y);
+    double Sv = 2.0 * sqrt(o12 * o12 + o13 * o13 + o23 * o23);
+    vec3 gn = s->nuhat_grad[q];
+    double gsq = gn.x * gn.x + gn.y * gn.y + gn.z * gn.z;
+    double cross = (SA_CB2 / SA_SIGMA) * gsq;
+    double cw1 = sa_cw1();
+    if (nuHat >= 0.0) {
+        double chi = nuHat / nuL;
+        double chi3 = chi * chi * chi;
+        double cv1_3 = SA_CV1 * SA_CV1 * SA_CV1;
+        double fv1 = chi3 / (chi3 + cv1_3);
+        double fv2 = 1.0 - chi / (1.0 + chi * fv1);
+        double dSq = d * d;
+        double kd = SA_KAPPA * SA_KAPPA * dSq;
+        double Sbar = (nuHat / kd) * fv2;
+        double Shat;
+        if (Sbar >= -SA_C2 * Sv) Shat = Sv + Sbar;
+        else Shat = Sv + (Sv * (SA_C2 * SA_C2 * Sv + SA_C3 * Sbar)) / ((SA_C3 - 2.0 * SA_C2) * Sv - Sbar);
+        double r;
+        if (Shat * kd <= 0.0) r = 10.0;
+        else r = dmin(nuHat / (Shat * kd), 10.0);
+        double r2 = r * r;
+        double r6 = r2 * r2 * r2;
+        double g = r + SA_CW2 * (r6 - r);
+        double g6 = pow(g, 6.0);
+        double cw3_6 = pow(SA_CW3, 6.0);
+        double fw = g * pow((1.0 + cw3_6) / (g6 + cw3_6), 1.0 / 6.0);
+        double ft2 = SA_CT3 * exp(-SA_CT4 * chi * chi);
+        double P = SA_CB1 * (1.0 - ft2) * Shat * nuHat;
+        double D = (cw1 * fw - (SA_CB1 / (SA_KAPPA * SA_KAPPA)) * ft2) * (nuHat * nuHat / dSq);
+        return P - D + cross;
+    }
+    double dSq = d * d;
+    double Pn = SA_CB1 * (1.0 - SA_CT3) * Sv * nuHat;
+    double Dn = cw1 * (nuHat * nuHat / dSq);
+    return Pn + Dn + cross;
+}
+
+/* TurbulenceModelSA::updateSolution (src/turbulence_model_sa.cpp:649-841):
+ * diagonal (time term, convective and diffusive spectral radii, destruction
+ * Jacobian), a forward and a backward Gauss-Seidel sweep over the nodes in
+ * storage order with upwind face couplings, under-relaxed update clamped to
+ * +-1e5 nu. Returns 1 when an increment is NaN/Inf (the reference's
+ * "Turbulence model diverged"). */
+static int sa_update(oracle_solver* s, double* const* U) {
+    const int is1D = s->topology == TOPO_1D, is3D = s->topology == TOPO_3D;
+    const double cw1 = sa_cw1();
+    for (long q = 0; q < s->n; q++) {
+        double inv = 1.0 / U[0][q];
+        s->sa_vel[q] = v3(U[1][q] * inv, U[2][q] * inv, U[3][q] * inv);
+    }
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                long q = idx3(s, i, j, k);
+                vec3 v = s->sa_vel[q];
+                double vol = s->vol[q], nuHat = s->nuhat[q];
+                vec3 sW = s->sI[sIi(s, i, j, k)], sE = s->sI[sIi(s, i + 1, j, k)];
+                vec3 sS = s->sJ[sJi(s, i, j, k)], sN = s->sJ[sJi(s, i, j + 1, k)];
+                vec3 sB = s->sK[sKi(s, i, j, k)], sT = s->sK[sKi(s, i, j, k + 1)];
+                double lamW = fabs(vdot(v, sW)), lamE = fabs(vdot(v, sE));
+                double lamS = 0.0, lamN = 0.0, lamB = 0.0, lamT = 0.0;
+                if (!is1D) { lamS = fabs(vdot(v, sS)); lamN = fabs(vdot(v, sN)); }
+                if (is3D) { lamB = fabs(vdot(v, sB)); lamT = fabs(vdot(v, sT)); }
+                double sigC = 0.5 * (lamW + lamE + lamS + lamN + lamB + lamT);
+                double nuDiff = (s->nul[q] + dmax(0.0, nuHat)) / SA_SIGMA;
+                double sq = vdot(sW, sW) + vdot(sE, sE);
+                if (!is1D) sq += vdot(sS, sS) + vdot(sN, sN);
+                if (is3D) sq += vdot(sB, sB) + vdot(sT, sT);
+                double sigV = (nuDiff / vol) * sq;
+                double d = s->wdist[q];
+                double dSq = dmax(d * d, 1e-16);
+                double sigD = vol * (2.0 * cw1 * fabs(nuHat) / dSq);
+                s->sa_diag[q] = (vol / s->dt[q]) + sigC + sigV + sigD;
+            }
+    for (long q = 0; q < s->n; q++) s->sa_dstar[q] = s->sa_dnu[q] = 0.0;
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                long q = idx3(s, i, j, k);
+                double rhs = -s->sa_res[q];
+                if (i > 0) {
+                    double Vn = vdot(s->sa_vel[idx3(s, i - 1, j, k)], s->sI[sIi(s, i, j, k)]);
+                    rhs += 0.5 * (Vn + fabs(Vn)) * s->sa_dstar[idx3(s, i - 1, j, k)];
+                }
+                if (!is1D && j > 0) {
+                    double Vn = vdot(s->sa_vel[idx3(s, i, j - 1, k)], s->sJ[sJi(s, i, j, k)]);
+                    rhs += 0.5 * (Vn + fabs(Vn)) * s->sa_dstar[idx3(s, i, j - 1, k)];
+                }
+                if (is3D && k > 0) {
+                    double Vn = vdot(s->sa_vel[idx3(s, i, j, k - 1)], s->sK[sKi(s, i, j, k)]);
+                    rhs += 0.5 * (Vn + fabs(Vn)) * s->sa_dstar[idx3(s, i, j, k - 1)];
+                }
+                s->sa_dstar[q] = rhs / s->sa_diag[q];
+            }
+    for (long i = s->ni - 1; i >= 0; i--)
+        for (long j = s->nj - 1; j >= 0; j--)
+            for (long k = s->nk - 1; k >= 0; k--) {
+                long q = idx3(s, i, j, k);
+                double sum = 0.0;
+                if (i + 1 < s->ni) {
+                    double Vn = vdot(s->sa_vel[idx3(s, i + 1, j, k)], s->sI[sIi(s, i + 1, j, k)]);
+                    sum += 0.5 * (fabs(Vn) - Vn) * s->sa_dnu[idx3(s, i + 1, j, k)];
+                }
+                if (!is1D && j + 1 < s->nj) {
+                    double Vn = vdot(s->sa_vel[idx3(s, i, j + 1, k)], s->sJ[sJi(s, i, j + 1, k)]);
+                    sum += 0.5 * (fabs(Vn) - Vn) * s->sa_dnu[idx3(s, i, j + 1, k)];
+                }
+                if (is3D && k + 1 < s->nk) {
+                    double Vn = vdot(s->sa_vel[idx3(s, i, j, k + 1)], s->sK[sKi(s, i, j, k + 1)]);
+                    sum += 0.5 * (fabs(Vn) - Vn) * s->sa_dnu[idx3(s, i, j, k + 1)];
+                }
+                s->sa_dnu[q] = s->sa_dstar[q] + sum / s->sa_diag[q];
+            }
+    int diverged = 0;
+    for (long q = 0; q < s->n; q++) {
+        double dNu = s->sa_dnu[q] * s->sa_relax;
+        if (isnan(dNu) || isinf(dNu)) diverged = 1;
+        double nn = s->nuhat[q] + dNu;
+        double mx = 1.0e5 * dmax(s->nul[q], 1e-12);
+        nn = dmax(-mx, dmin(nn, mx));
+        s->nuhat[q] = nn;
+    }
+    return diverged;
+}
+
+/* TurbulenceModelSA::solve (src/turbulence_model_sa.cpp:347-368), called once
+ * per iteration before the Runge-Kutta stages with the iteration's time
+ * step (Solver::updateTurbulenceSolution, src/solver.cpp:3061-3071). */
+static int sa_solve(oracle_solver* s, double* const* U) {
+    sa_boundary_values(s);
+    sa_gradient(s);
+    sa_mean_flow(s, U);
+    memset(s->sa_res, 0, sizeof(double) * s->n);
+    sa_flux_dir(s, 0, U);
+    if (s->topology != TOPO_1D) sa_flux_dir(s, 1, U);
+    if (s->topology == TOPO_3D) sa_flux_dir(s, 2, U);
+    for (long i = 0; i < s->ni; i++)
+        for (long j = 0; j < s->nj; j++)
+            for (long k = 0; k < s->nk; k++) {
+                long q = idx3(s, i, j, k);
+                double Qt = sa_source(s, q);
+                s->sa_res[q] -= Qt * s->vol[q];
+            }
+    int div = sa_update(s, U);
+    sa_boundary_values(s);
+    return div;
 }
 
 /* Solver::computeResiduals (src/solver.cpp:1783-1833). */
@@ -1762,7 +2090,10 @@ static void compute_timestep(oracle_solver* s, double* const* U) {
                 double rho = W.v[0];
                 double a = f_sound_speed_rho_u_et(s, W.v[0], u, W.v[4]);
                 double mu = 0.0, mut = 0.0;
-                if (s->viscous) mu = f_mu(s, f_temperature_rho_u_et(s, W.v[0], u, W.v[4]));
+                if (s->viscous) {
+                    mu = f_mu(s, f_temperature_rho_u_et(s, W.v[0], u, W.v[4]));
+                    mut = sa_mut(s, rho, idx3(s, i, j, k));
+                }
                 double nu = mu / rho, nut = mut / rho;
                 double ui = fabs(vdot(u, dI)), uj = fabs(vdot(u, dJ)), uk = fabs(vdot(u, dK));
                 double lc = (ui + a) / dsI;
@@ -2466,13 +2797,9 @@ static int build_boundary_structures(oracle_solver* s) {
 /* setTransportProperties of FluidIdeal (src/fluid_ideal.cpp:209-222) and
  * FluidReal (src/fluid_real.cpp:378-385) with Config::getViscosityModel and
  * getFluidMuConstant (src/config.cpp:575-598); FluidReal's viscosity stays at
- * its 2.0e-5 default unless the model is constant. The Spalart-Allmaras
- * model is outside the oracle. */
+ * its 2.0e-5 default unless the model is constant. */
 static int read_transport(oracle_solver* s) {
     config* c = &s->cfg;
-    int turb = 0;
-    if (cfg_bool(c, "TURBULENCE_ACTIVE", 0, &turb)) return 1;
-    if (turb) return fail("TURBULENCE_ACTIVE: the Spalart-Allmaras model is outside the oracle's scope");
     const char* m = cfg_get(c, "FLUID_VISCOSITY_MODEL");
     int has_mu = cfg_get(c, "FLUID_MU_CONSTANT") || cfg_get(c, "FLUID_CONSTANT_MU");
     if (!m || !strcmp(m, "None")) s->visc_const = has_mu;
@@ -2527,6 +2854,113 @@ static int build_wall_mask(oracle_solver* s) {
         s->grad[v] = (vec3*)calloc(s->n, sizeof(vec3));
         s->gfield[v] = (double*)calloc(s->n, sizeof(double));
     }
+    return 0;
+}
+
+/* Config::isTurbulenceActive / getTurbulenceModel (src/config.cpp:165-207)
+ * and the settings TurbulenceModelSA reads (include/config.hpp:126-133, 229,
+ * 377). The oracle restates SA for ideal-gas, viscous runs started from the
+ * initial field. */
+static int read_turbulence(oracle_solver* s) {
+    config* c = &s->cfg;
+    int turb = 0;
+    if (cfg_bool(c, "TURBULENCE_ACTIVE", 0, &turb)) return 1;
+    s->sa = 0;
+    if (!turb) return 0;
+    const char* m = cfg_get(c, "TURBULENCE_MODEL");
+    if (!m) return fail("Not found value for key \"TURBULENCE_MODEL\" in configuration.");
+    if (!strcmp(m, "None")) return 0;
+    if (strcmp(m, "SA")) return fail("Invalid value for key \"TURBULENCE_MODEL\" in configuration.");
+    if (!s->viscous) return fail("the Spalart-Allmaras model needs VISCOSITY_ACTIVE in the oracle");
+    if (s->real) return fail("the Spalart-Allmaras model with FLUID_MODEL = real is outside the oracle's scope");
+    int restart = 0;
+    if (cfg_bool(c, "RESTART_SOLUTION", 0, &restart)) return 1;
+    if (restart) return fail("a restarted Spalart-Allmaras field is outside the oracle's scope");
+    s->sa = 1;
+    if (cfg_float_def(c, "TURBULENT_PRANDTL_NUMBER", 0.86, &s->sa_prt)) return 1;
+    if (cfg_float_def(c, "IMPLICIT_UNDER_RELAXATION", 1.0, &s->sa_relax)) return 1;
+    return 0;
+}
+
+/* reconstructNuTildeFromEddyViscosity (src/math_utils.cpp:641-675): nu hat
+ * whose fv1 nu hat rho equals mu_t (Newton on chi^4 - y chi^3 - cv1^3 y). */
+static double sa_nutilde_of_eddy(double mu_t, double mu_L, double rho) {
+    if (mu_t <= 0.0 || mu_L <= 0.0 || rho <= 0.0) return 0.0;
+    double nu = mu_L / rho;
+    double y = mu_t / mu_L;
+    double cv1_3 = SA_CV1 * SA_CV1 * SA_CV1;
+    double cv1_3_y = cv1_3 * y;
+    double chi = dmax(y, pow(cv1_3_y, 0.25));
+    for (int it = 0; it < 12; ++it) {
+        double chi2 = chi * chi;
+        double chi3 = chi2 * chi;
+        double chi4 = chi3 * chi;
+        double f = chi4 - y * chi3 - cv1_3_y;
+        double df = 4.0 * chi3 - 3.0 * y * chi2;
+        if (fabs(df) < 1e-14) break;
+        double delta = f / df;
+        chi -= delta;
+        if (fabs(delta) < 1e-10 * (1.0 + chi)) break;
+    }
+    return dmax(0.0, chi * nu);
+}
+
+/* Solver::computeWallDistance / computeMinimumDistanceToBoundary
+ * (src/solver.cpp:657-698): per node the least distance to a node of a
+ * no-slip wall patch; TurbulenceModelSA::setupInitialValues /
+ * initializeFromZero (src/turbulence_model_sa.cpp:32-71): nu hat = scaling
+ * mu(T_init) / rho(p_init, T_init) everywhere. */
+static int setup_sa(oracle_solver* s) {
+    if (!s->sa) return 0;
+    config* c = &s->cfg;
+    s->nuhat = (double*)calloc(s->n, sizeof(double));
+    s->nul = (double*)calloc(s->n, sizeof(double));
+    s->wdist = (double*)calloc(s->n, sizeof(double));
+    s->sa_res = (double*)calloc(s->n, sizeof(double));
+    s->sa_diag = (double*)calloc(s->n, sizeof(double));
+    s->sa_dstar = (double*)calloc(s->n, sizeof(double));
+    s->sa_dnu = (double*)calloc(s->n, sizeof(double));
+    s->nuhat_grad = (vec3*)calloc(s->n, sizeof(vec3));
+    s->sa_vel = (vec3*)calloc(s->n, sizeof(vec3));
+    for (long q = 0; q < s->n; q++) {
+        double mn = 1.0E9;
+        for (int m = 0; m < s->npatches; m++) {
+            const patch* p = &s->patches[m];
+            if (p->type != BC_NO_SLIP_WALL) continue;
+            long r[6], st[3];
+            patch_nodes(s, p, r, st);
+            double pm = 1.0E9;
+            for (long ib = r[0]; ib < r[1]; ib++)
+                for (long jb = r[2]; jb < r[3]; jb++)
+                    for (long kb = r[4]; kb < r[5]; kb++) {
+                        vec3 a = s->vert[q], b = s->vert[idx3(s, ib, jb, kb)];
+                        double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+                        double dd = sqrt(dx * dx + dy * dy + dz * dz);
+                        if (dd < pm) pm = dd;
+                    }
+            if (pm < mn) mn = pm;
+        }
+        s->wdist[q] = mn;
+    }
+    double T, p;
+    if (cfg_float(c, "INIT_TEMPERATURE", &T) || cfg_float(c, "INIT_PRESSURE", &p)) return 1;
+    double rho = p / (s->rgas * T);
+    s->sa_init_nu = f_mu(s, T) / rho;
+    if (cfg_get(c, "TURBULENCE_NU_TILDE_RATIO")) {
+        if (cfg_float(c, "TURBULENCE_NU_TILDE_RATIO", &s->sa_ff_scale)) return 1;
+    } else if (cfg_get(c, "TURBULENCE_EDDY_VISCOSITY_RATIO")) {
+        double ratio;
+        if (cfg_float(c, "TURBULENCE_EDDY_VISCOSITY_RATIO", &ratio)) return 1;
+        s->sa_ff_scale = sa_nutilde_of_eddy(ratio, 1.0, 1.0);
+    } else {
+        s->sa_ff_scale = 3.0;
+    }
+    if (cfg_get(c, "TURBULENCE_INIT_NU_TILDE_RATIO")) {
+        if (cfg_float(c, "TURBULENCE_INIT_NU_TILDE_RATIO", &s->sa_init_scale)) return 1;
+    } else {
+        s->sa_init_scale = s->sa_ff_scale;
+    }
+    for (long q = 0; q < s->n; q++) s->nuhat[q] = s->sa_init_scale * s->sa_init_nu;
     return 0;
 }
 
@@ -2605,6 +3039,7 @@ static int read_settings(oracle_solver* s) {
         s->cp = (s->gamma * s->rgas) / (s->gamma - 1);
     }
     if (s->viscous && read_transport(s)) return 1;
+    if (read_turbulence(s)) return 1;
 
     if (cfg_bool(c, "SIMULATION_IS_STEADY", 1, &s->steady)) return 1;
     if (cfg_int_def(c, "RESIDUALS_DROP_CONVERGENCE", 16, &s->drop)) return 1;
@@ -3031,6 +3466,7 @@ int oracle_create(const char* ini_path, oracle_solver** out) {
     if (read_boundaries(s, path) || build_boundary_structures(s)) { oracle_destroy(s); return 1; }
     resolve_turbo_dir(s);
     if (s->viscous && build_wall_mask(s)) { oracle_destroy(s); return 1; }
+    if (setup_sa(s)) { oracle_destroy(s); return 1; }
     for (int m = 0; m < s->npatches; m++) {
         if (s->patches[m].type == BC_THROTTLE) { s->need_turbo = 1; s->throttle_kt = s->patches[m].values[0]; }
         if (s->patches[m].type == BC_MASS_FLOW) s->need_turbo = 1; /* src/solver.cpp:1311-1316 */
@@ -3103,6 +3539,8 @@ void oracle_destroy(oracle_solver* s) {
     free(s->dt);
     free(s->wall);
     for (int v = 0; v < 4; v++) { free(s->grad[v]); free(s->gfield[v]); }
+    free(s->nuhat); free(s->nul); free(s->wdist); free(s->sa_res); free(s->sa_diag); free(s->sa_dstar);
+    free(s->sa_dnu); free(s->nuhat_grad); free(s->sa_vel);
     free(s->hist);
     free(s);
 }
@@ -3140,6 +3578,10 @@ int oracle_run(oracle_solver* s, long n_iter, long* n_done, int* converged) {
         compute_timestep(s, s->Utmp);
         if (s->nprofiles || s->greitzer) update_radial_profiles(s, s->Utmp);
         no_slip_momentum(s, s->Utmp);
+        if (s->sa) {  /* Solver::solve: computeSolutionGradient, updateTurbulenceSolution */
+            solution_gradient(s, s->Utmp);
+            if (sa_solve(s, s->Utmp)) { *n_done = it - s->iter; s->iter = it; return 2; }
+        }
         for (int st = 0; st < s->nstages; st++) {
             solution_gradient(s, s->Utmp);
             compute_residuals(s, s->Utmp, it);
@@ -3181,6 +3623,13 @@ int oracle_residual(oracle_solver* s, double* dt, double* r0, double* r1, double
     double* outs[5] = {r0, r1, r2, r3, r4};
     for (int c = 0; c < 5; c++) memcpy(outs[c], s->R[c], sizeof(double) * s->n);
     return 0;
+}
+
+/* The Spalart-Allmaras working variable nu hat per node (0 when the model is
+ * off); returns whether the model is on. */
+int oracle_get_nuhat(const oracle_solver* s, double* out) {
+    for (long q = 0; q < s->n; q++) out[q] = s->sa ? s->nuhat[q] : 0.0;
+    return s->sa;
 }
 
 void oracle_get_state(const oracle_solver* s, double* rho, double* rhou, double* rhov, double* rhow,

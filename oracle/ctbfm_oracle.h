@@ -41,6 +41,9 @@ int oracle_residual(oracle_solver* s, double* dt, double* r0, double* r1, double
                     double* r3, double* r4);
 
 /* Conservative state (reference layout, (i*nj + j)*nk + k). */
+/* Spalart-Allmaras working variable per node (zeros without the model);
+ * returns 1 when the model is on. */
+int oracle_get_nuhat(const oracle_solver* s, double* out);
 void oracle_get_state(const oracle_solver* s, double* rho, double* rhou, double* rhov,
                       double* rhow, double* rhoe);
 void oracle_set_state(oracle_solver* s, const double* rho, const double* rhou,

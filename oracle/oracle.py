@@ -53,6 +53,8 @@ def _load():
         lib.oracle_residual.argtypes = [vp] + [dp] * 6
         lib.oracle_residual.restype = ctypes.c_int
         lib.oracle_get_state.argtypes = [vp] + [dp] * 5
+        lib.oracle_get_nuhat.argtypes = [vp, dp]
+        lib.oracle_get_nuhat.restype = ctypes.c_int
         lib.oracle_set_state.argtypes = [vp] + [dp] * 5
         lib.oracle_history.argtypes = [vp, dp, dp, dp, dp]
         lib.oracle_history.restype = ctypes.c_long
@@ -111,6 +113,12 @@ class Oracle:
         u = np.zeros((5, self.n))
         _load().oracle_get_state(self._h, *[_ptr(u[c]) for c in range(5)])
         return u
+
+    def nuhat(self) -> np.ndarray:
+        """The Spalart-Allmaras working variable per node (zeros without it)."""
+        out = np.zeros(self.n)
+        _load().oracle_get_nuhat(self._h, _ptr(out))
+        return out
 
     def set_state(self, u: np.ndarray):
         u = np.ascontiguousarray(u, dtype=np.float64)
@@ -187,4 +195,6 @@ def ref_harness(mode: str, ini_path: str, n_iter: Optional[int] = None,
         res["massflow"] = take(6 * done).reshape(done, 6)
         res["turbo"] = take(4 * done).reshape(done, 4)
         res["hub"] = take(done)
+        if off + 8 * n <= raw.size:  # the Spalart-Allmaras working variable
+            res["nuhat"] = take(n)
     return res

@@ -197,6 +197,11 @@ int main(int argc, char** argv) {
             for (const auto& r : massflows) for (double v : r) writeF64(f, v);
             for (const auto& r : turbo) for (double v : r) writeF64(f, v);
             for (double v : hubPressure) writeF64(f, v);
+            // the Spalart-Allmaras working variable, when the model is on
+            if (config.isTurbulenceActive() && config.getTurbulenceModel() == TurbulenceModel::SPALART_ALLMARAS)
+                for (size_t i = 0; i < ni; ++i)
+                    for (size_t j = 0; j < nj; ++j)
+                        for (size_t k = 0; k < nk; ++k) writeF64(f, solver._turbulenceModel->getWorkingVariable(i, j, k));
             return 0;
         }
         std::cerr << "unknown mode " << mode << "\n";

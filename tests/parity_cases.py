@@ -198,6 +198,12 @@ def _viscous(c, mu=None, walls=(2, 3), **settings):
     return c.with_settings(**kw)
 
 
+def _sa(c, **settings):
+    """The Spalart-Allmaras model (TURBULENCE_MODEL = SA,
+    src/turbulence_model_sa.cpp) on a viscous run."""
+    return c.with_settings(TURBULENCE_ACTIVE="yes", TURBULENCE_MODEL="SA", **settings)
+
+
 def _co2_viscous():
     c = _co2(cases.bump2d(ni=24, nj=12, mach=0.3))
     return _viscous(c, mu=5e-3, FLUID_CP="1200.0", FLUID_PRANDTL_NUMBER="0.9")
@@ -247,6 +253,13 @@ CASES = {
     "annulus_viscous_roe": (lambda: _viscous(cases.annulus3d(ni=20, nj=8, nk=9, bfm_model="None"),
                                              BFM_ACTIVE="no", BLOCKAGE_ACTIVE="no"), 10),
     "co2_bump_viscous": (_co2_viscous, 20),
+    "bump_sa": (lambda: _sa(_viscous(cases.bump2d(ni=24, nj=12))), 20),
+    "bump_sa_roe_relaxed": (lambda: _sa(_viscous(cases.bump2d(ni=24, nj=12, scheme="Roe", muscl=True,
+                                                              limiter="van albada", rk=3, cfl=0.8)),
+                                        TURBULENCE_NU_TILDE_RATIO="5.0", IMPLICIT_UNDER_RELAXATION="0.8"), 20),
+    "meridional_sa_duct": (lambda: _sa(_viscous(cases.meridional(ni=24, nj=10, p_ratio=0.95), BFM_ACTIVE="no",
+                                                BLOCKAGE_ACTIVE="no"), TURBULENCE_EDDY_VISCOSITY_RATIO="0.5"), 20),
+    "sector45_sa": (lambda: _sa(_viscous(_sector(45.0)), TURBULENT_PRANDTL_NUMBER="0.9"), 10),
     "meridional_lift_drag": (lambda: _lift_drag(cases.meridional(ni=24, nj=10, rows=cases.MAP_ROWS)), 20),
     "meridional_hall_stalled": (lambda: _stalled("Hall"), 20),
     "meridional_thollet_off_design_stalled": (_thollet_off_design, 20),
