@@ -242,6 +242,30 @@ struct alignas(16) DevCaseT {
     const R* gwR[3];
     R* G[12];
     R* V[3][4];
+    // TURBULENCE_MODEL = SA (TurbulenceModelSA): the working variable nu hat,
+    // the laminar kinematic viscosity of the model's last solve, the wall
+    // distance, the Green-Gauss gradient of nu hat, the node velocities and the
+    // work arrays of the implicit update (residual, diagonal, forward and
+    // backward increments); per face of each swept direction the distances of
+    // the face centre to its left and right node (interpolateScalar); the
+    // boundary patches in the boundary file's order as rows of 10 ints (kind:
+    // 0 no-slip wall, 1 inlet / farfield, 2 outlet-like; node range [r0, r1) x
+    // [r2, r3) x [r4, r5); donor step i, j, k)
+    int sa;
+    int sa_npatch;
+    double sa_init_nu, sa_ff, sa_relax, sa_prt;
+    R* nuhat;
+    R* nul;
+    const R* sa_wd;
+    R* sa_res;
+    R* sa_diag;
+    R* sa_dstar;
+    R* sa_dnu;
+    R* sa_g[3];
+    R* sa_vel[3];
+    const R* sa_dL[3];
+    const R* sa_dR[3];
+    const int* sa_bc;
     Control* ctl;
     double* hist;  // kHistWidth doubles per iteration row
     long long hist_cap;

@@ -52,6 +52,9 @@ struct BatchView {
     bool viscous = false;  // some member is viscous (VISCOSITY_ACTIVE)
     TileList vnode;        // nodes of the viscous instances (k_grad)
     TileList vface[3];     // every face of each swept direction of the viscous instances (k_vfaces)
+    bool sa = false;       // some member runs the Spalart-Allmaras model
+    TileList sanode;       // nodes of the SA instances (k_prim, k_grad, k_sa_prep, k_sa_res, k_sa_update)
+    TileList sainst;       // one tile per SA instance (k_sa_bc, k_sa_sweep)
     TileList inst;        // one tile per instance (k_pre, k_finalize)
     TileList bint;        // 8 plane tiles per instance that needs turbo performance
     TileList bintAll;     // 8 plane tiles for every instance
@@ -72,6 +75,10 @@ struct Launcher {
     static cudaError_t viscous(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t nodes(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     static cudaError_t periodic(const BatchView<R>& b, int stage, int force, cudaStream_t s);
+    // TurbulenceModelSA::solve of the SA members, once per iteration before
+    // the stages: primitives and solution gradient of U^n, boundary values,
+    // nu hat gradient, residual, the two sweeps, update, boundary values
+    static cudaError_t turbulence(const BatchView<R>& b, cudaStream_t s);
     // k_stage over the fused members' boxes (fusedMode 1)
     static cudaError_t fused(const BatchView<R>& b, int stage, int force, cudaStream_t s);
     // dynamic shared memory of a k_stage block of an instance with box

@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(256, 3) k_vfaces(const DevCaseT<R>* cases, con
         for (int v = 0; v < 4; v++)
             gr[v] = v3((c.G[3 * v][qL] + c.G[3 * v][qR]) * R(0.5), (c.G[3 * v + 1][qL] + c.G[3 * v + 1][qR]) * R(0.5),
                        (c.G[3 * v + 2][qL] + c.G[3 * v + 2][qR]) * R(0.5));
-        const R muEddy = (R(0) + R(0)) * R(0.5);
+        const R muEddy = (saEddy(c, U[0][qL], qL) + saEddy(c, U[0][qR], qR)) * R(0.5);
         const V3<R> n = v3(__ldg(F.nx + f), __ldg(F.ny + f), __ldg(F.nz + f));
         const R area = __ldg(F.area + f);
         R flux[4];
@@ -704,6 +704,9 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
 // ------------------------------------------------------------ fused stage
 #include "stage_fused.cuh"
 
+// ------------------------------------------------------- Spalart-Allmaras
+#include "sa.cuh"
+
 // ------------------------------------------------------------- time step
 // Solver::computeTimestepArray (src/solver.cpp:1531-1630):
 // dt = CFL / (sum_d (|u . e_d| + a) / |e_d| + 4 nu sum_d 1 / |e_d|^2) over the
@@ -733,7 +736,7 @@ __global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile
         R dt;
         if (c.viscous) {  // 4 (nu + nu_t) sum_d 1/|e_d|^2, nu_t = 0
             const R mu = molecularViscosity(c, temperature_rho_u_et(gs, W.v[0], u, W.v[4]));
-            const R nu = mu / W.v[0], nut = R(0) / W.v[0];
+            const R nu = mu / W.v[0], nut = saEddy(c, W.v[0], q) / W.v[0];
             const R dsI = c.edge[3][q], dsJ = c.edge[7][q];
             R ih2 = R(1) / (dsI * dsI);
             ih2 += R(1) / (dsJ * dsJ);
@@ -1275,10 +1278,28 @@ cudaError_t Launcher<R>::stage(const BatchView<R>& b, int stage, int force, cuda
 }
 
 template <typename R>
+cudaError_t Launcher<R>::turbulence(const BatchView<R>& b, cudaStream_t s) {
+    if (!b.sa || !b.sanode.n) return cudaSuccess;
+    const TileList& n = b.sanode;
+    const TileList& m = b.sainst;
+    launchK(k_prim<R>, n.n, 256, s, b.cases, n.tiles, 0, 0);
+    launchK(k_grad<R, 0>, n.n, 256, s, b.cases, n.tiles, 0, 0);
+    launchK(k_sa_bc<R>, m.n, 256, s, b.cases, m.tiles, 0);
+    launchK(k_sa_prep<R, 0>, n.n, 256, s, b.cases, n.tiles, 0);
+    launchK(k_sa_res<R>, n.n, 256, s, b.cases, n.tiles, 0);
+    launchK(k_sa_sweep<R, 1>, m.n, 1024, s, b.cases, m.tiles, 0);
+    launchK(k_sa_sweep<R, 0>, m.n, 1024, s, b.cases, m.tiles, 0);
+    launchK(k_sa_update<R>, n.n, 256, s, b.cases, n.tiles, 0);
+    launchK(k_sa_bc<R>, m.n, 256, s, b.cases, m.tiles, 0);
+    return cudaGetLastError();
+}
+
+template <typename R>
 cudaError_t Launcher<R>::iteration(const BatchView<R>& b, int nstages, cudaStream_t s) {
     cudaError_t e = boundaryIntegrals(b, false, 0, s);
     if (e == cudaSuccess) e = timeStep(b, 0, s);
     if (e == cudaSuccess) e = pre(b, false, true, true, 0, s);
+    if (e == cudaSuccess) e = turbulence(b, s);
     for (int st = 0; st < nstages && e == cudaSuccess; st++) e = stage(b, st, 0, s);
     if (e == cudaSuccess) e = finalize(b, 0, s);
     return e;

@@ -42,10 +42,28 @@ CTBFM_DI R gradientTemperature(const DevCaseT<R>& c, Gas<R> gs, const S5<R>& W) 
     return (W.v[4] - (u * u + v * v + w * w) * R(0.5)) * R((c.gamma - 1.0) / c.rgas);
 }
 
+// TurbulenceModelSA::getEddyViscosity (src/turbulence_model_sa.cpp:843-858):
+// fv1 rho nu_hat with the laminar viscosity of the model's last solve (0
+// before the first, and 0 without the model: TurbulenceModelNone).
+template <typename R>
+CTBFM_DI R saEddy(const DevCaseT<R>& c, R rho, long long q) {
+    if (!c.sa) return R(0);
+    const R nuHat = c.nuhat[q];
+    if (nuHat <= R(0)) return R(0);
+    const R nuL = c.nul[q];
+    if (nuL <= R(0)) return R(0);
+    const R chi = nuHat / nuL;
+    const R chi3 = chi * chi * chi;
+    const R cv1_3 = R(7.1) * R(7.1) * R(7.1);
+    const R fv1 = chi3 / (chi3 + cv1_3);
+    return fv1 * rho * nuHat;
+}
+
 // Solver::computeViscousFlux (src/solver.cpp:2174-2226) with
 // computeViscousStressTensor (src/math_utils.cpp:593-608), on the face
 // average Ua of the two node states and the averaged gradients; n = S/|S|.
-// TurbulenceModelNone gives eddy viscosity and conductivity 0. The mass
+// The eddy conductivity is mu_t cp / Pr_t with SA (getEddyThermalConductivity,
+// include/turbulence_model_sa.hpp:73) and 0 without a model. The mass
 // component is 0 and not returned: the result holds momentum x, y, z and
 // energy.
 template <typename R>
@@ -57,7 +75,8 @@ CTBFM_DI void viscousFlux(const DevCaseT<R>& c, Gas<R> gs, const S5<R>& Ua, V3<R
     const R muL = molecularViscosity(c, T);
     const R kappaL = R(c.vcp) * muL / R(c.vpr);
     const R muT = muL + muEddy;
-    const R kT = kappaL + R(0);
+    const R kappaEddy = c.sa ? muEddy * R(c.vcp) / R(c.sa_prt) : R(0);
+    const R kT = kappaL + kappaEddy;
     const R lam = R(-2.0 / 3.0) * muT;
     const R xx = lam * (gu.x + gv.y + gw.z) + R(2) * muT * gu.x;
     const R yy = lam * (gu.x + gv.y + gw.z) + R(2) * muT * gv.y;

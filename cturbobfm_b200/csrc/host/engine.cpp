@@ -70,6 +70,8 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     for (auto* m : members_) (bfmRareModel(m->c) ? view_.bfmRare : view_.bfmCommon) = true;
     view_.viscous = false;
     for (auto* m : members_) view_.viscous = view_.viscous || m->c.viscous;
+    view_.sa = false;
+    for (auto* m : members_) view_.sa = view_.sa || m->c.sa;
     view_.fusedMode = 1;
     refresh(nullptr);
     cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
@@ -83,7 +85,8 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
 template <typename R>
 void GroupT<R>::buildTiles() {
     const int M = static_cast<int>(members_.size());
-    std::vector<Tile> node, snode[2], face[2][3][2][3], fbox[2], per, inst, bint, bintAll, vnode, vface[3];
+    std::vector<Tile> node, snode[2], face[2][3][2][3], fbox[2], per, inst, bint, bintAll, vnode, vface[3], sanode,
+        sainst;
     auto cover = [](std::vector<Tile>& out, int m, long long count, long long size) {
         int local = 0;
         for (long long s = 0; s < count; s += size) out.push_back({m, local++, s, std::min<long long>(size, count - s)});
@@ -131,6 +134,10 @@ void GroupT<R>::buildTiles() {
                 cover(vface[d], m, static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2)),
                       kTileSize);
         }
+        if (c.sa) {
+            cover(sanode, m, c.n, kTileSize);
+            sainst.push_back({m, 0, 0, 1});
+        }
         if (c.periodic && cover(per, m, static_cast<long long>(c.ni) * c.nj, kPeriodicTile) != c.per_tiles)
             throw std::logic_error("periodic tile count mismatch");
         inst.push_back({m, 0, 0, 1});
@@ -157,6 +164,8 @@ void GroupT<R>::buildTiles() {
     for (int s = 0; s < 2; s++) add(view_.fbox[s], fbox[s]);
     add(view_.per, per);
     add(view_.vnode, vnode);
+    add(view_.sanode, sanode);
+    add(view_.sainst, sainst);
     for (int d = 0; d < 3; d++) add(view_.vface[d], vface[d]);
     add(view_.inst, inst);
     add(view_.bint, bint);

@@ -13,7 +13,11 @@ void writeSolutionCsv(const std::string& path, const Config& config, const Mesh&
                       const double* const U[5], const std::map<std::string, std::vector<double>>* extra) {
     // Config::getOutputFieldsType (src/config.cpp:629-647)
     const std::string t = config.has("OUTPUT_FIELDS_TYPE") ? config.get("OUTPUT_FIELDS_TYPE") : "None";
-    const bool primaryOnly = t == "primary" || t == "Primary" || t == "PRIMARY";
+    // with a turbulence model the secondary fields are written whatever the
+    // type (Output::updateOutputArrays, src/output.cpp:141-143)
+    const bool primaryOnly = (t == "primary" || t == "Primary" || t == "PRIMARY") &&
+                             !(config.parseBool("TURBULENCE_ACTIVE", false) && config.has("TURBULENCE_MODEL") &&
+                               config.get("TURBULENCE_MODEL") == "SA");
     const bool turbo = t == "turbo_bfm" || t == "Turbo_bfm" || t == "TURBO_BFM";
     if (turbo && config.isBFMActive())
         throw ConfigError("OUTPUT_FIELDS_TYPE = turbo_bfm (body forces, deviation angle) is not written by this library");

@@ -117,8 +117,6 @@ SourceBFMChima::SourceBFMChima(const Config& config) : SourceBFMBase(config), le
 }
 
 Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_(config.getTopology()) {
-    if (config.parseBool("TURBULENCE_ACTIVE", false))
-        throw ConfigError("TURBULENCE_ACTIVE: the Spalart-Allmaras model is outside this library's scope");
     // Config::getFluidModel (src/config.cpp:468-481)
     const std::string fluid = config.has("FLUID_MODEL") ? config.get("FLUID_MODEL") : "None";
     if (fluid == "real" || fluid == "Real" || fluid == "REAL") {
@@ -156,6 +154,7 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     readBoundaries();
     buildBoundaryStructures();
     buildWallMask();
+    setupTurbulence();
     validateSettings();
     setupScalars();
     cudaCheck(cudaGetDevice(&device_), "cudaGetDevice");
@@ -245,6 +244,125 @@ void Solver::setupTransport() {
     }
     c.vcp = config_.parseFloat("FLUID_CP");
     c.vpr = config_.parseFloat("FLUID_PRANDTL_NUMBER");
+}
+
+// reconstructNuTildeFromEddyViscosity (src/math_utils.cpp:641-675): nu hat
+// whose fv1 nu hat rho is mu_t (Newton on chi^4 - y chi^3 - cv1^3 y).
+static double nuTildeOfEddyViscosity(double mu_t, double mu_L, double rho, double cv1) {
+    if (mu_t <= 0.0 || mu_L <= 0.0 || rho <= 0.0) return 0.0;
+    const double nu = mu_L / rho;
+    const double y = mu_t / mu_L;
+    const double cv1_3 = cv1 * cv1 * cv1;
+    const double cv1_3_y = cv1_3 * y;
+    double chi = std::max(y, std::pow(cv1_3_y, 0.25));
+    for (int iter = 0; iter < 12; ++iter) {
+        const double chi2 = chi * chi;
+        const double chi3 = chi2 * chi;
+        const double chi4 = chi3 * chi;
+        const double f = chi4 - y * chi3 - cv1_3_y;
+        const double df = 4.0 * chi3 - 3.0 * y * chi2;
+        if (std::abs(df) < 1e-14) break;
+        const double delta = f / df;
+        chi -= delta;
+        if (std::abs(delta) < 1e-10 * (1.0 + chi)) break;
+    }
+    return std::max(0.0, chi * nu);
+}
+
+// Config::isTurbulenceActive / getTurbulenceModel (src/config.cpp:165-207);
+// TurbulenceModelSA::setupInitialValues / initializeFromZero
+// (src/turbulence_model_sa.cpp:32-71); Solver::computeWallDistance /
+// computeMinimumDistanceToBoundary (src/solver.cpp:657-698): the least
+// distance of each node to a node of a no-slip wall patch; the boundary rows
+// of updateBoundaryValues (src/turbulence_model_sa.cpp:250-345) in the
+// boundary file's order. The model runs with VISCOSITY_ACTIVE, the ideal gas
+// and a start from the initial field (a restarted turbulence field is outside
+// this library's scope).
+void Solver::setupTurbulence() {
+    DevCaseT<double>& c = proto_;
+    c.sa = 0;
+    if (!config_.parseBool("TURBULENCE_ACTIVE", false)) return;
+    if (!config_.has("TURBULENCE_MODEL"))
+        throw ConfigError("Not found value for key \"TURBULENCE_MODEL\" in configuration.");
+    const std::string model = config_.get("TURBULENCE_MODEL");
+    if (model == "None") return;
+    if (model != "SA") throw ConfigError("Invalid value for key \"TURBULENCE_MODEL\" in configuration.");
+    if (!c.viscous) throw ConfigError("TURBULENCE_MODEL = SA needs VISCOSITY_ACTIVE in this library");
+    if (table_) throw ConfigError("the Spalart-Allmaras model with FLUID_MODEL = real is outside this library's scope");
+    if (config_.parseBool("RESTART_SOLUTION", false))
+        throw ConfigError("a restarted Spalart-Allmaras field is outside this library's scope");
+    c.sa = 1;
+    c.sa_prt = config_.has("TURBULENT_PRANDTL_NUMBER") ? config_.parseFloat("TURBULENT_PRANDTL_NUMBER") : 0.86;
+    c.sa_relax = config_.has("IMPLICIT_UNDER_RELAXATION") ? config_.parseFloat("IMPLICIT_UNDER_RELAXATION") : 1.0;
+    const double T = config_.getInitTemperature(), p = config_.getInitPressure();
+    const double rho = p / (c.rgas * T);
+    const double mu = c.visc_const ? c.mu_const
+                                   : c.suth_mu * std::pow(T / c.suth_T, 1.5) * ((c.suth_T + c.suth_S) / (T + c.suth_S));
+    c.sa_init_nu = mu / rho;
+    if (config_.has("TURBULENCE_NU_TILDE_RATIO")) c.sa_ff = config_.parseFloat("TURBULENCE_NU_TILDE_RATIO");
+    else if (config_.has("TURBULENCE_EDDY_VISCOSITY_RATIO"))
+        c.sa_ff = nuTildeOfEddyViscosity(config_.parseFloat("TURBULENCE_EDDY_VISCOSITY_RATIO"), 1.0, 1.0, 7.1);
+    else c.sa_ff = 3.0;
+    const double initScale =
+        config_.has("TURBULENCE_INIT_NU_TILDE_RATIO") ? config_.parseFloat("TURBULENCE_INIT_NU_TILDE_RATIO") : c.sa_ff;
+    saInitNuHat_ = initScale * c.sa_init_nu;
+    const long NI = mesh_.ni(), NJ = mesh_.nj(), NK = mesh_.nk(), N = mesh_.nodes();
+    // node range and donor step of a patch (fetchBoundaryNodesIndexRange,
+    // src/boundary_base.cpp:227-267; Boundary::computeOrientation,
+    // include/boundary_base.hpp:109-119)
+    auto range = [&](const auto& b, long r[6], int st[3]) {
+        r[0] = b.i_min; r[1] = b.i_max; r[2] = b.j_min; r[3] = b.j_max; r[4] = b.k_min; r[5] = b.k_max;
+        if (r[0] == r[1] && r[0] == 0) r[1] = 1;
+        else if (r[0] == r[1] && r[0] == NI) { r[0] = NI - 1; r[1] = r[0] + 1; }
+        else if (r[2] == r[3] && r[2] == 0) r[3] = 1;
+        else if (r[2] == r[3] && r[2] == NJ) { r[2] = NJ - 1; r[3] = r[2] + 1; }
+        else if (r[4] == r[5] && r[4] == 0) r[5] = 1;
+        else if (r[4] == r[5] && r[4] == NK) { r[4] = NK - 1; r[5] = r[4] + 1; }
+        else throw ConfigError("Invalid indexing on boundary condition specs for patch " + b.name);
+        st[0] = st[1] = st[2] = 0;
+        if (b.i_min == b.i_max) st[0] = b.i_min == 0 ? 1 : -1;
+        else if (b.j_min == b.j_max) st[1] = b.j_min == 0 ? 1 : -1;
+        else if (b.k_min == b.k_max) st[2] = b.k_min == 0 ? 1 : -1;
+    };
+    const auto& P = mesh_.vertices();
+    saWd_.assign(static_cast<size_t>(N), 1.0E9);
+    saBc_.clear();
+    for (const auto& b : boundaries_) {
+        long r[6];
+        int st[3];
+        int kind = -1;
+        if (b.type == kBcNoSlipWall) kind = 0;
+        else if (b.type == kBcInlet || b.type == kBcInletSupersonic || b.type == kBcFarfield) kind = 1;
+        else if (b.type == kBcOutlet || b.type == kBcRadialEq || b.type == kBcThrottle || b.type == kBcMassFlow ||
+                 b.type == kBcOutletSupersonic || b.type == kBcInviscidWall || b.type == kBcTransparent)
+            kind = 2;
+        if (kind < 0) continue;
+        range(b, r, st);
+        saBc_.insert(saBc_.end(), {kind, int(r[0]), int(r[1]), int(r[2]), int(r[3]), int(r[4]), int(r[5]), st[0],
+                                   st[1], st[2]});
+    }
+    c.sa_npatch = static_cast<int>(saBc_.size() / 10);
+    for (long q = 0; q < N; q++) {
+        double mn = 1.0E9;
+        for (const auto& b : boundaries_) {
+            if (b.type != kBcNoSlipWall) continue;
+            long r[6];
+            int st[3];
+            range(b, r, st);
+            double pm = 1.0E9;
+            for (long ib = r[0]; ib < r[1]; ib++)
+                for (long jb = r[2]; jb < r[3]; jb++)
+                    for (long kb = r[4]; kb < r[5]; kb++) {
+                        const auto& a = P[q];
+                        const auto& w = P[mesh_.idx(ib, jb, kb)];
+                        const double dx = a.x - w.x, dy = a.y - w.y, dz = a.z - w.z;
+                        const double dd = std::sqrt(dx * dx + dy * dy + dz * dz);
+                        if (dd < pm) pm = dd;
+                    }
+            if (pm < mn) mn = pm;
+        }
+        saWd_[q] = mn;
+    }
 }
 
 // The nodes of every no-slip wall patch (Solver::buildBoundaryFluxes,
@@ -703,6 +821,7 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         }
         if (c.viscous) {  // raw S and the Green-Gauss weights of the face's left and right node
             std::vector<double> sx(S.size()), sy(S.size()), sz(S.size()), wl(S.size(), 0.0), wr(S.size(), 0.0);
+            std::vector<double> dl(c.sa ? S.size() : 0, 0.0), dr(c.sa ? S.size() : 0, 0.0);
             const auto& C = mesh_.centers(d);
             const auto& P = mesh_.vertices();
             const long nfi = NI + (d == 0), nfj = NJ + (d == 1), nfk = NK + (d == 2);
@@ -728,12 +847,22 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
                             const double d0 = (C[f] - P[ql]).magnitude(), d1 = (C[f] - P[qr]).magnitude();
                             wl[f] = d0 / (d0 + d1);
                         }
+                        // interpolateScalar of the SA gradient (src/math_utils.cpp:457-460): the
+                        // face centre's distances to the left and the right node
+                        if (c.sa) {
+                            dl[f] = (C[f] - P[ql]).magnitude();
+                            dr[f] = (C[f] - P[qr]).magnitude();
+                        }
                     }
             c.sraw[d][0] = inst.uploadR(sx);
             c.sraw[d][1] = inst.uploadR(sy);
             c.sraw[d][2] = inst.uploadR(sz);
             c.gwL[d] = inst.uploadR(wl);
             c.gwR[d] = inst.uploadR(wr);
+            if (c.sa) {
+                c.sa_dL[d] = inst.uploadR(dl);
+                c.sa_dR[d] = inst.uploadR(dr);
+            }
             if (d < 2 || topo_ == Topology::ThreeD)
                 for (int v = 0; v < 4; v++) c.V[d][v] = inst.allocR(S.size());
         }
@@ -797,6 +926,23 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
             c.G[g] = inst.allocR(N);
             cudaCheck(cudaMemset(c.G[g], 0, N * sizeof(R)), "cudaMemset");
         }
+    }
+    if (c.sa) {  // Spalart-Allmaras: nu hat, laminar viscosity (0 until the first solve), work arrays
+        c.nuhat = const_cast<R*>(inst.uploadR(std::vector<double>(static_cast<size_t>(N), saInitNuHat_)));
+        c.nul = inst.allocR(N);
+        cudaCheck(cudaMemset(c.nul, 0, N * sizeof(R)), "cudaMemset");
+        c.sa_wd = inst.uploadR(saWd_);
+        c.sa_res = inst.allocR(N);
+        c.sa_diag = inst.allocR(N);
+        c.sa_dstar = inst.allocR(N);
+        c.sa_dnu = inst.allocR(N);
+        for (int x = 0; x < 3; x++) {
+            c.sa_g[x] = inst.allocR(N);
+            c.sa_vel[x] = inst.allocR(N);
+        }
+        void* d = inst.allocBytes(saBc_.size() * sizeof(int));
+        cudaCheck(cudaMemcpy(d, saBc_.data(), saBc_.size() * sizeof(int), cudaMemcpyHostToDevice), "cudaMemcpy");
+        c.sa_bc = static_cast<const int*>(d);
     }
     // boundary planes (raw surface vectors) for the surface integrals
     for (int b = 0; b < 6; b++) {
@@ -1231,7 +1377,9 @@ void Solver::writeSolution(const std::string& path) {
 
 // Output::updateViscousFields (src/output.cpp:240-306) with
 // computeWallShearStress (:308-367): molecular viscosity of every node's
-// temperature, eddy viscosity 0 (no turbulence model), and on the nodes of
+// temperature, the eddy viscosity of the model (0 without one; with SA
+// getEddyViscosity of the state's density and the model's last laminar
+// viscosity) and its working variable ("Nu Tilde"), and on the nodes of
 // each no-slip wall (patch order; a later patch overwrites a shared node)
 // the wall shear stress from the latest stage's velocity gradients and
 // y+ = sqrt(|tau_w| rho) d / mu, d the wall-distance step to the next node
@@ -1258,6 +1406,29 @@ void Solver::viscousOutputFields(const double* const U[5], std::map<std::string,
     for (long q = 0; q < N; q++) {
         const Vec3 u(U[1][q] / U[0][q], U[2][q] / U[0][q], U[3][q] / U[0][q]);
         muL[q] = mu(fluid->temperature_rho_u_et(U[0][q], u, U[4][q] / U[0][q]));
+    }
+    if (c.sa) {  // TurbulenceModelSA::getEddyViscosity / getWorkingVariable
+        std::vector<double> nuHat(static_cast<size_t>(N)), nuL(static_cast<size_t>(N));
+        visit([&](auto& inst, auto&) {
+            using R = std::remove_reference_t<decltype(*inst.c.U[0])>;
+            std::vector<R> tmp(static_cast<size_t>(N));
+            cudaCheck(cudaMemcpy(tmp.data(), inst.c.nuhat, N * sizeof(R), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            nuHat.assign(tmp.begin(), tmp.end());
+            cudaCheck(cudaMemcpy(tmp.data(), inst.c.nul, N * sizeof(R), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            nuL.assign(tmp.begin(), tmp.end());
+        });
+        auto& eddy = out["Eddy Viscosity"];
+        for (long q = 0; q < N; q++) {
+            double e = 0.0;
+            if (nuHat[q] > 0.0 && nuL[q] > 0.0) {
+                const double chi = nuHat[q] / nuL[q];
+                const double chi3 = chi * chi * chi;
+                const double cv1_3 = 7.1 * 7.1 * 7.1;
+                e = chi3 / (chi3 + cv1_3) * U[0][q] * nuHat[q];
+            }
+            eddy[q] = e;
+        }
+        out["Nu Tilde"] = nuHat;
     }
     std::array<std::vector<double>, 12> G;
     visit([&](auto& inst, auto&) {
@@ -1470,6 +1641,16 @@ void Solver::promoteToFP64() {
     auto grp = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{inst.get()});
     grp->setFusedMode(fusion_);
     const DevCaseT<float>& f = i32_->c;
+    if (proto_.sa) {  // the model's nu hat and laminar viscosity carry over
+        std::vector<float> tf(static_cast<size_t>(N));
+        std::vector<double> td(static_cast<size_t>(N));
+        const std::pair<const float*, double*> pairs[2] = {{f.nuhat, inst->c.nuhat}, {f.nul, inst->c.nul}};
+        for (const auto& pr : pairs) {
+            cudaCheck(cudaMemcpy(tf.data(), pr.first, N * sizeof(float), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            std::copy(tf.begin(), tf.end(), td.begin());
+            cudaCheck(cudaMemcpy(pr.second, td.data(), N * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+        }
+    }
     if (proto_.nprofiles)
         cudaCheck(cudaMemcpy(inst->c.prof_p, f.prof_p, profP_.size() * sizeof(double), cudaMemcpyDeviceToDevice),
                   "cudaMemcpy");

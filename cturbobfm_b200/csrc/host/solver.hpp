@@ -106,6 +106,9 @@ private:
     void setupModels();
     void setupTransport();
     void buildWallMask();
+    // TURBULENCE_ACTIVE / TURBULENCE_MODEL: the Spalart-Allmaras settings,
+    // wall distance and boundary table (nothing without the model)
+    void setupTurbulence();
     void viscousOutputFields(const double* const U[5], std::map<std::string, std::vector<double>>& out);
     // copies a state to the device as it is (setState adds the no-slip wall
     // preprocessing of viscous runs)
@@ -140,6 +143,11 @@ private:
     DevCaseT<double> proto_{};  // scalar settings shared by both precisions
     std::vector<signed char> mapI_, mapJ_, mapK_;
     std::vector<unsigned char> wall_;  // viscous runs: 1 on no-slip wall nodes
+    // Spalart-Allmaras: wall distance per node, the boundary rows of DevCaseT
+    // sa_bc and the initial nu hat
+    std::vector<double> saWd_;
+    std::vector<int> saBc_;
+    double saInitNuHat_ = 0.0;
     std::vector<double> profP_, profR_;
 
     std::unique_ptr<InstanceT<double>> i64_;

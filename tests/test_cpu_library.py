@@ -141,7 +141,11 @@ def _viscous_bump(walls="no_slip_wall, 0, 0, 0", **settings):
 
 
 @pytest.mark.parametrize("walls,settings,message", [
-    ("no_slip_wall, 0, 0, 0", {"TURBULENCE_ACTIVE": "yes"}, "Spalart-Allmaras"),
+    ("no_slip_wall, 0, 0, 0", {"TURBULENCE_ACTIVE": "yes"}, "Not found value for key \"TURBULENCE_MODEL\""),
+    ("no_slip_wall, 0, 0, 0", {"TURBULENCE_ACTIVE": "yes", "TURBULENCE_MODEL": "kOmega"},
+     "Invalid value for key \"TURBULENCE_MODEL\""),
+    ("no_slip_wall, 0, 0, 0", {"TURBULENCE_ACTIVE": "yes", "TURBULENCE_MODEL": "SA", "RESTART_SOLUTION": "yes"},
+     "restarted Spalart-Allmaras field"),
     ("no_slip_wall, 0, 0, 0", {"FLUID_VISCOSITY_MODEL": "Power"}, "Unknown ViscosityModel: Power"),
     ("no_slip_wall, 0, 0, 0", {"FLUID_CP": None}, "Not found value for key \"FLUID_CP\""),
     ("no_slip_wall, 0, 0, 0", {"FLUID_PRANDTL_NUMBER": None}, "Not found value for key \"FLUID_PRANDTL_NUMBER\""),
