@@ -154,9 +154,9 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     readBoundaries();
     buildBoundaryStructures();
     buildWallMask();
-    setupTurbulence();
     validateSettings();
     setupScalars();
+    setupTurbulence();  // after setupScalars: needs the gas constant
     cudaCheck(cudaGetDevice(&device_), "cudaGetDevice");
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = ownStream_;
