@@ -99,6 +99,18 @@ class Case:
         return dataclasses.replace(self, settings=s)
 
     # -- file output ------------------------------------------------------
+    def write_side_files(self, directory: str) -> None:
+        """Writes the input files the settings name besides the grid and the
+        boundaries (the fluid table, ``files``) into ``directory``."""
+        os.makedirs(directory, exist_ok=True)
+        for name, text in (self.files or {}).items():
+            with open(os.path.join(directory, name), "w") as f:
+                f.write(text)
+        if self.table is not None:
+            from . import fluid_table
+
+            fluid_table.write(os.path.join(directory, self.settings["FLUID_TABLE_FILE"]), **self.table)
+
     def write(self, directory: str) -> str:
         """Writes grid.csv, boundaries.csv and input.ini; returns the ini path."""
         os.makedirs(directory, exist_ok=True)
@@ -120,13 +132,7 @@ class Case:
         settings["BOUNDARY_CONDITIONS_FILEPATH"] = "boundaries.csv"
         for p in self.patches:
             settings[p.name] = p.spec
-        for name, text in (self.files or {}).items():
-            with open(os.path.join(directory, name), "w") as f:
-                f.write(text)
-        if self.table is not None:
-            from . import fluid_table
-
-            fluid_table.write(os.path.join(directory, settings["FLUID_TABLE_FILE"]), **self.table)
+        self.write_side_files(directory)
         ini = os.path.join(directory, "input.ini")
         with open(ini, "w") as f:
             f.write("[CFD]\n")

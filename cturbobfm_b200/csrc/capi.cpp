@@ -77,6 +77,47 @@ int statusCode(ctbfm_solver* s) {
     return CTBFM_OK;
 }
 
+// A checked, owned copy of a case description; std::invalid_argument
+// (CTBFM_E_ARGUMENT) for a malformed one.
+std::unique_ptr<ctbfm::CaseData> caseData(const ctbfm_case_desc* d) {
+    if (d->ni < 1 || d->nj < 1 || d->nk < 1) throw std::invalid_argument("ni, nj and nk must be at least 1");
+    if (d->nj > (int64_t(1) << 40) / d->ni || d->nk > (int64_t(1) << 40) / (d->ni * d->nj))
+        throw std::invalid_argument("the grid is too large");
+    if (!d->x || !d->y || !d->z) throw std::invalid_argument("null grid coordinates");
+    if (d->n_fields < 0 || d->n_patches < 0 || d->n_settings < 0)
+        throw std::invalid_argument("negative count in the case description");
+    if (d->n_fields > 0 && (!d->field_names || !d->fields)) throw std::invalid_argument("null grid field arrays");
+    if (d->n_patches > 0 && !d->patches) throw std::invalid_argument("null patch array");
+    if (d->n_settings > 0 && (!d->keys || !d->values)) throw std::invalid_argument("null settings arrays");
+    auto c = std::make_unique<ctbfm::CaseData>();
+    c->ni = static_cast<long>(d->ni);
+    c->nj = static_cast<long>(d->nj);
+    c->nk = static_cast<long>(d->nk);
+    const size_t n = static_cast<size_t>(d->ni * d->nj * d->nk);
+    c->x.assign(d->x, d->x + n);
+    c->y.assign(d->y, d->y + n);
+    c->z.assign(d->z, d->z + n);
+    for (int32_t q = 0; q < d->n_fields; q++) {
+        if (!d->field_names[q] || !d->fields[q]) throw std::invalid_argument("null grid field name or values");
+        c->fields.emplace_back(d->field_names[q], std::vector<double>(d->fields[q], d->fields[q] + n));
+    }
+    for (int32_t q = 0; q < d->n_patches; q++) {
+        const ctbfm_patch& p = d->patches[q];
+        if (!p.name) throw std::invalid_argument("null patch name");
+        ctbfm::PatchRow row;
+        row.name = p.name;
+        const int64_t r[6] = {p.i_min, p.i_max, p.j_min, p.j_max, p.k_min, p.k_max};
+        for (int a = 0; a < 6; a++) row.range[a] = static_cast<long>(r[a]);
+        c->patches.push_back(std::move(row));
+    }
+    for (int32_t q = 0; q < d->n_settings; q++) {
+        if (!d->keys[q] || !d->values[q]) throw std::invalid_argument("null setting key or value");
+        c->settings.emplace_back(d->keys[q], d->values[q]);
+    }
+    c->directory = d->directory ? d->directory : "";
+    return c;
+}
+
 }  // namespace
 
 extern "C" {
@@ -93,6 +134,20 @@ int ctbfm_create_from_ini(const char* ini_path, ctbfm_solver** out) {
         s->config = std::make_unique<ctbfm::Config>(ini_path);
         s->mesh = std::make_unique<ctbfm::Mesh>(*s->config);
         s->solver = std::make_unique<ctbfm::Solver>(*s->config, *s->mesh);
+        *out = s.release();
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_create(const ctbfm_case_desc* d, ctbfm_solver** out) {
+    if (!d || !out) return setError(CTBFM_E_ARGUMENT, "null argument");
+    *out = nullptr;
+    return guarded([&] {
+        const std::unique_ptr<ctbfm::CaseData> data = caseData(d);
+        auto s = std::make_unique<ctbfm_solver>();
+        s->config = std::make_unique<ctbfm::Config>(data->settings, data->directory);
+        s->mesh = data->mesh(*s->config);
+        s->solver = std::make_unique<ctbfm::Solver>(*s->config, *s->mesh, &data->patches);
         *out = s.release();
         return CTBFM_OK;
     });
@@ -382,6 +437,15 @@ int ctbfm_server_submit(ctbfm_server* s, const char* ini_path, int64_t* request_
     if (!s || !ini_path) return setError(CTBFM_E_ARGUMENT, "null argument");
     return guarded([&] {
         const long long id = s->server->submit(ini_path);
+        if (request_id) *request_id = id;
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_server_submit_case(ctbfm_server* s, const ctbfm_case_desc* desc, int64_t* request_id) {
+    if (!s || !desc) return setError(CTBFM_E_ARGUMENT, "null argument");
+    return guarded([&] {
+        const long long id = s->server->submit(caseData(desc));
         if (request_id) *request_id = id;
         return CTBFM_OK;
     });

@@ -40,6 +40,15 @@ Config::Config(const std::string& path) {
     }
 }
 
+Config::Config(const std::vector<std::pair<std::string, std::string>>& settings, const std::string& directory)
+    : dir_(directory) {
+    for (const auto& kv : settings) {
+        const std::string key = trim(kv.first, " \t\r\n");
+        if (key.empty()) throw ConfigError("empty setting key");
+        data_[key] = trim(kv.second, " \t\r\n");
+    }
+}
+
 std::string Config::get(const std::string& key) const {
     auto it = data_.find(key);
     return it == data_.end() ? std::string() : it->second;

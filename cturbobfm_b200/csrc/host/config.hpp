@@ -24,6 +24,10 @@ public:
 class Config {
 public:
     explicit Config(const std::string& path);
+    // Settings given in memory as key/value strings, trimmed as the file
+    // reader trims them; files that settings still name resolve against
+    // `directory` ("" = the current directory).
+    Config(const std::vector<std::pair<std::string, std::string>>& settings, const std::string& directory);
 
     bool has(const std::string& key) const { return data_.count(key) > 0; }
     std::string get(const std::string& key) const;

@@ -12,6 +12,30 @@ Mesh::Mesh(const Config& config) : topo_(config.getTopology()) {
     std::string path = config.gridFilePath();
     if (!path.empty() && path[0] != '/') path = config.directory() + "/" + path;
     readGrid(path);
+    build(config, path);
+}
+
+Mesh::Mesh(const Config& config, long ni, long nj, long nk, const double* x, const double* y, const double* z,
+           const std::vector<std::pair<std::string, const double*>>& fields)
+    : ni_(ni), nj_(nj), nk_(nk), topo_(config.getTopology()) {
+    if (ni < 1 || nj < 1 || nk < 1) throw ConfigError("the grid needs ni, nj, nk >= 1");
+    if (nj > (1L << 40) / ni || nk > (1L << 40) / (ni * nj)) throw ConfigError("the grid is too large");
+    if (!x || !y || !z) throw ConfigError("the grid needs x, y and z");
+    const long n = ni * nj * nk;
+    vert_.resize(n);
+    for (long q = 0; q < n; q++) vert_[q] = Vec3(x[q], y[q], z[q]);
+    for (const auto& f : fields) {
+        if (f.first.empty() || !f.second) throw ConfigError("a grid field needs a name and values");
+        if (f.first == "x" || f.first == "y" || f.first == "z" || fields_.count(f.first))
+            throw ConfigError("grid field " + f.first + " given twice");
+        fields_[f.first].assign(f.second, f.second + n);
+    }
+    ndim_ = (nj_ == 1 && nk_ == 1) ? 1 : (nk_ == 1 ? 2 : 3);
+    build(config, "the grid arrays");
+}
+
+// The dual grid and every metric, from the vertices (src/mesh.cpp:11-677).
+void Mesh::build(const Config& config, const std::string& source) {
     if (topo_ == Topology::OneD) throw ConfigError("1-D topology is outside this library's scope");
     if ((topo_ == Topology::ThreeD) != (nk_ > 1))
         throw ConfigError("TOPOLOGY does not match the grid's NK");
@@ -23,7 +47,7 @@ Mesh::Mesh(const Config& config) : topo_(config.getTopology()) {
     interfaces();
     finiteVolumes();
     if (config.isBFMActive()) {
-        if (!hasField("blockage")) throw ConfigError("blockage not found in: " + path);
+        if (!hasField("blockage")) throw ConfigError("blockage not found in: " + source);
         blockageGradientGreenGauss();
     }
 }

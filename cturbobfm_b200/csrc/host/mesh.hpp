@@ -32,6 +32,11 @@ struct Vec3 {
 class Mesh {
 public:
     Mesh(const Config& config);
+    // A grid given in memory: ni*nj*nk coordinates and further columns
+    // (blockage, blade normals, ...) with node (i, j, k) at (i*nj + j)*nk + k,
+    // the grid file's row order. The arrays are copied.
+    Mesh(const Config& config, long ni, long nj, long nk, const double* x, const double* y, const double* z,
+         const std::vector<std::pair<std::string, const double*>>& fields);
 
     long ni() const { return ni_; }
     long nj() const { return nj_; }
@@ -72,6 +77,7 @@ public:
 
 private:
     void readGrid(const std::string& path);
+    void build(const Config& config, const std::string& source);
     void dual2d(bool axisymmetric);
     void dual3d();
     void interfaces();

@@ -42,6 +42,17 @@ long long Server::submit(const std::string& iniPath) {
     auto j = std::make_unique<Job>();
     j->ini = iniPath;
     j->t_submit = now();
+    return enqueue(std::move(j));
+}
+
+long long Server::submit(std::unique_ptr<CaseData> data) {
+    auto j = std::make_unique<Job>();
+    j->data = std::move(data);
+    j->t_submit = now();
+    return enqueue(std::move(j));
+}
+
+long long Server::enqueue(std::unique_ptr<Job> j) {
     std::lock_guard<std::mutex> l(mu_);
     j->id = nextId_++;
     prep_.push_back(j.get());
@@ -68,8 +79,13 @@ void Server::worker() {
         int err = 0;
         std::string msg;
         try {
-            cfg = std::make_unique<Config>(j->ini);
-            mesh = std::make_unique<Mesh>(*cfg);
+            if (j->data) {
+                cfg = std::make_unique<Config>(j->data->settings, j->data->directory);
+                mesh = j->data->mesh(*cfg);
+            } else {
+                cfg = std::make_unique<Config>(j->ini);
+                mesh = std::make_unique<Mesh>(*cfg);
+            }
         } catch (const std::exception& e) {
             err = 1;  // CTBFM_E_CONFIG
             msg = e.what();
@@ -77,6 +93,10 @@ void Server::worker() {
         std::lock_guard<std::mutex> l(mu_);
         j->config = std::move(cfg);
         j->mesh = std::move(mesh);
+        if (j->data) {
+            j->patches = std::move(j->data->patches);
+            j->data.reset();
+        }
         j->error = err;
         j->message = msg;
         j->nodes = j->mesh ? static_cast<long long>(j->mesh->nodes()) : 0;
@@ -176,7 +196,7 @@ void Server::admit() {
             continue;
         }
         try {
-            j->solver = std::make_unique<Solver>(*j->config, *j->mesh);
+            j->solver = std::make_unique<Solver>(*j->config, *j->mesh, j->ini.empty() ? &j->patches : nullptr);
         } catch (const ConfigError& e) {
             const std::string msg = e.what();
             retire(std::move(j), nullptr, 1, msg);
@@ -264,7 +284,7 @@ void Server::process(const std::vector<Control>& ctl) {
             j->rerun = true;
             j->config->set("GPU_PRECISION", "fp64");
             try {
-                j->solver = std::make_unique<Solver>(*j->config, *j->mesh);
+                j->solver = std::make_unique<Solver>(*j->config, *j->mesh, j->ini.empty() ? &j->patches : nullptr);
                 j->bytes = j->solver->deviceBytes();
                 used_ += j->bytes;
             } catch (const std::exception& e) {

@@ -55,6 +55,8 @@ public:
 
     // Queues a request (thread safe); its host preparation starts at once.
     long long submit(const std::string& iniPath);
+    // The same for a case held in memory (the server keeps the copy).
+    long long submit(std::unique_ptr<CaseData> data);
     // One scheduling round: waits for the chunk the previous round enqueued
     // and retires, promotes and re-runs from its results; the solves built
     // during that chunk join the batches; the next chunk of `chunk`
@@ -71,6 +73,8 @@ private:
     struct Job {
         long long id = 0;
         std::string ini;
+        std::unique_ptr<CaseData> data;  // in-memory case, released once the mesh is built
+        std::vector<PatchRow> patches;   // its boundary patches
         double t_submit = 0, t_admit = 0;
         bool prepared = false;
         int error = 0;
@@ -82,6 +86,7 @@ private:
         size_t bytes = 0;
         bool rerun = false;  // a diverged float solve restarted in FP64
     };
+    long long enqueue(std::unique_ptr<Job> j);
     void worker();
     void rebuild();
     // builds the Solvers of queued requests that fit the slots, memory and

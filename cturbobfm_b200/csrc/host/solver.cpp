@@ -116,7 +116,8 @@ SourceBFMChima::SourceBFMChima(const Config& config) : SourceBFMBase(config), le
     te_ = static_cast<int>(config.parseFloat("TRAILING_EDGE_INDEX"));
 }
 
-Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_(config.getTopology()) {
+Solver::Solver(Config& config, Mesh& mesh, const std::vector<PatchRow>* patches)
+    : config_(config), mesh_(mesh), topo_(config.getTopology()) {
     // Config::getFluidModel (src/config.cpp:468-481)
     const std::string fluid = config.has("FLUID_MODEL") ? config.get("FLUID_MODEL") : "None";
     if (fluid == "real" || fluid == "Real" || fluid == "REAL") {
@@ -151,7 +152,7 @@ Solver::Solver(Config& config, Mesh& mesh) : config_(config), mesh_(mesh), topo_
     // every setting and input file is validated before the first CUDA call,
     // so that input errors are reported as such on any machine
     setupModels();
-    readBoundaries();
+    readBoundaries(patches);
     buildBoundaryStructures();
     buildWallMask();
     validateSettings();
@@ -397,52 +398,65 @@ void Solver::buildWallMask() {
 }
 
 // Solver::readBoundaryFile (src/solver.cpp:232-294).
-void Solver::readBoundaries() {
-    std::string path = config_.boundaryConditionsFilePath();
-    if (!path.empty() && path[0] != '/') path = config_.directory() + "/" + path;
-    std::ifstream file(path);
-    if (!file.is_open()) throw ConfigError("Cannot open file: " + path);
-    std::string line;
-    bool inData = false;
-    while (std::getline(file, line)) {
-        if (!line.empty() && line.back() == '\r') line.pop_back();
-        if (line.empty()) continue;
-        if (line.find('=') != std::string::npos) continue;
-        if (line.find("PATCH_NAME") != std::string::npos) {
-            inData = true;
-            continue;
-        }
-        if (!inData) continue;
-        std::stringstream ss(line);
-        std::string tok;
-        BoundaryPatch p;
-        std::getline(ss, tok, ',');
-        tok.erase(std::remove(tok.begin(), tok.end(), ' '), tok.end());
-        p.name = tok;
-        long v[6];
-        for (int q = 0; q < 6; q++) {
-            if (!std::getline(ss, tok, ',')) throw ConfigError("bad boundary row for " + p.name);
-            tok.erase(std::remove(tok.begin(), tok.end(), ' '), tok.end());
-            v[q] = std::stoi(tok);
-        }
-        p.i_min = v[0]; p.i_max = v[1]; p.j_min = v[2]; p.j_max = v[3]; p.k_min = v[4]; p.k_max = v[5];
-        const std::vector<std::string> info = config_.parseList(p.name);
-        if (info.empty()) throw ConfigError("Boundary info for " + p.name + " is missing in configuration.");
-        p.type = boundaryTypeFromString(info[0]);
-        for (size_t q = 1; q < info.size(); q++) {
-            try {
-                p.values.push_back(std::stod(info[q]));
-            } catch (const std::exception&) {
-                throw ConfigError("Invalid float format for boundary value \"" + info[q] + "\" in configuration.");
+void Solver::readBoundaries(const std::vector<PatchRow>* patches) {
+    if (patches) {
+        for (const PatchRow& row : *patches) addBoundary(row);
+    } else {
+        std::string path = config_.boundaryConditionsFilePath();
+        if (!path.empty() && path[0] != '/') path = config_.directory() + "/" + path;
+        std::ifstream file(path);
+        if (!file.is_open()) throw ConfigError("Cannot open file: " + path);
+        std::string line;
+        bool inData = false;
+        while (std::getline(file, line)) {
+            if (!line.empty() && line.back() == '\r') line.pop_back();
+            if (line.empty()) continue;
+            if (line.find('=') != std::string::npos) continue;
+            if (line.find("PATCH_NAME") != std::string::npos) {
+                inData = true;
+                continue;
             }
+            if (!inData) continue;
+            std::stringstream ss(line);
+            std::string tok;
+            PatchRow row;
+            std::getline(ss, tok, ',');
+            tok.erase(std::remove(tok.begin(), tok.end(), ' '), tok.end());
+            row.name = tok;
+            for (int q = 0; q < 6; q++) {
+                if (!std::getline(ss, tok, ',')) throw ConfigError("bad boundary row for " + row.name);
+                tok.erase(std::remove(tok.begin(), tok.end(), ' '), tok.end());
+                row.range[q] = std::stoi(tok);
+            }
+            addBoundary(row);
         }
-        if (p.i_min == p.i_max) p.orientation = p.i_min == 0 ? 0 : 1;
-        else if (p.j_min == p.j_max) p.orientation = p.j_min == 0 ? 2 : 3;
-        else p.orientation = p.k_min == 0 ? 4 : 5;
-        boundaries_.push_back(std::move(p));
     }
     if (boundaries_.size() > static_cast<size_t>(kMaxPatches))
         throw ConfigError("more than 16 boundary patches");
+}
+
+// One patch: its index range, and its type and values from the setting of
+// the same name (src/solver.cpp:296-345 via Config::getBoundaryInfo).
+void Solver::addBoundary(const PatchRow& row) {
+    BoundaryPatch p;
+    p.name = row.name;
+    if (p.name.empty()) throw ConfigError("a boundary patch needs a name");
+    const long* v = row.range;
+    p.i_min = v[0]; p.i_max = v[1]; p.j_min = v[2]; p.j_max = v[3]; p.k_min = v[4]; p.k_max = v[5];
+    const std::vector<std::string> info = config_.parseList(p.name);
+    if (info.empty()) throw ConfigError("Boundary info for " + p.name + " is missing in configuration.");
+    p.type = boundaryTypeFromString(info[0]);
+    for (size_t q = 1; q < info.size(); q++) {
+        try {
+            p.values.push_back(std::stod(info[q]));
+        } catch (const std::exception&) {
+            throw ConfigError("Invalid float format for boundary value \"" + info[q] + "\" in configuration.");
+        }
+    }
+    if (p.i_min == p.i_max) p.orientation = p.i_min == 0 ? 0 : 1;
+    else if (p.j_min == p.j_max) p.orientation = p.j_min == 0 ? 2 : 3;
+    else p.orientation = p.k_min == 0 ? 4 : 5;
+    boundaries_.push_back(std::move(p));
 }
 
 // Solver::buildBoundaryDataStructures, buildBoundaryFluxes,

@@ -37,11 +37,36 @@ struct BoundaryPatch {
     std::unique_ptr<BoundaryBase> flux;
 };
 
+// One row of the boundary-conditions file (PATCH_NAME, I_MIN .. K_MAX).
+struct PatchRow {
+    std::string name;
+    long range[6] = {0, 0, 0, 0, 0, 0};  // i_min, i_max, j_min, j_max, k_min, k_max
+};
+
+// A case held in memory, owned: what input.ini, the grid CSV and
+// boundaries.csv carry.
+struct CaseData {
+    std::vector<std::pair<std::string, std::string>> settings;
+    std::string directory;  // where files that settings name resolve ("" = current directory)
+    long ni = 0, nj = 0, nk = 0;
+    std::vector<double> x, y, z;  // node (i, j, k) at (i*nj + j)*nk + k
+    std::vector<std::pair<std::string, std::vector<double>>> fields;
+    std::vector<PatchRow> patches;
+
+    std::unique_ptr<Mesh> mesh(const Config& config) const {
+        std::vector<std::pair<std::string, const double*>> f;
+        for (const auto& c : fields) f.emplace_back(c.first, c.second.data());
+        return std::make_unique<Mesh>(config, ni, nj, nk, x.data(), y.data(), z.data(), f);
+    }
+};
+
 enum Precision { kFP64 = 0, kFP32Kahan = 1 };
 
 class Solver {
 public:
-    Solver(Config& config, Mesh& mesh);
+    // The boundary patches come from the file BOUNDARY_CONDITIONS_FILEPATH
+    // names, or from `patches` when it is given (an in-memory case).
+    Solver(Config& config, Mesh& mesh, const std::vector<PatchRow>* patches = nullptr);
     ~Solver();
     Solver(const Solver&) = delete;
     Solver& operator=(const Solver&) = delete;
@@ -100,7 +125,8 @@ public:
     InstanceT<float>* instance32() { return i32_.get(); }
 
 private:
-    void readBoundaries();
+    void readBoundaries(const std::vector<PatchRow>* patches);
+    void addBoundary(const PatchRow& row);
     void buildBoundaryStructures();
     void setupScalars();
     void setupModels();

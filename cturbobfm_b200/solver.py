@@ -74,6 +74,68 @@ class Result(ctypes.Structure):
     ]
 
 
+class PatchDesc(ctypes.Structure):
+    """ctbfm_patch: one row of boundaries.csv."""
+
+    _fields_ = [("name", ctypes.c_char_p)] + [(f, ctypes.c_int64) for f in
+                                              ("i_min", "i_max", "j_min", "j_max", "k_min", "k_max")]
+
+
+class CaseDesc(ctypes.Structure):
+    """ctbfm_case_desc: settings, grid arrays and patches held in memory."""
+
+    _fields_ = [
+        ("ni", ctypes.c_int64),
+        ("nj", ctypes.c_int64),
+        ("nk", ctypes.c_int64),
+        ("x", ctypes.POINTER(ctypes.c_double)),
+        ("y", ctypes.POINTER(ctypes.c_double)),
+        ("z", ctypes.POINTER(ctypes.c_double)),
+        ("n_fields", ctypes.c_int32),
+        ("field_names", ctypes.POINTER(ctypes.c_char_p)),
+        ("fields", ctypes.POINTER(ctypes.POINTER(ctypes.c_double))),
+        ("n_patches", ctypes.c_int32),
+        ("patches", ctypes.POINTER(PatchDesc)),
+        ("n_settings", ctypes.c_int32),
+        ("keys", ctypes.POINTER(ctypes.c_char_p)),
+        ("values", ctypes.POINTER(ctypes.c_char_p)),
+        ("directory", ctypes.c_char_p),
+    ]
+
+
+def case_desc(case, directory: Optional[str] = None):
+    """The ctbfm_case_desc of a ``cases.Case`` (its settings, grid arrays and
+    patches, each patch's type and values under the patch's name as in
+    input.ini) and the objects that keep its buffers alive. Files the case
+    names (a fluid table, the Chima scaling functions) are written to
+    ``directory``, against which the settings that name files resolve."""
+    if case.table is not None or case.files:
+        if directory is None:
+            raise ValueError(f"case {case.name} names input files: pass a directory to write them to")
+        case.write_side_files(directory)
+    ni, nj, nk = case.shape
+    arrays = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (case.x, case.y, case.z)]
+    names = list(case.fields.keys())
+    cols = [np.ascontiguousarray(case.fields[n], dtype=np.float64).reshape(-1) for n in names]
+    settings = dict(case.settings)
+    for p in case.patches:
+        settings[p.name] = p.spec
+    keys = [k.encode() for k in settings]
+    vals = [str(v).encode() for v in settings.values()]
+    pats = (PatchDesc * max(len(case.patches), 1))()
+    pnames = [p.name.encode() for p in case.patches]
+    for q, p in enumerate(case.patches):
+        pats[q] = PatchDesc(pnames[q], p.i_min, p.i_max, p.j_min, p.j_max, p.k_min, p.k_max)
+    fname_arr = (ctypes.c_char_p * max(len(names), 1))(*[n.encode() for n in names])
+    col_arr = (ctypes.POINTER(ctypes.c_double) * max(len(cols), 1))(*[_ptr(c) for c in cols])
+    key_arr = (ctypes.c_char_p * max(len(keys), 1))(*keys)
+    val_arr = (ctypes.c_char_p * max(len(vals), 1))(*vals)
+    d = CaseDesc(ni, nj, nk, _ptr(arrays[0]), _ptr(arrays[1]), _ptr(arrays[2]), len(names), fname_arr, col_arr,
+                 len(case.patches), pats, len(keys), key_arr, val_arr,
+                 os.path.abspath(directory).encode() if directory else None)
+    return d, (arrays, cols, keys, vals, pnames, pats, fname_arr, col_arr, key_arr, val_arr)
+
+
 _lib = None
 
 # Every symbol include/ctbfm.h declares, with its ctypes signature.
@@ -82,6 +144,7 @@ _VP = ctypes.c_void_p
 _I64 = ctypes.c_int64
 SIGNATURES = {
     "ctbfm_create_from_ini": ([ctypes.c_char_p, ctypes.POINTER(_VP)], ctypes.c_int),
+    "ctbfm_create": ([ctypes.POINTER(CaseDesc), ctypes.POINTER(_VP)], ctypes.c_int),
     "ctbfm_destroy": ([_VP], None),
     "ctbfm_set_stream": ([_VP, _VP], ctypes.c_int),
     "ctbfm_get_info": ([_VP, ctypes.POINTER(Info)], ctypes.c_int),
@@ -112,6 +175,7 @@ SIGNATURES = {
                              ctypes.POINTER(_VP)], ctypes.c_int),
     "ctbfm_server_destroy": ([_VP], None),
     "ctbfm_server_submit": ([_VP, ctypes.c_char_p, ctypes.POINTER(_I64)], ctypes.c_int),
+    "ctbfm_server_submit_case": ([_VP, ctypes.POINTER(CaseDesc), ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_server_pump": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "ctbfm_server_results": ([_VP, ctypes.POINTER(Result), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
                              ctypes.c_int),
@@ -154,6 +218,23 @@ class Solver:
         lib = load_library()
         h = _VP()
         _check(lib.ctbfm_create_from_ini(os.path.abspath(ini_path).encode(), ctypes.byref(h)))
+        self._adopt(h)
+
+    @classmethod
+    def from_case(cls, case, directory: Optional[str] = None) -> "Solver":
+        """A solver built from a ``cases.Case`` held in memory (ctbfm_create):
+        no input.ini, grid or boundaries file is written. ``directory`` takes
+        the other files the case names and is where settings that name files
+        resolve."""
+        desc, keep = case_desc(case, directory)
+        h = _VP()
+        _check(load_library().ctbfm_create(ctypes.byref(desc), ctypes.byref(h)))
+        del keep
+        self = cls.__new__(cls)
+        self._adopt(h)
+        return self
+
+    def _adopt(self, h):
         self._h = h
         inf = self.info()
         self.shape = (int(inf.ni), int(inf.nj), int(inf.nk))
@@ -377,6 +458,14 @@ class Server:
     def submit(self, ini_path: str) -> int:
         rid = _I64(0)
         _check(load_library().ctbfm_server_submit(self._h, os.path.abspath(ini_path).encode(), ctypes.byref(rid)))
+        return int(rid.value)
+
+    def submit_case(self, case, directory: Optional[str] = None) -> int:
+        """Queues a ``cases.Case`` held in memory (ctbfm_server_submit_case)."""
+        desc, keep = case_desc(case, directory)
+        rid = _I64(0)
+        _check(load_library().ctbfm_server_submit_case(self._h, ctypes.byref(desc), ctypes.byref(rid)))
+        del keep
         return int(rid.value)
 
     def pump(self):

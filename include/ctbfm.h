@@ -9,6 +9,8 @@
  *   ctbfm_create_from_ini   Config(input.ini) + Mesh(config) + Solver(config, mesh)
  *                           (src/turbobfm.cpp:15-27, src/config.cpp:8-13,
  *                            src/mesh.cpp:11-40, src/solver.cpp:18-31)
+ *   ctbfm_create            Solver(Config&, Mesh&) (include/solver.hpp:49-53) with
+ *                           the settings, grid and patches given in memory
  *   ctbfm_solve             Solver::solve() explicit branch (src/solver.cpp:1296-1424)
  *   ctbfm_step              n iterations of that loop (src/solver.cpp:1337-1398),
  *                           never past N_ITERATIONS
@@ -84,6 +86,47 @@ typedef struct {
  * boundaries.csv it names resolve relative to the ini's directory) and uploads
  * everything to the current CUDA device. */
 int ctbfm_create_from_ini(const char* ini_path, ctbfm_solver** out);
+
+/* One boundary patch: a row of the reference's boundaries.csv
+ * (PATCH_NAME, I_MIN, I_MAX, J_MIN, J_MAX, K_MIN, K_MAX). Its type and values
+ * come from the setting of the same name, as in input.ini
+ * ("inlet" = "inlet, 101325, 288.15, 1, 0, 0"). */
+typedef struct {
+    const char* name;
+    int64_t i_min, i_max, j_min, j_max, k_min, k_max;
+} ctbfm_patch;
+
+/* A case held in memory: what input.ini, the grid CSV and boundaries.csv carry
+ * (the reference's Config, Mesh and boundary table, include/solver.hpp:49-53).
+ * Node (i, j, k) of every grid array is element (i*nj + j)*nk + k, the grid
+ * CSV's row order. ctbfm_create copies everything; the caller's arrays and
+ * strings may be released when it returns. */
+typedef struct {
+    int64_t ni, nj, nk;               /* nodes per direction (nk = 1 in 2-D) */
+    const double* x;                  /* ni*nj*nk node coordinates */
+    const double* y;
+    const double* z;
+    int32_t n_fields;                 /* further grid columns: blockage, normalAxial, ... */
+    const char* const* field_names;   /* n_fields column names, as in the grid CSV header */
+    const double* const* fields;      /* n_fields arrays of ni*nj*nk values */
+    int32_t n_patches;
+    const ctbfm_patch* patches;
+    int32_t n_settings;               /* input.ini settings as strings: keys[q] = values[q] */
+    const char* const* keys;
+    const char* const* values;
+    const char* directory;            /* where the files that settings still name resolve
+                                         (FLUID_TABLE_FILE, CHIMA_SCALING_FUNCTIONS_FILEPATH,
+                                         RESTART_SOLUTION_FILEPATH); NULL = the current directory.
+                                         GRID_FILE and BOUNDARY_CONDITIONS_FILEPATH are not read. */
+} ctbfm_case_desc;
+
+/* Builds a solver from a case held in memory (the same checks, results and
+ * errors as ctbfm_create_from_ini on the same values) and uploads everything to
+ * the current CUDA device. Returns CTBFM_E_ARGUMENT for a malformed
+ * description (null arrays, negative counts) and CTBFM_E_CONFIG for settings
+ * the ini path would reject. Replaces Solver(Config&, Mesh&)
+ * (include/solver.hpp:49-53) with the Config and Mesh built in memory. */
+int ctbfm_create(const ctbfm_case_desc* desc, ctbfm_solver** out);
 
 /* Releases device memory, graphs and streams owned by the solver. */
 void ctbfm_destroy(ctbfm_solver* s);
@@ -290,6 +333,11 @@ void ctbfm_server_destroy(ctbfm_server* s);
 
 /* Queues the operating point of an input.ini; thread safe. */
 int ctbfm_server_submit(ctbfm_server* s, const char* ini_path, int64_t* request_id);
+
+/* Queues the operating point of a case held in memory (copied before the call
+ * returns; see ctbfm_create); thread safe. A malformed description returns
+ * CTBFM_E_ARGUMENT here; invalid settings come back as the request's error. */
+int ctbfm_server_submit_case(ctbfm_server* s, const ctbfm_case_desc* desc, int64_t* request_id);
 
 /* One scheduling round on the calling thread (admit, advance every admitted
  * solve by chunk_iterations, retire, promote). n_active / n_waiting
