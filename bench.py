@@ -247,6 +247,8 @@ def algorithmic_bytes(case, kernel: str) -> float:
 
 SPLIT_STAGE = ("k_prim", "k_faces_I", "k_faces_J", "k_faces_K", "k_nodes", "k_periodic")
 FUSED_STAGE = ("k_stage", "k_periodic")
+STAGE_KERNEL_NAMES = {"split": "split (k_prim, k_faces, k_nodes)", "fused": "fused (k_stage)",
+                      "persistent": "persistent (k_run, 32 iterations per launch)"}
 
 
 def calls_per_iteration(case, kernel: str, fused: bool = False) -> int:
@@ -254,6 +256,8 @@ def calls_per_iteration(case, kernel: str, fused: bool = False) -> int:
     (its timing covers all launches of one call), for the fused or the split
     stage."""
     s = case.n_stages
+    if kernel == "k_prim":  # later stages read the primitives the node kernels store
+        return 0 if fused else 1
     if kernel in SPLIT_STAGE + FUSED_STAGE:
         return s if kernel in (FUSED_STAGE if fused else SPLIT_STAGE) else 0
     return {"k_dt": 1, "k_pre": 1, "k_finalize": 1, "k_bint": 0}.get(kernel, 0)
@@ -363,10 +367,9 @@ def run_ours(args):
             v32 = n * stages * args.steps / (ms32 / 1e3)
             b32 = stage_bytes_per_cell(case, 4)
             pk = measured_peaks().get("hbm_gbs", 6650.0)
-            inf32 = s32.info()
+            mode32, ms32_tuned = s32.stage_kernels()
             fp32 = {"value": v32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "status": s32.status,
-                    "stage_kernels": "fused (k_stage)" if inf32.fused_stage else "split (k_prim, k_faces, k_nodes)",
-                    "stage_autotuned_ms": {"split": inf32.tuned_stage_ms[0], "fused": inf32.tuned_stage_ms[1]},
+                    "stage_kernels": STAGE_KERNEL_NAMES[mode32], "stage_autotuned_ms": ms32_tuned,
                     "stage_roofline": {"bytes_per_cell_stage": b32, "achieved": v32 * b32 / 1e9, "peak": pk,
                                        "unit": "GB/s", "frac": v32 * b32 / 1e9 / pk},
                     "speedup_vs_fp64": ms_max / ms32,
@@ -393,7 +396,8 @@ def run_ours(args):
 
     # per-kernel device times (CUDA events on the launching stream)
     prof = solver.profile_kernels(reps=10)
-    fused = bool(solver.info().fused_stage)
+    mode, _ = solver.stage_kernels()
+    fused = mode == "fused"
     shares = {k: prof[k] * calls_per_iteration(case, k, fused) for k in prof}
     total = sum(shares.values()) or 1.0
     dominant = max(shares, key=shares.get)
@@ -402,7 +406,10 @@ def run_ours(args):
     alg = algorithmic_bytes(case, dominant)
     achieved = alg / (prof[dominant] / 1e3) / 1e9 if prof[dominant] > 0 else 0.0
     traffic = traffic_table().get(dominant)
-    launches = args.steps * (1 + sum(launches_per_iteration(case, k, fused) for k in prof if prof[k] > 0))
+    if mode == "persistent":  # k_set_limits and one k_run per 32 iterations
+        launches = 1 + -(-args.steps // 32)
+    else:
+        launches = args.steps * (1 + sum(launches_per_iteration(case, k, fused) for k in prof if prof[k] > 0))
     clk = clocks.summary()
 
     if world > 1:
@@ -420,7 +427,7 @@ def run_ours(args):
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "l2": f"inputs larger than L2: device working set {solver_bytes(solver, case) / 2**20:.0f} MiB > 126 MiB",
             "face_tiles_autotuned": list(solver.info().face_tile),
-            "stage_autotuned_ms": {"split": solver.info().tuned_stage_ms[0], "fused": solver.info().tuned_stage_ms[1]},
+            "stage_autotuned_ms": solver.stage_kernels()[1],
         },
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 5 * 8 * n,
@@ -466,10 +473,13 @@ MAP_WORKLOAD = ("compressor map: 256 axisymmetric BFM instances (Hall, MAP_ROWS 
                 "CFL 2.2, outlet ramp 2000 its, residual drop {drop} orders")
 
 
-def _map_launches_per_iteration(case, fused: bool) -> int:
-    # k_bint, k_dt, k_pre, per stage k_stage (fused) or k_prim + k_faces I +
-    # k_faces J + k_nodes (split), k_finalize
-    return 3 + (1 if fused else 4) * case.n_stages + 1
+def _map_launches_per_iteration(case, mode: str) -> float:
+    # k_bint, k_dt, k_pre, per stage k_stage (fused) or k_faces I + k_faces J +
+    # k_nodes (split; k_prim in stage 0 only), k_finalize; one k_run per 32
+    # iterations (persistent)
+    if mode == "persistent":
+        return 1.0 / 32
+    return 3 + (case.n_stages if mode == "fused" else 3 * case.n_stages + 1) + 1
 
 
 def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
@@ -492,16 +502,15 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
         with Batch([solvers[i] for i in active]) as b:
             b.set_stream(stream.cuda_stream)
             b.autotune()
-            fused, stage_ms = b.stage_kernels()
+            mode, stage_ms = b.stage_kernels()
             if first is None:
-                first = {"stage_kernels": "fused (k_stage)" if fused else "split (k_prim, k_faces, k_nodes)",
-                         "stage_autotuned_ms": {"split": stage_ms[0], "fused": stage_ms[1]}}
-            per_iteration = _map_launches_per_iteration(case, fused)
+                first = {"stage_kernels": STAGE_KERNEL_NAMES[mode], "stage_autotuned_ms": stage_ms}
+            per_iteration = _map_launches_per_iteration(case, mode)
             start = len(active)
             while True:
                 b.step(chunk)
                 st = b.status()
-                launches += chunk * per_iteration + 4  # + k_set_limits and three control gathers
+                launches += int(np.ceil(chunk * per_iteration)) + 4  # + k_set_limits and three control gathers
                 for j, i in enumerate(active):
                     status[i] = st["status"][j]
                     iters[i] = st["iterations"][j]
@@ -541,16 +550,15 @@ def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: 
         with Batch([solvers[i] for i in active]) as b:
             b.set_stream(stream.cuda_stream)
             b.autotune()
-            fused, stage_ms = b.stage_kernels()
+            mode, stage_ms = b.stage_kernels()
             if first is None:
-                first = {"stage_kernels": "fused (k_stage)" if fused else "split (k_prim, k_faces, k_nodes)",
-                         "stage_autotuned_ms": {"split": stage_ms[0], "fused": stage_ms[1]}}
-            per_iteration = _map_launches_per_iteration(case, fused)
+                first = {"stage_kernels": STAGE_KERNEL_NAMES[mode], "stage_autotuned_ms": stage_ms}
+            per_iteration = _map_launches_per_iteration(case, mode)
             start = len(active)
             while True:
                 b.step(chunk)
                 st = b.status()
-                launches += chunk * per_iteration + 4
+                launches += int(np.ceil(chunk * per_iteration)) + 4
                 for j, i in enumerate(active):
                     status[i] = st["status"][j]
                     iters[i] = st["iterations"][j]

@@ -2,10 +2,10 @@
 C++ layer (g++), linked with the static CUDA runtime.
 
 Flags that carry the numerical contract:
-  * double kernels (kernels.cu, noalloc.cu): ``--fmad=false`` (no
+  * double kernels (kernels.cu, kernels_persist.cu, noalloc.cu): ``--fmad=false`` (no
     multiply-add contraction; IEEE double division and square root are
     nvcc's defaults);
-  * float kernels (kernels_f32.cu): contraction allowed, approximate
+  * float kernels (kernels_f32.cu, kernels_persist_f32.cu): contraction allowed, approximate
     float division and square root, denormals flushed (the float path is
     a stated-tolerance path; its faces run 38 % faster than with IEEE
     division); the compensated (Kahan) state update has no product to
@@ -16,6 +16,7 @@ Flags that carry the numerical contract:
 
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -33,7 +34,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 # (source, float kernels: contraction and approximate division / square root)
-CU_SOURCES = [("device/kernels.cu", False), ("device/kernels_f32.cu", True), ("device/noalloc.cu", False)]
+CU_SOURCES = [("device/kernels.cu", False), ("device/kernels_f32.cu", True), ("device/kernels_persist.cu", False),
+              ("device/kernels_persist_f32.cu", True), ("device/noalloc.cu", False)]
 FAST_F32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 CPP_SOURCES = ["host/config.cpp", "host/mesh.cpp", "host/engine.cpp", "host/fluid_table.cpp", "host/restart.cpp",
                "host/output.cpp", "host/solver.cpp", "host/batch.cpp", "host/server.cpp", "capi.cpp"]
@@ -68,13 +70,18 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = _all_headers()
     objs = []
+    jobs = []
     for src, fmad in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, os.path.basename(src) + ".o")
         if force or _stale(o, [s] + headers):
-            _run([NVCC, *ARCH, "-lineinfo", "-O3", *(FAST_F32 if fmad else ["--fmad=false"]), "-std=c++17",
-                  "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3", "-c", s, "-o", o])
+            jobs.append([NVCC, *ARCH, "-lineinfo", "-O3", *(FAST_F32 if fmad else ["--fmad=false"]), "-std=c++17",
+                         "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3", "-c", s, "-o", o])
         objs.append(o)
+    # the device units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd) for cmd in jobs]:
+            f.result()
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, os.path.basename(src) + ".o")

@@ -64,6 +64,8 @@ int guarded(F&& f) {
 
 int statusCode(ctbfm_solver* s) {
     const ctbfm::Control c = s->solver->control();
+    if (c.status == 3)
+        return setError(CTBFM_E_CUDA, "device error: a grid barrier wait of the persistent kernel ran out");
     if (c.status == 2) {
         int var = 0;
         for (int v = 0; v < 5; v++)
@@ -186,7 +188,8 @@ int ctbfm_get_info(const ctbfm_solver* s, ctbfm_info* out) {
         out->device_bytes = static_cast<int64_t>(s->solver->deviceBytes());
         for (int d = 0; d < 3; d++) out->face_tile[d] = s->solver->faceTile(d);
         out->fused_stage = s->solver->fusedStage() ? 1 : 0;
-        for (int m = 0; m < 2; m++) out->tuned_stage_ms[m] = s->solver->tunedStageMs(m);
+        out->persistent_stage = s->solver->persistentStage() ? 1 : 0;
+        for (int m = 0; m < 3; m++) out->tuned_stage_ms[m] = s->solver->tunedStageMs(m);
         return CTBFM_OK;
     });
 }
@@ -364,11 +367,11 @@ int ctbfm_batch_autotune(ctbfm_batch* b) {
     });
 }
 
-int ctbfm_batch_stage_kernels(ctbfm_batch* b, int32_t* fused, double stage_ms[2]) {
-    if (!b || !fused || !stage_ms) return setError(CTBFM_E_ARGUMENT, "bad argument");
+int ctbfm_batch_stage_kernels(ctbfm_batch* b, int32_t* mode, double stage_ms[3]) {
+    if (!b || !mode || !stage_ms) return setError(CTBFM_E_ARGUMENT, "bad argument");
     return guarded([&] {
-        *fused = b->batch->fusedMode();
-        for (int m = 0; m < 2; m++) stage_ms[m] = b->batch->stageMs(m);
+        *mode = b->batch->persistent() ? 2 : b->batch->fusedMode();
+        for (int m = 0; m < 3; m++) stage_ms[m] = b->batch->stageMs(m);
         return CTBFM_OK;
     });
 }

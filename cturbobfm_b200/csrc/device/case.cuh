@@ -77,7 +77,7 @@ struct Control {
     long long it;       // iterations completed
     long long it_stop;  // kernels of iteration it+1 run only while it < it_stop
     long long hist_base;
-    int status;  // 0 running, 1 converged, 2 diverged
+    int status;  // 0 running, 1 converged, 2 diverged, 3 stopped by a device error (a grid barrier wait ran out)
     int has_init;
     int has_turbo;
     int pad;

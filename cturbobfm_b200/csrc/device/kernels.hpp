@@ -95,6 +95,37 @@ struct Launcher {
 extern template struct Launcher<double>;
 extern template struct Launcher<float>;
 
+// State of the persistent kernel's grid barrier (device memory, zeroed when
+// allocated; every launch leaves count at 0).
+struct GridSync {
+    unsigned count;  // blocks arrived at the current barrier
+    unsigned gen;    // barrier generation
+    int error;       // 1: a barrier wait ran out and the kernel stopped
+    int active[2];   // instances still running after a finalize phase (alternate iterations)
+    int pad;
+};
+
+// The persistent iteration kernel k_run (persist.cuh): one cooperative
+// launch runs whole iterations of a batch, its phases (time step, pre-stage,
+// and per stage faces, nodes, periodic planes, then finalize) separated by a
+// grid barrier instead of kernel boundaries. For batches of ideal-gas,
+// inviscid members without the SA model and with one advection scheme.
+template <typename R>
+struct Persistent {
+    // n iterations (fewer if every member stops); scheme 0 JST, 1 Roe
+    static cudaError_t run(const BatchView<R>& b, int scheme, int nstages, long long n, GridSync* gs,
+                           cudaStream_t s);
+    // `reps` forced stage-0 evaluations, as the autotuner times the other
+    // stage kernels
+    static cudaError_t tuneStage(const BatchView<R>& b, int scheme, int reps, GridSync* gs, cudaStream_t s);
+    // blocks of one launch for this batch (co-resident blocks, at most the
+    // largest phase's tiles)
+    static int gridBlocks(const BatchView<R>& b, int scheme);
+};
+
+extern template struct Persistent<double>;
+extern template struct Persistent<float>;
+
 constexpr int kKernelKinds = 11;
 constexpr int kTileSize = 256;  // elements per tile (one per thread)
 // fused stage kernel: nodes per box (one per thread) and the faces (all

@@ -375,10 +375,7 @@ __global__ void __launch_bounds__(256, 3) k_vfaces(const DevCaseT<R>* cases, con
 // n-1 and n (n = nj or nk, at least 3), the k index fastest where the line
 // is not along k, so that warps of one launch take one code path.
 template <int DIR, int SCHEME, typename R, int FL, int SET>
-__global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
+__device__ __forceinline__ void b_faces(const DevCaseT<R>& c, const Tile& tl, int stage) {
     const long long it = c.ctl->it + 1;
     const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const int nfj = c.nj + (DIR == 1), nfk = c.nk + (DIR == 2);
@@ -467,8 +464,9 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
             if (plain) {
                 if (SCHEME == 0) {
                     flux = fluxJstPR(gs, load5(U, qL - st), load5(U, qL), load5(U, qR), load5(U, qR + st),
-                                     load5(c.W, qL), load5(c.W, qR), __ldg(c.Wp + qL - st), __ldg(c.Wp + qL),
-                                     __ldg(c.Wp + qR), __ldg(c.Wp + qR + st), __ldg(c.Wr + qL), __ldg(c.Wr + qR), n);
+                                     load5(c.W, qL), load5(c.W, qR), CTBFM_LDS(c.Wp + qL - st), CTBFM_LDS(c.Wp + qL),
+                                     CTBFM_LDS(c.Wp + qR), CTBFM_LDS(c.Wp + qR + st), CTBFM_LDS(c.Wr + qL),
+                                     CTBFM_LDS(c.Wr + qR), n);
                 } else {
                     flux = fluxRoeW(gs, c.muscl, c.limiter, c.muscl ? load5(c.W, qL - st) : zero5<R>(),
                                     load5(c.W, qL), load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5<R>(), n);
@@ -502,26 +500,45 @@ __global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(co
     }
 }
 
+template <int DIR, int SCHEME, typename R, int FL, int SET>
+__global__ void __launch_bounds__(256, (facesMinBlocks<SCHEME, R>())) k_faces(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl, FL)) return;
+    b_faces<DIR, SCHEME, R, FL, SET>(c, tl, stage);
+}
+
 // Primitives of the stage input (getPrimitiveVariablesFromConservative,
 // src/math_utils.cpp:49-57), once per node for the face kernels; for JST
 // also each node's pressure and spectral radius |u| + a, which the JST flux
 // of every face reads at its four (pressure) and two (radius) stencil nodes
 // (the same values the flux computed per face before).
+// The node kernels of stages 0 .. nstages-2 store the primitives of the
+// state they write, which the next stage's faces read, so k_prim runs only
+// for stage 0 (and residual-only evaluations).
+template <typename R>
+__device__ __forceinline__ void storePrim(const DevCaseT<R>& c, long long q, const S5<R>& U) {
+    const Gas<R> gs{R(c.gamma), R(c.rgas), c.lut};
+    const S5<R> W = primOf(U);
+    store5(c.W, q, W);
+    if (c.Wp) {
+        c.Wp[q] = pressurePrim(gs, W);
+        c.Wr[q] = jstR(gs, W);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void b_prim(const DevCaseT<R>& c, const Tile& tl, int stage) {
+    R* const* U = stageIn(c, stage);
+    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) storePrim(c, q, load5(U, q));
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
     __shared__ DevCaseT<R> c;
     Tile tl;
     if (!enter(cases, tiles, c, stage, force, tl)) return;
-    R* const* U = stageIn(c, stage);
-    const Gas<R> gs{R(c.gamma), R(c.rgas), c.lut};
-    for (long long q = tl.start + threadIdx.x; q < tl.start + tl.count; q += blockDim.x) {
-        const S5<R> W = primOf(load5(U, q));
-        store5(c.W, q, W);
-        if (c.Wp) {
-            c.Wp[q] = pressurePrim(gs, W);
-            c.Wr[q] = jstR(gs, W);
-        }
-    }
+    b_prim<R>(c, tl, stage);
 }
 
 // ------------------------------------------------------------------ nodes
@@ -531,10 +548,7 @@ __global__ void __launch_bounds__(256) k_prim(const DevCaseT<R>* cases, const Ti
 // U(k) = U^n - R * (alpha*dt/V); with the compensated state the update is a
 // Kahan sum carrying the rounding error of U^n. stage -1 writes R to S2.
 template <typename R, int FL, int BX>
-__global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, stage, force, tl, FL, BX)) return;
+__device__ __forceinline__ void b_nodes(const DevCaseT<R>& c, const Tile& tl, int stage) {
     const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const double t = c.ctl->t;
     const R dtg = R(c.ctl->dt_min);
@@ -614,6 +628,7 @@ __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevC
             for (int v = 0; v < 5; v++) Un1.v[v] = Un.v[v] - Res.v[v] * fac;
         }
         store5(Uout, q, Un1);
+        if (stage < c.nstages - 1) storePrim(c, q, Un1);
         if (last)
 #pragma unroll
             for (int v = 0; v < 5; v++) acc[v] += static_cast<double>(Res.v[v]) * static_cast<double>(Res.v[v]);
@@ -626,15 +641,20 @@ __global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevC
     }
 }
 
+template <typename R, int FL, int BX>
+__global__ void __launch_bounds__(256, (nodesMinBlocks<R>())) k_nodes(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl, FL, BX)) return;
+    b_nodes<R, FL, BX>(c, tl, stage);
+}
+
 // Solver::enforcePeriodicityOnResiduals (src/solver.cpp:1836-1853), the
 // no-slip walls on the averaged residuals (:1856-1863), the update
 // of the two periodic planes and Solver::enforcePeriodicityOnSolution
 // (src/solver.cpp:2308-2327). One thread per (i, j) pair.
 template <typename R>
-__global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, stage, force, tl)) return;
+__device__ __forceinline__ void b_periodic(const DevCaseT<R>& c, const Tile& tl, int stage) {
     const R dtg = R(c.ctl->dt_min);
     const bool resOnly = stage < 0;
     const bool last = !resOnly && stage == c.nstages - 1;
@@ -685,8 +705,13 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
             U1 = load5(c.U, q1) - Rb * f1;
         }
         const S5<R> Ua = (U0 + rotState(U1, cm, sm)) * R(0.5);
+        const S5<R> Ub = rotState(Ua, cp, sp);
         store5(Uout, q0, Ua);
-        store5(Uout, q1, rotState(Ua, cp, sp));
+        store5(Uout, q1, Ub);
+        if (stage < c.nstages - 1) {
+            storePrim(c, q0, Ua);
+            storePrim(c, q1, Ub);
+        }
         if (last)
 #pragma unroll
             for (int v = 0; v < 5; v++)
@@ -701,6 +726,14 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
     }
 }
 
+template <typename R>
+__global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, const Tile* tiles, int stage, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, stage, force, tl)) return;
+    b_periodic<R>(c, tl, stage);
+}
+
 // ------------------------------------------------------------ fused stage
 #include "stage_fused.cuh"
 
@@ -712,10 +745,7 @@ __global__ void __launch_bounds__(256) k_periodic(const DevCaseT<R>* cases, cons
 // dt = CFL / (sum_d (|u . e_d| + a) / |e_d| + 4 nu sum_d 1 / |e_d|^2) over the
 // dual-node edges, the viscous term only for viscous instances.
 template <typename R, int FL>
-__global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile* tiles, int force) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, 0, force, tl, FL)) return;
+__device__ __forceinline__ void b_dt(const DevCaseT<R>& c, const Tile& tl) {
     if (c.dt_method == 2) return;
     const Gas<R> gs{R(c.gamma), R(c.rgas), FL ? c.lut : nullptr};
     const R cfl = R(c.cfl);
@@ -752,6 +782,14 @@ __global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile
     if (threadIdx.x == 0) c.partial[(c.node_tiles + c.per_tiles) * 5 + tl.local] = mn;
 }
 
+template <typename R, int FL>
+__global__ void __launch_bounds__(256) k_dt(const DevCaseT<R>* cases, const Tile* tiles, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl, FL)) return;
+    b_dt<R, FL>(c, tl);
+}
+
 // ------------------------------------------------------ boundary integrals
 // Solver::updateMassFlows (src/solver.cpp:1633-1649) and the mass-weighted
 // total pressure / temperature integrals of Solver::updateTurboPerformance
@@ -785,10 +823,7 @@ __device__ __forceinline__ int turboPlane(const DevCaseT<R>& c, int m) {
 }
 
 template <typename R, int FL>
-__global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Tile* tiles, int force) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, 0, force, tl, FL)) return;
+__device__ __forceinline__ void b_bint(const DevCaseT<R>& c, const Tile& tl) {
     const Gas<double> gs{c.gamma, c.rgas, FL ? c.lut : nullptr};
     const int blk = tl.local;
     const int plane = blk < 6 ? blk : turboPlane(c, blk - 6);
@@ -831,6 +866,14 @@ __global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Ti
     }
 }
 
+template <typename R, int FL>
+__global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Tile* tiles, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl, FL)) return;
+    b_bint<R, FL>(c, tl);
+}
+
 // ------------------------------------------------------------ pre-stage
 // Global min(dt); turbo performance with FluidIdeal::computeTotalEfficiency_PRtt_TRt
 // (src/fluid_ideal.cpp:179-191); GreitzerModel::computePlenumPressure
@@ -838,11 +881,8 @@ __global__ void __launch_bounds__(256) k_bint(const DevCaseT<R>* cases, const Ti
 // (src/solver.cpp:2688-2787) with integrateRadialEquilibrium
 // (src/math_utils.cpp:141-170). All double. One block per instance.
 template <typename R>
-__global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Tile* tiles, int forceTurbo, int dtpart,
-                                             int profiles, int force) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, 0, force, tl)) return;
+__device__ __forceinline__ void b_pre(const DevCaseT<R>& c, const Tile& tl, int forceTurbo, int dtpart,
+                                      int profiles) {
     Control* ctl = c.ctl;
     if (!dtpart) {
     } else if (c.dt_method == 2) {
@@ -957,6 +997,15 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
     }
 }
 
+template <typename R>
+__global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Tile* tiles, int forceTurbo, int dtpart,
+                                             int profiles, int force) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl)) return;
+    b_pre<R>(c, tl, forceTurbo, dtpart, profiles);
+}
+
 // ------------------------------------------------------------- finalize
 // Solver::computeLogResidualNorm (src/solver.cpp:1488-1508),
 // printInfoResiduals' initial maximum (src/solver.cpp:1426-1439),
@@ -965,11 +1014,7 @@ __global__ void __launch_bounds__(256) k_pre(const DevCaseT<R>* cases, const Til
 // fusedMode 1: instances that ran the fused stage kernel have their norm
 // partials in its region (one per box) instead of the node tiles'.
 template <typename R>
-__global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, const Tile* tiles, int force,
-                                                  int fusedMode) {
-    __shared__ DevCaseT<R> c;
-    Tile tl;
-    if (!enter(cases, tiles, c, 0, force, tl)) return;
+__device__ __forceinline__ void b_finalize(const DevCaseT<R>& c, const Tile& tl, int fusedMode) {
     Control* ctl = c.ctl;
     const bool fz = fusedMode && c.fuse_ok;
     const int na = fz ? c.nboxes : c.node_tiles;
@@ -1039,6 +1084,15 @@ __global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, cons
             }
         }
     }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_finalize(const DevCaseT<R>* cases, const Tile* tiles, int force,
+                                                  int fusedMode) {
+    __shared__ DevCaseT<R> c;
+    Tile tl;
+    if (!enter(cases, tiles, c, 0, force, tl)) return;
+    b_finalize<R>(c, tl, fusedMode);
 }
 
 // Copies every instance's control block into one array (one D2H copy for a
@@ -1268,7 +1322,8 @@ cudaError_t Launcher<R>::finalize(const BatchView<R>& b, int force, cudaStream_t
 
 template <typename R>
 cudaError_t Launcher<R>::stage(const BatchView<R>& b, int stage, int force, cudaStream_t s) {
-    cudaError_t e = prim(b, stage, force, s);
+    // later stages read the primitives the previous stage's node kernels stored
+    cudaError_t e = stage <= 0 ? prim(b, stage, force, s) : cudaSuccess;
     for (int d = 0; d < 3 && e == cudaSuccess; d++) e = faces(b, d, stage, force, s);
     if (e == cudaSuccess) e = viscous(b, stage, force, s);
     if (e == cudaSuccess) e = nodes(b, stage, force, s);

@@ -110,9 +110,20 @@ CTBFM_DI R rmin(R a, R b) {  // std::min
     return (b < a) ? b : a;
 }
 
+// Loads of arrays the loop rewrites (states, primitives): through the
+// read-only data path in kernels that never see them change while they run;
+// plain coherent loads in the persistent kernel, whose later phases read
+// what its earlier phases wrote (CTBFM_COHERENT_LOADS).
+#ifdef CTBFM_COHERENT_LOADS
+#define CTBFM_LDS(p) (*(p))
+#else
+#define CTBFM_LDS(p) __ldg(p)
+#endif
+
 template <typename R>
 CTBFM_DI S5<R> load5(R* const* U, long long q) {
-    return s5(__ldg(U[0] + q), __ldg(U[1] + q), __ldg(U[2] + q), __ldg(U[3] + q), __ldg(U[4] + q));
+    return s5(CTBFM_LDS(U[0] + q), CTBFM_LDS(U[1] + q), CTBFM_LDS(U[2] + q), CTBFM_LDS(U[3] + q),
+              CTBFM_LDS(U[4] + q));
 }
 template <typename R>
 CTBFM_DI void store5(R* const* U, long long q, const S5<R>& s) {

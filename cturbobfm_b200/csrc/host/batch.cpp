@@ -27,9 +27,13 @@ Batch::Batch(const std::vector<Solver*>& members) : members_(members) {
         g64_ = std::make_unique<GroupT<double>>(v);
     }
     // the split stage if a member asks for it, else the fused stage if a
-    // member asks for it, else autotuned
-    int fusion = 2;
-    for (Solver* m : members_) fusion = std::min(fusion, m->stageFusion() == 0 ? 0 : (m->stageFusion() == 1 ? 1 : 2));
+    // member asks for it, else the persistent kernel if a member asks for it
+    // (split if the batch cannot run it), else autotuned
+    static const int rank[4] = {0, 1, 3, 2};  // by GPU_STAGE_FUSION: split, fused, auto, persistent
+    static const int byRank[4] = {0, 1, 3, 2};
+    int r = 3;
+    for (Solver* m : members_) r = std::min(r, rank[m->stageFusion()]);
+    const int fusion = byRank[r];
     if (g32_) g32_->setFusedMode(fusion);
     else g64_->setFusedMode(fusion);
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -74,7 +78,10 @@ long long Batch::step(long long n) {
     enqueue(n);
     controls(after.data());
     long long most = 0;
-    for (size_t i = 0; i < members_.size(); i++) most = std::max(most, after[i].it - before[i].it);
+    for (size_t i = 0; i < members_.size(); i++) {
+        if (after[i].status == 3) throw CudaError("device error: a grid barrier wait of the persistent kernel ran out");
+        most = std::max(most, after[i].it - before[i].it);
+    }
     return most;
 }
 

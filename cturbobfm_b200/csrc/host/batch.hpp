@@ -34,6 +34,7 @@ public:
     // runs the group's autotuner now (face tiles, stage fusion) unless it has run
     void autotune();
     int fusedMode() const { return g32_ ? g32_->fusedMode() : g64_->fusedMode(); }
+    bool persistent() const { return g32_ ? g32_->persistent() : g64_->persistent(); }
     GroupTuning tuning() const { return g32_ ? g32_->tuning() : g64_->tuning(); }
     void adopt(const GroupTuning& t) {
         if (g32_) g32_->adopt(t);

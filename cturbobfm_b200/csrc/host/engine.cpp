@@ -73,6 +73,13 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     view_.sa = false;
     for (auto* m : members_) view_.sa = view_.sa || m->c.sa;
     view_.fusedMode = 1;
+    scheme_ = members_[0]->c.scheme;
+    persistOk_ = !view_.real && !view_.viscous && !view_.sa;
+    for (auto* m : members_) persistOk_ = persistOk_ && m->c.scheme == scheme_;
+    if (persistOk_) {
+        cudaCheck(cudaMalloc(&dSync_, sizeof(GridSync)), "cudaMalloc");
+        cudaCheck(cudaMemset(dSync_, 0, sizeof(GridSync)), "cudaMemset");
+    }
     refresh(nullptr);
     cudaCheck(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     cudaCheck(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -231,26 +238,26 @@ void GroupT<R>::tune(cudaStream_t s) {
     }
     view_.fusedMode = mode;
     buildTiles();
-    // stage fusion: forced stage-0 evaluations (they rewrite only the first
-    // stage buffer and the periodic residuals, which the next stage 0
-    // recomputes) with the split and with the fused stage kernels; the fused
-    // kernel is kept when at least 2 % faster
+    // stage kernels: forced stage-0 evaluations (they rewrite only the first
+    // stage buffer, the primitives and the periodic residuals, which the next
+    // stage 0 recomputes) with the split stage, the fused stage kernel and
+    // the persistent kernel, each as it runs; another than the split stage is
+    // kept when at least 2 % faster than the best so far
     bool anyFused = false;
     for (auto* m : members_) anyFused = anyFused || m->c.fuse_ok;
-    if (fusionAuto_ && anyFused) {
-        float ms[2] = {0.f, 0.f};
-        for (int mode2 = 0; mode2 < 2; mode2++) {
-            view_.fusedMode = mode2;
-            cudaCheck(Launcher<R>::stage(view_, 0, 1, s), "launch stage (tuning)");
-            cudaCheck(cudaEventRecord(e0, s), "cudaEventRecord");
-            for (int r = 0; r < 3; r++) cudaCheck(Launcher<R>::stage(view_, 0, 1, s), "launch stage (tuning)");
-            cudaCheck(cudaEventRecord(e1, s), "cudaEventRecord");
-            cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
-            cudaCheck(cudaEventElapsedTime(&ms[mode2], e0, e1), "cudaEventElapsedTime");
+    if (fusionAuto_ && (anyFused || persistOk_)) {
+        stageMs_[0] = timeStage(0, s, e0, e1);
+        stageMs_[1] = anyFused ? timeStage(1, s, e0, e1) : 0.f;
+        stageMs_[2] = persistOk_ ? timeStage(2, s, e0, e1) : 0.f;
+        int best = 0;
+        float bestMs = stageMs_[0];
+        if (anyFused && stageMs_[1] < 0.98f * bestMs) {
+            best = 1;
+            bestMs = stageMs_[1];
         }
-        stageMs_[0] = ms[0] / 3;
-        stageMs_[1] = ms[1] / 3;
-        view_.fusedMode = ms[1] < 0.98f * ms[0] ? 1 : 0;
+        if (persistOk_ && stageMs_[2] < 0.98f * bestMs) best = 2;
+        view_.fusedMode = best == 1 ? 1 : 0;
+        persist_ = best == 2;
         if (graph_) {
             cudaGraphExecDestroy(graph_);
             graph_ = nullptr;
@@ -262,6 +269,46 @@ void GroupT<R>::tune(cudaStream_t s) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+// Time of one forced stage-0 evaluation in stage mode `mode` (0 split,
+// 1 fused, 2 persistent) as it runs in the loop: the split and fused stages
+// from a captured graph of `reps` evaluations, the persistent kernel as a
+// k_run of `reps` evaluations; each timed after one untimed run.
+template <typename R>
+float GroupT<R>::timeStage(int mode, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    constexpr int reps = 4;
+    struct ExecGuard {
+        cudaGraphExec_t g = nullptr;
+        ~ExecGuard() {
+            if (g) cudaGraphExecDestroy(g);
+        }
+    } exec;
+    view_.fusedMode = mode == 1 ? 1 : 0;
+    if (mode < 2) {
+        cudaGraph_t g = nullptr;
+        cudaCheck(cudaStreamBeginCapture(captureStream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        cudaError_t e = cudaSuccess;
+        for (int r = 0; r < reps && e == cudaSuccess; r++) e = Launcher<R>::stage(view_, 0, 1, captureStream_);
+        const cudaError_t e2 = cudaStreamEndCapture(captureStream_, &g);
+        cudaCheck(e, "launch stage (tuning)");
+        cudaCheck(e2, "cudaStreamEndCapture");
+        const cudaError_t e3 = cudaGraphInstantiate(&exec.g, g, 0);
+        cudaGraphDestroy(g);
+        cudaCheck(e3, "cudaGraphInstantiate");
+    }
+    auto run = [&] {
+        if (mode < 2) cudaCheck(cudaGraphLaunch(exec.g, s), "cudaGraphLaunch");
+        else cudaCheck(Persistent<R>::tuneStage(view_, scheme_, reps, dSync_, s), "launch k_run (tuning)");
+    };
+    run();
+    cudaCheck(cudaEventRecord(e0, s), "cudaEventRecord");
+    run();
+    cudaCheck(cudaEventRecord(e1, s), "cudaEventRecord");
+    cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    float ms = 0.f;
+    cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+    return ms / reps;
 }
 
 template <typename R>
@@ -277,8 +324,8 @@ GroupTuning GroupT<R>::tuning() const {
     t.valid = selfTuned_;
     for (int d = 0; d < 3; d++) t.faceTile[d] = faceTile_[d];
     t.fusedMode = view_.fusedMode;
-    t.stageMs[0] = stageMs_[0];
-    t.stageMs[1] = stageMs_[1];
+    t.persistent = persist_;
+    for (int k = 0; k < 3; k++) t.stageMs[k] = stageMs_[k];
     t.nodes = nodes();
     return t;
 }
@@ -287,19 +334,23 @@ template <typename R>
 void GroupT<R>::adopt(const GroupTuning& t) {
     if (!t.valid) return;
     for (int d = 0; d < 3; d++) faceTile_[d] = t.faceTile[d];
-    stageMs_[0] = t.stageMs[0];
-    stageMs_[1] = t.stageMs[1];
+    for (int k = 0; k < 3; k++) stageMs_[k] = t.stageMs[k];
     buildTiles();  // also drops captured graphs
-    if (fusionAuto_) view_.fusedMode = t.fusedMode;
+    if (fusionAuto_) {
+        view_.fusedMode = t.fusedMode;
+        persist_ = t.persistent && persistOk_;
+    }
     tuned_ = true;
 }
 
 template <typename R>
 void GroupT<R>::setFusedMode(int mode) {
     fusionAuto_ = mode == 2;
-    if (mode == 2) mode = sizeof(R) == sizeof(float) ? 1 : 0;  // until the autotuner has timed both
-    if ((mode != 0) == (view_.fusedMode != 0)) return;
-    view_.fusedMode = mode != 0 ? 1 : 0;
+    if (mode == 2) mode = sizeof(R) == sizeof(float) ? 1 : 0;  // until the autotuner has timed them
+    persist_ = mode == 3 && persistOk_;
+    const int fused = mode == 1 ? 1 : 0;
+    if (fused == view_.fusedMode) return;
+    view_.fusedMode = fused;
     if (graph_) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
@@ -320,6 +371,7 @@ GroupT<R>::~GroupT() {
     }
     cudaFree(dCases_);
     cudaFree(dTiles_);
+    cudaFree(dSync_);
 }
 
 // One pageable host-to-device copy per member, ordered on s: each call returns
@@ -355,6 +407,12 @@ void GroupT<R>::enqueue(long long n, cudaStream_t s) {
     if (n <= 0) return;
     if (!tuned_ && autotune_ && n >= kTuneMinIterations) tune(s);
     cudaCheck(Launcher<R>::setLimits(view_, n, s), "launch k_set_limits");
+    if (persist_) {
+        for (long long left = n; left > 0; left -= kRunIterations)
+            cudaCheck(Persistent<R>::run(view_, scheme_, nstages_, std::min(left, kRunIterations), dSync_, s),
+                      "launch k_run");
+        return;
+    }
     long long left = n;
     if (left >= graphIters_) {
         if (!graph_) graph_ = captureIterations(graphIters_);

@@ -54,7 +54,8 @@ struct GroupTuning {
     bool valid = false;
     int faceTile[3] = {kTileSize, kTileSize, kTileSize};
     int fusedMode = 0;
-    float stageMs[2] = {0.f, 0.f};
+    bool persistent = false;
+    float stageMs[3] = {0.f, 0.f, 0.f};
     long long nodes = 0;
 };
 
@@ -80,15 +81,22 @@ public:
     void tune(cudaStream_t s);
     void setAutotune(bool on) { autotune_ = on; }
     // Stage kernels: 0 the split stage for every member, 1 the fused stage
-    // kernel for the members that can run it (the others split), 2 chosen by
-    // the autotuner (until it has run: fused in float, split in double, the
-    // faster ones on the workloads measured). FP64 results are the same
-    // either way; the captured graphs are rebuilt.
+    // kernel for the members that can run it (the others split), 3 the
+    // persistent iteration kernel k_run (split when the group cannot run it),
+    // 2 chosen by the autotuner (until it has run: fused in float, split in
+    // double, the faster ones on the workloads measured). FP64 results are
+    // the same either way; the captured graphs are rebuilt.
     void setFusedMode(int mode);
     bool tuned() const { return tuned_; }
     int fusedMode() const { return view_.fusedMode; }
+    // iterations run as k_run launches
+    bool persistent() const { return persist_; }
+    // every member can run in k_run: ideal gas, inviscid, no SA model, one
+    // advection scheme
+    bool persistentOk() const { return persistOk_; }
     int faceTile(int d) const { return faceTile_[d]; }
-    // the autotuner's stage timings (ms per stage: split, fused; 0 untimed)
+    // the autotuner's stage timings (ms per stage: split, fused, persistent;
+    // 0 untimed)
     float stageMs(int mode) const { return stageMs_[mode]; }
     long long nodes() const;
     // the autotuner's choices (valid once this group's own autotuner has run)
@@ -112,7 +120,16 @@ private:
     cudaGraphExec_t graph1_ = nullptr;  // one iteration
     int graphIters_ = 8;
     int faceTile_[3] = {kTileSize, kTileSize, kTileSize};
-    float stageMs_[2] = {0.f, 0.f};
+    float stageMs_[3] = {0.f, 0.f, 0.f};
+    bool persistOk_ = false;
+    bool persist_ = false;
+    int scheme_ = 0;
+    GridSync* dSync_ = nullptr;
+    // iterations per k_run launch: keeps a launch short (a few to tens of
+    // milliseconds), so that a cooperative launch waiting for room next to
+    // another group's kernels never waits long
+    static constexpr long long kRunIterations = 32;
+    float timeStage(int mode, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1);
     bool tuned_ = false;
     bool autotune_ = true;
     bool fusionAuto_ = false;

@@ -119,6 +119,10 @@ void Server::retire(std::unique_ptr<Job> job, const Control* ctl, int error, con
     r.message = msg;
     if (job->solver && ctl) {
         r.status = ctl->status;
+        if (ctl->status == 3 && !r.error) {
+            r.error = 2;  // CTBFM_E_CUDA
+            r.message = "device error: a grid barrier wait of the persistent kernel ran out";
+        }
         r.iterations = ctl->it;
         r.precision = job->solver->precision();
         try {

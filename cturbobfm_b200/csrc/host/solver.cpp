@@ -142,11 +142,18 @@ Solver::Solver(Config& config, Mesh& mesh, const std::vector<PatchRow>* patches)
     // ("fused"), the split stage kernels ("split") or the faster of the two
     // as the autotuner measures them ("auto", the default); FP64 results are
     // the same either way
+    // ("fused"), the split stage kernels ("split"), the persistent iteration
+    // kernel ("persistent": one cooperative launch per 32 iterations, for
+    // ideal-gas inviscid cases without the SA model) or the fastest of them
+    // as the autotuner measures them ("auto")
     const std::string fusion = config.has("GPU_STAGE_FUSION") ? config.get("GPU_STAGE_FUSION") : "auto";
     if (fusion == "fused") fusion_ = 1;
     else if (fusion == "split") fusion_ = 0;
     else if (fusion == "auto") fusion_ = 2;
-    else throw ConfigError("Invalid value for key \"GPU_STAGE_FUSION\" (auto, fused or split)");
+    else if (fusion == "persistent") fusion_ = 3;
+    else throw ConfigError("Invalid value for key \"GPU_STAGE_FUSION\" (auto, fused, split or persistent)");
+    if (fusion_ == 3 && (table_ || config.isViscosityActive() || config.parseBool("TURBULENCE_ACTIVE", false)))
+        throw ConfigError("GPU_STAGE_FUSION = persistent runs ideal-gas inviscid cases without a turbulence model");
     coeffs_ = config.getTimeIntegrationCoeffs();
     maxIter_ = config.getMaxIterations();
     // every setting and input file is validated before the first CUDA call,

@@ -77,7 +77,10 @@ public:
     int stageFusion() const { return fusion_; }
     bool realGas() const { return table_ != nullptr; }
     int faceTile(int d) const { return g64_ ? g64_->faceTile(d) : g32_->faceTile(d); }
+    // the autotuner's time of one stage: 0 split, 1 fused, 2 persistent
     double tunedStageMs(int mode) const { return g64_ ? g64_->stageMs(mode) : g32_->stageMs(mode); }
+    // iterations run in the persistent kernel k_run
+    bool persistentStage() const { return g64_ ? g64_->persistent() : g32_->persistent(); }
     // the group runs the fused stage kernel and this instance can run it
     bool fusedStage() const {
         return g64_ ? (g64_->fusedMode() && i64_->c.fuse_ok) : (g32_->fusedMode() && i32_->c.fuse_ok);

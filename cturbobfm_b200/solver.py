@@ -25,7 +25,8 @@ CTBFM_E_DIVERGED = 3
 CTBFM_E_ARGUMENT = 4
 CTBFM_E_UNSUPPORTED = 5
 
-STATUS_RUNNING, STATUS_CONVERGED, STATUS_DIVERGED = 0, 1, 2
+STATUS_RUNNING, STATUS_CONVERGED, STATUS_DIVERGED, STATUS_DEVICE_ERROR = 0, 1, 2, 3
+STAGE_MODES = ("split", "fused", "persistent")
 PRECISION_FP64, PRECISION_FP32_KAHAN = 0, 1
 
 
@@ -54,7 +55,8 @@ class Info(ctypes.Structure):
         ("device_bytes", ctypes.c_int64),
         ("face_tile", ctypes.c_int32 * 3),
         ("fused_stage", ctypes.c_int32),
-        ("tuned_stage_ms", ctypes.c_double * 2),
+        ("persistent_stage", ctypes.c_int32),
+        ("tuned_stage_ms", ctypes.c_double * 3),
     ]
 
 
@@ -258,6 +260,12 @@ class Solver:
         except Exception:
             pass
 
+    def stage_kernels(self):
+        """(mode, {mode: ms}) as Batch.stage_kernels, from ctbfm_get_info."""
+        inf = self.info()
+        mode = "persistent" if inf.persistent_stage else ("fused" if inf.fused_stage else "split")
+        return mode, {k: float(v) for k, v in zip(STAGE_MODES, inf.tuned_stage_ms)}
+
     def promote_fp64(self):
         """Continues a fp32_kahan solve in FP64 (no-op for FP64 solvers)."""
         _check(load_library().ctbfm_promote_fp64(self._h))
@@ -405,12 +413,13 @@ class Batch:
         _check(load_library().ctbfm_batch_autotune(self._h))
 
     def stage_kernels(self):
-        """(fused, (split ms, fused ms)): the batch's stage kernels and the
-        autotuner's stage timings (ctbfm_batch_stage_kernels)."""
+        """(mode, {mode: ms}): the batch's stage kernels ("split", "fused" or
+        "persistent") and the autotuner's time of one stage in each (0: not
+        timed) (ctbfm_batch_stage_kernels)."""
         f = ctypes.c_int32(0)
-        ms = np.zeros(2)
+        ms = np.zeros(3)
         _check(load_library().ctbfm_batch_stage_kernels(self._h, ctypes.byref(f), _ptr(ms)))
-        return bool(f.value), (float(ms[0]), float(ms[1]))
+        return STAGE_MODES[f.value], {k: float(v) for k, v in zip(STAGE_MODES, ms)}
 
     def step(self, n_iter: int) -> int:
         done = _I64(0)

@@ -63,7 +63,9 @@ enum {
 enum {
     CTBFM_STATUS_RUNNING = 0,
     CTBFM_STATUS_CONVERGED = 1,
-    CTBFM_STATUS_DIVERGED = 2
+    CTBFM_STATUS_DIVERGED = 2,
+    CTBFM_STATUS_DEVICE_ERROR = 3  /* stopped by a device error: a grid barrier wait of the
+                                      persistent kernel ran out (reported as CTBFM_E_CUDA) */
 };
 
 typedef struct {
@@ -79,7 +81,11 @@ typedef struct {
     int32_t face_tile[3];     /* faces per block chosen by the autotuner per direction (I, J, K) */
     int32_t fused_stage;      /* 1: each Runge-Kutta stage runs as the fused kernel k_stage;
                                  0: as the split kernels k_prim, k_faces, k_nodes */
-    double tuned_stage_ms[2]; /* the autotuner's time of one stage, split and fused (0: not timed) */
+    int32_t persistent_stage; /* 1: whole iterations run in the persistent kernel k_run (one
+                                 cooperative launch per 32 iterations, phases separated by a
+                                 grid barrier) */
+    double tuned_stage_ms[3]; /* the autotuner's time of one stage: split, fused, persistent
+                                 (0: not timed) */
 } ctbfm_info;
 
 /* Builds a solver from an input.ini in the reference's format (the grid CSV and
@@ -265,11 +271,12 @@ int ctbfm_batch_enqueue(ctbfm_batch* b, int64_t n_iter);
 /* ctbfm_autotune for the batch's group. */
 int ctbfm_batch_autotune(ctbfm_batch* b);
 
-/* The batch's stage kernels: *fused = 1 when its members that can run the
- * fused stage kernel k_stage do, and the autotuner's time of one stage of the
- * whole batch with the split and with the fused kernels (0 when not timed).
- * No counterpart in the reference. */
-int ctbfm_batch_stage_kernels(ctbfm_batch* b, int32_t* fused, double stage_ms[2]);
+/* The batch's stage kernels: *mode = 0 the split kernels, 1 the fused stage
+ * kernel k_stage (for the members that can run it), 2 the persistent kernel
+ * k_run; and the autotuner's time of one stage of the whole batch in each
+ * (split, fused, persistent; 0 when not timed). No counterpart in the
+ * reference. */
+int ctbfm_batch_stage_kernels(ctbfm_batch* b, int32_t* mode, double stage_ms[3]);
 
 /* enqueue + synchronise. *n_done (nullable) receives the most iterations any
  * member advanced. A diverged member is reported through

@@ -155,6 +155,8 @@ def _viscous_bump(walls="no_slip_wall, 0, 0, 0", **settings):
      "Missing constant viscosity value"),
     ("no_slip_wall", {}, "needs the wall velocity"),
     ("no_slip_wall, 10, 0, 0", {}, "moving walls"),
+    ("no_slip_wall, 0, 0, 0", {"GPU_STAGE_FUSION": "persistent"},
+     "GPU_STAGE_FUSION = persistent runs ideal-gas inviscid cases"),
 ])
 def test_viscous_settings_are_checked_before_device_work(lib, tmp_path, walls, settings, message):
     """Viscous runs: the transport keys and the no-slip walls are read with
