@@ -498,11 +498,15 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
     active = list(range(m))
     launches = 0
     first = None
+    batches = []
     while active:
+        t_set = time.perf_counter()
         with Batch([solvers[i] for i in active]) as b:
             b.set_stream(stream.cuda_stream)
             b.autotune()
             mode, stage_ms = b.stage_kernels()
+            batches.append({"members": len(active), "stage_kernels": mode,
+                            "setup_s": round(time.perf_counter() - t_set, 4)})
             if first is None:
                 first = {"stage_kernels": STAGE_KERNEL_NAMES[mode], "stage_autotuned_ms": stage_ms}
             per_iteration = _map_launches_per_iteration(case, mode)
@@ -518,6 +522,7 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
                 if len(done) * 4 >= start or len(done) == len(active):
                     break
         active = [i for i in active if not (status[i] != 0 or iters[i] >= n_iter)]
+    first["batches"] = batches
     return status, iters, launches, first
 
 
@@ -544,13 +549,17 @@ def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: 
     ready = np.zeros(m, bool)
     launches = 0
     first = None
+    batches = []
     active = list(range(m))
     # phase A: float
     while active:
+        t_set = time.perf_counter()
         with Batch([solvers[i] for i in active]) as b:
             b.set_stream(stream.cuda_stream)
             b.autotune()
             mode, stage_ms = b.stage_kernels()
+            batches.append({"members": len(active), "stage_kernels": mode,
+                            "setup_s": round(time.perf_counter() - t_set, 4)})
             if first is None:
                 first = {"stage_kernels": STAGE_KERNEL_NAMES[mode], "stage_autotuned_ms": stage_ms}
             per_iteration = _map_launches_per_iteration(case, mode)
@@ -574,15 +583,55 @@ def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: 
     # phase B: FP64 to convergence
     promote = [i for i in range(m) if status[i] == 0 and iters[i] < n_iter]
     it_a = iters.copy()
+    t_pro = time.perf_counter()
     for i in promote:
         solvers[i].promote_fp64()
+    first["promote_s"] = round(time.perf_counter() - t_pro, 3)
+    first["batches"] = batches
     if promote:
-        s_b, i_b, l_b, _ = _solve_batched([solvers[i] for i in promote], stream, chunk, n_iter, case)
+        s_b, i_b, l_b, kb = _solve_batched([solvers[i] for i in promote], stream, chunk, n_iter, case)
         for j, i in enumerate(promote):
             status[i], iters[i] = s_b[j], i_b[j]
         launches += l_b
+        first["batches_fp64"] = kb["batches"]
     fp64_iters = int(sum(iters[i] - it_a[i] for i in promote))
     return status, iters, launches, first, len(promote), fp64_iters
+
+
+def _serve_map(cases32, chunk: int, stall: int, host_threads: int = 8):
+    """The precision pattern through the serving API: every instance
+    submitted from memory (ctbfm_server_submit_case) at once to a Server
+    that prepares them on host threads, admits them as they are ready, runs
+    the fp32_kahan solves and the solves it moved to FP64 (within one order
+    of the residual drop, or stalled for `stall` iterations) as two batches
+    on two streams that overlap on the device, and retires each at
+    convergence. Wall time from the first submission to the last result,
+    host preparation and device set-up included."""
+    import numpy as np
+
+    from cturbobfm_b200 import Server
+
+    w0 = time.perf_counter()
+    res = {}
+    with Server(chunk=chunk, stall_window=stall, host_threads=host_threads, promote_orders=1.0) as srv:
+        ids = [srv.submit_case(c) for c in cases32]
+        while len(res) < len(ids) and time.perf_counter() - w0 < 1200:
+            active, _ = srv.pump()
+            for r in srv.results():
+                res[r["id"]] = r
+            if not active:
+                time.sleep(0.001)
+        stats = srv.stats()
+    sec = time.perf_counter() - w0
+    rs = [res.get(i) for i in ids]
+    status = np.array([r["status"] if r else -1 for r in rs])
+    turbo = np.array([r["turbo"] if r else [np.nan] * 4 for r in rs])
+    iters = np.array([r["iterations"] if r else 0 for r in rs])
+    conv = int((status == 1).sum())
+    return {"seconds": sec, "converged": conv, "diverged": int((status == 2).sum()),
+            "points_per_hour": conv / sec * 3600.0, "status": status, "turbo": turbo, "iterations": iters,
+            "errors": int(sum(1 for r in rs if r is None or r["error"])),
+            "server_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in stats.items()}}
 
 
 def map_cpu_baseline(inis, iterations, n_iter: int):
@@ -695,6 +744,8 @@ def map_line(args):
                             "node_stage_per_s": float((nodes * iters).sum() * 4 / sec), "launches": launches,
                             "device_bytes": bytes_up, "promoted_to_fp64": promoted,
                             "fp64_iteration_share": fp64_iters / max(1, int(iters.sum())), **kern}
+        if not args.map_skip_served:
+            results["served_fp32_kahan"] = _serve_map(cs32, args.map_chunk, args.map_stall)
         # the plain FP64 path: one drop-in solver at a time, to convergence
         sample = list(range(min(args.map_plain, len(inis64))))
         plain_sec, plain_conv, plain = 0.0, 0, []
@@ -738,7 +789,8 @@ def map_line(args):
         "batched_fp32_kahan": {k: r32[k] for k in ("seconds", "setup_seconds", "converged", "diverged",
                                                    "points_per_hour", "node_stage_per_s", "stage_kernels",
                                                    "stage_autotuned_ms", "promoted_to_fp64",
-                                                   "fp64_iteration_share")},
+                                                   "fp64_iteration_share", "promote_s", "batches",
+                                                   "batches_fp64") if k in r32},
         "precision_pattern": ("fp32_kahan for every instance until it is within one order of the residual drop or "
                               f"stalls for {args.map_stall} iterations, then the same solve continued in FP64 from "
                               "its current state to convergence (FP64 convergence test and converged state)"),
@@ -752,6 +804,23 @@ def map_line(args):
         "iterations_fp32": {"min": int(min(r32["iterations"])), "median": float(np.median(r32["iterations"])),
                             "max": int(max(r32["iterations"]))},
     }
+    if "served_fp32_kahan" in results:
+        rs = results["served_fp32_kahan"]
+        line["served_fp32_kahan"] = {k: rs[k] for k in ("seconds", "converged", "diverged", "points_per_hour",
+                                                         "errors", "server_stats")}
+        line["served_fp32_kahan"]["how"] = ("ctbfm_server_submit_case of all instances at t = 0, chunk "
+                                            f"{args.map_chunk}, float and FP64 batches on two streams; wall "
+                                            "time from the first submission to the last result")
+        line["served_fp32_kahan"]["speedup_vs_plain_fp64"] = rs["points_per_hour"] / plain_pph if plain_pph else None
+        if "batched_fp64" in results:
+            r64 = results["batched_fp64"]
+            both = (rs["status"] == 1) & (r64["status"] == 1)
+            if both.any():
+                emf = np.abs(rs["turbo"][both, 0] - r64["turbo"][both, 0]) / np.abs(r64["turbo"][both, 0])
+                epr = np.abs(rs["turbo"][both, 1] - r64["turbo"][both, 1]) / np.abs(r64["turbo"][both, 1])
+                line["served_fp32_kahan"]["vs_batched_fp64_rel_err"] = {
+                    "massflow_max": float(emf.max()), "pr_tt_max": float(epr.max()),
+                    "above_1e-4": int(((emf > 1e-4) | (epr > 1e-4)).sum()), "instances": int(both.sum())}
     if "batched_fp32_only" in results:
         r = results["batched_fp32_only"]
         line["batched_fp32_only"] = {k: r[k] for k in ("seconds", "converged", "diverged", "points_per_hour",
@@ -1060,6 +1129,8 @@ def main():
     ap.add_argument("--map-chunk", type=int, default=250)
     ap.add_argument("--map-plain", type=int, default=8, help="instances solved one at a time on the plain FP64 path")
     ap.add_argument("--map-skip-fp64-batch", action="store_true")
+    ap.add_argument("--map-skip-served", action="store_true",
+                    help="leave out the map run through the serving API")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[5.0, 20.0, 80.0])
     ap.add_argument("--serve-n", type=int, default=48)
     ap.add_argument("--serve-chunk", type=int, default=100)

@@ -428,6 +428,31 @@ int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_
     });
 }
 
+int ctbfm_server_set_promotion(ctbfm_server* s, double orders) {
+    if (!s || !(orders >= 0.0)) return setError(CTBFM_E_ARGUMENT, "bad argument");
+    return guarded([&] {
+        s->server->setPromoteOrders(orders);
+        return CTBFM_OK;
+    });
+}
+
+int ctbfm_server_get_stats(ctbfm_server* s, ctbfm_server_stats* out) {
+    if (!s || !out) return setError(CTBFM_E_ARGUMENT, "null argument");
+    return guarded([&] {
+        const ctbfm::ServerStats& st = s->server->stats();
+        out->rounds = st.rounds;
+        out->rebuilds = st.rebuilds;
+        out->promotions = st.promotions;
+        out->reruns = st.reruns;
+        out->wait_s = st.wait_s;
+        out->process_s = st.process_s;
+        out->rebuild_s = st.rebuild_s;
+        out->enqueue_s = st.enqueue_s;
+        out->admit_s = st.admit_s;
+        return CTBFM_OK;
+    });
+}
+
 void ctbfm_server_destroy(ctbfm_server* s) {
     if (!s) return;
     try {

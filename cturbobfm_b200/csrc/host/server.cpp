@@ -110,31 +110,37 @@ size_t Server::estimate(const Job& j) const {
     return static_cast<size_t>(per * static_cast<double>(j.nodes) * 1.05) + (size_t(1) << 20);
 }
 
-void Server::retire(std::unique_ptr<Job> job, const Control* ctl, int error, const std::string& msg) {
+// The result of a request, reported now; the job itself stays as it is.
+void Server::report(Job& job, const Control* ctl, int error, const std::string& msg) {
     ServerResult r;
-    r.id = job->id;
-    r.t_submit = job->t_submit;
-    r.t_admit = job->t_admit;
+    r.id = job.id;
+    r.t_submit = job.t_submit;
+    r.t_admit = job.t_admit;
     r.error = error;
     r.message = msg;
-    if (job->solver && ctl) {
+    if (job.solver && ctl) {
         r.status = ctl->status;
         if (ctl->status == 3 && !r.error) {
             r.error = 2;  // CTBFM_E_CUDA
             r.message = "device error: a grid barrier wait of the persistent kernel ran out";
         }
         r.iterations = ctl->it;
-        r.precision = job->solver->precision();
+        r.precision = job.solver->precision();
         try {
-            job->solver->getTurbo(r.massflow, r.turbo);
+            job.solver->getTurbo(r.massflow, r.turbo);
         } catch (const std::exception& e) {
             r.error = 2;  // CTBFM_E_CUDA
             r.message = e.what();
         }
     }
-    job.reset();  // releases the solve's device memory
     r.t_done = now();
     done_.push_back(std::move(r));
+}
+
+// Reports and releases a job that no batch refers to.
+void Server::retire(std::unique_ptr<Job> job, const Control* ctl, int error, const std::string& msg) {
+    report(*job, ctl, error, msg);
+    job.reset();  // releases the solve's device memory
 }
 
 void Server::rebuild() {
@@ -164,7 +170,6 @@ void Server::rebuild() {
     };
     if (!m32.empty()) b32_ = build(m32, 1);
     if (!m64.empty()) b64_ = build(m64, 0);
-    dirty_ = false;
 }
 
 // Admission in arrival order while slots, device memory and the node limit
@@ -228,7 +233,6 @@ void Server::joinPending() {
         active_.push_back(std::move(j));
     }
     pending_.clear();
-    dirty_ = true;
 }
 
 std::vector<Control> Server::gather() {
@@ -247,108 +251,155 @@ std::vector<Control> Server::gather() {
     return ctl;
 }
 
+// After a chunk, with both batches idle: marks the changes, which wait for
+// the next rebuild. A finished solve is reported at once; a float solve that
+// moves to FP64 is paused in its float batch (status 4, which the kernels
+// skip) at exactly this iteration, so its result depends on its own request
+// alone, however long the move waits.
 void Server::process(const std::vector<Control>& ctl) {
-    std::vector<std::unique_ptr<Job>> keep;
-    std::vector<size_t> promote, rerun;
     for (size_t i = 0; i < active_.size(); i++) {
+        Job& j = *active_[i];
+        if (j.action) continue;
         const Control& c = ctl[i];
-        auto& j = active_[i];
-        if (opt_.stall_window > 0 && c.status == 2 && j->solver->precision() == kFP32Kahan && !j->rerun) {
-            rerun.push_back(keep.size());
-            keep.push_back(std::move(j));
+        const bool f32 = j.solver->precision() == kFP32Kahan;
+        if (opt_.stall_window > 0 && c.status == 2 && f32 && !j.rerun) {
+            j.action = 3;
             continue;
         }
-        if (c.status != 0 || c.it >= j->solver->maxIterations()) {
-            if (!dirty_) {
-                b32_.reset();
-                b64_.reset();
-                dirty_ = true;
-            }
+        if (c.status != 0 || c.it >= j.solver->maxIterations()) {
+            report(j, &c, 0, "");
+            j.action = 1;
+            continue;
+        }
+        if (f32 && ((opt_.stall_window > 0 && c.it - c.it_best >= opt_.stall_window) ||
+                    (opt_.promote_orders > 0 && c.best_drop >= j.solver->residualDrop() - opt_.promote_orders))) {
+            j.solver->setStatus(4);
+            j.action = 2;
+        }
+    }
+}
+
+void Server::applyChanges() {
+    b32_.reset();
+    b64_.reset();
+    std::vector<std::unique_ptr<Job>> keep;
+    for (auto& j : active_) {
+        if (j->action == 1) {
             used_ -= std::min(used_, j->bytes);
             usedNodes_ -= std::min(usedNodes_, j->nodes);
-            retire(std::move(j), &c, 0, "");
+            j.reset();
             continue;
         }
-        if (opt_.stall_window > 0 && j->solver->precision() == kFP32Kahan && c.it - c.it_best >= opt_.stall_window)
-            promote.push_back(keep.size());
-        keep.push_back(std::move(j));
-    }
-    active_ = std::move(keep);
-    if (!rerun.empty()) {
-        // A float solve whose residual became NaN/Inf starts again from its
-        // initial state in FP64; the outcome depends on the request alone.
-        b32_.reset();
-        b64_.reset();
-        dirty_ = true;
-        std::vector<size_t> failed;
-        for (size_t k : rerun) {
-            auto& j = active_[k];
+        if (j->action == 2) {
+            used_ -= std::min(used_, j->bytes);
+            j->solver->setStatus(0);
+            j->solver->promoteToFP64();
+            j->bytes = j->solver->deviceBytes();
+            used_ += j->bytes;
+            stats_.promotions++;
+        } else if (j->action == 3) {
+            // a float solve whose residual became NaN/Inf starts again from
+            // its initial state in FP64; the outcome depends on the request alone
             used_ -= std::min(used_, j->bytes);
             j->solver.reset();
             j->rerun = true;
             j->config->set("GPU_PRECISION", "fp64");
+            stats_.reruns++;
             try {
                 j->solver = std::make_unique<Solver>(*j->config, *j->mesh, j->ini.empty() ? &j->patches : nullptr);
                 j->bytes = j->solver->deviceBytes();
                 used_ += j->bytes;
             } catch (const std::exception& e) {
-                j->message = e.what();
-                failed.push_back(k);
+                usedNodes_ -= std::min(usedNodes_, j->nodes);
+                const std::string msg = e.what();
+                retire(std::move(j), nullptr, 2, msg);
+                continue;
             }
         }
-        for (auto it = failed.rbegin(); it != failed.rend(); ++it) {
-            auto j = std::move(active_[*it]);
-            active_.erase(active_.begin() + static_cast<long>(*it));
-            usedNodes_ -= std::min(usedNodes_, j->nodes);
-            const std::string msg = j->message;
-            retire(std::move(j), nullptr, 2, msg);
-        }
-        for (size_t& k : promote)  // indices after the erased entries shift down
-            k -= static_cast<size_t>(std::count_if(failed.begin(), failed.end(), [k](size_t f) { return f < k; }));
+        j->action = 0;
+        keep.push_back(std::move(j));
     }
-    if (!promote.empty()) {
-        b32_.reset();
-        b64_.reset();
-        for (size_t k : promote) {
-            auto& j = active_[k];
-            used_ -= std::min(used_, j->bytes);
-            j->solver->promoteToFP64();
-            j->bytes = j->solver->deviceBytes();
-            used_ += j->bytes;
-        }
-        dirty_ = true;
-    }
+    active_ = std::move(keep);
 }
 
+// Rounds that marked changes (finished, paused or diverged solves, solves
+// built during a chunk) may wait before the batches are rebuilt for them,
+// unless they make up a quarter of the membership or nothing is left running.
+constexpr int kMaxWaitRounds = 2;
+
 void Server::pump(int* nActive, int* nWaiting) {
-    // 1. the chunk in flight: wait for it, then retire / re-run / promote
-    //    with the batches idle
+    double t = now();
+    // 1. the chunk in flight: wait for it, then mark what finished, diverged
+    //    or moves to FP64, with the batches idle
     if (inflight_) {
         const std::vector<Control> ctl = gather();
         inflight_ = false;
+        const double t1 = now();
+        stats_.wait_s += t1 - t;
         process(ctl);
+        t = now();
+        stats_.process_s += t - t1;
     }
-    // 2. the solves built during that chunk join; with nothing on the device,
-    //    requests are admitted right away
-    joinPending();
-    if (active_.empty()) {
+    // with nothing on the device, requests are admitted right away
+    if (active_.empty() && pending_.empty()) {
         admit();
-        joinPending();
+        const double t1 = now();
+        stats_.admit_s += t1 - t;
+        t = t1;
     }
-    // 3. the next chunk for every admitted solve; the two precision groups
-    //    run on their own streams and overlap on the device
-    if (!active_.empty()) {
-        if (dirty_) rebuild();
-        if (b32_) b32_->enqueue(opt_.chunk);
-        if (b64_) b64_->enqueue(opt_.chunk);
+    // 2. the batches are rebuilt for the marked changes and the solves built
+    //    during the last chunk once they are worth it (a quarter of the
+    //    membership, nothing left running, no batch yet, or waiting
+    //    kMaxWaitRounds rounds); until then the batches run unchanged, their
+    //    graphs and tuning reused
+    auto count = [this](size_t& changed, size_t running[2]) {
+        changed = pending_.size();
+        running[0] = running[1] = 0;
+        for (auto& j : active_) {
+            if (j->action) changed++;
+            else running[j->solver->precision() == kFP32Kahan ? 1 : 0]++;
+        }
+    };
+    size_t changed = 0, running[2] = {0, 0};
+    count(changed, running);
+    if (changed) {
+        waitRounds_++;
+        const size_t members = active_.size() + pending_.size();
+        if ((!b32_ && !b64_) || running[0] + running[1] == 0 || changed * 4 >= members ||
+            waitRounds_ >= kMaxWaitRounds) {
+            applyChanges();
+            joinPending();
+            rebuild();
+            stats_.rebuilds++;
+            waitRounds_ = 0;
+            count(changed, running);
+        }
+        const double t1 = now();
+        stats_.rebuild_s += t1 - t;
+        t = t1;
+    }
+    // 3. the next chunk of every batch with a running member; the two
+    //    precision groups run on their own streams and overlap on the device
+    if (b32_ && running[1]) {
+        b32_->enqueue(opt_.chunk);
         inflight_ = true;
+    }
+    if (b64_ && running[0]) {
+        b64_->enqueue(opt_.chunk);
+        inflight_ = true;
+    }
+    if (inflight_) {
+        stats_.rounds++;
         // a batch that timed its own tuning hands it on to later batches
         if (b32_ && b32_->tuning().valid) tuned_[1] = b32_->tuning();
         if (b64_ && b64_->tuning().valid) tuned_[0] = b64_->tuning();
     }
+    const double t2 = now();
+    stats_.enqueue_s += t2 - t;
     // 4. while the chunk runs, build the next requests that fit (device
-    //    allocation and upload); they join at the next round
+    //    allocation and upload); they join at a later round
     admit();
+    stats_.admit_s += now() - t2;
     if (nActive) *nActive = static_cast<int>(active_.size() + pending_.size());
     if (nWaiting) {
         std::lock_guard<std::mutex> l(mu_);

@@ -6,7 +6,9 @@
 // (one Batch per working precision, each on its own stream, so FP32 and FP64
 // work overlaps), and retire the moment they converge, diverge or reach
 // N_ITERATIONS. A fp32_kahan solve whose convergence progress stalls for
-// stall_window iterations continues in FP64.
+// stall_window iterations, or that comes within promote_orders of its
+// residual drop, continues in FP64 (the precision pattern: float for the
+// bulk of the iterations, the convergence test and state in FP64).
 #pragma once
 
 #include <condition_variable>
@@ -36,6 +38,19 @@ struct ServerResult {
     std::string message;
 };
 
+// Where a server's time went (seconds of wall time on the pumping thread).
+struct ServerStats {
+    long long rounds = 0;      // scheduling rounds that enqueued a chunk
+    long long rebuilds = 0;    // batch rebuilds (membership changes applied)
+    long long promotions = 0;  // fp32_kahan solves continued in FP64
+    long long reruns = 0;      // diverged fp32_kahan solves run again in FP64
+    double wait_s = 0;         // waiting for the chunk in flight (the device busy)
+    double process_s = 0;      // retiring, pausing and reporting after a chunk
+    double rebuild_s = 0;      // applying changes (promotions, releases) and rebuilding the batches
+    double enqueue_s = 0;      // enqueueing chunks (includes a new batch's autotuning)
+    double admit_s = 0;        // building admitted solves (device allocation, upload) while a chunk runs
+};
+
 struct ServerOptions {
     size_t budget_bytes = 0;      // device memory the admitted solves may hold (0: 90 % of free)
     int max_active = 1024;        // admitted solves at most
@@ -44,6 +59,8 @@ struct ServerOptions {
     long long stall_window = 0;   // fp32_kahan -> FP64 after this many iterations without progress, and
                                   // diverged fp32_kahan solves re-run in FP64 (0: neither)
     int host_threads = 4;         // workers preparing requests
+    double promote_orders = 0.0;  // fp32_kahan -> FP64 once within this many orders of the residual drop
+                                  // (best_drop >= RESIDUALS_DROP_CONVERGENCE - promote_orders; 0: off)
 };
 
 class Server {
@@ -53,6 +70,8 @@ public:
     Server(const Server&) = delete;
     Server& operator=(const Server&) = delete;
 
+    // Sets ServerOptions::promote_orders (before the first submission).
+    void setPromoteOrders(double orders) { opt_.promote_orders = orders; }
     // Queues a request (thread safe); its host preparation starts at once.
     long long submit(const std::string& iniPath);
     // The same for a case held in memory (the server keeps the copy).
@@ -67,6 +86,7 @@ public:
     void pump(int* active, int* waiting);
     // Requests finished since the last call.
     std::vector<ServerResult> take();
+    const ServerStats& stats() const { return stats_; }
     double now() const;
 
 private:
@@ -85,6 +105,11 @@ private:
         std::unique_ptr<Solver> solver;  // declared last: released before the mesh and config it refers to
         size_t bytes = 0;
         bool rerun = false;  // a diverged float solve restarted in FP64
+        // a change that waits for the next rebuild of the batches: 1 finished
+        // (result reported; its device memory is held while a batch refers to
+        // it), 2 continues in FP64 (paused in its float batch), 3 runs again
+        // from its initial state in FP64 (diverged; the kernels skip it)
+        int action = 0;
     };
     long long enqueue(std::unique_ptr<Job> j);
     void worker();
@@ -100,6 +125,10 @@ private:
     // stalled float solves (batches idle)
     void process(const std::vector<Control>& ctl);
     void retire(std::unique_ptr<Job> job, const Control* ctl, int error, const std::string& msg);
+    void report(Job& job, const Control* ctl, int error, const std::string& msg);
+    // the marked changes, with both batches released: finished solves
+    // released, paused ones promoted, diverged ones rebuilt in FP64
+    void applyChanges();
     size_t estimate(const Job& j) const;
 
     ServerOptions opt_;
@@ -119,11 +148,12 @@ private:
     GroupTuning tuned_[2];
     std::unique_ptr<Batch> b64_, b32_;
     std::vector<int> idx64_, idx32_;  // active_ index of each batch member
-    bool dirty_ = false;
     size_t used_ = 0;
     long long usedNodes_ = 0;
     double bytesPerNode_[2] = {0, 0};  // measured per precision (0: not yet)
     std::vector<ServerResult> done_;
+    ServerStats stats_;
+    int waitRounds_ = 0;  // rounds in which marked changes waited for a rebuild
 };
 
 }  // namespace ctbfm

@@ -1645,6 +1645,11 @@ void Solver::profileKernels(int reps, double* outMs) {
     });
 }
 
+void Solver::setStatus(int status) {
+    Control* d = g64_ ? i64_->c.ctl : i32_->c.ctl;
+    cudaCheck(cudaMemcpy(&d->status, &status, sizeof(int), cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
 void Solver::promoteToFP64() {
     if (prec_ == kFP64) return;
     const long N = mesh_.nodes();

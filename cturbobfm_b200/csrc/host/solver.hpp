@@ -105,6 +105,9 @@ public:
     // (Output::writeSolution, src/output.cpp:384-398), at `path`.
     void writeSolution(const std::string& path);
     void getTurbo(double massflow[6], double turbo[4]);
+    // Writes the status word of the device control block (the server pauses
+    // a member with a status the kernels skip, and releases it again).
+    void setStatus(int status);
     Control control();  // synchronous copy of the control block
     void profileKernels(int reps, double* outMs);
     // Continues a fp32_kahan solve in FP64: the state U - Uc, the control
@@ -122,6 +125,8 @@ public:
     int topology() const { return static_cast<int>(topo_); }
     int stages() const { return static_cast<int>(coeffs_.size()); }
     long maxIterations() const { return maxIter_; }
+    // RESIDUALS_DROP_CONVERGENCE
+    int residualDrop() const { return config_.getResidualsDropConvergence(); }
 
     // device data for batches (nullptr when the solver runs the other precision)
     InstanceT<double>* instance64() { return i64_.get(); }

@@ -60,6 +60,11 @@ class Info(ctypes.Structure):
     ]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int64) for f in ("rounds", "rebuilds", "promotions", "reruns")] + \
+        [(f, ctypes.c_double) for f in ("wait_s", "process_s", "rebuild_s", "enqueue_s", "admit_s")]
+
+
 class Result(ctypes.Structure):
     _fields_ = [
         ("id", ctypes.c_int64),
@@ -176,6 +181,8 @@ SIGNATURES = {
     "ctbfm_server_create": ([ctypes.c_uint64, ctypes.c_int32, _I64, _I64, _I64, ctypes.c_int32,
                              ctypes.POINTER(_VP)], ctypes.c_int),
     "ctbfm_server_destroy": ([_VP], None),
+    "ctbfm_server_set_promotion": ([_VP, ctypes.c_double], ctypes.c_int),
+    "ctbfm_server_get_stats": ([_VP, ctypes.POINTER(ServerStats)], ctypes.c_int),
     "ctbfm_server_submit": ([_VP, ctypes.c_char_p, ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_server_submit_case": ([_VP, ctypes.POINTER(CaseDesc), ctypes.POINTER(_I64)], ctypes.c_int),
     "ctbfm_server_pump": ([_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -441,11 +448,13 @@ class Server:
     """Continuous batching of operating-point solves (ctbfm_server_*)."""
 
     def __init__(self, budget_bytes: int = 0, max_active: int = 1024, chunk: int = 200, stall_window: int = 0,
-                 host_threads: int = 4, max_active_nodes: int = 0):
+                 host_threads: int = 4, max_active_nodes: int = 0, promote_orders: float = 0.0):
         h = _VP()
         _check(load_library().ctbfm_server_create(int(budget_bytes), int(max_active), int(max_active_nodes), int(chunk),
                                                   int(stall_window), int(host_threads), ctypes.byref(h)))
         self._h = h
+        if promote_orders > 0:
+            _check(load_library().ctbfm_server_set_promotion(h, float(promote_orders)))
 
     def close(self):
         if getattr(self, "_h", None):
@@ -476,6 +485,12 @@ class Server:
         _check(load_library().ctbfm_server_submit_case(self._h, ctypes.byref(desc), ctypes.byref(rid)))
         del keep
         return int(rid.value)
+
+    def stats(self) -> Dict[str, float]:
+        """Where the pumping thread's time went (ctbfm_server_get_stats)."""
+        st = ServerStats()
+        _check(load_library().ctbfm_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
 
     def pump(self):
         a, w = ctypes.c_int32(0), ctypes.c_int32(0)

@@ -338,6 +338,26 @@ int ctbfm_server_create(uint64_t device_budget_bytes, int32_t max_active, int64_
                         int64_t chunk_iterations, int64_t stall_window, int32_t host_threads, ctbfm_server** out);
 void ctbfm_server_destroy(ctbfm_server* s);
 
+/* The precision pattern's other trigger: a fp32_kahan solve continues in FP64
+ * once its best residual drop comes within `orders` of its
+ * RESIDUALS_DROP_CONVERGENCE (best_drop >= drop - orders), at a scheduling
+ * round; 0 (the default) turns it off. Set before the first submission. */
+int ctbfm_server_set_promotion(ctbfm_server* s, double orders);
+
+/* Where the pumping thread's time went since the server was created. */
+typedef struct {
+    int64_t rounds;      /* scheduling rounds that enqueued a chunk */
+    int64_t rebuilds;    /* batch rebuilds (membership changes applied, a few rounds' worth at a time) */
+    int64_t promotions;  /* fp32_kahan solves continued in FP64 */
+    int64_t reruns;      /* diverged fp32_kahan solves run again in FP64 */
+    double wait_s;       /* seconds waiting for the chunk in flight (the device busy) */
+    double process_s;    /* seconds reporting and marking after a chunk */
+    double rebuild_s;    /* seconds applying changes and rebuilding batches */
+    double enqueue_s;    /* seconds enqueueing chunks (a new batch's autotuning included) */
+    double admit_s;      /* seconds building admitted solves, while a chunk runs */
+} ctbfm_server_stats;
+int ctbfm_server_get_stats(ctbfm_server* s, ctbfm_server_stats* out);
+
 /* Queues the operating point of an input.ini; thread safe. */
 int ctbfm_server_submit(ctbfm_server* s, const char* ini_path, int64_t* request_id);
 
