@@ -447,6 +447,9 @@ int ctbfm_server_get_stats(ctbfm_server* s, ctbfm_server_stats* out) {
         out->wait_s = st.wait_s;
         out->process_s = st.process_s;
         out->rebuild_s = st.rebuild_s;
+        out->promote_s = st.promote_s;
+        out->release_s = st.release_s;
+        out->batch_s = st.batch_s;
         out->enqueue_s = st.enqueue_s;
         out->admit_s = st.admit_s;
         return CTBFM_OK;

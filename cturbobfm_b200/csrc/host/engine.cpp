@@ -14,10 +14,23 @@ InstanceT<R>::~InstanceT() {
 
 template <typename R>
 void* InstanceT<R>::allocBytes(size_t n) {
-    void* p = nullptr;
-    cudaCheck(cudaMalloc(&p, std::max<size_t>(n, 16)), "cudaMalloc");
-    allocs_.push_back(p);
-    bytes_ += std::max<size_t>(n, 16);
+    const size_t a = (std::max<size_t>(n, 16) + 255) & ~size_t(255);
+    if (!slab_ || slabUsed_ + a > slabCap_) {
+        constexpr size_t kMinSlab = size_t(1) << 20;
+        size_t cap = std::max(a, hint_ ? hint_ : kMinSlab);
+        if (slab_) cap = std::max(cap, 2 * slabCap_);
+        hint_ = 0;
+        void* p = nullptr;
+        cudaCheck(cudaMalloc(&p, cap), "cudaMalloc");
+        allocs_.push_back(p);
+        slab_ = static_cast<char*>(p);
+        slabCap_ = cap;
+        slabUsed_ = 0;
+        bytes_ += cap;
+    }
+    void* p = slab_ + slabUsed_;
+    slabUsed_ += a;
+    used_ += a;
     return p;
 }
 
@@ -333,9 +346,11 @@ GroupTuning GroupT<R>::tuning() const {
 template <typename R>
 void GroupT<R>::adopt(const GroupTuning& t) {
     if (!t.valid) return;
-    for (int d = 0; d < 3; d++) faceTile_[d] = t.faceTile[d];
     for (int k = 0; k < 3; k++) stageMs_[k] = t.stageMs[k];
-    buildTiles();  // also drops captured graphs
+    bool same = true;
+    for (int d = 0; d < 3; d++) same = same && faceTile_[d] == t.faceTile[d];
+    for (int d = 0; d < 3; d++) faceTile_[d] = t.faceTile[d];
+    if (!same) buildTiles();  // also drops captured graphs
     if (fusionAuto_) {
         view_.fusedMode = t.fusedMode;
         persist_ = t.persistent && persistOk_;
@@ -374,13 +389,15 @@ GroupT<R>::~GroupT() {
     cudaFree(dSync_);
 }
 
-// One pageable host-to-device copy per member, ordered on s: each call returns
-// once its source is staged, so the host copy may change right after.
+// The members' descriptions gathered on the host and sent in one pageable
+// host-to-device copy, ordered on s: the call returns once its source is
+// staged, so the host copies may change right after.
 template <typename R>
 void GroupT<R>::refresh(cudaStream_t s) {
-    for (size_t i = 0; i < members_.size(); i++)
-        cudaCheck(cudaMemcpyAsync(dCases_ + i, &members_[i]->c, sizeof(DevCaseT<R>), cudaMemcpyHostToDevice, s),
-                  "cudaMemcpyAsync");
+    std::vector<DevCaseT<R>> all(members_.size());
+    for (size_t i = 0; i < members_.size(); i++) all[i] = members_[i]->c;
+    cudaCheck(cudaMemcpyAsync(dCases_, all.data(), all.size() * sizeof(DevCaseT<R>), cudaMemcpyHostToDevice, s),
+              "cudaMemcpyAsync");
 }
 
 // Captures `iters` whole iterations into one executable graph.

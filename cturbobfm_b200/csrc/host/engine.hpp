@@ -37,14 +37,25 @@ public:
     double* allocD(size_t n);
     const R* uploadR(const std::vector<double>& v);
     const double* uploadD(const std::vector<double>& v);
+    // Device arrays are carved (256-byte aligned) from a few large
+    // allocations: the first of `reserve` bytes (when set before the first
+    // array), each further one at least double the previous. One cudaMalloc
+    // and one cudaFree per slab instead of one per array keeps creating and
+    // promoting solves cheap.
+    void reserve(size_t bytes) { hint_ = bytes; }
     void* allocBytes(size_t n);
     size_t deviceBytes() const { return bytes_; }
+    size_t usedBytes() const { return used_; }
 
     DevCaseT<R> c{};  // host copy of the description, pointers into this instance's device arrays
 
 private:
     std::vector<void*> allocs_;
-    size_t bytes_ = 0;
+    size_t bytes_ = 0;   // held: the slabs
+    size_t used_ = 0;    // carved
+    char* slab_ = nullptr;
+    size_t slabUsed_ = 0, slabCap_ = 0;
+    size_t hint_ = 0;
 };
 
 // What a group's autotuner chose (face tiles, stage fusion) and on how many

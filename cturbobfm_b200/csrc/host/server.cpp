@@ -284,10 +284,12 @@ void Server::applyChanges() {
     b64_.reset();
     std::vector<std::unique_ptr<Job>> keep;
     for (auto& j : active_) {
+        const double t0 = now();
         if (j->action == 1) {
             used_ -= std::min(used_, j->bytes);
             usedNodes_ -= std::min(usedNodes_, j->nodes);
             j.reset();
+            stats_.release_s += now() - t0;
             continue;
         }
         if (j->action == 2) {
@@ -316,6 +318,7 @@ void Server::applyChanges() {
                 continue;
             }
         }
+        if (j->action) stats_.promote_s += now() - t0;
         j->action = 0;
         keep.push_back(std::move(j));
     }
@@ -369,7 +372,9 @@ void Server::pump(int* nActive, int* nWaiting) {
             waitRounds_ >= kMaxWaitRounds) {
             applyChanges();
             joinPending();
+            const double tb = now();
             rebuild();
+            stats_.batch_s += now() - tb;
             stats_.rebuilds++;
             waitRounds_ = 0;
             count(changed, running);

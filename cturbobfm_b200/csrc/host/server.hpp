@@ -47,6 +47,9 @@ struct ServerStats {
     double wait_s = 0;         // waiting for the chunk in flight (the device busy)
     double process_s = 0;      // retiring, pausing and reporting after a chunk
     double rebuild_s = 0;      // applying changes (promotions, releases) and rebuilding the batches
+    double promote_s = 0;      //   of which promoting solves to FP64 (and re-creating diverged ones)
+    double release_s = 0;      //   of which releasing finished solves
+    double batch_s = 0;        //   of which building the two batches
     double enqueue_s = 0;      // enqueueing chunks (includes a new batch's autotuning)
     double admit_s = 0;        // building admitted solves (device allocation, upload) while a chunk runs
 };

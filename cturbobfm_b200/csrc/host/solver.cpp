@@ -6,6 +6,7 @@
 #include "restart.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cctype>
 #include <cmath>
 #include <cstring>
@@ -178,15 +179,29 @@ Solver::Solver(Config& config, Mesh& mesh, const std::vector<PatchRow>* patches)
     }
     cudaCheck(cudaMallocHost(reinterpret_cast<void**>(&hostCtl_), sizeof(Control)), "cudaMallocHost");
     std::memset(hostCtl_, 0, sizeof(Control));
+    // the device arrays of a solve come from one slab when its size is
+    // known: the bytes per node of the last solve of this precision, with
+    // slack (a further slab when they do not fit)
+    static std::atomic<double> perNode[2] = {{0.0}, {0.0}};
+    const double nodesD = static_cast<double>(mesh_.nodes());
+    auto reserveLike = [&](auto& inst, int p) {
+        const double b = perNode[p].load();
+        if (b > 0) inst.reserve(static_cast<size_t>(b * nodesD * 1.1) + (size_t(1) << 16));
+    };
+    auto learn = [&](const auto& inst, int p) { perNode[p].store(static_cast<double>(inst.usedBytes()) / nodesD); };
     if (prec_ == kFP32Kahan) {
         i32_ = std::make_unique<InstanceT<float>>();
+        reserveLike(*i32_, 1);
         uploadArrays(*i32_);
+        learn(*i32_, 1);
         g32_ = std::make_unique<GroupT<float>>(std::vector<InstanceT<float>*>{i32_.get()});
         g32_->setFusedMode(fusion_);
         initializeState(*i32_, *g32_);
     } else {
         i64_ = std::make_unique<InstanceT<double>>();
+        reserveLike(*i64_, 0);
         uploadArrays(*i64_);
+        learn(*i64_, 0);
         g64_ = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{i64_.get()});
         g64_->setFusedMode(fusion_);
         initializeState(*i64_, *g64_);
@@ -1663,6 +1678,7 @@ void Solver::promoteToFP64() {
     const Control ctl = control();
     proto_.compensated = 0;
     auto inst = std::make_unique<InstanceT<double>>();
+    inst->reserve(2 * i32_->usedBytes() + (size_t(1) << 16));  // float arrays become double
     uploadArrays(*inst);
     auto grp = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{inst.get()});
     grp->setFusedMode(fusion_);

@@ -352,7 +352,10 @@ typedef struct {
     int64_t reruns;      /* diverged fp32_kahan solves run again in FP64 */
     double wait_s;       /* seconds waiting for the chunk in flight (the device busy) */
     double process_s;    /* seconds reporting and marking after a chunk */
-    double rebuild_s;    /* seconds applying changes and rebuilding batches */
+    double rebuild_s;    /* seconds applying changes and rebuilding batches, of which */
+    double promote_s;    /*   promoting solves to FP64 (and re-creating diverged ones), */
+    double release_s;    /*   releasing finished solves, */
+    double batch_s;      /*   building the two batches */
     double enqueue_s;    /* seconds enqueueing chunks (a new batch's autotuning included) */
     double admit_s;      /* seconds building admitted solves, while a chunk runs */
 } ctbfm_server_stats;

@@ -76,8 +76,11 @@ def test_budget_admits_one_solve_at_a_time(tmp_path):
     from cturbobfm_b200 import Server, Solver
 
     inis = [_write(_req(f"r{m}", 64, 24, 1.0 + 0.05 * m, 0.95), str(tmp_path)) for m in range(3)]
-    with Solver(inis[0]) as p:
-        one = int(p.info().device_bytes)
+    # a solve's device slab is sized like the previous solve of its precision
+    # (the first one of a process grows its slabs): measure the second
+    for _ in range(2):
+        with Solver(inis[0]) as p:
+            one = int(p.info().device_bytes)
     with Server(budget_bytes=int(one * 1.5), chunk=200) as s:
         ids = [s.submit(i) for i in inis]
         res = _drain(s, 3)
