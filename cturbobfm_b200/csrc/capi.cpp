@@ -450,6 +450,7 @@ int ctbfm_server_get_stats(ctbfm_server* s, ctbfm_server_stats* out) {
         out->promote_s = st.promote_s;
         out->release_s = st.release_s;
         out->batch_s = st.batch_s;
+        out->prepare_s = st.prepare_s;
         out->enqueue_s = st.enqueue_s;
         out->admit_s = st.admit_s;
         return CTBFM_OK;

@@ -38,8 +38,8 @@ Batch::Batch(const std::vector<Solver*>& members) : members_(members) {
     else g64_->setFusedMode(fusion);
     cudaCheck(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = ownStream_;
-    cudaCheck(cudaMalloc(reinterpret_cast<void**>(&dCtl_), members_.size() * sizeof(Control)), "cudaMalloc");
-    cudaCheck(cudaMallocHost(reinterpret_cast<void**>(&hCtl_), members_.size() * sizeof(Control)), "cudaMallocHost");
+    dCtl_ = static_cast<Control*>(deviceAlloc(members_.size() * sizeof(Control)));
+    hCtl_ = static_cast<Control*>(pinnedAlloc(members_.size() * sizeof(Control)));
 }
 
 Batch::~Batch() {
@@ -47,8 +47,8 @@ Batch::~Batch() {
     if (stream_ && stream_ != ownStream_) cudaStreamSynchronize(stream_);
     g32_.reset();
     g64_.reset();
-    if (dCtl_) cudaFree(dCtl_);
-    if (hCtl_) cudaFreeHost(hCtl_);
+    deviceFree(dCtl_);
+    pinnedFree(hCtl_, members_.size() * sizeof(Control));
     if (ownStream_) cudaStreamDestroy(ownStream_);
 }
 

@@ -1,15 +1,112 @@
 // Device-side engine: see engine.hpp.
 #include "engine.hpp"
 
+#include <cstdint>
+#include <map>
+#include <mutex>
+
 #include <algorithm>
 
 namespace ctbfm {
 
 // ---------------------------------------------------------------- InstanceT
 
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex gPoolMu;
+cudaMemPool_t gPools[kMaxDevices] = {};
+
+cudaMemPool_t poolOf(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) throw CudaError("device index out of range");
+    std::lock_guard<std::mutex> lock(gPoolMu);
+    if (!gPools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        cudaCheck(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;  // released blocks stay in the pool
+        cudaCheck(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+        gPools[dev] = pool;
+    }
+    return gPools[dev];
+}
+
+std::mutex gPinnedMu;
+std::map<size_t, std::vector<void*>> gPinned;  // free pinned blocks by size class
+
+size_t pinnedClass(size_t bytes) {
+    size_t c = 256;
+    while (c < bytes) c *= 2;
+    return c;
+}
+
+}  // namespace
+
+void* deviceAlloc(size_t bytes) {
+    int dev = 0;
+    cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+    void* p = nullptr;
+    cudaMemPool_t pool = poolOf(dev);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), pool, cudaStreamLegacy);
+    if (e == cudaErrorMemoryAllocation) {  // hand the pool's idle blocks back to the device and try again
+        (void)cudaGetLastError();
+        cudaCheck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        cudaCheck(cudaMemPoolTrimTo(pool, 0), "cudaMemPoolTrimTo");
+        e = cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), pool, cudaStreamLegacy);
+    }
+    cudaCheck(e, "cudaMallocFromPoolAsync");
+    cudaCheck(cudaStreamSynchronize(cudaStreamLegacy), "cudaStreamSynchronize");
+    return p;
+}
+
+void deviceFree(void* p) noexcept {
+    if (!p) return;
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, cudaStreamLegacy);
+}
+
+size_t devicePoolIdle() {
+    int dev = 0;
+    cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+    cudaMemPool_t pool = poolOf(dev);
+    uint64_t reserved = 0, used = 0;
+    cudaCheck(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved), "cudaMemPoolGetAttribute");
+    cudaCheck(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used), "cudaMemPoolGetAttribute");
+    return reserved > used ? static_cast<size_t>(reserved - used) : 0;
+}
+
+void* pinnedAlloc(size_t bytes) {
+    const size_t c = pinnedClass(bytes);
+    {
+        std::lock_guard<std::mutex> lock(gPinnedMu);
+        auto& v = gPinned[c];
+        if (!v.empty()) {
+            void* p = v.back();
+            v.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaCheck(cudaMallocHost(&p, c), "cudaMallocHost");
+    return p;
+}
+
+void pinnedFree(void* p, size_t bytes) noexcept {
+    if (!p) return;
+    try {
+        std::lock_guard<std::mutex> lock(gPinnedMu);
+        gPinned[pinnedClass(bytes)].push_back(p);
+    } catch (...) {
+        cudaFreeHost(p);
+    }
+}
+
 template <typename R>
 InstanceT<R>::~InstanceT() {
-    for (void* p : allocs_) cudaFree(p);
+    for (void* p : allocs_) deviceFree(p);
 }
 
 template <typename R>
@@ -20,8 +117,7 @@ void* InstanceT<R>::allocBytes(size_t n) {
         size_t cap = std::max(a, hint_ ? hint_ : kMinSlab);
         if (slab_) cap = std::max(cap, 2 * slabCap_);
         hint_ = 0;
-        void* p = nullptr;
-        cudaCheck(cudaMalloc(&p, cap), "cudaMalloc");
+        void* p = deviceAlloc(cap);
         allocs_.push_back(p);
         slab_ = static_cast<char*>(p);
         slabCap_ = cap;
@@ -74,7 +170,7 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     for (auto* m : members_) nstages_ = std::max(nstages_, m->c.nstages);
     const int M = static_cast<int>(members_.size());
     buildTiles();
-    cudaCheck(cudaMalloc(&dCases_, M * sizeof(DevCaseT<R>)), "cudaMalloc");
+    dCases_ = static_cast<DevCaseT<R>*>(deviceAlloc(M * sizeof(DevCaseT<R>)));
     view_.cases = dCases_;
     view_.m = M;
     view_.ideal = view_.real = false;
@@ -90,7 +186,7 @@ GroupT<R>::GroupT(std::vector<InstanceT<R>*> members) : members_(std::move(membe
     persistOk_ = !view_.real && !view_.viscous && !view_.sa;
     for (auto* m : members_) persistOk_ = persistOk_ && m->c.scheme == scheme_;
     if (persistOk_) {
-        cudaCheck(cudaMalloc(&dSync_, sizeof(GridSync)), "cudaMalloc");
+        dSync_ = static_cast<GridSync*>(deviceAlloc(sizeof(GridSync)));
         cudaCheck(cudaMemset(dSync_, 0, sizeof(GridSync)), "cudaMemset");
     }
     refresh(nullptr);
@@ -190,9 +286,9 @@ void GroupT<R>::buildTiles() {
     add(view_.inst, inst);
     add(view_.bint, bint);
     add(view_.bintAll, bintAll);
-    if (dTiles_) cudaCheck(cudaFree(dTiles_), "cudaFree");
+    deviceFree(dTiles_);
     dTiles_ = nullptr;
-    cudaCheck(cudaMalloc(&dTiles_, std::max<size_t>(all.size(), 1) * sizeof(Tile)), "cudaMalloc");
+    dTiles_ = static_cast<Tile*>(deviceAlloc(std::max<size_t>(all.size(), 1) * sizeof(Tile)));
     cudaCheck(cudaMemcpy(dTiles_, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice), "cudaMemcpy");
     // a copy from pageable memory may still be in flight when cudaMemcpy
     // returns, and the kernels run on non-blocking streams: wait for it (the
@@ -384,9 +480,9 @@ GroupT<R>::~GroupT() {
         cudaStreamSynchronize(captureStream_);
         cudaStreamDestroy(captureStream_);
     }
-    cudaFree(dCases_);
-    cudaFree(dTiles_);
-    cudaFree(dSync_);
+    deviceFree(dCases_);
+    deviceFree(dTiles_);
+    deviceFree(dSync_);
 }
 
 // The members' descriptions gathered on the host and sent in one pageable

@@ -25,6 +25,20 @@ inline void cudaCheck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Device memory of instances, groups and batches: a library-owned
+// stream-ordered pool per device that keeps released blocks for reuse, so
+// creating, promoting and releasing solves costs no driver mapping or
+// unmapping. A block is ready when deviceAlloc returns; deviceFree first
+// waits for the device's outstanding work (as cudaFree does), then returns
+// the block to the pool.
+void* deviceAlloc(size_t bytes);
+void deviceFree(void* p) noexcept;
+// bytes the current device's pool holds that no user holds (free for reuse)
+size_t devicePoolIdle();
+// Pinned host blocks (control-block copies), recycled by size class.
+void* pinnedAlloc(size_t bytes);
+void pinnedFree(void* p, size_t bytes) noexcept;
+
 template <typename R>
 class InstanceT {
 public:

@@ -189,6 +189,7 @@ void Server::admit() {
                 if (budget == 0) {
                     size_t freeB = 0, totalB = 0;
                     cudaCheck(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
+                    freeB += devicePoolIdle();  // released solves' blocks, kept for reuse
                     budget = used_ + freeB * 9 / 10;
                 }
                 if (used_ + need > budget && !idle) break;
@@ -280,8 +281,10 @@ void Server::process(const std::vector<Control>& ctl) {
 }
 
 void Server::applyChanges() {
+    const double td = now();
     b32_.reset();
     b64_.reset();
+    stats_.batch_s += now() - td;
     std::vector<std::unique_ptr<Job>> keep;
     for (auto& j : active_) {
         const double t0 = now();
@@ -294,8 +297,7 @@ void Server::applyChanges() {
         }
         if (j->action == 2) {
             used_ -= std::min(used_, j->bytes);
-            j->solver->setStatus(0);
-            j->solver->promoteToFP64();
+            j->solver->commitPromotion();  // prepared while a chunk ran, or now
             j->bytes = j->solver->deviceBytes();
             used_ += j->bytes;
             stats_.promotions++;
@@ -401,10 +403,16 @@ void Server::pump(int* nActive, int* nWaiting) {
     }
     const double t2 = now();
     stats_.enqueue_s += t2 - t;
-    // 4. while the chunk runs, build the next requests that fit (device
-    //    allocation and upload); they join at a later round
+    // 4. while the chunk runs: the FP64 side of the paused solves (their
+    //    float state does not change while they are paused), then the next
+    //    requests that fit (device allocation and upload); both join at a
+    //    later round
+    for (auto& j : active_)
+        if (j->action == 2 && !j->solver->promotionPrepared()) j->solver->preparePromotion();
+    const double t3 = now();
+    stats_.prepare_s += t3 - t2;
     admit();
-    stats_.admit_s += now() - t2;
+    stats_.admit_s += now() - t3;
     if (nActive) *nActive = static_cast<int>(active_.size() + pending_.size());
     if (nWaiting) {
         std::lock_guard<std::mutex> l(mu_);

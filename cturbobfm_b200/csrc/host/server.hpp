@@ -49,7 +49,8 @@ struct ServerStats {
     double rebuild_s = 0;      // applying changes (promotions, releases) and rebuilding the batches
     double promote_s = 0;      //   of which promoting solves to FP64 (and re-creating diverged ones)
     double release_s = 0;      //   of which releasing finished solves
-    double batch_s = 0;        //   of which building the two batches
+    double batch_s = 0;        //   of which releasing and building the two batches
+    double prepare_s = 0;      // building the FP64 side of paused solves, while a chunk runs
     double enqueue_s = 0;      // enqueueing chunks (includes a new batch's autotuning)
     double admit_s = 0;        // building admitted solves (device allocation, upload) while a chunk runs
 };

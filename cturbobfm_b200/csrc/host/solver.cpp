@@ -177,7 +177,7 @@ Solver::Solver(Config& config, Mesh& mesh, const std::vector<PatchRow>* patches)
         size_t bytes = 0;
         cudaCheck(noallocScratch(device_, &scratch, &bytes), "static scratch set-up (cudaGetSymbolAddress)");
     }
-    cudaCheck(cudaMallocHost(reinterpret_cast<void**>(&hostCtl_), sizeof(Control)), "cudaMallocHost");
+    hostCtl_ = static_cast<Control*>(pinnedAlloc(sizeof(Control)));
     std::memset(hostCtl_, 0, sizeof(Control));
     // the device arrays of a solve come from one slab when its size is
     // known: the bytes per node of the last solve of this precision, with
@@ -700,11 +700,12 @@ void Solver::validateSettings() {
 
 Solver::~Solver() {
     if (ownStream_) cudaStreamSynchronize(ownStream_);
+    if (stream_ && stream_ != ownStream_) cudaStreamSynchronize(stream_);
     g32_.reset();
     g64_.reset();
     i32_.reset();
     i64_.reset();
-    if (hostCtl_) cudaFreeHost(hostCtl_);
+    pinnedFree(hostCtl_, sizeof(Control));
     if (ownStream_) cudaStreamDestroy(ownStream_);
 }
 
@@ -1210,6 +1211,7 @@ void Solver::initializeState(InstanceT<R>& inst, GroupT<R>& grp) {
 // ------------------------------------------------------------------ running
 
 void Solver::enqueue(long long n) {
+    promo_.reset();  // a prepared promotion holds the state before these iterations
     visit([&](auto& inst, auto& grp) { grp.enqueue(n, stream_); (void)inst; });
 }
 
@@ -1554,6 +1556,7 @@ void Solver::viscousOutputFields(const double* const U[5], std::map<std::string,
 // density * 0 (walls at rest). Every iteration keeps it there, so doing it
 // whenever a state is set gives the reference's states.
 void Solver::setState(const double* const in[5]) {
+    promo_.reset();
     if (!proto_.viscous) {
         uploadState(in);
         return;
@@ -1666,7 +1669,12 @@ void Solver::setStatus(int status) {
 }
 
 void Solver::promoteToFP64() {
-    if (prec_ == kFP64) return;
+    preparePromotion();
+    commitPromotion();
+}
+
+void Solver::preparePromotion() {
+    if (prec_ == kFP64 || promo_) return;
     const long N = mesh_.nodes();
     std::array<std::vector<double>, 5> U;
     double* out[5];
@@ -1675,18 +1683,20 @@ void Solver::promoteToFP64() {
         out[v] = U[v].data();
     }
     getState(out);
-    const Control ctl = control();
+    auto p = std::make_unique<Promotion>();
+    p->ctl = control();
     proto_.compensated = 0;
-    auto inst = std::make_unique<InstanceT<double>>();
-    inst->reserve(2 * i32_->usedBytes() + (size_t(1) << 16));  // float arrays become double
-    uploadArrays(*inst);
-    auto grp = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{inst.get()});
-    grp->setFusedMode(fusion_);
+    p->inst = std::make_unique<InstanceT<double>>();
+    InstanceT<double>& inst = *p->inst;
+    inst.reserve(2 * i32_->usedBytes() + (size_t(1) << 16));  // float arrays become double
+    uploadArrays(inst);
+    p->grp = std::make_unique<GroupT<double>>(std::vector<InstanceT<double>*>{&inst});
+    p->grp->setFusedMode(fusion_);
     const DevCaseT<float>& f = i32_->c;
     if (proto_.sa) {  // the model's nu hat and laminar viscosity carry over
         std::vector<float> tf(static_cast<size_t>(N));
         std::vector<double> td(static_cast<size_t>(N));
-        const std::pair<const float*, double*> pairs[2] = {{f.nuhat, inst->c.nuhat}, {f.nul, inst->c.nul}};
+        const std::pair<const float*, double*> pairs[2] = {{f.nuhat, inst.c.nuhat}, {f.nul, inst.c.nul}};
         for (const auto& pr : pairs) {
             cudaCheck(cudaMemcpy(tf.data(), pr.first, N * sizeof(float), cudaMemcpyDeviceToHost), "cudaMemcpy");
             std::copy(tf.begin(), tf.end(), td.begin());
@@ -1694,16 +1704,37 @@ void Solver::promoteToFP64() {
         }
     }
     if (proto_.nprofiles)
-        cudaCheck(cudaMemcpy(inst->c.prof_p, f.prof_p, profP_.size() * sizeof(double), cudaMemcpyDeviceToDevice),
+        cudaCheck(cudaMemcpy(inst.c.prof_p, f.prof_p, profP_.size() * sizeof(double), cudaMemcpyDeviceToDevice),
                   "cudaMemcpy");
-    cudaCheck(cudaMemcpy(inst->c.hist, f.hist, static_cast<size_t>(proto_.hist_cap) * kHistWidth * sizeof(double),
+    cudaCheck(cudaMemcpy(inst.c.hist, f.hist, static_cast<size_t>(proto_.hist_cap) * kHistWidth * sizeof(double),
                          cudaMemcpyDeviceToDevice),
               "cudaMemcpy");
-    i64_ = std::move(inst);
-    g64_ = std::move(grp);
-    prec_ = kFP64;
+    // the state (setState: no-slip wall nodes carry no momentum)
+    std::array<std::vector<double>, 3> mom;
     const double* in[5] = {U[0].data(), U[1].data(), U[2].data(), U[3].data(), U[4].data()};
-    setState(in);
+    if (proto_.viscous)
+        for (int v = 0; v < 3; v++) {
+            mom[v] = U[v + 1];
+            for (long q = 0; q < N; q++)
+                if (wall_[static_cast<size_t>(q)]) mom[v][q] = U[0][q] * 0.0;
+            in[v + 1] = mom[v].data();
+        }
+    for (int v = 0; v < 5; v++)
+        cudaCheck(cudaMemcpyAsync(inst.c.U[v], in[v], N * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                  "cudaMemcpyAsync");
+    cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    promo_ = std::move(p);
+}
+
+void Solver::commitPromotion() {
+    if (prec_ == kFP64) return;
+    if (!promo_) preparePromotion();
+    Control ctl = promo_->ctl;
+    if (ctl.status == 4) ctl.status = 0;  // paused by a server: running again
+    i64_ = std::move(promo_->inst);
+    g64_ = std::move(promo_->grp);
+    promo_.reset();
+    prec_ = kFP64;
     *hostCtl_ = ctl;
     cudaCheck(cudaMemcpy(i64_->c.ctl, hostCtl_, sizeof(Control), cudaMemcpyHostToDevice), "cudaMemcpy");
     g32_.reset();

@@ -115,6 +115,15 @@ public:
     // profiles and the history move to a new FP64 instance; the float
     // instance is released. No-op on an FP64 solver.
     void promoteToFP64();
+    // promoteToFP64 in two steps: prepare builds the FP64 instance from the
+    // current float state (device arrays, uploads, the state converted) and
+    // may run while other groups' kernels run, as long as nothing advances
+    // this solve (paused, or not in a running batch); commit swaps it in and
+    // releases the float instance, with no batch referring to the solve. A
+    // paused status (4) in the copied control block becomes running.
+    void preparePromotion();
+    void commitPromotion();
+    bool promotionPrepared() const { return promo_ != nullptr; }
     long long history(long long maxRows, double* lognorm, double* massflow, double* turbo, double* hub,
                       double* time = nullptr);
     size_t deviceBytes() const;
@@ -188,6 +197,12 @@ private:
     std::unique_ptr<GroupT<double>> g64_;
     std::unique_ptr<InstanceT<float>> i32_;
     std::unique_ptr<GroupT<float>> g32_;
+    struct Promotion {
+        std::unique_ptr<InstanceT<double>> inst;
+        std::unique_ptr<GroupT<double>> grp;
+        Control ctl;
+    };
+    std::unique_ptr<Promotion> promo_;  // a prepared promotion, not yet committed
     Control* hostCtl_ = nullptr;  // pinned
     cudaStream_t ownStream_ = nullptr, stream_ = nullptr;
     int device_ = 0;  // the CUDA device current when the solver was created

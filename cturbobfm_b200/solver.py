@@ -63,7 +63,7 @@ class Info(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(f, ctypes.c_int64) for f in ("rounds", "rebuilds", "promotions", "reruns")] + \
         [(f, ctypes.c_double) for f in ("wait_s", "process_s", "rebuild_s", "promote_s", "release_s", "batch_s",
-                                        "enqueue_s", "admit_s")]
+                                        "prepare_s", "enqueue_s", "admit_s")]
 
 
 class Result(ctypes.Structure):

@@ -355,7 +355,8 @@ typedef struct {
     double rebuild_s;    /* seconds applying changes and rebuilding batches, of which */
     double promote_s;    /*   promoting solves to FP64 (and re-creating diverged ones), */
     double release_s;    /*   releasing finished solves, */
-    double batch_s;      /*   building the two batches */
+    double batch_s;      /*   releasing and building the two batches */
+    double prepare_s;    /* seconds building the FP64 side of paused solves, while a chunk runs */
     double enqueue_s;    /* seconds enqueueing chunks (a new batch's autotuning included) */
     double admit_s;      /* seconds building admitted solves, while a chunk runs */
 } ctbfm_server_stats;
