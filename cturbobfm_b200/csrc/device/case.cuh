@@ -107,6 +107,9 @@ struct Control {
 // A block's share of a batched launch: `count` consecutive elements (nodes,
 // faces, periodic pairs, planes or instances) of instance `inst`, starting at
 // `start`; `local` numbers the tiles of that instance (reduction partials).
+// plane points per block of the boundary integrals (k_bint)
+constexpr int kBintChunk = 1024;
+
 struct Tile {
     int inst;
     int local;
@@ -177,6 +180,13 @@ struct alignas(16) DevCaseT {
     const double* bsx[6];
     const double* bsy[6];
     const double* bsz[6];
+    // the eight boundary integrals (mass flow through planes 0..5, the Pt /
+    // Tt / Ht / s integrals over the two turbo planes) are summed in chunks of
+    // kBintChunk plane points, one block each, into bint_part (4 sums per
+    // chunk), which k_pre adds in chunk order; the chunks of integral b are
+    // bint_off[b] .. bint_off[b+1]-1
+    double* bint_part;
+    int bint_off[9];
     // BFM fields (nullptr when absent)
     const R* blk;
     const R* gbx;

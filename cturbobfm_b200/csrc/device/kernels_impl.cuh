@@ -830,8 +830,9 @@ __device__ __forceinline__ void b_bint(const DevCaseT<R>& c, const Tile& tl) {
     int na, nb;
     planeExtent(c, plane, na, nb);
     const long long cnt = static_cast<long long>(na) * nb;
+    const long long end = tl.start + tl.count < cnt ? tl.start + tl.count : cnt;
     double s[4] = {0.0, 0.0, 0.0, 0.0};
-    for (long long e = threadIdx.x; e < cnt; e += blockDim.x) {
+    for (long long e = tl.start + threadIdx.x; e < end; e += blockDim.x) {
         const int a = static_cast<int>(e / nb), bb = static_cast<int>(e % nb);
         const long long q = planeNode(c, plane, a, bb);
         const double sx = c.bsx[plane][e], sy = c.bsy[plane][e], sz = c.bsz[plane][e];
@@ -856,12 +857,29 @@ __device__ __forceinline__ void b_bint(const DevCaseT<R>& c, const Tile& tl) {
     }
     blockSum<4>(s);
     if (threadIdx.x == 0) {
-        if (blk < 6) c.ctl->massflow[blk] = s[0];
-        else {
-            c.ctl->pt_int[blk - 6] = s[0];
-            c.ctl->tt_int[blk - 6] = s[1];
-            c.ctl->ht_int[blk - 6] = s[2];
-            c.ctl->s_int[blk - 6] = s[3];
+        double* part = c.bint_part + (c.bint_off[blk] + tl.start / kBintChunk) * 4;
+#pragma unroll
+        for (int v = 0; v < 4; v++) part[v] = s[v];
+    }
+}
+
+// The boundary integrals from their chunk partials, added in chunk order
+// (one thread; k_pre after k_bint).
+template <typename R>
+__device__ __forceinline__ void combineBoundaryIntegrals(const DevCaseT<R>& c) {
+    Control* ctl = c.ctl;
+    for (int b = 0; b < 8; b++) {
+        double s[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k = c.bint_off[b]; k < c.bint_off[b + 1]; k++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) s[v] += c.bint_part[k * 4 + v];
+        if (b < 6) {
+            ctl->massflow[b] = s[0];
+        } else {
+            ctl->pt_int[b - 6] = s[0];
+            ctl->tt_int[b - 6] = s[1];
+            ctl->ht_int[b - 6] = s[2];
+            ctl->s_int[b - 6] = s[3];
         }
     }
 }
@@ -896,6 +914,7 @@ __device__ __forceinline__ void b_pre(const DevCaseT<R>& c, const Tile& tl, int 
     }
     if (threadIdx.x != 0) return;
     if (c.need_turbo || forceTurbo) {
+        combineBoundaryIntegrals(c);
         const int p0 = turboPlane(c, 0), p1 = turboPlane(c, 1);
         double mflow = 0.5 * (fabs(ctl->massflow[p0]) + fabs(ctl->massflow[p1]));
         if (c.topo == 2) mflow *= 2.0 * M_PI / c.wedge;

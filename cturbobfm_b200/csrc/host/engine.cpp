@@ -257,10 +257,12 @@ void GroupT<R>::buildTiles() {
         if (c.periodic && cover(per, m, static_cast<long long>(c.ni) * c.nj, kPeriodicTile) != c.per_tiles)
             throw std::logic_error("periodic tile count mismatch");
         inst.push_back({m, 0, 0, 1});
-        for (int b = 0; b < 8; b++) {
-            bintAll.push_back({m, b, 0, 1});
-            if (c.need_turbo) bint.push_back({m, b, 0, 1});
-        }
+        for (int b = 0; b < 8; b++)
+            for (int k = c.bint_off[b]; k < c.bint_off[b + 1]; k++) {
+                const Tile t{m, b, static_cast<long long>(k - c.bint_off[b]) * kBintChunk, kBintChunk};
+                bintAll.push_back(t);
+                if (c.need_turbo) bint.push_back(t);
+            }
     }
     view_.fusedSmem = smem;
     std::vector<Tile> all;

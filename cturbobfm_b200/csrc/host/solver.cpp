@@ -1004,6 +1004,22 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         c.bsy[b] = inst.uploadD(sy);
         c.bsz[b] = inst.uploadD(sz);
     }
+    {  // chunks of the eight boundary integrals (k_bint / k_pre)
+        auto points = [&](int plane) -> long {
+            if (plane <= 1) return NJ * NK;
+            if (plane <= 3) return NI * NK;
+            return NI * NJ;
+        };
+        const int td = c.turbo_dir;
+        const int turbo[2] = {td == 1 ? 1 : (td == 2 ? 2 : (td == 3 ? 3 : 0)),
+                              td == 1 ? 0 : (td == 2 ? 3 : (td == 3 ? 2 : 1))};
+        c.bint_off[0] = 0;
+        for (int b = 0; b < 8; b++) {
+            const long p = points(b < 6 ? b : turbo[b - 6]);
+            c.bint_off[b + 1] = c.bint_off[b] + static_cast<int>((p + kBintChunk - 1) / kBintChunk);
+        }
+        c.bint_part = inst.allocD(static_cast<size_t>(c.bint_off[8]) * 4);
+    }
     // BFM fields (include/types.hpp:1036-1078 names)
     c.blk = c.gbx = c.gby = c.gbz = c.nax = c.nrad = c.ntan = c.rpm = c.stwl = c.bpresent = c.nblades = nullptr;
     c.cosmetal = c.devpivot = c.devstall = c.ldbeta0 = c.ldkp = c.dangmom = c.dentropy = nullptr;
