@@ -472,27 +472,49 @@ __device__ __forceinline__ void b_faces(const DevCaseT<R>& c, const Tile& tl, in
                                     load5(c.W, qL), load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5<R>(), n);
                 }
             } else {
+                // the three real stencil nodes take the primitives (and, for
+                // JST, pressures and spectral radii) stored per node, the same
+                // values as converting their states here; only the ghost state
+                // (extrapolated, or rotated across the periodic seam) is
+                // converted
                 const S5<R> Ul = load5(U, qL), Ur = load5(U, qR);
                 S5<R> Ull, Urr;
+                long long qReal;  // the real outer node: qL - st (ghost on the right) or qR + st
+                const bool ghostLeft = dface == 1;
                 if (DIR == 2 && c.periodic) {
-                    if (dface == 1) {
+                    if (ghostLeft) {
                         Ull = rotState(load5(U, nodeIdx(c, fi, fj, c.nk - 2)), R(c.per_cos_m), R(c.per_sin_m));
-                        Urr = load5(U, qR + 1);
+                        qReal = qR + 1;
+                        Urr = load5(U, qReal);
                     } else {  // dface == nlast - 1
-                        Ull = load5(U, qR - 2);
+                        qReal = qR - 2;
+                        Ull = load5(U, qReal);
                         Urr = rotState(load5(U, nodeIdx(c, fi, fj, 1)), R(c.per_cos_p), R(c.per_sin_p));
                     }
                 } else {
-                    if (dface == 1) {
+                    if (ghostLeft) {
                         Ull = Ul - (Ur - Ul);
-                        Urr = load5(U, qR + st);
+                        qReal = qR + st;
+                        Urr = load5(U, qReal);
                     } else {  // dface == nlast - 1
-                        Ull = load5(U, qL - st);
+                        qReal = qL - st;
+                        Ull = load5(U, qReal);
                         Urr = Ur + (Ur - Ul);
                     }
                 }
-                if (SCHEME == 0) flux = fluxJst(gs, Ull, Ul, Ur, Urr, n);
-                else flux = fluxRoe(gs, c.muscl, c.limiter, Ull, Ul, Ur, Urr, n);
+                const S5<R> Wl = load5(c.W, qL), Wr = load5(c.W, qR);
+                if (SCHEME == 0) {
+                    const S5<R> Wg = primOf(ghostLeft ? Ull : Urr);
+                    const R pg = pressurePrim(gs, Wg), pReal = CTBFM_LDS(c.Wp + qReal);
+                    flux = fluxJstPR(gs, Ull, Ul, Ur, Urr, Wl, Wr, ghostLeft ? pg : pReal, CTBFM_LDS(c.Wp + qL),
+                                     CTBFM_LDS(c.Wp + qR), ghostLeft ? pReal : pg, CTBFM_LDS(c.Wr + qL),
+                                     CTBFM_LDS(c.Wr + qR), n);
+                } else if (c.muscl) {
+                    const S5<R> Wg = primOf(ghostLeft ? Ull : Urr), Wreal = load5(c.W, qReal);
+                    flux = fluxRoeW(gs, 1, c.limiter, ghostLeft ? Wg : Wreal, Wl, Wr, ghostLeft ? Wreal : Wg, n);
+                } else {
+                    flux = fluxRoeW(gs, 0, c.limiter, zero5<R>(), Wl, Wr, zero5<R>(), n);
+                }
             }
         }
 #pragma unroll
@@ -596,8 +618,11 @@ __device__ __forceinline__ void b_nodes(const DevCaseT<R>& c, const Tile& tl, in
             }
         }
         if (c.viscous) addViscousResidual(c, i, j, k, Res);
-        const S5<R> Unode = load5(Uin, q);
-        applySources<BX>(c, gs, Uin, i, j, k, q, Unode, t, Res);
+        if (hasSources(c)) {  // the stage input's primitives (and JST pressure) stored per node
+            const S5<R> Wn = load5(c.W, q);
+            const R pn = c.Wp ? CTBFM_LDS(c.Wp + q) : pressure_rho_u_et(gs, Wn.v[0], velOf(Wn), Wn.v[4]);
+            applySourcesW<BX>(c, gs, Uin, i, j, k, q, Wn, pn, t, Res);
+        }
         if (c.periodic && (k == 0 || k == nk - 1)) {
             const long long pq = (k == 0 ? 0 : c.n / nk) + static_cast<long long>(i) * nj + j;
             store5(c.Rp, pq, Res);

@@ -329,15 +329,12 @@ CTBFM_DI S5<R> bfmTotalSource(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int 
 }
 
 // Solver::computeSourceResiduals (src/solver.cpp:2790-2924) applied to one
-// node's residual R.
+// node's residual R, given the node's primitives W and pressure p of the
+// stage input (the values primOf and pressure_rho_u_et give for it).
 template <int BX, typename R>
-CTBFM_DI void applySources(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
-                           const S5<R>& Unode, double t, S5<R>& Res) {
-    if (c.topo == 1 && !c.bfm) return;
-    if (c.topo == 0 && !c.bfm) return;
-    const S5<R> W = primOf(Unode);
+CTBFM_DI void applySourcesW(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
+                            const S5<R>& W, R p, double t, S5<R>& Res) {
     const R vol = c.vol[q];
-    const R p = pressure_rho_u_et(gs, W.v[0], velOf(W), W.v[4]);
     bool geo = false, gong = false;
     if (c.topo == 1) geo = gong = (c.bpresent[q] > R(0));
     else if (c.topo == 2) geo = true;
@@ -369,6 +366,20 @@ CTBFM_DI void applySources(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, 
         const V3<R> gb = v3(c.gbx[q], c.gby[q], c.gbz[q]);
         if (mag(gb) > R(1E-10)) Res = Res - bfmTotalSource<BX>(c, gs, U, i, j, k, q, W, t);
     }
+}
+
+template <typename R>
+CTBFM_DI bool hasSources(const DevCaseT<R>& c) {
+    return c.topo == 2 || c.bfm;
+}
+
+// The same from the node's conservative stage input.
+template <int BX, typename R>
+CTBFM_DI void applySources(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
+                           const S5<R>& Unode, double t, S5<R>& Res) {
+    if (!hasSources(c)) return;
+    const S5<R> W = primOf(Unode);
+    applySourcesW<BX>(c, gs, U, i, j, k, q, W, pressure_rho_u_et(gs, W.v[0], velOf(W), W.v[4]), t, Res);
 }
 
 }  // namespace ctbfm

@@ -236,7 +236,9 @@ void GroupT<R>::buildTiles() {
                                                    : (d == 1 ? static_cast<long long>(c.ni) * c.nk
                                                              : static_cast<long long>(c.ni) * c.nj);
                     cover(face[mode][d][c.scheme][1], m, lines * (nline - 3), faceTile_[d]);
-                    cover(face[mode][d][c.scheme][2], m, lines * 4, faceTile_[d]);
+                    // the end faces are few and carry the boundary code:
+                    // one per thread, whatever the plain faces' tile
+                    cover(face[mode][d][c.scheme][2], m, lines * 4, kTileSize);
                 }
             }
         }
