@@ -196,6 +196,13 @@ struct alignas(16) DevCaseT {
     const R* nrad;
     const R* ntan;
     const R* rpm;
+    // per-node quantities of the blade fields alone, computed once on the
+    // host with the operations the force evaluates per stage (bit for bit in
+    // FP64): the camber normal over its magnitude (x/0 where the magnitude
+    // is 0), the blade pitch 2 pi r / N and the shaft speed rpm 2 pi / 60
+    const R* nhat[3];
+    const R* pitch;
+    const R* omega0;
     const R* stwl;
     const R* bpresent;
     const R* nblades;

@@ -54,10 +54,10 @@ struct BfmState {
     V3<R> relCyl, relCart, nCyl, invDirCyl, viscDirCyl;
 };
 
-// SourceBFMBase::computeDeviationAngle (src/source_bfm_base.cpp:152-166).
+// SourceBFMBase::computeDeviationAngle (src/source_bfm_base.cpp:152-166),
+// given the camber normal over its magnitude nn.
 template <typename R>
-CTBFM_DI R bfmDeviation(V3<R> rel, V3<R> ncam) {
-    const V3<R> nn = ncam / mag(ncam);
+CTBFM_DI R bfmDeviation(V3<R> rel, V3<R> nn) {
     const V3<R> vm = v3(rel.x, rel.y, R(0));
     V3<R> span = v3(-vm.y, vm.x, R(0));
     span = span / mag(span);
@@ -66,11 +66,11 @@ CTBFM_DI R bfmDeviation(V3<R> rel, V3<R> ncam) {
     return -asin(nv / mag(vin));
 }
 
-// SourceBFMBase::computeInviscidForceDirection (src/source_bfm_base.cpp:168-199).
+// SourceBFMBase::computeInviscidForceDirection (src/source_bfm_base.cpp:168-199),
+// given the normalized camber normal nd (zero for a zero normal).
 template <typename R>
-CTBFM_DI V3<R> bfmInviscidDir(const DevCaseT<R>& c, V3<R> rel, V3<R> ncam, R dev, long long q) {
+CTBFM_DI V3<R> bfmInviscidDir(const DevCaseT<R>& c, V3<R> rel, V3<R> nd, R dev, long long q) {
     const V3<R> rd = normalized(rel);
-    const V3<R> nd = normalized(ncam);
     V3<R> ver;
     if (c.stalled && dev > c.devstall[q]) ver = nd;
     else ver = normalized(nd - rd * dot(nd, rd));
@@ -85,16 +85,19 @@ CTBFM_DI void bfmFlowState(const DevCaseT<R>& c, long long q, const S5<R>& W, do
     b.cth = c.cost[q];
     b.sth = c.sint[q];
     const V3<R> velCyl = cylOfCart(velOf(W), b.cth, b.sth);
-    b.omega = c.rpm[q] * R(2) * R(M_PI) / R(60);
+    b.omega = c.omega0[q];  // rpm 2 pi / 60
     b.omega *= R(speedScaling(c, t));
     const V3<R> drag = v3(R(0), R(0), b.omega * b.radius);
     b.relCyl = velCyl - drag;
     b.relCart = cartOfCyl(b.relCyl, b.cth, b.sth);
     const R vmer = sqrt(velCyl.x * velCyl.x + velCyl.y * velCyl.y);
     b.vmer = vmer;
-    const R nb = c.nblades[q];
-    b.pitch = R(2) * R(M_PI) * b.radius / nb;
+    b.pitch = c.pitch[q];  // 2 pi r / N
     b.nCyl = v3(c.nax[q], c.nrad[q], c.ntan[q]);
+    // the camber normal over its magnitude; normalized() gives zero where the
+    // magnitude is zero, which the division leaves non-finite
+    const V3<R> nn = v3(c.nhat[0][q], c.nhat[1][q], c.nhat[2][q]);
+    const bool finite = isfinite(nn.x) && isfinite(nn.y) && isfinite(nn.z);
     b.blockage = c.blk[q];
     if (c.bfm_model == 3) {  // only Lift-Drag reads the staggered pitch and flow angle
         b.staggered = b.pitch * c.cosmetal[q];
@@ -103,8 +106,8 @@ CTBFM_DI void bfmFlowState(const DevCaseT<R>& c, long long q, const S5<R>& W, do
         b.staggered = R(0);
         b.flowAngle = R(0);
     }
-    b.dev = bfmDeviation(b.relCyl, b.nCyl);
-    b.invDirCyl = bfmInviscidDir(c, b.relCyl, b.nCyl, b.dev, q);
+    b.dev = bfmDeviation(b.relCyl, nn);
+    b.invDirCyl = bfmInviscidDir(c, b.relCyl, finite ? nn : v3(R(0), R(0), R(0)), b.dev, q);
     b.viscDirCyl = -normalized(b.relCyl);
 }
 

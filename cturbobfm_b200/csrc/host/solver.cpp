@@ -1022,6 +1022,7 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
     }
     // BFM fields (include/types.hpp:1036-1078 names)
     c.blk = c.gbx = c.gby = c.gbz = c.nax = c.nrad = c.ntan = c.rpm = c.stwl = c.bpresent = c.nblades = nullptr;
+    c.nhat[0] = c.nhat[1] = c.nhat[2] = c.pitch = c.omega0 = nullptr;
     c.cosmetal = c.devpivot = c.devstall = c.ldbeta0 = c.ldkp = c.dangmom = c.dentropy = nullptr;
     c.chima_mf = c.chima_turn = c.chima_loss = nullptr;
     c.metal = nullptr;
@@ -1050,6 +1051,27 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
             c.nrad = need("normalRadial");
             c.ntan = need("normalTangential");
             c.rpm = need("rpm");
+            {  // bfmFlowState's per-node constants, in the device's operation order
+                const auto& nx = mesh_.field("normalAxial");
+                const auto& ny = mesh_.field("normalRadial");
+                const auto& nz = mesh_.field("normalTangential");
+                const auto& nbl = mesh_.field("numberBlades");
+                const auto& rpm = mesh_.field("rpm");
+                std::vector<double> hx(N), hy(N), hz(N), pitch(N), om(N);
+                for (long q = 0; q < N; q++) {
+                    const double m = std::sqrt(nx[q] * nx[q] + ny[q] * ny[q] + nz[q] * nz[q]);
+                    hx[q] = nx[q] / m;
+                    hy[q] = ny[q] / m;
+                    hz[q] = nz[q] / m;
+                    pitch[q] = 2.0 * M_PI * rad[q] / nbl[q];
+                    om[q] = rpm[q] * 2.0 * M_PI / 60.0;
+                }
+                c.nhat[0] = inst.uploadR(hx);
+                c.nhat[1] = inst.uploadR(hy);
+                c.nhat[2] = inst.uploadR(hz);
+                c.pitch = inst.uploadR(pitch);
+                c.omega0 = inst.uploadR(om);
+            }
             mesh_.field("bladeLeanAngle");
             mesh_.field("bladeGasPathAngle");
             const auto& metal = mesh_.field("bladeMetalAngle");

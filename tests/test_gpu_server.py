@@ -131,15 +131,35 @@ def test_node_limit_admits_in_arrival_order(tmp_path):
     assert all(r["status"] == 1 for r in res.values())
 
 
+def _pressures_scaled(c, f):
+    """The same flow with every pressure (initial state, inlet total and
+    outlet static pressure) multiplied by f: an ideal-gas Euler solution
+    scales with it, density and energy with it, velocities and temperatures
+    unchanged."""
+    import dataclasses
+
+    st = dict(c.settings)
+    st["INIT_PRESSURE"] = repr(float(st["INIT_PRESSURE"]) * f)
+    patches = []
+    for p in c.patches:
+        parts = [x.strip() for x in p.spec.split(",")]
+        if parts[0] in ("inlet", "outlet"):
+            parts[1] = repr(float(parts[1]) * f)
+        patches.append(dataclasses.replace(p, spec=", ".join(parts)))
+    return dataclasses.replace(c, settings=st, patches=patches)
+
+
 def test_diverged_fp32_solve_is_run_again_in_fp64(tmp_path):
-    """A 3-D request of the serving mix (JST, RK4, CFL 2.2) whose fp32_kahan
-    solve blows up in its start-up transient while the FP64 solve converges:
-    a server allowed to move float solves to FP64 (stall_window > 0) runs it
-    again from its initial state in FP64, and the result is that of the
-    plain FP64 solve."""
+    """A request whose fp32_kahan solve diverges while the FP64 solve
+    converges: the bump channel with its pressures scaled by 1e36, so that
+    the energy (about 2.5e41) overflows float at once while FP64 solves the
+    scaled flow. A server allowed to move float solves to FP64
+    (stall_window > 0) runs it again from its initial state in FP64, and the
+    result is that of the plain FP64 solve."""
     from cturbobfm_b200 import Server, SolverDiverged, Solver
 
-    c = [c for _, c in cases.serving_requests(48, 5.0) if c.shape[2] > 1][1]
+    c = _pressures_scaled(cases.bump2d(ni=48, nj=20), 1e36).with_settings(
+        GPU_PRECISION="fp32_kahan", RESIDUALS_DROP_CONVERGENCE="2", N_ITERATIONS="10000")
     ini32 = _write(c, str(tmp_path / "f32"))
     with Solver(ini32) as s:
         with pytest.raises(SolverDiverged):
