@@ -851,6 +851,11 @@ template <typename R, int FL>
 __device__ __forceinline__ void b_bint(const DevCaseT<R>& c, const Tile& tl) {
     const Gas<double> gs{c.gamma, c.rgas, FL ? c.lut : nullptr};
     const int blk = tl.local;
+    // in 2-D the K_START and K_END planes are the same nodes (with other
+    // surface vectors): the plane-4 blocks sum both, K_END's mass flow in
+    // their second sum, and the plane-5 blocks have nothing to do
+    const bool pairK = blk == 4 && c.nk == 1;
+    if (blk == 5 && c.nk == 1) return;
     const int plane = blk < 6 ? blk : turboPlane(c, blk - 6);
     int na, nb;
     planeExtent(c, plane, na, nb);
@@ -864,6 +869,7 @@ __device__ __forceinline__ void b_bint(const DevCaseT<R>& c, const Tile& tl) {
         const S5<double> Uq = state64(c, c.U, q);
         if (blk < 6) {
             s[0] += sx * Uq.v[1] + sy * Uq.v[2] + sz * Uq.v[3];
+            if (pairK) s[1] += c.bsx[5][e] * Uq.v[1] + c.bsy[5][e] * Uq.v[2] + c.bsz[5][e] * Uq.v[3];
         } else {
             const S5<double> W = primOf(Uq);
             const double rho = W.v[0];
@@ -895,10 +901,14 @@ __device__ __forceinline__ void combineBoundaryIntegrals(const DevCaseT<R>& c) {
     Control* ctl = c.ctl;
     for (int b = 0; b < 8; b++) {
         double s[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int k = c.bint_off[b]; k < c.bint_off[b + 1]; k++)
+        const bool pairK = b == 5 && c.nk == 1;  // K_END summed by the K_START blocks (second sum)
+        const int src = pairK ? 4 : b;
+        for (int k = c.bint_off[src]; k < c.bint_off[src + 1]; k++)
 #pragma unroll
             for (int v = 0; v < 4; v++) s[v] += c.bint_part[k * 4 + v];
-        if (b < 6) {
+        if (pairK) {
+            ctl->massflow[5] = s[1];
+        } else if (b < 6) {
             ctl->massflow[b] = s[0];
         } else {
             ctl->pt_int[b - 6] = s[0];
