@@ -79,26 +79,64 @@ CTBFM_DI V3<R> bfmInviscidDir(const DevCaseT<R>& c, V3<R> rel, V3<R> nd, R dev, 
     return normalized(ver - sd * dot(ver, sd));
 }
 
+// A node's blade fields, loaded together before the tests that decide
+// whether they are used (blockage gradient, blade count), so that the loads
+// overlap instead of waiting on one another.
 template <typename R>
-CTBFM_DI void bfmFlowState(const DevCaseT<R>& c, long long q, const S5<R>& W, double t, BfmState<R>& b) {
-    b.radius = c.radius[q];
-    b.cth = c.cost[q];
-    b.sth = c.sint[q];
+struct BfmNode {
+    V3<R> gb;  // blockage gradient
+    R blk, nbl;
+    R radius, cth, sth, omega0, pitch;  // the force models' fields (zero for None / Blockage)
+    V3<R> n, nhat;
+};
+
+template <typename R>
+CTBFM_DI bool bfmForceModel(const DevCaseT<R>& c) {
+    return c.bfm_model == 1 || c.bfm_model == 2 || c.bfm_model == 3 || c.bfm_model == 5 || c.bfm_model == 6;
+}
+
+template <typename R>
+CTBFM_DI BfmNode<R> loadBfmNode(const DevCaseT<R>& c, long long q) {
+    BfmNode<R> f;
+    f.gb = v3(c.gbx[q], c.gby[q], c.gbz[q]);
+    f.blk = c.blk[q];
+    f.nbl = c.nblades[q];
+    if (bfmForceModel(c)) {
+        f.radius = c.radius[q];
+        f.cth = c.cost[q];
+        f.sth = c.sint[q];
+        f.omega0 = c.omega0[q];
+        f.pitch = c.pitch[q];
+        f.n = v3(c.nax[q], c.nrad[q], c.ntan[q]);
+        f.nhat = v3(c.nhat[0][q], c.nhat[1][q], c.nhat[2][q]);
+    } else {
+        f.radius = f.cth = f.sth = f.omega0 = f.pitch = R(0);
+        f.n = f.nhat = v3(R(0), R(0), R(0));
+    }
+    return f;
+}
+
+template <typename R>
+CTBFM_DI void bfmFlowState(const DevCaseT<R>& c, long long q, const S5<R>& W, double t, const BfmNode<R>& f,
+                           BfmState<R>& b) {
+    b.radius = f.radius;
+    b.cth = f.cth;
+    b.sth = f.sth;
     const V3<R> velCyl = cylOfCart(velOf(W), b.cth, b.sth);
-    b.omega = c.omega0[q];  // rpm 2 pi / 60
+    b.omega = f.omega0;  // rpm 2 pi / 60
     b.omega *= R(speedScaling(c, t));
     const V3<R> drag = v3(R(0), R(0), b.omega * b.radius);
     b.relCyl = velCyl - drag;
     b.relCart = cartOfCyl(b.relCyl, b.cth, b.sth);
     const R vmer = sqrt(velCyl.x * velCyl.x + velCyl.y * velCyl.y);
     b.vmer = vmer;
-    b.pitch = c.pitch[q];  // 2 pi r / N
-    b.nCyl = v3(c.nax[q], c.nrad[q], c.ntan[q]);
+    b.pitch = f.pitch;  // 2 pi r / N
+    b.nCyl = f.n;
     // the camber normal over its magnitude; normalized() gives zero where the
     // magnitude is zero, which the division leaves non-finite
-    const V3<R> nn = v3(c.nhat[0][q], c.nhat[1][q], c.nhat[2][q]);
+    const V3<R> nn = f.nhat;
     const bool finite = isfinite(nn.x) && isfinite(nn.y) && isfinite(nn.z);
-    b.blockage = c.blk[q];
+    b.blockage = f.blk;
     if (c.bfm_model == 3) {  // only Lift-Drag reads the staggered pitch and flow angle
         b.staggered = b.pitch * c.cosmetal[q];
         b.flowAngle = atan2(b.relCyl.z, vmer);
@@ -239,12 +277,12 @@ __device__ __noinline__ S5<R> correlationsForce(const DevCaseT<R>& c, Gas<R> gs,
 // (src/source_bfm_lift_drag.cpp:3-88).
 template <int BX, typename R>
 CTBFM_DI S5<R> bfmBodyForce(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
-                            const S5<R>& W, double t) {
+                            const S5<R>& W, double t, const BfmNode<R>& f) {
     // SourceBFMBase::computeBodyForceSource: no force for "None" / "Blockage"
     if (c.bfm_model != 1 && c.bfm_model != 2 && c.bfm_model != 3 && c.bfm_model != 5 && c.bfm_model != 6)
         return zero5<R>();
     BfmState<R> b;
-    bfmFlowState(c, q, W, t, b);
+    bfmFlowState(c, q, W, t, f, b);
     const R vol = c.vol[q];
     if (BX) {  // the node-kernel variant of the Chima and Correlations models
         if (c.bfm_model == 5) return chimaForce(c, gs, j, k, q, W, b, vol);
@@ -316,17 +354,16 @@ CTBFM_DI R bfmPerturbation(const DevCaseT<R>& c, long long q, double t) {
 // SourceBFMBase::computeTotalSource (src/source_bfm_base.cpp:25-84).
 template <int BX, typename R>
 CTBFM_DI S5<R> bfmTotalSource(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i, int j, int k, long long q,
-                              const S5<R>& W, double t) {
+                              const S5<R>& W, double t, const BfmNode<R>& f) {
     S5<R> blk = zero5<R>();
     if (c.blockage) {
         const V3<R> u = velOf(W);
         const R ht = totalEnthalpy_rho_u_et(gs, W.v[0], u, W.v[4]);
-        const V3<R> gb = v3(c.gbx[q], c.gby[q], c.gbz[q]);
-        const R ct = R(-1) / c.blk[q] * W.v[0] * dot(u, gb);
+        const R ct = R(-1) / f.blk * W.v[0] * dot(u, f.gb);
         blk = s5(ct, ct * u.x, ct * u.y, ct * u.z, ct * ht) * c.vol[q];
     }
-    if (c.nblades[q] == R(0)) return blk;
-    const S5<R> bf = bfmBodyForce<BX>(c, gs, U, i, j, k, q, W, t);
+    if (f.nbl == R(0)) return blk;
+    const S5<R> bf = bfmBodyForce<BX>(c, gs, U, i, j, k, q, W, t, f);
     const R pf = bfmPerturbation(c, q, t);
     return blk + bf * (R(1) + pf);
 }
@@ -366,8 +403,8 @@ CTBFM_DI void applySourcesW(const DevCaseT<R>& c, Gas<R> gs, R* const* U, int i,
         Res = Res - gongSource(c, U, om, i, j, k, vol);
     }
     if (c.bfm) {
-        const V3<R> gb = v3(c.gbx[q], c.gby[q], c.gbz[q]);
-        if (mag(gb) > R(1E-10)) Res = Res - bfmTotalSource<BX>(c, gs, U, i, j, k, q, W, t);
+        const BfmNode<R> f = loadBfmNode(c, q);
+        if (mag(f.gb) > R(1E-10)) Res = Res - bfmTotalSource<BX>(c, gs, U, i, j, k, q, W, t, f);
     }
 }
 
