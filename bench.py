@@ -634,6 +634,62 @@ def _serve_map(cases32, chunk: int, stall: int, host_threads: int = 8):
             "server_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in stats.items()}}
 
 
+MAPSTEP_METRIC = "batched map iteration time"
+
+
+def run_mapstep(args):
+    """One batched chunk of the compressor map: the first --map-n instances of
+    the map workload in one batch (--map-precision, stage kernels forced with
+    --stage or autotuned), --warmup untimed iterations, then --steps timed
+    iterations between cudaProfilerStart / Stop (a profiler run with
+    --profile-from-start off records exactly those launches). Prints the
+    device time per batched iteration."""
+    import torch
+
+    from cturbobfm_b200 import Batch, Solver, cases
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    cs = cases.compressor_map(n=args.map_n, precision=args.map_precision, drop=args.map_drop)
+    tmp = tempfile.TemporaryDirectory()
+    solvers = []
+    for i, c in enumerate(cs):
+        c = c.with_settings(GPU_STAGE_FUSION=args.stage)
+        d = os.path.join(tmp.name, str(i))
+        os.makedirs(d)
+        solvers.append(Solver(c.write(d)))
+    stream = torch.cuda.Stream()
+    nodes = sum(c.n_nodes for c in cs)
+    try:
+        with Batch(solvers) as b:
+            b.set_stream(stream.cuda_stream)
+            b.autotune()
+            b.step(args.warmup)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.profiler.start()
+            e0.record(stream)
+            b.enqueue(args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+            ms = e0.elapsed_time(e1) / args.steps
+            mode, stage_ms = b.stage_kernels()
+    finally:
+        for s in solvers:
+            s.close()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": MAPSTEP_METRIC, "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.map_precision == "fp64" else "f32+kahan (f64 integrals)", "data": "synthetic",
+        "config": {"workload": f"the first {args.map_n} instances of the compressor map, one batch, "
+                               f"{args.map_precision}", "nodes": nodes,
+                   "node_stage_per_s": nodes * 4 / (ms / 1e3), "stage_kernels": mode, "stage_autotuned_ms": stage_ms},
+    }))
+
+
 def map_cpu_baseline(inis, iterations, n_iter: int):
     """Converged op-points/hour of the reference build on the host cores: one
     single-threaded process per instance, all at once (the way the
@@ -1122,10 +1178,15 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["annulus", "map", "serve", "realgas", "viscous"], default="annulus",
+    ap.add_argument("--workload", choices=["annulus", "map", "mapstep", "serve", "realgas", "viscous"],
+                    default="annulus",
                     help="annulus: the 160x48x64 full-annulus loop (default); map: the batched compressor map; "
                          "serve: continuous batching of arriving requests")
     ap.add_argument("--map-n", type=int, default=256)
+    ap.add_argument("--map-precision", choices=["fp64", "fp32_kahan"], default="fp32_kahan",
+                    help="mapstep: the batch's GPU_PRECISION")
+    ap.add_argument("--stage", choices=["auto", "split", "fused", "persistent"], default="auto",
+                    help="mapstep: GPU_STAGE_FUSION of every member")
     ap.add_argument("--map-drop", type=int, default=4, help="RESIDUALS_DROP_CONVERGENCE of the map instances")
     ap.add_argument("--map-stall", type=int, default=3000,
                     help="float members without 0.05 orders of progress for this many iterations move to FP64")
@@ -1154,6 +1215,8 @@ def main():
         run_reference_arm(args)
     elif args.workload == "map":
         run_map(args)
+    elif args.workload == "mapstep":
+        run_mapstep(args)
     elif args.workload == "serve":
         run_serve(args)
     elif args.workload == "realgas":
