@@ -526,7 +526,8 @@ def _solve_batched(solvers, stream, chunk: int, n_iter: int, case):
     return status, iters, launches, first
 
 
-def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: int, stall: int):
+def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: int, stall: int,
+                          promote: float = 1.0):
     """The precision pattern on the map: every member runs batched in
     fp32_kahan until it is within one order of its residual drop (best_drop
     >= drop - 1), stops progressing (best_drop grew by less than 0.05 orders
@@ -574,7 +575,7 @@ def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: 
                     bd = st["best_drop"][j]
                     if bd >= mark[i] + 0.05:
                         mark[i], mark_it[i] = bd, iters[i]
-                    if bd >= drop - 1 or iters[i] - mark_it[i] >= stall:
+                    if bd >= drop - promote or iters[i] - mark_it[i] >= stall:
                         ready[i] = True
                 out = [i for i in active if status[i] != 0 or iters[i] >= n_iter or ready[i]]
                 if len(out) * 4 >= start or len(out) == len(active):
@@ -598,7 +599,7 @@ def _solve_fp32_then_fp64(solvers, stream, chunk: int, n_iter: int, case, drop: 
     return status, iters, launches, first, len(promote), fp64_iters
 
 
-def _serve_map(cases32, chunk: int, stall: int, host_threads: int = 8):
+def _serve_map(cases32, chunk: int, stall: int, promote: float = 1.0, host_threads: int = 8):
     """The precision pattern through the serving API: every instance
     submitted from memory (ctbfm_server_submit_case) at once to a Server
     that prepares them on host threads, admits them as they are ready, runs
@@ -613,7 +614,7 @@ def _serve_map(cases32, chunk: int, stall: int, host_threads: int = 8):
 
     w0 = time.perf_counter()
     res = {}
-    with Server(chunk=chunk, stall_window=stall, host_threads=host_threads, promote_orders=1.0) as srv:
+    with Server(chunk=chunk, stall_window=stall, host_threads=host_threads, promote_orders=promote) as srv:
         ids = [srv.submit_case(c) for c in cases32]
         while len(res) < len(ids) and time.perf_counter() - w0 < 1200:
             active, _ = srv.pump()
@@ -779,7 +780,8 @@ def map_line(args):
             promoted, fp64_iters = 0, 0
             if arm == "batched_fp32_kahan":
                 status, iters, launches, kern, promoted, fp64_iters = _solve_fp32_then_fp64(
-                    solvers, stream, args.map_chunk, n_iter, cs32[0], args.map_drop, args.map_stall)
+                    solvers, stream, args.map_chunk, n_iter, cs32[0], args.map_drop, args.map_stall,
+                    args.map_promote)
             else:
                 status, iters, launches, kern = _solve_batched(solvers, stream, args.map_chunk, n_iter, cs32[0])
             e1.record(stream)
@@ -801,7 +803,7 @@ def map_line(args):
                             "device_bytes": bytes_up, "promoted_to_fp64": promoted,
                             "fp64_iteration_share": fp64_iters / max(1, int(iters.sum())), **kern}
         if not args.map_skip_served:
-            results["served_fp32_kahan"] = _serve_map(cs32, args.map_chunk, args.map_stall)
+            results["served_fp32_kahan"] = _serve_map(cs32, args.map_chunk, args.map_stall, args.map_promote)
         # the plain FP64 path: one drop-in solver at a time, to convergence
         sample = list(range(min(args.map_plain, len(inis64))))
         plain_sec, plain_conv, plain = 0.0, 0, []
@@ -853,8 +855,9 @@ def map_line(args):
                                                    "stage_autotuned_ms", "promoted_to_fp64",
                                                    "fp64_iteration_share", "promote_s", "batches",
                                                    "batches_fp64") if k in r32},
-        "precision_pattern": ("fp32_kahan for every instance until it is within one order of the residual drop or "
-                              f"stalls for {args.map_stall} iterations, then the same solve continued in FP64 from "
+        "precision_pattern": (f"fp32_kahan for every instance until it is within {args.map_promote:g} orders of the "
+                              f"residual drop or stalls for {args.map_stall} iterations, then the same solve continued "
+                              "in FP64 from "
                               "its current state to convergence (FP64 convergence test and converged state)"),
         "plain_fp64": {"points_per_hour": plain_pph, "instances": len(sample), "converged": plain_conv,
                        "seconds": plain_sec, "iterations": [p[1] for p in plain]},
@@ -1194,6 +1197,8 @@ def main():
                     help="also run the map in fp32_kahan alone (no FP64 finish)")
     ap.add_argument("--no-map", action="store_true", help="leave the compressor-map object out of the default line")
     ap.add_argument("--map-chunk", type=int, default=250)
+    ap.add_argument("--map-promote", type=float, default=1.0,
+                    help="float members within this many orders of the residual drop move to FP64")
     ap.add_argument("--map-plain", type=int, default=8, help="instances solved one at a time on the plain FP64 path")
     ap.add_argument("--map-skip-fp64-batch", action="store_true")
     ap.add_argument("--map-skip-served", action="store_true",

@@ -793,25 +793,43 @@ void Solver::setupScalars() {
         } else {
             bks.push_back(1);
         }
-        for (int bk : bks)
-            for (int bj = 1; bj <= std::min(c.nj, 64); bj++)
-                for (int bi = 1; bi <= std::min(c.ni, kFusedBoxNodes / (bj * bk)); bi++) {
-                    const int nodes = bi * bj * bk;
-                    const int faces = (bi + 1) * bj * bk + bi * (bj + 1) * bk + (three ? bi * bj * (bk + 1) : 0);
-                    const int nW = nodes + 4 * bj * bk + 4 * bi * bk + (three ? 4 * bi * bj : 0);
-                    if (nodes > kFusedBoxNodes || faces > kFusedFaceCap) continue;
-                    if ((static_cast<size_t>(fields) * nW + 5 * static_cast<size_t>(faces)) * 8 > smemMax) continue;
-                    const double boxes = std::ceil(double(c.ni) / bi) * std::ceil(double(c.nj) / bj) *
-                                         std::ceil(double(c.nk) / bk);
-                    const double cost = std::ceil(faces / 256.0) + 0.15 * std::ceil(nW / 256.0) + 0.5;
-                    const double score = double(c.n) / boxes / cost;
-                    if (score > best + 1e-9) {
-                        best = score;
-                        bb[0] = bi;
-                        bb[1] = bj;
-                        bb[2] = bk;
+        // An instance whose best boxes would not give every SM a block runs
+        // latency-bound when alone: then the boxes that finish one stage in
+        // the fewest rounds of face evaluations (waves of 3 blocks per SM of
+        // a 148-SM device) are taken, the larger of equals.
+        constexpr double kSlots = 148.0 * 3.0;
+        for (int pass = 0; pass < 2; pass++) {
+            double bestTime = 1e30;
+            for (int bk : bks)
+                for (int bj = 1; bj <= std::min(c.nj, 64); bj++)
+                    for (int bi = 1; bi <= std::min(c.ni, kFusedBoxNodes / (bj * bk)); bi++) {
+                        const int nodes = bi * bj * bk;
+                        const int faces = (bi + 1) * bj * bk + bi * (bj + 1) * bk + (three ? bi * bj * (bk + 1) : 0);
+                        const int nW = nodes + 4 * bj * bk + 4 * bi * bk + (three ? 4 * bi * bj : 0);
+                        if (nodes > kFusedBoxNodes || faces > kFusedFaceCap) continue;
+                        if ((static_cast<size_t>(fields) * nW + 5 * static_cast<size_t>(faces)) * 8 > smemMax)
+                            continue;
+                        const double boxes = std::ceil(double(c.ni) / bi) * std::ceil(double(c.nj) / bj) *
+                                             std::ceil(double(c.nk) / bk);
+                        const double cost = std::ceil(faces / 256.0) + 0.15 * std::ceil(nW / 256.0) + 0.5;
+                        const double score = double(c.n) / boxes / cost;
+                        const double time = std::ceil(boxes / kSlots) * cost;
+                        const bool better = pass == 0 ? score > best + 1e-9
+                                                      : (time < bestTime - 1e-9 ||
+                                                         (time < bestTime + 1e-9 && score > best + 1e-9));
+                        if (better) {
+                            best = score;
+                            bestTime = time;
+                            bb[0] = bi;
+                            bb[1] = bj;
+                            bb[2] = bk;
+                        }
                     }
-                }
+            const double boxes = std::ceil(double(c.ni) / bb[0]) * std::ceil(double(c.nj) / bb[1]) *
+                                 std::ceil(double(c.nk) / bb[2]);
+            if (pass == 0 && (best < 0 || boxes >= 148.0)) break;
+            if (pass == 0) best = -1.0;
+        }
         if (best < 0) c.fuse_ok = 0;
         for (int d = 0; d < 3; d++) c.fbox[d] = bb[d];
     }
