@@ -380,6 +380,12 @@ void GroupT<R>::tune(cudaStream_t s) {
             graph1_ = nullptr;
         }
     }
+    // the iteration graphs of the chosen stage, captured now (capturing runs
+    // nothing), so that no later enqueue pays for the capture
+    if (!persist_) {
+        if (!graph_) graph_ = captureIterations(graphIters_);
+        if (!graph1_) graph1_ = captureIterations(1);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
 }
