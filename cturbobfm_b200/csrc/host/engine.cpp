@@ -222,13 +222,15 @@ void GroupT<R>::buildTiles() {
                 const long long nf =
                     static_cast<long long>(c.ni + (d == 0)) * (c.nj + (d == 1)) * (c.nk + (d == 2));
                 const int nline = d == 0 ? c.ni : (d == 1 ? c.nj : c.nk);  // nodes along a line of direction d
-                // K lines (and J lines whose rows of nk faces do not fill whole
-                // warps) run as two launches, plain faces 2 .. n-2 and the four
-                // end faces of every line, so the plain launch carries no
-                // boundary or extrapolation code; I faces and warp-aligned J rows
-                // run as one launch (splitting them measured slower: the four end
-                // planes of I make a large launch of boundary code)
-                const bool split = nline >= 3 && (d == 2 || (d == 1 && c.nk % 32 != 0));
+                // K lines (J lines whose rows of nk faces do not fill whole
+                // warps, and the I lines of 2-D grids) run as two launches,
+                // plain faces 2 .. n-2 and the four end faces of every line, so
+                // the plain launch carries no boundary or extrapolation code; 3-D
+                // I faces and warp-aligned J rows run as one launch (splitting
+                // them measured slower: the four end planes of 3-D I make a large
+                // launch of boundary code, 0.807 against 0.750 ms per iteration
+                // on the 160 x 48 x 64 annulus; 2-D map batch 2 % faster split)
+                const bool split = nline >= 3 && (d == 2 || (d == 1 && c.nk % 32 != 0) || (d == 0 && c.nk == 1));
                 if (!split) {
                     cover(face[mode][d][c.scheme][0], m, nf, faceTile_[d]);
                 } else {
