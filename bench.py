@@ -474,9 +474,15 @@ def run_ours(args):
 
 # ------------------------------------------------------------ compressor map
 MAP_METRIC = "converged op-points/hour"
-MAP_WORKLOAD = ("compressor map: 256 axisymmetric BFM instances (Hall, MAP_ROWS stage), NI x NJ ~ U{64..256} x "
-                "U{24..96}, p_out/pt_in ~ U[1.00,1.20], speed ~ U[0.85,1.00], PCG64 seed 20261203, JST, RK4, local dt "
+MAP_WORKLOAD = ("compressor map: {n} axisymmetric BFM instances (Hall, MAP_ROWS stage), NI x NJ ~ U{64..256} x "
+                "U{24..96}, p_out/pt_in ~ U[{p0},{p1}], speed ~ U[{s0},{s1}], PCG64 seed 20261203, JST, RK4, local dt "
                 "CFL 2.2, outlet ramp 2000 its, residual drop {drop} orders")
+
+
+def map_workload(args) -> str:
+    return (MAP_WORKLOAD.replace("{drop}", str(args.map_drop)).replace("{n}", str(args.map_n))
+            .replace("{p0}", f"{args.map_pratio[0]:.2f}").replace("{p1}", f"{args.map_pratio[1]:.2f}")
+            .replace("{s0}", f"{args.map_speed[0]:.2f}").replace("{s1}", f"{args.map_speed[1]:.2f}"))
 
 
 def _map_launches_per_iteration(case, mode: str) -> float:
@@ -752,7 +758,8 @@ def map_line(args):
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
-    cs32 = cases.compressor_map(n=args.map_n, precision="fp32_kahan", drop=args.map_drop)
+    cs32 = cases.compressor_map(n=args.map_n, precision="fp32_kahan", drop=args.map_drop,
+                                p_ratio_range=tuple(args.map_pratio), speed_range=tuple(args.map_speed))
     n_iter = int(cs32[0].settings["N_ITERATIONS"])
     tmp = tempfile.TemporaryDirectory()
 
@@ -843,7 +850,7 @@ def map_line(args):
         "steps": len(cs32), "warmup": 0, "ms_per_step": r32["seconds"] * 1e3 / max(1, len(cs32)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+kahan (f64 integrals)",
         "data": "synthetic",
-        "config": {"workload": MAP_WORKLOAD.replace("{drop}", str(args.map_drop)), "instances": len(cs32),
+        "config": {"workload": map_workload(args), "instances": len(cs32),
                    "nodes_total": int(nodes.sum()),
                    "chunk_iterations": args.map_chunk, "l2": "inputs larger than L2 (working set > 126 MiB)"},
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
@@ -1197,6 +1204,9 @@ def main():
     ap.add_argument("--stage", choices=["auto", "split", "fused", "persistent"], default="auto",
                     help="GPU_STAGE_FUSION of the timed solvers (mapstep: of every member; default: autotuned)")
     ap.add_argument("--map-drop", type=int, default=4, help="RESIDUALS_DROP_CONVERGENCE of the map instances")
+    ap.add_argument("--map-pratio", type=float, nargs=2, default=[1.00, 1.20],
+                    help="range of the outlet static pressure over the inlet total pressure")
+    ap.add_argument("--map-speed", type=float, nargs=2, default=[0.85, 1.00], help="range of the shaft-speed scaling")
     ap.add_argument("--map-stall", type=int, default=3000,
                     help="float members without 0.05 orders of progress for this many iterations move to FP64")
     ap.add_argument("--map-pure-fp32", action="store_true",
