@@ -91,6 +91,25 @@ def test_null_arguments(lib):
     assert lib.ctbfm_server_pump(None, None, None) == 4
     assert lib.ctbfm_server_results(None, None, 0, None) == 4
     lib.ctbfm_server_destroy(None)
+    assert lib.ctbfm_server_set_promotion(None, 1.0) == 4
+    assert lib.ctbfm_server_get_stats(None, None) == 4
+
+
+def test_server_promotion_and_statistics_arguments(lib):
+    import ctypes
+
+    from cturbobfm_b200 import Server, solver
+
+    with Server(chunk=10, host_threads=1) as s:
+        assert lib.ctbfm_server_set_promotion(s._h, -1.0) == 4
+        assert lib.ctbfm_server_set_promotion(s._h, float("nan")) == 4
+        assert lib.ctbfm_server_set_promotion(s._h, 0.5) == 0
+        assert lib.ctbfm_server_get_stats(s._h, None) == 4
+        st = s.stats()  # nothing pumped yet
+        assert st["rounds"] == 0 and st["rebuilds"] == 0 and st["promotions"] == 0
+        assert all(st[k] == 0.0 for k, _ in solver.ServerStats._fields_ if k.endswith("_s"))
+    with Server(chunk=10, host_threads=1, promote_orders=1.0) as s:
+        assert s.stats()["rounds"] == 0
 
 
 def test_server_reports_a_bad_request_without_device_work(lib, tmp_path):

@@ -222,3 +222,28 @@ def test_warm_started_request_is_the_same_alone_and_in_the_mix(tmp_path):
         assert r["iterations"] == plain[0]
         assert r["turbo"] == plain[1]
     assert first >= 0
+
+
+def test_float_solve_moves_to_fp64_within_an_order_of_its_drop(tmp_path):
+    """promote_orders = 1: a fp32_kahan request is paused on the device once
+    its best residual drop is within one order of RESIDUALS_DROP_CONVERGENCE,
+    its FP64 side built while the next chunk runs, and it converges in FP64;
+    the same request gives the same result alone and beside another one, and
+    the server statistics count the move."""
+    from cturbobfm_b200 import Server
+
+    a = _req("a", 64, 24, 1.05, 0.95, drop=4)
+    b = _req("b", 72, 26, 1.10, 0.90, drop=4)
+    ina, inb = _write(a, str(tmp_path)), _write(b, str(tmp_path))
+    with Server(chunk=100, promote_orders=1.0) as srv:
+        ra = srv.submit(ina)
+        alone = _drain(srv, 1)[ra]
+        st = srv.stats()
+    assert alone["status"] == 1 and alone["precision"] == 0 and alone["error"] == 0
+    assert st["promotions"] == 1 and st["rounds"] >= 1 and st["wait_s"] > 0
+    with Server(chunk=100, promote_orders=1.0) as srv:
+        ra, rb = srv.submit(ina), srv.submit(inb)
+        mix = _drain(srv, 2)
+    assert mix[ra]["iterations"] == alone["iterations"]
+    assert np.array_equal(np.array(mix[ra]["turbo"]), np.array(alone["turbo"]))
+    assert mix[rb]["status"] == 1 and mix[rb]["precision"] == 0
