@@ -48,6 +48,11 @@ struct DevFacesT {
     const R* ny;
     const R* nz;
     const R* area;
+    // Roe: the second vector of the face's normal triad, (-ny, nx, 0) over
+    // its magnitude ((1, 0, 0) for an axial normal), computed on the host
+    // with the device's operations; its z component is 0 (nullptr for JST)
+    const R* n2x;
+    const R* n2y;
     R* c[5];
 };
 

@@ -469,7 +469,8 @@ __device__ __forceinline__ void b_faces(const DevCaseT<R>& c, const Tile& tl, in
                                      CTBFM_LDS(c.Wr + qR), n);
                 } else {
                     flux = fluxRoeW(gs, c.muscl, c.limiter, c.muscl ? load5(c.W, qL - st) : zero5<R>(),
-                                    load5(c.W, qL), load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5<R>(), n);
+                                    load5(c.W, qL), load5(c.W, qR), c.muscl ? load5(c.W, qR + st) : zero5<R>(), n,
+                                    v3(__ldg(F.n2x + f), __ldg(F.n2y + f), R(0)));
                 }
             } else {
                 // the three real stencil nodes take the primitives (and, for
@@ -509,11 +510,15 @@ __device__ __forceinline__ void b_faces(const DevCaseT<R>& c, const Tile& tl, in
                     flux = fluxJstPR(gs, Ull, Ul, Ur, Urr, Wl, Wr, ghostLeft ? pg : pReal, CTBFM_LDS(c.Wp + qL),
                                      CTBFM_LDS(c.Wp + qR), ghostLeft ? pReal : pg, CTBFM_LDS(c.Wr + qL),
                                      CTBFM_LDS(c.Wr + qR), n);
-                } else if (c.muscl) {
-                    const S5<R> Wg = primOf(ghostLeft ? Ull : Urr), Wreal = load5(c.W, qReal);
-                    flux = fluxRoeW(gs, 1, c.limiter, ghostLeft ? Wg : Wreal, Wl, Wr, ghostLeft ? Wreal : Wg, n);
                 } else {
-                    flux = fluxRoeW(gs, 0, c.limiter, zero5<R>(), Wl, Wr, zero5<R>(), n);
+                    const V3<R> n2 = v3(__ldg(F.n2x + f), __ldg(F.n2y + f), R(0));
+                    if (c.muscl) {
+                        const S5<R> Wg = primOf(ghostLeft ? Ull : Urr), Wreal = load5(c.W, qReal);
+                        flux = fluxRoeW(gs, 1, c.limiter, ghostLeft ? Wg : Wreal, Wl, Wr, ghostLeft ? Wreal : Wg, n,
+                                        n2);
+                    } else {
+                        flux = fluxRoeW(gs, 0, c.limiter, zero5<R>(), Wl, Wr, zero5<R>(), n, n2);
+                    }
                 }
             }
         }

@@ -421,7 +421,20 @@ CTBFM_DI R roeAvg(R sl, R sr, R pl, R pr) {  // roeAverage with sl = sqrt(rhoL)
 // (include/advection_roe.hpp:63), on primitive states.
 template <typename R>
 CTBFM_DI S5<R> fluxRoeW(Gas<R> gs, int muscl, int lim, const S5<R>& Wll, S5<R> Wl, S5<R> Wr, const S5<R>& Wrr,
-                        V3<R> n1) {
+                        V3<R> n1, V3<R> n2);
+
+// The same, with the triad's second vector computed here from n1.
+template <typename R>
+CTBFM_DI S5<R> fluxRoeW(Gas<R> gs, int muscl, int lim, const S5<R>& Wll, const S5<R>& Wl, const S5<R>& Wr,
+                        const S5<R>& Wrr, V3<R> n1) {
+    // normal triad (:41-58); n1 = S.normalized() equals the stored unit normal
+    V3<R> n2 = (n1.x == R(0) && n1.y == R(0)) ? v3(R(1), R(0), R(0)) : v3(-n1.y, n1.x, R(0));
+    return fluxRoeW(gs, muscl, lim, Wll, Wl, Wr, Wrr, n1, normalized(n2));
+}
+
+template <typename R>
+CTBFM_DI S5<R> fluxRoeW(Gas<R> gs, int muscl, int lim, const S5<R>& Wll, S5<R> Wl, S5<R> Wr, const S5<R>& Wrr,
+                        V3<R> n1, V3<R> n2) {
     if (muscl) {
         S5<R> limL, limR;
 #pragma unroll
@@ -434,9 +447,6 @@ CTBFM_DI S5<R> fluxRoeW(Gas<R> gs, int muscl, int lim, const S5<R>& Wll, S5<R> W
 #pragma unroll
         for (int i = 0; i < 5; i++) Wr.v[i] -= limR.v[i] * (Wrr.v[i] - Wr.v[i]) * R(0.5);
     }
-    // normal triad (:41-58); n1 = S.normalized() equals the stored unit normal
-    V3<R> n2 = (n1.x == R(0) && n1.y == R(0)) ? v3(R(1), R(0), R(0)) : v3(-n1.y, n1.x, R(0));
-    n2 = normalized(n2);
     const V3<R> n3 = cross(n1, n2);
     const V3<R> uL = velOf(Wl), uR = velOf(Wr);
     const R rhoL = Wl.v[0], rhoR = Wr.v[0];

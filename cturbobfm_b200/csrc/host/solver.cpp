@@ -925,6 +925,22 @@ void Solver::uploadArrays(InstanceT<R>& inst) {
         c.f[d].ny = inst.uploadR(ny);
         c.f[d].nz = inst.uploadR(nz);
         c.f[d].area = inst.uploadR(ar);
+        c.f[d].n2x = c.f[d].n2y = nullptr;
+        if (c.scheme == 1) {  // AdvectionRoe's normal triad (src/advection_roe.cpp:41-58), second vector
+            std::vector<double> n2x(nx.size()), n2y(nx.size());
+            for (size_t f = 0; f < nx.size(); f++) {
+                double ax = -ny[f], ay = nx[f];
+                if (nx[f] == 0.0 && ny[f] == 0.0) {
+                    ax = 1.0;
+                    ay = 0.0;
+                }
+                const double m = std::sqrt(ax * ax + ay * ay + 0.0 * 0.0);
+                n2x[f] = m == 0.0 ? 0.0 : ax / m;
+                n2y[f] = m == 0.0 ? 0.0 : ay / m;
+            }
+            c.f[d].n2x = inst.uploadR(n2x);
+            c.f[d].n2y = inst.uploadR(n2y);
+        }
         for (int v = 0; v < 5; v++) c.f[d].c[v] = inst.allocR(S.size());
     }
     // per node: volume, radius, theta rotation, edges of the dual cell
