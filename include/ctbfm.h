@@ -156,9 +156,12 @@ int ctbfm_enqueue(ctbfm_solver* s, int64_t n_iter);
 
 /* Runs the autotuner now unless it has run (otherwise it runs at the first
  * enqueue of at least 64 iterations): face tiles per direction, and with
- * GPU_STAGE_FUSION = auto whether the fused or the split stage kernels are
- * faster, timed on forced first-stage evaluations that leave the state
- * unchanged. Synchronises the stream. No counterpart in the reference. */
+ * GPU_STAGE_FUSION = auto which of the split, fused and persistent stage
+ * kernels is fastest (the persistent kernel only where it is eligible: no
+ * real-gas table, viscosity or turbulence model, and in a batch one convection
+ * scheme for all members), timed on forced first-stage
+ * evaluations that leave the state unchanged. Synchronises the stream. No
+ * counterpart in the reference. */
 int ctbfm_autotune(ctbfm_solver* s);
 
 /* Runs the whole loop to N_ITERATIONS or convergence, like Solver::solve(). */
